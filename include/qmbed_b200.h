@@ -1,0 +1,195 @@
+/*
+ * qmbed_b200 — B200 (sm_100a) engine for QMBED's symmetry-reduced spin-chain
+ * Hamiltonian action and the Krylov solvers on it.
+ *
+ * Two C-ABI surfaces, both exported by libqmbed_b200.so:
+ *
+ *  1. The drop-in JSON boundary: the same six symbols the reference cdylib
+ *     `qmbed-capi` exports (bindings/capi/src/lib.rs:6089-6296) and that the
+ *     reference Python package binds at load time
+ *     (bindings/python/src/qmbed/_ffi.py:154-186). Requests and responses use
+ *     the reference JSON schema; a response string is owned by the caller
+ *     and released exactly once with qmbed_string_free.
+ *
+ *  2. A typed API (qmbed_gpu_*) over opaque handles with plain pointers and
+ *     sizes, used by the test suite and the benchmark. Every function returns
+ *     0 on success or a status code below; qmbed_gpu_last_error() returns the
+ *     message of the last failure on the calling thread.
+ *
+ * Complex arrays are interleaved (re, im) doubles. Basis states are split in
+ * low/high 64-bit words (hi may be NULL for chains of at most 64 sites).
+ */
+#ifndef QMBED_B200_H
+#define QMBED_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QMBED_API __attribute__((visibility("default")))
+
+/* Status codes: the categories of the reference QmbedError (src/error.rs:4-35). */
+enum {
+  QMBED_STATUS_OK = 0,
+  QMBED_STATUS_INVALID_OPERATOR = 1,
+  QMBED_STATUS_INVALID_COUPLING = 2,
+  QMBED_STATUS_INVALID_SITE = 3,
+  QMBED_STATUS_STATE_NOT_IN_BASIS = 4,
+  QMBED_STATUS_INVALID_SECTOR = 5,
+  QMBED_STATUS_INCOMPATIBLE_SYMMETRY = 6,
+  QMBED_STATUS_NON_HERMITIAN = 7,
+  QMBED_STATUS_INVALID_OPTIONS = 8,
+  QMBED_STATUS_DIMENSION_MISMATCH = 9,
+  QMBED_STATUS_RANK_DEFICIENT = 10,
+  QMBED_STATUS_UNSUPPORTED_BACKEND = 11,
+  QMBED_STATUS_INTERNAL_STATE = 13,
+  QMBED_STATUS_NON_CONVERGENCE = 14,
+  QMBED_STATUS_CUDA_ERROR = 20
+};
+
+/* Spin normalisation (reference SpinNormalization, src/basis/mod.rs:1006-1014). */
+enum { QMBED_ANGULAR_MOMENTUM = 0, QMBED_PAULI = 1, QMBED_PAULI_CARTESIAN = 2 };
+
+/* Operator storage on the device. */
+enum {
+  QMBED_STORAGE_MATRIX_FREE = 0, /* terms expanded on every application */
+  QMBED_STORAGE_PACKED = 1       /* rows assembled once on the GPU (packed u32 entries when real) */
+};
+
+/* Spectral targets (reference SpectrumTarget, src/solve/mod.rs:332-347). */
+enum {
+  QMBED_SMALLEST_ALGEBRAIC = 0,
+  QMBED_LARGEST_ALGEBRAIC = 1,
+  QMBED_SMALLEST_MAGNITUDE = 2,
+  QMBED_LARGEST_MAGNITUDE = 3,
+  QMBED_BOTH_ENDS = 4,
+  QMBED_SHIFT = 5
+};
+
+/* Solver modes. */
+enum {
+  QMBED_MODE_PLAIN_FP64 = 0, /* the reference algorithms in FP64 */
+  QMBED_MODE_MIXED = 1       /* FP32 vectors and H.v, FP64 recurrences, FP64 refinement to tolerance */
+};
+
+typedef struct qmbed_basis_s* qmbed_basis;
+typedef struct qmbed_operator_s* qmbed_operator;
+
+QMBED_API const char* qmbed_gpu_last_error(void);
+QMBED_API int qmbed_gpu_device_count(int* count);
+/* Number of kernels this library has launched in the process so far. */
+QMBED_API int qmbed_gpu_launch_count(uint64_t* count);
+
+/* SpinBasis1D::builder(sites).up(up).momentum(k).parity(p).build()
+ * (reference src/basis/mod.rs:1312-1412, spin one half). up < 0: no fixed
+ * magnetisation; parity 0: no reflection sector. */
+QMBED_API int qmbed_gpu_spin_basis_create(int device, int sites, int up, int has_momentum, int momentum, int parity,
+                                          int normalization, qmbed_basis* out);
+QMBED_API int qmbed_gpu_basis_destroy(qmbed_basis basis);
+/* Basis::len (src/basis/mod.rs:106). */
+QMBED_API int qmbed_gpu_basis_dimension(qmbed_basis basis, uint64_t* dimension);
+/* Basis::state over [offset, offset+count) plus the orbit sizes of
+ * spin_symmetry_sector (src/basis/mod.rs:715-848); any output may be NULL. */
+QMBED_API int qmbed_gpu_basis_states(qmbed_basis basis, uint64_t offset, uint64_t count, uint64_t* lo, uint64_t* hi,
+                                     uint16_t* orbit);
+/* Basis::reduction_image + Basis::index for physical states
+ * (src/basis/mod.rs:1536-1560, 1429-1442): index -1 when the state's orbit is
+ * not in the sector; phase is complex (2 doubles per state). */
+QMBED_API int qmbed_gpu_basis_images(qmbed_basis basis, const uint64_t* lo, const uint64_t* hi, uint64_t n,
+                                     int64_t* index, double* phase, uint16_t* orbit);
+QMBED_API int qmbed_gpu_basis_build_seconds(qmbed_basis basis, double* seconds);
+
+/* OperatorBuilder::on(&basis).terms(...).checks(...).build(format)
+ * (src/operator/mod.rs:2040-2216). Terms are flattened: term t has arity[t]
+ * symbols (one of "Iz+-xy" each) taken in order from `symbols`, and
+ * n_couplings[t] couplings, each with a complex coefficient (2 doubles) and
+ * arity[t] site indices taken in order from `sites`. */
+QMBED_API int qmbed_gpu_operator_create(qmbed_basis basis, int n_terms, const int* arity, const char* symbols,
+                                        const int* n_couplings, const double* coefficients, const int* sites,
+                                        int check_hermitian, int check_particles, int storage, qmbed_operator* out);
+QMBED_API int qmbed_gpu_operator_destroy(qmbed_operator op);
+QMBED_API int qmbed_gpu_operator_info(qmbed_operator op, uint64_t* dimension, int* is_real, int* storage,
+                                      uint64_t* nnz_offdiag, int* value_codes, double* assembly_seconds);
+/* LinearOperator::apply / apply_real (src/operator/mod.rs:1401-1548) on device
+ * buffers of the given precision (64 or 32); complex_vectors selects
+ * interleaved complex vectors. stream may be NULL (default stream). */
+QMBED_API int qmbed_gpu_operator_apply_device(qmbed_operator op, int precision, int complex_vectors, const void* x,
+                                              void* y, void* stream, int force_matrix_free);
+/* The same action on host buffers (FP64; complex interleaved when complex_vectors). */
+QMBED_API int qmbed_gpu_operator_apply_host(qmbed_operator op, int complex_vectors, const double* x, double* y,
+                                            int force_matrix_free);
+/* Assembled rows (diagonal included, orbit factors applied) of an operator
+ * with stored rows: first call with cols == NULL to get *nnz_total. */
+QMBED_API int qmbed_gpu_operator_export_csr(qmbed_operator op, uint64_t* nnz_total, uint64_t* row_ptr, uint32_t* cols,
+                                            double* values);
+/* Operand-byte model of one application: D(b_state + s_y) + (D + nnz_off) s_x. */
+QMBED_API int qmbed_gpu_operator_operand_bytes(qmbed_operator op, int precision, int complex_vectors, double* bytes);
+
+typedef struct {
+  uint64_t eigenpairs;
+  int target;
+  double shift;
+  uint64_t krylov_dimension; /* 0: None */
+  double tolerance;
+  uint64_t max_iterations;
+  uint64_t seed;
+  int mode; /* QMBED_MODE_* */
+} qmbed_eigsh_options;
+
+typedef struct {
+  uint64_t iterations;
+  uint64_t reorthogonalization_passes;
+  uint64_t conditional_second_passes;
+  uint64_t fp32_iterations;
+  uint64_t fp64_iterations;
+  uint64_t operator_applications;
+  int converged;
+  int complex_vectors;
+} qmbed_eigsh_info;
+
+/* eigsh / eigsh_with_initial_subspace (src/solve/mod.rs:2335-2417). initial
+ * holds n_initial host vectors (complex, dimension each) or is NULL;
+ * eigenvectors (complex, eigenpairs x dimension) may be NULL. */
+QMBED_API int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, const double* initial,
+                              int n_initial, double* eigenvalues, double* residuals, double* eigenvectors,
+                              qmbed_eigsh_info* info);
+
+/* ExpmActionPlan::new (src/solve/mod.rs:126-184): degree, scaling, trace
+ * shift (complex) and the exact stored 1-norm of A - shift. */
+QMBED_API int qmbed_gpu_expm_plan(qmbed_operator op, double coef_re, double coef_im, uint64_t max_degree,
+                                  double tolerance, uint64_t max_substeps, uint64_t* degree, uint64_t* scaling,
+                                  double* shift, double* one_norm);
+/* ExpmActionPlan::apply (src/solve/mod.rs:198-247) on n_vectors host vectors
+ * (complex, dimension each); precision 64 (complex128) or 32 (complex64 working vectors). */
+QMBED_API int qmbed_gpu_expm_apply_host(qmbed_operator op, double coef_re, double coef_im, uint64_t max_degree,
+                                        double tolerance, uint64_t max_substeps, int precision, const double* input,
+                                        double* output, uint64_t n_vectors);
+
+/* deterministic_start (src/solve/mod.rs:729-742): normalised LCG vector. */
+QMBED_API int qmbed_gpu_deterministic_start(int device, uint64_t n, uint64_t seed, double* out);
+
+/* ---- JSON boundary: the reference cdylib's exports --------------------- */
+/* qmbed_run_json (bindings/capi/src/lib.rs:6089-6106) */
+QMBED_API char* qmbed_run_json(const char* request);
+/* qmbed_command_json (bindings/capi/src/lib.rs:6120-6137) */
+QMBED_API char* qmbed_command_json(const char* request);
+/* qmbed_string_free (bindings/capi/src/lib.rs:6290-6296) */
+QMBED_API void qmbed_string_free(char* response);
+/* qmbed_evolve_model_with_drive_json (bindings/capi/src/lib.rs:6153-6190):
+ * present for load-time binding; answers an unsupported-backend error. */
+QMBED_API char* qmbed_evolve_model_with_drive_json(const char* request, void* callback, void* context);
+/* qmbed_register_user_basis_{32,64}_json (bindings/capi/src/lib.rs:6192-6282):
+ * present for load-time binding; answer an unsupported-backend error. */
+QMBED_API char* qmbed_register_user_basis_32_json(const char* request, void* op, void* next_state, void* pre_check,
+                                                  void* maps, size_t n_maps);
+QMBED_API char* qmbed_register_user_basis_64_json(const char* request, void* op, void* next_state, void* pre_check,
+                                                  void* maps, size_t n_maps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QMBED_B200_H */

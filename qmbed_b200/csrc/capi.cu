@@ -1,0 +1,957 @@
+// C ABI of libqmbed_b200.so: the typed qmbed_gpu_* API and the JSON
+// protocol of the reference cdylib (matrixlab-research/QMBED
+// bindings/capi/src/lib.rs). Exceptions never cross the boundary: every
+// entry point converts failures into a status code (typed API) or an error
+// response (JSON API), like the reference's catch_unwind wrappers
+// (lib.rs:6090-6104).
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qmbed_b200.h"
+#include "eigsh.cuh"
+#include "expm.cuh"
+#include "json.hpp"
+#include "operator.cuh"
+
+namespace qmbed {
+
+// Display texts of the reference error variants (src/error.rs:6-35).
+void raise(int code, const std::string& detail) {
+  std::string text;
+  switch (code) {
+    case QMBED_INVALID_OPERATOR: text = "invalid or unregistered operator: " + detail; break;
+    case QMBED_INVALID_COUPLING: text = "invalid coupling: " + detail; break;
+    case QMBED_INVALID_SITE: text = detail; break;
+    case QMBED_STATE_NOT_IN_BASIS: text = "state is not represented by this basis"; break;
+    case QMBED_INVALID_SECTOR: text = "invalid Hilbert-space sector: " + detail; break;
+    case QMBED_INCOMPATIBLE_SYMMETRY: text = "incompatible symmetry request: " + detail; break;
+    case QMBED_NON_HERMITIAN: text = "a Hermitian operator is required"; break;
+    case QMBED_INVALID_OPTIONS: text = "invalid options: " + detail; break;
+    case QMBED_DIMENSION_MISMATCH: text = "dimension mismatch: " + detail; break;
+    case QMBED_RANK_DEFICIENT: text = "the supplied vectors are numerically rank deficient"; break;
+    case QMBED_UNSUPPORTED_BACKEND: text = "unsupported backend: " + detail; break;
+    case QMBED_INTERNAL_STATE: text = "internal state error: " + detail; break;
+    case QMBED_CUDA_ERROR: text = "unsupported backend: CUDA error: " + detail; break;
+    default: text = detail; break;
+  }
+  throw Error(code, text);
+}
+
+std::atomic<unsigned long long> g_kernel_launches{0};
+
+void count_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void raise_nonconvergence(size_t iterations, double residual) {
+  char buffer[160];
+  std::snprintf(buffer, sizeof(buffer), "solver did not converge after %zu iterations; residual=%.6e", iterations,
+                residual);
+  Error e(QMBED_NON_CONVERGENCE, buffer);
+  e.iterations = iterations;
+  e.residual = residual;
+  throw e;
+}
+
+}  // namespace qmbed
+
+using namespace qmbed;
+
+struct qmbed_basis_s {
+  std::shared_ptr<SpinBasis> basis;
+};
+
+struct qmbed_operator_s {
+  std::shared_ptr<SpinOperator> op;
+  cudaStream_t stream = nullptr;
+  std::unique_ptr<BlockOps> ops;
+  std::mutex mu;
+  ~qmbed_operator_s() {
+    ops.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
+  BlockOps& block_ops() {
+    if (!ops) {
+      QMBED_CUDA(cudaSetDevice(op->basis().device()));
+      QMBED_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+      ops = std::make_unique<BlockOps>(op->basis().device(), stream);
+    }
+    return *ops;
+  }
+  LinearOperatorView view() {
+    BlockOps& b = block_ops();
+    SpinOperator* raw = op.get();
+    cudaStream_t s = b.stream();
+    return LinearOperatorView{raw->dim(), raw->is_real(),
+                              [raw, s](int prec, bool cplx, const void* x, void* y) { raw->apply(prec, cplx, x, y, s); }};
+  }
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F&& body) {
+  try {
+    body();
+    return QMBED_STATUS_OK;
+  } catch (const Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const json::ParseError& e) {
+    g_last_error = std::string("invalid options: ") + e.what();
+    return QMBED_STATUS_INVALID_OPTIONS;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "unsupported backend: host allocation failed";
+    return QMBED_STATUS_UNSUPPORTED_BACKEND;
+  } catch (const std::exception& e) {
+    g_last_error = std::string("internal state error: ") + e.what();
+    return QMBED_STATUS_INTERNAL_STATE;
+  }
+}
+
+std::vector<TermDesc> decode_terms(int n_terms, const int* arity, const char* symbols, const int* n_couplings,
+                                   const double* coefficients, const int* sites) {
+  if (n_terms < 0) raise(QMBED_INVALID_OPTIONS, "negative term count");
+  std::vector<TermDesc> terms(static_cast<size_t>(n_terms));
+  size_t sc = 0, cc = 0, ss = 0;
+  for (int t = 0; t < n_terms; ++t) {
+    if (arity[t] <= 0) raise(QMBED_INVALID_OPERATOR, "operator products cannot be empty");
+    terms[t].symbols.assign(symbols + sc, symbols + sc + arity[t]);
+    sc += static_cast<size_t>(arity[t]);
+    for (int c = 0; c < n_couplings[t]; ++c) {
+      CouplingDesc coupling;
+      coupling.coefficient = C64(coefficients[2 * cc], coefficients[2 * cc + 1]);
+      ++cc;
+      coupling.sites.assign(sites + ss, sites + ss + arity[t]);
+      ss += static_cast<size_t>(arity[t]);
+      terms[t].couplings.push_back(std::move(coupling));
+    }
+  }
+  return terms;
+}
+
+char* to_c_string(const std::string& s) {
+  char* out = static_cast<char*>(std::malloc(s.size() + 1));
+  if (!out) return nullptr;
+  std::memcpy(out, s.c_str(), s.size() + 1);
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// JSON protocol (bindings/capi/src/lib.rs:55-2204, 5513-5990)
+// ---------------------------------------------------------------------------
+using json::Value;
+
+int default_device() {
+  const char* env = std::getenv("QMBED_DEVICE");
+  return env ? std::atoi(env) : 0;
+}
+
+SpinBasisDesc parse_basis(const Value& b) {
+  const std::string kind = b.at("kind").as_string();
+  if (kind != "spin")
+    raise(QMBED_UNSUPPORTED_BACKEND, "the GPU engine implements spin-1/2 chain bases; `" + kind + "` is not supported");
+  SpinBasisDesc d{};
+  d.sites = static_cast<int>(b.at("sites").as_int());
+  if (b.has("spin_twice") && b.at("spin_twice").as_int() != 1)
+    raise(QMBED_UNSUPPORTED_BACKEND, "the GPU engine implements spin one half (spin_twice = 1)");
+  if (b.has("up") && b.has("up_sectors"))
+    raise(QMBED_INVALID_OPTIONS, "spin basis accepts either up or up_sectors, not both");
+  d.up = b.has("up") ? static_cast<int>(b.at("up").as_int()) : -1;
+  if (b.has("up_sectors")) {
+    const auto& sectors = b.at("up_sectors").items();
+    if (sectors.size() != 1) raise(QMBED_UNSUPPORTED_BACKEND, "unions of magnetisation sectors are not supported");
+    d.up = static_cast<int>(sectors[0].as_int());
+  }
+  d.has_momentum = b.has("momentum") ? 1 : 0;
+  d.momentum = d.has_momentum ? static_cast<int>(b.at("momentum").as_int()) : 0;
+  d.parity = b.has("parity") ? static_cast<int>(b.at("parity").as_int()) : 0;
+  d.normalization = (b.has("pauli") && b.at("pauli").as_bool()) ? kPauliCartesian : kAngularMomentum;
+  if (b.has("normalization")) {
+    const std::string n = b.at("normalization").as_string();
+    if (n == "angular_momentum") d.normalization = kAngularMomentum;
+    else if (n == "pauli") d.normalization = kPauli;
+    else if (n == "pauli_cartesian") d.normalization = kPauliCartesian;
+    else raise(QMBED_INVALID_OPTIONS, "unknown spin normalization `" + n + "`");
+  }
+  if (b.has("symmetries") && !b.at("symmetries").items().empty()) {
+    if (d.has_momentum || d.parity) raise(QMBED_INVALID_OPTIONS, "built-in and general spin symmetries cannot be mixed");
+    raise(QMBED_UNSUPPORTED_BACKEND, "general symmetry maps are not supported by the GPU engine");
+  }
+  if (b.has("matrix_symmetry"))
+    raise(QMBED_INVALID_OPTIONS, "matrix-valued symmetry sectors materialize as projected operator models");
+  if (b.has("reverse") && b.at("reverse").as_bool())
+    raise(QMBED_UNSUPPORTED_BACKEND, "maximum-representative ordering is not supported by the GPU engine");
+  return d;
+}
+
+// typed_local_operator (bindings/capi/src/lib.rs:6053-6071)
+char local_symbol(const std::string& name) {
+  if (name == "identity") return 'I';
+  if (name == "number") return 'n';
+  if (name == "z") return 'z';
+  if (name == "raising") return '+';
+  if (name == "lowering") return '-';
+  if (name == "x") return 'x';
+  if (name == "y") return 'y';
+  if (name.rfind("custom:", 0) == 0 && name.size() == 8) return name[7];
+  raise(QMBED_INVALID_OPERATOR, name);
+}
+
+std::vector<TermDesc> parse_terms(const Value& terms, C64 scale = C64(1.0, 0.0)) {
+  std::vector<TermDesc> out;
+  for (const Value& t : terms.items()) {
+    TermDesc term;
+    for (const Value& name : t.at("product").at("local").items()) term.symbols.push_back(local_symbol(name.as_string()));
+    if (term.symbols.empty()) raise(QMBED_INVALID_OPERATOR, "operator products cannot be empty");
+    for (const Value& c : t.at("couplings").items()) {
+      const auto& coef = c.at("coefficient").items();
+      if (coef.size() != 2) raise(QMBED_INVALID_OPTIONS, "coefficients are [re, im] pairs");
+      CouplingDesc coupling;
+      coupling.coefficient = scale * C64(coef[0].as_double(), coef[1].as_double());
+      for (const Value& s : c.at("sites").items()) {
+        const long long site = s.as_int();
+        if (site < 0) raise(QMBED_INVALID_OPTIONS, "sites are non-negative integers");
+        coupling.sites.push_back(static_cast<int>(site));
+      }
+      term.couplings.push_back(std::move(coupling));
+    }
+    out.push_back(std::move(term));
+  }
+  return out;
+}
+
+OperatorChecks parse_checks(const Value& request) {
+  OperatorChecks checks;
+  if (const Value* c = request.find("checks")) {
+    if (c->has("hermiticity")) checks.hermiticity = c->at("hermiticity").as_bool();
+    if (c->has("particle_conservation")) checks.particle_conservation = c->at("particle_conservation").as_bool();
+  }
+  return checks;
+}
+
+int parse_storage(const Value& request) {
+  if (!request.has("format")) return kStoragePacked;
+  const std::string f = request.at("format").as_string();
+  if (f == "matrix_free") return kStorageMatrixFree;
+  if (f == "dense" || f == "csc" || f == "csr" || f == "dia") return kStoragePacked;
+  raise(QMBED_INVALID_OPTIONS, "unknown storage format `" + f + "`");
+}
+
+struct SolverRequest {
+  EigshOptions options;
+  bool eigenvectors = false;
+  int mode = kModePlainFP64;
+  std::vector<std::vector<C64>> initial;
+};
+
+std::vector<C64> parse_vector(const Value& v) {
+  std::vector<C64> out;
+  for (const Value& pair : v.items()) {
+    const auto& p = pair.items();
+    if (p.size() != 2) raise(QMBED_INVALID_OPTIONS, "vector entries are [re, im] pairs");
+    out.emplace_back(p[0].as_double(), p[1].as_double());
+  }
+  return out;
+}
+
+SolverRequest parse_solver(const Value& s) {
+  SolverRequest r;
+  r.options.eigenpairs = static_cast<size_t>(s.at("eigenpairs").as_int());
+  const std::string kind = s.at("target").at("kind").as_string();
+  if (kind == "smallest_algebraic") r.options.target = kSmallestAlgebraic;
+  else if (kind == "largest_algebraic") r.options.target = kLargestAlgebraic;
+  else if (kind == "smallest_magnitude") r.options.target = kSmallestMagnitude;
+  else if (kind == "largest_magnitude") r.options.target = kLargestMagnitude;
+  else if (kind == "both_ends") r.options.target = kBothEnds;
+  else if (kind == "shift") {
+    r.options.target = kShift;
+    r.options.shift = s.at("target").at("value").as_double();
+  } else {
+    raise(QMBED_INVALID_OPTIONS, "unknown spectrum target `" + kind + "`");
+  }
+  if (s.has("krylov_dimension")) r.options.krylov_dimension = static_cast<size_t>(s.at("krylov_dimension").as_int());
+  if (s.has("tolerance")) r.options.tolerance = s.at("tolerance").as_double();
+  if (s.has("max_iterations")) r.options.max_iterations = static_cast<size_t>(s.at("max_iterations").as_int());
+  if (s.has("seed")) r.options.seed = static_cast<uint64_t>(s.at("seed").as_int());
+  if (s.has("eigenvectors")) r.eigenvectors = s.at("eigenvectors").as_bool();
+  if (s.has("initial_vector")) r.initial.push_back(parse_vector(s.at("initial_vector")));
+  else if (s.has("v0")) r.initial.push_back(parse_vector(s.at("v0")));
+  if (s.has("precision")) {
+    const std::string p = s.at("precision").as_string();
+    if (p == "mixed") r.mode = kModeMixed;
+    else if (p != "fp64") raise(QMBED_INVALID_OPTIONS, "precision must be `fp64` or `mixed`");
+  }
+  return r;
+}
+
+Value complex_pair(C64 v) {
+  Value p = Value::array();
+  p.push(Value::number(v.real()));
+  p.push(Value::number(v.imag()));
+  return p;
+}
+
+Value vectors_value(const std::vector<double>& host, uint64_t dim, size_t count) {
+  Value vs = Value::array();
+  for (size_t k = 0; k < count; ++k) {
+    Value v = Value::array();
+    for (uint64_t i = 0; i < dim; ++i) v.push(complex_pair(C64(host[2 * (k * dim + i)], host[2 * (k * dim + i) + 1])));
+    vs.push(std::move(v));
+  }
+  return vs;
+}
+
+// Runs eigsh and returns the SolveResult / Eigensystem JSON fields.
+Value solve(qmbed_operator_s& handle, const SolverRequest& request, bool tagged) {
+  std::lock_guard<std::mutex> lock(handle.mu);
+  LinearOperatorView view = handle.view();
+  EigshResult r = eigsh(view, request.options, request.initial, request.mode, handle.block_ops());
+  Value out = Value::object();
+  if (tagged) out.set("kind", Value::string("eigensystem"));
+  const uint64_t dim = view.dim;
+  out.set("dimension", Value::integer(static_cast<long long>(dim)));
+  Value values = Value::array(), residuals = Value::array();
+  for (double v : r.eigenvalues) values.push(Value::number(v));
+  for (double v : r.residuals) residuals.push(Value::number(v));
+  out.set("eigenvalues", std::move(values));
+  out.set("residuals", std::move(residuals));
+  out.set("iterations", Value::integer(static_cast<long long>(r.iterations)));
+  out.set("converged", Value::boolean(r.converged));
+  if (request.eigenvectors) {
+    const size_t k = r.eigenvalues.size();
+    std::vector<double> host(2 * k * dim, 0.0);
+    if (r.complex_vectors) {
+      QMBED_CUDA(cudaMemcpy(host.data(), r.vectors.get(), host.size() * 8, cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<double> real(k * dim);
+      QMBED_CUDA(cudaMemcpy(real.data(), r.vectors.get(), real.size() * 8, cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < real.size(); ++i) host[2 * i] = real[i];
+    }
+    out.set("eigenvectors", vectors_value(host, dim, k));
+  }
+  return out;
+}
+
+std::shared_ptr<qmbed_operator_s> make_operator(std::shared_ptr<SpinBasis> basis, const std::vector<TermDesc>& terms,
+                                                const OperatorChecks& checks, int storage) {
+  auto h = std::make_shared<qmbed_operator_s>();
+  h->op = std::make_shared<SpinOperator>(std::move(basis), terms, checks, storage);
+  return h;
+}
+
+struct Component {
+  std::string name;
+  std::vector<TermDesc> terms;
+  bool has_default;
+  C64 default_value;
+};
+
+struct Model {
+  std::shared_ptr<SpinBasis> basis;
+  std::vector<TermDesc> terms;
+  std::vector<Component> components;
+  OperatorChecks checks;
+  std::mutex mu;
+  std::map<std::string, std::shared_ptr<qmbed_operator_s>> cache;  // parameters+storage -> operator
+
+  std::shared_ptr<qmbed_operator_s> materialize(const Value* parameters, int storage, bool hermitian_check) {
+    std::map<std::string, C64> values;
+    if (parameters && parameters->is_object())
+      for (auto& kv : parameters->members()) {
+        bool known = false;
+        for (auto& c : components) known = known || c.name == kv.first;
+        if (!known) raise(QMBED_INVALID_OPTIONS, "unknown operator parameter \"" + kv.first + "\"");
+        const auto& p = kv.second.items();
+        values[kv.first] = C64(p.at(0).as_double(), p.at(1).as_double());
+      }
+    std::vector<TermDesc> all = terms;
+    std::string key = std::to_string(storage) + (hermitian_check ? "h" : "n");
+    for (auto& c : components) {
+      C64 v;
+      auto it = values.find(c.name);
+      if (it != values.end()) v = it->second;
+      else if (c.has_default) v = c.default_value;
+      else raise(QMBED_INVALID_OPTIONS, "operator parameter \"" + c.name + "\" has no default and was not supplied");
+      char buffer[96];
+      std::snprintf(buffer, sizeof(buffer), "|%.17g,%.17g", v.real(), v.imag());
+      key += buffer;
+      for (const TermDesc& t : c.terms) {
+        TermDesc scaled = t;
+        for (auto& coupling : scaled.couplings) coupling.coefficient *= v;
+        all.push_back(std::move(scaled));
+      }
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    OperatorChecks c = checks;
+    c.hermiticity = hermitian_check && checks.hermiticity;
+    auto op = make_operator(basis, all, c, storage);
+    cache[key] = op;
+    return op;
+  }
+};
+
+struct ExpmEntry {
+  std::shared_ptr<qmbed_operator_s> op;
+  ExpmPlan plan;
+};
+
+std::mutex g_registry_mu;
+std::map<uint64_t, std::shared_ptr<Model>> g_models;
+std::map<uint64_t, std::shared_ptr<ExpmEntry>> g_expm;
+std::atomic<uint64_t> g_next_model{1}, g_next_expm{1};
+
+uint64_t parse_handle(const std::string& text, const char* what) {
+  char* end = nullptr;
+  const unsigned long long value = std::strtoull(text.c_str(), &end, 10);
+  if (text.empty() || !end || *end != '\0' || value == 0)
+    raise(QMBED_INVALID_OPTIONS, std::string(what) + " handle \"" + text + "\" is not a positive integer");
+  return value;
+}
+
+std::shared_ptr<Model> registered_model(const std::string& text) {
+  const uint64_t id = parse_handle(text, "model");
+  std::lock_guard<std::mutex> lock(g_registry_mu);
+  auto it = g_models.find(id);
+  if (it == g_models.end()) raise(QMBED_INVALID_OPTIONS, "model handle " + text + " is not registered");
+  return it->second;
+}
+
+std::shared_ptr<ExpmEntry> registered_expm(const std::string& text) {
+  const uint64_t id = parse_handle(text, "exponential-action");
+  std::lock_guard<std::mutex> lock(g_registry_mu);
+  auto it = g_expm.find(id);
+  if (it == g_expm.end()) raise(QMBED_INVALID_OPTIONS, "exponential-action handle " + text + " is not registered");
+  return it->second;
+}
+
+std::shared_ptr<Model> build_model(const Value& request) {
+  auto model = std::make_shared<Model>();
+  model->basis = std::make_shared<SpinBasis>(parse_basis(request.at("basis")), default_device());
+  model->terms = parse_terms(request.at("terms"));
+  model->checks = parse_checks(request);
+  if (request.has("site_permutation")) raise(QMBED_UNSUPPORTED_BACKEND, "site permutations are not supported by the GPU engine");
+  if (const Value* comps = request.find("components"))
+    if (comps->is_array())
+      for (const Value& c : comps->items()) {
+        Component comp;
+        comp.name = c.at("name").as_string();
+        comp.terms = parse_terms(c.at("terms"));
+        comp.has_default = c.has("default");
+        if (comp.has_default) {
+          const auto& d = c.at("default").items();
+          comp.default_value = C64(d.at(0).as_double(), d.at(1).as_double());
+        }
+        model->components.push_back(std::move(comp));
+      }
+  return model;
+}
+
+std::vector<std::vector<C64>> parse_vectors(const Value& v) {
+  std::vector<std::vector<C64>> out;
+  for (const Value& vec : v.items()) out.push_back(parse_vector(vec));
+  return out;
+}
+
+Value apply_vectors(qmbed_operator_s& handle, const std::vector<std::vector<C64>>& vectors) {
+  std::lock_guard<std::mutex> lock(handle.mu);
+  const uint64_t dim = handle.op->dim();
+  BlockOps& ops = handle.block_ops();
+  DeviceBuffer x(std::max<uint64_t>(dim, 1) * 16), y(std::max<uint64_t>(dim, 1) * 16);
+  std::vector<double> host(2 * dim);
+  Value out = Value::object();
+  out.set("kind", Value::string("vectors"));
+  out.set("dimension", Value::integer(static_cast<long long>(vectors.empty() ? dim : vectors[0].size())));
+  Value vs = Value::array();
+  for (const auto& v : vectors) {
+    if (v.size() != dim) raise(QMBED_DIMENSION_MISMATCH, "vector length does not match the model dimension");
+    for (uint64_t i = 0; i < dim; ++i) {
+      host[2 * i] = v[i].real();
+      host[2 * i + 1] = v[i].imag();
+    }
+    QMBED_CUDA(cudaMemcpyAsync(x.get(), host.data(), 16 * dim, cudaMemcpyHostToDevice, ops.stream()));
+    handle.op->apply(64, true, x.get(), y.get(), ops.stream());
+    QMBED_CUDA(cudaMemcpyAsync(host.data(), y.get(), 16 * dim, cudaMemcpyDeviceToHost, ops.stream()));
+    ops.sync();
+    Value r = Value::array();
+    for (uint64_t i = 0; i < dim; ++i) r.push(complex_pair(C64(host[2 * i], host[2 * i + 1])));
+    vs.push(std::move(r));
+  }
+  out.set("vectors", std::move(vs));
+  return out;
+}
+
+Value run_request(const Value& request) {
+  auto model = build_model(request);
+  auto op = model->materialize(nullptr, parse_storage(request), true);
+  return solve(*op, parse_solver(request.at("solver")), false);
+}
+
+Value describe_basis(const Value& request) {
+  SpinBasis basis(parse_basis(request.at("basis")), default_device());
+  const uint64_t n = basis.dim();
+  std::vector<uint64_t> lo(n), hi(n);
+  basis.copy_states(0, n, lo.data(), hi.data(), nullptr);
+  Value out = Value::object();
+  out.set("kind", Value::string("basis"));
+  out.set("dimension", Value::integer(static_cast<long long>(n)));
+  Value states = Value::array();
+  for (uint64_t i = 0; i < n; ++i) {
+    unsigned __int128 s = (static_cast<unsigned __int128>(hi[i]) << 64) | lo[i];
+    std::string text;
+    if (s == 0) text = "0";
+    while (s > 0) {
+      text.insert(text.begin(), static_cast<char>('0' + static_cast<int>(s % 10)));
+      s /= 10;
+    }
+    states.push(Value::string(text));
+  }
+  out.set("states", std::move(states));
+  return out;
+}
+
+Value command(const Value& request) {
+  const std::string operation = request.at("operation").as_string();
+  if (operation == "describe_basis") return describe_basis(request);
+  if (operation == "eigsh") {
+    auto model = build_model(request);
+    auto op = model->materialize(nullptr, parse_storage(request), true);
+    return solve(*op, parse_solver(request.at("solver")), true);
+  }
+  if (operation == "materialize") {
+    auto model = build_model(request);
+    auto op = model->materialize(nullptr, kStoragePacked, model->checks.hermiticity);
+    std::vector<uint64_t> row_ptr;
+    std::vector<uint32_t> cols;
+    std::vector<C64> values;
+    op->op->export_csr(row_ptr, cols, values);
+    Value out = Value::object();
+    out.set("kind", Value::string("operator"));
+    Value shape = Value::array();
+    shape.push(Value::integer(static_cast<long long>(op->op->dim())));
+    shape.push(Value::integer(static_cast<long long>(op->op->dim())));
+    out.set("shape", std::move(shape));
+    out.set("format", Value::string(request.has("format") ? request.at("format").as_string() : "csc"));
+    Value entries = Value::array();
+    for (uint64_t r = 0; r + 1 < row_ptr.size(); ++r)
+      for (uint64_t p = row_ptr[r]; p < row_ptr[r + 1]; ++p) {
+        Value e = Value::object();
+        e.set("row", Value::integer(static_cast<long long>(r)));
+        e.set("column", Value::integer(static_cast<long long>(cols[p])));
+        e.set("value", complex_pair(values[p]));
+        entries.push(std::move(e));
+      }
+    out.set("entries", std::move(entries));
+    return out;
+  }
+  if (operation == "create_model") {
+    auto model = build_model(request);
+    const uint64_t id = g_next_model.fetch_add(1);
+    {
+      std::lock_guard<std::mutex> lock(g_registry_mu);
+      g_models[id] = model;
+    }
+    Value out = Value::object();
+    out.set("kind", Value::string("model"));
+    out.set("handle", Value::string(std::to_string(id)));
+    out.set("dimension", Value::integer(static_cast<long long>(model->basis->dim())));
+    return out;
+  }
+  if (operation == "describe_model") {
+    auto model = registered_model(request.at("handle").as_string());
+    Value out = Value::object();
+    out.set("kind", Value::string("model"));
+    out.set("handle", Value::string(request.at("handle").as_string()));
+    out.set("dimension", Value::integer(static_cast<long long>(model->basis->dim())));
+    return out;
+  }
+  if (operation == "eigsh_model") {
+    auto model = registered_model(request.at("handle").as_string());
+    auto op = model->materialize(request.find("parameters"), parse_storage(request), true);
+    return solve(*op, parse_solver(request.at("solver")), true);
+  }
+  if (operation == "apply_model") {
+    auto model = registered_model(request.at("handle").as_string());
+    if (request.has("action") && request.at("action").as_string() != "apply")
+      raise(QMBED_UNSUPPORTED_BACKEND, "only the direct action is supported by the GPU engine");
+    auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
+    return apply_vectors(*op, parse_vectors(request.at("vectors")));
+  }
+  if (operation == "create_expm_action") {
+    auto model = registered_model(request.at("handle").as_string());
+    auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
+    const auto& c = request.at("coefficient").items();
+    const C64 coefficient(c.at(0).as_double(), c.at(1).as_double());
+    const size_t max_degree = request.has("max_degree") ? static_cast<size_t>(request.at("max_degree").as_int()) : 55;
+    const double tolerance = request.has("tolerance") ? request.at("tolerance").as_double() : 0.5 * 2.220446049250313e-16;
+    const size_t substeps = request.has("max_substeps") ? static_cast<size_t>(request.at("max_substeps").as_int()) : 10000;
+    auto entry = std::make_shared<ExpmEntry>();
+    entry->op = op;
+    entry->plan = make_expm_plan(*op->op, coefficient, max_degree, tolerance, substeps);
+    const uint64_t id = g_next_expm.fetch_add(1);
+    {
+      std::lock_guard<std::mutex> lock(g_registry_mu);
+      g_expm[id] = entry;
+    }
+    Value out = Value::object();
+    out.set("kind", Value::string("expm_plan"));
+    out.set("handle", Value::string(std::to_string(id)));
+    out.set("dimension", Value::integer(static_cast<long long>(op->op->dim())));
+    return out;
+  }
+  if (operation == "apply_expm_action") {
+    auto entry = registered_expm(request.at("expm_handle").as_string());
+    auto vectors = parse_vectors(request.at("vectors"));
+    qmbed_operator_s& h = *entry->op;
+    std::lock_guard<std::mutex> lock(h.mu);
+    const uint64_t dim = h.op->dim();
+    BlockOps& ops = h.block_ops();
+    LinearOperatorView view{dim, h.op->is_real(), [&h, &ops](int prec, bool cplx, const void* x, void* y) {
+                              h.op->apply(prec, cplx, x, y, ops.stream());
+                            }};
+    DeviceBuffer state(std::max<uint64_t>(dim, 1) * 16);
+    std::vector<double> host(2 * dim);
+    Value out = Value::object();
+    out.set("kind", Value::string("vectors"));
+    out.set("dimension", Value::integer(static_cast<long long>(vectors.empty() ? dim : vectors[0].size())));
+    Value vs = Value::array();
+    for (const auto& v : vectors) {
+      if (v.size() != dim) raise(QMBED_DIMENSION_MISMATCH, "exponential batch column has the wrong length");
+      for (uint64_t i = 0; i < dim; ++i) {
+        host[2 * i] = v[i].real();
+        host[2 * i + 1] = v[i].imag();
+      }
+      QMBED_CUDA(cudaMemcpy(state.get(), host.data(), 16 * dim, cudaMemcpyHostToDevice));
+      expm_apply(entry->plan, view, state.get(), 64, ops);
+      QMBED_CUDA(cudaMemcpy(host.data(), state.get(), 16 * dim, cudaMemcpyDeviceToHost));
+      Value r = Value::array();
+      for (uint64_t i = 0; i < dim; ++i) r.push(complex_pair(C64(host[2 * i], host[2 * i + 1])));
+      vs.push(std::move(r));
+    }
+    out.set("vectors", std::move(vs));
+    return out;
+  }
+  if (operation == "release_model") {
+    const std::string text = request.at("handle").as_string();
+    const uint64_t id = parse_handle(text, "model");
+    std::lock_guard<std::mutex> lock(g_registry_mu);
+    if (!g_models.erase(id)) raise(QMBED_INVALID_OPTIONS, "model handle " + text + " is not registered");
+    Value out = Value::object();
+    out.set("kind", Value::string("released"));
+    out.set("handle", Value::string(text));
+    return out;
+  }
+  if (operation == "release_expm_action") {
+    const std::string text = request.at("expm_handle").as_string();
+    const uint64_t id = parse_handle(text, "exponential-action");
+    std::lock_guard<std::mutex> lock(g_registry_mu);
+    if (!g_expm.erase(id)) raise(QMBED_INVALID_OPTIONS, "exponential-action handle " + text + " is not registered");
+    Value out = Value::object();
+    out.set("kind", Value::string("released"));
+    out.set("handle", Value::string(text));
+    return out;
+  }
+  raise(QMBED_UNSUPPORTED_BACKEND, "operation `" + operation + "` is outside the GPU engine");
+}
+
+std::string respond(const char* request, bool command_api) {
+  if (!request) return R"({"status":"error","error":"request pointer is null"})";
+  Value response = Value::object();
+  try {
+    Value parsed;
+    try {
+      parsed = json::parse(request);
+    } catch (const json::ParseError& e) {
+      raise(QMBED_INVALID_OPTIONS, std::string(command_api ? "invalid binding command: " : "invalid binding request: ") + e.what());
+    }
+    Value result;
+    try {
+      result = command_api ? command(parsed) : run_request(parsed);
+    } catch (const json::ParseError& e) {
+      raise(QMBED_INVALID_OPTIONS, std::string(command_api ? "invalid binding command: " : "invalid binding request: ") + e.what());
+    }
+    response.set("status", Value::string("ok"));
+    response.set("result", std::move(result));
+  } catch (const Error& e) {
+    response = Value::object();
+    response.set("status", Value::string("error"));
+    response.set("error", Value::string(e.what()));
+  } catch (const std::exception& e) {
+    response = Value::object();
+    response.set("status", Value::string("error"));
+    response.set("error", Value::string(std::string("internal state error: ") + e.what()));
+  }
+  return response.dump();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* qmbed_gpu_last_error(void) { return g_last_error.c_str(); }
+
+int qmbed_gpu_device_count(int* count) {
+  return guarded([&] { QMBED_CUDA(cudaGetDeviceCount(count)); });
+}
+
+int qmbed_gpu_launch_count(uint64_t* count) {
+  return guarded([&] { *count = g_kernel_launches.load(std::memory_order_relaxed); });
+}
+
+int qmbed_gpu_spin_basis_create(int device, int sites, int up, int has_momentum, int momentum, int parity,
+                                int normalization, qmbed_basis* out) {
+  return guarded([&] {
+    SpinBasisDesc d{sites, up, has_momentum, momentum, parity, normalization};
+    auto h = new qmbed_basis_s;
+    try {
+      h->basis = std::make_shared<SpinBasis>(d, device);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int qmbed_gpu_basis_destroy(qmbed_basis basis) {
+  return guarded([&] { delete basis; });
+}
+
+int qmbed_gpu_basis_dimension(qmbed_basis basis, uint64_t* dimension) {
+  return guarded([&] { *dimension = basis->basis->dim(); });
+}
+
+int qmbed_gpu_basis_states(qmbed_basis basis, uint64_t offset, uint64_t count, uint64_t* lo, uint64_t* hi,
+                           uint16_t* orbit) {
+  return guarded([&] { basis->basis->copy_states(offset, count, lo, hi, orbit); });
+}
+
+int qmbed_gpu_basis_images(qmbed_basis basis, const uint64_t* lo, const uint64_t* hi, uint64_t n, int64_t* index,
+                           double* phase, uint16_t* orbit) {
+  return guarded([&] { basis->basis->images(lo, hi, n, index, phase, orbit); });
+}
+
+int qmbed_gpu_basis_build_seconds(qmbed_basis basis, double* seconds) {
+  return guarded([&] { *seconds = basis->basis->build_seconds(); });
+}
+
+int qmbed_gpu_operator_create(qmbed_basis basis, int n_terms, const int* arity, const char* symbols,
+                              const int* n_couplings, const double* coefficients, const int* sites,
+                              int check_hermitian, int check_particles, int storage, qmbed_operator* out) {
+  return guarded([&] {
+    auto terms = decode_terms(n_terms, arity, symbols, n_couplings, coefficients, sites);
+    OperatorChecks checks;
+    checks.hermiticity = check_hermitian != 0;
+    checks.particle_conservation = check_particles != 0;
+    auto h = new qmbed_operator_s;
+    try {
+      h->op = std::make_shared<SpinOperator>(basis->basis, terms, checks, storage);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int qmbed_gpu_operator_destroy(qmbed_operator op) {
+  return guarded([&] { delete op; });
+}
+
+int qmbed_gpu_operator_info(qmbed_operator op, uint64_t* dimension, int* is_real, int* storage, uint64_t* nnz_offdiag,
+                            int* value_codes, double* assembly_seconds) {
+  return guarded([&] {
+    if (dimension) *dimension = op->op->dim();
+    if (is_real) *is_real = op->op->is_real() ? 1 : 0;
+    if (storage) *storage = op->op->storage();
+    if (nnz_offdiag) *nnz_offdiag = op->op->nnz_offdiag();
+    if (value_codes) *value_codes = op->op->value_codes();
+    if (assembly_seconds) *assembly_seconds = op->op->assembly_seconds();
+  });
+}
+
+int qmbed_gpu_operator_apply_device(qmbed_operator op, int precision, int complex_vectors, const void* x, void* y,
+                                    void* stream, int force_matrix_free) {
+  return guarded([&] {
+    if (precision != 64 && precision != 32) raise(QMBED_INVALID_OPTIONS, "precision must be 64 or 32");
+    op->op->apply(precision, complex_vectors != 0, x, y, static_cast<cudaStream_t>(stream), force_matrix_free != 0);
+  });
+}
+
+int qmbed_gpu_operator_apply_host(qmbed_operator op, int complex_vectors, const double* x, double* y,
+                                  int force_matrix_free) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(op->mu);
+    const uint64_t n = op->op->dim();
+    const size_t bytes = std::max<uint64_t>(n, 1) * 8 * (complex_vectors ? 2 : 1);
+    BlockOps& ops = op->block_ops();
+    DeviceBuffer dx(bytes), dy(bytes);
+    QMBED_CUDA(cudaMemcpyAsync(dx.get(), x, n * 8 * (complex_vectors ? 2 : 1), cudaMemcpyHostToDevice, ops.stream()));
+    op->op->apply(64, complex_vectors != 0, dx.get(), dy.get(), ops.stream(), force_matrix_free != 0);
+    QMBED_CUDA(cudaMemcpyAsync(y, dy.get(), n * 8 * (complex_vectors ? 2 : 1), cudaMemcpyDeviceToHost, ops.stream()));
+    ops.sync();
+  });
+}
+
+int qmbed_gpu_operator_export_csr(qmbed_operator op, uint64_t* nnz_total, uint64_t* row_ptr, uint32_t* cols,
+                                  double* values) {
+  return guarded([&] {
+    std::vector<uint64_t> rp;
+    std::vector<uint32_t> c;
+    std::vector<C64> v;
+    op->op->export_csr(rp, c, v);
+    if (nnz_total) *nnz_total = c.size();
+    if (row_ptr) std::memcpy(row_ptr, rp.data(), rp.size() * sizeof(uint64_t));
+    if (cols) std::memcpy(cols, c.data(), c.size() * sizeof(uint32_t));
+    if (values)
+      for (size_t i = 0; i < v.size(); ++i) {
+        values[2 * i] = v[i].real();
+        values[2 * i + 1] = v[i].imag();
+      }
+  });
+}
+
+int qmbed_gpu_operator_operand_bytes(qmbed_operator op, int precision, int complex_vectors, double* bytes) {
+  return guarded([&] { *bytes = op->op->operand_bytes(precision, complex_vectors != 0); });
+}
+
+int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, const double* initial, int n_initial,
+                    double* eigenvalues, double* residuals, double* eigenvectors, qmbed_eigsh_info* info) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(op->mu);
+    EigshOptions o;
+    o.eigenpairs = options->eigenpairs;
+    o.target = options->target;
+    o.shift = options->shift;
+    o.krylov_dimension = options->krylov_dimension;
+    o.tolerance = options->tolerance;
+    o.max_iterations = options->max_iterations;
+    o.seed = options->seed;
+    const uint64_t n = op->op->dim();
+    std::vector<std::vector<C64>> init;
+    for (int k = 0; k < n_initial; ++k) {
+      std::vector<C64> v(n);
+      for (uint64_t i = 0; i < n; ++i) v[i] = C64(initial[2 * (k * n + i)], initial[2 * (k * n + i) + 1]);
+      init.push_back(std::move(v));
+    }
+    LinearOperatorView view = op->view();
+    EigshResult r = eigsh(view, o, init, options->mode, op->block_ops());
+    for (size_t i = 0; i < r.eigenvalues.size(); ++i) {
+      eigenvalues[i] = r.eigenvalues[i];
+      residuals[i] = r.residuals[i];
+    }
+    if (eigenvectors) {
+      const size_t k = r.eigenvalues.size();
+      if (r.complex_vectors) {
+        QMBED_CUDA(cudaMemcpy(eigenvectors, r.vectors.get(), k * n * 16, cudaMemcpyDeviceToHost));
+      } else {
+        std::vector<double> real(k * n);
+        QMBED_CUDA(cudaMemcpy(real.data(), r.vectors.get(), real.size() * 8, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < real.size(); ++i) {
+          eigenvectors[2 * i] = real[i];
+          eigenvectors[2 * i + 1] = 0.0;
+        }
+      }
+    }
+    if (info) {
+      info->iterations = r.iterations;
+      info->reorthogonalization_passes = r.reorthogonalization_passes;
+      info->conditional_second_passes = r.conditional_second_passes;
+      info->fp32_iterations = r.fp32_iterations;
+      info->fp64_iterations = r.fp64_iterations;
+      info->operator_applications = r.operator_applications;
+      info->converged = r.converged ? 1 : 0;
+      info->complex_vectors = r.complex_vectors ? 1 : 0;
+    }
+  });
+}
+
+int qmbed_gpu_expm_plan(qmbed_operator op, double coef_re, double coef_im, uint64_t max_degree, double tolerance,
+                        uint64_t max_substeps, uint64_t* degree, uint64_t* scaling, double* shift, double* one_norm) {
+  return guarded([&] {
+    ExpmPlan plan = make_expm_plan(*op->op, C64(coef_re, coef_im), max_degree, tolerance, max_substeps);
+    if (degree) *degree = plan.degree;
+    if (scaling) *scaling = plan.scaling;
+    if (shift) {
+      shift[0] = plan.shift.real();
+      shift[1] = plan.shift.imag();
+    }
+    if (one_norm) *one_norm = plan.one_norm;
+  });
+}
+
+int qmbed_gpu_expm_apply_host(qmbed_operator op, double coef_re, double coef_im, uint64_t max_degree,
+                              double tolerance, uint64_t max_substeps, int precision, const double* input,
+                              double* output, uint64_t n_vectors) {
+  return guarded([&] {
+    if (precision != 64 && precision != 32) raise(QMBED_INVALID_OPTIONS, "precision must be 64 or 32");
+    std::lock_guard<std::mutex> lock(op->mu);
+    ExpmPlan plan = make_expm_plan(*op->op, C64(coef_re, coef_im), max_degree, tolerance, max_substeps);
+    const uint64_t n = op->op->dim();
+    BlockOps& ops = op->block_ops();
+    LinearOperatorView view = op->view();
+    DeviceBuffer state64(std::max<uint64_t>(n, 1) * 16), state(std::max<uint64_t>(n, 1) * (precision == 64 ? 16 : 8));
+    for (uint64_t k = 0; k < n_vectors; ++k) {
+      QMBED_CUDA(cudaMemcpyAsync(state64.get(), input + 2 * k * n, n * 16, cudaMemcpyHostToDevice, ops.stream()));
+      ops.convert(state64.get(), 64, state.get(), precision, 2 * n);
+      expm_apply(plan, view, state.get(), precision, ops);
+      ops.convert(state.get(), precision, state64.get(), 64, 2 * n);
+      QMBED_CUDA(cudaMemcpyAsync(output + 2 * k * n, state64.get(), n * 16, cudaMemcpyDeviceToHost, ops.stream()));
+      ops.sync();
+    }
+  });
+}
+
+int qmbed_gpu_deterministic_start(int device, uint64_t n, uint64_t seed, double* out) {
+  return guarded([&] {
+    QMBED_CUDA(cudaSetDevice(device));
+    cudaStream_t stream;
+    QMBED_CUDA(cudaStreamCreate(&stream));
+    {
+      BlockOps ops(device, stream);
+      DeviceBuffer v(std::max<uint64_t>(n, 1) * 8);
+      ops.lcg_start(v.get(), n, seed, 64, false);
+      const double norm = ops.norm(v.get(), n, 64, false);
+      if (!std::isfinite(norm) || norm <= 2.220446049250313e-16) raise_nonconvergence(0, norm);
+      ops.scale(v.get(), n, norm, 64, false);
+      QMBED_CUDA(cudaMemcpyAsync(out, v.get(), n * 8, cudaMemcpyDeviceToHost, stream));
+      ops.sync();
+    }
+    cudaStreamDestroy(stream);
+  });
+}
+
+char* qmbed_run_json(const char* request) { return to_c_string(respond(request, false)); }
+
+char* qmbed_command_json(const char* request) { return to_c_string(respond(request, true)); }
+
+void qmbed_string_free(char* response) { std::free(response); }
+
+char* qmbed_evolve_model_with_drive_json(const char* request, void* callback, void* context) {
+  (void)request;
+  (void)callback;
+  (void)context;
+  return to_c_string(R"({"status":"error","error":"unsupported backend: driven evolution is outside the GPU engine"})");
+}
+
+char* qmbed_register_user_basis_32_json(const char* request, void* op, void* next_state, void* pre_check, void* maps,
+                                        size_t n_maps) {
+  (void)request, (void)op, (void)next_state, (void)pre_check, (void)maps, (void)n_maps;
+  return to_c_string(R"({"status":"error","error":"unsupported backend: user bases are outside the GPU engine"})");
+}
+
+char* qmbed_register_user_basis_64_json(const char* request, void* op, void* next_state, void* pre_check, void* maps,
+                                        size_t n_maps) {
+  (void)request, (void)op, (void)next_state, (void)pre_check, (void)maps, (void)n_maps;
+  return to_c_string(R"({"status":"error","error":"unsupported backend: user bases are outside the GPU engine"})");
+}
+
+}  // extern "C"

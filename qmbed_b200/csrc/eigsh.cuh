@@ -1,0 +1,60 @@
+// Selected Hermitian eigenpairs on the GPU: the reference eigsh dispatch
+// (dense / expanding Lanczos / thick restart) over device vectors.
+#pragma once
+
+#include <complex>
+#include <functional>
+#include <vector>
+
+#include "krylov.cuh"
+
+namespace qmbed {
+
+enum Target : int { kSmallestAlgebraic = 0, kLargestAlgebraic = 1, kSmallestMagnitude = 2, kLargestMagnitude = 3,
+                    kBothEnds = 4, kShift = 5 };
+
+// Reference EigshOptions (src/solve/mod.rs:349-449); krylov_dimension 0 = None.
+struct EigshOptions {
+  size_t eigenpairs = 1;
+  int target = kSmallestAlgebraic;
+  double shift = 0.0;
+  size_t krylov_dimension = 0;
+  double tolerance = 1.0e-10;
+  size_t max_iterations = 1000;
+  uint64_t seed = 0;
+};
+
+enum SolverMode : int {
+  kModePlainFP64 = 0,  // the reference algorithms, FP64 vectors
+  kModeMixed = 1,      // FP32 vectors and H.v, FP64 recurrences, then FP64 refinement to the tolerance
+};
+
+struct EigshResult {
+  std::vector<double> eigenvalues;
+  std::vector<double> residuals;
+  size_t iterations = 0;
+  size_t reorthogonalization_passes = 0;
+  size_t conditional_second_passes = 0;
+  bool converged = true;
+  bool complex_vectors = false;
+  DeviceBuffer vectors;  // FP64, n x k column-major (interleaved complex when complex_vectors)
+  // diagnostics
+  size_t fp32_iterations = 0;
+  size_t fp64_iterations = 0;
+  size_t operator_applications = 0;
+};
+
+// y = A x on device vectors for the given precision (64/32) and complex flag.
+using ApplyFn = std::function<void(int precision, bool cplx, const void* x, void* y)>;
+
+struct LinearOperatorView {
+  uint64_t dim;
+  bool real;  // supports real vectors
+  ApplyFn apply;
+};
+
+// Initial vectors are host arrays of dim complex values (may be empty).
+EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options,
+                  const std::vector<std::vector<C64>>& initial, int mode, BlockOps& ops);
+
+}  // namespace qmbed

@@ -1,0 +1,729 @@
+// Dense vector kernels for Lanczos / thick restart, reductions and the small
+// FP64 Hermitian eigensolver. All reductions accumulate in FP64 through a
+// fixed two-stage tree (per-block partials, then an ordered sum), so results
+// do not depend on scheduling.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "device_util.cuh"
+#include "krylov.cuh"
+
+namespace qmbed {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kChunk = 8;    // columns per pass of the multi-dot
+constexpr int kCombine = 4;  // outputs per pass of the combination kernel
+
+template <typename T, bool CPLX>
+__device__ inline void load(const T* __restrict__ p, uint64_t i, double& re, double& im) {
+  if (CPLX) {
+    re = static_cast<double>(p[2 * i]);
+    im = static_cast<double>(p[2 * i + 1]);
+  } else {
+    re = static_cast<double>(p[i]);
+    im = 0.0;
+  }
+}
+
+template <typename T, bool CPLX>
+__device__ inline void store(T* __restrict__ p, uint64_t i, double re, double im) {
+  if (CPLX) {
+    p[2 * i] = static_cast<T>(re);
+    p[2 * i + 1] = static_cast<T>(im);
+  } else {
+    p[i] = static_cast<T>(re);
+  }
+}
+
+__device__ inline double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// partials[(j * G + block) * 2 + {0,1}] = sum over this block's rows of conj(A_j) w.
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(kThreads) multi_dot_kernel(const T* __restrict__ A, uint64_t ld, int m,
+                                                              const T* __restrict__ w, uint64_t n,
+                                                              double* __restrict__ partials) {
+  __shared__ double red[kThreads / 32][2 * kChunk];
+  const int G = gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t stride = static_cast<uint64_t>(G) * blockDim.x;
+  for (int j0 = 0; j0 < m; j0 += kChunk) {
+    const int cnt = min(kChunk, m - j0);
+    double ar[kChunk], ai[kChunk];
+#pragma unroll
+    for (int jj = 0; jj < kChunk; ++jj) ar[jj] = ai[jj] = 0.0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+      double wr, wi;
+      load<T, CPLX>(w, i, wr, wi);
+#pragma unroll
+      for (int jj = 0; jj < kChunk; ++jj) {
+        if (jj < cnt) {
+          double xr, xi;
+          load<T, CPLX>(A + (j0 + jj) * ld * (CPLX ? 2 : 1), i, xr, xi);
+          ar[jj] += xr * wr + xi * wi;
+          ai[jj] += xr * wi - xi * wr;
+        }
+      }
+    }
+#pragma unroll
+    for (int jj = 0; jj < kChunk; ++jj) {
+      double a = warp_sum(ar[jj]);
+      double b = warp_sum(ai[jj]);
+      if (lane == 0) {
+        red[warp][2 * jj] = a;
+        red[warp][2 * jj + 1] = b;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * cnt) {
+      double total = 0.0;
+      for (int wv = 0; wv < kThreads / 32; ++wv) total += red[wv][threadIdx.x];
+      const int j = j0 + threadIdx.x / 2;
+      partials[(static_cast<uint64_t>(j) * G + blockIdx.x) * 2 + (threadIdx.x & 1)] = total;
+    }
+    __syncthreads();
+  }
+}
+
+// out[t] = sum_b partials[(t/2 * G + b) * 2 + t%2], in block order.
+__global__ void finish_kernel(const double* __restrict__ partials, int G, int count, double* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const int j = t / 2, c = t & 1;
+  double total = 0.0;
+  for (int b = 0; b < G; ++b) total += partials[(static_cast<uint64_t>(j) * G + b) * 2 + c];
+  out[t] = total;
+}
+
+// w -= sum_j h_j A_j; per-block partial of ||w||^2 when `partials` is set.
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(kThreads) subtract_kernel(const T* __restrict__ A, uint64_t ld, int m,
+                                                             const double* __restrict__ h, T* __restrict__ w,
+                                                             uint64_t n, double* __restrict__ partials) {
+  extern __shared__ double hs[];
+  for (int t = threadIdx.x; t < 2 * m; t += blockDim.x) hs[t] = h[t];
+  __syncthreads();
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  double sq = 0.0;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double sr = 0.0, si = 0.0;
+    for (int j = 0; j < m; ++j) {
+      double xr, xi;
+      load<T, CPLX>(A + j * ld * (CPLX ? 2 : 1), i, xr, xi);
+      const double hr = hs[2 * j], hi = hs[2 * j + 1];
+      sr += hr * xr - hi * xi;
+      si += hr * xi + hi * xr;
+    }
+    double wr, wi;
+    load<T, CPLX>(w, i, wr, wi);
+    wr -= sr;
+    wi -= si;
+    store<T, CPLX>(w, i, wr, wi);
+    if (partials) {
+      load<T, CPLX>(w, i, wr, wi);  // norm of the stored (rounded) value
+      sq += wr * wr + wi * wi;
+    }
+  }
+  if (partials) {
+    __shared__ double red[kThreads / 32];
+    sq = warp_sum(sq);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double total = 0.0;
+      for (int wv = 0; wv < kThreads / 32; ++wv) total += red[wv];
+      partials[2 * blockIdx.x] = total;
+      partials[2 * blockIdx.x + 1] = 0.0;
+    }
+  }
+}
+
+// out_k = sum_j Y[j + m k] A_j for k in [k0, k0 + kCombine).
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(kThreads) combine_kernel(const T* __restrict__ A, uint64_t ld, int m,
+                                                            const double* __restrict__ Y, int K, int k0,
+                                                            T* __restrict__ out, uint64_t ld_out, uint64_t n) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  const int cnt = min(kCombine, K - k0);
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double ar[kCombine], ai[kCombine];
+#pragma unroll
+    for (int kk = 0; kk < kCombine; ++kk) ar[kk] = ai[kk] = 0.0;
+    for (int j = 0; j < m; ++j) {
+      double xr, xi;
+      load<T, CPLX>(A + j * ld * (CPLX ? 2 : 1), i, xr, xi);
+#pragma unroll
+      for (int kk = 0; kk < kCombine; ++kk) {
+        if (kk < cnt) {
+          const uint64_t y = (static_cast<uint64_t>(k0 + kk) * m + j) * 2;
+          const double yr = __ldg(Y + y), yi = __ldg(Y + y + 1);
+          ar[kk] += yr * xr - yi * xi;
+          ai[kk] += yr * xi + yi * xr;
+        }
+      }
+    }
+#pragma unroll
+    for (int kk = 0; kk < kCombine; ++kk)
+      if (kk < cnt) store<T, CPLX>(out + (k0 + kk) * ld_out * (CPLX ? 2 : 1), i, ar[kk], ai[kk]);
+  }
+}
+
+template <typename T>
+__global__ void scale_kernel(T* __restrict__ w, uint64_t count, double divisor) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride)
+    w[i] = static_cast<T>(static_cast<double>(w[i]) / divisor);
+}
+
+template <typename S, typename D>
+__global__ void convert_kernel(const S* __restrict__ src, D* __restrict__ dst, uint64_t count) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride)
+    dst[i] = static_cast<D>(src[i]);
+}
+
+// Affine LCG state after k steps: x -> a x + c (mod 2^64), by squaring.
+__device__ inline uint64_t lcg_jump(uint64_t x, uint64_t k) {
+  uint64_t A = 1, C = 0;                                       // accumulated map
+  uint64_t a = 6364136223846793005ULL, c = 1442695040888963407ULL;  // current power
+  while (k) {
+    if (k & 1) {
+      A = a * A;
+      C = a * C + c;
+    }
+    c = a * c + c;
+    a = a * a;
+    k >>= 1;
+  }
+  return A * x + C;
+}
+
+template <typename T, bool CPLX>
+__global__ void lcg_start_kernel(T* __restrict__ out, uint64_t n, uint64_t seed, uint64_t per_thread) {
+  const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t i0 = t * per_thread;
+  if (i0 >= n) return;
+  const uint64_t i1 = min(i0 + per_thread, n);
+  uint64_t state = lcg_jump(seed | 1ULL, i0);
+  for (uint64_t i = i0; i < i1; ++i) {
+    state = state * 6364136223846793005ULL + 1442695040888963407ULL;
+    const uint64_t mantissa = state >> 11;
+    const double value = static_cast<double>(mantissa) / 9007199254740992.0 - 0.5;
+    store<T, CPLX>(out, i, value, 0.0);
+  }
+}
+
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(kThreads) residual_kernel(const T* __restrict__ y, const T* __restrict__ x,
+                                                             double lambda, uint64_t n,
+                                                             double* __restrict__ partials) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  double sq = 0.0;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double yr, yi, xr, xi;
+    load<T, CPLX>(y, i, yr, yi);
+    load<T, CPLX>(x, i, xr, xi);
+    const double dr = yr - lambda * xr, di = yi - lambda * xi;
+    sq += dr * dr + di * di;
+  }
+  __shared__ double red[kThreads / 32];
+  sq = warp_sum(sq);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double total = 0.0;
+    for (int wv = 0; wv < kThreads / 32; ++wv) total += red[wv];
+    partials[2 * blockIdx.x] = total;
+    partials[2 * blockIdx.x + 1] = 0.0;
+  }
+}
+
+// --- scans and reductions used by assembly -------------------------------------------
+constexpr int kScanItems = 4;
+
+__global__ void scan_block_totals_kernel(const uint32_t* __restrict__ counts, uint64_t n,
+                                         uint64_t* __restrict__ totals) {
+  const uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * kScanItems;
+  uint32_t local = 0;
+  for (int k = 0; k < kScanItems; ++k)
+    if (base + k < n) local += counts[base + k];
+  uint32_t total = block_reduce_sum_u32(local);
+  if (threadIdx.x == 0) totals[blockIdx.x] = total;
+}
+
+template <typename IDX>
+__global__ void scan_write_kernel(const uint32_t* __restrict__ counts, uint64_t n,
+                                  const uint64_t* __restrict__ block_offsets, IDX* __restrict__ out) {
+  const uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * kScanItems;
+  uint32_t local[kScanItems];
+  uint32_t sum = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    local[k] = base + k < n ? counts[base + k] : 0u;
+    sum += local[k];
+  }
+  uint64_t running = block_offsets[blockIdx.x] + block_exclusive_scan_u32(sum);
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k <= n) out[base + k] = static_cast<IDX>(running);
+    running += local[k];
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) sum_complex_kernel(const double* __restrict__ v, uint64_t n,
+                                                                double* __restrict__ partials) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  double re = 0.0, im = 0.0;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    re += v[2 * i];
+    im += v[2 * i + 1];
+  }
+  __shared__ double red[kThreads / 32][2];
+  re = warp_sum(re);
+  im = warp_sum(im);
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5][0] = re;
+    red[threadIdx.x >> 5][1] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double total = 0.0;
+    for (int wv = 0; wv < kThreads / 32; ++wv) total += red[wv][threadIdx.x];
+    partials[2 * blockIdx.x + threadIdx.x] = total;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) max_shifted_kernel(const double* __restrict__ diag,
+                                                                const double* __restrict__ offsum, uint64_t n,
+                                                                double sr, double si, double* __restrict__ partials) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  double m = 0.0;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    m = fmax(m, offsum[i] + hypot(diag[2 * i] - sr, diag[2 * i + 1] - si));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[kThreads / 32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double total = 0.0;
+    for (int wv = 0; wv < kThreads / 32; ++wv) total = fmax(total, red[wv]);
+    partials[blockIdx.x] = total;
+  }
+}
+
+// --- parallel cyclic Jacobi (one CTA) ---------------------------------------------------
+// A: np x np row-major complex (interleaved), V: np x np column-major complex.
+// Round-robin ordering pairs np/2 disjoint (p,q) per round; each rotation
+// zeroes |a_pq| after removing its phase (complex Jacobi rotation).
+__global__ void __launch_bounds__(1024) jacobi_kernel(int np, double* __restrict__ A, double* __restrict__ V,
+                                                      int max_sweeps) {
+  extern __shared__ int order[];
+  __shared__ double c_s[512], s_s[512], pr_s[512], pi_s[512];
+  __shared__ int p_s[512], q_s[512];
+  __shared__ double red[32][2];
+  __shared__ int done;
+  __shared__ double previous_off;
+  const int half = np / 2;
+  // Converged when the off-diagonal mass is at rounding level for this size,
+  // or when a sweep no longer reduces it (rounding floor reached).
+  const double floor_rel = (2.220446049250313e-16 * np) * (2.220446049250313e-16 * np) * 1e-2;
+  if (threadIdx.x == 0) previous_off = -1.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) order[i] = i;
+  for (int idx = threadIdx.x; idx < np * np; idx += blockDim.x) {
+    V[2 * idx] = (idx / np == idx % np) ? 1.0 : 0.0;
+    V[2 * idx + 1] = 0.0;
+  }
+  __syncthreads();
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    double off = 0.0, total = 0.0;
+    for (int idx = threadIdx.x; idx < np * np; idx += blockDim.x) {
+      const double v = A[2 * idx] * A[2 * idx] + A[2 * idx + 1] * A[2 * idx + 1];
+      total += v;
+      if (idx / np != idx % np) off += v;
+    }
+    off = warp_sum(off);
+    total = warp_sum(total);
+    if ((threadIdx.x & 31) == 0) {
+      red[threadIdx.x >> 5][0] = off;
+      red[threadIdx.x >> 5][1] = total;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double o = 0.0, t = 0.0;
+      for (int wv = 0; wv < static_cast<int>(blockDim.x >> 5); ++wv) {
+        o += red[wv][0];
+        t += red[wv][1];
+      }
+      done = (o <= floor_rel * t || o == 0.0 || (sweep > 2 && previous_off >= 0.0 && o >= 0.25 * previous_off)) ? 1 : 0;
+      previous_off = o;
+    }
+    __syncthreads();
+    if (done) break;
+    for (int round = 0; round < np - 1; ++round) {
+      for (int t = threadIdx.x; t < half; t += blockDim.x) {
+        int p = order[t], q = order[np - 1 - t];
+        if (p > q) {
+          const int tmp = p;
+          p = q;
+          q = tmp;
+        }
+        p_s[t] = p;
+        q_s[t] = q;
+        const double br = A[2 * (p * np + q)], bi = A[2 * (p * np + q) + 1];
+        const double mag = hypot(br, bi);
+        if (mag == 0.0) {
+          c_s[t] = 1.0;
+          s_s[t] = 0.0;
+          pr_s[t] = 1.0;
+          pi_s[t] = 0.0;
+        } else {
+          const double app = A[2 * (p * np + p)], aqq = A[2 * (q * np + q)];
+          const double theta = (aqq - app) / (2.0 * mag);
+          const double tt = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          const double c = 1.0 / sqrt(tt * tt + 1.0);
+          c_s[t] = c;
+          s_s[t] = tt * c;
+          pr_s[t] = br / mag;
+          pi_s[t] = bi / mag;
+        }
+      }
+      __syncthreads();
+      // rows: A <- J^H A
+      for (int idx = threadIdx.x; idx < half * np; idx += blockDim.x) {
+        const int t = idx / np, k = idx % np;
+        const int p = p_s[t], q = q_s[t];
+        const double c = c_s[t], s = s_s[t], fr = pr_s[t], fi = pi_s[t];
+        const double apr = A[2 * (p * np + k)], api = A[2 * (p * np + k) + 1];
+        const double aqr = A[2 * (q * np + k)], aqi = A[2 * (q * np + k) + 1];
+        // p: c a_p - s phase a_q ; q: s conj(phase) a_p + c a_q
+        A[2 * (p * np + k)] = c * apr - s * (fr * aqr - fi * aqi);
+        A[2 * (p * np + k) + 1] = c * api - s * (fr * aqi + fi * aqr);
+        A[2 * (q * np + k)] = s * (fr * apr + fi * api) + c * aqr;
+        A[2 * (q * np + k) + 1] = s * (fr * api - fi * apr) + c * aqi;
+      }
+      __syncthreads();
+      // columns: A <- A J, V <- V J
+      for (int idx = threadIdx.x; idx < half * np; idx += blockDim.x) {
+        const int t = idx / np, k = idx % np;
+        const int p = p_s[t], q = q_s[t];
+        const double c = c_s[t], s = s_s[t], fr = pr_s[t], fi = pi_s[t];
+        {
+          const double apr = A[2 * (k * np + p)], api = A[2 * (k * np + p) + 1];
+          const double aqr = A[2 * (k * np + q)], aqi = A[2 * (k * np + q) + 1];
+          // p: c a_p - s conj(phase) a_q ; q: s phase a_p + c a_q
+          A[2 * (k * np + p)] = c * apr - s * (fr * aqr + fi * aqi);
+          A[2 * (k * np + p) + 1] = c * api - s * (fr * aqi - fi * aqr);
+          A[2 * (k * np + q)] = s * (fr * apr - fi * api) + c * aqr;
+          A[2 * (k * np + q) + 1] = s * (fr * api + fi * apr) + c * aqi;
+        }
+        {
+          const double vpr = V[2 * (p * np + k)], vpi = V[2 * (p * np + k) + 1];
+          const double vqr = V[2 * (q * np + k)], vqi = V[2 * (q * np + k) + 1];
+          V[2 * (p * np + k)] = c * vpr - s * (fr * vqr + fi * vqi);
+          V[2 * (p * np + k) + 1] = c * vpi - s * (fr * vqi - fi * vqr);
+          V[2 * (q * np + k)] = s * (fr * vpr - fi * vpi) + c * vqr;
+          V[2 * (q * np + k) + 1] = s * (fr * vpi + fi * vpr) + c * vqi;
+        }
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < half; t += blockDim.x) {
+        const int p = p_s[t], q = q_s[t];
+        if (c_s[t] != 1.0 || s_s[t] != 0.0) {
+          A[2 * (p * np + q)] = A[2 * (p * np + q) + 1] = 0.0;
+          A[2 * (q * np + p)] = A[2 * (q * np + p) + 1] = 0.0;
+          A[2 * (p * np + p) + 1] = 0.0;
+          A[2 * (q * np + q) + 1] = 0.0;
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        const int last = order[np - 1];
+        for (int i = np - 1; i > 1; --i) order[i] = order[i - 1];
+        order[1] = last;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+int sm_count(int device) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return sms;
+}
+
+int reduction_grid(uint64_t n, int sms) {
+  uint64_t blocks = (n + kThreads - 1) / kThreads;
+  return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(blocks, static_cast<uint64_t>(4) * sms)));
+}
+
+int stream_grid(uint64_t n, int sms) {
+  uint64_t blocks = (n + kThreads - 1) / kThreads;
+  return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(blocks, static_cast<uint64_t>(8) * sms)));
+}
+
+}  // namespace
+
+uint64_t exclusive_scan_counts(const uint32_t* counts, uint64_t n, DeviceBuffer& row_ptr, bool* is64) {
+  const uint64_t per_block = static_cast<uint64_t>(kThreads) * kScanItems;
+  const uint64_t blocks = std::max<uint64_t>(1, (n + 1 + per_block - 1) / per_block);
+  DeviceBuffer totals(blocks * sizeof(uint64_t));
+  scan_block_totals_kernel<<<static_cast<unsigned>(blocks), kThreads>>>(counts, n, totals.as<uint64_t>());
+  QMBED_LAUNCH_CHECK();
+  std::vector<uint64_t> host(blocks);
+  QMBED_CUDA(cudaMemcpy(host.data(), totals.get(), blocks * 8, cudaMemcpyDeviceToHost));
+  uint64_t running = 0;
+  for (uint64_t b = 0; b < blocks; ++b) {
+    const uint64_t t = host[b];
+    host[b] = running;
+    running += t;
+  }
+  QMBED_CUDA(cudaMemcpy(totals.get(), host.data(), blocks * 8, cudaMemcpyHostToDevice));
+  *is64 = running >= (1ULL << 32);
+  if (*is64) {
+    row_ptr.allocate((n + 1) * sizeof(uint64_t));
+    scan_write_kernel<uint64_t><<<static_cast<unsigned>(blocks), kThreads>>>(counts, n, totals.as<uint64_t>(),
+                                                                            row_ptr.as<uint64_t>());
+  } else {
+    row_ptr.allocate((n + 1) * sizeof(uint32_t));
+    scan_write_kernel<uint32_t><<<static_cast<unsigned>(blocks), kThreads>>>(counts, n, totals.as<uint64_t>(),
+                                                                            row_ptr.as<uint32_t>());
+  }
+  QMBED_LAUNCH_CHECK();
+  return running;
+}
+
+C64 device_sum_complex(const double* v, uint64_t n) {
+  int device = 0;
+  cudaGetDevice(&device);
+  const int G = reduction_grid(n, sm_count(device));
+  DeviceBuffer partials(2 * G * sizeof(double));
+  sum_complex_kernel<<<G, kThreads>>>(v, n, partials.as<double>());
+  QMBED_LAUNCH_CHECK();
+  std::vector<double> host(2 * G);
+  QMBED_CUDA(cudaMemcpy(host.data(), partials.get(), host.size() * 8, cudaMemcpyDeviceToHost));
+  double re = 0.0, im = 0.0;
+  for (int b = 0; b < G; ++b) {
+    re += host[2 * b];
+    im += host[2 * b + 1];
+  }
+  return C64(re, im);
+}
+
+double device_max_shifted_column(const double* diag, const double* offsum, uint64_t n, C64 shift) {
+  int device = 0;
+  cudaGetDevice(&device);
+  const int G = reduction_grid(n, sm_count(device));
+  DeviceBuffer partials(G * sizeof(double));
+  max_shifted_kernel<<<G, kThreads>>>(diag, offsum, n, shift.real(), shift.imag(), partials.as<double>());
+  QMBED_LAUNCH_CHECK();
+  std::vector<double> host(G);
+  QMBED_CUDA(cudaMemcpy(host.data(), partials.get(), host.size() * 8, cudaMemcpyDeviceToHost));
+  double m = 0.0;
+  for (double v : host) m = std::max(m, v);
+  return m;
+}
+
+BlockOps::BlockOps(int device, cudaStream_t stream) : device_(device), stream_(stream) {
+  QMBED_CUDA(cudaSetDevice(device_));
+  sms_ = sm_count(device_);
+}
+
+BlockOps::~BlockOps() {
+  if (host_results_) cudaFreeHost(host_results_);
+}
+
+void BlockOps::ensure_partials(size_t doubles) {
+  if (partials_doubles_ < doubles) {
+    partials_.allocate(doubles * sizeof(double));
+    partials_doubles_ = doubles;
+  }
+  if (host_results_doubles_ < doubles) {
+    if (host_results_) cudaFreeHost(host_results_);
+    host_results_ = nullptr;
+    QMBED_CUDA(cudaMallocHost(&host_results_, doubles * sizeof(double)));
+    host_results_doubles_ = doubles;
+    results_.allocate(doubles * sizeof(double));
+  }
+}
+
+void BlockOps::ensure_coeffs(size_t bytes) {
+  if (coeffs_bytes_ < bytes) {
+    coeffs_.allocate(bytes);
+    coeffs_bytes_ = bytes;
+  }
+}
+
+void BlockOps::sync() { QMBED_CUDA(cudaStreamSynchronize(stream_)); }
+
+#define QMBED_DISPATCH(precision, cplx, KERNEL_CALL)          \
+  do {                                                        \
+    if ((precision) == 64) {                                  \
+      using T = double;                                       \
+      if (cplx) { constexpr bool C = true; KERNEL_CALL; }     \
+      else { constexpr bool C = false; KERNEL_CALL; }         \
+    } else {                                                  \
+      using T = float;                                        \
+      if (cplx) { constexpr bool C = true; KERNEL_CALL; }     \
+      else { constexpr bool C = false; KERNEL_CALL; }         \
+    }                                                         \
+  } while (0)
+
+void BlockOps::dots(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx,
+                    C64* out) {
+  if (m <= 0) return;
+  const int G = reduction_grid(n, sms_);
+  ensure_partials(static_cast<size_t>(m) * G * 2 + 2 * static_cast<size_t>(m) + 64);
+  QMBED_DISPATCH(precision, cplx,
+                 (multi_dot_kernel<T, C><<<G, kThreads, 0, stream_>>>(static_cast<const T*>(A), ld, m,
+                                                                      static_cast<const T*>(w), n,
+                                                                      partials_.as<double>())));
+  QMBED_LAUNCH_CHECK();
+  const int count = 2 * m;
+  finish_kernel<<<(count + 127) / 128, 128, 0, stream_>>>(partials_.as<double>(), G, count, results_.as<double>());
+  QMBED_LAUNCH_CHECK();
+  QMBED_CUDA(cudaMemcpyAsync(host_results_, results_.get(), count * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  sync();
+  for (int j = 0; j < m; ++j) out[j] = C64(host_results_[2 * j], host_results_[2 * j + 1]);
+}
+
+double BlockOps::norm(const void* w, uint64_t n, int precision, bool cplx) {
+  C64 v;
+  dots(w, n, 1, w, n, precision, cplx, &v);
+  return std::sqrt(std::max(v.real(), 0.0));
+}
+
+double BlockOps::subtract(const void* A, uint64_t ld, int m, const C64* h, void* w, uint64_t n, int precision,
+                          bool cplx, bool want_norm) {
+  if (m <= 0 && !want_norm) return 0.0;
+  if (m <= 0) return norm(w, n, precision, cplx);
+  ensure_coeffs(static_cast<size_t>(m) * 16);
+  QMBED_CUDA(cudaMemcpyAsync(coeffs_.get(), h, static_cast<size_t>(m) * 16, cudaMemcpyHostToDevice, stream_));
+  const int G = reduction_grid(n, sms_);
+  ensure_partials(2 * static_cast<size_t>(G) + 64);
+  const size_t smem = static_cast<size_t>(m) * 16;
+  double* partials = want_norm ? partials_.as<double>() : nullptr;
+  QMBED_DISPATCH(precision, cplx, ({
+                   auto kernel = subtract_kernel<T, C>;
+                   if (smem > 48 * 1024)
+                     QMBED_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     static_cast<int>(smem)));
+                   kernel<<<G, kThreads, smem, stream_>>>(static_cast<const T*>(A), ld, m, coeffs_.as<double>(),
+                                                          static_cast<T*>(w), n, partials);
+                 }));
+  QMBED_LAUNCH_CHECK();
+  if (!want_norm) return 0.0;
+  QMBED_CUDA(cudaMemcpyAsync(host_results_, partials_.get(), 2 * G * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  sync();
+  double total = 0.0;
+  for (int b = 0; b < G; ++b) total += host_results_[2 * b];
+  return std::sqrt(total);
+}
+
+void BlockOps::combine(const void* A, uint64_t ld, int m, const C64* Y, int K, void* out, uint64_t ld_out, uint64_t n,
+                       int precision, bool cplx) {
+  if (K <= 0) return;
+  ensure_coeffs(static_cast<size_t>(m) * K * 16);
+  QMBED_CUDA(cudaMemcpyAsync(coeffs_.get(), Y, static_cast<size_t>(m) * K * 16, cudaMemcpyHostToDevice, stream_));
+  const int G = stream_grid(n, sms_);
+  for (int k0 = 0; k0 < K; k0 += kCombine) {
+    QMBED_DISPATCH(precision, cplx,
+                   (combine_kernel<T, C><<<G, kThreads, 0, stream_>>>(static_cast<const T*>(A), ld, m,
+                                                                      coeffs_.as<double>(), K, k0,
+                                                                      static_cast<T*>(out), ld_out, n)));
+    QMBED_LAUNCH_CHECK();
+  }
+  sync();  // Y lives in caller memory reused on the next call
+}
+
+void BlockOps::scale(void* w, uint64_t n, double divisor, int precision, bool cplx) {
+  const uint64_t count = n * (cplx ? 2 : 1);
+  const int G = stream_grid(count, sms_);
+  if (precision == 64) scale_kernel<double><<<G, kThreads, 0, stream_>>>(static_cast<double*>(w), count, divisor);
+  else scale_kernel<float><<<G, kThreads, 0, stream_>>>(static_cast<float*>(w), count, divisor);
+  QMBED_LAUNCH_CHECK();
+}
+
+void BlockOps::convert(const void* src, int src_precision, void* dst, int dst_precision, uint64_t elements) {
+  const int G = stream_grid(elements, sms_);
+  if (src_precision == dst_precision) {
+    copy(src, dst, elements * (src_precision == 64 ? 8 : 4));
+    return;
+  }
+  if (src_precision == 64)
+    convert_kernel<double, float><<<G, kThreads, 0, stream_>>>(static_cast<const double*>(src),
+                                                               static_cast<float*>(dst), elements);
+  else
+    convert_kernel<float, double><<<G, kThreads, 0, stream_>>>(static_cast<const float*>(src),
+                                                               static_cast<double*>(dst), elements);
+  QMBED_LAUNCH_CHECK();
+}
+
+void BlockOps::copy(const void* src, void* dst, uint64_t bytes) {
+  if (bytes == 0 || src == dst) return;
+  QMBED_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream_));
+}
+
+void BlockOps::lcg_start(void* out, uint64_t n, uint64_t seed, int precision, bool cplx) {
+  const uint64_t per_thread = 64;
+  const uint64_t threads = (n + per_thread - 1) / per_thread;
+  const unsigned blocks = static_cast<unsigned>(std::max<uint64_t>(1, (threads + kThreads - 1) / kThreads));
+  QMBED_DISPATCH(precision, cplx,
+                 (lcg_start_kernel<T, C><<<blocks, kThreads, 0, stream_>>>(static_cast<T*>(out), n, seed,
+                                                                           per_thread)));
+  QMBED_LAUNCH_CHECK();
+}
+
+double BlockOps::residual_norm(const void* y, const void* x, double lambda, uint64_t n, int precision, bool cplx) {
+  const int G = reduction_grid(n, sms_);
+  ensure_partials(2 * static_cast<size_t>(G) + 64);
+  QMBED_DISPATCH(precision, cplx,
+                 (residual_kernel<T, C><<<G, kThreads, 0, stream_>>>(static_cast<const T*>(y),
+                                                                     static_cast<const T*>(x), lambda, n,
+                                                                     partials_.as<double>())));
+  QMBED_LAUNCH_CHECK();
+  QMBED_CUDA(cudaMemcpyAsync(host_results_, partials_.get(), 2 * G * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  sync();
+  double total = 0.0;
+  for (int b = 0; b < G; ++b) total += host_results_[2 * b];
+  return std::sqrt(total);
+}
+
+void device_hermitian_eigen(int n, const std::vector<C64>& a, std::vector<double>& values, std::vector<C64>& vectors,
+                            cudaStream_t stream) {
+  values.assign(n, 0.0);
+  vectors.assign(static_cast<size_t>(n) * n, C64(0.0, 0.0));
+  if (n == 0) return;
+  if (n == 1) {
+    values[0] = a[0].real();
+    vectors[0] = C64(1.0, 0.0);
+    return;
+  }
+  if (n > 1024) raise(QMBED_UNSUPPORTED_BACKEND, "projected eigenproblems above 1024 are not supported");
+  const int np = n + (n & 1);
+  std::vector<double> host(2 * static_cast<size_t>(np) * np, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      host[2 * (static_cast<size_t>(i) * np + j)] = a[static_cast<size_t>(i) * n + j].real();
+      host[2 * (static_cast<size_t>(i) * np + j) + 1] = a[static_cast<size_t>(i) * n + j].imag();
+    }
+  DeviceBuffer dA(host.size() * 8), dV(host.size() * 8);
+  QMBED_CUDA(cudaMemcpyAsync(dA.get(), host.data(), host.size() * 8, cudaMemcpyHostToDevice, stream));
+  const int threads = std::min(1024, std::max(32, ((np / 2 * np) + 31) / 32 * 32));
+  jacobi_kernel<<<1, threads, np * sizeof(int), stream>>>(np, dA.as<double>(), dV.as<double>(), 100);
+  QMBED_LAUNCH_CHECK();
+  std::vector<double> hv(host.size());
+  QMBED_CUDA(cudaMemcpyAsync(host.data(), dA.get(), host.size() * 8, cudaMemcpyDeviceToHost, stream));
+  QMBED_CUDA(cudaMemcpyAsync(hv.data(), dV.get(), hv.size() * 8, cudaMemcpyDeviceToHost, stream));
+  QMBED_CUDA(cudaStreamSynchronize(stream));
+  for (int i = 0; i < n; ++i) values[i] = host[2 * (static_cast<size_t>(i) * np + i)];
+  for (int col = 0; col < n; ++col)
+    for (int row = 0; row < n; ++row)
+      vectors[static_cast<size_t>(col) * n + row] =
+          C64(hv[2 * (static_cast<size_t>(col) * np + row)], hv[2 * (static_cast<size_t>(col) * np + row) + 1]);
+}
+
+}  // namespace qmbed

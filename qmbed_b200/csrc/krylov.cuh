@@ -1,0 +1,70 @@
+// Dense vector kernels for the Krylov solvers (K5/K6), small FP64 eigensolver
+// on the GPU (K7) and device reductions. Every reduction accumulates in FP64
+// over a fixed tree, so reruns are bitwise reproducible.
+#pragma once
+
+#include <complex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace qmbed {
+
+using C64 = std::complex<double>;
+
+// row_ptr = exclusive scan of per-row counts (u32 when the total fits).
+uint64_t exclusive_scan_counts(const uint32_t* counts, uint64_t n, DeviceBuffer& row_ptr, bool* is64);
+C64 device_sum_complex(const double* interleaved, uint64_t n);
+double device_max_shifted_column(const double* diag, const double* offsum, uint64_t n, C64 shift);
+
+// Column-major panels of `n`-element vectors with leading dimension `ld`
+// (elements, complex counted once). Precision 64 or 32, real or complex.
+class BlockOps {
+ public:
+  BlockOps(int device, cudaStream_t stream);
+  ~BlockOps();
+  BlockOps(const BlockOps&) = delete;
+  BlockOps& operator=(const BlockOps&) = delete;
+
+  cudaStream_t stream() const { return stream_; }
+  int sms() const { return sms_; }
+
+  // out[j] = <A_j, w> (conjugate-linear in A) for j < m.
+  void dots(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx, C64* out);
+  double norm(const void* w, uint64_t n, int precision, bool cplx);
+  // w -= sum_j h_j A_j; returns ||w|| afterwards when `want_norm`.
+  double subtract(const void* A, uint64_t ld, int m, const C64* h, void* w, uint64_t n, int precision, bool cplx,
+                  bool want_norm);
+  // out_k = sum_j Y[j + m k] A_j for k < K.
+  void combine(const void* A, uint64_t ld, int m, const C64* Y, int K, void* out, uint64_t ld_out, uint64_t n,
+               int precision, bool cplx);
+  void scale(void* w, uint64_t n, double factor, int precision, bool cplx);
+  // dst (dst_precision) = src (src_precision), `elements` scalars (complex = 2).
+  void convert(const void* src, int src_precision, void* dst, int dst_precision, uint64_t elements);
+  void copy(const void* src, void* dst, uint64_t bytes);
+  // Reference LCG start vector (deterministic_start, src/solve/mod.rs:729-742),
+  // unnormalised, real part only; imaginary parts zero for complex vectors.
+  void lcg_start(void* out, uint64_t n, uint64_t seed, int precision, bool cplx);
+  // r = y - lambda x; returns ||r||  (FP64 accumulation).
+  double residual_norm(const void* y, const void* x, double lambda, uint64_t n, int precision, bool cplx);
+  void sync();
+
+ private:
+  void ensure_partials(size_t doubles);
+  void ensure_coeffs(size_t bytes);
+  int device_;
+  cudaStream_t stream_;
+  int sms_ = 148;
+  DeviceBuffer partials_, results_, coeffs_;
+  size_t partials_doubles_ = 0, coeffs_bytes_ = 0;
+  double* host_results_ = nullptr;  // pinned
+  size_t host_results_doubles_ = 0;
+};
+
+// Eigen-decomposition of a small dense Hermitian matrix (row-major, n <= 2048)
+// by parallel cyclic Jacobi in one CTA. Values are returned unsorted with
+// column-major eigenvectors.
+void device_hermitian_eigen(int n, const std::vector<C64>& a, std::vector<double>& values, std::vector<C64>& vectors,
+                            cudaStream_t stream);
+
+}  // namespace qmbed

@@ -1,0 +1,114 @@
+// Spin-chain Hamiltonian on a sector basis: matrix-free action and packed
+// sparse storage, both built from the same per-row term expansion.
+#pragma once
+
+#include <complex>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "basis.cuh"
+
+namespace qmbed {
+
+using C64 = std::complex<double>;
+
+struct CouplingDesc {
+  C64 coefficient;
+  std::vector<int> sites;
+};
+
+// One local operator product (reference OperatorSpec, src/operator/mod.rs:195-319).
+struct TermDesc {
+  std::string symbols;  // one character per site: I z + - x y (reference LocalOperator::symbol)
+  std::vector<CouplingDesc> couplings;
+};
+
+// One coupling of one product, ready for the device. `sym`/`site` are the
+// product in application order: position n-1 acts first, like the reference
+// visit loop (src/basis/mod.rs:1150-1228).
+struct Instance {
+  double cr, ci;   // coefficient used in the column-form value
+  int n;           // arity
+  int diagonal;    // every symbol is I or z: the target is the source state
+  char sym[kMaxArity];
+  uint8_t site[kMaxArity];
+};
+
+struct LocalFactors {
+  double z[2];       // z action on digit 0 / 1
+  double raise;      // + on digit 0
+  double lower;      // - on digit 1
+  double xy_scale;   // x/y branch scale
+};
+
+enum StorageKind : int {
+  kStorageMatrixFree = 0,  // expand terms on every application
+  kStoragePacked = 1,      // u32 entries: column | value code << column bits (real operators)
+  kStorageWide = 2,        // u32 columns + explicit values
+};
+
+enum Precision : int { kFP64 = 64, kFP32 = 32 };
+
+struct OperatorChecks {
+  bool hermiticity = true;
+  bool particle_conservation = true;
+};
+
+class SpinOperator {
+ public:
+  SpinOperator(std::shared_ptr<SpinBasis> basis, const std::vector<TermDesc>& terms, const OperatorChecks& checks,
+               int storage);
+
+  uint64_t dim() const { return basis_->dim(); }
+  bool is_real() const { return real_; }
+  int storage() const { return storage_; }
+  const SpinBasis& basis() const { return *basis_; }
+  std::shared_ptr<SpinBasis> basis_ptr() const { return basis_; }
+  uint64_t nnz_offdiag() const { return nnz_off_; }
+  int value_codes() const { return n_codes_; }
+  double assembly_seconds() const { return assembly_seconds_; }
+
+  // y = H x on device vectors. Real operators take real vectors unless
+  // `complex_vectors`; complex operators always take interleaved complex.
+  // `force_matrix_free` runs the on-the-fly expansion regardless of storage.
+  void apply(int precision, bool complex_vectors, const void* x, void* y, cudaStream_t stream,
+             bool force_matrix_free = false) const;
+
+  // Dense Hermitian check of the assembled operator at tolerance 1e-12
+  // (OperatorBuilder::build + is_hermitian, src/operator/mod.rs:2212).
+  bool check_hermitian() const;
+
+  // Assembled rows on the host (for tests): row pointer, columns, values.
+  void export_csr(std::vector<uint64_t>& row_ptr, std::vector<uint32_t>& cols, std::vector<C64>& values) const;
+
+  // Exact stored 1-norm and trace shift (shifted_trace_and_one_norm,
+  // src/solve/mod.rs:59-104), computed on the device.
+  void trace_and_one_norm(C64* shift, double* one_norm) const;
+
+  // Bytes per application in the operand model D(b_state + s_y) + (D + nnz_off) s_x.
+  double operand_bytes(int precision, bool complex_vectors) const;
+
+ private:
+  void build_instances(const std::vector<TermDesc>& terms, const OperatorChecks& checks);
+  void assemble();
+  void ensure_scratch(int precision, bool complex_vectors) const;
+
+  std::shared_ptr<SpinBasis> basis_;
+  int storage_;
+  bool real_ = true;
+  LocalFactors factors_{};
+  int n_inst_ = 0;
+  DeviceBuffer inst_adj_, inst_fwd_;
+  DeviceBuffer inv_sqrt_;   // 257 doubles: 1/sqrt(R)
+  // Assembled storage.
+  uint64_t nnz_off_ = 0;
+  int col_bits_ = 0, n_codes_ = 0;
+  bool row_ptr64_ = false;
+  DeviceBuffer row_ptr_, entries_, values64_, values32_, code_table_, diag64_, diag32_;
+  double assembly_seconds_ = 0.0;
+  mutable DeviceBuffer scaled_x_;   // x / sqrt(R) for symmetric packed storage
+  mutable size_t scaled_bytes_ = 0;
+};
+
+}  // namespace qmbed

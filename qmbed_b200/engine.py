@@ -1,0 +1,296 @@
+"""Typed handles over the GPU engine: sector bases and operators.
+
+These wrap the ``qmbed_gpu_*`` C ABI. Host arrays are numpy arrays; device
+entry points take any object exposing ``data_ptr()`` (a torch CUDA tensor).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import EigshInfoC, EigshOptionsC, QmbedError, check, lib
+
+NORMALIZATIONS = {"angular_momentum": 0, "pauli": 1, "pauli_cartesian": 2}
+TARGETS = {
+    "smallest_algebraic": 0,
+    "largest_algebraic": 1,
+    "smallest_magnitude": 2,
+    "largest_magnitude": 3,
+    "both_ends": 4,
+    "shift": 5,
+}
+MODES = {"fp64": 0, "mixed": 1}
+STORAGE = {"matrix_free": 0, "packed": 1}
+
+
+def _ptr(array):
+    if array is None:
+        return None
+    if hasattr(array, "data_ptr"):
+        return ctypes.c_void_p(array.data_ptr())
+    return array.ctypes.data_as(ctypes.c_void_p)
+
+
+class GpuBasis:
+    """Spin-1/2 chain sector enumerated on the GPU (SpinBasis1D)."""
+
+    def __init__(self, sites: int, up: int | None = None, momentum: int | None = None, parity: int | None = None,
+                 normalization: str = "angular_momentum", device: int = 0):
+        handle = ctypes.c_void_p()
+        check(lib().qmbed_gpu_spin_basis_create(
+            device, sites, -1 if up is None else up, 0 if momentum is None else 1,
+            0 if momentum is None else momentum, 0 if parity is None else parity,
+            NORMALIZATIONS[normalization], ctypes.byref(handle)))
+        self.handle = handle
+        self.sites, self.up, self.momentum, self.parity = sites, up, momentum, parity
+        self.normalization = normalization
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().qmbed_gpu_basis_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        dim = ctypes.c_uint64()
+        check(lib().qmbed_gpu_basis_dimension(self.handle, ctypes.byref(dim)))
+        return dim.value
+
+    @property
+    def build_seconds(self) -> float:
+        value = ctypes.c_double()
+        check(lib().qmbed_gpu_basis_build_seconds(self.handle, ctypes.byref(value)))
+        return value.value
+
+    def states(self, offset: int = 0, count: int | None = None):
+        """Return (lo, hi, orbit) arrays for basis rows [offset, offset+count)."""
+        n = len(self) - offset if count is None else count
+        lo = np.zeros(n, np.uint64)
+        hi = np.zeros(n, np.uint64)
+        orbit = np.zeros(n, np.uint16)
+        check(lib().qmbed_gpu_basis_states(self.handle, offset, n, _ptr(lo), _ptr(hi), _ptr(orbit)))
+        return lo, hi, orbit
+
+    def images(self, lo, hi=None):
+        lo = np.ascontiguousarray(lo, np.uint64)
+        hi = None if hi is None else np.ascontiguousarray(hi, np.uint64)
+        n = len(lo)
+        index = np.zeros(n, np.int64)
+        phase = np.zeros(n, np.complex128)
+        orbit = np.zeros(n, np.uint16)
+        check(lib().qmbed_gpu_basis_images(self.handle, _ptr(lo), _ptr(hi), n, _ptr(index), _ptr(phase), _ptr(orbit)))
+        return index, phase, orbit
+
+
+def encode_terms(terms):
+    """Flatten ``[(label, [(coefficient, sites), ...]), ...]`` for the C ABI."""
+    arity, symbols, n_couplings, coefficients, sites = [], [], [], [], []
+    for label, couplings in terms:
+        label = label.replace("|", "")
+        arity.append(len(label))
+        symbols.append(label)
+        n_couplings.append(len(couplings))
+        for coefficient, coupling_sites in couplings:
+            coefficient = complex(coefficient)
+            coefficients += [coefficient.real, coefficient.imag]
+            sites += list(coupling_sites)
+    return (np.asarray(arity, np.int32), "".join(symbols).encode(), np.asarray(n_couplings, np.int32),
+            np.asarray(coefficients, np.float64), np.asarray(sites, np.int32))
+
+
+@dataclass
+class EigshResult:
+    eigenvalues: np.ndarray
+    residuals: np.ndarray
+    eigenvectors: np.ndarray | None
+    iterations: int
+    reorthogonalization_passes: int
+    conditional_second_passes: int
+    fp32_iterations: int
+    fp64_iterations: int
+    operator_applications: int
+    converged: bool
+
+
+class GpuOperator:
+    """Hamiltonian assembled from local terms on a GPU basis (OperatorBuilder)."""
+
+    def __init__(self, basis: GpuBasis, terms, storage: str = "packed", check_hermitian: bool = True,
+                 check_particles: bool = True):
+        arity, symbols, n_couplings, coefficients, sites = encode_terms(terms)
+        handle = ctypes.c_void_p()
+        check(lib().qmbed_gpu_operator_create(basis.handle, len(arity), _ptr(arity), symbols, _ptr(n_couplings),
+                                              _ptr(coefficients), _ptr(sites), int(check_hermitian),
+                                              int(check_particles), STORAGE[storage], ctypes.byref(handle)))
+        self.handle = handle
+        self.basis = basis
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().qmbed_gpu_operator_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        dim, real, storage, nnz, codes, seconds = (ctypes.c_uint64(), ctypes.c_int(), ctypes.c_int(),
+                                                   ctypes.c_uint64(), ctypes.c_int(), ctypes.c_double())
+        check(lib().qmbed_gpu_operator_info(self.handle, ctypes.byref(dim), ctypes.byref(real), ctypes.byref(storage),
+                                            ctypes.byref(nnz), ctypes.byref(codes), ctypes.byref(seconds)))
+        return {"dimension": dim.value, "is_real": bool(real.value), "storage": storage.value,
+                "nnz_offdiag": nnz.value, "value_codes": codes.value, "assembly_seconds": seconds.value}
+
+    @property
+    def dim(self) -> int:
+        return self.info()["dimension"]
+
+    @property
+    def is_real(self) -> bool:
+        return self.info()["is_real"]
+
+    def apply(self, x, force_matrix_free: bool = False) -> np.ndarray:
+        """y = H x on host vectors (FP64). Real input uses the real action when possible."""
+        x = np.asarray(x)
+        complex_vectors = np.iscomplexobj(x) or not self.is_real
+        if complex_vectors:
+            xin = np.ascontiguousarray(x, np.complex128)
+            y = np.zeros_like(xin)
+        else:
+            xin = np.ascontiguousarray(x, np.float64)
+            y = np.zeros_like(xin)
+        check(lib().qmbed_gpu_operator_apply_host(self.handle, int(complex_vectors), _ptr(xin), _ptr(y),
+                                                  int(force_matrix_free)))
+        return y
+
+    def apply_device(self, x, y, precision: int = 64, complex_vectors: bool = False, stream=None,
+                     force_matrix_free: bool = False) -> None:
+        """y = H x on device tensors (``data_ptr()``), FP64 or FP32."""
+        check(lib().qmbed_gpu_operator_apply_device(self.handle, precision, int(complex_vectors), _ptr(x), _ptr(y),
+                                                    None if stream is None else ctypes.c_void_p(stream),
+                                                    int(force_matrix_free)))
+
+    def operand_bytes(self, precision: int = 64, complex_vectors: bool = False) -> float:
+        value = ctypes.c_double()
+        check(lib().qmbed_gpu_operator_operand_bytes(self.handle, precision, int(complex_vectors), ctypes.byref(value)))
+        return value.value
+
+    def csr(self):
+        """Assembled rows (diagonal included) as (row_ptr, cols, values)."""
+        nnz = ctypes.c_uint64()
+        check(lib().qmbed_gpu_operator_export_csr(self.handle, ctypes.byref(nnz), None, None, None))
+        n = self.dim
+        row_ptr = np.zeros(n + 1, np.uint64)
+        cols = np.zeros(nnz.value, np.uint32)
+        values = np.zeros(nnz.value, np.complex128)
+        check(lib().qmbed_gpu_operator_export_csr(self.handle, ctypes.byref(nnz), _ptr(row_ptr), _ptr(cols),
+                                                  _ptr(values)))
+        return row_ptr, cols, values
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        row_ptr, cols, values = self.csr()
+        return sp.csr_matrix((values, cols.astype(np.int64), row_ptr.astype(np.int64)), shape=(self.dim, self.dim))
+
+    def eigsh(self, eigenpairs: int, target: str = "smallest_algebraic", shift: float = 0.0,
+              krylov_dimension: int | None = None, tolerance: float = 1e-10, max_iterations: int = 1000,
+              seed: int = 0, initial=None, eigenvectors: bool = False, mode: str = "fp64") -> EigshResult:
+        n = self.dim
+        options = EigshOptionsC(eigenpairs, TARGETS[target], shift, krylov_dimension or 0, tolerance, max_iterations,
+                                seed, MODES[mode])
+        if initial is not None:
+            initial = np.ascontiguousarray(np.atleast_2d(np.asarray(initial, np.complex128)))
+            n_initial = initial.shape[0]
+        else:
+            n_initial = 0
+        values = np.zeros(eigenpairs)
+        residuals = np.zeros(eigenpairs)
+        vectors = np.zeros((eigenpairs, n), np.complex128) if eigenvectors else None
+        info = EigshInfoC()
+        check(lib().qmbed_gpu_eigsh(self.handle, ctypes.byref(options), _ptr(initial), n_initial, _ptr(values),
+                                    _ptr(residuals), _ptr(vectors), ctypes.byref(info)))
+        return EigshResult(values, residuals, vectors, info.iterations, info.reorthogonalization_passes,
+                           info.conditional_second_passes, info.fp32_iterations, info.fp64_iterations,
+                           info.operator_applications, bool(info.converged))
+
+    def expm_plan(self, coefficient: complex, max_degree: int = 55, tolerance: float = 0.5 * np.finfo(float).eps,
+                  max_substeps: int = 10_000):
+        degree, scaling, one_norm = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double()
+        shift = (ctypes.c_double * 2)()
+        coefficient = complex(coefficient)
+        check(lib().qmbed_gpu_expm_plan(self.handle, coefficient.real, coefficient.imag, max_degree, tolerance,
+                                        max_substeps, ctypes.byref(degree), ctypes.byref(scaling), shift,
+                                        ctypes.byref(one_norm)))
+        return degree.value, scaling.value, complex(shift[0], shift[1]), one_norm.value
+
+    def expm_apply(self, coefficient: complex, vectors, max_degree: int = 55,
+                   tolerance: float = 0.5 * np.finfo(float).eps, max_substeps: int = 10_000,
+                   precision: int = 64) -> np.ndarray:
+        x = np.ascontiguousarray(np.atleast_2d(np.asarray(vectors, np.complex128)))
+        y = np.zeros_like(x)
+        coefficient = complex(coefficient)
+        check(lib().qmbed_gpu_expm_apply_host(self.handle, coefficient.real, coefficient.imag, max_degree, tolerance,
+                                              max_substeps, precision, _ptr(x), _ptr(y), x.shape[0]))
+        return y if np.ndim(vectors) > 1 else y[0]
+
+
+def deterministic_start(n: int, seed: int, device: int = 0) -> np.ndarray:
+    out = np.zeros(n)
+    check(lib().qmbed_gpu_deterministic_start(device, n, seed, _ptr(out)))
+    return out
+
+
+def launch_count() -> int:
+    """Kernels launched by libqmbed_b200.so in this process so far."""
+    count = ctypes.c_uint64()
+    check(lib().qmbed_gpu_launch_count(ctypes.byref(count)))
+    return count.value
+
+
+def device_count() -> int:
+    count = ctypes.c_int()
+    check(lib().qmbed_gpu_device_count(ctypes.byref(count)))
+    return count.value
+
+
+def heisenberg_terms(sites: int, j: float = 1.0, delta: float = 1.0, periodic: bool = True, j2: float = 0.0):
+    """H = J sum_<ij> [ (S+S- + S-S+)/2 + Delta SzSz ] (+ J2 next-nearest), the reference test model."""
+    bonds = [(i, (i + 1) % sites) for i in range(sites if periodic else sites - 1)]
+    terms = [
+        ("zz", [(j * delta, b) for b in bonds]),
+        ("+-", [(0.5 * j, b) for b in bonds]),
+        ("-+", [(0.5 * j, b) for b in bonds]),
+    ]
+    if j2:
+        bonds2 = [(i, (i + 2) % sites) for i in range(sites if periodic else sites - 2)]
+        terms += [
+            ("zz", [(j2 * delta, b) for b in bonds2]),
+            ("+-", [(0.5 * j2, b) for b in bonds2]),
+            ("-+", [(0.5 * j2, b) for b in bonds2]),
+        ]
+    return terms
+
+
+def tfim_terms(sites: int, j: float = 1.0, g: float = 1.0, fields=None, periodic: bool = False):
+    """Transverse-field Ising chain with optional longitudinal fields (Pauli normalisation)."""
+    bonds = [(i, (i + 1) % sites) for i in range(sites if periodic else sites - 1)]
+    terms = [("zz", [(-j, b) for b in bonds]), ("x", [(-g, (i,)) for i in range(sites)])]
+    if fields is not None:
+        terms.append(("z", [(float(h), (i,)) for i, h in enumerate(fields)]))
+    return terms
+
+
+__all__ = ["GpuBasis", "GpuOperator", "EigshResult", "QmbedError", "deterministic_start", "device_count",
+           "heisenberg_terms", "tfim_terms", "encode_terms"]

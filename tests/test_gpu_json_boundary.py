@@ -1,0 +1,83 @@
+"""The JSON drop-in boundary (qmbed_run_json / qmbed_command_json) on the GPU.
+
+Requests use the reference schema (bindings/capi/src/lib.rs:55-741,
+2064-2204); answers are checked against the reference's own C-ABI test
+anchors and against the CPU oracle.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def heisenberg_request_terms(sites, periodic=True, delta=1.0):
+    bonds = [[i, (i + 1) % sites] for i in range(sites if periodic else sites - 1)]
+    return [
+        {"product": {"local": ["z", "z"]}, "couplings": [{"coefficient": [delta, 0.0], "sites": b} for b in bonds]},
+        {"product": {"local": ["raising", "lowering"]},
+         "couplings": [{"coefficient": [0.5, 0.0], "sites": b} for b in bonds]},
+        {"product": {"local": ["lowering", "raising"]},
+         "couplings": [{"coefficient": [0.5, 0.0], "sites": b} for b in bonds]},
+    ]
+
+
+def test_typed_json_request_reaches_the_solver():
+    """bindings/capi/src/lib.rs:6311-6329: the dimer answers -0.75, 0.25."""
+    from qmbed_b200._lib import run
+    result = run({"basis": {"kind": "spin", "sites": 2}, "terms": heisenberg_request_terms(2, periodic=False),
+                  "solver": {"eigenpairs": 2, "target": {"kind": "smallest_algebraic"}, "tolerance": 1e-12}})
+    assert result["dimension"] == 4
+    np.testing.assert_allclose(result["eigenvalues"], [-0.75, 0.25], atol=1e-12)
+    assert result["converged"] is True
+
+
+def test_reference_style_python_api(oracle):
+    import qmbed_b200 as q
+    basis = q.SpinBasis(sites=16, up=8, momentum=0, parity=1)
+    for precision in ("fp64", "mixed"):
+        result = q.eigsh(basis, q.heisenberg_specs(16), q.EigshOptions(3, krylov_dimension=32, tolerance=1e-10,
+                                                                        seed=3, precision=precision))
+        o = oracle.Operator.build(oracle.Basis(16, up=8, momentum=0, parity=1), oracle.heisenberg_terms(16))
+        expected = o.eigsh(3, krylov_dimension=32, tolerance=1e-10, seed=3).eigenvalues
+        np.testing.assert_allclose(result.eigenvalues, expected, rtol=1e-10)
+
+
+def test_models_apply_and_expm_commands(oracle):
+    import qmbed_b200 as q
+    request = {"basis": {"kind": "spin", "sites": 10, "up": 5, "momentum": 0},
+               "terms": heisenberg_request_terms(10)[1:],
+               "components": [{"name": "delta", "terms": heisenberg_request_terms(10)[:1], "default": [1.0, 0.0]}]}
+    with q.NativeModel(request) as model:
+        o = oracle.Operator.build(oracle.Basis(10, up=5, momentum=0), oracle.heisenberg_terms(10, delta=0.4))
+        x = oracle.deterministic_start(model.dimension, 5)
+        y = model.apply(x, parameters={"delta": 0.4})
+        np.testing.assert_allclose(y[0], o.apply(x), atol=1e-13)
+        r = model.eigsh(q.EigshOptions(2, tolerance=1e-12, seed=2), parameters={"delta": 0.4})
+        np.testing.assert_allclose(r.eigenvalues, o.eigsh(2, tolerance=1e-12, seed=2).eigenvalues, rtol=1e-10)
+        with q.NativeExpmAction(model, -0.5j, parameters={"delta": 0.4}) as plan:
+            out = plan.apply(x)
+            np.testing.assert_allclose(out[0], o.expm_apply(-0.5j, x), atol=1e-12)
+
+
+def test_error_responses_carry_reference_texts():
+    from qmbed_b200 import QmbedError
+    from qmbed_b200._lib import command, run
+    with pytest.raises(QmbedError, match="incompatible symmetry request"):
+        run({"basis": {"kind": "spin", "sites": 4, "up": 2, "momentum": 1, "parity": 1},
+             "terms": heisenberg_request_terms(4), "solver": {"eigenpairs": 1, "target": {"kind": "smallest_algebraic"}}})
+    with pytest.raises(QmbedError, match="model handle 99999 is not registered"):
+        command({"operation": "eigsh_model", "handle": "99999",
+                 "solver": {"eigenpairs": 1, "target": {"kind": "smallest_algebraic"}}})
+    with pytest.raises(QmbedError, match="a Hermitian operator is required"):
+        run({"basis": {"kind": "spin", "sites": 4, "up": 2},
+             "terms": heisenberg_request_terms(4)[1:2],
+             "solver": {"eigenpairs": 1, "target": {"kind": "smallest_algebraic"}}})
+
+
+def test_describe_basis_lists_decimal_states(oracle):
+    from qmbed_b200._lib import command
+    result = command({"operation": "describe_basis", "basis": {"kind": "spin", "sites": 8, "up": 4, "momentum": 0}})
+    states, _ = oracle.Basis(8, up=4, momentum=0).states()
+    assert result["dimension"] == len(states)
+    assert result["states"] == [str(int(s)) for s in states]

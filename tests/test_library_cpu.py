@@ -1,0 +1,86 @@
+"""Host-side checks of libqmbed_b200.so that need no GPU: the library loads,
+exports every symbol its header declares, and the JSON boundary rejects
+malformed requests with the reference's error texts before touching CUDA."""
+
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.fixture(scope="module")
+def library():
+    from qmbed_b200 import build
+    build.build()
+    from qmbed_b200._lib import lib
+    return lib()
+
+
+def declared_symbols():
+    names = set()
+    for header in (ROOT / "include").glob("*.h"):
+        text = header.read_text()
+        names |= set(re.findall(r"QMBED_API\s+[\w\s\*]+?\b(qmbed_\w+)\s*\(", text))
+    return names
+
+
+def test_every_declared_symbol_is_exported(library):
+    names = declared_symbols()
+    assert {"qmbed_run_json", "qmbed_command_json", "qmbed_string_free", "qmbed_evolve_model_with_drive_json",
+            "qmbed_register_user_basis_32_json", "qmbed_register_user_basis_64_json"} <= names
+    for name in names:
+        assert hasattr(library, name), name
+    exported = subprocess.run(["nm", "-D", "--defined-only", str(ROOT / "qmbed_b200" / "libqmbed_b200.so")],
+                              capture_output=True, text=True, check=True).stdout
+    public = {line.split()[-1] for line in exported.splitlines() if " T " in line}
+    assert public == names, public ^ names
+
+
+def _json(library, symbol, payload: bytes) -> dict:
+    import json
+    pointer = getattr(library, symbol)(payload)
+    try:
+        return json.loads(ctypes.string_at(pointer))
+    finally:
+        library.qmbed_string_free(pointer)
+
+
+def test_malformed_requests_are_errors_not_crashes(library):
+    r = _json(library, "qmbed_run_json", b"{not json")
+    assert r["status"] == "error" and r["error"].startswith("invalid options: invalid binding request")
+    r = _json(library, "qmbed_command_json", b'{"operation":"no_such_operation"}')
+    assert r["status"] == "error" and "no_such_operation" in r["error"]
+    r = _json(library, "qmbed_run_json", b'{"basis":{"kind":"boson","sites":3,"states_per_site":2},'
+                                         b'"terms":[],"solver":{"eigenpairs":1,"target":{"kind":"smallest_algebraic"}}}')
+    assert r["status"] == "error" and r["error"].startswith("unsupported backend")
+    r = _json(library, "qmbed_command_json", b'{"operation":"release_model","handle":"abc"}')
+    assert r["status"] == "error" and "is not a positive integer" in r["error"]
+    pointer = library.qmbed_run_json(None)
+    assert b"request pointer is null" in ctypes.string_at(pointer)
+    library.qmbed_string_free(pointer)
+
+
+def test_placeholder_exports_answer_unsupported(library):
+    library.qmbed_evolve_model_with_drive_json.restype = ctypes.c_void_p
+    pointer = library.qmbed_evolve_model_with_drive_json(b"{}", None, None)
+    assert b"unsupported backend" in ctypes.string_at(pointer)
+    library.qmbed_string_free(pointer)
+
+
+def test_struct_layouts_match_the_header(library):
+    from qmbed_b200._lib import EigshInfoC, EigshOptionsC
+    assert ctypes.sizeof(EigshOptionsC) == 64
+    assert ctypes.sizeof(EigshInfoC) == 56
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    code = ("import os, sys; os.environ['QMBED_B200_LIBRARY']=sys.argv[1];"
+            "from qmbed_b200._lib import lib, QmbedError\n"
+            "try:\n lib()\nexcept QmbedError as e:\n print('raised', e)\n")
+    out = subprocess.run(["python", "-c", code, str(tmp_path / "missing.so")], capture_output=True, text=True,
+                         cwd=ROOT)
+    assert "raised" in out.stdout and "not found" in out.stdout
