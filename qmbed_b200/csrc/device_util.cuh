@@ -56,7 +56,7 @@ __device__ inline uint32_t block_exclusive_scan_u32(uint32_t v) {
 // Branch-free search of an ascending array of unique states; returns the
 // index of `key` or -1 (the lookup of SpinBasis1D::index, mod.rs:1429-1442).
 template <typename S>
-__device__ inline int64_t find_sorted(const S* __restrict__ states, uint64_t n, S key) {
+__host__ __device__ inline int64_t find_sorted(const S* __restrict__ states, uint64_t n, S key) {
   if (n == 0) return -1;
   uint64_t base = 0, len = n;
   while (len > 1) {
@@ -70,7 +70,7 @@ __device__ inline int64_t find_sorted(const S* __restrict__ states, uint64_t n, 
 // Colex rank of a fixed-weight state, -1 when the weight differs
 // (fixed_weight_state_index, reference src/basis/mod.rs:640-659).
 template <typename S>
-__device__ inline int64_t colex_rank_checked(S state, int sites, int weight, const uint64_t* __restrict__ binom) {
+__host__ __device__ inline int64_t colex_rank_checked(S state, int sites, int weight, const uint64_t* __restrict__ binom) {
   if (popcount_state(state) != weight) return -1;
   uint64_t rank = 0;
   int ordinal = 1;

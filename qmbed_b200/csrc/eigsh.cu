@@ -153,7 +153,8 @@ void upload_vector(Ctx& c, const std::vector<C64>& host, void* device) {
         buffer[i] = host[i].real();
       }
     }
-    QMBED_CUDA(cudaMemcpy(device, buffer.data(), buffer.size() * 8, cudaMemcpyHostToDevice));
+    QMBED_CUDA(cudaMemcpyAsync(device, buffer.data(), buffer.size() * 8, cudaMemcpyHostToDevice, c.ops.stream()));
+    c.ops.sync();
   } else {
     std::vector<float> buffer(c.cplx ? 2 * n : n);
     for (uint64_t i = 0; i < n; ++i) {
@@ -164,7 +165,8 @@ void upload_vector(Ctx& c, const std::vector<C64>& host, void* device) {
         buffer[i] = static_cast<float>(host[i].real());
       }
     }
-    QMBED_CUDA(cudaMemcpy(device, buffer.data(), buffer.size() * 4, cudaMemcpyHostToDevice));
+    QMBED_CUDA(cudaMemcpyAsync(device, buffer.data(), buffer.size() * 4, cudaMemcpyHostToDevice, c.ops.stream()));
+    c.ops.sync();
   }
 }
 
@@ -489,17 +491,16 @@ EigshResult thick_restart(Ctx& c, const EigshOptions& o, const Panel* initial, i
 EigshResult dense_eigsh(Ctx& c, const EigshOptions& o) {
   const uint64_t n = c.n;
   Panel E, Hc;
-  E.alloc(n, 1, 64, true);
+  E.alloc(n, static_cast<int>(n), 64, true);  // identity columns
   Hc.alloc(n, static_cast<int>(n), 64, true);
-  std::vector<double> unit(2 * n, 0.0);
-  for (uint64_t j = 0; j < n; ++j) {
-    std::fill(unit.begin(), unit.end(), 0.0);
-    unit[2 * j] = 1.0;
-    QMBED_CUDA(cudaMemcpy(E.col(0), unit.data(), unit.size() * 8, cudaMemcpyHostToDevice));
-    c.op.apply(64, true, E.col(0), Hc.col(static_cast<int>(j)));
-  }
-  std::vector<double> host(2 * n * n);
-  QMBED_CUDA(cudaMemcpy(host.data(), Hc.col(0), host.size() * 8, cudaMemcpyDeviceToHost));
+  std::vector<double> host(2 * n * n, 0.0);
+  for (uint64_t j = 0; j < n; ++j) host[2 * (j * n + j)] = 1.0;
+  // All copies go through the solver stream: the operator runs there, and a
+  // legacy-stream copy would not be ordered against it.
+  QMBED_CUDA(cudaMemcpyAsync(E.col(0), host.data(), host.size() * 8, cudaMemcpyHostToDevice, c.ops.stream()));
+  for (uint64_t j = 0; j < n; ++j) c.op.apply(64, true, E.col(static_cast<int>(j)), Hc.col(static_cast<int>(j)));
+  QMBED_CUDA(cudaMemcpyAsync(host.data(), Hc.col(0), host.size() * 8, cudaMemcpyDeviceToHost, c.ops.stream()));
+  c.ops.sync();
   std::vector<C64> dense(n * n);  // row-major
   for (uint64_t j = 0; j < n; ++j)
     for (uint64_t i = 0; i < n; ++i) dense[i * n + j] = C64(host[2 * (j * n + i)], host[2 * (j * n + i) + 1]);

@@ -357,7 +357,9 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(int np, double* __restrict
         o += red[wv][0];
         t += red[wv][1];
       }
-      done = (o <= floor_rel * t || o == 0.0 || (sweep > 2 && previous_off >= 0.0 && o >= 0.25 * previous_off)) ? 1 : 0;
+      // stagnation counts only once the off-diagonal mass is near rounding level
+      const bool stalled = sweep > 4 && previous_off >= 0.0 && o >= 0.5 * previous_off && o <= 1e-24 * t;
+      done = (o <= floor_rel * t || o == 0.0 || stalled) ? 1 : 0;
       previous_off = o;
     }
     __syncthreads();

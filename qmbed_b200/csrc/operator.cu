@@ -52,13 +52,13 @@ struct OpView {
 };
 
 template <typename S>
-__device__ inline S row_state(const OpView<S>& v, uint64_t r) {
+__host__ __device__ inline S row_state(const OpView<S>& v, uint64_t r) {
   return v.direct ? static_cast<S>(r) : v.states[r];
 }
 
 // Applies one product to `s` right to left; false when the action is zero.
 template <typename S>
-__device__ inline bool apply_instance(const Instance& in, S s, const LocalFactors& f, S& t, double& ar, double& ai) {
+__host__ __device__ inline bool apply_instance(const Instance& in, S s, const LocalFactors& f, S& t, double& ar, double& ai) {
   t = s;
   ar = 1.0;
   ai = 0.0;
@@ -115,7 +115,7 @@ struct Located {
 };
 
 template <typename S>
-__device__ inline Located locate(const OpView<S>& v, S t) {
+__host__ __device__ inline Located locate(const OpView<S>& v, S t) {
   Located out{-1, 1.0, 0.0, 1};
   if ((t & ~v.mask) != 0) return out;
   if (v.direct) {
@@ -226,7 +226,7 @@ struct RowList {
 // (the packed format applies it through the scaled input vector) and the
 // diagonal is returned separately. Entries are sorted by column and coalesced.
 template <typename S>
-__device__ inline void collect_row(const OpView<S>& v, const Instance* inst, int n_inst, uint64_t r, bool with_ratio,
+__host__ __device__ inline void collect_row(const OpView<S>& v, const Instance* inst, int n_inst, uint64_t r, bool with_ratio,
                                    RowList& out) {
   const S s = row_state(v, r);
   const double sqrt_r = v.p.symmetric ? v.inv_sqrt[257 + v.orbits[r]] : 1.0;
@@ -300,7 +300,7 @@ __device__ inline void collect_row(const OpView<S>& v, const Instance* inst, int
 
 // |H[r,c]| <= eps entries are not stored (reference drop rule, mod.rs:2162-2164).
 template <typename S>
-__device__ inline bool keep_entry(const OpView<S>& v, uint64_t r, const RowList& row, int i) {
+__host__ __device__ inline bool keep_entry(const OpView<S>& v, uint64_t r, const RowList& row, int i) {
   double ratio = 1.0;
   if (v.p.symmetric) ratio = v.inv_sqrt[257 + v.orbits[r]] * v.inv_sqrt[v.orbits[row.col[i]]];
   return hypot(row.re[i], row.im[i]) * ratio > 2.220446049250313e-16;

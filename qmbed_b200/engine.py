@@ -96,10 +96,16 @@ def encode_terms(terms):
     arity, symbols, n_couplings, coefficients, sites = [], [], [], [], []
     for label, couplings in terms:
         label = label.replace("|", "")
+        if not label:
+            raise QmbedError("invalid or unregistered operator: operator products cannot be empty", 1)
         arity.append(len(label))
         symbols.append(label)
         n_couplings.append(len(couplings))
         for coefficient, coupling_sites in couplings:
+            if len(coupling_sites) != len(label):
+                # OperatorSpec::from_product (src/operator/mod.rs:226-247)
+                raise QmbedError(f'invalid coupling: operator "{label}" has arity {len(label)}, but a coupling has '
+                                 f"{len(coupling_sites)} sites", 2)
             coefficient = complex(coefficient)
             coefficients += [coefficient.real, coefficient.imag]
             sites += list(coupling_sites)

@@ -129,10 +129,14 @@ def test_assembled_rows_match_oracle(engine, oracle, model, sites, up, momentum,
     g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity, normalization=norm), terms)
     a = o.to_scipy().tocsr()
     b = g.to_scipy().tocsr()
-    a.sort_indices()
-    b.sort_indices()
+    # values agree entry by entry; exact cancellations in the reference's
+    # phase sums can leave ~1e-16 residues, so the pattern is compared above 1e-13
+    assert abs(a - b).max() <= 1e-13
+    for m in (a, b):
+        m.data[np.abs(m.data) <= 1e-13] = 0
+        m.eliminate_zeros()
+        m.sort_indices()
     assert np.array_equal(a.indptr, b.indptr) and np.array_equal(a.indices, b.indices)
-    assert np.abs(a.data - b.data).max() <= 1e-13
 
 
 def test_fp32_action(engine, oracle):
