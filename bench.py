@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--mode", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI leg (profiling runs)")
     p.add_argument("--hv-launches", type=int, default=20)
     return p.parse_args()
 
@@ -294,14 +295,14 @@ def main():
     d2h = vectors.nbytes + values.nbytes + residuals.nbytes
     barrier()
     e2e_times = []
-    for _ in range(max(1, min(args.steps, 2))):
+    for _ in range(0 if args.no_e2e else max(1, min(args.steps, 2))):
         t_e2e = time.perf_counter()
         check(lib().qmbed_gpu_eigsh(op.handle, ctypes.byref(options), v0.ctypes.data_as(ctypes.c_void_p), 1,
                                     values.ctypes.data_as(ctypes.c_void_p), residuals.ctypes.data_as(ctypes.c_void_p),
                                     vectors.ctypes.data_as(ctypes.c_void_p), ctypes.byref(e2e_info)))
         e2e_times.append(time.perf_counter() - t_e2e)
-    e2e_value = statistics.median(e2e_times)
-    if world > 1:
+    e2e_value = statistics.median(e2e_times) if e2e_times else None
+    if world > 1 and e2e_value is not None:
         t = torch.tensor([e2e_value], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_value = float(t.item()) / world
