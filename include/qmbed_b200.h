@@ -118,6 +118,22 @@ QMBED_API int qmbed_gpu_operator_info(qmbed_operator op, uint64_t* dimension, in
  * interleaved complex vectors. stream may be NULL (default stream). */
 QMBED_API int qmbed_gpu_operator_apply_device(qmbed_operator op, int precision, int complex_vectors, const void* x,
                                               void* y, void* stream, int force_matrix_free);
+/* The same action as qmbed_gpu_operator_apply_device, for callers that cannot
+ * let a library allocate device memory (applications that manage all GPU
+ * memory through their own pool or budget, or that cannot afford the device
+ * synchronisation of cudaMalloc/cudaFree in their loop). No counterpart in the
+ * reference: it is an addition of this library. It allocates nothing; the
+ * x / sqrt(R) vector of symmetry sectors with stored rows goes to a fixed
+ * 32 MiB array in device global memory, reserved on every GPU where the
+ * library's device code is loaded and held until the process exits. Vectors
+ * are limited to 32 MiB (dimension x (2 if complex) x (8 FP64 | 4 FP32) bytes);
+ * larger ones return QMBED_STATUS_DIMENSION_MISMATCH. The first call on a
+ * device looks up the array's device address (once per device, cached); make
+ * that first call before any stream capture. All calls share the array and it
+ * keeps the last call's contents (each call overwrites the part it reads), so
+ * calls that overlap on the GPU (other streams, other host threads) race. */
+QMBED_API int qmbed_gpu_operator_apply_device_noalloc(qmbed_operator op, int precision, int complex_vectors,
+                                                      const void* x, void* y, void* stream);
 /* The same action on host buffers (FP64; complex interleaved when complex_vectors). */
 QMBED_API int qmbed_gpu_operator_apply_host(qmbed_operator op, int complex_vectors, const double* x, double* y,
                                             int force_matrix_free);

@@ -7,6 +7,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -693,6 +694,19 @@ std::string respond(const char* request, bool command_api) {
 }
 
 }  // namespace
+
+namespace qmbed {
+
+// Status/last-error wrapper and handle access for entry points defined in
+// other translation units.
+int noalloc_guarded(const std::function<void()>& body) { return guarded(body); }
+
+const SpinOperator& operator_of(qmbed_operator_s* op) {
+  if (!op || !op->op) raise(QMBED_INVALID_OPTIONS, "operator handle is null");
+  return *op->op;
+}
+
+}  // namespace qmbed
 
 extern "C" {
 

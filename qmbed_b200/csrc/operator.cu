@@ -961,6 +961,69 @@ void SpinOperator::apply(int precision, bool complex_vectors, const void* x, voi
   QMBED_LAUNCH_CHECK();
 }
 
+void SpinOperator::apply_with_scratch(int precision, bool complex_vectors, const void* x, void* y,
+                                      cudaStream_t stream, void* scratch, size_t scratch_bytes) const {
+  QMBED_CUDA(cudaSetDevice(basis_->device()));
+  const uint64_t n = dim();
+  if (n == 0) return;
+  const bool cplx = complex_vectors;
+  const bool stored_symmetric = storage_ != kStorageMatrixFree && basis_->symmetric() && !(real_ && cplx);
+  if (!stored_symmetric) {
+    apply(precision, complex_vectors, x, y, stream);  // these paths hold no scaled vector
+    return;
+  }
+  if (!real_ && !cplx) raise(QMBED_UNSUPPORTED_BACKEND, "real action requires an operator with real-valued storage");
+  const int comps = cplx ? 2 : 1;
+  const size_t need = static_cast<size_t>(n) * comps * (precision == kFP64 ? 8 : 4);
+  if (need > scratch_bytes)
+    raise(QMBED_DIMENSION_MISMATCH, "the scaled input needs " + std::to_string(need) + " bytes of scratch, " +
+                                        std::to_string(scratch_bytes) + " available");
+  {
+    const int grid = grid_for(n * comps, 256, 16);
+    if (precision == kFP64)
+      scale_by_orbit_kernel<double><<<grid, 256, 0, stream>>>(n, comps, basis_->orbits(), inv_sqrt_.as<double>(),
+                                                               static_cast<const double*>(x),
+                                                               static_cast<double*>(scratch));
+    else
+      scale_by_orbit_kernel<float><<<grid, 256, 0, stream>>>(n, comps, basis_->orbits(), inv_sqrt_.as<double>(),
+                                                              static_cast<const float*>(x),
+                                                              static_cast<float*>(scratch));
+    QMBED_LAUNCH_CHECK();
+  }
+  const void* xs = scratch;
+  constexpr int kLanes = 4;
+  const int grid = grid_for(n * kLanes, 256, 8);
+  using True = std::true_type;
+  if (storage_ == kStoragePacked && !cplx) {
+    auto launch = [&](auto ttag, auto itag) {
+      using T = decltype(ttag);
+      using I = decltype(itag);
+      const T* diag = precision == kFP64 ? reinterpret_cast<const T*>(diag64_.get()) : reinterpret_cast<const T*>(diag32_.get());
+      spmv_packed_kernel<T, I, True::value, kLanes><<<grid, 256, 0, stream>>>(
+          n, row_ptr_.as<I>(), entries_.as<uint32_t>(), col_bits_, code_table_.as<double>(), n_codes_, diag,
+          basis_->orbits(), inv_sqrt_.as<double>(), static_cast<const T*>(xs), static_cast<const T*>(x),
+          static_cast<T*>(y));
+    };
+    if (precision == kFP64) row_ptr64_ ? launch(double{}, uint64_t{}) : launch(double{}, uint32_t{});
+    else row_ptr64_ ? launch(float{}, uint64_t{}) : launch(float{}, uint32_t{});
+    QMBED_LAUNCH_CHECK();
+    return;
+  }
+  auto launch = [&](auto ttag, auto itag) {
+    using T = decltype(ttag);
+    using I = decltype(itag);
+    auto kernel = cplx ? spmv_wide_kernel<T, I, True::value, kLanes, true> : spmv_wide_kernel<T, I, True::value, kLanes, false>;
+    const T* diag = precision == kFP64 ? reinterpret_cast<const T*>(diag64_.get()) : reinterpret_cast<const T*>(diag32_.get());
+    const T* vals = precision == kFP64 ? reinterpret_cast<const T*>(values64_.get()) : reinterpret_cast<const T*>(values32_.get());
+    kernel<<<grid, 256, 0, stream>>>(n, row_ptr_.as<I>(), entries_.as<uint32_t>(), vals, diag, basis_->orbits(),
+                                     inv_sqrt_.as<double>(), static_cast<const T*>(xs), static_cast<const T*>(x),
+                                     static_cast<T*>(y));
+  };
+  if (precision == kFP64) row_ptr64_ ? launch(double{}, uint64_t{}) : launch(double{}, uint32_t{});
+  else row_ptr64_ ? launch(float{}, uint64_t{}) : launch(float{}, uint32_t{});
+  QMBED_LAUNCH_CHECK();
+}
+
 void SpinOperator::export_csr(std::vector<uint64_t>& row_ptr, std::vector<uint32_t>& cols,
                               std::vector<C64>& values) const {
   QMBED_CUDA(cudaSetDevice(basis_->device()));

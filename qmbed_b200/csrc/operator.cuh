@@ -75,6 +75,13 @@ class SpinOperator {
   void apply(int precision, bool complex_vectors, const void* x, void* y, cudaStream_t stream,
              bool force_matrix_free = false) const;
 
+  // The same action with the x / sqrt(R) vector of symmetric stored rows
+  // written to caller-provided device memory (`scratch`, `scratch_bytes`)
+  // instead of a buffer this object allocates. Paths that need no such
+  // vector run exactly as apply().
+  void apply_with_scratch(int precision, bool complex_vectors, const void* x, void* y, cudaStream_t stream,
+                          void* scratch, size_t scratch_bytes) const;
+
   // Dense Hermitian check of the assembled operator at tolerance 1e-12
   // (OperatorBuilder::build + is_hermitian, src/operator/mod.rs:2212).
   bool check_hermitian() const;

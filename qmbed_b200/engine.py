@@ -188,6 +188,16 @@ class GpuOperator:
                                                     None if stream is None else ctypes.c_void_p(stream),
                                                     int(force_matrix_free)))
 
+    def apply_device_noalloc(self, x, y, precision: int = 64, complex_vectors: bool = False, stream=None) -> None:
+        """y = H x on device tensors without any device allocation by the library.
+
+        For callers that manage all GPU memory themselves: the scaled input of
+        symmetry sectors goes to a fixed 32 MiB device array shared by all
+        calls, so vectors are limited to 32 MiB and concurrent calls race.
+        """
+        check(lib().qmbed_gpu_operator_apply_device_noalloc(self.handle, precision, int(complex_vectors), _ptr(x),
+                                                            _ptr(y), None if stream is None else ctypes.c_void_p(stream)))
+
     def operand_bytes(self, precision: int = 64, complex_vectors: bool = False) -> float:
         value = ctypes.c_double()
         check(lib().qmbed_gpu_operator_operand_bytes(self.handle, precision, int(complex_vectors), ctypes.byref(value)))
