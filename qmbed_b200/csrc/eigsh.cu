@@ -116,15 +116,23 @@ struct Ortho {
 // orthonormalize_*_with_projection (src/solve/mod.rs:1520-1642): remove the
 // first `ncols` panel columns (locked then basis) from w, a DGKS second pass
 // when the norm drops below 1/sqrt(2), then normalise.
-Ortho orthonormalize(Ctx& c, const Panel& Q, int ncols, int projection_from, void* w) {
+// `src` is read, the orthogonalised vector is built in `w` (may equal src),
+// and the normalised result is written to `slot` (in place when null).
+Ortho orthonormalize(Ctx& c, const Panel& Q, int ncols, int projection_from, const void* src, void* w,
+                     void* slot = nullptr) {
   Ortho out{false, 1, 0, {}};
-  const double before = c.norm(w);
   std::vector<C64> h(std::max(ncols, 1));
-  double norm = before;
+  double before, norm;
   if (ncols > 0) {
-    c.ops.dots(Q.col(0), Q.n, ncols, w, c.n, c.prec, c.cplx, h.data());
-    norm = c.ops.subtract(Q.col(0), Q.n, ncols, h.data(), w, c.n, c.prec, c.cplx, true);
+    double before_sq = 0.0;
+    c.ops.dots(Q.col(0), Q.n, ncols, src, c.n, c.prec, c.cplx, h.data(), &before_sq);
+    before = std::sqrt(std::max(before_sq, 0.0));
+    norm = c.ops.subtract(Q.col(0), Q.n, ncols, h.data(), w, c.n, c.prec, c.cplx, true, src);
     out.projection.assign(h.begin() + projection_from, h.begin() + ncols);
+  } else {
+    before = c.norm(src);
+    norm = before;
+    if (src != w) c.copy(src, w);
   }
   const bool second = before > kEps && norm <= kDgks * before;
   if (second) {
@@ -136,7 +144,8 @@ Ortho orthonormalize(Ctx& c, const Panel& Q, int ncols, int projection_from, voi
     out.second_passes = 1;
   }
   if (!std::isfinite(norm) || norm <= 1.0e-14) return out;
-  c.scale(w, norm);
+  if (slot) c.ops.scale_into(w, slot, c.n, norm, c.prec, c.cplx);
+  else c.scale(w, norm);
   out.ok = true;
   return out;
 }
@@ -246,8 +255,7 @@ EigshResult lanczos_window(Ctx& c, const EigshOptions& o, const void* initial_de
     size = it + 1;
     if (it + 1 == krylov || beta <= 1.0e-14) break;
     betas.push_back(beta);
-    c.copy(out, V.col(static_cast<int>(it + 1)));
-    c.scale(V.col(static_cast<int>(it + 1)), beta);
+    c.ops.scale_into(out, V.col(static_cast<int>(it + 1)), n, beta, c.prec, c.cplx);
   }
   if (size <= o.eigenpairs) nonconvergence(size, std::numeric_limits<double>::infinity());
   std::vector<C64> T(size * size, C64(0.0, 0.0));
@@ -341,35 +349,26 @@ EigshResult thick_restart(Ctx& c, const EigshOptions& o, const Panel* initial, i
       if (reuse) {
         const double norm = c.norm(RC.col(i));
         if (std::isfinite(norm) && norm > 1.0e-14) {
-          c.copy(RC.col(i), slot);
-          c.scale(slot, norm);
-          c.copy(RCA.col(i), W.col(a));
-          c.scale(W.col(a), norm);
+          c.ops.scale_into(RC.col(i), slot, n, norm, c.prec, c.cplx);
+          c.ops.scale_into(RCA.col(i), W.col(a), n, norm, c.prec, c.cplx);
           ++b;
           ++a;
         }
       } else {
-        c.copy(RC.col(i), tmp);
-        Ortho r = orthonormalize(c, Q, l + b, l, tmp);
+        Ortho r = orthonormalize(c, Q, l + b, l, RC.col(i), tmp, slot);
         passes += r.passes;
         seconds += r.second_passes;
-        if (r.ok) {
-          c.copy(tmp, slot);
-          ++b;
-        }
+        if (r.ok) ++b;
       }
       if (b >= m / 2) break;
     }
     retained = 0;
     if (b == 0) {
       start_vector(c, o.seed + cycle * 0x9e3779b9ULL, tmp);
-      Ortho r = orthonormalize(c, Q, l, l, tmp);
+      Ortho r = orthonormalize(c, Q, l, l, tmp, tmp, Q.col(l));
       passes += r.passes;
       seconds += r.second_passes;
-      if (r.ok) {
-        c.copy(tmp, Q.col(l));
-        b = 1;
-      }
+      if (r.ok) b = 1;
     }
     if (b == 0) break;
     const int known = a;
@@ -377,15 +376,11 @@ EigshResult thick_restart(Ctx& c, const EigshOptions& o, const Panel* initial, i
     if (reuse) {
       for (int column = 0; column < known; ++column) {
         if (b >= m) break;
-        c.copy(W.col(column), tmp);
-        Ortho r = orthonormalize(c, Q, l + b, l, tmp);
+        Ortho r = orthonormalize(c, Q, l + b, l, W.col(column), tmp, Q.col(l + b));
         passes += r.passes;
         seconds += r.second_passes;
         projection_columns.emplace_back(r.projection.begin(), r.projection.begin() + column + 1);
-        if (r.ok) {
-          c.copy(tmp, Q.col(l + b));
-          ++b;
-        }
+        if (r.ok) ++b;
       }
     }
     int cursor = known;
@@ -393,15 +388,12 @@ EigshResult thick_restart(Ctx& c, const EigshOptions& o, const Panel* initial, i
       c.apply(Q.col(l + cursor), W.col(a));
       ++iterations;
       ++a;
-      c.copy(W.col(a - 1), tmp);
-      Ortho r = orthonormalize(c, Q, l + b, l, tmp);
+      // the raw action stays in W; the orthonormalised direction lands in the next basis slot
+      Ortho r = orthonormalize(c, Q, l + b, l, W.col(a - 1), tmp, b < m ? Q.col(l + b) : nullptr);
       passes += r.passes;
       seconds += r.second_passes;
       projection_columns.emplace_back(r.projection.begin(), r.projection.begin() + cursor + 1);
-      if (b < m && r.ok) {
-        c.copy(tmp, Q.col(l + b));
-        ++b;
-      }
+      if (b < m && r.ok) ++b;
       ++cursor;
     }
     b = std::min(b, a);
@@ -448,12 +440,10 @@ EigshResult thick_restart(Ctx& c, const EigshOptions& o, const Panel* initial, i
       const Candidate& cand = candidates[rank];
       const bool converged = cand.residual <= o.tolerance * std::max(std::fabs(cand.value), 1.0);
       if (rank < active && converged && l < k) {
-        c.copy(C.col(cand.slot), tmp);
-        Ortho r = orthonormalize(c, Q, l, 0, tmp);
+        Ortho r = orthonormalize(c, Q, l, 0, C.col(cand.slot), tmp, Q.col(l));
         passes += r.passes;
         seconds += r.second_passes;
         if (r.ok) {
-          c.copy(tmp, Q.col(l));
           locked_values.push_back(cand.value);
           locked_residuals.push_back(cand.residual);
           ++l;

@@ -44,14 +44,16 @@ __device__ inline double warp_sum(double v) {
 }
 
 // partials[(j * G + block) * 2 + {0,1}] = sum over this block's rows of conj(A_j) w.
+// With `with_self`, column m receives sum |w|^2 (computed in the first pass).
 template <typename T, bool CPLX>
 __global__ void __launch_bounds__(kThreads) multi_dot_kernel(const T* __restrict__ A, uint64_t ld, int m,
                                                               const T* __restrict__ w, uint64_t n,
-                                                              double* __restrict__ partials) {
+                                                              double* __restrict__ partials, int with_self) {
   __shared__ double red[kThreads / 32][2 * kChunk];
   const int G = gridDim.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t stride = static_cast<uint64_t>(G) * blockDim.x;
+  double self = 0.0;
   for (int j0 = 0; j0 < m; j0 += kChunk) {
     const int cnt = min(kChunk, m - j0);
     double ar[kChunk], ai[kChunk];
@@ -60,6 +62,7 @@ __global__ void __launch_bounds__(kThreads) multi_dot_kernel(const T* __restrict
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
       double wr, wi;
       load<T, CPLX>(w, i, wr, wi);
+      if (j0 == 0) self += wr * wr + wi * wi;
 #pragma unroll
       for (int jj = 0; jj < kChunk; ++jj) {
         if (jj < cnt) {
@@ -88,46 +91,76 @@ __global__ void __launch_bounds__(kThreads) multi_dot_kernel(const T* __restrict
     }
     __syncthreads();
   }
+  if (with_self) {
+    const double s = warp_sum(self);
+    if (lane == 0) red[warp][0] = s;
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      double total = 0.0;
+      if (threadIdx.x == 0)
+        for (int wv = 0; wv < kThreads / 32; ++wv) total += red[wv][0];
+      partials[(static_cast<uint64_t>(m) * G + blockIdx.x) * 2 + threadIdx.x] = total;
+    }
+  }
 }
 
-// out[t] = sum_b partials[(t/2 * G + b) * 2 + t%2], in block order.
-__global__ void finish_kernel(const double* __restrict__ partials, int G, int count, double* __restrict__ out) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// out[t] = sum_b partials[(t/2 * G + b) * 2 + t%2]: one block per output,
+// strided per-thread sums then a shared-memory tree, both in a fixed order.
+constexpr int kFinishThreads = 128;
+__global__ void __launch_bounds__(kFinishThreads) finish_kernel(const double* __restrict__ partials, int G, int count,
+                                                                double* __restrict__ out) {
+  const int t = blockIdx.x;
   if (t >= count) return;
   const int j = t / 2, c = t & 1;
   double total = 0.0;
-  for (int b = 0; b < G; ++b) total += partials[(static_cast<uint64_t>(j) * G + b) * 2 + c];
-  out[t] = total;
+  for (int b = threadIdx.x; b < G; b += kFinishThreads) total += partials[(static_cast<uint64_t>(j) * G + b) * 2 + c];
+  __shared__ double tree[kFinishThreads];
+  tree[threadIdx.x] = total;
+  __syncthreads();
+  for (int width = kFinishThreads / 2; width > 0; width >>= 1) {
+    if (threadIdx.x < width) tree[threadIdx.x] += tree[threadIdx.x + width];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[t] = tree[0];
 }
 
-// w -= sum_j h_j A_j; per-block partial of ||w||^2 when `partials` is set.
+// w = src - sum_j h_j A_j (src may be w); per-block partial of ||w||^2 when
+// `partials` is set.
 template <typename T, bool CPLX>
 __global__ void __launch_bounds__(kThreads) subtract_kernel(const T* __restrict__ A, uint64_t ld, int m,
-                                                             const double* __restrict__ h, T* __restrict__ w,
+                                                             const double* __restrict__ h, const T* src, T* w,
                                                              uint64_t n, double* __restrict__ partials) {
   extern __shared__ double hs[];
   for (int t = threadIdx.x; t < 2 * m; t += blockDim.x) hs[t] = h[t];
   __syncthreads();
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  const uint64_t col = ld * (CPLX ? 2 : 1);
   double sq = 0.0;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-    double sr = 0.0, si = 0.0;
-    for (int j = 0; j < m; ++j) {
-      double xr, xi;
-      load<T, CPLX>(A + j * ld * (CPLX ? 2 : 1), i, xr, xi);
-      const double hr = hs[2 * j], hi = hs[2 * j + 1];
-      sr += hr * xr - hi * xi;
-      si += hr * xi + hi * xr;
-    }
     double wr, wi;
-    load<T, CPLX>(w, i, wr, wi);
-    wr -= sr;
-    wi -= si;
-    store<T, CPLX>(w, i, wr, wi);
-    if (partials) {
-      load<T, CPLX>(w, i, wr, wi);  // norm of the stored (rounded) value
-      sq += wr * wr + wi * wi;
+    load<T, CPLX>(src, i, wr, wi);
+    double sr = 0.0, si = 0.0;
+    // batches of kChunk independent loads keep several requests in flight per thread
+    for (int j0 = 0; j0 < m; j0 += kChunk) {
+      double xr[kChunk], xi[kChunk];
+#pragma unroll
+      for (int jj = 0; jj < kChunk; ++jj) {
+        if (j0 + jj < m) load<T, CPLX>(A + (j0 + jj) * col, i, xr[jj], xi[jj]);
+        else xr[jj] = xi[jj] = 0.0;
+      }
+#pragma unroll
+      for (int jj = 0; jj < kChunk; ++jj) {
+        if (j0 + jj < m) {
+          const double hr = hs[2 * (j0 + jj)], hi = hs[2 * (j0 + jj) + 1];
+          sr += hr * xr[jj] - hi * xi[jj];
+          si += hr * xi[jj] + hi * xr[jj];
+        }
+      }
     }
+    // norm of the value as stored (rounded to T)
+    const T rr = static_cast<T>(wr - sr), ri = static_cast<T>(wi - si);
+    store<T, CPLX>(w, i, static_cast<double>(rr), static_cast<double>(ri));
+    if (partials) sq += static_cast<double>(rr) * static_cast<double>(rr) + (CPLX ? static_cast<double>(ri) * static_cast<double>(ri) : 0.0);
   }
   if (partials) {
     __shared__ double red[kThreads / 32];
@@ -150,20 +183,29 @@ __global__ void __launch_bounds__(kThreads) combine_kernel(const T* __restrict__
                                                             T* __restrict__ out, uint64_t ld_out, uint64_t n) {
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   const int cnt = min(kCombine, K - k0);
+  const uint64_t col = ld * (CPLX ? 2 : 1);
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
     double ar[kCombine], ai[kCombine];
 #pragma unroll
     for (int kk = 0; kk < kCombine; ++kk) ar[kk] = ai[kk] = 0.0;
-    for (int j = 0; j < m; ++j) {
-      double xr, xi;
-      load<T, CPLX>(A + j * ld * (CPLX ? 2 : 1), i, xr, xi);
+    for (int j0 = 0; j0 < m; j0 += kChunk) {
+      double xr[kChunk], xi[kChunk];
 #pragma unroll
-      for (int kk = 0; kk < kCombine; ++kk) {
-        if (kk < cnt) {
-          const uint64_t y = (static_cast<uint64_t>(k0 + kk) * m + j) * 2;
-          const double yr = __ldg(Y + y), yi = __ldg(Y + y + 1);
-          ar[kk] += yr * xr - yi * xi;
-          ai[kk] += yr * xi + yi * xr;
+      for (int jj = 0; jj < kChunk; ++jj) {
+        if (j0 + jj < m) load<T, CPLX>(A + (j0 + jj) * col, i, xr[jj], xi[jj]);
+        else xr[jj] = xi[jj] = 0.0;
+      }
+#pragma unroll
+      for (int jj = 0; jj < kChunk; ++jj) {
+        if (j0 + jj >= m) continue;
+#pragma unroll
+        for (int kk = 0; kk < kCombine; ++kk) {
+          if (kk < cnt) {
+            const uint64_t y = (static_cast<uint64_t>(k0 + kk) * m + j0 + jj) * 2;
+            const double yr = __ldg(Y + y), yi = __ldg(Y + y + 1);
+            ar[kk] += yr * xr[jj] - yi * xi[jj];
+            ai[kk] += yr * xi[jj] + yi * xr[jj];
+          }
         }
       }
     }
@@ -178,6 +220,13 @@ __global__ void scale_kernel(T* __restrict__ w, uint64_t count, double divisor) 
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride)
     w[i] = static_cast<T>(static_cast<double>(w[i]) / divisor);
+}
+
+template <typename T>
+__global__ void scale_into_kernel(const T* __restrict__ src, T* __restrict__ dst, uint64_t count, double divisor) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride)
+    dst[i] = static_cast<T>(static_cast<double>(src[i]) / divisor);
 }
 
 template <typename S, typename D>
@@ -575,21 +624,38 @@ void BlockOps::sync() { QMBED_CUDA(cudaStreamSynchronize(stream_)); }
   } while (0)
 
 void BlockOps::dots(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx,
-                    C64* out) {
-  if (m <= 0) return;
+                    C64* out, double* self_sq) {
+  if (m <= 0) {
+    if (self_sq) *self_sq = std::pow(norm(w, n, precision, cplx), 2);
+    return;
+  }
   const int G = reduction_grid(n, sms_);
-  ensure_partials(static_cast<size_t>(m) * G * 2 + 2 * static_cast<size_t>(m) + 64);
+  const int columns = m + (self_sq ? 1 : 0);
+  ensure_partials(static_cast<size_t>(columns) * G * 2 + 2 * static_cast<size_t>(columns) + 64);
   QMBED_DISPATCH(precision, cplx,
                  (multi_dot_kernel<T, C><<<G, kThreads, 0, stream_>>>(static_cast<const T*>(A), ld, m,
                                                                       static_cast<const T*>(w), n,
-                                                                      partials_.as<double>())));
+                                                                      partials_.as<double>(), self_sq ? 1 : 0)));
   QMBED_LAUNCH_CHECK();
-  const int count = 2 * m;
-  finish_kernel<<<(count + 127) / 128, 128, 0, stream_>>>(partials_.as<double>(), G, count, results_.as<double>());
+  const int count = 2 * columns;
+  finish_kernel<<<count, kFinishThreads, 0, stream_>>>(partials_.as<double>(), G, count, results_.as<double>());
   QMBED_LAUNCH_CHECK();
   QMBED_CUDA(cudaMemcpyAsync(host_results_, results_.get(), count * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   sync();
   for (int j = 0; j < m; ++j) out[j] = C64(host_results_[2 * j], host_results_[2 * j + 1]);
+  if (self_sq) *self_sq = host_results_[2 * m];
+}
+
+void BlockOps::scale_into(const void* src, void* dst, uint64_t n, double divisor, int precision, bool cplx) {
+  const uint64_t count = n * (cplx ? 2 : 1);
+  const int G = stream_grid(count, sms_);
+  if (precision == 64)
+    scale_into_kernel<double><<<G, kThreads, 0, stream_>>>(static_cast<const double*>(src), static_cast<double*>(dst),
+                                                           count, divisor);
+  else
+    scale_into_kernel<float><<<G, kThreads, 0, stream_>>>(static_cast<const float*>(src), static_cast<float*>(dst),
+                                                          count, divisor);
+  QMBED_LAUNCH_CHECK();
 }
 
 double BlockOps::norm(const void* w, uint64_t n, int precision, bool cplx) {
@@ -599,7 +665,8 @@ double BlockOps::norm(const void* w, uint64_t n, int precision, bool cplx) {
 }
 
 double BlockOps::subtract(const void* A, uint64_t ld, int m, const C64* h, void* w, uint64_t n, int precision,
-                          bool cplx, bool want_norm) {
+                          bool cplx, bool want_norm, const void* src) {
+  if (m <= 0 && src && src != w) copy(src, w, n * (cplx ? 2 : 1) * (precision == 64 ? 8 : 4));
   if (m <= 0 && !want_norm) return 0.0;
   if (m <= 0) return norm(w, n, precision, cplx);
   ensure_coeffs(static_cast<size_t>(m) * 16);
@@ -614,7 +681,8 @@ double BlockOps::subtract(const void* A, uint64_t ld, int m, const C64* h, void*
                      QMBED_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                      static_cast<int>(smem)));
                    kernel<<<G, kThreads, smem, stream_>>>(static_cast<const T*>(A), ld, m, coeffs_.as<double>(),
-                                                          static_cast<T*>(w), n, partials);
+                                                          static_cast<const T*>(src ? src : w), static_cast<T*>(w), n,
+                                                          partials);
                  }));
   QMBED_LAUNCH_CHECK();
   if (!want_norm) return 0.0;

@@ -29,12 +29,16 @@ class BlockOps {
   cudaStream_t stream() const { return stream_; }
   int sms() const { return sms_; }
 
-  // out[j] = <A_j, w> (conjugate-linear in A) for j < m.
-  void dots(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx, C64* out);
+  // out[j] = <A_j, w> (conjugate-linear in A) for j < m; with self_sq, also
+  // ||w||^2 from the same pass over w.
+  void dots(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx, C64* out,
+            double* self_sq = nullptr);
   double norm(const void* w, uint64_t n, int precision, bool cplx);
-  // w -= sum_j h_j A_j; returns ||w|| afterwards when `want_norm`.
+  // w = src - sum_j h_j A_j (src = w when null); returns ||w|| when `want_norm`.
   double subtract(const void* A, uint64_t ld, int m, const C64* h, void* w, uint64_t n, int precision, bool cplx,
-                  bool want_norm);
+                  bool want_norm, const void* src = nullptr);
+  // dst = src / divisor
+  void scale_into(const void* src, void* dst, uint64_t n, double divisor, int precision, bool cplx);
   // out_k = sum_j Y[j + m k] A_j for k < K.
   void combine(const void* A, uint64_t ld, int m, const C64* Y, int K, void* out, uint64_t ld_out, uint64_t n,
                int precision, bool cplx);

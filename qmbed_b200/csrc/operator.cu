@@ -461,18 +461,37 @@ __global__ void __launch_bounds__(256) spmv_packed_kernel(uint64_t n, const IDX*
   const int lane = threadIdx.x % LANES;
   const uint64_t group = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LANES;
   const uint64_t groups = static_cast<uint64_t>(gridDim.x) * blockDim.x / LANES;
+  constexpr int kBatch = 4;  // entries per lane issued together: loads, then gathers, then FMAs
   for (uint64_t r = group; r < n; r += groups) {
-    T acc = 0;
     const IDX begin = row_ptr[r], end = row_ptr[r + 1];
-    for (IDX p = begin + lane; p < end; p += LANES) {
-      const uint32_t e = __ldg(entries + p);
-      acc += table[e >> col_bits] * xs[e & col_mask];
+    // per-row operands requested before the entry loop so their latency overlaps it
+    T d = 0, xr = 0;
+    uint16_t orbit = 0;
+    if (lane == 0) {
+      d = diag[r];
+      xr = x[r];
+      if (SCALED) orbit = orbits[r];
+    }
+    T acc = 0;
+    for (IDX p0 = begin + lane; p0 < end; p0 += LANES * kBatch) {
+      uint32_t e[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const IDX p = p0 + u * LANES;
+        e[u] = p < end ? __ldg(entries + p) : 0u;
+      }
+      T g[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) g[u] = (p0 + u * LANES < end) ? xs[e[u] & col_mask] : static_cast<T>(0);
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u)
+        if (p0 + u * LANES < end) acc += table[e[u] >> col_bits] * g[u];
     }
 #pragma unroll
     for (int o = LANES / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, LANES);
     if (lane == 0) {
-      const T scale = SCALED ? sqrt_r[orbits[r]] : static_cast<T>(1);
-      y[r] = scale * acc + diag[r] * x[r];
+      const T scale = SCALED ? sqrt_r[orbit] : static_cast<T>(1);
+      y[r] = scale * acc + d * xr;
     }
   }
 }
