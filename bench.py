@@ -283,9 +283,12 @@ def main():
         traffic = json.loads(traffic_file.read_text()).get("dram_bytes_per_launch")
 
     # --- end to end through the C ABI with host buffers ---
-    v0 = np.ascontiguousarray(np.zeros((1, dim), np.complex128))
+    # pinned host buffers: the step's input vector and its result vectors
+    v0_t = torch.zeros((1, dim), dtype=torch.complex128, pin_memory=True)
+    v0 = v0_t.numpy()
     v0[0].real = engine.deterministic_start(dim, rank, device=local_rank)
-    vectors = np.zeros((args.eigenpairs, dim), np.complex128)
+    vectors_t = torch.zeros((args.eigenpairs, dim), dtype=torch.complex128, pin_memory=True)
+    vectors = vectors_t.numpy()
     values = np.zeros(args.eigenpairs)
     residuals = np.zeros(args.eigenpairs)
     options = EigshOptionsC(args.eigenpairs, 0, 0.0, args.krylov, args.tolerance, 1000, rank,

@@ -313,7 +313,16 @@ Value vectors_value(const std::vector<double>& host, uint64_t dim, size_t count)
 Value solve(qmbed_operator_s& handle, const SolverRequest& request, bool tagged) {
   std::lock_guard<std::mutex> lock(handle.mu);
   LinearOperatorView view = handle.view();
-  EigshResult r = eigsh(view, request.options, request.initial, request.mode, handle.block_ops());
+  std::vector<double> initial;
+  for (const auto& v : request.initial) {
+    if (v.size() != view.dim) raise(QMBED_DIMENSION_MISMATCH, "eigsh initial vector does not match the operator");
+    for (const C64& x : v) {
+      initial.push_back(x.real());
+      initial.push_back(x.imag());
+    }
+  }
+  EigshResult r = eigsh(view, request.options, initial.data(), static_cast<int>(request.initial.size()), request.mode,
+                        handle.block_ops());
   Value out = Value::object();
   if (tagged) out.set("kind", Value::string("eigensystem"));
   const uint64_t dim = view.dim;
@@ -850,30 +859,26 @@ int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, const
     o.max_iterations = options->max_iterations;
     o.seed = options->seed;
     const uint64_t n = op->op->dim();
-    std::vector<std::vector<C64>> init;
-    for (int k = 0; k < n_initial; ++k) {
-      std::vector<C64> v(n);
-      for (uint64_t i = 0; i < n; ++i) v[i] = C64(initial[2 * (k * n + i)], initial[2 * (k * n + i) + 1]);
-      init.push_back(std::move(v));
-    }
+    if (n_initial < 0 || (n_initial > 0 && !initial)) raise(QMBED_INVALID_OPTIONS, "invalid initial vectors");
     LinearOperatorView view = op->view();
-    EigshResult r = eigsh(view, o, init, options->mode, op->block_ops());
+    EigshResult r = eigsh(view, o, initial, n_initial, options->mode, op->block_ops());
     for (size_t i = 0; i < r.eigenvalues.size(); ++i) {
       eigenvalues[i] = r.eigenvalues[i];
       residuals[i] = r.residuals[i];
     }
     if (eigenvectors) {
       const size_t k = r.eigenvalues.size();
+      BlockOps& ops = op->block_ops();
       if (r.complex_vectors) {
-        QMBED_CUDA(cudaMemcpy(eigenvectors, r.vectors.get(), k * n * 16, cudaMemcpyDeviceToHost));
+        QMBED_CUDA(cudaMemcpyAsync(eigenvectors, r.vectors.get(), k * n * 16, cudaMemcpyDeviceToHost, ops.stream()));
       } else {
-        std::vector<double> real(k * n);
-        QMBED_CUDA(cudaMemcpy(real.data(), r.vectors.get(), real.size() * 8, cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < real.size(); ++i) {
-          eigenvectors[2 * i] = real[i];
-          eigenvectors[2 * i + 1] = 0.0;
-        }
+        // widen to interleaved complex on the device, then one copy into the caller's buffer
+        DeviceBuffer wide(std::max<size_t>(k * n, 1) * 16);
+        ops.widen_real(r.vectors.as<double>(), wide.as<double>(), k * n);
+        QMBED_CUDA(cudaMemcpyAsync(eigenvectors, wide.get(), k * n * 16, cudaMemcpyDeviceToHost, ops.stream()));
+        ops.sync();
       }
+      ops.sync();
     }
     if (info) {
       info->iterations = r.iterations;

@@ -29,9 +29,9 @@ constexpr size_t kFullKrylovDenseFallback = 2048;
 constexpr size_t kTridiagonalWindow = 96;
 constexpr double kEps = 2.220446049250313e-16;
 const double kDgks = 1.0 / std::sqrt(2.0);
-// FP32 vectors resolve residuals to about 1e-6 of the spectral scale; the
-// mixed solver hands over to FP64 refinement below this relative level.
-constexpr double kMixedHandover = 2.0e-5;
+// FP32 vectors resolve residuals to about 1e-7 of the spectral scale; the mixed
+// solver hands over to FP64 refinement below this relative level.
+constexpr double kMixedHandover = 2.0e-6;
 
 struct Panel {
   DeviceBuffer buf;
@@ -594,24 +594,33 @@ void validate(const EigshOptions& o, uint64_t n) {
 
 }  // namespace
 
-EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options,
-                  const std::vector<std::vector<C64>>& initial, int mode, BlockOps& ops) {
+EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options, const double* initial, int n_initial,
+                  int mode, BlockOps& ops) {
   const uint64_t n = op.dim;
   validate(options, n);
+  // validate_eigsh_initial (src/solve/mod.rs:660-688)
   bool complex_initial = false;
-  for (const auto& v : initial) {
-    if (v.size() != n) raise(QMBED_DIMENSION_MISMATCH, "eigsh initial vector does not match the operator");
+  for (int k = 0; k < n_initial; ++k) {
+    const double* v = initial + 2 * static_cast<size_t>(k) * n;
     double sq = 0.0;
-    for (const C64& x : v) {
-      if (!std::isfinite(x.real()) || !std::isfinite(x.imag()))
+    for (uint64_t i = 0; i < n; ++i) {
+      const double re = v[2 * i], im = v[2 * i + 1];
+      if (!std::isfinite(re) || !std::isfinite(im))
         raise(QMBED_INVALID_OPTIONS, "eigsh initial vector must contain only finite values");
-      if (std::fabs(x.imag()) > 1.0e-14) complex_initial = true;
-      sq += std::norm(x);
+      if (std::fabs(im) > 1.0e-14) complex_initial = true;
+      sq += re * re + im * im;
     }
     if (!std::isfinite(std::sqrt(sq)) || std::sqrt(sq) <= kEps)
       raise(QMBED_INVALID_OPTIONS, "eigsh initial vector must have nonzero finite norm");
   }
   const bool cplx = !op.real || complex_initial;
+  // One upload of the caller's vectors; precision/real-part conversion on the device.
+  DeviceBuffer staged;
+  if (n_initial > 0) {
+    staged.allocate(static_cast<size_t>(n_initial) * n * 16);
+    QMBED_CUDA(cudaMemcpyAsync(staged.get(), initial, static_cast<size_t>(n_initial) * n * 16,
+                               cudaMemcpyHostToDevice, ops.stream()));
+  }
   Ctx c64{op, ops, 64, cplx, n};
   if (n <= kGuaranteedDense || (n <= kAutomaticDense && options.krylov_dimension == 0)) {
     EigshResult r = dense_eigsh(c64, options);
@@ -620,10 +629,11 @@ EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options,
     return r;
   }
   auto upload_initial = [&](Ctx& c, Panel& panel) {
-    if (initial.empty()) return 0;
-    panel.alloc(n, static_cast<int>(initial.size()), c.prec, c.cplx);
-    for (size_t i = 0; i < initial.size(); ++i) upload_vector(c, initial[i], panel.col(static_cast<int>(i)));
-    return static_cast<int>(initial.size());
+    if (n_initial == 0) return 0;
+    panel.alloc(n, n_initial, c.prec, c.cplx);
+    for (int i = 0; i < n_initial; ++i)
+      c.ops.import_complex(staged.as<double>() + 2 * static_cast<size_t>(i) * n, panel.col(i), n, c.prec, c.cplx);
+    return n_initial;
   };
   if (mode == kModePlainFP64) {
     Panel init;
@@ -633,8 +643,8 @@ EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options,
     r.fp64_iterations = r.iterations;
     return r;
   }
-  // Mixed precision: FP32 vectors to the handover tolerance, then FP64
-  // thick restart seeded with the FP32 Ritz subspace to the requested one.
+  // Mixed precision: FP32 vectors and H.v to the handover tolerance, then the
+  // FP64 thick restart seeded with the FP32 Ritz vectors to the requested one.
   Ctx c32{op, ops, 32, cplx, n};
   EigshOptions first = options;
   first.tolerance = std::max(options.tolerance, kMixedHandover);
@@ -645,13 +655,16 @@ EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options,
     phase1 = expanding(c32, first, &init32, n_init32);
   } catch (const Error& e) {
     if (e.code != QMBED_NON_CONVERGENCE) throw;
+    // the FP64 reference algorithms as the fallback, with the spent work counted
     Panel init;
     const int n_init = upload_initial(c64, init);
-    EigshResult r = expanding(c64, options, &init, n_init);
+    EigshOptions rest = options;
+    rest.max_iterations = options.max_iterations > e.iterations ? options.max_iterations - e.iterations : 1;
+    EigshResult r = expanding(c64, rest, &init, n_init);
     r.fp32_iterations = e.iterations;
+    r.fp64_iterations = r.iterations;
     r.iterations += e.iterations;
     r.operator_applications = c32.applications + c64.applications;
-    r.fp64_iterations = r.iterations - e.iterations;
     return r;
   }
   const int k = static_cast<int>(phase1.eigenvalues.size());

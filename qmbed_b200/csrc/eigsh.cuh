@@ -53,8 +53,9 @@ struct LinearOperatorView {
   ApplyFn apply;
 };
 
-// Initial vectors are host arrays of dim complex values (may be empty).
-EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options,
-                  const std::vector<std::vector<C64>>& initial, int mode, BlockOps& ops);
+// Initial vectors: `n_initial` host vectors of dim complex values,
+// interleaved (re, im) doubles, contiguous (may be null when n_initial = 0).
+EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options, const double* initial, int n_initial,
+                  int mode, BlockOps& ops);
 
 }  // namespace qmbed

@@ -229,6 +229,21 @@ __global__ void scale_into_kernel(const T* __restrict__ src, T* __restrict__ dst
     dst[i] = static_cast<T>(static_cast<double>(src[i]) / divisor);
 }
 
+__global__ void widen_real_kernel(const double* __restrict__ src, double* __restrict__ dst, uint64_t n) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    dst[2 * i] = src[i];
+    dst[2 * i + 1] = 0.0;
+  }
+}
+
+template <typename D>
+__global__ void real_part_strided_kernel(const double* __restrict__ src, D* __restrict__ dst, uint64_t n) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    dst[i] = static_cast<D>(src[2 * i]);
+}
+
 template <typename S, typename D>
 __global__ void convert_kernel(const S* __restrict__ src, D* __restrict__ dst, uint64_t count) {
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
@@ -729,6 +744,23 @@ void BlockOps::convert(const void* src, int src_precision, void* dst, int dst_pr
   else
     convert_kernel<float, double><<<G, kThreads, 0, stream_>>>(static_cast<const float*>(src),
                                                                static_cast<double*>(dst), elements);
+  QMBED_LAUNCH_CHECK();
+}
+
+void BlockOps::widen_real(const double* src, double* dst, uint64_t n) {
+  const int G = stream_grid(n, sms_);
+  widen_real_kernel<<<G, kThreads, 0, stream_>>>(src, dst, n);
+  QMBED_LAUNCH_CHECK();
+}
+
+void BlockOps::import_complex(const double* src, void* dst, uint64_t n, int precision, bool cplx) {
+  if (cplx) {
+    convert(src, 64, dst, precision, 2 * n);
+    return;
+  }
+  const int G = stream_grid(n, sms_);
+  if (precision == 64) real_part_strided_kernel<double><<<G, kThreads, 0, stream_>>>(src, static_cast<double*>(dst), n);
+  else real_part_strided_kernel<float><<<G, kThreads, 0, stream_>>>(src, static_cast<float*>(dst), n);
   QMBED_LAUNCH_CHECK();
 }
 

@@ -46,6 +46,10 @@ class BlockOps {
   // dst (dst_precision) = src (src_precision), `elements` scalars (complex = 2).
   void convert(const void* src, int src_precision, void* dst, int dst_precision, uint64_t elements);
   void copy(const void* src, void* dst, uint64_t bytes);
+  // dst[2i] = src[i], dst[2i+1] = 0 (FP64).
+  void widen_real(const double* src, double* dst, uint64_t n);
+  // dst (precision, complex or real part only) from an interleaved complex FP64 device vector.
+  void import_complex(const double* src, void* dst, uint64_t n, int precision, bool cplx);
   // Reference LCG start vector (deterministic_start, src/solve/mod.rs:729-742),
   // unnormalised, real part only; imaginary parts zero for complex vectors.
   void lcg_start(void* out, uint64_t n, uint64_t seed, int precision, bool cplx);

@@ -463,14 +463,16 @@ __global__ void __launch_bounds__(256) spmv_packed_kernel(uint64_t n, const IDX*
   const uint64_t groups = static_cast<uint64_t>(gridDim.x) * blockDim.x / LANES;
   constexpr int kBatch = 4;  // entries per lane issued together: loads, then gathers, then FMAs
   for (uint64_t r = group; r < n; r += groups) {
-    const IDX begin = row_ptr[r], end = row_ptr[r + 1];
+    // Streamed arrays (row pointers, entries, diagonal, x, orbits) are read
+    // evict-first so the L2 keeps the gathered vector xs.
+    const IDX begin = __ldcs(row_ptr + r), end = __ldcs(row_ptr + r + 1);
     // per-row operands requested before the entry loop so their latency overlaps it
     T d = 0, xr = 0;
     uint16_t orbit = 0;
     if (lane == 0) {
-      d = diag[r];
-      xr = x[r];
-      if (SCALED) orbit = orbits[r];
+      d = __ldcs(diag + r);
+      xr = __ldcs(x + r);
+      if (SCALED) orbit = __ldcs(orbits + r);
     }
     T acc = 0;
     for (IDX p0 = begin + lane; p0 < end; p0 += LANES * kBatch) {
@@ -478,7 +480,7 @@ __global__ void __launch_bounds__(256) spmv_packed_kernel(uint64_t n, const IDX*
 #pragma unroll
       for (int u = 0; u < kBatch; ++u) {
         const IDX p = p0 + u * LANES;
-        e[u] = p < end ? __ldg(entries + p) : 0u;
+        e[u] = p < end ? __ldcs(entries + p) : 0u;
       }
       T g[kBatch];
 #pragma unroll
@@ -491,7 +493,7 @@ __global__ void __launch_bounds__(256) spmv_packed_kernel(uint64_t n, const IDX*
     for (int o = LANES / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, LANES);
     if (lane == 0) {
       const T scale = SCALED ? sqrt_r[orbit] : static_cast<T>(1);
-      y[r] = scale * acc + d * xr;
+      __stcs(y + r, scale * acc + d * xr);
     }
   }
 }
@@ -550,7 +552,7 @@ __global__ void scale_by_orbit_kernel(uint64_t n, int comps, const uint16_t* __r
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n * comps; i += stride) {
     const uint64_t r = i / comps;
-    xs[i] = x[i] * static_cast<T>(inv_sqrt[orbits[r]]);
+    xs[i] = __ldcs(x + i) * static_cast<T>(inv_sqrt[__ldcs(orbits + r)]);
   }
 }
 
