@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--eigenpairs", type=int, default=4)
     p.add_argument("--krylov", type=int, default=40)
     p.add_argument("--tolerance", type=float, default=1e-10)
-    p.add_argument("--mode", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--mode", default="filtered", choices=["filtered", "mixed", "fp64"])
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI leg (profiling runs)")
@@ -277,8 +277,35 @@ def main():
     hv64_s = hv64_start.elapsed_time(hv64_stop) / 1000.0 / args.hv_launches
     del x, y, x64, y64
 
+    # --- block action (FP32, 8 vectors, three-term step): the filter kernel of the filtered solver ---
+    block = None
+    if args.mode == "filtered":
+        nb = 8
+        zb = torch.rand((dim, nb), dtype=torch.float32, device="cuda")
+        pb = torch.rand_like(zb)
+        step = dict(precision=32, alpha=1.0 / 16.0, beta=0.0, gamma=0.5, p=pb, stream=stream)
+        for _ in range(3):
+            op.apply_block_device(zb, pb, nb, **step)
+        b_start, b_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b_start.record()
+        for _ in range(args.hv_launches):
+            op.apply_block_device(zb, pb, nb, **step)
+        b_stop.record()
+        torch.cuda.synchronize()
+        block_s = b_start.elapsed_time(b_stop) / 1000.0 / args.hv_launches
+        # nb operand-model H.v plus the block of the third term
+        block_bytes = nb * hv_bytes + dim * nb * 4
+        block = {"nb": nb, "ms": block_s * 1e3, "operand_bytes": block_bytes, "gbs": block_bytes / block_s / 1e9,
+                 "per_vector_ms": block_s * 1e3 / nb}
+        del zb, pb
+
+    if block:
+        kernel, achieved_top = "spmm_packed_kernel (FP32 block action, 8 vectors)", block["gbs"]
+        traffic_file = ROOT / "profiles" / f"spmm_packed_L{sites}_traffic.json"
+    else:
+        kernel, achieved_top = "spmv_packed_kernel (FP32 H.v)", achieved
+        traffic_file = ROOT / "profiles" / f"spmv_packed_L{sites}_traffic.json"
     traffic = None
-    traffic_file = ROOT / "profiles" / "spmv_packed_L34_traffic.json"
     if traffic_file.exists():
         traffic = json.loads(traffic_file.read_text()).get("dram_bytes_per_launch")
 
@@ -292,7 +319,7 @@ def main():
     values = np.zeros(args.eigenpairs)
     residuals = np.zeros(args.eigenpairs)
     options = EigshOptionsC(args.eigenpairs, 0, 0.0, args.krylov, args.tolerance, 1000, rank,
-                            1 if args.mode == "mixed" else 0)
+                            engine.MODES[args.mode])
     e2e_info = EigshInfoC()
     h2d = v0.nbytes
     d2h = vectors.nbytes + values.nbytes + residuals.nbytes
@@ -324,7 +351,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * elapsed / args.steps, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.mode == "mixed" else "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.mode == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": {"workload": f"heisenberg L={sites} k=0 p=+1 up={sites // 2} dim={dim}, {args.eigenpairs} "
                                    f"lowest, krylov {args.krylov}, tol {args.tolerance:g}, mode {args.mode}",
@@ -340,8 +367,9 @@ def main():
             "hv": {"fp32_ms": hv_s * 1e3, "fp64_ms": hv64_s * 1e3, "operand_bytes_fp32": hv_bytes,
                    "operand_bytes_fp64": op.operand_bytes(64), "fp32_gbs": achieved,
                    "fp64_gbs": op.operand_bytes(64) / hv64_s / 1e9},
-            "roofline": {"bound": "hbm", "kernel": "spmv_packed_kernel (FP32 H.v)", "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "block_action": block,
+            "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved_top,
+                         "peak": peak, "unit": "GB/s", "frac": achieved_top / peak, "traffic": traffic,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "_fallback" not in peaks
                          else "fallback 6650 GB/s"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -72,7 +72,9 @@ enum {
 /* Solver modes. */
 enum {
   QMBED_MODE_PLAIN_FP64 = 0, /* the reference algorithms in FP64 */
-  QMBED_MODE_MIXED = 1       /* FP32 vectors and H.v, FP64 recurrences, FP64 refinement to tolerance */
+  QMBED_MODE_MIXED = 1,      /* FP32 vectors and H.v, FP64 recurrences, FP64 refinement to tolerance */
+  QMBED_MODE_FILTERED = 2    /* block Chebyshev-filtered subspace iteration, FP32 then FP64, for the
+                                smallest algebraic pairs of real packed operators; otherwise as MIXED */
 };
 
 typedef struct qmbed_basis_s* qmbed_basis;
@@ -118,6 +120,18 @@ QMBED_API int qmbed_gpu_operator_info(qmbed_operator op, uint64_t* dimension, in
  * interleaved complex vectors. stream may be NULL (default stream). */
 QMBED_API int qmbed_gpu_operator_apply_device(qmbed_operator op, int precision, int complex_vectors, const void* x,
                                               void* y, void* stream, int force_matrix_free);
+/* Block action on row-major n x nb device blocks (nb = 8 or 16), in the
+ * orbit-scaled coordinates z = x / sqrt(R) of symmetry sectors (z = x without
+ * symmetry): out = alpha * (S^-1 H S) z + beta * z + gamma * p, S = diag(sqrt(R)).
+ * p may be NULL; out may equal p but not z. One call is one step of a
+ * three-term recurrence over nb vectors (the Chebyshev filter of the
+ * QMBED_MODE_FILTERED solver). Real operators with packed storage only
+ * (otherwise QMBED_STATUS_UNSUPPORTED_BACKEND). No counterpart in the
+ * reference, whose operators act on one vector at a time
+ * (LinearOperator::apply_real, src/operator/mod.rs:1414-1485). */
+QMBED_API int qmbed_gpu_operator_apply_block_device(qmbed_operator op, int precision, int nb, const void* z,
+                                                    const void* p, void* out, double alpha, double beta, double gamma,
+                                                    void* stream);
 /* The same action as qmbed_gpu_operator_apply_device, for callers that cannot
  * let a library allocate device memory (applications that manage all GPU
  * memory through their own pool or budget, or that cannot afford the device

@@ -101,6 +101,7 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_operator_apply_device.argtypes = [vp, i, i, vp, vp, vp, i]
     L.qmbed_gpu_operator_apply_host.argtypes = [vp, i, vp, vp, i]
     L.qmbed_gpu_operator_apply_device_noalloc.argtypes = [vp, i, i, vp, vp, vp]
+    L.qmbed_gpu_operator_apply_block_device.argtypes = [vp, i, i, vp, vp, vp, d, d, d, vp]
     L.qmbed_gpu_operator_export_csr.argtypes = [vp, P(u64), vp, vp, vp]
     L.qmbed_gpu_operator_operand_bytes.argtypes = [vp, i, i, P(d)]
     L.qmbed_gpu_eigsh.argtypes = [vp, P(EigshOptionsC), vp, i, vp, vp, vp, P(EigshInfoC)]

@@ -87,8 +87,14 @@ struct qmbed_operator_s {
     BlockOps& b = block_ops();
     SpinOperator* raw = op.get();
     cudaStream_t s = b.stream();
-    return LinearOperatorView{raw->dim(), raw->is_real(),
-                              [raw, s](int prec, bool cplx, const void* x, void* y) { raw->apply(prec, cplx, x, y, s); }};
+    LinearOperatorView v{raw->dim(), raw->is_real(),
+                         [raw, s](int prec, bool cplx, const void* x, void* y) { raw->apply(prec, cplx, x, y, s); }};
+    if (raw->supports_block()) {
+      v.block_apply = [raw, s](int prec, int nb, const void* z, const void* p, void* out, double alpha, double beta,
+                               double gamma) { raw->apply_block(prec, nb, z, p, out, alpha, beta, gamma, s); };
+      v.weights = raw->basis().symmetric() ? raw->basis().orbits() : nullptr;
+    }
+    return v;
   }
 };
 
@@ -287,7 +293,8 @@ SolverRequest parse_solver(const Value& s) {
   if (s.has("precision")) {
     const std::string p = s.at("precision").as_string();
     if (p == "mixed") r.mode = kModeMixed;
-    else if (p != "fp64") raise(QMBED_INVALID_OPTIONS, "precision must be `fp64` or `mixed`");
+    else if (p == "filtered") r.mode = kModeFiltered;
+    else if (p != "fp64") raise(QMBED_INVALID_OPTIONS, "precision must be `fp64`, `mixed` or `filtered`");
   }
   return r;
 }
@@ -806,6 +813,16 @@ int qmbed_gpu_operator_apply_device(qmbed_operator op, int precision, int comple
   return guarded([&] {
     if (precision != 64 && precision != 32) raise(QMBED_INVALID_OPTIONS, "precision must be 64 or 32");
     op->op->apply(precision, complex_vectors != 0, x, y, static_cast<cudaStream_t>(stream), force_matrix_free != 0);
+  });
+}
+
+int qmbed_gpu_operator_apply_block_device(qmbed_operator op, int precision, int nb, const void* z, const void* p,
+                                          void* out, double alpha, double beta, double gamma, void* stream) {
+  return guarded([&] {
+    if (precision != 64 && precision != 32) raise(QMBED_INVALID_OPTIONS, "precision must be 64 or 32");
+    if (nb != 8 && nb != 16) raise(QMBED_INVALID_OPTIONS, "block width must be 8 or 16");
+    if (!z || !out || z == out) raise(QMBED_INVALID_OPTIONS, "block action needs distinct input and output blocks");
+    op->op->apply_block(precision, nb, z, p, out, alpha, beta, gamma, static_cast<cudaStream_t>(stream));
   });
 }
 

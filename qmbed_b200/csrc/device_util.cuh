@@ -7,6 +7,32 @@ namespace qmbed {
 
 constexpr int kBinomStride = 129;  // binomial table is [n][k], n,k <= 128
 
+// 16-byte vector access to rows of row-major blocks (addresses 16-byte aligned).
+// load16 reads through the read-only path: only for data no thread of the
+// launch writes. load16_rw is the coherent form for rows a launch rewrites.
+__device__ __forceinline__ void load16(const float* p, float (&v)[4]) {
+  const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void load16(const double* p, double (&v)[2]) {
+  const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+  v[0] = t.x; v[1] = t.y;
+}
+__device__ __forceinline__ void load16_rw(const float* p, float (&v)[4]) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void load16_rw(const double* p, double (&v)[2]) {
+  const double2 t = *reinterpret_cast<const double2*>(p);
+  v[0] = t.x; v[1] = t.y;
+}
+__device__ __forceinline__ void store16(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store16(double* p, const double (&v)[2]) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+}
+
 __device__ inline uint32_t warp_sum_u32(uint32_t v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;

@@ -18,6 +18,7 @@
 #include <numeric>
 
 #include "eigsh.cuh"
+#include "filtered.cuh"
 
 namespace qmbed {
 
@@ -598,6 +599,8 @@ EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options, con
                   int mode, BlockOps& ops) {
   const uint64_t n = op.dim;
   validate(options, n);
+  if (mode != kModePlainFP64 && mode != kModeMixed && mode != kModeFiltered)
+    raise(QMBED_INVALID_OPTIONS, "unknown solver mode");
   // validate_eigsh_initial (src/solve/mod.rs:660-688)
   bool complex_initial = false;
   for (int k = 0; k < n_initial; ++k) {
@@ -635,6 +638,13 @@ EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options, con
       c.ops.import_complex(staged.as<double>() + 2 * static_cast<size_t>(i) * n, panel.col(i), n, c.prec, c.cplx);
     return n_initial;
   };
+  if (mode == kModeFiltered && filtered_applicable(op, options, complex_initial)) {
+    try {
+      return filtered_eigsh(op, options, staged.as<double>(), n_initial, ops);
+    } catch (const Error& e) {
+      if (e.code != QMBED_NON_CONVERGENCE) throw;  // otherwise the mixed Lanczos path below decides
+    }
+  }
   if (mode == kModePlainFP64) {
     Panel init;
     const int n_init = upload_initial(c64, init);

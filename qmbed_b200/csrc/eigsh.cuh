@@ -27,6 +27,8 @@ struct EigshOptions {
 enum SolverMode : int {
   kModePlainFP64 = 0,  // the reference algorithms, FP64 vectors
   kModeMixed = 1,      // FP32 vectors and H.v, FP64 recurrences, then FP64 refinement to the tolerance
+  kModeFiltered = 2,   // block Chebyshev-filtered subspace iteration, FP32 then FP64 (real operators
+                       // with a block action, smallest algebraic); other requests run as kModeMixed
 };
 
 struct EigshResult {
@@ -47,10 +49,17 @@ struct EigshResult {
 // y = A x on device vectors for the given precision (64/32) and complex flag.
 using ApplyFn = std::function<void(int precision, bool cplx, const void* x, void* y)>;
 
+// out = alpha * (S^-1 H S) z + beta * z + gamma * p on row-major n x nb blocks in
+// the coordinates z = S^-1 x, S = diag(sqrt(weights)) (SpinOperator::apply_block).
+using BlockApplyFn = std::function<void(int precision, int nb, const void* z, const void* p, void* out, double alpha,
+                                        double beta, double gamma)>;
+
 struct LinearOperatorView {
   uint64_t dim;
   bool real;  // supports real vectors
   ApplyFn apply;
+  BlockApplyFn block_apply = nullptr;  // empty when the operator has no block action
+  const uint16_t* weights = nullptr;   // orbit sizes R of the block coordinates; null when every R is 1
 };
 
 // Initial vectors: `n_initial` host vectors of dim complex values,

@@ -1,0 +1,573 @@
+// Block Chebyshev-filtered subspace iteration for the smallest algebraic
+// eigenpairs of a real Hermitian operator.
+//
+// Method: the scaled Chebyshev filter recurrence of Zhou, Saad, Tiago and
+// Chelikowsky (J. Comput. Phys. 219, 2006, Algorithm 4.1 "scaled"), followed
+// by an orthonormalisation of the block through the eigen-decomposition of its
+// Gram matrix and a Rayleigh-Ritz step. The filter interval [cut, upper] is
+// damped, everything below `cut` is amplified. `upper` comes from a short
+// Lanczos run (largest Ritz value plus the last beta, the bound estimator of
+// Zhou and Li, Linear Algebra Appl. 435, 2011); `cut` is the largest Ritz
+// value of the block (by interlacing it lies at or above the block's share of
+// the spectrum).
+//
+// All block work happens in the orbit-scaled coordinates z = S^-1 x,
+// S = diag(sqrt(R)): the packed rows then need no orbit factor, inner products
+// carry the weight R (x.y = sum_r R_r z_r w_r) and the eigenvectors are x = S z.
+// Blocks are row-major n x nb so that one gathered column is one contiguous
+// 32/64-byte read for all nb vectors.
+//
+// Precision: FP32 blocks and block action (FP32 accumulation) with FP64 Gram
+// and Ritz matrices until every wanted residual is below 1e-5 of max(|lambda|,1)
+// (or stops improving), then FP64 blocks to the requested tolerance. The
+// acceptance test is the reference's r <= tol * max(|lambda|, 1)
+// (src/solve/mod.rs:1255, 1863), with r = ||H x - lambda x|| for ||x|| = 1.
+// The small symmetric eigenproblems run on the GPU (device Jacobi).
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <numeric>
+#include <type_traits>
+#include <vector>
+
+#include "device_util.cuh"
+#include "filtered.cuh"
+
+namespace qmbed {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kGramElems = 2048;            // block elements staged per tile of the Gram kernel
+constexpr double kFilterHandover = 1.0e-5;  // FP32 phase target (relative residual)
+constexpr int kMaxOuter = 80;               // outer iterations per precision phase
+constexpr int kBoundSteps = 24;             // Lanczos steps of the spectral bound estimate
+constexpr int kMaxDegree = 60;
+constexpr size_t kMaxFilteredPairs = 12;
+constexpr uint64_t kMinFilteredDim = 1024;
+
+// partial[b][i * NB + j] = sum over the rows of block b of w_r a[r][i] b[r][j]  (FP64)
+template <typename T, int NB>
+__global__ void __launch_bounds__(kThreads) block_gram_kernel(uint64_t n, const T* __restrict__ a,
+                                                               const T* __restrict__ b,
+                                                               const uint16_t* __restrict__ weights,
+                                                               double* __restrict__ partial) {
+  constexpr int kRows = kGramElems / NB;
+  constexpr int kPairs = NB * NB;
+  constexpr int kSplit = kThreads / kPairs;
+  static_assert(kThreads % kPairs == 0, "pairs must divide the block");
+  __shared__ double sa[kGramElems];
+  __shared__ double sb[kGramElems];
+  __shared__ double red[kThreads];
+  const int pair = threadIdx.x % kPairs, sub = threadIdx.x / kPairs;
+  const int i = pair / NB, j = pair % NB;
+  const uint64_t limit = n * NB;
+  double acc = 0.0;
+  for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kRows; t0 < n; t0 += static_cast<uint64_t>(gridDim.x) * kRows) {
+    const uint64_t base = t0 * NB;
+#pragma unroll
+    for (int q = 0; q < kGramElems / kThreads; ++q) {
+      const int e = q * kThreads + threadIdx.x;
+      const uint64_t g = base + e;
+      double va = 0.0, vb = 0.0;
+      if (g < limit) {
+        const double w = weights ? static_cast<double>(weights[t0 + e / NB]) : 1.0;
+        va = w * static_cast<double>(a[g]);
+        vb = static_cast<double>(b[g]);
+      }
+      sa[e] = va;
+      sb[e] = vb;
+    }
+    __syncthreads();
+    for (int r = sub; r < kRows; r += kSplit) acc += sa[r * NB + i] * sb[r * NB + j];
+    __syncthreads();
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < kPairs) {
+    double s = 0.0;
+    for (int q = 0; q < kSplit; ++q) s += red[q * kPairs + threadIdx.x];
+    partial[static_cast<uint64_t>(blockIdx.x) * kPairs + threadIdx.x] = s;
+  }
+}
+
+// out[t] = sum_b partial[b][t] in block order (deterministic).
+__global__ void reduce_partials_kernel(const double* __restrict__ partial, int blocks, int count,
+                                       double* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  double s = 0.0;
+  for (int b = 0; b < blocks; ++b) s += partial[static_cast<size_t>(b) * count + t];
+  out[t] = s;
+}
+
+// out[r][:] = z[r][:] C (C row-major NB x NB, FP64 arithmetic; out must not
+// alias z). With RESID also
+// partial[b][q] = sum_r w_r ((w[r][:] C)_q - theta_q out[r][q])^2.
+// Each thread produces 8 outputs of one row (NB / 8 threads per row), which
+// keeps the per-thread state near 100 registers instead of hoisting all of C.
+template <typename T, int NB, bool RESID>
+__global__ void __launch_bounds__(kThreads, 2) block_rotate_kernel(uint64_t n, const T* __restrict__ z,
+                                                                    T* __restrict__ out, const T* __restrict__ w,
+                                                                    const double* __restrict__ coeff,
+                                                                    const double* __restrict__ theta,
+                                                                    const uint16_t* __restrict__ weights,
+                                                                    double* __restrict__ partial) {
+  constexpr int VEC = 16 / sizeof(T);
+  constexpr int OUT = 8;
+  constexpr int SPLIT = NB / OUT;
+  static_assert(NB % OUT == 0 && 32 % SPLIT == 0, "rows must split evenly across lanes");
+  __shared__ double c[NB * NB];
+  __shared__ double th[NB];
+  __shared__ double red[kThreads / 32][NB];
+  for (int i = threadIdx.x; i < NB * NB; i += blockDim.x) c[i] = coeff[i];
+  if (RESID)
+    for (int i = threadIdx.x; i < NB; i += blockDim.x) th[i] = theta[i];
+  __syncthreads();
+  double res[OUT];
+#pragma unroll
+  for (int q = 0; q < OUT; ++q) res[q] = 0.0;
+  // the grid stride is a multiple of SPLIT, so a thread keeps its part
+  const int part = static_cast<int>(threadIdx.x % SPLIT);
+  const uint64_t total = n * SPLIT;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const uint64_t r = t / SPLIT;
+    double zin[NB];
+#pragma unroll
+    for (int v = 0; v < NB; v += VEC) {
+      T x[VEC];
+      load16(z + r * NB + v, x);
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) zin[v + q] = static_cast<double>(x[q]);
+    }
+    double zo[OUT];
+#pragma unroll
+    for (int q = 0; q < OUT; ++q) {
+      const int col = part * OUT + q;
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < NB; ++j) s = fma(zin[j], c[j * NB + col], s);
+      zo[q] = s;
+    }
+#pragma unroll
+    for (int v = 0; v < OUT; v += VEC) {
+      T x[VEC];
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) x[q] = static_cast<T>(zo[v + q]);
+      store16(out + r * NB + part * OUT + v, x);
+    }
+    if (RESID) {
+      double win[NB];
+#pragma unroll
+      for (int v = 0; v < NB; v += VEC) {
+        T x[VEC];
+        load16(w + r * NB + v, x);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) win[v + q] = static_cast<double>(x[q]);
+      }
+      const double wr = weights ? static_cast<double>(weights[r]) : 1.0;
+#pragma unroll
+      for (int q = 0; q < OUT; ++q) {
+        const int col = part * OUT + q;
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) s = fma(win[j], c[j * NB + col], s);
+        const double d = s - th[col] * zo[q];
+        res[q] = fma(wr * d, d, res[q]);
+      }
+    }
+  }
+  if (RESID) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < OUT; ++q) {
+      double v = res[q];
+      for (int o = 16; o >= SPLIT; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane < SPLIT) red[warp][lane * OUT + q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NB) {
+      double s = 0.0;
+      for (int q = 0; q < kThreads / 32; ++q) s += red[q][threadIdx.x];
+      partial[static_cast<uint64_t>(blockIdx.x) * NB + threadIdx.x] = s;
+    }
+  }
+}
+
+// out[i * n + r] = sqrt(R_r) z[r][i] for i < k (FP64, column-major).
+template <typename T, int NB>
+__global__ void block_export_kernel(uint64_t n, const T* __restrict__ z, int k, const uint16_t* __restrict__ weights,
+                                    double* __restrict__ out) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
+    const double s = weights ? sqrt(static_cast<double>(weights[r])) : 1.0;
+    for (int i = 0; i < k; ++i) out[static_cast<uint64_t>(i) * n + r] = s * static_cast<double>(z[r * NB + i]);
+  }
+}
+
+// z[r][i] = cols[i * n + r] / sqrt(R_r) for i < NB (FP64 column-major input).
+template <typename T, int NB>
+__global__ void block_import_kernel(uint64_t n, const double* __restrict__ cols, const uint16_t* __restrict__ weights,
+                                    T* __restrict__ z) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
+    const double s = weights ? 1.0 / sqrt(static_cast<double>(weights[r])) : 1.0;
+    for (int i = 0; i < NB; ++i) z[r * NB + i] = static_cast<T>(s * cols[static_cast<uint64_t>(i) * n + r]);
+  }
+}
+
+template <typename F>
+void dispatch_block(int prec, int nb, F&& f) {
+  using NB8 = std::integral_constant<int, 8>;
+  using NB16 = std::integral_constant<int, 16>;
+  if (prec == 64) {
+    if (nb == 8) f(double{}, NB8{});
+    else f(double{}, NB16{});
+  } else {
+    if (nb == 8) f(float{}, NB8{});
+    else f(float{}, NB16{});
+  }
+}
+
+// Ascending eigenpairs of a real symmetric m x m matrix (row-major, symmetrised
+// here) on the device; V row-major with eigenvectors as columns.
+void symmetric_eigen(int m, const std::vector<double>& a, std::vector<double>& values, std::vector<double>& V,
+                     cudaStream_t stream) {
+  std::vector<C64> ac(static_cast<size_t>(m) * m);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) ac[static_cast<size_t>(i) * m + j] = C64(0.5 * (a[i * m + j] + a[j * m + i]), 0.0);
+  std::vector<double> vals;
+  std::vector<C64> vecs;
+  device_hermitian_eigen(m, ac, vals, vecs, stream);
+  std::vector<int> order(m);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int l, int r) { return vals[l] < vals[r]; });
+  values.assign(m, 0.0);
+  V.assign(static_cast<size_t>(m) * m, 0.0);
+  for (int q = 0; q < m; ++q) {
+    const int col = order[q];
+    values[q] = vals[col];
+    // eigenvectors of a real matrix are real up to one phase: remove it
+    C64 big(0.0, 0.0);
+    for (int i = 0; i < m; ++i)
+      if (std::abs(vecs[static_cast<size_t>(col) * m + i]) > std::abs(big)) big = vecs[static_cast<size_t>(col) * m + i];
+    const C64 phase = std::abs(big) > 0.0 ? std::conj(big) / std::abs(big) : C64(1.0, 0.0);
+    for (int i = 0; i < m; ++i) V[static_cast<size_t>(i) * m + q] = (vecs[static_cast<size_t>(col) * m + i] * phase).real();
+  }
+}
+
+class BlockSolver {
+ public:
+  BlockSolver(const LinearOperatorView& op, const EigshOptions& o, BlockOps& ops, int nb)
+      : op_(op), o_(o), ops_(ops), n_(op.dim), nb_(nb), blocks_(2 * ops.sms()) {
+    partial_.allocate(static_cast<size_t>(blocks_) * 2 * nb * nb * sizeof(double));
+    result_.allocate(static_cast<size_t>(nb) * nb * sizeof(double));
+    coeff_.allocate((static_cast<size_t>(nb) * nb + nb) * sizeof(double));
+  }
+
+  size_t applications = 0;
+  size_t block_actions = 0;
+
+  // out = alpha * Ht z + beta * z + gamma * p
+  void act(int prec, const void* z, const void* p, void* out, double alpha, double beta, double gamma) {
+    op_.block_apply(prec, nb_, z, p, out, alpha, beta, gamma);
+    applications += static_cast<size_t>(nb_);
+    ++block_actions;
+  }
+
+  // G[i][j] = sum_r R_r a[r][i] b[r][j]
+  std::vector<double> gram(int prec, const void* a, const void* b) {
+    const cudaStream_t s = ops_.stream();
+    dispatch_block(prec, nb_, [&](auto ttag, auto nbtag) {
+      using T = decltype(ttag);
+      constexpr int NB = decltype(nbtag)::value;
+      block_gram_kernel<T, NB><<<blocks_, kThreads, 0, s>>>(n_, static_cast<const T*>(a), static_cast<const T*>(b),
+                                                            op_.weights, partial_.as<double>());
+    });
+    QMBED_LAUNCH_CHECK();
+    return reduce(nb_ * nb_);
+  }
+
+  // out = z C (out must not alias z); with `resid` returns the squared
+  // weighted residual norms of (w C) - out diag(theta).
+  std::vector<double> rotate(int prec, const void* z, void* out, const void* w, const std::vector<double>& C,
+                             const std::vector<double>& theta, bool resid) {
+    const cudaStream_t s = ops_.stream();
+    std::vector<double> host(C);
+    host.resize(static_cast<size_t>(nb_) * nb_ + nb_, 0.0);
+    for (size_t q = 0; q < theta.size() && q < static_cast<size_t>(nb_); ++q) host[static_cast<size_t>(nb_) * nb_ + q] = theta[q];
+    QMBED_CUDA(cudaMemcpyAsync(coeff_.get(), host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    const double* c = coeff_.as<double>();
+    dispatch_block(prec, nb_, [&](auto ttag, auto nbtag) {
+      using T = decltype(ttag);
+      constexpr int NB = decltype(nbtag)::value;
+      if (resid)
+        block_rotate_kernel<T, NB, true><<<blocks_, kThreads, 0, s>>>(
+            n_, static_cast<const T*>(z), static_cast<T*>(out), static_cast<const T*>(w), c, c + NB * NB,
+            op_.weights, partial_.as<double>());
+      else
+        block_rotate_kernel<T, NB, false><<<blocks_, kThreads, 0, s>>>(
+            n_, static_cast<const T*>(z), static_cast<T*>(out), nullptr, c, nullptr, op_.weights, nullptr);
+    });
+    QMBED_LAUNCH_CHECK();
+    if (!resid) return {};
+    return reduce(nb_);
+  }
+
+  // Orthonormal block (weighted inner product) spanning the columns of *A,
+  // left in *A (B is scratch; the pointers may be exchanged).
+  void orthonormalize(int prec, void*& A, void*& B, int passes) {
+    for (int pass = 0; pass < passes; ++pass) {
+      std::vector<double> G = gram(prec, A, A), mu, V;
+      symmetric_eigen(nb_, G, mu, V, ops_.stream());
+      const double top = std::max(mu.back(), std::numeric_limits<double>::min());
+      const double floor = top * (prec == 64 ? 1.0e-28 : 1.0e-14);
+      std::vector<double> C(static_cast<size_t>(nb_) * nb_);
+      for (int j = 0; j < nb_; ++j)
+        for (int q = 0; q < nb_; ++q) C[static_cast<size_t>(j) * nb_ + q] = V[static_cast<size_t>(j) * nb_ + q] / std::sqrt(std::max(mu[q], floor));
+      rotate(prec, A, B, nullptr, C, {}, false);
+      std::swap(A, B);
+    }
+  }
+
+  // Rayleigh-Ritz on the orthonormal block *A (B, W scratch): *A becomes the
+  // Ritz vectors, ascending values in theta, residual norms in res.
+  void rayleigh_ritz(int prec, void*& A, void*& B, void* W, std::vector<double>& theta, std::vector<double>& res) {
+    act(prec, A, nullptr, W, 1.0, 0.0, 0.0);
+    std::vector<double> Tm = gram(prec, A, W), Y;
+    symmetric_eigen(nb_, Tm, theta, Y, ops_.stream());
+    std::vector<double> r2 = rotate(prec, A, B, W, Y, theta, true);
+    std::swap(A, B);
+    res.assign(nb_, 0.0);
+    for (int q = 0; q < nb_; ++q) res[q] = std::sqrt(std::max(r2[q], 0.0));
+  }
+
+  // Scaled Chebyshev filter of degree d on [cut, upper] with spectrum lower
+  // estimate `lower`; the block in *A is filtered, B is scratch. On return *A
+  // holds the filtered block (the two pointers may be exchanged).
+  void filter(int prec, void*& A, void*& B, int degree, double lower, double cut, double upper) {
+    if (degree <= 0) return;
+    const double e = 0.5 * (upper - cut), c = 0.5 * (upper + cut);
+    const double sigma1 = e / (lower - c);
+    double sigma = sigma1;
+    act(prec, A, nullptr, B, sigma1 / e, -sigma1 * c / e, 0.0);
+    void* prev = A;
+    void* cur = B;
+    for (int i = 2; i <= degree; ++i) {
+      const double next = 1.0 / (2.0 / sigma1 - sigma);
+      act(prec, cur, prev, prev, 2.0 * next / e, -2.0 * next * c / e, -sigma * next);
+      std::swap(prev, cur);
+      sigma = next;
+    }
+    A = cur;
+    B = prev;
+  }
+
+  void import_columns(int prec, const double* cols, void* z) {
+    const int G = std::max(1, std::min<int>(static_cast<int>((n_ + kThreads - 1) / kThreads), 8 * ops_.sms()));
+    dispatch_block(prec, nb_, [&](auto ttag, auto nbtag) {
+      using T = decltype(ttag);
+      constexpr int NB = decltype(nbtag)::value;
+      block_import_kernel<T, NB><<<G, kThreads, 0, ops_.stream()>>>(n_, cols, op_.weights, static_cast<T*>(z));
+    });
+    QMBED_LAUNCH_CHECK();
+  }
+
+  void export_columns(int prec, const void* z, int k, double* out) {
+    const int G = std::max(1, std::min<int>(static_cast<int>((n_ + kThreads - 1) / kThreads), 8 * ops_.sms()));
+    dispatch_block(prec, nb_, [&](auto ttag, auto nbtag) {
+      using T = decltype(ttag);
+      constexpr int NB = decltype(nbtag)::value;
+      block_export_kernel<T, NB><<<G, kThreads, 0, ops_.stream()>>>(n_, static_cast<const T*>(z), k, op_.weights, out);
+    });
+    QMBED_LAUNCH_CHECK();
+  }
+
+ private:
+  std::vector<double> reduce(int count) {
+    const cudaStream_t s = ops_.stream();
+    reduce_partials_kernel<<<(count + 127) / 128, 128, 0, s>>>(partial_.as<double>(), blocks_, count, result_.as<double>());
+    QMBED_LAUNCH_CHECK();
+    std::vector<double> host(count);
+    QMBED_CUDA(cudaMemcpyAsync(host.data(), result_.get(), count * sizeof(double), cudaMemcpyDeviceToHost, s));
+    QMBED_CUDA(cudaStreamSynchronize(s));
+    return host;
+  }
+
+  const LinearOperatorView& op_;
+  const EigshOptions& o_;
+  BlockOps& ops_;
+  uint64_t n_;
+  int nb_;
+  int blocks_;
+  DeviceBuffer partial_, result_, coeff_;
+};
+
+struct Bounds {
+  std::vector<double> theta;  // ascending Ritz values
+  double beta = 0.0;          // last Lanczos beta
+  int steps = 0;
+};
+
+// Spectral bounds from a short Lanczos run in FP32 without reorthogonalisation
+// (only the extreme Ritz values are used). `start` is an FP64 real vector.
+Bounds lanczos_bounds(const LinearOperatorView& op, BlockOps& ops, const double* start, size_t& applications) {
+  const uint64_t n = op.dim;
+  const int m = static_cast<int>(std::min<uint64_t>(kBoundSteps, n - 1));
+  DeviceBuffer a(n * 4), b(n * 4), w(n * 4);
+  void* prev = a.get();
+  void* cur = b.get();
+  ops.convert(start, 64, cur, 32, n);
+  const double n0 = ops.norm(cur, n, 32, false);
+  if (!(n0 > 0.0)) raise(QMBED_INVALID_OPTIONS, "eigsh start vector has zero norm");
+  ops.scale(cur, n, n0, 32, false);
+  std::vector<double> alpha, beta;
+  double b_prev = 0.0;
+  for (int j = 0; j < m; ++j) {
+    op.apply(32, false, cur, w.get());
+    ++applications;
+    C64 h;
+    ops.dots(cur, n, 1, w.get(), n, 32, false, &h);
+    double norm = ops.subtract(cur, n, 1, &h, w.get(), n, 32, false, j == 0);
+    if (j > 0) {
+      const C64 hb(b_prev, 0.0);
+      norm = ops.subtract(prev, n, 1, &hb, w.get(), n, 32, false, true);
+    }
+    alpha.push_back(h.real());
+    beta.push_back(norm);
+    if (!(norm > 1.0e-10 * std::max(1.0, std::fabs(h.real())))) break;
+    std::swap(prev, cur);
+    ops.scale_into(w.get(), cur, n, norm, 32, false);
+    b_prev = norm;
+  }
+  const int size = static_cast<int>(alpha.size());
+  std::vector<double> T(static_cast<size_t>(size) * size, 0.0), vals, vecs;
+  for (int i = 0; i < size; ++i) {
+    T[static_cast<size_t>(i) * size + i] = alpha[i];
+    if (i + 1 < size) T[static_cast<size_t>(i) * size + i + 1] = T[static_cast<size_t>(i + 1) * size + i] = beta[i];
+  }
+  symmetric_eigen(size, T, vals, vecs, ops.stream());
+  return Bounds{vals, beta.back(), size};
+}
+
+}  // namespace
+
+bool filtered_applicable(const LinearOperatorView& op, const EigshOptions& o, bool complex_initial) {
+  return static_cast<bool>(op.block_apply) && op.real && !complex_initial && o.target == kSmallestAlgebraic &&
+         o.eigenpairs <= kMaxFilteredPairs && op.dim >= kMinFilteredDim;
+}
+
+EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, const double* staged_initial,
+                           int n_initial, BlockOps& ops) {
+  const uint64_t n = op.dim;
+  const int k = static_cast<int>(o.eigenpairs);
+  const int nb = k <= 5 ? 8 : 16;
+  BlockSolver solver(op, o, ops, nb);
+
+  // Start columns: the caller's vectors (real parts), then reference
+  // deterministic starts with seeds o.seed + j * 0x9e3779b9.
+  DeviceBuffer cols(static_cast<size_t>(n) * nb * sizeof(double));
+  auto col = [&](int j) { return cols.as<double>() + static_cast<size_t>(j) * n; };
+  const int used = std::min(n_initial, nb);
+  for (int j = 0; j < used; ++j) ops.import_complex(staged_initial + 2 * static_cast<size_t>(j) * n, col(j), n, 64, false);
+  for (int j = used; j < nb; ++j) ops.lcg_start(col(j), n, o.seed + static_cast<uint64_t>(j - used) * 0x9e3779b9ULL, 64, false);
+
+  size_t bound_applications = 0;
+  const Bounds bd = lanczos_bounds(op, ops, col(0), bound_applications);
+  const double upper = bd.theta.back() + bd.beta;
+  double lower = bd.theta.front();
+  double cut = bd.theta[std::min<size_t>(nb, bd.theta.size()) - 1];
+
+  std::vector<double> theta, res;
+  int iterations[2] = {0, 0};
+  auto rho = [&](double x, double c, double e) { return std::acosh(std::max((c - x) / e, 1.0)); };
+
+  // One precision phase: filter, orthonormalise, Rayleigh-Ritz until every
+  // wanted residual meets target * max(|theta|, 1). Returns whether it did.
+  auto phase = [&](int prec, void*& A, void*& B, void* W, double target, int& it) {
+    double best = std::numeric_limits<double>::infinity();
+    int stall = 0;
+    while (true) {
+      double worst = 0.0;
+      bool done = true;
+      for (int i = 0; i < k; ++i) {
+        const double scale = std::max(std::fabs(theta[i]), 1.0);
+        worst = std::max(worst, res[i] / scale);
+        if (!(res[i] <= target * scale)) done = false;
+      }
+      if (done) return true;
+      if (worst < 0.5 * best) {
+        best = worst;
+        stall = 0;
+      } else if (++stall >= 3) {
+        return false;
+      }
+      if (it >= kMaxOuter) return false;
+      lower = std::min(lower, theta.front());
+      cut = theta.back();
+      if (!(cut > theta.front())) cut = theta.front() + 1.0e-3 * (upper - theta.front());
+      const double e = 0.5 * (upper - cut), c = 0.5 * (upper + cut);
+      if (!(e > 0.0)) return false;
+      double need = 1.0;
+      for (int i = 0; i < k; ++i) {
+        const double goal = 0.5 * target * std::max(std::fabs(theta[i]), 1.0);
+        if (res[i] > goal) need = std::max(need, std::log(res[i] / goal) / std::max(rho(theta[i], c, e), 1.0e-3));
+      }
+      const double spread = std::max(rho(theta.front(), c, e), 1.0e-3);
+      const double cap = std::log(prec == 64 ? 1.0e11 : 1.0e5) / spread;
+      const int degree = static_cast<int>(std::max(2.0, std::min({std::ceil(need), cap, static_cast<double>(kMaxDegree)})));
+      solver.filter(prec, A, B, degree, lower, cut, upper);
+      solver.orthonormalize(prec, A, B, prec == 64 ? 1 : 2);
+      solver.rayleigh_ritz(prec, A, B, W, theta, res);
+      ++it;
+    }
+  };
+
+  bool reached = false;
+  {
+    // FP32 phase
+    DeviceBuffer a32(static_cast<size_t>(n) * nb * 4), b32(static_cast<size_t>(n) * nb * 4),
+        w32(static_cast<size_t>(n) * nb * 4);
+    void* A = a32.get();
+    void* B = b32.get();
+    solver.import_columns(32, cols.as<double>(), A);
+    solver.orthonormalize(32, A, B, 2);
+    solver.rayleigh_ritz(32, A, B, w32.get(), theta, res);
+    phase(32, A, B, w32.get(), std::max(kFilterHandover, o.tolerance), iterations[0]);
+    // FP64 phase seeded with the FP32 block
+    DeviceBuffer a64(static_cast<size_t>(n) * nb * 8), b64(static_cast<size_t>(n) * nb * 8);
+    ops.convert(A, 32, a64.get(), 64, static_cast<uint64_t>(n) * nb);
+    a32.release();
+    b32.release();
+    w32.release();
+    cols.release();
+    DeviceBuffer w64(static_cast<size_t>(n) * nb * 8);
+    void* A64 = a64.get();
+    void* B64 = b64.get();
+    solver.orthonormalize(64, A64, B64, 2);
+    solver.rayleigh_ritz(64, A64, B64, w64.get(), theta, res);
+    reached = phase(64, A64, B64, w64.get(), o.tolerance, iterations[1]);
+    const size_t total = static_cast<size_t>(iterations[0] + iterations[1]);
+    if (!reached) {
+      double worst = 0.0;
+      for (int i = 0; i < k; ++i) worst = std::max(worst, res[i]);
+      raise_nonconvergence(total, worst);
+    }
+    EigshResult r;
+    r.eigenvalues.assign(theta.begin(), theta.begin() + k);
+    r.residuals.assign(res.begin(), res.begin() + k);
+    r.iterations = total;
+    r.fp32_iterations = static_cast<size_t>(iterations[0]);
+    r.fp64_iterations = static_cast<size_t>(iterations[1]);
+    r.converged = true;
+    r.complex_vectors = false;
+    r.vectors.allocate(static_cast<size_t>(n) * k * sizeof(double));
+    solver.export_columns(64, A64, k, r.vectors.as<double>());
+    ops.sync();
+    r.operator_applications = solver.applications + bound_applications;
+    return r;
+  }
+}
+
+}  // namespace qmbed

@@ -544,6 +544,73 @@ __global__ void __launch_bounds__(256) spmv_wide_kernel(uint64_t n, const IDX* _
   }
 }
 
+// Block action in orbit-scaled coordinates on row-major blocks of NB columns.
+// With z = x / sqrt(R) the stored rows give (S^-1 H S z)_r = sum_k c_k z_col + d_r z_r,
+// so no orbit factor appears in the loop. Per row:
+//   out[r][:] = alpha * (sum_k table[code_k] z[col_k][:] + d_r z[r][:]) + beta * z[r][:] + gamma * p[r][:]
+// which is one step of a three-term (Chebyshev) recurrence. A row's NB values
+// are LPR consecutive 16-byte vectors, one per lane, so the gather of a column
+// is one contiguous NB-element read shared by LPR lanes. `out` may alias `p`
+// (each row is read before it is written by the same lane), never `z`.
+template <typename T, typename IDX, int NB, bool HAS_P>
+__global__ void __launch_bounds__(256) spmm_packed_kernel(uint64_t n, const IDX* __restrict__ row_ptr,
+                                                          const uint32_t* __restrict__ entries, int col_bits,
+                                                          const double* __restrict__ code_values, int n_codes,
+                                                          const T* __restrict__ diag, const T* __restrict__ z,
+                                                          const T* p, T* out, T alpha, T beta, T gamma) {
+  constexpr int VEC = 16 / sizeof(T);
+  constexpr int LPR = NB / VEC;
+  static_assert(NB % VEC == 0 && 32 % LPR == 0, "block width must fill whole 16-byte lanes of a warp");
+  __shared__ T table[kMaxCodes];
+  for (int i = threadIdx.x; i < n_codes; i += blockDim.x) table[i] = static_cast<T>(code_values[i]);
+  __syncthreads();
+  const uint32_t col_mask = col_bits >= 32 ? 0xffffffffu : ((1u << col_bits) - 1u);
+  const int part = threadIdx.x % LPR;
+  const uint64_t group = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPR;
+  const uint64_t groups = static_cast<uint64_t>(gridDim.x) * blockDim.x / LPR;
+  constexpr int kBatch = 4;
+  for (uint64_t r = group; r < n; r += groups) {
+    const IDX begin = __ldcs(row_ptr + r), end = __ldcs(row_ptr + r + 1);
+    const T d = __ldcs(diag + r);
+    T self[VEC];
+    load16(z + r * NB + part * VEC, self);
+    T acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = 0;
+    for (IDX p0 = begin; p0 < end; p0 += kBatch) {
+      uint32_t e[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) e[u] = p0 + u < end ? __ldcs(entries + p0 + u) : 0u;
+      T g[kBatch][VEC];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        if (p0 + u < end) {
+          load16(z + static_cast<uint64_t>(e[u] & col_mask) * NB + part * VEC, g[u]);
+        } else {
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) g[u][v] = 0;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const T c = p0 + u < end ? table[e[u] >> col_bits] : static_cast<T>(0);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) acc[v] += c * g[u][v];
+      }
+    }
+    T o[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) o[v] = alpha * (acc[v] + d * self[v]) + beta * self[v];
+    if (HAS_P) {
+      T q[VEC];
+      load16_rw(p + r * NB + part * VEC, q);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) o[v] += gamma * q[v];
+    }
+    store16(out + r * NB + part * VEC, o);
+  }
+}
+
 // xs = x / sqrt(R) elementwise (complex vectors scale both parts).
 template <typename T>
 __global__ void scale_by_orbit_kernel(uint64_t n, int comps, const uint16_t* __restrict__ orbits,
@@ -1042,6 +1109,43 @@ void SpinOperator::apply_with_scratch(int precision, bool complex_vectors, const
   };
   if (precision == kFP64) row_ptr64_ ? launch(double{}, uint64_t{}) : launch(double{}, uint32_t{});
   else row_ptr64_ ? launch(float{}, uint64_t{}) : launch(float{}, uint32_t{});
+  QMBED_LAUNCH_CHECK();
+}
+
+bool SpinOperator::supports_block() const { return real_ && storage_ == kStoragePacked; }
+
+void SpinOperator::apply_block(int precision, int nb, const void* z, const void* p, void* out, double alpha,
+                               double beta, double gamma, cudaStream_t stream) const {
+  QMBED_CUDA(cudaSetDevice(basis_->device()));
+  if (!supports_block()) raise(QMBED_UNSUPPORTED_BACKEND, "block action needs real packed rows");
+  const uint64_t n = dim();
+  if (n == 0) return;
+  auto launch = [&](auto ttag, auto itag, auto nbtag, auto ptag) {
+    using T = decltype(ttag);
+    using I = decltype(itag);
+    constexpr int NB = decltype(nbtag)::value;
+    constexpr bool HP = decltype(ptag)::value;
+    constexpr int LPR = NB / (16 / static_cast<int>(sizeof(T)));
+    const T* diag = precision == kFP64 ? reinterpret_cast<const T*>(diag64_.get()) : reinterpret_cast<const T*>(diag32_.get());
+    const int grid = grid_for(n * LPR, 256, 8);
+    spmm_packed_kernel<T, I, NB, HP><<<grid, 256, 0, stream>>>(
+        n, row_ptr_.as<I>(), entries_.as<uint32_t>(), col_bits_, code_table_.as<double>(), n_codes_, diag,
+        static_cast<const T*>(z), static_cast<const T*>(p), static_cast<T*>(out), static_cast<T>(alpha),
+        static_cast<T>(beta), static_cast<T>(gamma));
+  };
+  using NB8 = std::integral_constant<int, 8>;
+  using NB16 = std::integral_constant<int, 16>;
+  auto by_p = [&](auto ttag, auto itag, auto nbtag) {
+    if (p) launch(ttag, itag, nbtag, std::true_type{});
+    else launch(ttag, itag, nbtag, std::false_type{});
+  };
+  auto by_nb = [&](auto ttag, auto itag) {
+    if (nb == 8) by_p(ttag, itag, NB8{});
+    else if (nb == 16) by_p(ttag, itag, NB16{});
+    else raise(QMBED_INVALID_OPTIONS, "block width must be 8 or 16");
+  };
+  if (precision == kFP64) row_ptr64_ ? by_nb(double{}, uint64_t{}) : by_nb(double{}, uint32_t{});
+  else row_ptr64_ ? by_nb(float{}, uint64_t{}) : by_nb(float{}, uint32_t{});
   QMBED_LAUNCH_CHECK();
 }
 

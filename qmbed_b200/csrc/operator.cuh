@@ -82,6 +82,14 @@ class SpinOperator {
   void apply_with_scratch(int precision, bool complex_vectors, const void* x, void* y, cudaStream_t stream,
                           void* scratch, size_t scratch_bytes) const;
 
+  // Block action in orbit-scaled coordinates z = x / sqrt(R) on row-major
+  // n x nb blocks (nb = 8 or 16, precision 64/32):
+  //   out = alpha * (S^-1 H S) z + beta * z + gamma * p     (p may be null; out may alias p, not z)
+  // Available for real operators with packed rows (supports_block()).
+  bool supports_block() const;
+  void apply_block(int precision, int nb, const void* z, const void* p, void* out, double alpha, double beta,
+                   double gamma, cudaStream_t stream) const;
+
   // Dense Hermitian check of the assembled operator at tolerance 1e-12
   // (OperatorBuilder::build + is_hermitian, src/operator/mod.rs:2212).
   bool check_hermitian() const;

@@ -22,7 +22,7 @@ TARGETS = {
     "both_ends": 4,
     "shift": 5,
 }
-MODES = {"fp64": 0, "mixed": 1}
+MODES = {"fp64": 0, "mixed": 1, "filtered": 2}
 STORAGE = {"matrix_free": 0, "packed": 1}
 
 
@@ -187,6 +187,17 @@ class GpuOperator:
         check(lib().qmbed_gpu_operator_apply_device(self.handle, precision, int(complex_vectors), _ptr(x), _ptr(y),
                                                     None if stream is None else ctypes.c_void_p(stream),
                                                     int(force_matrix_free)))
+
+    def apply_block_device(self, z, out, nb: int, precision: int = 64, alpha: float = 1.0, beta: float = 0.0,
+                           gamma: float = 0.0, p=None, stream=None) -> None:
+        """out = alpha (S^-1 H S) z + beta z + gamma p on row-major n x nb device blocks.
+
+        Coordinates are orbit-scaled (z = x / sqrt(R) in symmetry sectors); real
+        operators with packed storage only.
+        """
+        check(lib().qmbed_gpu_operator_apply_block_device(self.handle, precision, nb, _ptr(z), _ptr(p), _ptr(out),
+                                                          alpha, beta, gamma,
+                                                          None if stream is None else ctypes.c_void_p(stream)))
 
     def apply_device_noalloc(self, x, y, precision: int = 64, complex_vectors: bool = False, stream=None) -> None:
         """y = H x on device tensors without any device allocation by the library.

@@ -219,6 +219,9 @@ def test_eigsh_l18_anchor(engine, oracle, anchors):
     (20, 10, 0, None, None, 4, "mixed"),
     (16, 8, 0, 1, 40, 4, "mixed"),
     (16, 8, 3, None, 24, 3, "mixed"),
+    (20, 10, 0, None, None, 4, "filtered"),  # block Chebyshev filter
+    (16, 8, 0, 1, 40, 4, "filtered"),        # below the block method's size: mixed Lanczos
+    (16, 8, 3, None, 24, 3, "filtered"),     # complex sector: mixed Lanczos
 ])
 def test_eigsh_matches_oracle(engine, oracle, sites, up, momentum, parity, krylov, k, mode):
     terms = oracle.heisenberg_terms(sites, delta=0.95)
@@ -237,8 +240,81 @@ def test_eigsh_matches_oracle(engine, oracle, sites, up, momentum, parity, krylo
         assert abs(np.linalg.norm(x) - 1.0) < 1e-10
     if mode == "fp64" and krylov is None:
         assert r.iterations == ro.iterations
-    if mode == "mixed":
+    if mode in ("mixed", "filtered"):
         assert r.fp32_iterations > 0
+
+
+@pytest.mark.parametrize("sites,up,momentum,parity,k,delta", [
+    (20, 10, 0, 1, 4, 1.0),       # symmetry sector: weighted block coordinates, 8-wide block
+    (18, 9, None, None, 4, 0.8),  # no symmetry: unit weights
+    (20, 10, 0, None, 7, 0.7),    # 16-wide block
+    (22, 11, 11, -1, 2, 1.2),     # k = pi sector
+])
+def test_filtered_eigsh_matches_oracle(engine, oracle, sites, up, momentum, parity, k, delta):
+    terms = oracle.heisenberg_terms(sites, delta=delta)
+    o = oracle.Operator.build(oracle.Basis(sites, up=up, momentum=momentum, parity=parity), terms)
+    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity), terms)
+    ro = o.eigsh(k, tolerance=1e-12, seed=3)
+    r = g.eigsh(k, tolerance=1e-10, seed=3, mode="filtered", eigenvectors=True)
+    # the block method ran (it makes no Gram-Schmidt passes) in both precisions
+    assert r.reorthogonalization_passes == 0
+    assert r.fp32_iterations > 0 and r.fp64_iterations > 0
+    assert _rel(r.eigenvalues, ro.eigenvalues) <= 1e-10
+    for value, vector, residual in zip(r.eigenvalues, r.eigenvectors, r.residuals):
+        x = vector.real
+        assert np.max(np.abs(vector.imag)) == 0.0
+        true_residual = np.linalg.norm(g.apply(x) - value * x)
+        assert true_residual <= 1e-10 * max(abs(value), 1.0) * 1.5
+        assert abs(true_residual - residual) <= 1e-12 * max(abs(value), 1.0)
+        assert abs(np.linalg.norm(x) - 1.0) < 1e-10
+    again = g.eigsh(k, tolerance=1e-10, seed=3, mode="filtered")
+    assert np.array_equal(again.eigenvalues, r.eigenvalues)  # bitwise reproducible
+
+
+def test_filtered_eigsh_warm_start(engine, oracle):
+    terms = oracle.heisenberg_terms(20, delta=0.9)
+    g = engine.GpuOperator(engine.GpuBasis(20, up=10, momentum=0, parity=1), terms)
+    first = g.eigsh(3, tolerance=1e-10, seed=8, mode="filtered", eigenvectors=True)
+    second = g.eigsh(3, tolerance=1e-10, seed=8, mode="filtered", initial=first.eigenvectors)
+    assert 2 * second.operator_applications < first.operator_applications
+    np.testing.assert_allclose(second.eigenvalues, first.eigenvalues, rtol=1e-12)
+
+
+@pytest.mark.parametrize("sites,up,momentum,parity,nb,precision", [
+    (16, 8, 0, 1, 8, 64), (16, 8, 0, 1, 16, 64), (16, 8, 0, 1, 8, 32), (14, 7, None, None, 16, 32),
+    (18, 9, 9, 1, 8, 64),
+])
+def test_block_action_matches_columnwise_apply(engine, oracle, sites, up, momentum, parity, nb, precision):
+    import torch
+    terms = oracle.heisenberg_terms(sites, delta=0.85)
+    ob = oracle.Basis(sites, up=up, momentum=momentum, parity=parity)
+    o = oracle.Operator.build(ob, terms)
+    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity), terms)
+    n = g.dim
+    _, orbits = ob.states()
+    s = np.sqrt(np.asarray(orbits, np.float64)) if momentum is not None or parity is not None else np.ones(n)
+    rng = np.random.default_rng(5)
+    z, p = rng.standard_normal((n, nb)), rng.standard_normal((n, nb))
+    alpha, beta, gamma = 0.7, -0.3, 0.45
+    expected = np.empty((n, nb))
+    for j in range(nb):
+        hx = o.apply(s * z[:, j]).real
+        expected[:, j] = alpha * hx / s + beta * z[:, j] + gamma * p[:, j]
+    dtype = torch.float64 if precision == 64 else torch.float32
+    zd = torch.tensor(z, dtype=dtype, device="cuda").contiguous()
+    pd = torch.tensor(p, dtype=dtype, device="cuda").contiguous()
+    g.apply_block_device(zd, pd, nb, precision=precision, alpha=alpha, beta=beta, gamma=gamma, p=pd)
+    torch.cuda.synchronize()
+    got = pd.double().cpu().numpy()
+    err = np.linalg.norm(got - expected) / np.linalg.norm(expected)
+    assert err <= (1e-14 if precision == 64 else 1e-6)
+    # without the third term
+    out = torch.empty_like(zd)
+    g.apply_block_device(zd, out, nb, precision=precision, alpha=1.0, beta=0.0)
+    torch.cuda.synchronize()
+    ref = np.stack([o.apply(s * z[:, j]).real / s for j in range(nb)], axis=1)
+    err = np.linalg.norm(out.double().cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err <= (1e-14 if precision == 64 else 1e-6)
 
 
 def test_eigsh_initial_subspace_warm_start(engine, oracle):
