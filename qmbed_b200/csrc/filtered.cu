@@ -24,7 +24,10 @@
 // (src/solve/mod.rs:1255, 1863), with r = ||H x - lambda x|| for ||x|| = 1.
 // The small symmetric eigenproblems run on the GPU (device Jacobi).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <limits>
 #include <numeric>
 #include <type_traits>
@@ -407,6 +410,7 @@ class BlockSolver {
 struct Bounds {
   std::vector<double> theta;  // ascending Ritz values
   double beta = 0.0;          // last Lanczos beta
+  double top_residual = 0.0;  // ||H y - theta_max y|| of the top Ritz pair
   int steps = 0;
 };
 
@@ -448,7 +452,9 @@ Bounds lanczos_bounds(const LinearOperatorView& op, BlockOps& ops, const double*
     if (i + 1 < size) T[static_cast<size_t>(i) * size + i + 1] = T[static_cast<size_t>(i + 1) * size + i] = beta[i];
   }
   symmetric_eigen(size, T, vals, vecs, ops.stream());
-  return Bounds{vals, beta.back(), size};
+  // residual norm of the top Ritz pair: |beta_m| times the last component of its vector
+  const double top_residual = std::fabs(beta.back() * vecs[static_cast<size_t>(size - 1) * size + (size - 1)]);
+  return Bounds{vals, beta.back(), top_residual, size};
 }
 
 }  // namespace
@@ -467,20 +473,38 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
 
   // Start columns: the caller's vectors (real parts), then reference
   // deterministic starts with seeds o.seed + j * 0x9e3779b9.
-  DeviceBuffer cols(static_cast<size_t>(n) * nb * sizeof(double));
-  auto col = [&](int j) { return cols.as<double>() + static_cast<size_t>(j) * n; };
+  // Workspace slots of the handle: 0 start columns, 1-3 FP32 blocks, 4-6 FP64 blocks.
+  const size_t block32 = static_cast<size_t>(n) * nb * 4, block64 = static_cast<size_t>(n) * nb * 8;
+  double* cols = static_cast<double*>(ops.workspace(0, block64));
+  auto col = [&](int j) { return cols + static_cast<size_t>(j) * n; };
   const int used = std::min(n_initial, nb);
   for (int j = 0; j < used; ++j) ops.import_complex(staged_initial + 2 * static_cast<size_t>(j) * n, col(j), n, 64, false);
   for (int j = used; j < nb; ++j) ops.lcg_start(col(j), n, o.seed + static_cast<uint64_t>(j - used) * 0x9e3779b9ULL, 64, false);
 
+  // QMBED_FILTER_TRACE=1 prints one line per outer iteration to stderr
+  const char* trace_env = std::getenv("QMBED_FILTER_TRACE");
+  const bool trace = trace_env && trace_env[0] == '1';
+  const auto started = std::chrono::steady_clock::now();
+  auto stamp = [&](const char* what) {
+    if (!trace) return;
+    ops.sync();
+    std::fprintf(stderr, "[filter] %s at %.1f ms\n", what,
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - started).count());
+  };
   size_t bound_applications = 0;
   const Bounds bd = lanczos_bounds(op, ops, col(0), bound_applications);
-  const double upper = bd.theta.back() + bd.beta;
+  // Upper end of the damped interval: the top Ritz value plus its residual
+  // norm and 1% of the Ritz range. Components a little above it grow only
+  // like exp(d sqrt(2 delta)), far below the amplification of the wanted end.
+  const double upper = bd.theta.back() + bd.top_residual + 0.01 * (bd.theta.back() - bd.theta.front());
   double lower = bd.theta.front();
-  double cut = bd.theta[std::min<size_t>(nb, bd.theta.size()) - 1];
+  // First cut: the k-th Ritz value, which lies at or above the k-th eigenvalue.
+  double cut = bd.theta[std::min<size_t>(k, bd.theta.size()) - 1];
+  if (!(cut > lower)) cut = lower + 0.1 * (upper - lower);
 
   std::vector<double> theta, res;
   int iterations[2] = {0, 0};
+  bool first_filter = true;
   auto rho = [&](double x, double c, double e) { return std::acosh(std::max((c - x) / e, 1.0)); };
 
   // One precision phase: filter, orthonormalise, Rayleigh-Ritz until every
@@ -505,7 +529,9 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
       }
       if (it >= kMaxOuter) return false;
       lower = std::min(lower, theta.front());
-      cut = theta.back();
+      // the first filter of a start block uses the Lanczos cut when it is lower
+      cut = first_filter ? std::min(theta.back(), cut) : theta.back();
+      first_filter = false;
       if (!(cut > theta.front())) cut = theta.front() + 1.0e-3 * (upper - theta.front());
       const double e = 0.5 * (upper - cut), c = 0.5 * (upper + cut);
       if (!(e > 0.0)) return false;
@@ -514,40 +540,49 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
         const double goal = 0.5 * target * std::max(std::fabs(theta[i]), 1.0);
         if (res[i] > goal) need = std::max(need, std::log(res[i] / goal) / std::max(rho(theta[i], c, e), 1.0e-3));
       }
-      const double spread = std::max(rho(theta.front(), c, e), 1.0e-3);
-      const double cap = std::log(prec == 64 ? 1.0e11 : 1.0e5) / spread;
+      const double spread = std::max(rho(lower, c, e), 1.0e-3);
+      // The block is orthonormalised through its Gram matrix: the weakest
+      // direction keeps accuracy eps * kappa (FP32 data) or eps * kappa^2 (FP64
+      // Gram of FP64 data), kappa ~ exp(degree * rho(theta_0)). Cap kappa.
+      const double cap = std::log(prec == 64 ? 1.0e6 : 1.0e5) / spread;
       const int degree = static_cast<int>(std::max(2.0, std::min({std::ceil(need), cap, static_cast<double>(kMaxDegree)})));
+      const auto t0 = std::chrono::steady_clock::now();
       solver.filter(prec, A, B, degree, lower, cut, upper);
       solver.orthonormalize(prec, A, B, prec == 64 ? 1 : 2);
       solver.rayleigh_ritz(prec, A, B, W, theta, res);
       ++it;
+      if (trace) {
+        double after = 0.0;
+        for (int i = 0; i < k; ++i) after = std::max(after, res[i] / std::max(std::fabs(theta[i]), 1.0));
+        std::fprintf(stderr, "[filter] fp%d it=%d degree=%d need=%.1f cap=%.1f lower=%.6f cut=%.6f upper=%.6f "
+                     "worst %.3e -> %.3e  %.1f ms\n", prec, it, degree, need, cap, lower, cut, upper, worst, after,
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+      }
     }
   };
 
   bool reached = false;
   {
     // FP32 phase
-    DeviceBuffer a32(static_cast<size_t>(n) * nb * 4), b32(static_cast<size_t>(n) * nb * 4),
-        w32(static_cast<size_t>(n) * nb * 4);
-    void* A = a32.get();
-    void* B = b32.get();
-    solver.import_columns(32, cols.as<double>(), A);
+    void* A = ops.workspace(1, block32);
+    void* B = ops.workspace(2, block32);
+    void* W = ops.workspace(3, block32);
+    stamp("bounds and start columns");
+    solver.import_columns(32, cols, A);
     solver.orthonormalize(32, A, B, 2);
-    solver.rayleigh_ritz(32, A, B, w32.get(), theta, res);
-    phase(32, A, B, w32.get(), std::max(kFilterHandover, o.tolerance), iterations[0]);
+    solver.rayleigh_ritz(32, A, B, W, theta, res);
+    stamp("fp32 start block");
+    phase(32, A, B, W, std::max(kFilterHandover, o.tolerance), iterations[0]);
     // FP64 phase seeded with the FP32 block
-    DeviceBuffer a64(static_cast<size_t>(n) * nb * 8), b64(static_cast<size_t>(n) * nb * 8);
-    ops.convert(A, 32, a64.get(), 64, static_cast<uint64_t>(n) * nb);
-    a32.release();
-    b32.release();
-    w32.release();
-    cols.release();
-    DeviceBuffer w64(static_cast<size_t>(n) * nb * 8);
-    void* A64 = a64.get();
-    void* B64 = b64.get();
+    void* A64 = ops.workspace(4, block64);
+    void* B64 = ops.workspace(5, block64);
+    void* W64 = ops.workspace(6, block64);
+    ops.convert(A, 32, A64, 64, static_cast<uint64_t>(n) * nb);
+    stamp("fp32 phase");
     solver.orthonormalize(64, A64, B64, 2);
-    solver.rayleigh_ritz(64, A64, B64, w64.get(), theta, res);
-    reached = phase(64, A64, B64, w64.get(), o.tolerance, iterations[1]);
+    solver.rayleigh_ritz(64, A64, B64, W64, theta, res);
+    stamp("fp64 start block");
+    reached = phase(64, A64, B64, W64, o.tolerance, iterations[1]);
     const size_t total = static_cast<size_t>(iterations[0] + iterations[1]);
     if (!reached) {
       double worst = 0.0;
@@ -565,6 +600,7 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
     r.vectors.allocate(static_cast<size_t>(n) * k * sizeof(double));
     solver.export_columns(64, A64, k, r.vectors.as<double>());
     ops.sync();
+    stamp("export");
     r.operator_applications = solver.applications + bound_applications;
     return r;
   }

@@ -602,6 +602,23 @@ BlockOps::~BlockOps() {
   if (host_results_) cudaFreeHost(host_results_);
 }
 
+void* BlockOps::workspace(int slot, size_t bytes) {
+  if (slot < 0 || slot > 64) raise(QMBED_INTERNAL_STATE, "workspace slot out of range");
+  if (workspace_.size() <= static_cast<size_t>(slot)) workspace_.resize(slot + 1);
+  DeviceBuffer& b = workspace_[slot];
+  if (b.bytes() < bytes) {
+    QMBED_CUDA(cudaStreamSynchronize(stream_));  // the old buffer may still be read by queued work
+    b.release();
+    b.allocate(bytes);
+  }
+  return b.get();
+}
+
+void BlockOps::release_workspace() {
+  QMBED_CUDA(cudaStreamSynchronize(stream_));
+  workspace_.clear();
+}
+
 void BlockOps::ensure_partials(size_t doubles) {
   if (partials_doubles_ < doubles) {
     partials_.allocate(doubles * sizeof(double));

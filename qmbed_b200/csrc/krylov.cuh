@@ -57,6 +57,12 @@ class BlockOps {
   double residual_norm(const void* y, const void* x, double lambda, uint64_t n, int precision, bool cplx);
   void sync();
 
+  // Device buffer `slot` of at least `bytes`, kept for later calls on this
+  // handle (grown, never shrunk) so that repeated solves reuse their blocks,
+  // like the reference EigshWorkspace (src/solve/mod.rs:477-526).
+  void* workspace(int slot, size_t bytes);
+  void release_workspace();
+
  private:
   void ensure_partials(size_t doubles);
   void ensure_coeffs(size_t bytes);
@@ -64,6 +70,7 @@ class BlockOps {
   cudaStream_t stream_;
   int sms_ = 148;
   DeviceBuffer partials_, results_, coeffs_;
+  std::vector<DeviceBuffer> workspace_;
   size_t partials_doubles_ = 0, coeffs_bytes_ = 0;
   double* host_results_ = nullptr;  // pinned
   size_t host_results_doubles_ = 0;
