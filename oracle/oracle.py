@@ -79,6 +79,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_expm_apply.argtypes = [vp, d, d, ll, d, ll, vp, vp]
         L.oracle_hermitian_eigen.argtypes = [ll, vp, vp, vp]
         L.oracle_tridiagonal_eigen.argtypes = [ll, vp, vp, vp, vp]
+        L.oracle_evolve.argtypes = [vp, vp, ll, vp, ll, d, ll, vp, vp]
+        L.oracle_expm_lanczos.argtypes = [vp, vp, d, ll, vp]
         _LIB = L
     return _LIB
 
@@ -273,6 +275,31 @@ class Operator:
         _check(lib().oracle_expm_apply(self.handle, coefficient.real, coefficient.imag, max_degree, tolerance,
                                        max_substeps, _ptr(x), _ptr(y)))
         return y
+
+    def evolve(self, initial, times, krylov_dimension: int = 30, tolerance: float = 1e-10,
+               max_substeps: int = 10_000):
+        """Adaptive Hermitian Krylov evolution exp(-i H t) v on a time grid.
+
+        Returns (states[n_times, dim], diagnostics dict) like
+        evolve_with_diagnostics (src/solve/mod.rs:3374-3406)."""
+        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        t = np.ascontiguousarray(np.asarray(times, np.float64))
+        states = np.zeros((len(t), self.dim), np.complex128)
+        diag = np.zeros(7)
+        _check(lib().oracle_evolve(self.handle, _ptr(x), len(t), _ptr(t), krylov_dimension, tolerance, max_substeps,
+                                   _ptr(states), _ptr(diag)))
+        return states, dict(zip(EVOLUTION_DIAGNOSTICS, [int(v) for v in diag[:6]] + [float(diag[6])]))
+
+    def expm_lanczos(self, initial, time: float, krylov_dimension: int = 30) -> np.ndarray:
+        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        y = np.zeros(self.dim, np.complex128)
+        _check(lib().oracle_expm_lanczos(self.handle, _ptr(x), time, krylov_dimension, _ptr(y)))
+        return y
+
+
+EVOLUTION_DIAGNOSTICS = ("lanczos_projections", "matrix_vector_products", "real_lanczos_projections",
+                         "real_matrix_vector_products", "accepted_substeps", "rejected_trial_intervals",
+                         "maximum_estimated_error")
 
 
 def deterministic_start(n: int, seed: int) -> np.ndarray:

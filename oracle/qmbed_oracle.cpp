@@ -1515,6 +1515,268 @@ std::vector<C64> expm_apply(const ExpmPlan& plan, const Operator& op, const std:
 }
 
 // ----------------------------------------------------------------------------
+// Hermitian Krylov exponential action and adaptive evolution
+// (src/solve/mod.rs:2909-3054 lanczos_projection(_real), 3056-3129 projected
+// exponential coefficients/action, 3131-3195 residual amplitude and error
+// bound, 3197-3316 evolve_hermitian_adaptive_grid, 3432-3454 expm_lanczos).
+// ----------------------------------------------------------------------------
+struct Projection {
+  double initial_norm = 0.0;
+  bool real = false;
+  std::vector<std::vector<double>> rbasis;
+  std::vector<std::vector<C64>> cbasis;
+  double residual_beta = 0.0;
+  std::vector<double> eigenvalues;
+  std::vector<double> eigenvectors;  // column-major size x size
+  size_t size() const { return real ? rbasis.size() : cbasis.size(); }
+  double vec(size_t row, size_t col) const { return eigenvectors[row + size() * col]; }
+};
+
+double cnorm(const std::vector<C64>& v) {
+  double s = 0.0;
+  for (const C64& x : v) s += std::norm(x);
+  return std::sqrt(s);
+}
+
+void finish_projection(Projection& p, const std::vector<double>& alphas, const std::vector<double>& betas) {
+  const size_t size = p.size();
+  std::vector<double> d(alphas.begin(), alphas.begin() + static_cast<long>(size));
+  std::vector<double> e(size > 0 ? size - 1 : 0);
+  for (size_t i = 0; i + 1 < size; ++i) e[i] = betas[i];
+  tridiagonal_eigen(size, d, e, p.eigenvalues, p.eigenvectors);
+}
+
+// lanczos_projection_real (src/solve/mod.rs:2985-3054)
+Projection lanczos_projection_real(const Operator& op, const std::vector<C64>& initial, size_t dimension) {
+  Projection p;
+  p.real = true;
+  double sq = 0.0;
+  for (const C64& x : initial) sq += x.real() * x.real();
+  p.initial_norm = std::sqrt(sq);
+  const size_t krylov = std::max<size_t>(std::min(dimension, initial.size()), 1);
+  std::vector<double> first(initial.size());
+  for (size_t i = 0; i < initial.size(); ++i) first[i] = initial[i].real() / p.initial_norm;
+  p.rbasis.push_back(first);
+  std::vector<double> alphas, betas, applied(initial.size());
+  for (size_t it = 0; it < krylov; ++it) {
+    op.apply_real(p.rbasis[it].data(), applied.data());
+    double alpha = 0.0;
+    for (size_t i = 0; i < applied.size(); ++i) alpha += p.rbasis[it][i] * applied[i];
+    alphas.push_back(alpha);
+    for (size_t i = 0; i < applied.size(); ++i) applied[i] -= alpha * p.rbasis[it][i];
+    if (it > 0)
+      for (size_t i = 0; i < applied.size(); ++i) applied[i] -= betas[it - 1] * p.rbasis[it - 1][i];
+    double bsq = 0.0;
+    for (double x : applied) bsq += x * x;
+    const double beta = std::sqrt(bsq);
+    p.residual_beta = beta;
+    if (it + 1 == krylov || beta <= 1.0e-14) break;
+    betas.push_back(beta);
+    for (double& x : applied) x /= beta;
+    p.rbasis.push_back(applied);
+  }
+  finish_projection(p, alphas, betas);
+  return p;
+}
+
+// lanczos_projection (src/solve/mod.rs:2909-2983)
+Projection lanczos_projection(const Operator& op, const std::vector<C64>& initial, size_t dimension) {
+  Projection p;
+  p.initial_norm = cnorm(initial);
+  if (p.initial_norm <= EPS) return p;
+  bool real_state = true;
+  for (const C64& x : initial) real_state = real_state && x.imag() == 0.0;
+  if (op.real && real_state) return lanczos_projection_real(op, initial, dimension);
+  const size_t krylov = std::max<size_t>(std::min(dimension, initial.size()), 1);
+  std::vector<C64> first = initial;
+  for (C64& x : first) x /= p.initial_norm;
+  p.cbasis.push_back(first);
+  std::vector<double> alphas, betas;
+  std::vector<C64> applied(initial.size());
+  for (size_t it = 0; it < krylov; ++it) {
+    op.apply(p.cbasis[it].data(), applied.data());
+    C64 alpha(0.0, 0.0);
+    for (size_t i = 0; i < applied.size(); ++i) alpha += std::conj(p.cbasis[it][i]) * applied[i];
+    if (std::fabs(alpha.imag()) > 1.0e-10) fail(ERR_NON_HERMITIAN, "");
+    alphas.push_back(alpha.real());
+    for (size_t i = 0; i < applied.size(); ++i) applied[i] -= alpha.real() * p.cbasis[it][i];
+    if (it > 0)
+      for (size_t i = 0; i < applied.size(); ++i) applied[i] -= betas[it - 1] * p.cbasis[it - 1][i];
+    const double beta = cnorm(applied);
+    p.residual_beta = beta;
+    if (it + 1 == krylov || beta <= 1.0e-14) break;
+    betas.push_back(beta);
+    for (C64& x : applied) x /= beta;
+    p.cbasis.push_back(applied);
+  }
+  finish_projection(p, alphas, betas);
+  return p;
+}
+
+// projected_exponential_coefficients (src/solve/mod.rs:3056-3075), Hamiltonian form
+std::vector<C64> projected_coefficients(const Projection& p, double interval) {
+  const size_t size = p.size();
+  std::vector<C64> c(size, C64(0.0, 0.0));
+  for (size_t e = 0; e < size; ++e) {
+    const C64 weight = p.initial_norm * p.vec(0, e) * std::exp(C64(0.0, -interval * p.eigenvalues[e]));
+    for (size_t b = 0; b < size; ++b) c[b] += p.vec(b, e) * weight;
+  }
+  return c;
+}
+
+// projected_exponential_action(_from_coefficients) (src/solve/mod.rs:3077-3129)
+std::vector<C64> projected_action(const Projection& p, double interval, size_t n) {
+  std::vector<C64> out(n, C64(0.0, 0.0));
+  if (p.size() == 0) return out;
+  const std::vector<C64> c = projected_coefficients(p, interval);
+  for (size_t b = 0; b < p.size(); ++b) {
+    if (p.real) {
+      for (size_t i = 0; i < n; ++i) out[i] += C64(c[b].real() * p.rbasis[b][i], c[b].imag() * p.rbasis[b][i]);
+    } else {
+      for (size_t i = 0; i < n; ++i) out[i] += c[b] * p.cbasis[b][i];
+    }
+  }
+  const double norm = cnorm(out);
+  if (norm > EPS && std::isfinite(norm)) {
+    const double scale = p.initial_norm / norm;
+    for (C64& x : out) x *= scale;
+  }
+  return out;
+}
+
+// projected_residual_amplitude (src/solve/mod.rs:3131-3144)
+double residual_amplitude(const Projection& p, double interval) {
+  if (p.size() == 0) return 0.0;
+  const size_t last = p.size() - 1;
+  C64 a(0.0, 0.0);
+  for (size_t e = 0; e < p.eigenvalues.size(); ++e)
+    a += p.initial_norm * p.vec(0, e) * p.vec(last, e) * std::exp(C64(0.0, -interval * p.eigenvalues[e]));
+  return std::abs(a);
+}
+
+// projected_exponential_error_bound (src/solve/mod.rs:3146-3195)
+double error_bound(const Projection& p, double interval, size_t n) {
+  const double duration = std::fabs(interval);
+  if (duration <= EPS || p.size() == 0 || p.size() == n || p.residual_beta <= 1.0e-14) return 0.0;
+  double lo = INFINITY, hi = -INFINITY;
+  for (double v : p.eigenvalues) {
+    lo = std::min(lo, v);
+    hi = std::max(hi, v);
+  }
+  const double span = duration * std::max(hi - lo, 0.0);
+  const size_t oscillations = static_cast<size_t>(std::min(std::ceil(span / M_PI), 60.0));
+  size_t intervals = std::min<size_t>(16 + 4 * oscillations, 256);
+  if (intervals % 2 != 0) ++intervals;
+  const double direction = interval > 0 ? 1.0 : (interval < 0 ? -1.0 : 0.0);
+  const double step = duration / static_cast<double>(intervals);
+  double integral = 0.0;
+  for (size_t i = 0; i <= intervals; ++i) {
+    const double w = (i == 0 || i == intervals) ? 1.0 : (i % 2 == 0 ? 2.0 : 4.0);
+    integral += w * residual_amplitude(p, direction * step * static_cast<double>(i));
+  }
+  return 1.25 * p.residual_beta * step * integral / 3.0;
+}
+
+struct EvolveDiagnostics {
+  double lanczos_projections = 0, matrix_vector_products = 0, real_lanczos_projections = 0,
+         real_matrix_vector_products = 0, accepted_substeps = 0, rejected_trial_intervals = 0,
+         maximum_estimated_error = 0;
+};
+
+// EvolutionOptions::validate (src/solve/mod.rs:2510-2530)
+void validate_evolution(const std::vector<double>& times, size_t krylov, double tolerance, size_t max_substeps) {
+  bool ok = !times.empty();
+  for (size_t i = 0; i < times.size(); ++i) {
+    ok = ok && std::isfinite(times[i]);
+    if (i > 0) ok = ok && !(times[i - 1] > times[i]);
+  }
+  if (!ok) fail(ERR_INVALID_OPTIONS, "times must be a nonempty finite nondecreasing grid");
+  if (krylov == 0 || !std::isfinite(tolerance) || tolerance <= 0.0 || max_substeps == 0)
+    fail(ERR_INVALID_OPTIONS, "evolution controls must be positive");
+}
+
+// evolve_hermitian_adaptive_grid (src/solve/mod.rs:3197-3316)
+std::vector<std::vector<C64>> evolve_adaptive(const Operator& op, const std::vector<C64>& initial,
+                                              const std::vector<double>& times, size_t krylov, double tolerance,
+                                              size_t max_substeps, EvolveDiagnostics& d) {
+  std::vector<std::vector<C64>> states;
+  std::vector<C64> current = initial;
+  double current_time = 0.0;
+  size_t output = 0, substeps = 0;
+  const double local_tolerance = tolerance / static_cast<double>(std::max<size_t>(times.size(), 1));
+  const size_t n = initial.size();
+  while (output < times.size()) {
+    const double target = times[output];
+    if (std::fabs(target - current_time) <= 16.0 * EPS * std::max(std::fabs(target), 1.0)) {
+      states.push_back(current);
+      current_time = target;
+      ++output;
+      continue;
+    }
+    if (substeps >= max_substeps) fail_nonconvergence(substeps, std::fabs(target - current_time));
+    const Projection p = lanczos_projection(op, current, krylov);
+    d.lanczos_projections += 1;
+    d.matrix_vector_products += static_cast<double>(p.size());
+    if (p.real) {
+      d.real_lanczos_projections += 1;
+      d.real_matrix_vector_products += static_cast<double>(p.size());
+    }
+    const double threshold = local_tolerance * std::max(cnorm(current), 1.0);
+    std::vector<std::pair<double, std::vector<C64>>> accepted;
+    for (size_t t = output; t < times.size(); ++t) {
+      const double interval = times[t] - current_time;
+      const double error = error_bound(p, interval, n);
+      d.maximum_estimated_error = std::max(d.maximum_estimated_error, error);
+      if (error > threshold) {
+        d.rejected_trial_intervals += 1;
+        break;
+      }
+      accepted.push_back({times[t], projected_action(p, interval, n)});
+    }
+    if (!accepted.empty()) {
+      for (auto& a : accepted) states.push_back(a.second);
+      current_time = accepted.back().first;
+      current = accepted.back().second;
+      output += accepted.size();
+      ++substeps;
+      d.accepted_substeps += 1;
+      continue;
+    }
+    const double target_interval = target - current_time;
+    const double direction = target_interval > 0 ? 1.0 : (target_interval < 0 ? -1.0 : 0.0);
+    const double minimum = 16.0 * EPS * std::max(std::fabs(target), 1.0);
+    double rejected = std::fabs(target_interval), accepted_mag = rejected;
+    for (;;) {
+      const double error = error_bound(p, direction * accepted_mag, n);
+      d.maximum_estimated_error = std::max(d.maximum_estimated_error, error);
+      if (error <= threshold || accepted_mag <= minimum) break;
+      d.rejected_trial_intervals += 1;
+      rejected = accepted_mag;
+      accepted_mag *= 0.5;
+    }
+    if (accepted_mag > minimum && rejected > accepted_mag) {
+      for (int i = 0; i < 8; ++i) {
+        const double trial = 0.5 * (accepted_mag + rejected);
+        const double error = error_bound(p, direction * trial, n);
+        d.maximum_estimated_error = std::max(d.maximum_estimated_error, error);
+        if (error <= threshold) {
+          accepted_mag = trial;
+        } else {
+          d.rejected_trial_intervals += 1;
+          rejected = trial;
+        }
+      }
+    }
+    const double interval = direction * accepted_mag;
+    current_time += interval;
+    current = projected_action(p, interval, n);
+    ++substeps;
+    d.accepted_substeps += 1;
+  }
+  return states;
+}
+
+// ----------------------------------------------------------------------------
 // C ABI used by the tests (ctypes).
 // ----------------------------------------------------------------------------
 thread_local std::string g_last_error;
@@ -1738,6 +2000,49 @@ int oracle_hermitian_eigen(long long n, const double* a, double* values, double*
     for (long long i = 0; i < n * n; ++i) {
       vectors[2 * i] = v[static_cast<size_t>(i)].real();
       vectors[2 * i + 1] = v[static_cast<size_t>(i)].imag();
+    }
+  });
+}
+
+// evolve (src/solve/mod.rs:3374-3406) with hamiltonian = true: `initial` and
+// each of the n_times output states are interleaved complex vectors.
+// diagnostics[7]: EvolutionDiagnostics fields in declaration order.
+int oracle_evolve(void* handle, const double* initial, long long n_times, const double* times, long long krylov,
+                  double tolerance, long long max_substeps, double* states, double* diagnostics) {
+  return guarded([&] {
+    const Operator& op = *static_cast<Operator*>(handle);
+    std::vector<double> grid(times, times + n_times);
+    validate_evolution(grid, static_cast<size_t>(std::max(krylov, 0LL)), tolerance,
+                       static_cast<size_t>(std::max(max_substeps, 0LL)));
+    std::vector<C64> v(op.rows);
+    for (size_t i = 0; i < op.rows; ++i) v[i] = C64(initial[2 * i], initial[2 * i + 1]);
+    EvolveDiagnostics d;
+    auto out = evolve_adaptive(op, v, grid, static_cast<size_t>(krylov), tolerance, static_cast<size_t>(max_substeps), d);
+    for (size_t t = 0; t < out.size(); ++t)
+      for (size_t i = 0; i < op.rows; ++i) {
+        states[2 * (t * op.rows + i)] = out[t][i].real();
+        states[2 * (t * op.rows + i) + 1] = out[t][i].imag();
+      }
+    const double fields[7] = {d.lanczos_projections, d.matrix_vector_products, d.real_lanczos_projections,
+                              d.real_matrix_vector_products, d.accepted_substeps, d.rejected_trial_intervals,
+                              d.maximum_estimated_error};
+    for (int i = 0; i < 7; ++i) diagnostics[i] = fields[i];
+  });
+}
+
+// expm_lanczos (src/solve/mod.rs:3432-3454): exp(-i t H) v from one projection.
+int oracle_expm_lanczos(void* handle, const double* initial, double time, long long krylov, double* out) {
+  return guarded([&] {
+    const Operator& op = *static_cast<Operator*>(handle);
+    if (krylov <= 0) fail(ERR_INVALID_OPTIONS, "Lanczos dimension and tolerance must be positive");
+    if (!std::isfinite(time)) fail(ERR_INVALID_OPTIONS, "exponential time must be finite");
+    std::vector<C64> v(op.rows);
+    for (size_t i = 0; i < op.rows; ++i) v[i] = C64(initial[2 * i], initial[2 * i + 1]);
+    const Projection p = lanczos_projection(op, v, static_cast<size_t>(krylov));
+    const std::vector<C64> r = projected_action(p, time, op.rows);
+    for (size_t i = 0; i < op.rows; ++i) {
+      out[2 * i] = r[i].real();
+      out[2 * i + 1] = r[i].imag();
     }
   });
 }

@@ -283,3 +283,56 @@ def test_all_formats_share_action(oracle):
     op = oracle.Operator.build(oracle.Basis(2), oracle.heisenberg_terms(2, periodic=False))
     x = np.array([1 - 0.5j, -2 + 0.25j, 0.75 + 1j, 0.5 - 1.5j])
     np.testing.assert_allclose(op.apply(x), op.dense() @ x, atol=1e-12)
+
+
+def _diagonal32():
+    return np.array([-2.0 + 4.0 * i / 31.0 for i in range(32)])
+
+
+def test_adaptive_evolution_anchor(oracle, anchors):
+    a = anchors["adaptive_evolution"]
+    values = _diagonal32()
+    op = oracle.Operator.diagonal(values)
+    initial = np.full(32, 1.0 / np.sqrt(32.0), complex)
+    states, d = op.evolve(initial, a["times"], krylov_dimension=a["krylov_dimension"], tolerance=a["tolerance"])
+    assert d["lanczos_projections"] > 1
+    assert d["matrix_vector_products"] == a["krylov_dimension"] * d["lanczos_projections"]
+    assert d["accepted_substeps"] == d["lanczos_projections"]
+    assert d["rejected_trial_intervals"] > 0
+    np.testing.assert_allclose(states[0], initial, atol=0)
+    expected = initial * np.exp(-1j * a["times"][2] * values)
+    assert np.max(np.abs(states[2] - expected)) < a["final_state_abs_tol"]
+
+
+def test_evolve_and_expm_lanczos_match_dense_exponential(oracle):
+    from scipy.linalg import expm
+    for sites, momentum, parity in ((10, 0, 1), (9, 2, None)):
+        basis = oracle.Basis(sites, up=sites // 2, momentum=momentum, parity=parity)
+        op = oracle.Operator.build(basis, oracle.heisenberg_terms(sites, delta=0.8))
+        n = op.dim
+        dense = np.zeros((n, n), complex)
+        for j in range(n):
+            e = np.zeros(n, complex)
+            e[j] = 1.0
+            dense[:, j] = op.apply(e)
+        rng = np.random.default_rng(sites)
+        v = rng.standard_normal(n) + (0.0 if op.is_real else 1j * rng.standard_normal(n))
+        v /= np.linalg.norm(v)
+        times = [0.0, 0.3, 0.3, 1.7, 4.0]
+        states, d = op.evolve(v, times, krylov_dimension=16, tolerance=1e-10)
+        for t, s in zip(times, states):
+            assert np.linalg.norm(s - expm(-1j * t * dense) @ v) <= 1e-9
+        assert d["accepted_substeps"] >= 1
+        w = op.expm_lanczos(v, 0.4, krylov_dimension=min(n, 40))
+        assert np.linalg.norm(w - expm(-0.4j * dense) @ v) <= 1e-10
+
+
+def test_evolution_option_errors(oracle):
+    from oracle.oracle import OracleError
+    op = oracle.Operator.diagonal(_diagonal32())
+    v = np.ones(32, complex)
+    for times, krylov, tol in (([], 8, 1e-10), ([1.0, 0.5], 8, 1e-10), ([np.inf], 8, 1e-10), ([1.0], 0, 1e-10),
+                               ([1.0], 8, 0.0)):
+        with pytest.raises(OracleError) as e:
+            op.evolve(v, times, krylov_dimension=krylov, tolerance=tol)
+        assert e.value.code == 8
