@@ -198,6 +198,20 @@ QMBED_API int qmbed_gpu_expm_apply_host(qmbed_operator op, double coef_re, doubl
                                         double tolerance, uint64_t max_substeps, int precision, const double* input,
                                         double* output, uint64_t n_vectors);
 
+/* evolve / evolve_with_diagnostics with hamiltonian = true (src/solve/mod.rs:
+ * 3197-3316, 3374-3406): exp(-i H t) initial at each of n_times nondecreasing
+ * times by adaptive Lanczos projections without reorthogonalisation. initial
+ * is one host vector (interleaved complex); states receives n_times vectors.
+ * diagnostics (may be NULL) receives the 7 EvolutionDiagnostics fields in
+ * declaration order (src/solve/mod.rs:2546-2555). */
+QMBED_API int qmbed_gpu_evolve(qmbed_operator op, const double* initial, int n_times, const double* times,
+                               uint64_t krylov_dimension, double tolerance, uint64_t max_substeps, double* states,
+                               double* diagnostics);
+/* expm_lanczos (src/solve/mod.rs:3432-3454): exp(-i H time) initial from one
+ * Lanczos projection of dimension krylov_dimension; host vectors. */
+QMBED_API int qmbed_gpu_expm_lanczos(qmbed_operator op, const double* initial, double time,
+                                     uint64_t krylov_dimension, double* out);
+
 /* deterministic_start (src/solve/mod.rs:729-742): normalised LCG vector. */
 QMBED_API int qmbed_gpu_deterministic_start(int device, uint64_t n, uint64_t seed, double* out);
 

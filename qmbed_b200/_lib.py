@@ -108,6 +108,8 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_expm_plan.argtypes = [vp, d, d, u64, d, u64, P(u64), P(u64), vp, P(d)]
     L.qmbed_gpu_expm_apply_host.argtypes = [vp, d, d, u64, d, u64, i, vp, vp, u64]
     L.qmbed_gpu_deterministic_start.argtypes = [i, u64, u64, vp]
+    L.qmbed_gpu_evolve.argtypes = [vp, vp, i, vp, u64, d, u64, vp, vp]
+    L.qmbed_gpu_expm_lanczos.argtypes = [vp, vp, d, u64, vp]
     for name in ("qmbed_run_json", "qmbed_command_json"):
         getattr(L, name).argtypes = [ctypes.c_char_p]
         getattr(L, name).restype = ctypes.c_void_p

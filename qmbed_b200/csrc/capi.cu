@@ -16,6 +16,7 @@
 
 #include "../../include/qmbed_b200.h"
 #include "eigsh.cuh"
+#include "evolve.cuh"
 #include "expm.cuh"
 #include "json.hpp"
 #include "operator.cuh"
@@ -656,6 +657,55 @@ Value command(const Value& request) {
     out.set("vectors", std::move(vs));
     return out;
   }
+  if (operation == "evolve_model") {
+    // command_evolve_model (bindings/capi/src/lib.rs:4673-4694), EvolutionRequest
+    // defaults 64 / 1e-10 / 10000 (lib.rs:431-441, 596-606)
+    auto model = registered_model(request.at("handle").as_string());
+    const Value& ev = request.at("evolution");
+    if (ev.has("imaginary_time") && ev.at("imaginary_time").as_bool())
+      raise(QMBED_INVALID_OPTIONS, "static imaginary-time evolution is not exposed by this command yet");
+    EvolutionOptions o;
+    for (const Value& t : ev.at("times").items()) o.times.push_back(t.as_double());
+    o.krylov_dimension = ev.has("krylov_dimension") ? static_cast<size_t>(ev.at("krylov_dimension").as_int()) : 64;
+    o.tolerance = ev.has("tolerance") ? ev.at("tolerance").as_double() : 1.0e-10;
+    o.max_substeps = ev.has("max_substeps") ? static_cast<size_t>(ev.at("max_substeps").as_int()) : 10000;
+    auto vectors = parse_vectors(request.at("vectors"));
+    if (vectors.empty()) raise(QMBED_INVALID_OPTIONS, "a state batch must contain at least one column");
+    auto op = model->materialize(request.find("parameters"), kStoragePacked, true);
+    qmbed_operator_s& h = *op;
+    std::lock_guard<std::mutex> lock(h.mu);
+    const uint64_t dim = h.op->dim();
+    std::vector<std::vector<double>> per_column;
+    for (const auto& v : vectors) {
+      if (v.size() != dim) raise(QMBED_DIMENSION_MISMATCH, "evolution operator and initial state do not match");
+      std::vector<double> host(2 * dim), states(2 * dim * o.times.size());
+      for (uint64_t i = 0; i < dim; ++i) {
+        host[2 * i] = v[i].real();
+        host[2 * i + 1] = v[i].imag();
+      }
+      EvolutionDiagnostics d;
+      evolve(h.view(), host.data(), o, states.data(), d, h.block_ops());
+      per_column.push_back(std::move(states));
+    }
+    Value out = Value::object();
+    out.set("kind", Value::string("trajectory"));
+    out.set("dimension", Value::integer(static_cast<long long>(dim)));
+    Value times = Value::array();
+    for (double t : o.times) times.push(Value::number(t));
+    out.set("times", std::move(times));
+    Value states = Value::array();
+    for (size_t t = 0; t < o.times.size(); ++t) {
+      Value columns = Value::array();
+      for (const auto& col : per_column) {
+        Value r = Value::array();
+        for (uint64_t i = 0; i < dim; ++i) r.push(complex_pair(C64(col[2 * (t * dim + i)], col[2 * (t * dim + i) + 1])));
+        columns.push(std::move(r));
+      }
+      states.push(std::move(columns));
+    }
+    out.set("states", std::move(states));
+    return out;
+  }
   if (operation == "release_model") {
     const std::string text = request.at("handle").as_string();
     const uint64_t id = parse_handle(text, "model");
@@ -943,6 +993,40 @@ int qmbed_gpu_expm_apply_host(qmbed_operator op, double coef_re, double coef_im,
       QMBED_CUDA(cudaMemcpyAsync(output + 2 * k * n, state64.get(), n * 16, cudaMemcpyDeviceToHost, ops.stream()));
       ops.sync();
     }
+  });
+}
+
+int qmbed_gpu_evolve(qmbed_operator op, const double* initial, int n_times, const double* times,
+                     uint64_t krylov_dimension, double tolerance, uint64_t max_substeps, double* states,
+                     double* diagnostics) {
+  return guarded([&] {
+    if (!initial || !states || n_times < 0 || (n_times > 0 && !times))
+      raise(QMBED_INVALID_OPTIONS, "evolution needs an initial state, a time grid and an output array");
+    std::lock_guard<std::mutex> lock(op->mu);
+    EvolutionOptions o;
+    o.times.assign(times, times + n_times);
+    o.krylov_dimension = krylov_dimension;
+    o.tolerance = tolerance;
+    o.max_substeps = max_substeps;
+    EvolutionDiagnostics d;
+    evolve(op->view(), initial, o, states, d, op->block_ops());
+    if (diagnostics) {
+      const double fields[7] = {static_cast<double>(d.lanczos_projections), static_cast<double>(d.matrix_vector_products),
+                                static_cast<double>(d.real_lanczos_projections),
+                                static_cast<double>(d.real_matrix_vector_products),
+                                static_cast<double>(d.accepted_substeps), static_cast<double>(d.rejected_trial_intervals),
+                                d.maximum_estimated_error};
+      for (int i = 0; i < 7; ++i) diagnostics[i] = fields[i];
+    }
+  });
+}
+
+int qmbed_gpu_expm_lanczos(qmbed_operator op, const double* initial, double time, uint64_t krylov_dimension,
+                           double* out) {
+  return guarded([&] {
+    if (!initial || !out) raise(QMBED_INVALID_OPTIONS, "expm_lanczos needs input and output vectors");
+    std::lock_guard<std::mutex> lock(op->mu);
+    expm_lanczos(op->view(), initial, time, krylov_dimension, out, op->block_ops());
   });
 }
 

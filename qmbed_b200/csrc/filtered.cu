@@ -6,10 +6,13 @@
 // by an orthonormalisation of the block through the eigen-decomposition of its
 // Gram matrix and a Rayleigh-Ritz step. The filter interval [cut, upper] is
 // damped, everything below `cut` is amplified. `upper` comes from a short
-// Lanczos run (largest Ritz value plus the last beta, the bound estimator of
-// Zhou and Li, Linear Algebra Appl. 435, 2011); `cut` is the largest Ritz
-// value of the block (by interlacing it lies at or above the block's share of
-// the spectrum).
+// Lanczos run: the largest Ritz value plus the residual norm of its Ritz pair
+// and 1% of the Ritz range (after the bound estimators of Zhou and Li, Linear
+// Algebra Appl. 435, 2011); `cut` is the largest Ritz value of the block (by
+// interlacing it lies at or above the block's share of the spectrum). The
+// filter degree per outer iteration follows the estimated convergence rate
+// acosh((c - theta_i) / e) of the slowest wanted pair, capped so that the
+// Gram-based orthonormalisation keeps the weakest block direction.
 //
 // All block work happens in the orbit-scaled coordinates z = S^-1 x,
 // S = diag(sqrt(R)): the packed rows then need no orbit factor, inner products
@@ -233,33 +236,6 @@ void dispatch_block(int prec, int nb, F&& f) {
   }
 }
 
-// Ascending eigenpairs of a real symmetric m x m matrix (row-major, symmetrised
-// here) on the device; V row-major with eigenvectors as columns.
-void symmetric_eigen(int m, const std::vector<double>& a, std::vector<double>& values, std::vector<double>& V,
-                     cudaStream_t stream) {
-  std::vector<C64> ac(static_cast<size_t>(m) * m);
-  for (int i = 0; i < m; ++i)
-    for (int j = 0; j < m; ++j) ac[static_cast<size_t>(i) * m + j] = C64(0.5 * (a[i * m + j] + a[j * m + i]), 0.0);
-  std::vector<double> vals;
-  std::vector<C64> vecs;
-  device_hermitian_eigen(m, ac, vals, vecs, stream);
-  std::vector<int> order(m);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int l, int r) { return vals[l] < vals[r]; });
-  values.assign(m, 0.0);
-  V.assign(static_cast<size_t>(m) * m, 0.0);
-  for (int q = 0; q < m; ++q) {
-    const int col = order[q];
-    values[q] = vals[col];
-    // eigenvectors of a real matrix are real up to one phase: remove it
-    C64 big(0.0, 0.0);
-    for (int i = 0; i < m; ++i)
-      if (std::abs(vecs[static_cast<size_t>(col) * m + i]) > std::abs(big)) big = vecs[static_cast<size_t>(col) * m + i];
-    const C64 phase = std::abs(big) > 0.0 ? std::conj(big) / std::abs(big) : C64(1.0, 0.0);
-    for (int i = 0; i < m; ++i) V[static_cast<size_t>(i) * m + q] = (vecs[static_cast<size_t>(col) * m + i] * phase).real();
-  }
-}
-
 class BlockSolver {
  public:
   BlockSolver(const LinearOperatorView& op, const EigshOptions& o, BlockOps& ops, int nb)
@@ -323,7 +299,7 @@ class BlockSolver {
   void orthonormalize(int prec, void*& A, void*& B, int passes) {
     for (int pass = 0; pass < passes; ++pass) {
       std::vector<double> G = gram(prec, A, A), mu, V;
-      symmetric_eigen(nb_, G, mu, V, ops_.stream());
+      device_symmetric_eigen(nb_, G, mu, V, ops_.stream());
       const double top = std::max(mu.back(), std::numeric_limits<double>::min());
       const double floor = top * (prec == 64 ? 1.0e-28 : 1.0e-14);
       std::vector<double> C(static_cast<size_t>(nb_) * nb_);
@@ -339,7 +315,7 @@ class BlockSolver {
   void rayleigh_ritz(int prec, void*& A, void*& B, void* W, std::vector<double>& theta, std::vector<double>& res) {
     act(prec, A, nullptr, W, 1.0, 0.0, 0.0);
     std::vector<double> Tm = gram(prec, A, W), Y;
-    symmetric_eigen(nb_, Tm, theta, Y, ops_.stream());
+    device_symmetric_eigen(nb_, Tm, theta, Y, ops_.stream());
     std::vector<double> r2 = rotate(prec, A, B, W, Y, theta, true);
     std::swap(A, B);
     res.assign(nb_, 0.0);
@@ -451,7 +427,7 @@ Bounds lanczos_bounds(const LinearOperatorView& op, BlockOps& ops, const double*
     T[static_cast<size_t>(i) * size + i] = alpha[i];
     if (i + 1 < size) T[static_cast<size_t>(i) * size + i + 1] = T[static_cast<size_t>(i + 1) * size + i] = beta[i];
   }
-  symmetric_eigen(size, T, vals, vecs, ops.stream());
+  device_symmetric_eigen(size, T, vals, vecs, ops.stream());
   // residual norm of the top Ritz pair: |beta_m| times the last component of its vector
   const double top_residual = std::fabs(beta.back() * vecs[static_cast<size_t>(size - 1) * size + (size - 1)]);
   return Bounds{vals, beta.back(), top_residual, size};
@@ -561,49 +537,60 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
     }
   };
 
-  bool reached = false;
-  {
+  void* A64 = ops.workspace(4, block64);
+  void* B64 = ops.workspace(5, block64);
+  void* W64 = ops.workspace(6, block64);
+  stamp("bounds and start columns");
+  // A caller's subspace is first judged in FP64 as given: when it already
+  // holds the wanted pairs to the FP32 level, the FP32 phase is skipped (and
+  // when it meets the tolerance, no filter step runs at all).
+  bool fp64_start = false;
+  if (used > 0) {
+    solver.import_columns(64, cols, A64);
+    solver.orthonormalize(64, A64, B64, 2);
+    solver.rayleigh_ritz(64, A64, B64, W64, theta, res);
+    double worst = 0.0;
+    for (int i = 0; i < k; ++i) worst = std::max(worst, res[i] / std::max(std::fabs(theta[i]), 1.0));
+    fp64_start = worst <= kFilterHandover;
+  }
+  if (!fp64_start) {
     // FP32 phase
     void* A = ops.workspace(1, block32);
     void* B = ops.workspace(2, block32);
     void* W = ops.workspace(3, block32);
-    stamp("bounds and start columns");
     solver.import_columns(32, cols, A);
     solver.orthonormalize(32, A, B, 2);
     solver.rayleigh_ritz(32, A, B, W, theta, res);
     stamp("fp32 start block");
     phase(32, A, B, W, std::max(kFilterHandover, o.tolerance), iterations[0]);
     // FP64 phase seeded with the FP32 block
-    void* A64 = ops.workspace(4, block64);
-    void* B64 = ops.workspace(5, block64);
-    void* W64 = ops.workspace(6, block64);
     ops.convert(A, 32, A64, 64, static_cast<uint64_t>(n) * nb);
     stamp("fp32 phase");
     solver.orthonormalize(64, A64, B64, 2);
     solver.rayleigh_ritz(64, A64, B64, W64, theta, res);
     stamp("fp64 start block");
-    reached = phase(64, A64, B64, W64, o.tolerance, iterations[1]);
-    const size_t total = static_cast<size_t>(iterations[0] + iterations[1]);
-    if (!reached) {
-      double worst = 0.0;
-      for (int i = 0; i < k; ++i) worst = std::max(worst, res[i]);
-      raise_nonconvergence(total, worst);
-    }
-    EigshResult r;
-    r.eigenvalues.assign(theta.begin(), theta.begin() + k);
-    r.residuals.assign(res.begin(), res.begin() + k);
-    r.iterations = total;
-    r.fp32_iterations = static_cast<size_t>(iterations[0]);
-    r.fp64_iterations = static_cast<size_t>(iterations[1]);
-    r.converged = true;
-    r.complex_vectors = false;
-    r.vectors.allocate(static_cast<size_t>(n) * k * sizeof(double));
-    solver.export_columns(64, A64, k, r.vectors.as<double>());
-    ops.sync();
-    stamp("export");
-    r.operator_applications = solver.applications + bound_applications;
-    return r;
   }
+  const bool reached = phase(64, A64, B64, W64, o.tolerance, iterations[1]);
+  const size_t total = static_cast<size_t>(iterations[0] + iterations[1]);
+  if (!reached) {
+    double worst = 0.0;
+    for (int i = 0; i < k; ++i) worst = std::max(worst, res[i]);
+    raise_nonconvergence(total, worst);
+  }
+  EigshResult r;
+  r.eigenvalues.assign(theta.begin(), theta.begin() + k);
+  r.residuals.assign(res.begin(), res.begin() + k);
+  r.iterations = total;
+  r.fp32_iterations = static_cast<size_t>(iterations[0]);
+  r.fp64_iterations = static_cast<size_t>(iterations[1]);
+  r.converged = true;
+  r.complex_vectors = false;
+  r.vectors.allocate(static_cast<size_t>(n) * k * sizeof(double));
+  solver.export_columns(64, A64, k, r.vectors.as<double>());
+  ops.sync();
+  stamp("export");
+  r.operator_applications = solver.applications + bound_applications;
+  return r;
 }
 
 }  // namespace qmbed

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <numeric>
 
 #include "device_util.cuh"
 #include "krylov.cuh"
@@ -843,6 +844,33 @@ void device_hermitian_eigen(int n, const std::vector<C64>& a, std::vector<double
     for (int row = 0; row < n; ++row)
       vectors[static_cast<size_t>(col) * n + row] =
           C64(hv[2 * (static_cast<size_t>(col) * np + row)], hv[2 * (static_cast<size_t>(col) * np + row) + 1]);
+}
+
+// Ascending eigenpairs of a real symmetric m x m matrix (row-major, symmetrised
+// here) on the device; V row-major with eigenvectors as columns.
+void device_symmetric_eigen(int m, const std::vector<double>& a, std::vector<double>& values, std::vector<double>& V,
+                     cudaStream_t stream) {
+  std::vector<C64> ac(static_cast<size_t>(m) * m);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) ac[static_cast<size_t>(i) * m + j] = C64(0.5 * (a[i * m + j] + a[j * m + i]), 0.0);
+  std::vector<double> vals;
+  std::vector<C64> vecs;
+  device_hermitian_eigen(m, ac, vals, vecs, stream);
+  std::vector<int> order(m);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int l, int r) { return vals[l] < vals[r]; });
+  values.assign(m, 0.0);
+  V.assign(static_cast<size_t>(m) * m, 0.0);
+  for (int q = 0; q < m; ++q) {
+    const int col = order[q];
+    values[q] = vals[col];
+    // eigenvectors of a real matrix are real up to one phase: remove it
+    C64 big(0.0, 0.0);
+    for (int i = 0; i < m; ++i)
+      if (std::abs(vecs[static_cast<size_t>(col) * m + i]) > std::abs(big)) big = vecs[static_cast<size_t>(col) * m + i];
+    const C64 phase = std::abs(big) > 0.0 ? std::conj(big) / std::abs(big) : C64(1.0, 0.0);
+    for (int i = 0; i < m; ++i) V[static_cast<size_t>(i) * m + q] = (vecs[static_cast<size_t>(col) * m + i] * phase).real();
+  }
 }
 
 }  // namespace qmbed

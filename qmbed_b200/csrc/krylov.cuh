@@ -82,4 +82,10 @@ class BlockOps {
 void device_hermitian_eigen(int n, const std::vector<C64>& a, std::vector<double>& values, std::vector<C64>& vectors,
                             cudaStream_t stream);
 
+// Ascending eigenpairs of a real symmetric m x m matrix (row-major; the
+// symmetric part is used) by the same device Jacobi, with real eigenvectors
+// as the columns of V (row-major V[i * m + j]).
+void device_symmetric_eigen(int m, const std::vector<double>& a, std::vector<double>& values, std::vector<double>& V,
+                            cudaStream_t stream);
+
 }  // namespace qmbed

@@ -441,8 +441,21 @@ __global__ void __launch_bounds__(128) column_norm_kernel(OpView<S> v, const Ins
   }
 }
 
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+  using type = float2;
+};
+template <>
+struct Pair<double> {
+  using type = double2;
+};
+
 // y[r] = sqrt(R_r) * sum_k table[code_k] * xs[col_k] + d[r] * x[r]  (real operators).
-template <typename T, typename IDX, bool SCALED, int LANES>
+// With CPLX the vectors are interleaved complex and each gather reads the
+// (re, im) pair of a column as one 8/16-byte load.
+template <typename T, typename IDX, bool SCALED, int LANES, bool CPLX>
 __global__ void __launch_bounds__(256) spmv_packed_kernel(uint64_t n, const IDX* __restrict__ row_ptr,
                                                           const uint32_t* __restrict__ entries, int col_bits,
                                                           const double* __restrict__ code_values, int n_codes,
@@ -451,6 +464,7 @@ __global__ void __launch_bounds__(256) spmv_packed_kernel(uint64_t n, const IDX*
                                                           const double* __restrict__ sqrt_table,
                                                           const T* __restrict__ xs, const T* __restrict__ x,
                                                           T* __restrict__ y) {
+  using P2 = typename Pair<T>::type;
   __shared__ T table[kMaxCodes];
   __shared__ T sqrt_r[257];
   for (int i = threadIdx.x; i < n_codes; i += blockDim.x) table[i] = static_cast<T>(code_values[i]);
@@ -459,6 +473,8 @@ __global__ void __launch_bounds__(256) spmv_packed_kernel(uint64_t n, const IDX*
   __syncthreads();
   const uint32_t col_mask = col_bits >= 32 ? 0xffffffffu : ((1u << col_bits) - 1u);
   const int lane = threadIdx.x % LANES;
+  // the lanes of one row shuffle among themselves only
+  const unsigned group_mask = (LANES == 32 ? 0xffffffffu : ((1u << LANES) - 1u)) << ((threadIdx.x & 31) / LANES * LANES);
   const uint64_t group = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LANES;
   const uint64_t groups = static_cast<uint64_t>(gridDim.x) * blockDim.x / LANES;
   constexpr int kBatch = 4;  // entries per lane issued together: loads, then gathers, then FMAs
@@ -467,14 +483,20 @@ __global__ void __launch_bounds__(256) spmv_packed_kernel(uint64_t n, const IDX*
     // evict-first so the L2 keeps the gathered vector xs.
     const IDX begin = __ldcs(row_ptr + r), end = __ldcs(row_ptr + r + 1);
     // per-row operands requested before the entry loop so their latency overlaps it
-    T d = 0, xr = 0;
+    T d = 0, xr = 0, xi = 0;
     uint16_t orbit = 0;
     if (lane == 0) {
       d = __ldcs(diag + r);
-      xr = __ldcs(x + r);
+      if (CPLX) {
+        const P2 v = __ldcs(reinterpret_cast<const P2*>(x) + r);
+        xr = v.x;
+        xi = v.y;
+      } else {
+        xr = __ldcs(x + r);
+      }
       if (SCALED) orbit = __ldcs(orbits + r);
     }
-    T acc = 0;
+    T acc = 0, acc_i = 0;
     for (IDX p0 = begin + lane; p0 < end; p0 += LANES * kBatch) {
       uint32_t e[kBatch];
 #pragma unroll
@@ -482,18 +504,48 @@ __global__ void __launch_bounds__(256) spmv_packed_kernel(uint64_t n, const IDX*
         const IDX p = p0 + u * LANES;
         e[u] = p < end ? __ldcs(entries + p) : 0u;
       }
-      T g[kBatch];
+      if (CPLX) {
+        P2 g[kBatch];
 #pragma unroll
-      for (int u = 0; u < kBatch; ++u) g[u] = (p0 + u * LANES < end) ? xs[e[u] & col_mask] : static_cast<T>(0);
+        for (int u = 0; u < kBatch; ++u) {
+          if (p0 + u * LANES < end) {
+            g[u] = reinterpret_cast<const P2*>(xs)[e[u] & col_mask];
+          } else {
+            g[u].x = 0;
+            g[u].y = 0;
+          }
+        }
 #pragma unroll
-      for (int u = 0; u < kBatch; ++u)
-        if (p0 + u * LANES < end) acc += table[e[u] >> col_bits] * g[u];
+        for (int u = 0; u < kBatch; ++u)
+          if (p0 + u * LANES < end) {
+            const T c = table[e[u] >> col_bits];
+            acc += c * g[u].x;
+            acc_i += c * g[u].y;
+          }
+      } else {
+        T g[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) g[u] = (p0 + u * LANES < end) ? xs[e[u] & col_mask] : static_cast<T>(0);
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u)
+          if (p0 + u * LANES < end) acc += table[e[u] >> col_bits] * g[u];
+      }
     }
 #pragma unroll
-    for (int o = LANES / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, LANES);
+    for (int o = LANES / 2; o > 0; o >>= 1) {
+      acc += __shfl_xor_sync(group_mask, acc, o, LANES);
+      if (CPLX) acc_i += __shfl_xor_sync(group_mask, acc_i, o, LANES);
+    }
     if (lane == 0) {
       const T scale = SCALED ? sqrt_r[orbit] : static_cast<T>(1);
-      __stcs(y + r, scale * acc + d * xr);
+      if (CPLX) {
+        P2 out;
+        out.x = scale * acc + d * xr;
+        out.y = scale * acc_i + d * xi;
+        __stcs(reinterpret_cast<P2*>(y) + r, out);
+      } else {
+        __stcs(y + r, scale * acc + d * xr);
+      }
     }
   }
 }
@@ -508,6 +560,7 @@ __global__ void __launch_bounds__(256) spmv_wide_kernel(uint64_t n, const IDX* _
                                                         const T* __restrict__ xs, const T* __restrict__ x,
                                                         T* __restrict__ y) {
   const int lane = threadIdx.x % LANES;
+  const unsigned group_mask = (LANES == 32 ? 0xffffffffu : ((1u << LANES) - 1u)) << ((threadIdx.x & 31) / LANES * LANES);
   const uint64_t group = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LANES;
   const uint64_t groups = static_cast<uint64_t>(gridDim.x) * blockDim.x / LANES;
   for (uint64_t r = group; r < n; r += groups) {
@@ -527,8 +580,8 @@ __global__ void __launch_bounds__(256) spmv_wide_kernel(uint64_t n, const IDX* _
     }
 #pragma unroll
     for (int o = LANES / 2; o > 0; o >>= 1) {
-      ar += __shfl_xor_sync(0xffffffffu, ar, o, LANES);
-      ai += __shfl_xor_sync(0xffffffffu, ai, o, LANES);
+      ar += __shfl_xor_sync(group_mask, ar, o, LANES);
+      ai += __shfl_xor_sync(group_mask, ai, o, LANES);
     }
     if (lane == 0) {
       const T scale = SCALED ? static_cast<T>(sqrt_table[257 + orbits[r]]) : static_cast<T>(1);
@@ -994,16 +1047,17 @@ void SpinOperator::apply(int precision, bool complex_vectors, const void* x, voi
   }
   constexpr int kLanes = 4;
   const int grid = grid_for(n * kLanes, 256, 8);
-  if (storage_ == kStoragePacked && !cplx) {
+  if (storage_ == kStoragePacked) {
     auto launch = [&](auto ttag, auto itag, auto stag) {
       using T = decltype(ttag);
       using I = decltype(itag);
       constexpr bool SC = decltype(stag)::value;
       const T* diag = precision == kFP64 ? reinterpret_cast<const T*>(diag64_.get()) : reinterpret_cast<const T*>(diag32_.get());
-      spmv_packed_kernel<T, I, SC, kLanes><<<grid, 256, 0, stream>>>(
-          n, row_ptr_.as<I>(), entries_.as<uint32_t>(), col_bits_, code_table_.as<double>(), n_codes_, diag,
-          basis_->orbits(), inv_sqrt_.as<double>(), static_cast<const T*>(xs), static_cast<const T*>(x),
-          static_cast<T*>(y));
+      auto kernel = cplx ? spmv_packed_kernel<T, I, SC, kLanes, true> : spmv_packed_kernel<T, I, SC, kLanes, false>;
+      kernel<<<grid, 256, 0, stream>>>(n, row_ptr_.as<I>(), entries_.as<uint32_t>(), col_bits_,
+                                       code_table_.as<double>(), n_codes_, diag, basis_->orbits(),
+                                       inv_sqrt_.as<double>(), static_cast<const T*>(xs), static_cast<const T*>(x),
+                                       static_cast<T*>(y));
     };
     using True = std::true_type;
     using False = std::false_type;
@@ -1018,7 +1072,7 @@ void SpinOperator::apply(int precision, bool complex_vectors, const void* x, voi
     return;
   }
   if (real_ && cplx) {
-    // Stored rows of a real operator hold real diagonals; complex vectors take the matrix-free path.
+    // Wide rows of a real operator keep a real diagonal: complex vectors take the matrix-free path.
     apply(precision, complex_vectors, x, y, stream, true);
     return;
   }
@@ -1055,7 +1109,9 @@ void SpinOperator::apply_with_scratch(int precision, bool complex_vectors, const
   const uint64_t n = dim();
   if (n == 0) return;
   const bool cplx = complex_vectors;
-  const bool stored_symmetric = storage_ != kStorageMatrixFree && basis_->symmetric() && !(real_ && cplx);
+  // wide rows of a real operator with complex vectors run matrix-free (their diagonal is real)
+  const bool stored_symmetric = storage_ != kStorageMatrixFree && basis_->symmetric() &&
+                                !(real_ && cplx && storage_ == kStorageWide);
   if (!stored_symmetric) {
     apply(precision, complex_vectors, x, y, stream);  // these paths hold no scaled vector
     return;
@@ -1082,15 +1138,17 @@ void SpinOperator::apply_with_scratch(int precision, bool complex_vectors, const
   constexpr int kLanes = 4;
   const int grid = grid_for(n * kLanes, 256, 8);
   using True = std::true_type;
-  if (storage_ == kStoragePacked && !cplx) {
+  if (storage_ == kStoragePacked) {
     auto launch = [&](auto ttag, auto itag) {
       using T = decltype(ttag);
       using I = decltype(itag);
       const T* diag = precision == kFP64 ? reinterpret_cast<const T*>(diag64_.get()) : reinterpret_cast<const T*>(diag32_.get());
-      spmv_packed_kernel<T, I, True::value, kLanes><<<grid, 256, 0, stream>>>(
-          n, row_ptr_.as<I>(), entries_.as<uint32_t>(), col_bits_, code_table_.as<double>(), n_codes_, diag,
-          basis_->orbits(), inv_sqrt_.as<double>(), static_cast<const T*>(xs), static_cast<const T*>(x),
-          static_cast<T*>(y));
+      auto kernel = cplx ? spmv_packed_kernel<T, I, True::value, kLanes, true>
+                         : spmv_packed_kernel<T, I, True::value, kLanes, false>;
+      kernel<<<grid, 256, 0, stream>>>(n, row_ptr_.as<I>(), entries_.as<uint32_t>(), col_bits_,
+                                       code_table_.as<double>(), n_codes_, diag, basis_->orbits(),
+                                       inv_sqrt_.as<double>(), static_cast<const T*>(xs), static_cast<const T*>(x),
+                                       static_cast<T*>(y));
     };
     if (precision == kFP64) row_ptr64_ ? launch(double{}, uint64_t{}) : launch(double{}, uint32_t{});
     else row_ptr64_ ? launch(float{}, uint64_t{}) : launch(float{}, uint32_t{});

@@ -23,6 +23,9 @@ TARGETS = {
     "shift": 5,
 }
 MODES = {"fp64": 0, "mixed": 1, "filtered": 2}
+EVOLUTION_DIAGNOSTICS = ("lanczos_projections", "matrix_vector_products", "real_lanczos_projections",
+                         "real_matrix_vector_products", "accepted_substeps", "rejected_trial_intervals",
+                         "maximum_estimated_error")
 STORAGE = {"matrix_free": 0, "packed": 1}
 
 
@@ -251,6 +254,26 @@ class GpuOperator:
         return EigshResult(values, residuals, vectors, info.iterations, info.reorthogonalization_passes,
                            info.conditional_second_passes, info.fp32_iterations, info.fp64_iterations,
                            info.operator_applications, bool(info.converged))
+
+    def evolve(self, initial, times, krylov_dimension: int = 30, tolerance: float = 1e-10,
+               max_substeps: int = 10_000):
+        """exp(-i H t) initial on a nondecreasing time grid (reference evolve).
+
+        Returns (states[n_times, dim], diagnostics dict)."""
+        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        t = np.ascontiguousarray(np.asarray(times, np.float64))
+        states = np.zeros((len(t), self.dim), np.complex128)
+        diag = np.zeros(7)
+        check(lib().qmbed_gpu_evolve(self.handle, _ptr(x), len(t), _ptr(t), krylov_dimension, tolerance,
+                                     max_substeps, _ptr(states), _ptr(diag)))
+        return states, dict(zip(EVOLUTION_DIAGNOSTICS, [int(v) for v in diag[:6]] + [float(diag[6])]))
+
+    def expm_lanczos(self, initial, time: float, krylov_dimension: int = 30) -> np.ndarray:
+        """exp(-i H time) initial from one Lanczos projection (reference expm_lanczos)."""
+        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        y = np.zeros(self.dim, np.complex128)
+        check(lib().qmbed_gpu_expm_lanczos(self.handle, _ptr(x), time, krylov_dimension, _ptr(y)))
+        return y
 
     def expm_plan(self, coefficient: complex, max_degree: int = 55, tolerance: float = 0.5 * np.finfo(float).eps,
                   max_substeps: int = 10_000):
