@@ -13,9 +13,12 @@
 // operator and gives a gather (one writer per output row, no atomics).
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <set>
 #include <tuple>
 
@@ -603,9 +606,12 @@ __global__ void __launch_bounds__(256) spmv_wide_kernel(uint64_t n, const IDX* _
 //   out[r][:] = alpha * (sum_k table[code_k] z[col_k][:] + d_r z[r][:]) + beta * z[r][:] + gamma * p[r][:]
 // which is one step of a three-term (Chebyshev) recurrence. A row's NB values
 // are LPR consecutive 16-byte vectors, one per lane, so the gather of a column
-// is one contiguous NB-element read shared by LPR lanes. `out` may alias `p`
+// is one contiguous NB-element read shared by LPR lanes. ES lane groups split
+// the row's entries between them (partial sums combined by shuffles within
+// the row's lanes) and each lane issues KB entry loads, then KB gathers, before
+// its FMAs: both raise the loads in flight per warp. `out` may alias `p`
 // (each row is read before it is written by the same lane), never `z`.
-template <typename T, typename IDX, int NB, bool HAS_P>
+template <typename T, typename IDX, int NB, bool HAS_P, int ES, int KB>
 __global__ void __launch_bounds__(256) spmm_packed_kernel(uint64_t n, const IDX* __restrict__ row_ptr,
                                                           const uint32_t* __restrict__ entries, int col_bits,
                                                           const double* __restrict__ code_values, int n_codes,
@@ -613,31 +619,30 @@ __global__ void __launch_bounds__(256) spmm_packed_kernel(uint64_t n, const IDX*
                                                           const T* p, T* out, T alpha, T beta, T gamma) {
   constexpr int VEC = 16 / sizeof(T);
   constexpr int LPR = NB / VEC;
-  static_assert(NB % VEC == 0 && 32 % LPR == 0, "block width must fill whole 16-byte lanes of a warp");
+  constexpr int G = LPR * ES;  // lanes per row
+  static_assert(NB % VEC == 0 && G <= 32 && 32 % G == 0, "a row's lanes must tile a warp");
   __shared__ T table[kMaxCodes];
   for (int i = threadIdx.x; i < n_codes; i += blockDim.x) table[i] = static_cast<T>(code_values[i]);
   __syncthreads();
   const uint32_t col_mask = col_bits >= 32 ? 0xffffffffu : ((1u << col_bits) - 1u);
-  const int part = threadIdx.x % LPR;
-  const uint64_t group = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / LPR;
-  const uint64_t groups = static_cast<uint64_t>(gridDim.x) * blockDim.x / LPR;
-  constexpr int kBatch = 4;
+  const int gl = threadIdx.x % G;
+  const int part = gl % LPR, split = gl / LPR;
+  const unsigned group_mask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << ((threadIdx.x & 31) / G * G);
+  const uint64_t group = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G;
+  const uint64_t groups = static_cast<uint64_t>(gridDim.x) * blockDim.x / G;
   for (uint64_t r = group; r < n; r += groups) {
     const IDX begin = __ldcs(row_ptr + r), end = __ldcs(row_ptr + r + 1);
-    const T d = __ldcs(diag + r);
-    T self[VEC];
-    load16(z + r * NB + part * VEC, self);
     T acc[VEC];
 #pragma unroll
     for (int v = 0; v < VEC; ++v) acc[v] = 0;
-    for (IDX p0 = begin; p0 < end; p0 += kBatch) {
-      uint32_t e[kBatch];
+    for (IDX p0 = begin + split; p0 < end; p0 += ES * KB) {
+      uint32_t e[KB];
 #pragma unroll
-      for (int u = 0; u < kBatch; ++u) e[u] = p0 + u < end ? __ldcs(entries + p0 + u) : 0u;
-      T g[kBatch][VEC];
+      for (int u = 0; u < KB; ++u) e[u] = p0 + u * ES < end ? __ldcs(entries + p0 + u * ES) : 0u;
+      T g[KB][VEC];
 #pragma unroll
-      for (int u = 0; u < kBatch; ++u) {
-        if (p0 + u < end) {
+      for (int u = 0; u < KB; ++u) {
+        if (p0 + u * ES < end) {
           load16(z + static_cast<uint64_t>(e[u] & col_mask) * NB + part * VEC, g[u]);
         } else {
 #pragma unroll
@@ -645,24 +650,41 @@ __global__ void __launch_bounds__(256) spmm_packed_kernel(uint64_t n, const IDX*
         }
       }
 #pragma unroll
-      for (int u = 0; u < kBatch; ++u) {
-        const T c = p0 + u < end ? table[e[u] >> col_bits] : static_cast<T>(0);
+      for (int u = 0; u < KB; ++u) {
+        const T c = p0 + u * ES < end ? table[e[u] >> col_bits] : static_cast<T>(0);
 #pragma unroll
         for (int v = 0; v < VEC; ++v) acc[v] += c * g[u][v];
       }
     }
-    T o[VEC];
+    if (ES > 1) {
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) o[v] = alpha * (acc[v] + d * self[v]) + beta * self[v];
-    if (HAS_P) {
-      T q[VEC];
-      load16_rw(p + r * NB + part * VEC, q);
+      for (int o = LPR; o < G; o <<= 1)
 #pragma unroll
-      for (int v = 0; v < VEC; ++v) o[v] += gamma * q[v];
+        for (int v = 0; v < VEC; ++v) acc[v] += __shfl_xor_sync(group_mask, acc[v], o, G);
     }
-    store16(out + r * NB + part * VEC, o);
+    if (split == 0) {
+      const T d = __ldcs(diag + r);
+      T self[VEC];
+      load16(z + r * NB + part * VEC, self);
+      T o[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) o[v] = alpha * (acc[v] + d * self[v]) + beta * self[v];
+      if (HAS_P) {
+        T q[VEC];
+        load16_rw(p + r * NB + part * VEC, q);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) o[v] += gamma * q[v];
+      }
+      store16(out + r * NB + part * VEC, o);
+    }
   }
 }
+
+// Shapes of the block action tried by the autotuner: (ES, KB).
+constexpr int kBlockShapes = 4;
+constexpr int kBlockShapeES[kBlockShapes] = {1, 1, 2, 4};
+constexpr int kBlockShapeKB[kBlockShapes] = {4, 8, 4, 2};
+constexpr uint64_t kTuneMinRows = 1u << 20;  // smaller operators use shape 0 untimed
 
 // xs = x / sqrt(R) elementwise (complex vectors scale both parts).
 template <typename T>
@@ -1172,39 +1194,107 @@ void SpinOperator::apply_with_scratch(int precision, bool complex_vectors, const
 
 bool SpinOperator::supports_block() const { return real_ && storage_ == kStoragePacked; }
 
-void SpinOperator::apply_block(int precision, int nb, const void* z, const void* p, void* out, double alpha,
-                               double beta, double gamma, cudaStream_t stream) const {
-  QMBED_CUDA(cudaSetDevice(basis_->device()));
-  if (!supports_block()) raise(QMBED_UNSUPPORTED_BACKEND, "block action needs real packed rows");
+void SpinOperator::launch_block(int shape, int precision, int nb, const void* z, const void* p, void* out,
+                                double alpha, double beta, double gamma, cudaStream_t stream) const {
   const uint64_t n = dim();
-  if (n == 0) return;
-  auto launch = [&](auto ttag, auto itag, auto nbtag, auto ptag) {
+  auto launch = [&](auto ttag, auto itag, auto nbtag, auto ptag, auto estag, auto kbtag) {
     using T = decltype(ttag);
     using I = decltype(itag);
     constexpr int NB = decltype(nbtag)::value;
     constexpr bool HP = decltype(ptag)::value;
-    constexpr int LPR = NB / (16 / static_cast<int>(sizeof(T)));
+    constexpr int ES = decltype(estag)::value;
+    constexpr int KB = decltype(kbtag)::value;
+    constexpr int G = NB / (16 / static_cast<int>(sizeof(T))) * ES;
     const T* diag = precision == kFP64 ? reinterpret_cast<const T*>(diag64_.get()) : reinterpret_cast<const T*>(diag32_.get());
-    const int grid = grid_for(n * LPR, 256, 8);
-    spmm_packed_kernel<T, I, NB, HP><<<grid, 256, 0, stream>>>(
+    const int grid = grid_for(n * G, 256, 8);
+    spmm_packed_kernel<T, I, NB, HP, ES, KB><<<grid, 256, 0, stream>>>(
         n, row_ptr_.as<I>(), entries_.as<uint32_t>(), col_bits_, code_table_.as<double>(), n_codes_, diag,
         static_cast<const T*>(z), static_cast<const T*>(p), static_cast<T*>(out), static_cast<T>(alpha),
         static_cast<T>(beta), static_cast<T>(gamma));
   };
   using NB8 = std::integral_constant<int, 8>;
   using NB16 = std::integral_constant<int, 16>;
+  auto by_shape = [&](auto ttag, auto itag, auto nbtag, auto ptag) {
+    switch (shape) {
+      case 1: launch(ttag, itag, nbtag, ptag, std::integral_constant<int, 1>{}, std::integral_constant<int, 8>{}); break;
+      case 2: launch(ttag, itag, nbtag, ptag, std::integral_constant<int, 2>{}, std::integral_constant<int, 4>{}); break;
+      case 3: launch(ttag, itag, nbtag, ptag, std::integral_constant<int, 4>{}, std::integral_constant<int, 2>{}); break;
+      default: launch(ttag, itag, nbtag, ptag, std::integral_constant<int, 1>{}, std::integral_constant<int, 4>{}); break;
+    }
+  };
   auto by_p = [&](auto ttag, auto itag, auto nbtag) {
-    if (p) launch(ttag, itag, nbtag, std::true_type{});
-    else launch(ttag, itag, nbtag, std::false_type{});
+    if (p) by_shape(ttag, itag, nbtag, std::true_type{});
+    else by_shape(ttag, itag, nbtag, std::false_type{});
   };
   auto by_nb = [&](auto ttag, auto itag) {
     if (nb == 8) by_p(ttag, itag, NB8{});
-    else if (nb == 16) by_p(ttag, itag, NB16{});
-    else raise(QMBED_INVALID_OPTIONS, "block width must be 8 or 16");
+    else by_p(ttag, itag, NB16{});
   };
   if (precision == kFP64) row_ptr64_ ? by_nb(double{}, uint64_t{}) : by_nb(double{}, uint32_t{});
   else row_ptr64_ ? by_nb(float{}, uint64_t{}) : by_nb(float{}, uint32_t{});
   QMBED_LAUNCH_CHECK();
+}
+
+// Autotuner: the first call of each (precision, width, with/without p) on an
+// operator of at least kTuneMinRows rows times every shape on the caller's
+// inputs (output to a scratch block, so the caller's p is untouched) and keeps
+// the fastest; later calls reuse it.
+int SpinOperator::block_shape(int precision, int nb, const void* z, const void* p, double alpha, double beta,
+                              double gamma, cudaStream_t stream) const {
+  // QMBED_BLOCK_SHAPE=<index> pins a shape (for tests of every shape)
+  const char* forced = std::getenv("QMBED_BLOCK_SHAPE");
+  if (forced && forced[0] >= '0' && forced[0] < '0' + kBlockShapes && forced[1] == '\0') return forced[0] - '0';
+  const int key = precision * 1000 + nb * 10 + (p ? 1 : 0);
+  std::lock_guard<std::mutex> lock(tune_mu_);
+  auto it = block_shapes_.find(key);
+  if (it != block_shapes_.end()) return it->second;
+  const uint64_t n = dim();
+  int best = 0;
+  if (n >= kTuneMinRows) {
+    DeviceBuffer scratch(static_cast<size_t>(n) * nb * (precision == kFP64 ? 8 : 4));
+    cudaEvent_t start, stop;
+    QMBED_CUDA(cudaEventCreate(&start));
+    QMBED_CUDA(cudaEventCreate(&stop));
+    float best_ms = 0.0f;
+    for (int shape = 0; shape < kBlockShapes; ++shape) {
+      launch_block(shape, precision, nb, z, p, scratch.get(), alpha, beta, gamma, stream);  // warm
+      QMBED_CUDA(cudaEventRecord(start, stream));
+      for (int rep = 0; rep < 3; ++rep)
+        launch_block(shape, precision, nb, z, p, scratch.get(), alpha, beta, gamma, stream);
+      QMBED_CUDA(cudaEventRecord(stop, stream));
+      QMBED_CUDA(cudaEventSynchronize(stop));
+      float ms = 0.0f;
+      QMBED_CUDA(cudaEventElapsedTime(&ms, start, stop));
+      if (shape == 0 || ms < best_ms) {
+        best_ms = ms;
+        best = shape;
+      }
+      const char* trace = std::getenv("QMBED_FILTER_TRACE");
+      if (trace && trace[0] == '1')
+        std::fprintf(stderr, "[block tune] fp%d nb=%d p=%d shape ES=%d KB=%d: %.3f ms\n", precision, nb, p ? 1 : 0,
+                     kBlockShapeES[shape], kBlockShapeKB[shape], ms / 3.0f);
+    }
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+  }
+  block_shapes_[key] = best;
+  return best;
+}
+
+int SpinOperator::tuned_block_shape(int precision, int nb, bool with_p) const {
+  std::lock_guard<std::mutex> lock(tune_mu_);
+  auto it = block_shapes_.find(precision * 1000 + nb * 10 + (with_p ? 1 : 0));
+  return it == block_shapes_.end() ? -1 : it->second;
+}
+
+void SpinOperator::apply_block(int precision, int nb, const void* z, const void* p, void* out, double alpha,
+                               double beta, double gamma, cudaStream_t stream) const {
+  QMBED_CUDA(cudaSetDevice(basis_->device()));
+  if (!supports_block()) raise(QMBED_UNSUPPORTED_BACKEND, "block action needs real packed rows");
+  if (nb != 8 && nb != 16) raise(QMBED_INVALID_OPTIONS, "block width must be 8 or 16");
+  if (dim() == 0) return;
+  const int shape = block_shape(precision, nb, z, p, alpha, beta, gamma, stream);
+  launch_block(shape, precision, nb, z, p, out, alpha, beta, gamma, stream);
 }
 
 void SpinOperator::export_csr(std::vector<uint64_t>& row_ptr, std::vector<uint32_t>& cols,

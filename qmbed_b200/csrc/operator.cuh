@@ -3,6 +3,8 @@
 #pragma once
 
 #include <complex>
+#include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <vector>
@@ -86,9 +88,13 @@ class SpinOperator {
   // n x nb blocks (nb = 8 or 16, precision 64/32):
   //   out = alpha * (S^-1 H S) z + beta * z + gamma * p     (p may be null; out may alias p, not z)
   // Available for real operators with packed rows (supports_block()).
+  // The kernel shape (entry split across lanes, entry batch depth) is chosen
+  // per (precision, nb, p given) by timing on the first call (autotuner).
   bool supports_block() const;
   void apply_block(int precision, int nb, const void* z, const void* p, void* out, double alpha, double beta,
                    double gamma, cudaStream_t stream) const;
+  // Index of the shape the autotuner chose, or -1 before the first call.
+  int tuned_block_shape(int precision, int nb, bool with_p) const;
 
   // Dense Hermitian check of the assembled operator at tolerance 1e-12
   // (OperatorBuilder::build + is_hermitian, src/operator/mod.rs:2212).
@@ -108,6 +114,10 @@ class SpinOperator {
   void build_instances(const std::vector<TermDesc>& terms, const OperatorChecks& checks);
   void assemble();
   void ensure_scratch(int precision, bool complex_vectors) const;
+  void launch_block(int shape, int precision, int nb, const void* z, const void* p, void* out, double alpha,
+                    double beta, double gamma, cudaStream_t stream) const;
+  int block_shape(int precision, int nb, const void* z, const void* p, double alpha, double beta, double gamma,
+                  cudaStream_t stream) const;
 
   std::shared_ptr<SpinBasis> basis_;
   int storage_;
@@ -124,6 +134,8 @@ class SpinOperator {
   double assembly_seconds_ = 0.0;
   mutable DeviceBuffer scaled_x_;   // x / sqrt(R) for symmetric packed storage
   mutable size_t scaled_bytes_ = 0;
+  mutable std::mutex tune_mu_;
+  mutable std::map<int, int> block_shapes_;  // autotuned block-action shape per key
 };
 
 }  // namespace qmbed

@@ -280,12 +280,15 @@ def test_filtered_eigsh_warm_start(engine, oracle):
     np.testing.assert_allclose(second.eigenvalues, first.eigenvalues, rtol=1e-12)
 
 
+@pytest.mark.parametrize("shape", ["0", "1", "2", "3"])
 @pytest.mark.parametrize("sites,up,momentum,parity,nb,precision", [
     (16, 8, 0, 1, 8, 64), (16, 8, 0, 1, 16, 64), (16, 8, 0, 1, 8, 32), (14, 7, None, None, 16, 32),
     (18, 9, 9, 1, 8, 64),
 ])
-def test_block_action_matches_columnwise_apply(engine, oracle, sites, up, momentum, parity, nb, precision):
+def test_block_action_matches_columnwise_apply(engine, oracle, monkeypatch, sites, up, momentum, parity, nb,
+                                               precision, shape):
     import torch
+    monkeypatch.setenv("QMBED_BLOCK_SHAPE", shape)  # every kernel shape the autotuner may pick
     terms = oracle.heisenberg_terms(sites, delta=0.85)
     ob = oracle.Basis(sites, up=up, momentum=momentum, parity=parity)
     o = oracle.Operator.build(ob, terms)
@@ -371,3 +374,21 @@ def test_tfim_quench_step_matches_oracle(engine, oracle):
         x_g = g.expm_apply(-0.1j, x)
         assert np.linalg.norm(x_g - x_o) <= 1e-12
         x = x_o
+
+
+def test_block_action_autotuned_shape_agrees(engine, oracle, monkeypatch):
+    import torch
+    # above the autotuner's size threshold: the first call times every shape
+    g = engine.GpuOperator(engine.GpuBasis(30, up=15, momentum=0, parity=1), oracle.heisenberg_terms(30))
+    n, nb = g.dim, 8
+    assert n >= 1 << 20
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    z = torch.randn((n, nb), dtype=torch.float32, device="cuda", generator=gen)
+    p = torch.randn((n, nb), dtype=torch.float32, device="cuda", generator=gen)
+    tuned, pinned = torch.empty_like(z), torch.empty_like(z)
+    g.apply_block_device(z, tuned, nb, precision=32, alpha=0.3, beta=0.1, gamma=-0.2, p=p)
+    g.apply_block_device(z, tuned, nb, precision=32, alpha=0.3, beta=0.1, gamma=-0.2, p=p)  # cached shape
+    monkeypatch.setenv("QMBED_BLOCK_SHAPE", "0")
+    g.apply_block_device(z, pinned, nb, precision=32, alpha=0.3, beta=0.1, gamma=-0.2, p=p)
+    torch.cuda.synchronize()
+    assert torch.linalg.norm(tuned - pinned) <= 1e-6 * torch.linalg.norm(pinned)
