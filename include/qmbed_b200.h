@@ -212,6 +212,22 @@ QMBED_API int qmbed_gpu_evolve(qmbed_operator op, const double* initial, int n_t
 QMBED_API int qmbed_gpu_expm_lanczos(qmbed_operator op, const double* initial, double time,
                                      uint64_t krylov_dimension, double* out);
 
+/* exp(-i H t) initial at each of n_times nondecreasing times (from 0) by a
+ * Chebyshev expansion per interval on the spectral interval [e_min, e_max]
+ * (NaN for both: the guaranteed bound +-sum|coefficients|), with working
+ * precision 64 (complex128) or 32 (complex64). The same states as evolve /
+ * expm_multiply (src/solve/mod.rs:3374-3406, 116-248) within the tolerance;
+ * the Chebyshev form has no counterpart in the reference. Operators with the
+ * structured flip-chain action only (full space, matrix-free storage, terms
+ * that are z products or a single x); otherwise QMBED_STATUS_UNSUPPORTED_BACKEND.
+ * states receives every time's state, or only the last one when final_only
+ * is nonzero (for long trajectories of large chains). info (may be NULL)
+ * receives: H applications, intervals, e_min, e_max used, and the largest
+ * drift of the state norm. */
+QMBED_API int qmbed_gpu_chebyshev_evolve(qmbed_operator op, const double* initial, int n_times, const double* times,
+                                         double e_min, double e_max, double tolerance, int precision, int final_only,
+                                         double* states, double* info);
+
 /* deterministic_start (src/solve/mod.rs:729-742): normalised LCG vector. */
 QMBED_API int qmbed_gpu_deterministic_start(int device, uint64_t n, uint64_t seed, double* out);
 

@@ -110,6 +110,7 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_deterministic_start.argtypes = [i, u64, u64, vp]
     L.qmbed_gpu_evolve.argtypes = [vp, vp, i, vp, u64, d, u64, vp, vp]
     L.qmbed_gpu_expm_lanczos.argtypes = [vp, vp, d, u64, vp]
+    L.qmbed_gpu_chebyshev_evolve.argtypes = [vp, vp, i, vp, d, d, d, i, i, vp, vp]
     for name in ("qmbed_run_json", "qmbed_command_json"):
         getattr(L, name).argtypes = [ctypes.c_char_p]
         getattr(L, name).restype = ctypes.c_void_p

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/qmbed_b200.h"
+#include "chebyshev.cuh"
 #include "eigsh.cuh"
 #include "evolve.cuh"
 #include "expm.cuh"
@@ -1027,6 +1028,27 @@ int qmbed_gpu_expm_lanczos(qmbed_operator op, const double* initial, double time
     if (!initial || !out) raise(QMBED_INVALID_OPTIONS, "expm_lanczos needs input and output vectors");
     std::lock_guard<std::mutex> lock(op->mu);
     expm_lanczos(op->view(), initial, time, krylov_dimension, out, op->block_ops());
+  });
+}
+
+int qmbed_gpu_chebyshev_evolve(qmbed_operator op, const double* initial, int n_times, const double* times,
+                               double e_min, double e_max, double tolerance, int precision, int final_only,
+                               double* states, double* info) {
+  return guarded([&] {
+    if (!initial || !states || n_times < 0 || (n_times > 0 && !times))
+      raise(QMBED_INVALID_OPTIONS, "evolution needs an initial state, a time grid and an output array");
+    std::lock_guard<std::mutex> lock(op->mu);
+    if (std::isnan(e_min) && std::isnan(e_max)) flip_chain_norm_bounds(*op->op, &e_min, &e_max);
+    ChebyshevInfo ci;
+    chebyshev_evolve(*op->op, initial, std::vector<double>(times, times + n_times), e_min, e_max, tolerance, precision,
+                     final_only != 0, states, ci, op->block_ops());
+    if (info) {
+      info[0] = static_cast<double>(ci.applications);
+      info[1] = static_cast<double>(ci.intervals);
+      info[2] = ci.e_min;
+      info[3] = ci.e_max;
+      info[4] = ci.max_norm_drift;
+    }
   });
 }
 

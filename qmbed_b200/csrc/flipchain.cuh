@@ -1,0 +1,54 @@
+// Structured action of full-space spin-1/2 chains whose terms are products of
+// z (diagonal) or a single x (one bit flip): transverse-field Ising chains and
+// their relatives. No matrix is stored: the diagonal is evaluated from the bits
+// of the state index, and the flips read the vector through two shared-memory
+// tiled passes (low bits in a contiguous tile, high bits in a strided tile).
+#pragma once
+
+#include <complex>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+namespace qmbed {
+
+struct FlipChainDesc {
+  int sites = 0;
+  std::vector<uint64_t> z_masks;   // diagonal products: sites of the z factors
+  std::vector<double> z_coefs;     // coefficient x z1^|mask|, so D(s) = sum c (-1)^popcount(~s & mask)
+  std::vector<double> x_coefs;     // per site: amplitude of the single flip of that bit
+};
+
+// out = alpha * (H x) + beta * x + gamma * p + kappa * q  on full-space
+// vectors (real or interleaved complex, FP64 or FP32); p and q may be null;
+// out may alias p (rows are read before they are written), never x or q.
+// kappa is complex (applied to complex vectors; its real part for real ones).
+struct FlipStep {
+  double alpha = 1.0, beta = 0.0, gamma = 0.0;
+  double kappa_re = 0.0, kappa_im = 0.0;
+};
+
+class FlipChain {
+ public:
+  explicit FlipChain(const FlipChainDesc& d);
+  uint64_t dim() const { return 1ull << sites_; }
+  int sites() const { return sites_; }
+  // y = H x (step = identity coefficients) or the fused three/four-term form.
+  void apply(int precision, bool cplx, const void* x, void* out, const void* p, const void* q, const FlipStep& step,
+             cudaStream_t stream) const;
+  // Gershgorin-type bounds: |D| max over the diagonal terms plus sum |x|.
+  double norm_bound() const;
+
+ private:
+  int sites_;
+  int n_diag_;
+  DeviceBuffer diag_masks_, diag_coefs_, x_coefs_;
+  mutable DeviceBuffer partial_;  // low-bit diagonal tables (both precisions) + pass A partial sums
+  mutable size_t partial_bytes_ = 0;
+  mutable int tables_ready_ = 0;  // bit 1: FP64 table, bit 2: FP32 table
+  mutable int table_tb_[2] = {0, 0};
+  std::vector<double> host_diag_coefs_, host_x_;
+};
+
+}  // namespace qmbed

@@ -769,7 +769,8 @@ SpinOperator::SpinOperator(std::shared_ptr<SpinBasis> basis, const std::vector<T
   table[257 + 0] = 0.0;
   inv_sqrt_.allocate(table.size() * sizeof(double));
   QMBED_CUDA(cudaMemcpy(inv_sqrt_.get(), table.data(), table.size() * sizeof(double), cudaMemcpyHostToDevice));
-  if (checks.hermiticity && !check_hermitian()) raise(QMBED_NON_HERMITIAN, "");
+  // flip chains have real coefficients on symmetric flips and a real diagonal: Hermitian by construction
+  if (checks.hermiticity && !flip_ && !check_hermitian()) raise(QMBED_NON_HERMITIAN, "");
   if (storage_ != kStorageMatrixFree) {
     if (dim() >= (1ULL << 32)) {
       storage_ = kStorageMatrixFree;  // columns do not fit 32 bits: keep the action matrix-free
@@ -869,6 +870,56 @@ void SpinOperator::build_instances(const std::vector<TermDesc>& terms, const Ope
   }
   real_ = real;
   n_inst_ = static_cast<int>(adj.size());
+  // Full-space chains whose products are z's (diagonal) or one x with
+  // identities (a single bit flip) and real coefficients act through the
+  // structured flip-chain kernels (matrix-free storage only).
+  flip_.reset();
+  if (storage_ == kStorageMatrixFree && basis_->direct() && !basis_->symmetric() && basis_->params().up < 0 &&
+      sites <= 40 && factors_.raise == factors_.lower) {
+    FlipChainDesc d;
+    d.sites = sites;
+    d.x_coefs.assign(static_cast<size_t>(sites), 0.0);
+    std::map<uint64_t, double> diag;
+    bool ok = true;
+    for (const Instance& f : fwd) {
+      if (f.ci != 0.0) {
+        ok = false;
+        break;
+      }
+      uint64_t zmask = 0, seen = 0;
+      int flip_site = -1, nz = 0;
+      for (int q = 0; q < f.n && ok; ++q) {
+        if (f.sym[q] == 'I') continue;
+        const uint64_t bit = 1ull << f.site[q];
+        if (seen & bit) ok = false;
+        seen |= bit;
+        if (f.sym[q] == 'z') {
+          zmask |= bit;
+          ++nz;
+        } else if (f.sym[q] == 'x' && flip_site < 0) {
+          flip_site = f.site[q];
+        } else {
+          ok = false;
+        }
+      }
+      if (!ok || (flip_site >= 0 && nz > 0)) {
+        ok = false;
+        break;
+      }
+      if (flip_site >= 0) d.x_coefs[static_cast<size_t>(flip_site)] += f.cr * factors_.raise * factors_.xy_scale;
+      else diag[zmask] += f.cr * std::pow(factors_.z[1], nz);
+    }
+    if (ok && diag.size() <= 256) {
+      for (const auto& [mask, c] : diag) {
+        d.z_masks.push_back(mask);
+        d.z_coefs.push_back(c);
+      }
+      flip_ = std::make_unique<FlipChain>(d);
+      uint64_t flips = 0;
+      for (double c : d.x_coefs) flips += c != 0.0 ? 1 : 0;
+      nnz_off_ = flips * dim();
+    }
+  }
   inst_adj_.allocate(std::max<size_t>(adj.size(), 1) * sizeof(Instance));
   inst_fwd_.allocate(std::max<size_t>(fwd.size(), 1) * sizeof(Instance));
   if (!adj.empty()) {
@@ -1026,6 +1077,10 @@ void SpinOperator::apply(int precision, bool complex_vectors, const void* x, voi
   if (!real_ && !complex_vectors)
     raise(QMBED_UNSUPPORTED_BACKEND, "real action requires an operator with real-valued storage");
   const bool cplx = complex_vectors;
+  if (flip_ && !force_matrix_free) {
+    flip_->apply(precision, cplx, x, y, nullptr, nullptr, FlipStep{}, stream);
+    return;
+  }
   if (storage_ == kStorageMatrixFree || force_matrix_free) {
     const int grid = grid_for(n, 256, 8);
     const size_t smem = n_inst_ <= kSmemInstances ? static_cast<size_t>(n_inst_) * sizeof(Instance) : 0;
@@ -1135,7 +1190,9 @@ void SpinOperator::apply_with_scratch(int precision, bool complex_vectors, const
   const bool stored_symmetric = storage_ != kStorageMatrixFree && basis_->symmetric() &&
                                 !(real_ && cplx && storage_ == kStorageWide);
   if (!stored_symmetric) {
-    apply(precision, complex_vectors, x, y, stream);  // these paths hold no scaled vector
+    // these paths hold no scaled vector; flip chains take the on-the-fly
+    // expansion, whose kernels need no work buffer either
+    apply(precision, complex_vectors, x, y, stream, flip_ != nullptr);
     return;
   }
   if (!real_ && !cplx) raise(QMBED_UNSUPPORTED_BACKEND, "real action requires an operator with real-valued storage");

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "basis.cuh"
+#include "flipchain.cuh"
 
 namespace qmbed {
 
@@ -96,6 +97,10 @@ class SpinOperator {
   // Index of the shape the autotuner chose, or -1 before the first call.
   int tuned_block_shape(int precision, int nb, bool with_p) const;
 
+  // The structured flip-chain action, when this operator has that form
+  // (full space, matrix-free storage, z products and single x flips).
+  const FlipChain* flip_chain() const { return flip_.get(); }
+
   // Dense Hermitian check of the assembled operator at tolerance 1e-12
   // (OperatorBuilder::build + is_hermitian, src/operator/mod.rs:2212).
   bool check_hermitian() const;
@@ -134,6 +139,7 @@ class SpinOperator {
   double assembly_seconds_ = 0.0;
   mutable DeviceBuffer scaled_x_;   // x / sqrt(R) for symmetric packed storage
   mutable size_t scaled_bytes_ = 0;
+  std::unique_ptr<FlipChain> flip_;
   mutable std::mutex tune_mu_;
   mutable std::map<int, int> block_shapes_;  // autotuned block-action shape per key
 };

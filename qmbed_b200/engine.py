@@ -275,6 +275,21 @@ class GpuOperator:
         check(lib().qmbed_gpu_expm_lanczos(self.handle, _ptr(x), time, krylov_dimension, _ptr(y)))
         return y
 
+    def chebyshev_evolve(self, initial, times, e_min: float = float("nan"), e_max: float = float("nan"),
+                         tolerance: float = 1e-10, precision: int = 64, final_only: bool = False):
+        """exp(-i H t) initial on a time grid by Chebyshev expansions (flip-chain operators).
+
+        [e_min, e_max] must contain the spectrum; NaN uses the guaranteed
+        +-sum|coefficients| bound. Returns (states[n_times or 1, dim], info dict)."""
+        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        t = np.ascontiguousarray(np.asarray(times, np.float64))
+        states = np.zeros((1 if final_only else len(t), self.dim), np.complex128)
+        info = np.zeros(5)
+        check(lib().qmbed_gpu_chebyshev_evolve(self.handle, _ptr(x), len(t), _ptr(t), e_min, e_max, tolerance,
+                                               precision, int(final_only), _ptr(states), _ptr(info)))
+        return states, {"applications": int(info[0]), "intervals": int(info[1]), "e_min": float(info[2]),
+                        "e_max": float(info[3]), "max_norm_drift": float(info[4])}
+
     def expm_plan(self, coefficient: complex, max_degree: int = 55, tolerance: float = 0.5 * np.finfo(float).eps,
                   max_substeps: int = 10_000):
         degree, scaling, one_norm = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double()
