@@ -228,6 +228,43 @@ QMBED_API int qmbed_gpu_chebyshev_evolve(qmbed_operator op, const double* initia
                                          double e_min, double e_max, double tolerance, int precision, int final_only,
                                          double* states, double* info);
 
+/* Extreme Ritz values of a steps-step FP64 Lanczos run without
+ * reorthogonalisation from deterministic_start(seed) (src/solve/mod.rs:
+ * 729-742), as used for spectral bounds: out receives the smallest and largest
+ * Ritz values and the residual norms of their Ritz pairs (4 doubles). The
+ * Ritz values lie inside the spectrum. No counterpart in the reference, whose
+ * Lanczos routines return converged eigenpairs only. */
+QMBED_API int qmbed_gpu_lanczos_extremes(qmbed_operator op, int steps, uint64_t seed, double* out);
+
+/* Learned spectral bounds: a fully connected ReLU network (inputs ->
+ * hidden_layers x width -> outputs, FP32) trained and evaluated by this
+ * library's own GPU kernels. It maps model parameters (size, couplings,
+ * statistics of random fields) to spectral bounds that set the Chebyshev
+ * interval and degree; every prediction used by a solver is checked by a short
+ * Lanczos run first. No counterpart in the reference. Parameters are
+ * flattened per linear map: W (in x out, row-major) then b (out). */
+typedef struct qmbed_mlp_s* qmbed_mlp;
+QMBED_API int qmbed_gpu_mlp_create(int device, int inputs, int outputs, int width, int hidden_layers, uint64_t seed,
+                                   qmbed_mlp* out);
+QMBED_API int qmbed_gpu_mlp_destroy(qmbed_mlp mlp);
+QMBED_API int qmbed_gpu_mlp_parameter_count(qmbed_mlp mlp, uint64_t* count);
+QMBED_API int qmbed_gpu_mlp_get_parameters(qmbed_mlp mlp, float* out);
+QMBED_API int qmbed_gpu_mlp_set_parameters(qmbed_mlp mlp, const float* in);
+/* Input scaling (x - in_mean) / in_std and output scaling y * out_std + out_mean. */
+QMBED_API int qmbed_gpu_mlp_set_scaling(qmbed_mlp mlp, const float* in_mean, const float* in_std,
+                                        const float* out_mean, const float* out_std);
+QMBED_API int qmbed_gpu_mlp_get_scaling(qmbed_mlp mlp, float* in_mean, float* in_std, float* out_mean,
+                                        float* out_std);
+/* Mean squared error of the unscaled network on n samples (X: n x inputs,
+ * Y: n x outputs, row-major) and its gradient for every parameter. */
+QMBED_API int qmbed_gpu_mlp_gradients(qmbed_mlp mlp, const float* X, const float* Y, int n, float* grads,
+                                      float* loss);
+/* Fits the scaling to (X, Y), then trains with Adam (mini-batches, cosine
+ * learning-rate decay); loss receives the final full-batch loss (scaled units). */
+QMBED_API int qmbed_gpu_mlp_train(qmbed_mlp mlp, const float* X, const float* Y, int n, int epochs, int batch,
+                                  float learning_rate, uint64_t seed, float* loss);
+QMBED_API int qmbed_gpu_mlp_predict(qmbed_mlp mlp, const float* X, int n, float* Y);
+
 /* deterministic_start (src/solve/mod.rs:729-742): normalised LCG vector. */
 QMBED_API int qmbed_gpu_deterministic_start(int device, uint64_t n, uint64_t seed, double* out);
 

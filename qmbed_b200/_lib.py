@@ -111,6 +111,17 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_evolve.argtypes = [vp, vp, i, vp, u64, d, u64, vp, vp]
     L.qmbed_gpu_expm_lanczos.argtypes = [vp, vp, d, u64, vp]
     L.qmbed_gpu_chebyshev_evolve.argtypes = [vp, vp, i, vp, d, d, d, i, i, vp, vp]
+    L.qmbed_gpu_lanczos_extremes.argtypes = [vp, i, u64, vp]
+    L.qmbed_gpu_mlp_create.argtypes = [i, i, i, i, i, u64, P(vp)]
+    L.qmbed_gpu_mlp_destroy.argtypes = [vp]
+    L.qmbed_gpu_mlp_parameter_count.argtypes = [vp, P(u64)]
+    L.qmbed_gpu_mlp_get_parameters.argtypes = [vp, vp]
+    L.qmbed_gpu_mlp_set_parameters.argtypes = [vp, vp]
+    L.qmbed_gpu_mlp_set_scaling.argtypes = [vp, vp, vp, vp, vp]
+    L.qmbed_gpu_mlp_get_scaling.argtypes = [vp, vp, vp, vp, vp]
+    L.qmbed_gpu_mlp_gradients.argtypes = [vp, vp, vp, i, vp, P(ctypes.c_float)]
+    L.qmbed_gpu_mlp_train.argtypes = [vp, vp, vp, i, i, i, ctypes.c_float, u64, P(ctypes.c_float)]
+    L.qmbed_gpu_mlp_predict.argtypes = [vp, vp, i, vp]
     for name in ("qmbed_run_json", "qmbed_command_json"):
         getattr(L, name).argtypes = [ctypes.c_char_p]
         getattr(L, name).restype = ctypes.c_void_p

@@ -20,6 +20,7 @@
 #include "evolve.cuh"
 #include "expm.cuh"
 #include "json.hpp"
+#include "mlp.cuh"
 #include "operator.cuh"
 
 namespace qmbed {
@@ -1049,6 +1050,94 @@ int qmbed_gpu_chebyshev_evolve(qmbed_operator op, const double* initial, int n_t
       info[3] = ci.e_max;
       info[4] = ci.max_norm_drift;
     }
+  });
+}
+
+int qmbed_gpu_lanczos_extremes(qmbed_operator op, int steps, uint64_t seed, double* out) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(op->mu);
+    const RitzExtremes r = lanczos_extremes(op->view(), steps, seed, op->block_ops());
+    out[0] = r.min;
+    out[1] = r.max;
+    out[2] = r.min_residual;
+    out[3] = r.max_residual;
+  });
+}
+
+struct qmbed_mlp_s {
+  std::unique_ptr<Mlp> net;
+  std::mutex mu;
+};
+
+int qmbed_gpu_mlp_create(int device, int inputs, int outputs, int width, int hidden_layers, uint64_t seed,
+                         qmbed_mlp* out) {
+  return guarded([&] {
+    auto h = std::make_unique<qmbed_mlp_s>();
+    h->net = std::make_unique<Mlp>(device, inputs, outputs, width, hidden_layers, seed);
+    *out = h.release();
+  });
+}
+
+int qmbed_gpu_mlp_destroy(qmbed_mlp mlp) {
+  return guarded([&] { delete mlp; });
+}
+
+int qmbed_gpu_mlp_parameter_count(qmbed_mlp mlp, uint64_t* count) {
+  return guarded([&] { *count = mlp->net->parameter_count(); });
+}
+
+int qmbed_gpu_mlp_get_parameters(qmbed_mlp mlp, float* out) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(mlp->mu);
+    mlp->net->get_parameters(out);
+  });
+}
+
+int qmbed_gpu_mlp_set_parameters(qmbed_mlp mlp, const float* in) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(mlp->mu);
+    mlp->net->set_parameters(in);
+  });
+}
+
+int qmbed_gpu_mlp_set_scaling(qmbed_mlp mlp, const float* in_mean, const float* in_std, const float* out_mean,
+                              const float* out_std) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(mlp->mu);
+    const int ni = mlp->net->inputs(), no = mlp->net->outputs();
+    mlp->net->set_scaling(std::vector<float>(in_mean, in_mean + ni), std::vector<float>(in_std, in_std + ni),
+                          std::vector<float>(out_mean, out_mean + no), std::vector<float>(out_std, out_std + no));
+  });
+}
+
+int qmbed_gpu_mlp_get_scaling(qmbed_mlp mlp, float* in_mean, float* in_std, float* out_mean, float* out_std) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(mlp->mu);
+    mlp->net->get_scaling(in_mean, in_std, out_mean, out_std);
+  });
+}
+
+int qmbed_gpu_mlp_gradients(qmbed_mlp mlp, const float* X, const float* Y, int n, float* grads, float* loss) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(mlp->mu);
+    const float l = mlp->net->gradients(X, Y, n, grads);
+    if (loss) *loss = l;
+  });
+}
+
+int qmbed_gpu_mlp_train(qmbed_mlp mlp, const float* X, const float* Y, int n, int epochs, int batch,
+                        float learning_rate, uint64_t seed, float* loss) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(mlp->mu);
+    const float l = mlp->net->train(X, Y, n, epochs, batch, learning_rate, seed);
+    if (loss) *loss = l;
+  });
+}
+
+int qmbed_gpu_mlp_predict(qmbed_mlp mlp, const float* X, int n, float* Y) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(mlp->mu);
+    mlp->net->predict(X, n, Y);
   });
 }
 

@@ -595,6 +595,53 @@ void validate(const EigshOptions& o, uint64_t n) {
 
 }  // namespace
 
+RitzExtremes lanczos_extremes(const LinearOperatorView& op, int steps, uint64_t seed, BlockOps& ops) {
+  const uint64_t n = op.dim;
+  if (steps < 1) raise(QMBED_INVALID_OPTIONS, "Lanczos steps must be positive");
+  const bool cplx = !op.real;
+  const size_t es = cplx ? 16 : 8;
+  const int m = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(steps), n));
+  DeviceBuffer a(n * es), b(n * es), w(n * es);
+  void* prev = a.get();
+  void* cur = b.get();
+  ops.lcg_start(cur, n, seed, 64, cplx);
+  const double n0 = ops.norm(cur, n, 64, cplx);
+  if (!(n0 > kEps)) nonconvergence(0, n0);
+  ops.scale(cur, n, n0, 64, cplx);
+  std::vector<double> alpha, beta;
+  for (int j = 0; j < m; ++j) {
+    op.apply(64, cplx, cur, w.get());
+    C64 h;
+    ops.dots(cur, n, 1, w.get(), n, 64, cplx, &h);
+    const C64 ha(h.real(), 0.0);
+    double norm = ops.subtract(cur, n, 1, &ha, w.get(), n, 64, cplx, j == 0);
+    if (j > 0) {
+      const C64 hb(beta.back(), 0.0);
+      norm = ops.subtract(prev, n, 1, &hb, w.get(), n, 64, cplx, true);
+    }
+    alpha.push_back(h.real());
+    beta.push_back(norm);
+    if (!(norm > 1.0e-12 * std::max(1.0, std::fabs(h.real())))) break;
+    // the next vector overwrites the previous one
+    ops.scale_into(w.get(), prev, n, norm, 64, cplx);
+    std::swap(prev, cur);
+  }
+  const int size = static_cast<int>(alpha.size());
+  std::vector<double> T(static_cast<size_t>(size) * size, 0.0), vals, vecs;
+  for (int i = 0; i < size; ++i) {
+    T[static_cast<size_t>(i) * size + i] = alpha[i];
+    if (i + 1 < size) T[static_cast<size_t>(i) * size + i + 1] = T[static_cast<size_t>(i + 1) * size + i] = beta[i];
+  }
+  device_symmetric_eigen(size, T, vals, vecs, ops.stream());
+  RitzExtremes r;
+  r.steps = size;
+  r.min = vals.front();
+  r.max = vals.back();
+  r.min_residual = std::fabs(beta.back() * vecs[static_cast<size_t>(size - 1) * size + 0]);
+  r.max_residual = std::fabs(beta.back() * vecs[static_cast<size_t>(size - 1) * size + (size - 1)]);
+  return r;
+}
+
 EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options, const double* initial, int n_initial,
                   int mode, BlockOps& ops) {
   const uint64_t n = op.dim;

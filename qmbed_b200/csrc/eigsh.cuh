@@ -62,6 +62,17 @@ struct LinearOperatorView {
   const uint16_t* weights = nullptr;   // orbit sizes R of the block coordinates; null when every R is 1
 };
 
+// Extreme Ritz values of a `steps`-step FP64 Lanczos run without
+// reorthogonalisation from the reference deterministic start (seed), with
+// the residual norms |beta_m s_m| of their Ritz pairs: Ritz values lie inside
+// the spectrum, and an eigenvalue lies within the residual of each.
+struct RitzExtremes {
+  double min = 0.0, max = 0.0;
+  double min_residual = 0.0, max_residual = 0.0;
+  int steps = 0;
+};
+RitzExtremes lanczos_extremes(const LinearOperatorView& op, int steps, uint64_t seed, BlockOps& ops);
+
 // Initial vectors: `n_initial` host vectors of dim complex values,
 // interleaved (re, im) doubles, contiguous (may be null when n_initial = 0).
 EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options, const double* initial, int n_initial,

@@ -80,9 +80,10 @@ def test_chebyshev_matches_oracle_evolution(engine, oracle, precision, tol):
     assert info["intervals"] == 4 and info["applications"] > 0
     assert info["max_norm_drift"] <= (1e-9 if precision == 64 else 1e-5)
     # a tighter interval from the exact extremes gives the same states with fewer terms
-    dense = np.array([o.apply(np.eye(g.dim)[:, j]) for j in range(g.dim)]).T
-    w = np.linalg.eigvalsh(dense)
-    tight, tinfo = g.chebyshev_evolve(psi0, times, e_min=w[0] - 1e-3, e_max=w[-1] + 1e-3, precision=precision)
+    from qmbed_b200.learned import lanczos_extremes
+    lo, hi, r_lo, r_hi = lanczos_extremes(g, 300)
+    assert r_lo < 1e-6 and r_hi < 1e-6
+    tight, tinfo = g.chebyshev_evolve(psi0, times, e_min=lo - 1e-3, e_max=hi + 1e-3, precision=precision)
     assert max(float(np.linalg.norm(a - b)) for a, b in zip(tight, ref)) <= tol
     assert tinfo["applications"] < info["applications"]
 
