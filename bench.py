@@ -54,7 +54,66 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI leg (profiling runs)")
     p.add_argument("--hv-launches", type=int, default=20)
+    p.add_argument("--quench-sites", type=int, default=28,
+                   help="transverse-field Ising quench size (0 skips the quench section)")
+    p.add_argument("--quench-bounds", default="learned", choices=["learned", "lanczos", "norm"])
     return p.parse_args()
+
+
+def quench(sites: int, bounds_source: str, rank: int, local_rank: int) -> dict:
+    """Transverse-field Ising quench: J = 1, g = 1, h_i ~ U[-2, 2], open chain,
+    |up...up> evolved to t = 10 in 100 Chebyshev steps with complex64 working
+    vectors, checked against the same propagation with complex128 vectors."""
+    import torch
+    from qmbed_b200 import learned
+
+    g, width, seed = 1.0, 2.0, 2024 + rank
+    fields = learned.tfim_instance(sites, g, width, seed)
+    op = learned.tfim_operator(sites, g, fields, device=local_rank)
+    psi0 = np.zeros(op.dim, complex)
+    psi0[-1] = 1.0
+    times = [0.1 * (k + 1) for k in range(100)]
+    out = {"workload": f"tfim L={sites} obc J=1 g={g} h~U[-{width},{width}] seed {seed}, |up..up>, t=10 in 100 steps",
+           "dim": op.dim}
+    t0 = time.perf_counter()
+    if bounds_source == "learned":
+        x, y = learned.generate_tfim_bounds(96, sizes=(6, 8, 10, 12), seed=11)
+        model = learned.LearnedBounds()
+        loss = model.fit(x, y, epochs=300, seed=1)
+        interval = model.interval(op, sites, g, width, fields)
+        out["learned"] = {"training_instances": len(x), "final_loss": loss,
+                          "train_s": time.perf_counter() - t0}
+    norm_bound = (sites - 1) * 1.0 + sites * g + float(np.abs(fields).sum())  # sum of |coefficients|
+    if bounds_source == "lanczos":
+        interval = learned.lanczos_interval(op)
+    elif bounds_source == "norm":
+        interval = learned.Interval(-norm_bound, norm_bound, "norm", 0)
+    lanczos = learned.lanczos_interval(op)
+    torch.cuda.synchronize()
+    start = time.perf_counter()
+    states32, info32 = learned.propagate(op, psi0, times, interval, precision=32, final_only=True)
+    torch.cuda.synchronize()
+    t32 = time.perf_counter() - start
+    start = time.perf_counter()
+    states64, info64 = learned.propagate(op, psi0, times, interval, precision=64, final_only=True)
+    torch.cuda.synchronize()
+    t64 = time.perf_counter() - start
+    bytes_per_application = op.operand_bytes(32, complex_vectors=True)
+    out.update({
+        "bounds": {"source": interval.source, "e_min": interval.e_min, "e_max": interval.e_max,
+                   "used_complex64": [info32["source"], info32["e_min"], info32["e_max"]],
+                   "used_complex128": [info64["source"], info64["e_min"], info64["e_max"]],
+                   "bound_applications": interval.applications,
+                   "lanczos_interval": [lanczos.e_min, lanczos.e_max], "norm_bound": norm_bound},
+        "complex64": {"s": t32, "applications": info32["applications"],
+                      "ms_per_application": 1e3 * t32 / max(info32["applications"], 1),
+                      "operand_gbs": bytes_per_application * info32["applications"] / t32 / 1e9,
+                      "norm_drift": info32["max_norm_drift"]},
+        "complex128": {"s": t64, "applications": info64["applications"], "norm_drift": info64["max_norm_drift"]},
+        "complex64_error_vs_complex128": float(np.linalg.norm(states32[0] - states64[0])),
+        "operand_bytes_per_application_c64": bytes_per_application,
+    })
+    return out
 
 
 def sector_dimension_estimate(sites: int) -> float:
@@ -347,6 +406,10 @@ def main():
                          f"{sample['iterations']} H.v, {sample['solve_s']:.2f} s) scaled by rows and by "
                          f"{iterations_target} iterations to D={dim}"}
 
+    quench_result = None
+    if args.quench_sites > 0:
+        quench_result = quench(args.quench_sites, args.quench_bounds, rank, local_rank)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -368,6 +431,7 @@ def main():
                    "operand_bytes_fp64": op.operand_bytes(64), "fp32_gbs": achieved,
                    "fp64_gbs": op.operand_bytes(64) / hv64_s / 1e9},
             "block_action": block,
+            "quench": quench_result,
             "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved_top,
                          "peak": peak, "unit": "GB/s", "frac": achieved_top / peak, "traffic": traffic,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "_fallback" not in peaks

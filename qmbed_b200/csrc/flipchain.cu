@@ -1,15 +1,13 @@
 // Structured full-space chain action (diagonal z products + single bit flips).
 //
-// The action is y[s] = D(s) x[s] + sum_i c_i x[s ^ (1 << i)]. With the index
-// split s = j | (t << tb) for a tile of 2^tb consecutive elements:
-//   pass A  (tile = 2^tb consecutive elements in shared memory):
-//           D(s) x[s] and the flips of bits < tb.
-//   pass B  (tile = 2^P consecutive elements, for one 32-byte sector, times
-//           2^M values of the top M bits, in shared memory): the flips of the
-//           top M bits; the remaining middle bits [tb, L - M) read their
-//           partner from global memory, with the tile order chosen so that the
-//           partner tiles are in flight at the same time (L2 hits).
-// Pass B also applies the fused epilogue out = alpha y + beta x + gamma p + kappa q.
+// The action is y[s] = D(s) x[s] + sum_i c_i x[s ^ (1 << i)], computed in one
+// pass over tiles of 2^tb consecutive elements (64 KB) held in shared memory:
+// the flips of the low tb bits read the tile, the flips of the higher bits
+// read their partner element from global memory. A partner of bit i lies in
+// tile t ^ 2^(i - tb), a contiguous chunk, so those reads are fully coalesced,
+// and partner tiles within the L2 window (about 1900 tiles of 64 KB) are
+// served by L2. The fused epilogue out = alpha y + beta x + gamma p + kappa q
+// serves the Chebyshev (Clenshaw) step.
 // D(s) = D_low(j) + D_high(t) + D_cross(s): terms inside the low bits come from
 // a 2^tb table computed once, terms inside the high bits once per tile, and
 // only the terms spanning both are evaluated per element.
@@ -97,10 +95,9 @@ __global__ void diag_low_table_kernel(int tb, int nd, const uint64_t* __restrict
   }
 }
 
-// Pass A. With FINAL the flips of every bit are inside the tile (L <= tb) and
-// the epilogue is applied here; otherwise the partial sum goes to `partial`.
-template <typename T, bool CPLX, bool FINAL>
-__global__ void __launch_bounds__(kFlipThreads) flip_low_kernel(int sites, int tb, int nd,
+// One pass: tile flips, global-partner flips, diagonal and the epilogue.
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(kFlipThreads) flip_chain_kernel(int sites, int tb, int nd,
                                                                 const uint64_t* __restrict__ masks,
                                                                 const double* __restrict__ coefs,
                                                                 const T* __restrict__ low_table,
@@ -152,53 +149,10 @@ __global__ void __launch_bounds__(kFlipThreads) flip_low_kernel(int sites, int t
       const E xs = tile[j];
       E acc = scaled(d, xs);
       for (int i = 0; i < tb; ++i) acc = scale_add(acc, cx[i], tile[j ^ (1 << i)]);
-      if (FINAL) out[s] = epilogue(acc, xs, p, q, s, alpha, beta, gamma, kr, ki);
-      else out[s] = acc;
+      for (int i = tb; i < sites; ++i) acc = scale_add(acc, cx[i], x[s ^ (1ull << i)]);
+      out[s] = epilogue(acc, xs, p, q, s, alpha, beta, gamma, kr, ki);
     }
   }
-}
-
-// Pass B: flips of bits [tb, sites) on top of pass A's partial sums, then the epilogue.
-template <typename T, bool CPLX>
-__global__ void __launch_bounds__(kFlipThreads) flip_high_kernel(int sites, int tb, int pbits, int mbits,
-                                                                 const double* __restrict__ xcoef,
-                                                                 const typename Elem<T, CPLX>::type* __restrict__ x,
-                                                                 const typename Elem<T, CPLX>::type* __restrict__ partial,
-                                                                 typename Elem<T, CPLX>::type* out,
-                                                                 const typename Elem<T, CPLX>::type* p,
-                                                                 const typename Elem<T, CPLX>::type* q, T alpha,
-                                                                 T beta, T gamma, T kr, T ki) {
-  using E = typename Elem<T, CPLX>::type;
-  extern __shared__ unsigned char smem_raw[];
-  E* tile = reinterpret_cast<E*>(smem_raw);
-  __shared__ T cx[64];
-  if (threadIdx.x < sites) cx[threadIdx.x] = static_cast<T>(xcoef[threadIdx.x]);
-  const int hi0 = sites - mbits;          // first bit held in the tile's high part
-  const int unc = hi0 - tb;               // middle bits read from global memory
-  const int lowmid = tb - pbits;          // tile-id bits that sit between pbits and tb
-  const uint64_t tiles = 1ull << (sites - mbits - pbits);
-  const int count = 1 << (pbits + mbits);
-  const uint64_t lmask = (1ull << pbits) - 1ull;
-  for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    // tile id: the unc middle bits vary fastest, so partner tiles run together
-    const uint64_t mid_unc = t & ((1ull << unc) - 1ull);
-    const uint64_t mid_low = t >> unc;
-    const uint64_t fixed = (mid_low << pbits) | (mid_unc << tb);
-    __syncthreads();
-    for (int e = threadIdx.x; e < count; e += blockDim.x) {
-      const uint64_t s = (static_cast<uint64_t>(e) & lmask) | fixed | (static_cast<uint64_t>(e >> pbits) << hi0);
-      tile[e] = x[s];
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < count; e += blockDim.x) {
-      const uint64_t s = (static_cast<uint64_t>(e) & lmask) | fixed | (static_cast<uint64_t>(e >> pbits) << hi0);
-      E acc = partial[s];
-      for (int m = 0; m < mbits; ++m) acc = scale_add(acc, cx[hi0 + m], tile[e ^ (1 << (pbits + m))]);
-      for (int i = tb; i < hi0; ++i) acc = scale_add(acc, cx[i], x[s ^ (1ull << i)]);
-      out[s] = epilogue(acc, tile[e], p, q, s, alpha, beta, gamma, kr, ki);
-    }
-  }
-  (void)lowmid;
 }
 
 int log2_int(int v) {
@@ -238,26 +192,20 @@ void FlipChain::apply(int precision, bool cplx, const void* x, void* out, const 
   const int esize = (precision == 64 ? 8 : 4) * (cplx ? 2 : 1);
   const int tbits = log2_int(kTileBytes / esize);
   const int tb = std::min(sites_, tbits);
-  const int pbits = log2_int(32 / esize);
-  const bool two_pass = sites_ > tb;
-  const int mbits = two_pass ? std::min(sites_ - tb, tbits - pbits) : 0;
   const uint64_t n = dim();
   int device = 0, sms = 148;
   QMBED_CUDA(cudaGetDevice(&device));
   QMBED_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  // the low-bit diagonal table (2^tb values of the working precision), cached per precision
-  // fixed regions: FP64 table, FP32 table (each at most kTileBytes), then the partial sums
-  const size_t part_bytes = two_pass ? n * esize : 0;
-  const size_t need = 2 * static_cast<size_t>(kTileBytes) + part_bytes;
-  if (partial_bytes_ < need) {
-    partial_.allocate(need);
-    partial_bytes_ = need;
+  // low-bit diagonal tables (2^tb values of the working precision, at most
+  // kTileBytes each): FP64 table first, FP32 table second
+  const size_t need = 2 * static_cast<size_t>(kTileBytes);
+  if (tables_bytes_ < need) {
+    tables_.allocate(need);
+    tables_bytes_ = need;
     tables_ready_ = 0;
   }
   const int table_slot = precision == 64 ? 1 : 2;
-  unsigned char* base = static_cast<unsigned char*>(partial_.get());
-  void* table = base + (precision == 64 ? 0 : kTileBytes);
-  void* partial = base + 2 * static_cast<size_t>(kTileBytes);
+  void* table = static_cast<unsigned char*>(tables_.get()) + (precision == 64 ? 0 : kTileBytes);
   if (!(tables_ready_ & table_slot) || table_tb_[table_slot - 1] != tb) {
     const int blocks = static_cast<int>(std::min<uint64_t>(((1ull << tb) + 255) / 256, 1024));
     if (precision == 64)
@@ -270,40 +218,21 @@ void FlipChain::apply(int precision, bool cplx, const void* x, void* out, const 
     tables_ready_ |= table_slot;
     table_tb_[table_slot - 1] = tb;
   }
-  const size_t smem_a = static_cast<size_t>(esize) << tb;
-  const size_t smem_b = static_cast<size_t>(esize) << (pbits + mbits);
-  const int grid_a = static_cast<int>(std::min<uint64_t>(n >> tb, 3ull * sms));
-  const int grid_b = two_pass ? static_cast<int>(std::min<uint64_t>(1ull << (sites_ - mbits - pbits), 3ull * sms)) : 0;
+  const size_t smem = static_cast<size_t>(esize) << tb;
+  const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(n >> tb, 3ull * sms)));
   auto run = [&](auto ttag, auto ctag) {
     using T = decltype(ttag);
     constexpr bool C = decltype(ctag)::value;
     using E = typename Elem<T, C>::type;
     const T a = static_cast<T>(step.alpha), b = static_cast<T>(step.beta), g = static_cast<T>(step.gamma),
             kr = static_cast<T>(step.kappa_re), ki = static_cast<T>(step.kappa_im);
-    if (two_pass) {
-      auto ka = flip_low_kernel<T, C, false>;
-      QMBED_CUDA(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_a)));
-      ka<<<grid_a, kFlipThreads, smem_a, stream>>>(sites_, tb, n_diag_, diag_masks_.as<uint64_t>(),
-                                                   diag_coefs_.as<double>(), static_cast<const T*>(table),
-                                                   x_coefs_.as<double>(), static_cast<const E*>(x),
-                                                   static_cast<E*>(partial), nullptr, nullptr, a, b, g, kr, ki);
-      QMBED_LAUNCH_CHECK();
-      auto kb = flip_high_kernel<T, C>;
-      QMBED_CUDA(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_b)));
-      kb<<<grid_b, kFlipThreads, smem_b, stream>>>(sites_, tb, pbits, mbits, x_coefs_.as<double>(),
-                                                   static_cast<const E*>(x), static_cast<const E*>(partial),
-                                                   static_cast<E*>(out), static_cast<const E*>(p),
-                                                   static_cast<const E*>(q), a, b, g, kr, ki);
-      QMBED_LAUNCH_CHECK();
-    } else {
-      auto ka = flip_low_kernel<T, C, true>;
-      QMBED_CUDA(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_a)));
-      ka<<<std::max(grid_a, 1), kFlipThreads, smem_a, stream>>>(
-          sites_, tb, n_diag_, diag_masks_.as<uint64_t>(), diag_coefs_.as<double>(), static_cast<const T*>(table),
-          x_coefs_.as<double>(), static_cast<const E*>(x), static_cast<E*>(out), static_cast<const E*>(p),
-          static_cast<const E*>(q), a, b, g, kr, ki);
-      QMBED_LAUNCH_CHECK();
-    }
+    auto kernel = flip_chain_kernel<T, C>;
+    QMBED_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kernel<<<grid, kFlipThreads, smem, stream>>>(sites_, tb, n_diag_, diag_masks_.as<uint64_t>(),
+                                                 diag_coefs_.as<double>(), static_cast<const T*>(table),
+                                                 x_coefs_.as<double>(), static_cast<const E*>(x), static_cast<E*>(out),
+                                                 static_cast<const E*>(p), static_cast<const E*>(q), a, b, g, kr, ki);
+    QMBED_LAUNCH_CHECK();
   };
   if (precision == 64) cplx ? run(double{}, std::true_type{}) : run(double{}, std::false_type{});
   else cplx ? run(float{}, std::true_type{}) : run(float{}, std::false_type{});

@@ -1,8 +1,9 @@
 // Structured action of full-space spin-1/2 chains whose terms are products of
 // z (diagonal) or a single x (one bit flip): transverse-field Ising chains and
 // their relatives. No matrix is stored: the diagonal is evaluated from the bits
-// of the state index, and the flips read the vector through two shared-memory
-// tiled passes (low bits in a contiguous tile, high bits in a strided tile).
+// of the state index, and one pass over shared-memory tiles of consecutive
+// elements serves the low-bit flips from the tile and the high-bit flips from
+// coalesced reads of the partner tiles.
 #pragma once
 
 #include <complex>
@@ -44,8 +45,8 @@ class FlipChain {
   int sites_;
   int n_diag_;
   DeviceBuffer diag_masks_, diag_coefs_, x_coefs_;
-  mutable DeviceBuffer partial_;  // low-bit diagonal tables (both precisions) + pass A partial sums
-  mutable size_t partial_bytes_ = 0;
+  mutable DeviceBuffer tables_;  // low-bit diagonal tables (FP64, FP32)
+  mutable size_t tables_bytes_ = 0;
   mutable int tables_ready_ = 0;  // bit 1: FP64 table, bit 2: FP32 table
   mutable int table_tb_[2] = {0, 0};
   std::vector<double> host_diag_coefs_, host_x_;

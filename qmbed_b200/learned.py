@@ -196,8 +196,15 @@ def lanczos_interval(op: GpuOperator, steps: int = 40, seed: int = 0, margin: fl
 
 
 def propagate(op: GpuOperator, psi0, times, interval: Interval, precision: int = 64, tolerance: float = 1e-10,
-              final_only: bool = False, drift_limit: float = 1e-6):
-    """Chebyshev propagation on `interval`; repeats on the guaranteed bound if the norm drifts."""
+              final_only: bool = False, drift_limit: float | None = None):
+    """Chebyshev propagation on `interval`; repeats on the guaranteed bound if the norm drifts.
+
+    A spectrum that leaves the interval makes the norm grow exponentially with
+    the expansion degree, far beyond rounding: the default limit is 1e-8 of the
+    norm with complex128 vectors and 1e-4 with complex64 (whose rounding over a
+    long trajectory reaches 1e-6)."""
+    if drift_limit is None:
+        drift_limit = 1e-8 if precision == 64 else 1e-4
     states, info = op.chebyshev_evolve(psi0, times, interval.e_min, interval.e_max, tolerance=tolerance,
                                        precision=precision, final_only=final_only)
     info["source"] = interval.source

@@ -30,7 +30,7 @@ def _tfim(engine, sites, g=1.0, seed=0, periodic=False):
 
 @pytest.mark.parametrize("sites,normalization,periodic", [
     (10, "pauli", False), (11, "pauli", True), (12, "angular_momentum", False),
-    (16, "pauli", False),   # two passes with complex128 tiles
+    (16, "pauli", False),   # complex128 tiles of 12 bits: the top bits flip through global partner reads
     (18, "pauli", True),
 ])
 def test_flip_chain_action_matches_oracle(engine, oracle, sites, normalization, periodic):
@@ -49,7 +49,7 @@ def test_flip_chain_action_matches_oracle(engine, oracle, sites, normalization, 
 @pytest.mark.parametrize("precision,complex_vectors", [(32, False), (64, True)])
 def test_flip_chain_large_matches_generic_expansion(engine, precision, complex_vectors):
     import torch
-    sites = 26  # the high pass reads some middle bits from global memory at this size
+    sites = 26  # 12 to 14 bits flip through global partner reads at this size
     g = engine.GpuOperator(engine.GpuBasis(sites, normalization="pauli"), _tfim(engine, sites, seed=5),
                            storage="matrix_free")
     n = g.dim
