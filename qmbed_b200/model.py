@@ -171,6 +171,17 @@ class NativeModel:
         params = {k: [complex(v).real, complex(v).imag] for k, v in (parameters or {}).items()}
         return _vectors_result(self.execute("apply_model", vectors=_vectors_request(vectors), parameters=params))
 
+    def evolve(self, vectors, times, *, krylov_dimension: int = 64, tolerance: float = 1e-10,
+               max_substeps: int = 10_000, parameters: dict[str, complex] | None = None) -> np.ndarray:
+        """exp(-i H t) applied to each column at each time: the evolve_model
+        command (bindings/capi/src/lib.rs:4673-4694). Returns [time][column][component]."""
+        params = {k: [complex(v).real, complex(v).imag] for k, v in (parameters or {}).items()}
+        result = self.execute("evolve_model", vectors=_vectors_request(vectors), parameters=params,
+                              evolution={"times": [float(t) for t in times], "krylov_dimension": krylov_dimension,
+                                         "tolerance": tolerance, "max_substeps": max_substeps})
+        return np.array([[[complex(re, im) for re, im in column] for column in columns]
+                         for columns in result["states"]])
+
     def close(self) -> None:
         if self._handle is None:
             return

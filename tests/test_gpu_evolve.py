@@ -135,3 +135,23 @@ def test_evolve_model_json_anchor(anchors):
     with pytest.raises(QmbedError, match="at least one column"):
         _lib.command({"operation": "evolve_model", "handle": handle, "vectors": [], "evolution": {"times": [1.0]}})
     assert _lib.command({"operation": "release_model", "handle": handle})["kind"] == "released"
+
+
+def test_native_model_evolve(oracle):
+    from qmbed_b200.model import NativeModel
+    bonds = [[i, (i + 1) % 10] for i in range(10)]
+    request = {"basis": {"kind": "spin", "sites": 10, "up": 5, "momentum": 0},
+               "terms": [{"product": {"local": ["z", "z"]},
+                          "couplings": [{"coefficient": [1.0, 0.0], "sites": b} for b in bonds]},
+                         {"product": {"local": ["raising", "lowering"]},
+                          "couplings": [{"coefficient": [0.5, 0.0], "sites": b} for b in bonds]},
+                         {"product": {"local": ["lowering", "raising"]},
+                          "couplings": [{"coefficient": [0.5, 0.0], "sites": b} for b in bonds]}]}
+    o = oracle.Operator.build(oracle.Basis(10, up=5, momentum=0), oracle.heisenberg_terms(10))
+    v = oracle.deterministic_start(o.dim, 3).astype(complex)
+    with NativeModel(request) as model:
+        states = model.evolve([v], [0.5, 1.5], krylov_dimension=30)
+    ref, _ = o.evolve(v, [0.5, 1.5], krylov_dimension=30)
+    assert states.shape == (2, 1, o.dim)
+    for t in range(2):
+        assert np.linalg.norm(states[t][0] - ref[t]) <= 1e-9
