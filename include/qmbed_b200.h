@@ -56,7 +56,8 @@ enum { QMBED_ANGULAR_MOMENTUM = 0, QMBED_PAULI = 1, QMBED_PAULI_CARTESIAN = 2 };
 /* Operator storage on the device. */
 enum {
   QMBED_STORAGE_MATRIX_FREE = 0, /* terms expanded on every application */
-  QMBED_STORAGE_PACKED = 1       /* rows assembled once on the GPU (packed u32 entries when real) */
+  QMBED_STORAGE_PACKED = 1,      /* rows assembled once on the GPU (packed u32 entries when real) */
+  QMBED_STORAGE_EXPLICIT = 2     /* rows assembled once with an explicit FP64 value per entry */
 };
 
 /* Spectral targets (reference SpectrumTarget, src/solve/mod.rs:332-347). */
@@ -227,6 +228,23 @@ QMBED_API int qmbed_gpu_expm_lanczos(qmbed_operator op, const double* initial, d
 QMBED_API int qmbed_gpu_chebyshev_evolve(qmbed_operator op, const double* initial, int n_times, const double* times,
                                          double e_min, double e_max, double tolerance, int precision, int final_only,
                                          double* states, double* info);
+
+/* Lowest eigenvalues of every H(s, p) = sum_k coefficients[p][k] A_k(s) for
+ * n_sectors sectors s and n_points scan points p (<= 64), in one batched
+ * Lanczos run: each launch applies every sector's operator to every point.
+ * components[s * n_components + k] is A_k of sector s, created with
+ * QMBED_STORAGE_EXPLICIT on sector s's basis (all components of a sector share
+ * its basis handle). Plain three-term Lanczos in FP64 per pair (no
+ * reorthogonalisation; copies of converged Ritz values are merged); a pair is
+ * done when its wanted values move less than 1e-3 tolerance max(|E|, 1) in
+ * 10 steps, or when its Krylov space is exhausted. eigenvalues receives
+ * [sector][point][eigenpairs] (eigenpairs <= 4), steps the Lanczos steps per
+ * pair, info (may be NULL) the total steps and the applications summed over
+ * pairs. The reference solves each pair with eigsh (src/solve/mod.rs:
+ * 2335-2350); the batched form has no counterpart there. */
+QMBED_API int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
+                                    const double* coefficients, int eigenpairs, double tolerance, int max_steps,
+                                    uint64_t seed, double* eigenvalues, int* steps, double* info);
 
 /* Extreme Ritz values of a steps-step FP64 Lanczos run without
  * reorthogonalisation from deterministic_start(seed) (src/solve/mod.rs:

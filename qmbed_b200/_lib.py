@@ -112,6 +112,7 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_expm_lanczos.argtypes = [vp, vp, d, u64, vp]
     L.qmbed_gpu_chebyshev_evolve.argtypes = [vp, vp, i, vp, d, d, d, i, i, vp, vp]
     L.qmbed_gpu_lanczos_extremes.argtypes = [vp, i, u64, vp]
+    L.qmbed_gpu_scan_lowest.argtypes = [i, i, vp, i, vp, i, d, i, u64, vp, vp, vp]
     L.qmbed_gpu_mlp_create.argtypes = [i, i, i, i, i, u64, P(vp)]
     L.qmbed_gpu_mlp_destroy.argtypes = [vp]
     L.qmbed_gpu_mlp_parameter_count.argtypes = [vp, P(u64)]

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/qmbed_b200.h"
+#include "batched.cuh"
 #include "chebyshev.cuh"
 #include "eigsh.cuh"
 #include "evolve.cuh"
@@ -835,6 +836,7 @@ int qmbed_gpu_operator_create(qmbed_basis basis, int n_terms, const int* arity, 
     checks.particle_conservation = check_particles != 0;
     auto h = new qmbed_operator_s;
     try {
+      if (storage < 0 || storage > 2) raise(QMBED_INVALID_OPTIONS, "storage must be matrix_free, packed or explicit");
       h->op = std::make_shared<SpinOperator>(basis->basis, terms, checks, storage);
     } catch (...) {
       delete h;
@@ -1049,6 +1051,29 @@ int qmbed_gpu_chebyshev_evolve(qmbed_operator op, const double* initial, int n_t
       info[2] = ci.e_min;
       info[3] = ci.e_max;
       info[4] = ci.max_norm_drift;
+    }
+  });
+}
+
+int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
+                          const double* coefficients, int eigenpairs, double tolerance, int max_steps, uint64_t seed,
+                          double* eigenvalues, int* steps, double* info) {
+  return guarded([&] {
+    if (n_sectors < 1 || n_components < 1 || !components || !coefficients || !eigenvalues || !steps)
+      raise(QMBED_INVALID_OPTIONS, "a scan needs sectors, components, coefficients and outputs");
+    std::vector<std::vector<const SpinOperator*>> comps(static_cast<size_t>(n_sectors));
+    for (int s = 0; s < n_sectors; ++s)
+      for (int k = 0; k < n_components; ++k) comps[s].push_back(components[s * n_components + k]->op.get());
+    qmbed_operator_s& first = *components[0];
+    std::lock_guard<std::mutex> lock(first.mu);
+    QMBED_CUDA(cudaSetDevice(first.op->basis().device()));
+    const ScanResult r = scan_lowest(comps, std::vector<double>(coefficients, coefficients + n_points * n_components),
+                                     n_points, eigenpairs, tolerance, max_steps, seed, first.block_ops());
+    std::copy(r.eigenvalues.begin(), r.eigenvalues.end(), eigenvalues);
+    std::copy(r.steps.begin(), r.steps.end(), steps);
+    if (info) {
+      info[0] = static_cast<double>(r.total_steps);
+      info[1] = static_cast<double>(r.applications);
     }
   });
 }

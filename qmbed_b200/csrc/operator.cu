@@ -1249,6 +1249,19 @@ void SpinOperator::apply_with_scratch(int precision, bool complex_vectors, const
   QMBED_LAUNCH_CHECK();
 }
 
+SpinOperator::ExplicitRows SpinOperator::explicit_rows() const {
+  if (storage_ != kStorageWide) raise(QMBED_UNSUPPORTED_BACKEND, "the operator does not hold rows with explicit values");
+  ExplicitRows r;
+  r.n = dim();
+  r.row_ptr64 = row_ptr64_;
+  r.row_ptr = row_ptr_.get();
+  r.cols = entries_.as<uint32_t>();
+  r.values = values64_.as<double>();
+  r.diag = diag64_.as<double>();
+  r.diag_complex = !real_;
+  return r;
+}
+
 bool SpinOperator::supports_block() const { return real_ && storage_ == kStoragePacked; }
 
 void SpinOperator::launch_block(int shape, int precision, int nb, const void* z, const void* p, void* out,

@@ -97,6 +97,21 @@ class SpinOperator {
   // Index of the shape the autotuner chose, or -1 before the first call.
   int tuned_block_shape(int precision, int nb, bool with_p) const;
 
+  // Rows stored with explicit values (storage kStorageWide), for kernels that
+  // combine several operators on one basis. The values exclude the orbit
+  // factors: in coordinates z = x / sqrt(R) the action is
+  // (S^-1 H S z)_r = sum_e values[e] z[cols[e]] + diag[r] z[r].
+  struct ExplicitRows {
+    uint64_t n = 0;
+    bool row_ptr64 = false;
+    const void* row_ptr = nullptr;
+    const uint32_t* cols = nullptr;
+    const double* values = nullptr;  // interleaved complex FP64, one per entry
+    const double* diag = nullptr;    // FP64: real (n) for real operators, interleaved complex (2n) otherwise
+    bool diag_complex = false;
+  };
+  ExplicitRows explicit_rows() const;
+
   // The structured flip-chain action, when this operator has that form
   // (full space, matrix-free storage, z products and single x flips).
   const FlipChain* flip_chain() const { return flip_.get(); }

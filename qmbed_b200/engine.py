@@ -26,7 +26,7 @@ MODES = {"fp64": 0, "mixed": 1, "filtered": 2}
 EVOLUTION_DIAGNOSTICS = ("lanczos_projections", "matrix_vector_products", "real_lanczos_projections",
                          "real_matrix_vector_products", "accepted_substeps", "rejected_trial_intervals",
                          "maximum_estimated_error")
-STORAGE = {"matrix_free": 0, "packed": 1}
+STORAGE = {"matrix_free": 0, "packed": 1, "explicit": 2}
 
 
 def _ptr(array):
