@@ -96,7 +96,9 @@ __global__ void diag_low_table_kernel(int tb, int nd, const uint64_t* __restrict
 }
 
 // One pass: tile flips, global-partner flips, diagonal and the epilogue.
-template <typename T, bool CPLX>
+// TB > 0 fixes the tile bits at compile time (the tile loop unrolls); TB = 0
+// takes them from `tb` (chains shorter than a tile).
+template <typename T, bool CPLX, int TB>
 __global__ void __launch_bounds__(kFlipThreads) flip_chain_kernel(int sites, int tb, int nd,
                                                                 const uint64_t* __restrict__ masks,
                                                                 const double* __restrict__ coefs,
@@ -148,8 +150,23 @@ __global__ void __launch_bounds__(kFlipThreads) flip_chain_kernel(int sites, int
       for (int k = 0; k < nc; ++k) d += (__popcll(~s & cross_mask[k]) & 1) ? -cross_coef[k] : cross_coef[k];
       const E xs = tile[j];
       E acc = scaled(d, xs);
-      for (int i = 0; i < tb; ++i) acc = scale_add(acc, cx[i], tile[j ^ (1 << i)]);
-      for (int i = tb; i < sites; ++i) acc = scale_add(acc, cx[i], x[s ^ (1ull << i)]);
+      if (TB > 0) {
+#pragma unroll
+        for (int i = 0; i < TB; ++i) acc = scale_add(acc, cx[i], tile[j ^ (1 << i)]);
+      } else {
+        for (int i = 0; i < tb; ++i) acc = scale_add(acc, cx[i], tile[j ^ (1 << i)]);
+      }
+      // high bits: partner elements from global memory, four loads in flight per thread
+      int i = TB > 0 ? TB : tb;
+      for (; i + 4 <= sites; i += 4) {
+        const E y0 = x[s ^ (1ull << i)], y1 = x[s ^ (1ull << (i + 1))];
+        const E y2 = x[s ^ (1ull << (i + 2))], y3 = x[s ^ (1ull << (i + 3))];
+        acc = scale_add(acc, cx[i], y0);
+        acc = scale_add(acc, cx[i + 1], y1);
+        acc = scale_add(acc, cx[i + 2], y2);
+        acc = scale_add(acc, cx[i + 3], y3);
+      }
+      for (; i < sites; ++i) acc = scale_add(acc, cx[i], x[s ^ (1ull << i)]);
       out[s] = epilogue(acc, xs, p, q, s, alpha, beta, gamma, kr, ki);
     }
   }
@@ -226,7 +243,9 @@ void FlipChain::apply(int precision, bool cplx, const void* x, void* out, const 
     using E = typename Elem<T, C>::type;
     const T a = static_cast<T>(step.alpha), b = static_cast<T>(step.beta), g = static_cast<T>(step.gamma),
             kr = static_cast<T>(step.kappa_re), ki = static_cast<T>(step.kappa_im);
-    auto kernel = flip_chain_kernel<T, C>;
+    // the full-tile width for this element size, known at compile time
+    constexpr int kFull = (sizeof(E) == 4) ? 14 : (sizeof(E) == 8 ? 13 : 12);
+    auto kernel = tb == kFull ? flip_chain_kernel<T, C, kFull> : flip_chain_kernel<T, C, 0>;
     QMBED_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     kernel<<<grid, kFlipThreads, smem, stream>>>(sites_, tb, n_diag_, diag_masks_.as<uint64_t>(),
                                                  diag_coefs_.as<double>(), static_cast<const T*>(table),
