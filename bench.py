@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--quench-bounds", default="learned", choices=["learned", "lanczos", "norm"])
     p.add_argument("--xxz-sites", type=int, default=28,
                    help="XXZ plain/mixed/filtered comparison size (0 skips it)")
+    p.add_argument("--ftlm-sites", type=int, default=28,
+                   help="finite-temperature Lanczos size: 8 vectors x 100 steps (0 skips it)")
     p.add_argument("--scan-sites", type=int, default=26,
                    help="batched J1-J2 scan size: every momentum sector x 64 points (0 skips it)")
     return p.parse_args()
@@ -97,6 +99,69 @@ def xxz_section(sites: int, rank: int, local_rank: int) -> dict:
                      "max_rel_error_vs_fp64": float(np.max(np.abs(r.eigenvalues - ref) / np.abs(ref))),
                      "max_residual": float(np.max(r.residuals))}
     out["eigenvalues_fp64"] = ref.tolist()
+    return out
+
+
+def ftlm_section(sites: int, rank: int, local_rank: int, with_cpu: bool, vectors: int = 8,
+                 krylov: int = 100) -> dict:
+    """Finite-temperature Lanczos: `vectors` random start vectors (generated on
+    the GPU) x `krylov` fully reorthogonalised FP64 Lanczos steps on the
+    Heisenberg chain, Sz = 0, k = 0, p = +1; log Z and E at five temperatures."""
+    import torch
+    from qmbed_b200 import engine, lanczos
+
+    betas = [0.1, 0.5, 1.0, 2.0, 4.0]
+    seed = sites + rank
+
+    def operator(L):
+        basis = engine.GpuBasis(L, up=L // 2, momentum=0, parity=1, device=local_rank)
+        return engine.GpuOperator(basis, engine.heisenberg_terms(L, delta=1.0))
+
+    def timed(op, count):
+        lanczos.ftlm_sample(op, 1, betas, 20, seed=seed)  # warm-up (workspaces)
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        out = lanczos.ftlm_sample(op, count, betas, krylov, seed=seed)
+        stop.record()
+        torch.cuda.synchronize()
+        return out, start.elapsed_time(stop) / 1000.0
+
+    op = operator(sites)
+    n = op.dim
+    (logz, energy, lengths), seconds = timed(op, vectors)
+    steps = int(lengths.sum())
+    # algorithmic bytes per step j (FP64 real): overlaps read j+1 columns and w,
+    # the subtraction reads j+1 columns and w and writes w, scaling reads w and
+    # writes q_{j+1}; plus the packed H.v operands
+    panel = sum(sum((2 * (j + 1) + 5) * n * 8 for j in range(int(m))) for m in lengths)
+    hv = steps * op.operand_bytes(64)
+    avg_logz, avg_e = lanczos.ftlm_average(logz, energy)
+    out = {"workload": f"heisenberg L={sites} k=0 p=+1 up={sites // 2} dim={n}, {vectors} Rademacher start "
+                       f"vectors (seed {seed}) x {krylov} Lanczos steps with full DGKS reorthogonalisation, FP64",
+           "s": seconds, "s_per_vector": seconds / vectors, "lanczos_steps": steps,
+           "algorithmic_gbs": (panel + hv) / seconds / 1e9, "bytes_per_vector": (panel + hv) / vectors,
+           "inverse_temperatures": betas, "log_partition": avg_logz.tolist(), "energy_per_site":
+           (avg_e / sites).tolist(), "log_partition_spread": logz.std(axis=0).tolist()}
+    if with_cpu:
+        # the oracle's thermal iteration on the sampler's first start vector at
+        # L=24: parity of log Z and E, and the CPU time per vector
+        sys.path.insert(0, str(ROOT))
+        from oracle import oracle
+        small = 24
+        op24 = operator(small)
+        (lz24, e24, len24), gpu24 = timed(op24, 1)
+        v = lanczos.ftlm_start(op24, 0, seed=seed)
+        ob = oracle.Operator.build(oracle.Basis(small, up=small // 2, momentum=0, parity=1),
+                                   oracle.heisenberg_terms(small, delta=1.0))
+        t0 = time.perf_counter()
+        ref_lz, ref_e, ref_m = ob.thermal_iteration(v, betas, krylov)
+        cpu = time.perf_counter() - t0
+        out["cpu_sample"] = {"workload": f"one vector at L={small} (dim {op24.dim}), {krylov} steps", "cores": 1,
+                             "cpu_s_per_vector": cpu, "gpu_s_per_vector": gpu24,
+                             "max_abs_diff_log_partition": float(np.max(np.abs(lz24[0] - ref_lz))),
+                             "max_abs_diff_energy": float(np.max(np.abs(e24[0] - ref_e))),
+                             "krylov": [int(len24[0]), int(ref_m)]}
     return out
 
 
@@ -492,6 +557,9 @@ def main():
     if args.quench_sites > 0:
         quench_result = quench(args.quench_sites, args.quench_bounds, rank, local_rank)
     xxz_result = xxz_section(args.xxz_sites, rank, local_rank) if args.xxz_sites > 0 else None
+    ftlm_result = None
+    if args.ftlm_sites > 0:
+        ftlm_result = ftlm_section(args.ftlm_sites, rank, local_rank, rank == 0 and world == 1 and not args.no_cpu)
     scan_result = None
     if args.scan_sites > 0:
         scan_result = scan_section(args.scan_sites, rank, local_rank, rank == 0 and world == 1 and not args.no_cpu)
@@ -520,6 +588,7 @@ def main():
             "quench": quench_result,
             "scan": scan_result,
             "xxz": xxz_result,
+            "ftlm": ftlm_result,
             "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved_top,
                          "peak": peak, "unit": "GB/s", "frac": achieved_top / peak, "traffic": traffic,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "_fallback" not in peaks

@@ -283,6 +283,78 @@ QMBED_API int qmbed_gpu_mlp_train(qmbed_mlp mlp, const float* X, const float* Y,
                                   float learning_rate, uint64_t seed, float* loss);
 QMBED_API int qmbed_gpu_mlp_predict(qmbed_mlp mlp, const float* X, int n, float* Y);
 
+/* ---- Full Lanczos decompositions and thermal Lanczos (FTLM / LTLM) ------ */
+/* A device-resident lanczos_ritz decomposition (src/solve/mod.rs:2818-2857;
+ * the JSON "lanczos_operator" command, bindings/capi/src/lib.rs:4046-4075):
+ * the fully reorthogonalised Krylov basis of op from `initial` (dim complex
+ * values), kept in HBM, with its tridiagonal and ascending Ritz system. The
+ * recurrence stops after krylov_dimension vectors, when beta <= tolerance, or
+ * when the basis spans the operator's whole space. Krylov dimensions above
+ * 8192 answer QMBED_STATUS_UNSUPPORTED_BACKEND. */
+typedef struct qmbed_lanczos_s* qmbed_lanczos;
+QMBED_API int qmbed_gpu_lanczos_create(qmbed_operator op, const double* initial, uint64_t krylov_dimension,
+                                       double tolerance, qmbed_lanczos* out);
+/* release_lanczos (bindings/capi/src/lib.rs:1874-1886) */
+QMBED_API int qmbed_gpu_lanczos_destroy(qmbed_lanczos lanczos);
+/* dimension, Krylov length, initial norm, whether the basis is stored real,
+ * and the DGKS second passes taken (any pointer may be NULL). */
+QMBED_API int qmbed_gpu_lanczos_info(qmbed_lanczos lanczos, uint64_t* dimension, uint64_t* krylov_dimension,
+                                     double* initial_norm, int* is_real, uint64_t* second_passes);
+/* Ritz values (ascending), column-oriented eigenvectors (vectors[c * m + r] is
+ * row r of the eigenvector of values[c]), diagonal and off-diagonal of the
+ * tridiagonal (m - 1 values); any pointer may be NULL. */
+QMBED_API int qmbed_gpu_lanczos_ritz(qmbed_lanczos lanczos, double* values, double* vectors, double* diagonal,
+                                     double* off_diagonal);
+/* command_export_lanczos_basis (bindings/capi/src/lib.rs:4293-4310): m x dim complex. */
+QMBED_API int qmbed_gpu_lanczos_basis(qmbed_lanczos lanczos, double* basis);
+/* LanczosRitzDecomposition::linear_combination (src/solve/mod.rs:2636-2638,
+ * linear_combination_qt 3917-3940): out = sum_b coefficients[b] q_b. */
+QMBED_API int qmbed_gpu_lanczos_combine(qmbed_lanczos lanczos, const double* coefficients, double* out);
+/* LanczosRitzDecomposition::exponential_action (src/solve/mod.rs:2642-2671):
+ * out = |v| Q exp(c T) e_1. */
+QMBED_API int qmbed_gpu_lanczos_exponential(qmbed_lanczos lanczos, double coefficient_re, double coefficient_im,
+                                            double* out);
+/* thermal_observable_iteration (src/solve/mod.rs:3858-3872): observables
+ * (operators on the same space) projected on the GPU and contracted with the
+ * Ritz system; method 0 = FTLM, 1 = LTLM. values[o * n_betas + b] (complex),
+ * identity[b]. */
+QMBED_API int qmbed_gpu_lanczos_thermal(qmbed_lanczos lanczos, int method, int n_betas, const double* betas,
+                                        int n_observables, const qmbed_operator* observables, double* values,
+                                        double* identity);
+/* LanczosRitzDecomposition::project_thermal_observables for one observable
+ * (src/solve/mod.rs:3813-3856), on the GPU: FTLM (method 0) writes the m
+ * overlaps <q_i|A|q_0>, LTLM (method 1) the m x m values <q_j|A|q_i> at
+ * i * m + j (complex). */
+QMBED_API int qmbed_gpu_lanczos_project(qmbed_lanczos lanczos, int method, qmbed_operator observable,
+                                        double* matrix_elements);
+/* thermal_observable_contraction (src/solve/mod.rs:3785-3806) on host data,
+ * with the eigenvector matrix row-major (eigenvectors[r * m + c] = row r of
+ * the eigenvector of eigenvalues[c]) as the JSON "lanczos_thermal" command
+ * takes it (bindings/capi/src/lib.rs:4214-4237). matrix_elements holds the
+ * n_observables projections back to back (m or m * m complex values each). */
+QMBED_API int qmbed_gpu_thermal_contraction(int method, int m, const double* eigenvalues, const double* eigenvectors,
+                                            int n_observables, const double* matrix_elements, int n_betas,
+                                            const double* betas, double* values, double* identity);
+/* ftlm_static_iteration / ltlm_static_iteration (src/solve/mod.rs:3543-3568,
+ * thermal_lanczos_iteration 3464-3540): log Z and the mean energy at each
+ * inverse temperature from one start vector; krylov_out (may be NULL)
+ * receives the Krylov length. */
+QMBED_API int qmbed_gpu_thermal_iteration(qmbed_operator op, const double* initial, int n_betas, const double* betas,
+                                          uint64_t krylov_dimension, double tolerance, double* log_partition,
+                                          double* mean_energy, uint64_t* krylov_out);
+/* n_vectors FTLM iterations from random start vectors generated on the GPU
+ * (Rademacher +-1 entries for real operators, unit phases for complex ones,
+ * keyed by seed and the vector index): log_partition and mean_energy
+ * [vector][beta], lengths[vector] the Krylov lengths (may be NULL). The
+ * reference takes each start vector from its caller; the device sampler has
+ * no counterpart there. */
+/* Start vector `index` of qmbed_gpu_ftlm_sample for `seed` (dim complex
+ * values), so that a run can be repeated from the host. */
+QMBED_API int qmbed_gpu_ftlm_start(qmbed_operator op, uint64_t seed, int index, double* out);
+QMBED_API int qmbed_gpu_ftlm_sample(qmbed_operator op, int n_vectors, uint64_t seed, int n_betas, const double* betas,
+                                    uint64_t krylov_dimension, double tolerance, double* log_partition,
+                                    double* mean_energy, int* lengths);
+
 /* deterministic_start (src/solve/mod.rs:729-742): normalised LCG vector. */
 QMBED_API int qmbed_gpu_deterministic_start(int device, uint64_t n, uint64_t seed, double* out);
 

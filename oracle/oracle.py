@@ -81,6 +81,9 @@ def lib() -> ctypes.CDLL:
         L.oracle_tridiagonal_eigen.argtypes = [ll, vp, vp, vp, vp]
         L.oracle_evolve.argtypes = [vp, vp, ll, vp, ll, d, ll, vp, vp]
         L.oracle_expm_lanczos.argtypes = [vp, vp, d, ll, vp]
+        L.oracle_lanczos_ritz.argtypes = [vp, vp, ll, d, P(ll), P(d), vp, vp, vp, vp, vp]
+        L.oracle_thermal_iteration.argtypes = [vp, vp, ll, vp, ll, d, vp, vp, P(ll)]
+        L.oracle_thermal_observables.argtypes = [vp, vp, ll, d, i, ll, vp, ll, vp, vp, vp]
         _LIB = L
     return _LIB
 
@@ -295,6 +298,50 @@ class Operator:
         y = np.zeros(self.dim, np.complex128)
         _check(lib().oracle_expm_lanczos(self.handle, _ptr(x), time, krylov_dimension, _ptr(y)))
         return y
+
+
+    def lanczos_ritz(self, initial, krylov_dimension: int, tolerance: float = 1e-12):
+        """Full reorthogonalised Lanczos decomposition and its sorted Ritz system
+        (lanczos_ritz, src/solve/mod.rs:2818-2857). Returns a dict with basis
+        [m, dim], diagonal, off_diagonal, initial_norm, values and vectors
+        (vectors[:, c] is the eigenvector of values[c])."""
+        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        k = max(int(krylov_dimension), 0)
+        basis = np.zeros((max(k, 1), self.dim), np.complex128)
+        diag, off, values = np.zeros(max(k, 1)), np.zeros(max(k, 1)), np.zeros(max(k, 1))
+        vectors = np.zeros(max(k, 1) ** 2)
+        size, norm = ctypes.c_longlong(), ctypes.c_double()
+        _check(lib().oracle_lanczos_ritz(self.handle, _ptr(x), krylov_dimension, tolerance, ctypes.byref(size),
+                                         ctypes.byref(norm), _ptr(basis), _ptr(diag), _ptr(off), _ptr(values),
+                                         _ptr(vectors)))
+        m = size.value
+        return {"basis": basis[:m], "diagonal": diag[:m], "off_diagonal": off[:max(m - 1, 0)],
+                "initial_norm": norm.value, "values": values[:m],
+                "vectors": vectors[:m * m].reshape(m, m).T.copy()}
+
+    def thermal_iteration(self, initial, inverse_temperatures, krylov_dimension: int, tolerance: float = 1e-12):
+        """ftlm_static_iteration (src/solve/mod.rs:3543-3554): (log_partition, mean_energy, krylov_dimension)."""
+        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        b = np.ascontiguousarray(np.atleast_1d(np.asarray(inverse_temperatures, np.float64)))
+        lz, e = np.zeros(max(len(b), 1)), np.zeros(max(len(b), 1))
+        size = ctypes.c_longlong()
+        _check(lib().oracle_thermal_iteration(self.handle, _ptr(x), len(b), _ptr(b), krylov_dimension, tolerance,
+                                              _ptr(lz), _ptr(e), ctypes.byref(size)))
+        return lz[:len(b)], e[:len(b)], size.value
+
+    def thermal_observables(self, initial, observables, inverse_temperatures, krylov_dimension: int,
+                            tolerance: float = 1e-12, method: str = "ftlm"):
+        """ftlm_/ltlm_observable_iteration (src/solve/mod.rs:3858-3898):
+        (values[n_observables, n_betas] complex, identity[n_betas])."""
+        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        b = np.ascontiguousarray(np.atleast_1d(np.asarray(inverse_temperatures, np.float64)))
+        handles = (ctypes.c_void_p * max(len(observables), 1))(*[o.handle for o in observables])
+        values = np.zeros((max(len(observables), 1), max(len(b), 1)), np.complex128)
+        identity = np.zeros(max(len(b), 1))
+        _check(lib().oracle_thermal_observables(self.handle, _ptr(x), krylov_dimension, tolerance,
+                                                {"ftlm": 0, "ltlm": 1}[method], len(observables), handles, len(b),
+                                                _ptr(b), _ptr(values), _ptr(identity)))
+        return values[:len(observables), :len(b)], identity[:len(b)]
 
 
 EVOLUTION_DIAGNOSTICS = ("lanczos_projections", "matrix_vector_products", "real_lanczos_projections",

@@ -1777,6 +1777,219 @@ std::vector<std::vector<C64>> evolve_adaptive(const Operator& op, const std::vec
 }
 
 // ----------------------------------------------------------------------------
+// Full Lanczos decomposition and thermal Lanczos (src/solve/mod.rs:2674-2857
+// lanczos_iter / lanczos_full / lanczos_ritz, 3457-3568 thermal static
+// iteration, 3575-3940 projected observables and FTLM/LTLM contractions).
+// Complex arithmetic throughout, like the reference.
+// ----------------------------------------------------------------------------
+struct LanczosFull {
+  double initial_norm = 0.0;
+  std::vector<std::vector<C64>> basis;
+  std::vector<double> diagonal, off_diagonal;
+};
+
+// LanczosOptions::validate (src/solve/mod.rs:2590-2597)
+void validate_lanczos(size_t krylov, double tolerance) {
+  if (krylov == 0 || !std::isfinite(tolerance) || tolerance <= 0.0)
+    fail(ERR_INVALID_OPTIONS, "Lanczos dimension and tolerance must be positive");
+}
+
+C64 cinner(const std::vector<C64>& a, const std::vector<C64>& b) {
+  C64 s(0.0, 0.0);
+  for (size_t i = 0; i < a.size(); ++i) s += std::conj(a[i]) * b[i];
+  return s;
+}
+
+// lanczos_full over LanczosIter::next (src/solve/mod.rs:2694-2813): three-term
+// step, then modified Gram-Schmidt against every earlier vector and the
+// current one, repeated once when the norm fell to 1/sqrt(2) of its value
+// before (DGKS); stops after `krylov` vectors or when beta <= tolerance.
+LanczosFull lanczos_full(const Operator& op, const std::vector<C64>& initial, size_t krylov, double tolerance) {
+  validate_lanczos(krylov, tolerance);
+  if (op.rows != op.cols || initial.size() != op.rows)
+    fail(ERR_DIMENSION_MISMATCH, "Lanczos operator and initial vector do not match");
+  LanczosFull f;
+  f.initial_norm = cnorm(initial);
+  if (!std::isfinite(f.initial_norm) || f.initial_norm <= EPS) fail(ERR_NON_CONVERGENCE, "initial vector is zero");
+  std::vector<C64> current = initial, previous, applied(initial.size());
+  for (C64& x : current) x /= f.initial_norm;
+  double previous_beta = 0.0;
+  std::vector<double> betas;
+  for (size_t index = 0; index < krylov; ++index) {
+    op.apply(current.data(), applied.data());
+    const C64 alpha = cinner(current, applied);
+    if (std::fabs(alpha.imag()) > std::max(tolerance, 1.0e-10)) fail(ERR_NON_HERMITIAN, "");
+    for (size_t i = 0; i < applied.size(); ++i) applied[i] -= alpha.real() * current[i];
+    if (!previous.empty())
+      for (size_t i = 0; i < applied.size(); ++i) applied[i] -= previous_beta * previous[i];
+    auto sweep = [&] {
+      for (size_t b = 0; b <= f.basis.size(); ++b) {
+        const std::vector<C64>& q = b < f.basis.size() ? f.basis[b] : current;
+        const C64 c = cinner(q, applied);
+        for (size_t i = 0; i < applied.size(); ++i) applied[i] -= c * q[i];
+      }
+    };
+    const double before = cnorm(applied);
+    sweep();
+    if (before > EPS && cnorm(applied) <= DGKS_THRESHOLD * before) sweep();
+    const double beta = cnorm(applied);
+    f.diagonal.push_back(alpha.real());
+    betas.push_back(beta);
+    f.basis.push_back(current);
+    if (index + 1 < krylov && beta > tolerance) {
+      for (C64& x : applied) x /= beta;
+      previous = current;
+      current = applied;
+      previous_beta = beta;
+    } else {
+      break;
+    }
+  }
+  f.off_diagonal.assign(betas.begin(), betas.end() - 1);
+  return f;
+}
+
+// lanczos_ritz (src/solve/mod.rs:2818-2857): ascending Ritz values and the
+// eigenvectors of the tridiagonal, vectors[column][row].
+struct LanczosRitz {
+  LanczosFull d;
+  std::vector<double> values;
+  std::vector<std::vector<double>> vectors;
+};
+
+LanczosRitz lanczos_ritz(const Operator& op, const std::vector<C64>& initial, size_t krylov, double tolerance) {
+  LanczosRitz r;
+  r.d = lanczos_full(op, initial, krylov, tolerance);
+  const size_t m = r.d.diagonal.size();
+  std::vector<double> w, z;
+  tridiagonal_eigen(m, r.d.diagonal, r.d.off_diagonal, w, z);
+  std::vector<size_t> order(m);
+  for (size_t i = 0; i < m; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return w[a] < w[b]; });
+  for (size_t c : order) {
+    r.values.push_back(w[c]);
+    r.vectors.emplace_back(z.begin() + static_cast<long>(m * c), z.begin() + static_cast<long>(m * (c + 1)));
+  }
+  return r;
+}
+
+void validate_inverse_temperatures(const std::vector<double>& betas, bool nonnegative) {
+  bool ok = !betas.empty();
+  for (double b : betas) ok = ok && std::isfinite(b) && (!nonnegative || b >= 0.0);
+  if (!ok) fail(ERR_INVALID_OPTIONS, "inverse temperatures must be nonempty, finite, and nonnegative");
+}
+
+// thermal_lanczos_iteration (src/solve/mod.rs:3464-3540), shared by
+// ftlm_static_iteration and ltlm_static_iteration (3543-3568):
+// weights |v|^2 V[0,i]^2, log Z = ln(D / |v|^2) - beta E_min + ln sum w e^{-beta (E - E_min)}.
+void thermal_iteration(const Operator& op, const std::vector<C64>& initial, const std::vector<double>& betas,
+                       size_t krylov, double tolerance, std::vector<double>& log_partition,
+                       std::vector<double>& mean_energy, size_t& size) {
+  validate_lanczos(krylov, tolerance);
+  validate_inverse_temperatures(betas, true);
+  const LanczosRitz r = lanczos_ritz(op, initial, krylov, tolerance);
+  size = r.values.size();
+  const double norm_sq = r.d.initial_norm * r.d.initial_norm;
+  std::vector<double> weights(size);
+  double e_min = INFINITY;
+  for (size_t i = 0; i < size; ++i) {
+    weights[i] = norm_sq * r.vectors[i][0] * r.vectors[i][0];
+    e_min = std::min(e_min, r.values[i]);
+  }
+  log_partition.clear();
+  mean_energy.clear();
+  for (double beta : betas) {
+    double z = 0.0, e = 0.0;
+    for (size_t i = 0; i < size; ++i) {
+      const double b = weights[i] * std::exp(-beta * (r.values[i] - e_min));
+      z += b;
+      e += b * r.values[i];
+    }
+    if (z <= EPS) fail(ERR_NON_CONVERGENCE, "projected partition function vanished");
+    log_partition.push_back(std::log(static_cast<double>(op.rows) / norm_sq) - beta * e_min + std::log(z));
+    mean_energy.push_back(e / z);
+  }
+}
+
+// project_thermal_observables (src/solve/mod.rs:3813-3856): FTLM keeps
+// <q_i|A|q_0>; LTLM keeps <q_j|A|q_i> at i * m + j.
+std::vector<C64> project_observable(const LanczosRitz& r, const Operator& a, bool ltlm) {
+  const size_t m = r.d.basis.size();
+  if (m == 0 || a.rows != r.d.basis[0].size() || a.cols != a.rows)
+    fail(ERR_DIMENSION_MISMATCH, "thermal observables require unique names and matching square shapes");
+  std::vector<C64> out, applied(a.rows);
+  for (size_t input = 0; input < (ltlm ? m : 1); ++input) {
+    a.apply(r.d.basis[input].data(), applied.data());
+    for (size_t bra = 0; bra < m; ++bra) out.push_back(cinner(r.d.basis[bra], applied));
+  }
+  return out;
+}
+
+// ftlm_projected_contraction (src/solve/mod.rs:3646-3694): values[o][b] and identity[b].
+void ftlm_contraction(const LanczosRitz& r, const std::vector<std::vector<C64>>& projected,
+                      const std::vector<double>& betas, std::vector<std::vector<C64>>& values,
+                      std::vector<double>& identity) {
+  const size_t m = r.values.size();
+  values.assign(projected.size(), {});
+  identity.clear();
+  for (double beta : betas) {
+    std::vector<double> coefficient(m, 0.0);
+    for (size_t row = 0; row < m; ++row)
+      for (size_t e = 0; e < m; ++e)
+        coefficient[row] += r.vectors[e][row] * r.vectors[e][0] * std::exp(-beta * r.values[e]);
+    identity.push_back(coefficient[0]);
+    for (size_t o = 0; o < projected.size(); ++o) {
+      C64 s(0.0, 0.0);
+      for (size_t row = 0; row < m; ++row) s += projected[o][row] * coefficient[row];
+      values[o].push_back(s);
+    }
+  }
+}
+
+// ltlm_effective_dimension and ltlm_projected_contraction (src/solve/mod.rs:3696-3778)
+void ltlm_contraction(const LanczosRitz& r, const std::vector<std::vector<C64>>& projected,
+                      const std::vector<double>& betas, std::vector<std::vector<C64>>& values,
+                      std::vector<double>& identity) {
+  const size_t full = r.values.size();
+  double beta_min = INFINITY, first_max = 0.0;
+  for (double b : betas) beta_min = std::min(beta_min, b);
+  for (const auto& v : r.vectors) first_max = std::max(first_max, std::fabs(v[0]));
+  size_t m = full;
+  for (size_t e = 0; e < full; ++e)
+    if (std::exp(-r.values[e] * beta_min) * first_max < EPS) {
+      m = e;
+      break;
+    }
+  if (m == 0) fail(ERR_NON_CONVERGENCE, "no Ritz state carries Boltzmann weight");
+  identity.clear();
+  for (double beta : betas) {
+    double s = 0.0;
+    for (size_t e = 0; e < m; ++e) s += r.vectors[e][0] * r.vectors[e][0] * std::exp(-beta * r.values[e]);
+    identity.push_back(s);
+  }
+  values.assign(projected.size(), {});
+  for (size_t o = 0; o < projected.size(); ++o) {
+    std::vector<C64> t(m * m, C64(0.0, 0.0));
+    for (size_t left = 0; left < m; ++left)
+      for (size_t right = 0; right < m; ++right) {
+        C64 s(0.0, 0.0);
+        for (size_t in = 0; in < m; ++in)
+          for (size_t bra = 0; bra < m; ++bra)
+            s += r.vectors[left][in] * projected[o][in * full + bra] * r.vectors[right][bra];
+        t[left * m + right] = s;
+      }
+    for (double beta : betas) {
+      std::vector<double> w(m);
+      for (size_t e = 0; e < m; ++e) w[e] = r.vectors[e][0] * std::exp(-0.5 * beta * r.values[e]);
+      C64 s(0.0, 0.0);
+      for (size_t left = 0; left < m; ++left)
+        for (size_t right = 0; right < m; ++right) s += w[left] * t[left * m + right] * w[right];
+      values[o].push_back(s);
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
 // C ABI used by the tests (ctypes).
 // ----------------------------------------------------------------------------
 thread_local std::string g_last_error;
@@ -2053,6 +2266,85 @@ int oracle_tridiagonal_eigen(long long n, const double* diag, const double* off,
     tridiagonal_eigen(static_cast<size_t>(n), d, e, w, z);
     for (long long i = 0; i < n; ++i) values[i] = w[static_cast<size_t>(i)];
     for (long long i = 0; i < n * n; ++i) vectors[i] = z[static_cast<size_t>(i)];
+  });
+}
+
+// lanczos_ritz (src/solve/mod.rs:2818-2857). Outputs sized for `krylov`
+// vectors: basis[krylov][dim] interleaved complex, diagonal[krylov],
+// off_diagonal[krylov - 1], values[krylov], vectors[krylov * krylov] with
+// vectors[column * size + row]; *size receives the decomposition length.
+int oracle_lanczos_ritz(void* handle, const double* initial, long long krylov, double tolerance, long long* size,
+                        double* initial_norm, double* basis, double* diagonal, double* off_diagonal, double* values,
+                        double* vectors) {
+  return guarded([&] {
+    const Operator& op = *static_cast<Operator*>(handle);
+    std::vector<C64> v(op.rows);
+    for (size_t i = 0; i < op.rows; ++i) v[i] = C64(initial[2 * i], initial[2 * i + 1]);
+    const LanczosRitz r = lanczos_ritz(op, v, static_cast<size_t>(std::max(krylov, 0LL)), tolerance);
+    const size_t m = r.values.size();
+    *size = static_cast<long long>(m);
+    *initial_norm = r.d.initial_norm;
+    for (size_t b = 0; b < m; ++b) {
+      for (size_t i = 0; i < op.rows; ++i) {
+        basis[2 * (b * op.rows + i)] = r.d.basis[b][i].real();
+        basis[2 * (b * op.rows + i) + 1] = r.d.basis[b][i].imag();
+      }
+      diagonal[b] = r.d.diagonal[b];
+      if (b + 1 < m) off_diagonal[b] = r.d.off_diagonal[b];
+      values[b] = r.values[b];
+      for (size_t row = 0; row < m; ++row) vectors[b * m + row] = r.vectors[b][row];
+    }
+  });
+}
+
+// ftlm_static_iteration / ltlm_static_iteration (src/solve/mod.rs:3543-3568)
+int oracle_thermal_iteration(void* handle, const double* initial, long long n_betas, const double* betas,
+                             long long krylov, double tolerance, double* log_partition, double* mean_energy,
+                             long long* size) {
+  return guarded([&] {
+    const Operator& op = *static_cast<Operator*>(handle);
+    std::vector<C64> v(op.rows);
+    for (size_t i = 0; i < op.rows; ++i) v[i] = C64(initial[2 * i], initial[2 * i + 1]);
+    std::vector<double> lz, e;
+    size_t m = 0;
+    thermal_iteration(op, v, std::vector<double>(betas, betas + std::max(n_betas, 0LL)),
+                      static_cast<size_t>(std::max(krylov, 0LL)), tolerance, lz, e, m);
+    for (size_t b = 0; b < lz.size(); ++b) {
+      log_partition[b] = lz[b];
+      mean_energy[b] = e[b];
+    }
+    *size = static_cast<long long>(m);
+  });
+}
+
+// ftlm_observable_iteration / ltlm_observable_iteration (src/solve/mod.rs:3858-3898):
+// method 0 FTLM, 1 LTLM; values[o][b] interleaved complex, identity[b].
+int oracle_thermal_observables(void* handle, const double* initial, long long krylov, double tolerance, int method,
+                               long long n_observables, void* const* observables, long long n_betas,
+                               const double* betas, double* values, double* identity) {
+  return guarded([&] {
+    const Operator& op = *static_cast<Operator*>(handle);
+    std::vector<C64> v(op.rows);
+    for (size_t i = 0; i < op.rows; ++i) v[i] = C64(initial[2 * i], initial[2 * i + 1]);
+    const LanczosRitz r = lanczos_ritz(op, v, static_cast<size_t>(std::max(krylov, 0LL)), tolerance);
+    if (n_observables <= 0) fail(ERR_INVALID_OPTIONS, "thermal observables must be nonempty");
+    std::vector<double> grid(betas, betas + std::max(n_betas, 0LL));
+    validate_inverse_temperatures(grid, false);
+    std::vector<std::vector<C64>> projected;
+    for (long long o = 0; o < n_observables; ++o)
+      projected.push_back(project_observable(r, *static_cast<const Operator*>(observables[o]), method == 1));
+    std::vector<std::vector<C64>> out;
+    std::vector<double> id;
+    if (method == 1)
+      ltlm_contraction(r, projected, grid, out, id);
+    else
+      ftlm_contraction(r, projected, grid, out, id);
+    for (size_t o = 0; o < out.size(); ++o)
+      for (size_t b = 0; b < grid.size(); ++b) {
+        values[2 * (o * grid.size() + b)] = out[o][b].real();
+        values[2 * (o * grid.size() + b) + 1] = out[o][b].imag();
+      }
+    for (size_t b = 0; b < grid.size(); ++b) identity[b] = id[b];
   });
 }
 

@@ -113,6 +113,19 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_chebyshev_evolve.argtypes = [vp, vp, i, vp, d, d, d, i, i, vp, vp]
     L.qmbed_gpu_lanczos_extremes.argtypes = [vp, i, u64, vp]
     L.qmbed_gpu_scan_lowest.argtypes = [i, i, vp, i, vp, i, d, i, u64, vp, vp, vp]
+    L.qmbed_gpu_lanczos_create.argtypes = [vp, vp, u64, d, P(vp)]
+    L.qmbed_gpu_lanczos_destroy.argtypes = [vp]
+    L.qmbed_gpu_lanczos_info.argtypes = [vp, P(u64), P(u64), P(d), P(i), P(u64)]
+    L.qmbed_gpu_lanczos_ritz.argtypes = [vp, vp, vp, vp, vp]
+    L.qmbed_gpu_lanczos_basis.argtypes = [vp, vp]
+    L.qmbed_gpu_lanczos_combine.argtypes = [vp, vp, vp]
+    L.qmbed_gpu_lanczos_exponential.argtypes = [vp, d, d, vp]
+    L.qmbed_gpu_lanczos_thermal.argtypes = [vp, i, i, vp, i, vp, vp, vp]
+    L.qmbed_gpu_lanczos_project.argtypes = [vp, i, vp, vp]
+    L.qmbed_gpu_thermal_contraction.argtypes = [i, i, vp, vp, i, vp, i, vp, vp, vp]
+    L.qmbed_gpu_thermal_iteration.argtypes = [vp, vp, i, vp, u64, d, vp, vp, P(u64)]
+    L.qmbed_gpu_ftlm_start.argtypes = [vp, u64, i, vp]
+    L.qmbed_gpu_ftlm_sample.argtypes = [vp, i, u64, i, vp, u64, d, vp, vp, vp]
     L.qmbed_gpu_mlp_create.argtypes = [i, i, i, i, i, u64, P(vp)]
     L.qmbed_gpu_mlp_destroy.argtypes = [vp]
     L.qmbed_gpu_mlp_parameter_count.argtypes = [vp, P(u64)]

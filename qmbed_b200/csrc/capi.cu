@@ -23,6 +23,7 @@
 #include "json.hpp"
 #include "mlp.cuh"
 #include "operator.cuh"
+#include "thermal.cuh"
 
 namespace qmbed {
 
@@ -101,6 +102,53 @@ struct qmbed_operator_s {
     return v;
   }
 };
+
+struct qmbed_lanczos_s {
+  LanczosDecomposition d;
+  cudaStream_t stream = nullptr;
+  std::unique_ptr<BlockOps> ops;
+  std::mutex mu;
+  ~qmbed_lanczos_s() {
+    ops.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
+  BlockOps& block_ops() {
+    if (!ops) {
+      QMBED_CUDA(cudaSetDevice(d.device));
+      QMBED_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+      ops = std::make_unique<BlockOps>(d.device, stream);
+    }
+    return *ops;
+  }
+};
+
+namespace {
+
+// Host copy of a device column set, widened to interleaved complex.
+std::vector<double> lanczos_column_host(const LanczosDecomposition& d, int j) {
+  std::vector<double> out(2 * d.n, 0.0);
+  if (d.real) {
+    std::vector<double> re(d.n);
+    QMBED_CUDA(cudaMemcpy(re.data(), d.column(j), d.n * 8, cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < d.n; ++i) out[2 * i] = re[i];
+  } else {
+    QMBED_CUDA(cudaMemcpy(out.data(), d.column(j), d.n * 16, cudaMemcpyDeviceToHost));
+  }
+  return out;
+}
+
+void lanczos_vector_out(qmbed_lanczos_s& l, const std::vector<C64>& c, double* out) {
+  DeviceBuffer result(l.d.n * 16);
+  lanczos_combine(l.d, c, result.as<double>(), l.block_ops());
+  QMBED_CUDA(cudaMemcpy(out, result.get(), l.d.n * 16, cudaMemcpyDeviceToHost));
+}
+
+std::vector<double> beta_grid(int n_betas, const double* betas) {
+  if (n_betas < 0 || (n_betas > 0 && !betas)) raise(QMBED_INVALID_OPTIONS, "inverse temperatures must be nonempty");
+  return std::vector<double>(betas, betas + n_betas);
+}
+
+}  // namespace
 
 namespace {
 
@@ -429,6 +477,8 @@ std::mutex g_registry_mu;
 std::map<uint64_t, std::shared_ptr<Model>> g_models;
 std::map<uint64_t, std::shared_ptr<ExpmEntry>> g_expm;
 std::atomic<uint64_t> g_next_model{1}, g_next_expm{1};
+std::map<uint64_t, std::shared_ptr<qmbed_lanczos_s>> g_lanczos;
+std::atomic<uint64_t> g_next_lanczos{1};
 
 uint64_t parse_handle(const std::string& text, const char* what) {
   char* end = nullptr;
@@ -451,6 +501,26 @@ std::shared_ptr<ExpmEntry> registered_expm(const std::string& text) {
   std::lock_guard<std::mutex> lock(g_registry_mu);
   auto it = g_expm.find(id);
   if (it == g_expm.end()) raise(QMBED_INVALID_OPTIONS, "exponential-action handle " + text + " is not registered");
+  return it->second;
+}
+
+// parse_lanczos_handle / registered_lanczos (bindings/capi/src/lib.rs:1672-1872):
+// "lanczos:<positive integer>".
+uint64_t parse_lanczos_handle(const std::string& text) {
+  if (text.rfind("lanczos:", 0) != 0)
+    raise(QMBED_INVALID_OPTIONS, "Lanczos handle \"" + text + "\" does not use the lanczos: prefix");
+  const std::string digits = text.substr(8);
+  char* end = nullptr;
+  const unsigned long long value = std::strtoull(digits.c_str(), &end, 10);
+  if (digits.empty() || !end || *end != '\0') raise(QMBED_INVALID_OPTIONS, "Lanczos handle \"" + text + "\" is invalid");
+  return value;
+}
+
+std::shared_ptr<qmbed_lanczos_s> registered_lanczos(const std::string& text) {
+  const uint64_t id = parse_lanczos_handle(text);
+  std::lock_guard<std::mutex> lock(g_registry_mu);
+  auto it = g_lanczos.find(id);
+  if (it == g_lanczos.end()) raise(QMBED_INVALID_OPTIONS, "Lanczos handle " + text + " is not registered");
   return it->second;
 }
 
@@ -537,6 +607,19 @@ Value describe_basis(const Value& request) {
   }
   out.set("states", std::move(states));
   return out;
+}
+
+// OperatorExpressionRequest::Model (bindings/capi/src/lib.rs:791-798): a
+// registered model with optional parameter values and the direct action.
+// Matrix, scale, transform and binary expressions build operator algebra
+// outside the GPU engine.
+std::shared_ptr<qmbed_operator_s> expression_operator(const Value& e) {
+  const std::string kind = e.at("kind").as_string();
+  if (kind != "model") raise(QMBED_UNSUPPORTED_BACKEND, "operator expressions of kind `" + kind + "` are outside the GPU engine");
+  if (e.has("action") && e.at("action").as_string() != "apply")
+    raise(QMBED_UNSUPPORTED_BACKEND, "only the direct action is supported by the GPU engine");
+  auto model = registered_model(e.at("handle").as_string());
+  return model->materialize(e.find("parameters"), kStoragePacked, false);
 }
 
 Value command(const Value& request) {
@@ -707,6 +790,174 @@ Value command(const Value& request) {
       states.push(std::move(columns));
     }
     out.set("states", std::move(states));
+    return out;
+  }
+  if (operation == "lanczos_operator") {
+    // command_lanczos_operator (bindings/capi/src/lib.rs:4046-4075); tolerance
+    // default 1e-13 (default_lanczos_tolerance, lib.rs:2107-2109)
+    auto op = expression_operator(request.at("expression"));
+    const long long krylov = request.at("krylov_dimension").as_int();
+    if (krylov < 0) raise(QMBED_INVALID_OPTIONS, "krylov_dimension must be a nonnegative integer");
+    const double tolerance = request.has("tolerance") ? request.at("tolerance").as_double() : 1.0e-13;
+    const auto initial = parse_vector(request.at("initial"));
+    auto entry = std::make_shared<qmbed_lanczos_s>();
+    {
+      std::lock_guard<std::mutex> lock(op->mu);
+      const uint64_t dim = op->op->dim();
+      validate_lanczos(static_cast<size_t>(krylov), tolerance);
+      if (initial.size() != dim) raise(QMBED_DIMENSION_MISMATCH, "Lanczos operator and initial vector do not match");
+      std::vector<double> host(2 * dim);
+      for (uint64_t i = 0; i < dim; ++i) {
+        host[2 * i] = initial[i].real();
+        host[2 * i + 1] = initial[i].imag();
+      }
+      lanczos_ritz(op->view(), host.data(), static_cast<size_t>(krylov), tolerance, entry->d, op->block_ops());
+    }
+    const uint64_t id = g_next_lanczos.fetch_add(1);
+    {
+      std::lock_guard<std::mutex> lock(g_registry_mu);
+      g_lanczos[id] = entry;
+    }
+    const LanczosDecomposition& d = entry->d;
+    Value out = Value::object();
+    out.set("kind", Value::string("lanczos"));
+    out.set("handle", Value::string("lanczos:" + std::to_string(id)));
+    out.set("dimension", Value::integer(static_cast<long long>(initial.size())));
+    out.set("krylov_dimension", Value::integer(d.size));
+    out.set("initial_norm", Value::number(d.initial_norm));
+    Value values = Value::array(), vectors = Value::array();
+    for (int c = 0; c < d.size; ++c) {
+      values.push(Value::number(d.eigenvalues[c]));
+      Value v = Value::array();
+      for (int r = 0; r < d.size; ++r) v.push(Value::number(d.vec(r, c)));
+      vectors.push(std::move(v));
+    }
+    out.set("eigenvalues", std::move(values));
+    out.set("eigenvectors", std::move(vectors));
+    return out;
+  }
+  if (operation == "lanczos_combine" || operation == "lanczos_exponential") {
+    // command_lanczos_combine / command_lanczos_exponential (bindings/capi/src/lib.rs:4192-4212)
+    auto entry = registered_lanczos(request.at("lanczos_handle").as_string());
+    std::lock_guard<std::mutex> lock(entry->mu);
+    std::vector<C64> c;
+    if (operation == "lanczos_combine") {
+      c = parse_vector(request.at("coefficients"));
+    } else {
+      const auto& pair = request.at("coefficient").items();
+      if (pair.size() != 2) raise(QMBED_INVALID_OPTIONS, "coefficient is a [re, im] pair");
+      c = exponential_coefficients(entry->d, C64(pair[0].as_double(), pair[1].as_double()));
+    }
+    std::vector<double> host(2 * entry->d.n);
+    lanczos_vector_out(*entry, c, host.data());
+    Value out = Value::object();
+    out.set("kind", Value::string("vectors"));
+    out.set("dimension", Value::integer(static_cast<long long>(entry->d.n)));
+    out.set("vectors", vectors_value(host, entry->d.n, 1));
+    return out;
+  }
+  if (operation == "lanczos_thermal") {
+    // command_lanczos_thermal (bindings/capi/src/lib.rs:4214-4291): the
+    // eigenvector matrix arrives row-major; observables carry either a model
+    // expression (projected on the GPU through the handle's basis) or their
+    // projected matrix elements.
+    const std::string method_name = request.at("method").as_string();
+    if (method_name != "ftlm" && method_name != "ltlm") raise(QMBED_INVALID_OPTIONS, "method must be `ftlm` or `ltlm`");
+    const bool ltlm = method_name == "ltlm";
+    std::vector<double> eigenvalues;
+    for (const Value& v : request.at("eigenvalues").items()) eigenvalues.push_back(v.as_double());
+    const size_t m = eigenvalues.size();
+    const auto& rows = request.at("eigenvectors").items();
+    if (rows.size() != m) raise(QMBED_DIMENSION_MISMATCH, "Lanczos Ritz eigenvectors must be a square row-major matrix");
+    std::vector<std::vector<double>> columns(m, std::vector<double>(m));
+    for (size_t r = 0; r < m; ++r) {
+      const auto& row = rows[r].items();
+      if (row.size() != m) raise(QMBED_DIMENSION_MISMATCH, "Lanczos Ritz eigenvectors must be a square row-major matrix");
+      for (size_t c = 0; c < m; ++c) columns[c][r] = row[c].as_double();
+    }
+    std::vector<double> betas;
+    for (const Value& v : request.at("inverse_temperatures").items()) betas.push_back(v.as_double());
+    std::vector<std::string> names;
+    std::vector<std::vector<C64>> projected;
+    std::vector<std::pair<std::string, std::shared_ptr<qmbed_operator_s>>> native;
+    for (const Value& o : request.at("observables").items()) {
+      const bool has_expression = o.has("expression") && !o.at("expression").is_null();
+      const bool has_elements = o.has("matrix_elements") && !o.at("matrix_elements").items().empty();
+      if (has_expression == has_elements)
+        raise(QMBED_INVALID_OPTIONS, "each thermal observable needs exactly one expression or projected matrix");
+      if (has_expression) {
+        native.emplace_back(o.at("name").as_string(), expression_operator(o.at("expression")));
+      } else {
+        names.push_back(o.at("name").as_string());
+        projected.push_back(parse_vector(o.at("matrix_elements")));
+      }
+    }
+    if (!native.empty()) {
+      if (!request.has("lanczos_handle") || request.at("lanczos_handle").is_null())
+        raise(QMBED_INVALID_OPTIONS, "native thermal observables require a Lanczos handle");
+      auto entry = registered_lanczos(request.at("lanczos_handle").as_string());
+      std::lock_guard<std::mutex> lock(entry->mu);
+      if (static_cast<size_t>(entry->d.size) != m)
+        raise(QMBED_DIMENSION_MISMATCH, "Lanczos handle and supplied Ritz eigensystem dimensions differ");
+      for (auto& [name, op] : native) {
+        std::lock_guard<std::mutex> olock(op->mu);
+        names.push_back(name);
+        projected.push_back(project_observable(entry->d, op->view(), ltlm, op->block_ops()));
+      }
+    }
+    for (size_t i = 0; i < names.size(); ++i) {
+      bool unique = !names[i].empty();
+      for (size_t j = 0; j < i; ++j) unique = unique && names[j] != names[i];
+      if (!unique) raise(QMBED_DIMENSION_MISMATCH, "thermal observables require unique names and matching finite projections");
+    }
+    std::vector<std::vector<C64>> values;
+    std::vector<double> identity;
+    thermal_contraction(ltlm, eigenvalues, columns, projected, betas, values, identity);
+    Value out = Value::object();
+    out.set("kind", Value::string("thermal_lanczos"));
+    Value vals = Value::object();
+    for (size_t o = 0; o < names.size(); ++o) {
+      Value series = Value::array();
+      for (const C64& v : values[o]) series.push(complex_pair(v));
+      vals.set(names[o], std::move(series));
+    }
+    out.set("values", std::move(vals));
+    Value id = Value::array();
+    for (double v : identity) id.push(Value::number(v));
+    out.set("identity", std::move(id));
+    return out;
+  }
+  if (operation == "export_lanczos_basis") {
+    // command_export_lanczos_basis (bindings/capi/src/lib.rs:4293-4310)
+    auto entry = registered_lanczos(request.at("lanczos_handle").as_string());
+    std::lock_guard<std::mutex> lock(entry->mu);
+    QMBED_CUDA(cudaSetDevice(entry->d.device));
+    std::vector<double> host;
+    for (int j = 0; j < entry->d.size; ++j) {
+      const std::vector<double> col = lanczos_column_host(entry->d, j);
+      host.insert(host.end(), col.begin(), col.end());
+    }
+    Value out = Value::object();
+    out.set("kind", Value::string("lanczos_basis"));
+    out.set("dimension", Value::integer(static_cast<long long>(entry->d.n)));
+    out.set("vectors", vectors_value(host, entry->d.n, static_cast<size_t>(entry->d.size)));
+    return out;
+  }
+  if (operation == "release_lanczos") {
+    // release_lanczos (bindings/capi/src/lib.rs:1874-1886)
+    const std::string text = request.at("lanczos_handle").as_string();
+    const uint64_t id = parse_lanczos_handle(text);
+    std::shared_ptr<qmbed_lanczos_s> released;
+    {
+      std::lock_guard<std::mutex> lock(g_registry_mu);
+      auto it = g_lanczos.find(id);
+      if (it == g_lanczos.end()) raise(QMBED_INVALID_OPTIONS, "Lanczos handle " + text + " is not registered");
+      released = std::move(it->second);
+      g_lanczos.erase(it);
+    }
+    Value out = Value::object();
+    out.set("kind", Value::string("released"));
+    out.set("handle", Value::string("lanczos:" + std::to_string(id)));
     return out;
   }
   if (operation == "release_model") {
@@ -1163,6 +1414,200 @@ int qmbed_gpu_mlp_predict(qmbed_mlp mlp, const float* X, int n, float* Y) {
   return guarded([&] {
     std::lock_guard<std::mutex> lock(mlp->mu);
     mlp->net->predict(X, n, Y);
+  });
+}
+
+
+
+int qmbed_gpu_lanczos_create(qmbed_operator op, const double* initial, uint64_t krylov_dimension, double tolerance,
+                             qmbed_lanczos* out) {
+  return guarded([&] {
+    if (!out) raise(QMBED_INVALID_OPTIONS, "lanczos_create needs an output handle");
+    auto h = std::make_unique<qmbed_lanczos_s>();
+    {
+      std::lock_guard<std::mutex> lock(op->mu);
+      lanczos_ritz(op->view(), initial, krylov_dimension, tolerance, h->d, op->block_ops());
+    }
+    *out = h.release();
+  });
+}
+
+int qmbed_gpu_lanczos_destroy(qmbed_lanczos lanczos) {
+  return guarded([&] { delete lanczos; });
+}
+
+int qmbed_gpu_lanczos_info(qmbed_lanczos l, uint64_t* dimension, uint64_t* krylov_dimension, double* initial_norm,
+                           int* is_real, uint64_t* second_passes) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(l->mu);
+    if (dimension) *dimension = l->d.n;
+    if (krylov_dimension) *krylov_dimension = static_cast<uint64_t>(l->d.size);
+    if (initial_norm) *initial_norm = l->d.initial_norm;
+    if (is_real) *is_real = l->d.real ? 1 : 0;
+    if (second_passes) *second_passes = static_cast<uint64_t>(l->d.second_passes);
+  });
+}
+
+int qmbed_gpu_lanczos_ritz(qmbed_lanczos l, double* values, double* vectors, double* diagonal, double* off_diagonal) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(l->mu);
+    const int m = l->d.size;
+    for (int c = 0; c < m; ++c) {
+      if (values) values[c] = l->d.eigenvalues[c];
+      if (vectors)
+        for (int r = 0; r < m; ++r) vectors[static_cast<size_t>(c) * m + r] = l->d.vec(r, c);
+      if (diagonal) diagonal[c] = l->d.diagonal[c];
+      if (off_diagonal && c + 1 < m) off_diagonal[c] = l->d.off_diagonal[c];
+    }
+  });
+}
+
+int qmbed_gpu_lanczos_basis(qmbed_lanczos l, double* basis) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(l->mu);
+    QMBED_CUDA(cudaSetDevice(l->d.device));
+    for (int j = 0; j < l->d.size; ++j) {
+      const std::vector<double> col = lanczos_column_host(l->d, j);
+      std::memcpy(basis + 2 * static_cast<size_t>(j) * l->d.n, col.data(), col.size() * sizeof(double));
+    }
+  });
+}
+
+int qmbed_gpu_lanczos_combine(qmbed_lanczos l, const double* coefficients, double* out) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(l->mu);
+    if (!coefficients || !out) raise(QMBED_INVALID_OPTIONS, "linear combination needs coefficients and an output");
+    std::vector<C64> c(static_cast<size_t>(l->d.size));
+    for (int b = 0; b < l->d.size; ++b) c[b] = C64(coefficients[2 * b], coefficients[2 * b + 1]);
+    lanczos_vector_out(*l, c, out);
+  });
+}
+
+int qmbed_gpu_lanczos_exponential(qmbed_lanczos l, double coefficient_re, double coefficient_im, double* out) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(l->mu);
+    if (!out) raise(QMBED_INVALID_OPTIONS, "exponential action needs an output vector");
+    lanczos_vector_out(*l, exponential_coefficients(l->d, C64(coefficient_re, coefficient_im)), out);
+  });
+}
+
+int qmbed_gpu_lanczos_thermal(qmbed_lanczos l, int method, int n_betas, const double* betas, int n_observables,
+                              const qmbed_operator* observables, double* values, double* identity) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(l->mu);
+    if (method != 0 && method != 1) raise(QMBED_INVALID_OPTIONS, "thermal method must be FTLM (0) or LTLM (1)");
+    if (n_observables <= 0 || !observables) raise(QMBED_INVALID_OPTIONS, "thermal observables must be nonempty");
+    const std::vector<double> grid = beta_grid(n_betas, betas);
+    std::vector<std::vector<C64>> projected;
+    for (int o = 0; o < n_observables; ++o) {
+      qmbed_operator_s& a = *observables[o];
+      std::lock_guard<std::mutex> alock(a.mu);
+      projected.push_back(project_observable(l->d, a.view(), method == 1, a.block_ops()));
+    }
+    std::vector<std::vector<C64>> out;
+    std::vector<double> id;
+    thermal_contraction(method == 1, l->d.eigenvalues, ritz_columns(l->d), projected, grid, out, id);
+    for (size_t o = 0; o < out.size(); ++o)
+      for (size_t b = 0; b < grid.size(); ++b) {
+        values[2 * (o * grid.size() + b)] = out[o][b].real();
+        values[2 * (o * grid.size() + b) + 1] = out[o][b].imag();
+      }
+    for (size_t b = 0; b < grid.size(); ++b) identity[b] = id[b];
+  });
+}
+
+int qmbed_gpu_lanczos_project(qmbed_lanczos l, int method, qmbed_operator observable, double* matrix_elements) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(l->mu);
+    if (method != 0 && method != 1) raise(QMBED_INVALID_OPTIONS, "thermal method must be FTLM (0) or LTLM (1)");
+    if (!observable || !matrix_elements) raise(QMBED_INVALID_OPTIONS, "projection needs an observable and an output");
+    std::lock_guard<std::mutex> alock(observable->mu);
+    const std::vector<C64> p = project_observable(l->d, observable->view(), method == 1, observable->block_ops());
+    for (size_t i = 0; i < p.size(); ++i) {
+      matrix_elements[2 * i] = p[i].real();
+      matrix_elements[2 * i + 1] = p[i].imag();
+    }
+  });
+}
+
+int qmbed_gpu_thermal_contraction(int method, int m, const double* eigenvalues, const double* eigenvectors,
+                                  int n_observables, const double* matrix_elements, int n_betas, const double* betas,
+                                  double* values, double* identity) {
+  return guarded([&] {
+    if (method != 0 && method != 1) raise(QMBED_INVALID_OPTIONS, "thermal method must be FTLM (0) or LTLM (1)");
+    if (m < 0 || n_observables < 0 || (m > 0 && (!eigenvalues || !eigenvectors)))
+      raise(QMBED_DIMENSION_MISMATCH, "thermal Lanczos contraction requires a finite square Ritz eigensystem");
+    const std::vector<double> grid = beta_grid(n_betas, betas);
+    std::vector<double> e(eigenvalues, eigenvalues + m);
+    std::vector<std::vector<double>> columns(static_cast<size_t>(m), std::vector<double>(static_cast<size_t>(m)));
+    for (int c = 0; c < m; ++c)
+      for (int r = 0; r < m; ++r) columns[c][r] = eigenvectors[static_cast<size_t>(r) * m + c];
+    const size_t per = method == 1 ? static_cast<size_t>(m) * m : static_cast<size_t>(m);
+    std::vector<std::vector<C64>> projected(static_cast<size_t>(n_observables), std::vector<C64>(per));
+    for (int o = 0; o < n_observables; ++o)
+      for (size_t i = 0; i < per; ++i)
+        projected[o][i] = C64(matrix_elements[2 * (o * per + i)], matrix_elements[2 * (o * per + i) + 1]);
+    std::vector<std::vector<C64>> out;
+    std::vector<double> id;
+    thermal_contraction(method == 1, e, columns, projected, grid, out, id);
+    for (size_t o = 0; o < out.size(); ++o)
+      for (size_t b = 0; b < grid.size(); ++b) {
+        values[2 * (o * grid.size() + b)] = out[o][b].real();
+        values[2 * (o * grid.size() + b) + 1] = out[o][b].imag();
+      }
+    for (size_t b = 0; b < grid.size(); ++b) identity[b] = id[b];
+  });
+}
+
+int qmbed_gpu_thermal_iteration(qmbed_operator op, const double* initial, int n_betas, const double* betas,
+                                uint64_t krylov_dimension, double tolerance, double* log_partition,
+                                double* mean_energy, uint64_t* krylov_out) {
+  return guarded([&] {
+    validate_lanczos(krylov_dimension, tolerance);
+    const std::vector<double> grid = beta_grid(n_betas, betas);
+    std::lock_guard<std::mutex> lock(op->mu);
+    // validate the temperatures before the recurrence runs (src/solve/mod.rs:3473-3482)
+    bool ok = !grid.empty();
+    for (double b : grid) ok = ok && std::isfinite(b) && b >= 0.0;
+    if (!ok) raise(QMBED_INVALID_OPTIONS, "inverse temperatures must be nonempty, finite, and nonnegative");
+    LanczosDecomposition d;
+    lanczos_ritz(op->view(), initial, krylov_dimension, tolerance, d, op->block_ops());
+    const ThermalEstimate t = thermal_estimate(d, op->op->dim(), grid);
+    for (size_t b = 0; b < grid.size(); ++b) {
+      log_partition[b] = t.log_partition[b];
+      mean_energy[b] = t.mean_energy[b];
+    }
+    if (krylov_out) *krylov_out = static_cast<uint64_t>(t.krylov_dimension);
+  });
+}
+
+int qmbed_gpu_ftlm_sample(qmbed_operator op, int n_vectors, uint64_t seed, int n_betas, const double* betas,
+                          uint64_t krylov_dimension, double tolerance, double* log_partition, double* mean_energy,
+                          int* lengths) {
+  return guarded([&] {
+    const std::vector<double> grid = beta_grid(n_betas, betas);
+    std::lock_guard<std::mutex> lock(op->mu);
+    std::vector<double> lz, e;
+    std::vector<int> len;
+    ftlm_sample(op->view(), n_vectors, seed, krylov_dimension, tolerance, grid, lz, e, len, op->block_ops());
+    std::copy(lz.begin(), lz.end(), log_partition);
+    std::copy(e.begin(), e.end(), mean_energy);
+    if (lengths) std::copy(len.begin(), len.end(), lengths);
+  });
+}
+
+int qmbed_gpu_ftlm_start(qmbed_operator op, uint64_t seed, int index, double* out) {
+  return guarded([&] {
+    if (!out || index < 0) raise(QMBED_INVALID_OPTIONS, "start vector needs a nonnegative index and an output");
+    std::lock_guard<std::mutex> lock(op->mu);
+    const LinearOperatorView view = op->view();
+    BlockOps& ops = op->block_ops();
+    const uint64_t n = view.dim;
+    DeviceBuffer v(std::max<uint64_t>(n, 1) * 16), wide(std::max<uint64_t>(n, 1) * 16);
+    ftlm_start_vector(view, seed, index, v.as<double>(), ops);
+    if (view.real) ops.widen_real(v.as<double>(), wide.as<double>(), n);
+    QMBED_CUDA(cudaMemcpyAsync(out, view.real ? wide.get() : v.get(), n * 16, cudaMemcpyDeviceToHost, ops.stream()));
+    ops.sync();
   });
 }
 

@@ -679,6 +679,20 @@ void BlockOps::dots(const void* A, uint64_t ld, int m, const void* w, uint64_t n
   if (self_sq) *self_sq = host_results_[2 * m];
 }
 
+void BlockOps::dots_device(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx,
+                           double* out) {
+  if (m <= 0) return;
+  const int G = reduction_grid(n, sms_);
+  ensure_partials(static_cast<size_t>(m) * G * 2 + 2 * static_cast<size_t>(m) + 64);
+  QMBED_DISPATCH(precision, cplx,
+                 (multi_dot_kernel<T, C><<<G, kThreads, 0, stream_>>>(static_cast<const T*>(A), ld, m,
+                                                                      static_cast<const T*>(w), n,
+                                                                      partials_.as<double>(), 0)));
+  QMBED_LAUNCH_CHECK();
+  finish_kernel<<<2 * m, kFinishThreads, 0, stream_>>>(partials_.as<double>(), G, 2 * m, out);
+  QMBED_LAUNCH_CHECK();
+}
+
 void BlockOps::scale_into(const void* src, void* dst, uint64_t n, double divisor, int precision, bool cplx) {
   const uint64_t count = n * (cplx ? 2 : 1);
   const int G = stream_grid(count, sms_);

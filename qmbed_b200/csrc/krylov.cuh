@@ -33,6 +33,10 @@ class BlockOps {
   // ||w||^2 from the same pass over w.
   void dots(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx, C64* out,
             double* self_sq = nullptr);
+  // The same overlaps written to device memory (out: 2 m doubles,
+  // interleaved), with no host round trip.
+  void dots_device(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx,
+                   double* out);
   double norm(const void* w, uint64_t n, int precision, bool cplx);
   // w = src - sum_j h_j A_j (src = w when null); returns ||w|| when `want_norm`.
   double subtract(const void* A, uint64_t ld, int m, const C64* h, void* w, uint64_t n, int precision, bool cplx,

@@ -336,3 +336,77 @@ def test_evolution_option_errors(oracle):
         with pytest.raises(OracleError) as e:
             op.evolve(v, times, krylov_dimension=krylov, tolerance=tol)
         assert e.value.code == 8
+
+
+def test_thermal_two_level_anchor(oracle, anchors):
+    a = anchors["thermal_two_level"]
+    op = oracle.Operator.diagonal(a["diagonal"])
+    identity = oracle.Operator.diagonal([1.0, 1.0])
+    initial = np.full(2, 1.0 / np.sqrt(2.0), complex)
+    beta = a["inverse_temperatures"][1]
+    lz, energy, m = op.thermal_iteration(initial, a["inverse_temperatures"], a["krylov_dimension"], a["tolerance"])
+    partition = np.exp(beta) + np.exp(-2.0 * beta)
+    expected = (-np.exp(beta) + 2.0 * np.exp(-2.0 * beta)) / partition
+    assert m == 2
+    assert abs(lz[0] - np.log(2.0)) <= a["abs_tol"]
+    assert abs(lz[1] - np.log(partition)) <= a["abs_tol"]
+    assert abs(energy[1] - expected) <= a["abs_tol"]
+    for method in ("ftlm", "ltlm"):
+        values, ident = op.thermal_observables(initial, [op, identity], [beta], a["krylov_dimension"],
+                                               a["tolerance"], method)
+        assert abs(values[1, 0].real - ident[0]) <= a["abs_tol"]
+        assert abs(values[0, 0].real / ident[0] - expected) <= a["abs_tol"]
+
+
+def test_lanczos_full_orthonormal_anchor(oracle, anchors):
+    a = anchors["lanczos_full_orthonormal"]
+    op = oracle.Operator.diagonal(a["diagonal"])
+    r = op.lanczos_ritz(np.asarray(a["initial"], complex), a["krylov_dimension"], a["tolerance"])
+    q = r["basis"]
+    assert q.shape[0] == 3
+    assert np.max(np.abs(q.conj() @ q.T - np.eye(3))) <= a["orthonormality_abs_tol"]
+    np.testing.assert_allclose(r["values"], sorted(a["diagonal"]), atol=1e-12)
+
+
+def _exact_thermal(dense, v, betas):
+    """ln(D / |v|^2) + ln <v|e^{-beta H}|v> and <v|H e^{-beta H}|v> / <v|e^{-beta H}|v>."""
+    w, u = np.linalg.eigh(dense)
+    overlap = np.abs(u.conj().T @ v) ** 2
+    lz, e = [], []
+    for beta in betas:
+        boltzmann = overlap * np.exp(-beta * (w - w.min()))
+        lz.append(np.log(len(v) / np.vdot(v, v).real) - beta * w.min() + np.log(boltzmann.sum()))
+        e.append((boltzmann * w).sum() / boltzmann.sum())
+    return np.array(lz), np.array(e)
+
+
+@pytest.mark.parametrize("sites,momentum,parity", [(10, 0, 1), (9, 2, None)])
+def test_thermal_iteration_is_exact_on_an_exhausted_krylov_space(oracle, sites, momentum, parity):
+    """With the Krylov space exhausted (beta <= tolerance ends the recurrence)
+    the FTLM estimate of one vector equals <v|e^{-beta H}|v> exactly."""
+    basis = oracle.Basis(sites, up=sites // 2, momentum=momentum, parity=parity)
+    op = oracle.Operator.build(basis, oracle.heisenberg_terms(sites, delta=0.7))
+    dense = op.dense()
+    rng = np.random.default_rng(sites)
+    v = rng.standard_normal(op.dim) + (0.0 if op.is_real else 1j * rng.standard_normal(op.dim))
+    betas = [0.0, 0.3, 1.0, 4.0]
+    lz, e, m = op.thermal_iteration(v, betas, op.dim + 5, 1e-10)
+    assert m <= op.dim
+    exact_lz, exact_e = _exact_thermal(dense, v.astype(complex), betas)
+    np.testing.assert_allclose(lz, exact_lz, atol=1e-9)
+    np.testing.assert_allclose(e, exact_e, atol=1e-9)
+    assert abs(lz[0] - np.log(op.dim)) <= 1e-12
+
+
+def test_thermal_errors(oracle):
+    from oracle.oracle import OracleError
+    op = oracle.Operator.diagonal([-1.0, 2.0])
+    v = np.ones(2, complex)
+    for betas, krylov, tol, code in (([], 2, 1e-12, 8), ([-1.0], 2, 1e-12, 8), ([np.nan], 2, 1e-12, 8),
+                                     ([1.0], 0, 1e-12, 8), ([1.0], 2, 0.0, 8)):
+        with pytest.raises(OracleError) as e:
+            op.thermal_iteration(v, betas, krylov, tol)
+        assert e.value.code == code
+    with pytest.raises(OracleError) as e:
+        op.thermal_iteration(np.zeros(2, complex), [1.0], 2, 1e-12)
+    assert e.value.code == 14
