@@ -79,7 +79,7 @@ def xxz_section(sites: int, rank: int, local_rank: int) -> dict:
     terms = engine.heisenberg_terms(sites, delta=delta)
     basis = engine.GpuBasis(sites, up=sites // 2, momentum=0, parity=1, device=local_rank)
     out = {"workload": f"xxz L={sites} k=0 p=+1 up={sites // 2} Delta={delta:.6f} (seed {seed}), 6 lowest, tol 1e-10",
-           "dim": basis.dim}
+           "dim": len(basis)}
     runs = {}
     for storage, modes in (("matrix_free", ("fp64", "mixed")), ("packed", ("filtered",))):
         op = engine.GpuOperator(basis, terms, storage=storage)
@@ -118,7 +118,7 @@ def ftlm_section(sites: int, rank: int, local_rank: int, with_cpu: bool, vectors
         return engine.GpuOperator(basis, engine.heisenberg_terms(L, delta=1.0))
 
     def timed(op, count):
-        lanczos.ftlm_sample(op, 1, betas, 20, seed=seed)  # warm-up (workspaces)
+        lanczos.ftlm_sample(op, 1, betas, krylov, seed=seed)  # warm-up (allocations, first launches)
         torch.cuda.synchronize()
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()

@@ -44,6 +44,51 @@ __device__ inline double warp_sum(double v) {
   return v;
 }
 
+// Overlaps of a tall FP64 panel with one vector, one warp per column: each
+// block stages a slab of `slab` rows of w in shared memory and its warps
+// sweep the columns; every lane keeps eight independent loads in flight.
+// partials[(j * G + block) * 2 + {0,1}] as for multi_dot_kernel.
+constexpr int kMaxSlab = 2048;
+template <bool CPLX>
+__global__ void __launch_bounds__(kThreads) panel_dot_kernel(const double* __restrict__ A, uint64_t ld, int m,
+                                                             const double* __restrict__ w, uint64_t n, int slab,
+                                                             double* __restrict__ partials) {
+  constexpr int W = CPLX ? 2 : 1;
+  extern __shared__ __align__(16) double ws[];
+  const uint64_t r0 = static_cast<uint64_t>(blockIdx.x) * slab;
+  const int rows = static_cast<int>(min(static_cast<uint64_t>(slab), n - r0));
+  for (int t = threadIdx.x; t < rows * W; t += blockDim.x) ws[t] = w[r0 * W + t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const uint64_t G = gridDim.x;
+  for (int j = threadIdx.x >> 5; j < m; j += kThreads / 32) {
+    const double* q = A + static_cast<uint64_t>(j) * ld * W + r0 * W;
+    double sr = 0.0, si = 0.0;
+    for (int r = lane; r < rows; r += 32 * 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = r + 32 * u;
+        if (k < rows) {
+          if (CPLX) {
+            const double2 x = reinterpret_cast<const double2*>(q)[k];
+            const double2 y = reinterpret_cast<const double2*>(ws)[k];
+            sr += x.x * y.x + x.y * y.y;
+            si += x.x * y.y - x.y * y.x;
+          } else {
+            sr += q[k] * ws[k];
+          }
+        }
+      }
+    }
+    sr = warp_sum(sr);
+    if (CPLX) si = warp_sum(si);
+    if (lane == 0) {
+      partials[(static_cast<uint64_t>(j) * G + blockIdx.x) * 2] = sr;
+      partials[(static_cast<uint64_t>(j) * G + blockIdx.x) * 2 + 1] = si;
+    }
+  }
+}
+
 // partials[(j * G + block) * 2 + {0,1}] = sum over this block's rows of conj(A_j) w.
 // With `with_self`, column m receives sum |w|^2 (computed in the first pass).
 template <typename T, bool CPLX>
@@ -681,13 +726,31 @@ void BlockOps::dots(const void* A, uint64_t ld, int m, const void* w, uint64_t n
 
 void BlockOps::dots_device(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx,
                            double* out) {
-  if (m <= 0) return;
-  const int G = reduction_grid(n, sms_);
-  ensure_partials(static_cast<size_t>(m) * G * 2 + 2 * static_cast<size_t>(m) + 64);
-  QMBED_DISPATCH(precision, cplx,
-                 (multi_dot_kernel<T, C><<<G, kThreads, 0, stream_>>>(static_cast<const T*>(A), ld, m,
-                                                                      static_cast<const T*>(w), n,
-                                                                      partials_.as<double>(), 0)));
+  if (m <= 0 || n == 0) return;
+  int G;
+  if (precision == 64) {
+    // slabs of 256..2048 rows, sized for about eight blocks per SM
+    const uint64_t target = (n + 8ull * sms_ - 1) / (8ull * sms_);
+    const int slab = static_cast<int>(std::min<uint64_t>(kMaxSlab, std::max<uint64_t>(256, (target + 255) / 256 * 256)));
+    G = static_cast<int>((n + slab - 1) / slab);
+    ensure_partials(static_cast<size_t>(m) * G * 2 + 2 * static_cast<size_t>(m) + 64);
+    const size_t smem = static_cast<size_t>(slab) * (cplx ? 16 : 8);
+    if (cplx)
+      panel_dot_kernel<true><<<G, kThreads, smem, stream_>>>(static_cast<const double*>(A), ld, m,
+                                                             static_cast<const double*>(w), n, slab,
+                                                             partials_.as<double>());
+    else
+      panel_dot_kernel<false><<<G, kThreads, smem, stream_>>>(static_cast<const double*>(A), ld, m,
+                                                              static_cast<const double*>(w), n, slab,
+                                                              partials_.as<double>());
+  } else {
+    G = reduction_grid(n, sms_);
+    ensure_partials(static_cast<size_t>(m) * G * 2 + 2 * static_cast<size_t>(m) + 64);
+    QMBED_DISPATCH(precision, cplx,
+                   (multi_dot_kernel<T, C><<<G, kThreads, 0, stream_>>>(static_cast<const T*>(A), ld, m,
+                                                                        static_cast<const T*>(w), n,
+                                                                        partials_.as<double>(), 0)));
+  }
   QMBED_LAUNCH_CHECK();
   finish_kernel<<<2 * m, kFinishThreads, 0, stream_>>>(partials_.as<double>(), G, 2 * m, out);
   QMBED_LAUNCH_CHECK();

@@ -105,12 +105,15 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 }
 
 // One Gram-Schmidt pass of the Lanczos step over the basis panel Q (m
-// columns, leading dimension n, FP64 real or interleaved complex):
-// w -= sum_k h_k q_k with the overlaps h (device, interleaved complex).
-// Per-block partial sums, in a fixed order: partials[2b] = |w'|^2 for the
-// three-term residual w' = w - Re(h_{m-1}) q_{m-1} - beta q_{m-2} (when
-// `three_term`), partials[2b+1] = |w - sum_k h_k q_k|^2.
-template <bool CPLX>
+// columns, leading dimension n, FP64): w -= sum_k h_k q_k with the overlaps
+// h (device, interleaved complex). Per-block partial sums, in a fixed order:
+// partials[2b] = |w'|^2 for the three-term residual
+// w' = w - Re(h_{m-1}) q_{m-1} - beta q_{m-2} (when `three_term`),
+// partials[2b+1] = |w - sum_k h_k q_k|^2. Elements are complex values
+// (kComplex), pairs of real rows loaded as one 16-byte word (kRealPair, n
+// even), or single real rows (kReal).
+enum { kReal = 0, kRealPair = 1, kComplex = 2 };
+template <int MODE>
 __global__ void __launch_bounds__(kOrthoThreads) orthogonalize_kernel(const double* __restrict__ Q, uint64_t n, int m,
                                                                       const double* __restrict__ h, double beta,
                                                                       int three_term, double* __restrict__ w,
@@ -120,31 +123,34 @@ __global__ void __launch_bounds__(kOrthoThreads) orthogonalize_kernel(const doub
   for (int t = threadIdx.x; t < 2 * m; t += blockDim.x) hs[t] = h[t];
   __syncthreads();
   const double alpha = hs[2 * (m - 1)];
-  const uint64_t col = n * (CPLX ? 2 : 1);
+  // element count and the stride between columns, in elements
+  const uint64_t elems = MODE == kRealPair ? n / 2 : n;
+  const uint64_t col = MODE == kReal ? n : n / (MODE == kRealPair ? 2 : 1);
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   double before = 0.0, after = 0.0;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-    double wr, wi = 0.0;
-    if (CPLX) {
-      const double2 v = reinterpret_cast<const double2*>(w)[i];
-      wr = v.x;
-      wi = v.y;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < elems; i += stride) {
+    // (a, b): real and imaginary parts, or the two rows of a pair
+    double wa, wb = 0.0;
+    if (MODE == kReal) {
+      wa = w[i];
     } else {
-      wr = w[i];
+      const double2 v = reinterpret_cast<const double2*>(w)[i];
+      wa = v.x;
+      wb = v.y;
     }
-    double sr = 0.0, si = 0.0, lr = 0.0, li = 0.0, pr = 0.0, pi = 0.0;
+    double sa = 0.0, sb = 0.0, la = 0.0, lb = 0.0, pa = 0.0, pb = 0.0;
     for (int j0 = 0; j0 < m; j0 += kOrthoChunk) {
-      double xr[kOrthoChunk], xi[kOrthoChunk];
+      double xa[kOrthoChunk], xb[kOrthoChunk];
 #pragma unroll
       for (int jj = 0; jj < kOrthoChunk; ++jj) {
-        xr[jj] = xi[jj] = 0.0;
+        xa[jj] = xb[jj] = 0.0;
         if (j0 + jj < m) {
-          if (CPLX) {
-            const double2 v = reinterpret_cast<const double2*>(Q + static_cast<uint64_t>(j0 + jj) * col)[i];
-            xr[jj] = v.x;
-            xi[jj] = v.y;
+          if (MODE == kReal) {
+            xa[jj] = Q[static_cast<uint64_t>(j0 + jj) * col + i];
           } else {
-            xr[jj] = Q[static_cast<uint64_t>(j0 + jj) * col + i];
+            const double2 v = reinterpret_cast<const double2*>(Q)[static_cast<uint64_t>(j0 + jj) * col + i];
+            xa[jj] = v.x;
+            xb[jj] = v.y;
           }
         }
       }
@@ -153,27 +159,32 @@ __global__ void __launch_bounds__(kOrthoThreads) orthogonalize_kernel(const doub
         const int k = j0 + jj;
         if (k < m) {
           const double hr = hs[2 * k], hi = hs[2 * k + 1];
-          sr += hr * xr[jj] - hi * xi[jj];
-          si += hr * xi[jj] + hi * xr[jj];
+          if (MODE == kComplex) {
+            sa += hr * xa[jj] - hi * xb[jj];
+            sb += hr * xb[jj] + hi * xa[jj];
+          } else {  // real basis: the overlaps are real
+            sa += hr * xa[jj];
+            sb += hr * xb[jj];
+          }
           if (k == m - 1) {
-            lr = xr[jj];
-            li = xi[jj];
+            la = xa[jj];
+            lb = xb[jj];
           }
           if (k == m - 2) {
-            pr = xr[jj];
-            pi = xi[jj];
+            pa = xa[jj];
+            pb = xb[jj];
           }
         }
       }
     }
     if (three_term) {
-      const double br = wr - alpha * lr - beta * pr, bi = wi - alpha * li - beta * pi;
-      before += br * br + bi * bi;
+      const double ba = wa - alpha * la - beta * pa, bb = wb - alpha * lb - beta * pb;
+      before += ba * ba + bb * bb;
     }
-    const double rr = wr - sr, ri = wi - si;
-    if (CPLX) reinterpret_cast<double2*>(w)[i] = make_double2(rr, ri);
-    else w[i] = rr;
-    after += rr * rr + ri * ri;
+    const double ra = wa - sa, rb = wb - sb;
+    if (MODE == kReal) w[i] = ra;
+    else reinterpret_cast<double2*>(w)[i] = make_double2(ra, rb);
+    after += ra * ra + rb * rb;
   }
   before = block_sum(before, red);
   after = block_sum(after, red);
@@ -315,7 +326,10 @@ void lanczos_ritz_device(const LinearOperatorView& op, const double* initial, bo
   auto col = [&](int j) { return static_cast<char*>(d.basis.get()) + static_cast<size_t>(j) * n * width; };
   const cudaStream_t stream = ops.stream();
   const size_t smem = static_cast<size_t>(capacity) * 16;
-  auto kernel = cplx ? orthogonalize_kernel<true> : orthogonalize_kernel<false>;
+  // pairs of real rows move as 16-byte words when every column starts 16-byte aligned
+  const int mode = cplx ? kComplex : (n % 2 == 0 ? kRealPair : kReal);
+  auto kernel = mode == kComplex ? orthogonalize_kernel<kComplex>
+                                 : (mode == kRealPair ? orthogonalize_kernel<kRealPair> : orthogonalize_kernel<kReal>);
   if (smem > 48 * 1024)
     QMBED_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   // one Gram-Schmidt pass over q_0 .. q_{m-1}; returns (|w'|^2, |w''|^2, alpha)
