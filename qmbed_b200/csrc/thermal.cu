@@ -114,7 +114,7 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 // even), or single real rows (kReal).
 enum { kReal = 0, kRealPair = 1, kComplex = 2 };
 template <int MODE>
-__global__ void __launch_bounds__(kOrthoThreads) orthogonalize_kernel(const double* __restrict__ Q, uint64_t n, int m,
+__global__ void __launch_bounds__(kOrthoThreads, 4) orthogonalize_kernel(const double* __restrict__ Q, uint64_t n, int m,
                                                                       const double* __restrict__ h, double beta,
                                                                       int three_term, double* __restrict__ w,
                                                                       double* __restrict__ partials) {
@@ -127,6 +127,8 @@ __global__ void __launch_bounds__(kOrthoThreads) orthogonalize_kernel(const doub
   const uint64_t elems = MODE == kRealPair ? n / 2 : n;
   const uint64_t col = MODE == kReal ? n : n / (MODE == kRealPair ? 2 : 1);
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  // columns loaded ahead per element: eight 8-byte or four 16-byte words
+  constexpr int CH = MODE == kReal ? kOrthoChunk : kOrthoChunk / 2;
   double before = 0.0, after = 0.0;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < elems; i += stride) {
     // (a, b): real and imaginary parts, or the two rows of a pair
@@ -139,10 +141,10 @@ __global__ void __launch_bounds__(kOrthoThreads) orthogonalize_kernel(const doub
       wb = v.y;
     }
     double sa = 0.0, sb = 0.0, la = 0.0, lb = 0.0, pa = 0.0, pb = 0.0;
-    for (int j0 = 0; j0 < m; j0 += kOrthoChunk) {
-      double xa[kOrthoChunk], xb[kOrthoChunk];
+    for (int j0 = 0; j0 < m; j0 += CH) {
+      double xa[CH], xb[CH];
 #pragma unroll
-      for (int jj = 0; jj < kOrthoChunk; ++jj) {
+      for (int jj = 0; jj < CH; ++jj) {
         xa[jj] = xb[jj] = 0.0;
         if (j0 + jj < m) {
           if (MODE == kReal) {
@@ -155,7 +157,7 @@ __global__ void __launch_bounds__(kOrthoThreads) orthogonalize_kernel(const doub
         }
       }
 #pragma unroll
-      for (int jj = 0; jj < kOrthoChunk; ++jj) {
+      for (int jj = 0; jj < CH; ++jj) {
         const int k = j0 + jj;
         if (k < m) {
           const double hr = hs[2 * k], hi = hs[2 * k + 1];
