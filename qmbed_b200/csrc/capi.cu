@@ -610,16 +610,62 @@ Value describe_basis(const Value& request) {
 }
 
 // OperatorExpressionRequest::Model (bindings/capi/src/lib.rs:791-798): a
-// registered model with optional parameter values and the direct action.
+// registered model with optional parameter values and the normal action
+// (OperatorActionRequest, lib.rs:937-945; transpose, conjugate and adjoint
+// actions are not built).
 // Matrix, scale, transform and binary expressions build operator algebra
 // outside the GPU engine.
-std::shared_ptr<qmbed_operator_s> expression_operator(const Value& e) {
+std::shared_ptr<qmbed_operator_s> expression_operator(const Value& e, int storage = kStoragePacked) {
   const std::string kind = e.at("kind").as_string();
   if (kind != "model") raise(QMBED_UNSUPPORTED_BACKEND, "operator expressions of kind `" + kind + "` are outside the GPU engine");
-  if (e.has("action") && e.at("action").as_string() != "apply")
-    raise(QMBED_UNSUPPORTED_BACKEND, "only the direct action is supported by the GPU engine");
+  if (e.has("action") && e.at("action").as_string() != "normal")
+    raise(QMBED_UNSUPPORTED_BACKEND, "only the normal action is supported by the GPU engine");
   auto model = registered_model(e.at("handle").as_string());
-  return model->materialize(e.find("parameters"), kStoragePacked, false);
+  return model->materialize(e.find("parameters"), storage, false);
+}
+
+// ExpmActionPlan applied to a host column batch (the apply step of
+// ExpmMultiplyParallel, src/solve/mod.rs:252-326), one column at a time.
+Value expm_vectors(qmbed_operator_s& h, const ExpmPlan& plan, const std::vector<std::vector<C64>>& vectors) {
+  std::lock_guard<std::mutex> lock(h.mu);
+  const uint64_t dim = h.op->dim();
+  BlockOps& ops = h.block_ops();
+  LinearOperatorView view{dim, h.op->is_real(), [&h, &ops](int prec, bool cplx, const void* x, void* y) {
+                            h.op->apply(prec, cplx, x, y, ops.stream());
+                          }};
+  DeviceBuffer state(std::max<uint64_t>(dim, 1) * 16);
+  std::vector<double> host(2 * dim);
+  Value out = Value::object();
+  out.set("kind", Value::string("vectors"));
+  out.set("dimension", Value::integer(static_cast<long long>(vectors.empty() ? dim : vectors[0].size())));
+  Value vs = Value::array();
+  for (const auto& v : vectors) {
+    if (v.size() != dim) raise(QMBED_DIMENSION_MISMATCH, "exponential batch column has the wrong length");
+    for (uint64_t i = 0; i < dim; ++i) {
+      host[2 * i] = v[i].real();
+      host[2 * i + 1] = v[i].imag();
+    }
+    QMBED_CUDA(cudaMemcpy(state.get(), host.data(), 16 * dim, cudaMemcpyHostToDevice));
+    expm_apply(plan, view, state.get(), 64, ops);
+    QMBED_CUDA(cudaMemcpy(host.data(), state.get(), 16 * dim, cudaMemcpyDeviceToHost));
+    Value r = Value::array();
+    for (uint64_t i = 0; i < dim; ++i) r.push(complex_pair(C64(host[2 * i], host[2 * i + 1])));
+    vs.push(std::move(r));
+  }
+  out.set("vectors", std::move(vs));
+  return out;
+}
+
+// create_expm_action / expm_operator_expression options: ExpmMultiplyParallel
+// defaults 55 / eps/2 / 10000 (bindings/capi/src/lib.rs:2111-2121).
+ExpmPlan expm_plan_from(const Value& request, qmbed_operator_s& op) {
+  const auto& c = request.at("coefficient").items();
+  if (c.size() != 2) raise(QMBED_INVALID_OPTIONS, "coefficient is a [re, im] pair");
+  const C64 coefficient(c.at(0).as_double(), c.at(1).as_double());
+  const size_t max_degree = request.has("max_degree") ? static_cast<size_t>(request.at("max_degree").as_int()) : 55;
+  const double tolerance = request.has("tolerance") ? request.at("tolerance").as_double() : 0.5 * 2.220446049250313e-16;
+  const size_t substeps = request.has("max_substeps") ? static_cast<size_t>(request.at("max_substeps").as_int()) : 10000;
+  return make_expm_plan(*op.op, coefficient, max_degree, tolerance, substeps);
 }
 
 Value command(const Value& request) {
@@ -684,22 +730,18 @@ Value command(const Value& request) {
   }
   if (operation == "apply_model") {
     auto model = registered_model(request.at("handle").as_string());
-    if (request.has("action") && request.at("action").as_string() != "apply")
-      raise(QMBED_UNSUPPORTED_BACKEND, "only the direct action is supported by the GPU engine");
+    // OperatorActionRequest (bindings/capi/src/lib.rs:937-945): "normal" is the default
+    if (request.has("action") && request.at("action").as_string() != "normal")
+      raise(QMBED_UNSUPPORTED_BACKEND, "only the normal action is supported by the GPU engine");
     auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
     return apply_vectors(*op, parse_vectors(request.at("vectors")));
   }
   if (operation == "create_expm_action") {
     auto model = registered_model(request.at("handle").as_string());
     auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
-    const auto& c = request.at("coefficient").items();
-    const C64 coefficient(c.at(0).as_double(), c.at(1).as_double());
-    const size_t max_degree = request.has("max_degree") ? static_cast<size_t>(request.at("max_degree").as_int()) : 55;
-    const double tolerance = request.has("tolerance") ? request.at("tolerance").as_double() : 0.5 * 2.220446049250313e-16;
-    const size_t substeps = request.has("max_substeps") ? static_cast<size_t>(request.at("max_substeps").as_int()) : 10000;
     auto entry = std::make_shared<ExpmEntry>();
     entry->op = op;
-    entry->plan = make_expm_plan(*op->op, coefficient, max_degree, tolerance, substeps);
+    entry->plan = expm_plan_from(request, *op);
     const uint64_t id = g_next_expm.fetch_add(1);
     {
       std::lock_guard<std::mutex> lock(g_registry_mu);
@@ -713,35 +755,29 @@ Value command(const Value& request) {
   }
   if (operation == "apply_expm_action") {
     auto entry = registered_expm(request.at("expm_handle").as_string());
-    auto vectors = parse_vectors(request.at("vectors"));
-    qmbed_operator_s& h = *entry->op;
-    std::lock_guard<std::mutex> lock(h.mu);
-    const uint64_t dim = h.op->dim();
-    BlockOps& ops = h.block_ops();
-    LinearOperatorView view{dim, h.op->is_real(), [&h, &ops](int prec, bool cplx, const void* x, void* y) {
-                              h.op->apply(prec, cplx, x, y, ops.stream());
-                            }};
-    DeviceBuffer state(std::max<uint64_t>(dim, 1) * 16);
-    std::vector<double> host(2 * dim);
-    Value out = Value::object();
-    out.set("kind", Value::string("vectors"));
-    out.set("dimension", Value::integer(static_cast<long long>(vectors.empty() ? dim : vectors[0].size())));
-    Value vs = Value::array();
-    for (const auto& v : vectors) {
-      if (v.size() != dim) raise(QMBED_DIMENSION_MISMATCH, "exponential batch column has the wrong length");
-      for (uint64_t i = 0; i < dim; ++i) {
-        host[2 * i] = v[i].real();
-        host[2 * i + 1] = v[i].imag();
-      }
-      QMBED_CUDA(cudaMemcpy(state.get(), host.data(), 16 * dim, cudaMemcpyHostToDevice));
-      expm_apply(entry->plan, view, state.get(), 64, ops);
-      QMBED_CUDA(cudaMemcpy(host.data(), state.get(), 16 * dim, cudaMemcpyDeviceToHost));
-      Value r = Value::array();
-      for (uint64_t i = 0; i < dim; ++i) r.push(complex_pair(C64(host[2 * i], host[2 * i + 1])));
-      vs.push(std::move(r));
-    }
-    out.set("vectors", std::move(vs));
-    return out;
+    return expm_vectors(*entry->op, entry->plan, parse_vectors(request.at("vectors")));
+  }
+  if (operation == "eigsh_operator_expression") {
+    // command_eigsh_operator_expression (bindings/capi/src/lib.rs:4172-4190)
+    auto op = expression_operator(request.at("expression"), parse_storage(request));
+    return solve(*op, parse_solver(request.at("solver")), true);
+  }
+  if (operation == "apply_operator_expression") {
+    // command_apply_operator_expression (bindings/capi/src/lib.rs:4078-4105)
+    auto op = expression_operator(request.at("expression"));
+    const auto vectors = parse_vectors(request.at("vectors"));
+    bool ok = !vectors.empty();
+    for (const auto& v : vectors) ok = ok && v.size() == op->op->dim();
+    if (!ok) raise(QMBED_DIMENSION_MISMATCH, "operator expression inputs must be a nonempty batch matching its columns");
+    return apply_vectors(*op, vectors);
+  }
+  if (operation == "expm_operator_expression") {
+    // command_expm_operator_expression (bindings/capi/src/lib.rs:4135-4170)
+    auto op = expression_operator(request.at("expression"));
+    const ExpmPlan plan = expm_plan_from(request, *op);
+    const auto vectors = parse_vectors(request.at("vectors"));
+    if (vectors.empty()) raise(QMBED_INVALID_OPTIONS, "operator exponential requires a nonempty vector batch");
+    return expm_vectors(*op, plan, vectors);
   }
   if (operation == "evolve_model") {
     // command_evolve_model (bindings/capi/src/lib.rs:4673-4694), EvolutionRequest

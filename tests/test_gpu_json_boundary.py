@@ -81,3 +81,38 @@ def test_describe_basis_lists_decimal_states(oracle):
     states, _ = oracle.Basis(8, up=4, momentum=0).states()
     assert result["dimension"] == len(states)
     assert result["states"] == [str(int(s)) for s in states]
+
+
+def test_operator_expression_commands(oracle):
+    """eigsh/apply/expm_operator_expression (bindings/capi/src/lib.rs:4078-4190)
+    on the model expressions the reference's QuSpin-compatible layer sends."""
+    from qmbed_b200 import QmbedError
+    from qmbed_b200._lib import command
+    request = {"basis": {"kind": "spin", "sites": 10, "up": 5, "momentum": 0},
+               "terms": heisenberg_request_terms(10)[1:],
+               "components": [{"name": "delta", "terms": heisenberg_request_terms(10)[:1], "default": [1.0, 0.0]}]}
+    handle = command({"operation": "create_model", **request})["handle"]
+    o = oracle.Operator.build(oracle.Basis(10, up=5, momentum=0), oracle.heisenberg_terms(10, delta=0.4))
+    expr = {"kind": "model", "handle": handle, "parameters": {"delta": [0.4, 0.0]}, "action": "normal"}
+    x = oracle.deterministic_start(o.dim, 5)
+    xs = [[[float(v), 0.0] for v in x]]
+    applied = command({"operation": "apply_operator_expression", "expression": expr, "vectors": xs})
+    assert applied["kind"] == "vectors" and applied["dimension"] == o.dim
+    np.testing.assert_allclose([complex(*p) for p in applied["vectors"][0]], o.apply(x), atol=1e-13)
+    solved = command({"operation": "eigsh_operator_expression", "expression": expr, "format": "csr",
+                      "solver": {"eigenpairs": 2, "target": {"kind": "smallest_algebraic"}, "tolerance": 1e-12,
+                                 "seed": 2}})
+    np.testing.assert_allclose(solved["eigenvalues"], o.eigsh(2, tolerance=1e-12, seed=2).eigenvalues, rtol=1e-10)
+    exp = command({"operation": "expm_operator_expression", "expression": expr, "coefficient": [0.0, -0.5],
+                   "vectors": xs})
+    np.testing.assert_allclose([complex(*p) for p in exp["vectors"][0]], o.expm_apply(-0.5j, x), atol=1e-12)
+    # JSON errors carry the reference's Display texts (src/error.rs:6-35)
+    with pytest.raises(QmbedError, match="^dimension mismatch: operator expression inputs"):
+        command({"operation": "apply_operator_expression", "expression": expr, "vectors": []})
+    with pytest.raises(QmbedError, match="^invalid options: operator exponential requires a nonempty"):
+        command({"operation": "expm_operator_expression", "expression": expr, "coefficient": [0.0, -0.5],
+                 "vectors": []})
+    with pytest.raises(QmbedError, match="^unsupported backend: operator expressions of kind `matrix`"):
+        command({"operation": "apply_operator_expression", "vectors": xs,
+                 "expression": {"kind": "matrix", "operator": {"shape": [1, 1], "entries": []}}})
+    command({"operation": "release_model", "handle": handle})

@@ -284,14 +284,15 @@ def test_lanczos_json_resource_anchor(anchors):
                                         "couplings": [{"coefficient": [c_z, 0.0], "sites": [0]}]}]})["handle"]
 
     probe = model(0.0, 1.0)
-    z = [_lib.command({"operation": "apply_model", "handle": probe,
+    z = [_lib.command({"operation": "apply_model", "handle": probe, "action": "normal",
                        "vectors": [[[1.0 if i == j else 0.0, 0.0] for i in range(2)]]})["vectors"][0][j][0]
          for j in range(2)]
     d = a["diagonal"]
     b = (d[1] - d[0]) / (z[1] - z[0])
     h = model(d[0] - b * z[0], b)
     one = model(1.0, 0.0)
-    expr = {"kind": "model", "handle": h}
+    # the form the reference's QuSpin-compatible tools send for a hamiltonian
+    expr = {"kind": "model", "handle": h, "parameters": {}, "action": "normal"}
     result = _lib.command({"operation": "lanczos_operator", "expression": expr, "initial": a["initial"],
                            "krylov_dimension": a["krylov_dimension"], "tolerance": a["tolerance"]})
     assert result["kind"] == "lanczos" and result["krylov_dimension"] == 2
@@ -319,6 +320,9 @@ def test_lanczos_json_resource_anchor(anchors):
     with pytest.raises(QmbedError, match="exactly one expression"):
         _lib.command({"operation": "lanczos_thermal", "method": "ftlm", "eigenvalues": [0.0], "eigenvectors": [[1.0]],
                       "inverse_temperatures": [1.0], "observables": [{"name": "A"}]})
+    with pytest.raises(QmbedError, match="^unsupported backend: only the normal action"):
+        _lib.command({"operation": "lanczos_operator", "expression": {**expr, "action": "transpose"},
+                      "initial": a["initial"], "krylov_dimension": 2})
     assert _lib.command({"operation": "release_lanczos", "lanczos_handle": handle})["kind"] == "released"
     with pytest.raises(QmbedError):
         _lib.command({"operation": "export_lanczos_basis", "lanczos_handle": handle})
