@@ -355,6 +355,33 @@ QMBED_API int qmbed_gpu_ftlm_sample(qmbed_operator op, int n_vectors, uint64_t s
                                     uint64_t krylov_dimension, double tolerance, double* log_partition,
                                     double* mean_energy, int* lengths);
 
+/* ---- Cross-sector action and spectral functions ----------------------- */
+/* apply_sector_shift (src/operator/mod.rs:2305-2351): terms (same encoding as
+ * qmbed_gpu_operator_create) applied to vectors of `source`, reduced into
+ * `target` (same sites and normalisation; momentum, parity and particle
+ * number may differ). No Hermiticity or particle checks. */
+typedef struct qmbed_shift_s* qmbed_shift;
+QMBED_API int qmbed_gpu_shift_create(qmbed_basis source, qmbed_basis target, int n_terms, const int* arity,
+                                     const char* symbols, const int* n_couplings, const double* coefficients,
+                                     const int* sites, qmbed_shift* out);
+QMBED_API int qmbed_gpu_shift_destroy(qmbed_shift shift);
+/* Host vectors (interleaved complex): n_input = source dimension, n_output =
+ * target dimension, else QMBED_STATUS_DIMENSION_MISMATCH. */
+QMBED_API int qmbed_gpu_shift_apply_host(qmbed_shift shift, uint64_t n_input, const double* x, uint64_t n_output,
+                                         double* y);
+/* Device vectors (interleaved complex FP64), asynchronous on `stream`. */
+QMBED_API int qmbed_gpu_shift_apply_device(qmbed_shift shift, const double* x, double* y, void* stream);
+/* spectral_function (src/dynamics/mod.rs:964-1021): the probe applied to the
+ * source vector (host, n_source complex values), then every eigenpair of the
+ * target Hamiltonian when it has at most 128 states, else the Lanczos spectral
+ * measure of krylov_dimension steps (src/solve/mod.rs:2886-2907); out[f] =
+ * sum_e w_e eta / (pi ((omega_f + reference_energy - E_e)^2 + eta^2)). The
+ * probe's target sector must be the Hamiltonian's. */
+QMBED_API int qmbed_gpu_spectral_function(qmbed_operator target, qmbed_shift probe, uint64_t n_source,
+                                          const double* source, int n_frequencies, const double* frequencies,
+                                          double reference_energy, double broadening, uint64_t krylov_dimension,
+                                          double tolerance, double* out);
+
 /* deterministic_start (src/solve/mod.rs:729-742): normalised LCG vector. */
 QMBED_API int qmbed_gpu_deterministic_start(int device, uint64_t n, uint64_t seed, double* out);
 

@@ -81,6 +81,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_tridiagonal_eigen.argtypes = [ll, vp, vp, vp, vp]
         L.oracle_evolve.argtypes = [vp, vp, ll, vp, ll, d, ll, vp, vp]
         L.oracle_expm_lanczos.argtypes = [vp, vp, d, ll, vp]
+        L.oracle_sector_shift.argtypes = [vp, vp, i, vp, ctypes.c_char_p, vp, vp, vp, ll, vp, ll, vp]
+        L.oracle_spectral_function.argtypes = [vp, vp, ll, vp, d, d, ll, d, vp]
         L.oracle_lanczos_ritz.argtypes = [vp, vp, ll, d, P(ll), P(d), vp, vp, vp, vp, vp]
         L.oracle_thermal_iteration.argtypes = [vp, vp, ll, vp, ll, d, vp, vp, P(ll)]
         L.oracle_thermal_observables.argtypes = [vp, vp, ll, d, i, ll, vp, ll, vp, vp, vp]
@@ -342,6 +344,30 @@ class Operator:
                                                 {"ftlm": 0, "ltlm": 1}[method], len(observables), handles, len(b),
                                                 _ptr(b), _ptr(values), _ptr(identity)))
         return values[:len(observables), :len(b)], identity[:len(b)]
+
+
+    def spectral_function(self, created, frequencies, reference_energy: float, broadening: float,
+                          krylov_dimension: int = 64, tolerance: float = 1e-10) -> np.ndarray:
+        """spectral_function (src/dynamics/mod.rs:964-1021) of the probed vector
+        `created` (= probe applied to the source state) on this target Hamiltonian."""
+        x = np.ascontiguousarray(np.asarray(created, np.complex128))
+        f = np.ascontiguousarray(np.atleast_1d(np.asarray(frequencies, np.float64)))
+        out = np.zeros(max(f.size, 1))
+        _check(lib().oracle_spectral_function(self.handle, _ptr(x), f.size, _ptr(f), reference_energy, broadening,
+                                              krylov_dimension, tolerance, _ptr(out)))
+        return out[:f.size]
+
+
+def sector_shift(source: "Basis", target: "Basis", terms, vector) -> np.ndarray:
+    """apply_sector_shift (src/operator/mod.rs:2305-2351): `terms` applied to a
+    vector of `source`, reduced into `target`."""
+    arity, symbols, n_couplings, coefficients, sites = encode_terms(terms)
+    x = np.ascontiguousarray(np.asarray(vector, np.complex128))
+    y = np.zeros(len(target), np.complex128)
+    _check(lib().oracle_sector_shift(source.handle, target.handle, len(arity), _ptr(arity), symbols,
+                                     _ptr(n_couplings), _ptr(coefficients), _ptr(sites), x.size, _ptr(x), y.size,
+                                     _ptr(y)))
+    return y
 
 
 EVOLUTION_DIAGNOSTICS = ("lanczos_projections", "matrix_vector_products", "real_lanczos_projections",

@@ -1777,6 +1777,87 @@ std::vector<std::vector<C64>> evolve_adaptive(const Operator& op, const std::vec
 }
 
 // ----------------------------------------------------------------------------
+// Cross-sector action and spectral functions (src/operator/mod.rs:2305-2351
+// apply_sector_shift; src/dynamics/mod.rs:903-1021 SpectrumOptions and
+// spectral_function; src/solve/mod.rs:2886-2907 lanczos_spectral_measure,
+// 558-583 hermitian_eigenpairs_all).
+// ----------------------------------------------------------------------------
+std::vector<C64> apply_sector_shift(const SpinBasis& source, const SpinBasis& target, const std::vector<Term>& terms,
+                                    const std::vector<C64>& input) {
+  if (input.size() != source.len())
+    fail(ERR_DIMENSION_MISMATCH, "sector-shift state dimensions do not match source and target bases");
+  std::vector<C64> output(target.len(), C64(0.0, 0.0));
+  for (size_t column = 0; column < input.size(); ++column) {
+    const C64 value = input[column];
+    if (std::abs(value) <= EPS) continue;
+    const u128 state = source.states[column];
+    const size_t orbit = source.transition_orbit_size(state);
+    for (const Term& term : terms)
+      for (const Coupling& coupling : term.couplings)
+        source.visit_transitions(state, term.symbols, coupling.sites, [&](u128 unreduced, C64 local) {
+          size_t row;
+          C64 reduction;
+          if (!target.index_transition(unreduced, orbit, &row, &reduction)) return;
+          output[row] += value * coupling.coefficient * local * reduction;
+        });
+  }
+  return output;
+}
+
+// SpectrumOptions::validate (src/dynamics/mod.rs:945-962)
+void validate_spectrum(const std::vector<double>& frequencies, double reference_energy, double broadening,
+                       size_t krylov, double tolerance) {
+  bool ok = !frequencies.empty() && std::isfinite(reference_energy) && std::isfinite(broadening) &&
+            broadening > 0.0 && krylov > 0 && std::isfinite(tolerance) && tolerance > 0.0;
+  for (double f : frequencies) ok = ok && std::isfinite(f);
+  if (!ok) fail(ERR_INVALID_OPTIONS, "invalid spectrum frequency grid or numerical controls");
+}
+
+// spectral_function on the probed vector `created` (= probe |source>):
+// all eigenpairs when the target has at most 128 states, else the Lanczos
+// spectral measure of `krylov` steps; Lorentzians of width `broadening`.
+std::vector<double> spectral_function(const Operator& target, const std::vector<C64>& created,
+                                      const std::vector<double>& frequencies, double reference_energy,
+                                      double broadening, size_t krylov, double tolerance) {
+  validate_spectrum(frequencies, reference_energy, broadening, krylov, tolerance);
+  if (target.rows != target.cols || created.size() != target.rows)
+    fail(ERR_DIMENSION_MISMATCH, "target Hamiltonian, source, and probe shapes are incompatible");
+  std::vector<double> energies, weights;
+  const size_t n = target.rows;
+  if (n <= 128) {
+    std::vector<C64> dense(n * n, C64(0.0, 0.0));
+    for (size_t r = 0; r < n; ++r)
+      for (size_t p = target.row_ptr[r]; p < target.row_ptr[r + 1]; ++p) dense[r * n + target.col_idx[p]] += target.values[p];
+    for (size_t r = 0; r < n; ++r)
+      for (size_t c = 0; c < n; ++c)
+        if (std::abs(dense[r * n + c] - std::conj(dense[c * n + r])) > 1.0e-12) fail(ERR_NON_HERMITIAN, "");
+    std::vector<C64> vectors;
+    hermitian_jacobi(n, dense, energies, vectors);
+    for (size_t e = 0; e < n; ++e) {
+      C64 overlap(0.0, 0.0);
+      for (size_t i = 0; i < n; ++i) overlap += std::conj(vectors[i + n * e]) * created[i];
+      weights.push_back(std::norm(overlap));
+    }
+  } else {
+    const Projection p = lanczos_projection(target, created, krylov);
+    energies = p.eigenvalues;
+    for (size_t e = 0; e < p.eigenvalues.size(); ++e)
+      weights.push_back(p.initial_norm * p.initial_norm * p.vec(0, e) * p.vec(0, e));
+  }
+  std::vector<double> out;
+  const double pi = 3.14159265358979323846;
+  for (double frequency : frequencies) {
+    double sum = 0.0;
+    for (size_t e = 0; e < energies.size(); ++e) {
+      const double detuning = frequency + reference_energy - energies[e];
+      sum += weights[e] * broadening / (pi * (detuning * detuning + broadening * broadening));
+    }
+    out.push_back(sum);
+  }
+  return out;
+}
+
+// ----------------------------------------------------------------------------
 // Full Lanczos decomposition and thermal Lanczos (src/solve/mod.rs:2674-2857
 // lanczos_iter / lanczos_full / lanczos_ritz, 3457-3568 thermal static
 // iteration, 3575-3940 projected observables and FTLM/LTLM contractions).
@@ -2345,6 +2426,42 @@ int oracle_thermal_observables(void* handle, const double* initial, long long kr
         values[2 * (o * grid.size() + b) + 1] = out[o][b].imag();
       }
     for (size_t b = 0; b < grid.size(); ++b) identity[b] = id[b];
+  });
+}
+
+// apply_sector_shift (src/operator/mod.rs:2305-2351): input on `source`,
+// output on `target` (interleaved complex).
+int oracle_sector_shift(void* source, void* target, int n_terms, const int* arity, const char* symbols,
+                        const int* n_couplings, const double* coefficients, const int* sites, long long n_input,
+                        const double* input, long long n_output, double* output) {
+  return guarded([&] {
+    const SpinBasis& s = *static_cast<SpinBasis*>(source);
+    const SpinBasis& t = *static_cast<SpinBasis*>(target);
+    auto terms = decode_terms(n_terms, arity, symbols, n_couplings, coefficients, sites);
+    if (n_output != static_cast<long long>(t.len()))
+      fail(ERR_DIMENSION_MISMATCH, "sector-shift state dimensions do not match source and target bases");
+    std::vector<C64> x(static_cast<size_t>(std::max(n_input, 0LL)));
+    for (size_t i = 0; i < x.size(); ++i) x[i] = C64(input[2 * i], input[2 * i + 1]);
+    const std::vector<C64> y = apply_sector_shift(s, t, terms, x);
+    for (size_t i = 0; i < y.size(); ++i) {
+      output[2 * i] = y[i].real();
+      output[2 * i + 1] = y[i].imag();
+    }
+  });
+}
+
+// spectral_function (src/dynamics/mod.rs:964-1021) of the probed vector.
+int oracle_spectral_function(void* target, const double* created, long long n_frequencies, const double* frequencies,
+                             double reference_energy, double broadening, long long krylov, double tolerance,
+                             double* out) {
+  return guarded([&] {
+    const Operator& op = *static_cast<Operator*>(target);
+    std::vector<C64> v(op.rows);
+    for (size_t i = 0; i < op.rows; ++i) v[i] = C64(created[2 * i], created[2 * i + 1]);
+    const std::vector<double> f(frequencies, frequencies + std::max(n_frequencies, 0LL));
+    const std::vector<double> r = spectral_function(op, v, f, reference_energy, broadening,
+                                                    static_cast<size_t>(std::max(krylov, 0LL)), tolerance);
+    for (size_t i = 0; i < r.size(); ++i) out[i] = r[i];
   });
 }
 

@@ -124,6 +124,11 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_lanczos_project.argtypes = [vp, i, vp, vp]
     L.qmbed_gpu_thermal_contraction.argtypes = [i, i, vp, vp, i, vp, i, vp, vp, vp]
     L.qmbed_gpu_thermal_iteration.argtypes = [vp, vp, i, vp, u64, d, vp, vp, P(u64)]
+    L.qmbed_gpu_shift_create.argtypes = [vp, vp, i, vp, ctypes.c_char_p, vp, vp, vp, P(vp)]
+    L.qmbed_gpu_shift_destroy.argtypes = [vp]
+    L.qmbed_gpu_shift_apply_host.argtypes = [vp, u64, vp, u64, vp]
+    L.qmbed_gpu_shift_apply_device.argtypes = [vp, vp, vp, vp]
+    L.qmbed_gpu_spectral_function.argtypes = [vp, vp, u64, vp, i, vp, d, d, u64, d, vp]
     L.qmbed_gpu_ftlm_start.argtypes = [vp, u64, i, vp]
     L.qmbed_gpu_ftlm_sample.argtypes = [vp, i, u64, i, vp, u64, d, vp, vp, vp]
     L.qmbed_gpu_mlp_create.argtypes = [i, i, i, i, i, u64, P(vp)]

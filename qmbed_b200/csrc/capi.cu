@@ -23,6 +23,7 @@
 #include "json.hpp"
 #include "mlp.cuh"
 #include "operator.cuh"
+#include "spectrum.cuh"
 #include "thermal.cuh"
 
 namespace qmbed {
@@ -1644,6 +1645,102 @@ int qmbed_gpu_ftlm_start(qmbed_operator op, uint64_t seed, int index, double* ou
     if (view.real) ops.widen_real(v.as<double>(), wide.as<double>(), n);
     QMBED_CUDA(cudaMemcpyAsync(out, view.real ? wide.get() : v.get(), n * 16, cudaMemcpyDeviceToHost, ops.stream()));
     ops.sync();
+  });
+}
+
+struct qmbed_shift_s {
+  std::shared_ptr<SpinBasis> target;
+  std::shared_ptr<SpinOperator> terms;  // on the source basis
+  cudaStream_t stream = nullptr;
+  std::unique_ptr<BlockOps> ops;
+  std::mutex mu;
+  ~qmbed_shift_s() {
+    ops.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
+  BlockOps& block_ops() {
+    if (!ops) {
+      QMBED_CUDA(cudaSetDevice(target->device()));
+      QMBED_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+      ops = std::make_unique<BlockOps>(target->device(), stream);
+    }
+    return *ops;
+  }
+};
+
+int qmbed_gpu_shift_create(qmbed_basis source, qmbed_basis target, int n_terms, const int* arity, const char* symbols,
+                           const int* n_couplings, const double* coefficients, const int* sites, qmbed_shift* out) {
+  return guarded([&] {
+    if (!source || !target || !out) raise(QMBED_INVALID_OPTIONS, "a sector shift needs two bases and an output");
+    auto terms = decode_terms(n_terms, arity, symbols, n_couplings, coefficients, sites);
+    OperatorChecks checks;
+    checks.hermiticity = false;
+    checks.particle_conservation = false;
+    auto h = std::make_unique<qmbed_shift_s>();
+    h->target = target->basis;
+    h->terms = std::make_shared<SpinOperator>(source->basis, terms, checks, kStorageMatrixFree);
+    if (h->target->sites() != source->basis->sites() || h->target->device() != source->basis->device())
+      raise(QMBED_DIMENSION_MISMATCH, "sector-shift state dimensions do not match source and target bases");
+    *out = h.release();
+  });
+}
+
+int qmbed_gpu_shift_destroy(qmbed_shift shift) {
+  return guarded([&] { delete shift; });
+}
+
+int qmbed_gpu_shift_apply_device(qmbed_shift shift, const double* x, double* y, void* stream) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(shift->mu);
+    shift->terms->apply_shift(*shift->target, x, y, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int qmbed_gpu_shift_apply_host(qmbed_shift shift, uint64_t n_input, const double* x, uint64_t n_output, double* y) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(shift->mu);
+    const uint64_t ns = shift->terms->dim(), nt = shift->target->dim();
+    if (n_input != ns || n_output != nt)
+      raise(QMBED_DIMENSION_MISMATCH, "sector-shift state dimensions do not match source and target bases");
+    BlockOps& ops = shift->block_ops();
+    DeviceBuffer dx(std::max<uint64_t>(ns, 1) * 16), dy(std::max<uint64_t>(nt, 1) * 16);
+    QMBED_CUDA(cudaMemcpyAsync(dx.get(), x, ns * 16, cudaMemcpyHostToDevice, ops.stream()));
+    shift->terms->apply_shift(*shift->target, dx.as<double>(), dy.as<double>(), ops.stream());
+    QMBED_CUDA(cudaMemcpyAsync(y, dy.get(), nt * 16, cudaMemcpyDeviceToHost, ops.stream()));
+    ops.sync();
+  });
+}
+
+int qmbed_gpu_spectral_function(qmbed_operator target, qmbed_shift probe, uint64_t n_source, const double* source,
+                                int n_frequencies, const double* frequencies, double reference_energy,
+                                double broadening, uint64_t krylov_dimension, double tolerance, double* out) {
+  return guarded([&] {
+    if (!target || !probe || !source || !out || n_frequencies < 0 || (n_frequencies > 0 && !frequencies))
+      raise(QMBED_INVALID_OPTIONS, "a spectrum needs a target Hamiltonian, a probe, a source and a frequency grid");
+    SpectrumOptions o;
+    o.frequencies.assign(frequencies, frequencies + n_frequencies);
+    o.reference_energy = reference_energy;
+    o.broadening = broadening;
+    o.krylov_dimension = krylov_dimension;
+    o.tolerance = tolerance;
+    validate_spectrum(o);
+    std::lock_guard<std::mutex> lock(target->mu);
+    std::lock_guard<std::mutex> plock(probe->mu);
+    const uint64_t nt = target->op->dim(), ns = probe->terms->dim();
+    // the probe must land in the target Hamiltonian's sector
+    const SectorParams& a = probe->target->params();
+    const SectorParams& b = target->op->basis().params();
+    const bool same = a.sites == b.sites && a.up == b.up && a.has_momentum == b.has_momentum &&
+                      a.momentum == b.momentum && a.parity == b.parity &&
+                      probe->target->normalization() == target->op->basis().normalization();
+    if (!same || probe->target->dim() != nt || n_source != ns)
+      raise(QMBED_DIMENSION_MISMATCH, "target Hamiltonian, source, and probe shapes are incompatible");
+    BlockOps& ops = target->block_ops();
+    DeviceBuffer dx(std::max<uint64_t>(ns, 1) * 16), created(std::max<uint64_t>(nt, 1) * 16);
+    QMBED_CUDA(cudaMemcpyAsync(dx.get(), source, ns * 16, cudaMemcpyHostToDevice, ops.stream()));
+    probe->terms->apply_shift(*probe->target, dx.as<double>(), created.as<double>(), ops.stream());
+    const std::vector<double> r = spectral_function(target->view(), created.as<double>(), o, ops);
+    std::copy(r.begin(), r.end(), out);
   });
 }
 

@@ -8,6 +8,7 @@
 //   projected_exponential_error_bound     3146-3195
 //   evolve_hermitian_adaptive_grid        3197-3316
 //   expm_lanczos                          3432-3454
+//   lanczos_spectral_measure              2886-2907
 // The recurrence, the real fast path (real operator and exactly real state),
 // the a-posteriori error bound and the accept/halve/bisect step control are
 // the reference's. Basis vectors live in one column-major FP64 device panel;
@@ -194,6 +195,16 @@ bool host_vector_is_real(const double* v, uint64_t n) {
 }
 
 }  // namespace
+
+void lanczos_spectral_measure(const LinearOperatorView& op, const double* source, bool source_real, size_t krylov,
+                              std::vector<double>& energies, std::vector<double>& weights, BlockOps& ops) {
+  if (krylov == 0) raise(QMBED_INVALID_OPTIONS, "spectral Krylov dimension must be positive");
+  KrylovExp k(op, ops, krylov);
+  const Projection p = k.project(source, source_real);
+  energies = p.eigenvalues;
+  weights.assign(static_cast<size_t>(p.size), 0.0);
+  for (int e = 0; e < p.size; ++e) weights[e] = p.initial_norm * p.initial_norm * p.vec(0, e) * p.vec(0, e);
+}
 
 // EvolutionOptions::validate (src/solve/mod.rs:2510-2530)
 void validate_evolution(const EvolutionOptions& o) {

@@ -41,4 +41,11 @@ void evolve(const LinearOperatorView& op, const double* initial, const Evolution
 void expm_lanczos(const LinearOperatorView& op, const double* initial, double time, size_t krylov, double* out,
                   BlockOps& ops);
 
+// lanczos_spectral_measure (src/solve/mod.rs:2886-2907): Ritz values of the
+// unreorthogonalised Lanczos projection of a device vector (interleaved
+// complex FP64; `source_real` when every imaginary part is zero) and their
+// weights |v|^2 V[0, e]^2.
+void lanczos_spectral_measure(const LinearOperatorView& op, const double* source, bool source_real, size_t krylov,
+                              std::vector<double>& energies, std::vector<double>& weights, BlockOps& ops);
+
 }  // namespace qmbed

@@ -728,6 +728,48 @@ int grid_for(uint64_t work, int threads, int per_sm = 8) {
   return static_cast<int>(std::max<uint64_t>(1, std::min(blocks, cap)));
 }
 
+// apply_sector_shift (src/operator/mod.rs:2305-2351): one thread per source
+// column; the forward products act on the column's representative, each
+// target state is reduced into the target sector (index_transition,
+// src/basis/mod.rs:1561-1580: sqrt(R_source / R_target) conj(phase), or 1
+// when the target carries no symmetry) and added to its row atomically.
+template <typename S>
+__global__ void __launch_bounds__(128) sector_shift_kernel(OpView<S> src, OpView<S> tgt, const double* __restrict__ x,
+                                                           double* __restrict__ y) {
+  extern __shared__ Instance shared_inst[];
+  const bool in_smem = src.n_inst <= kSmemInstances;
+  if (in_smem)
+    for (int k = threadIdx.x; k < src.n_inst; k += blockDim.x) shared_inst[k] = src.inst[k];
+  __syncthreads();
+  const Instance* inst = in_smem ? shared_inst : src.inst;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t c = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < src.dim; c += stride) {
+    const double xr = x[2 * c], xi = x[2 * c + 1];
+    if (hypot(xr, xi) <= 2.220446049250313e-16) continue;
+    const S s = row_state(src, c);
+    const int orbit = src.p.symmetric ? src.orbits[c] : 1;
+    for (int k = 0; k < src.n_inst; ++k) {
+      S t;
+      double ar, ai;
+      if (!apply_instance(inst[k], s, src.f, t, ar, ai)) continue;
+      const Located L = locate(tgt, t);
+      if (L.col < 0) continue;
+      // coefficient * local amplitude * reduction amplitude
+      double wr = inst[k].cr * ar - inst[k].ci * ai;
+      double wi = inst[k].cr * ai + inst[k].ci * ar;
+      if (tgt.p.symmetric) {
+        const double ratio = tgt.inv_sqrt[257 + orbit] * tgt.inv_sqrt[L.orbit];
+        const double pr = L.pr * ratio, pi = -L.pi * ratio;
+        const double nr = wr * pr - wi * pi;
+        wi = wr * pi + wi * pr;
+        wr = nr;
+      }
+      atomicAdd(&y[2 * L.col], xr * wr - xi * wi);
+      atomicAdd(&y[2 * L.col + 1], xr * wi + xi * wr);
+    }
+  }
+}
+
 template <typename S>
 OpView<S> make_view(const SpinBasis& b, const DeviceBuffer& inst, int n_inst, const LocalFactors& f,
                     const DeviceBuffer& inv_sqrt) {
@@ -1365,6 +1407,27 @@ void SpinOperator::apply_block(int precision, int nb, const void* z, const void*
   if (dim() == 0) return;
   const int shape = block_shape(precision, nb, z, p, alpha, beta, gamma, stream);
   launch_block(shape, precision, nb, z, p, out, alpha, beta, gamma, stream);
+}
+
+void SpinOperator::apply_shift(const SpinBasis& target, const double* x, double* y, cudaStream_t stream) const {
+  QMBED_CUDA(cudaSetDevice(basis_->device()));
+  if (target.sites() != basis_->sites() || target.words() != basis_->words() ||
+      target.device() != basis_->device())
+    raise(QMBED_DIMENSION_MISMATCH, "sector-shift state dimensions do not match source and target bases");
+  QMBED_CUDA(cudaMemsetAsync(y, 0, std::max<uint64_t>(target.dim(), 1) * 16, stream));
+  if (dim() == 0 || target.dim() == 0 || n_inst_ == 0) return;
+  const int grid = grid_for(dim(), 128, 16);
+  const size_t smem = n_inst_ <= kSmemInstances ? static_cast<size_t>(n_inst_) * sizeof(Instance) : 0;
+  DeviceBuffer unused;
+  auto run = [&](auto tag) {
+    using S = decltype(tag);
+    auto src = make_view<S>(*basis_, inst_fwd_, n_inst_, factors_, inv_sqrt_);
+    auto tgt = make_view<S>(target, unused, 0, factors_, inv_sqrt_);
+    sector_shift_kernel<S><<<grid, 128, smem, stream>>>(src, tgt, x, y);
+  };
+  if (basis_->words() == 1) run(uint64_t{});
+  else run(u128{});
+  QMBED_LAUNCH_CHECK();
 }
 
 void SpinOperator::export_csr(std::vector<uint64_t>& row_ptr, std::vector<uint32_t>& cols,

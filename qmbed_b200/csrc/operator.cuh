@@ -122,6 +122,11 @@ class SpinOperator {
 
   // Assembled rows on the host (for tests): row pointer, columns, values.
   void export_csr(std::vector<uint64_t>& row_ptr, std::vector<uint32_t>& cols, std::vector<C64>& values) const;
+  // apply_sector_shift (src/operator/mod.rs:2305-2351): these terms applied to
+  // a vector of this operator's basis (the source) and reduced into `target`
+  // (same sites, same device). x: source dimension, y: target dimension,
+  // both interleaved complex FP64 on the device; y is overwritten.
+  void apply_shift(const SpinBasis& target, const double* x, double* y, cudaStream_t stream) const;
 
   // Exact stored 1-norm and trace shift (shifted_trace_and_one_norm,
   // src/solve/mod.rs:59-104), computed on the device.

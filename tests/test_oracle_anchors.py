@@ -410,3 +410,82 @@ def test_thermal_errors(oracle):
     with pytest.raises(OracleError) as e:
         op.thermal_iteration(np.zeros(2, complex), [1.0], 2, 1e-12)
     assert e.value.code == 14
+
+
+def _projector(oracle, sector, full_basis):
+    """Columns: the sector's basis vectors in the fixed-weight space (P[s, col] = phase / sqrt(R))."""
+    full_states, _ = full_basis.states()
+    position = {int(s): i for i, s in enumerate(full_states)}
+    reps, _ = sector.states()
+    P = np.zeros((len(full_states), len(reps)), np.complex128)
+    for col, rep in enumerate(reps.tolist()):
+        for s in full_states.tolist():
+            image = sector.image(s)
+            if image and image[0] == rep:
+                P[position[s], col] = image[1] / np.sqrt(image[2])
+    return P
+
+
+def _shift_matrix(oracle, source, target, terms):
+    n = len(source)
+    return np.column_stack([oracle.sector_shift(source, target, terms, np.eye(n)[c]) for c in range(n)])
+
+
+@pytest.mark.parametrize("sites,up_s,up_t,k_s,k_t,symbol,q", [
+    (4, 0, 1, 0, 1, "+", 1),     # tests/general_tensor_wide_basis.rs:164-217
+    (8, 4, 4, 1, 4, "z", 3),
+    (10, 4, 5, 2, 5, "+", 3),
+    (9, 4, 4, 0, 2, "z", 2),
+])
+def test_sector_shift_equals_projected_full_action(oracle, sites, up_s, up_t, k_s, k_t, symbol, q):
+    """apply_sector_shift (src/operator/mod.rs:2305-2351) between momentum
+    sectors equals P_t^dag O P_s with O acting on the fixed-weight spaces."""
+    terms = [(symbol, [(np.exp(-2j * np.pi * q * j / sites), (j,)) for j in range(sites)])]
+    source = oracle.Basis(sites, up=up_s, momentum=k_s)
+    target = oracle.Basis(sites, up=up_t, momentum=k_t)
+    full_s, full_t = oracle.Basis(sites, up=up_s), oracle.Basis(sites, up=up_t)
+    reduced = _shift_matrix(oracle, source, target, terms)
+    expected = _projector(oracle, target, full_t).conj().T @ _shift_matrix(oracle, full_s, full_t, terms) \
+        @ _projector(oracle, source, full_s)
+    np.testing.assert_allclose(reduced, expected, atol=1e-12)
+    assert np.max(np.abs(reduced)) > 0.5
+    if sites == 4:
+        assert reduced.shape == (1, 1) and abs(reduced[0, 0]) > 1.0
+
+
+def test_sector_shift_errors(oracle):
+    from oracle.oracle import OracleError
+    source, target = oracle.Basis(6, up=3), oracle.Basis(6, up=4)
+    with pytest.raises(OracleError) as e:
+        oracle.sector_shift(source, target, [("+", [(1.0, (0,))])], np.ones(3))
+    assert e.value.code == 9
+
+
+def test_spectrum_single_pole_anchor(oracle):
+    """tests/visible_contract.rs:1128-1143: H = [1], probe = [1], omega = 1,
+    broadening 0.5 gives 2/pi."""
+    h = oracle.Operator.diagonal([1.0])
+    out = h.spectral_function(np.ones(1, complex), [1.0], 0.0, 0.5, krylov_dimension=8, tolerance=1e-12)
+    assert abs(out[0] - 2.0 / np.pi) <= 1e-12
+
+
+@pytest.mark.parametrize("sites,k", [(10, 0), (14, 0)])
+def test_spectral_function_matches_dense_lehmann_sum(oracle, sites, k):
+    """S(q=pi, omega) of the ground state: the dense path (D <= 128) and the
+    Lanczos measure (D > 128) against the Lehmann sum from numpy."""
+    basis = oracle.Basis(sites, up=sites // 2, momentum=k)
+    h = oracle.Operator.build(basis, oracle.heisenberg_terms(sites))
+    target = oracle.Basis(sites, up=sites // 2, momentum=(k + sites // 2) % sites)
+    ht = oracle.Operator.build(target, oracle.heisenberg_terms(sites))
+    ground = h.eigsh(1, tolerance=1e-12, seed=1, eigenvectors=True)
+    probe = [("z", [((-1.0) ** j, (j,)) for j in range(sites)])]
+    created = oracle.sector_shift(basis, target, probe, ground.eigenvectors[0])
+    freqs = np.linspace(0.0, 4.0, 41)
+    e0, eta = ground.eigenvalues[0], 0.4
+    out = ht.spectral_function(created, freqs, e0, eta, krylov_dimension=min(ht.dim, 200))
+    w, u = np.linalg.eigh(ht.dense())
+    weight = np.abs(u.conj().T @ created) ** 2
+    exact = [(weight * eta / (np.pi * ((f + e0 - w) ** 2 + eta ** 2))).sum() for f in freqs]
+    tol = 1e-10 if ht.dim <= 128 else 1e-6
+    np.testing.assert_allclose(out, exact, atol=tol * max(exact))
+    assert np.all(out >= -1e-12)
