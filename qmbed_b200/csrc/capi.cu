@@ -829,6 +829,52 @@ Value command(const Value& request) {
     out.set("states", std::move(states));
     return out;
   }
+  if (operation == "apply_terms_between_models") {
+    // registered_cross_sector_action (bindings/capi/src/lib.rs:4871-4915) for
+    // two spin-sector models: apply_sector_shift of the request's terms
+    auto source = registered_model(request.at("source_handle").as_string());
+    auto target = registered_model(request.at("target_handle").as_string());
+    const auto terms = parse_terms(request.at("terms"));
+    const auto vectors = parse_vectors(request.at("vectors"));
+    OperatorChecks checks;
+    checks.hermiticity = false;
+    checks.particle_conservation = false;
+    if (source->basis->sites() != target->basis->sites() ||
+        source->basis->normalization() != target->basis->normalization())
+      raise(QMBED_INVALID_OPTIONS, "source and target models use different site conventions");
+    SpinOperator shift(source->basis, terms, checks, kStorageMatrixFree);
+    const uint64_t ns = source->basis->dim(), nt = target->basis->dim();
+    cudaStream_t stream;
+    QMBED_CUDA(cudaSetDevice(source->basis->device()));
+    QMBED_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    std::vector<double> host;
+    try {
+      DeviceBuffer dx(std::max<uint64_t>(ns, 1) * 16), dy(std::max<uint64_t>(nt, 1) * 16);
+      std::vector<double> in(2 * ns), out(2 * nt);
+      for (const auto& v : vectors) {
+        if (v.size() != ns)
+          raise(QMBED_DIMENSION_MISMATCH, "sector-shift state dimensions do not match source and target bases");
+        for (uint64_t i = 0; i < ns; ++i) {
+          in[2 * i] = v[i].real();
+          in[2 * i + 1] = v[i].imag();
+        }
+        QMBED_CUDA(cudaMemcpyAsync(dx.get(), in.data(), ns * 16, cudaMemcpyHostToDevice, stream));
+        shift.apply_shift(*target->basis, dx.as<double>(), dy.as<double>(), stream);
+        QMBED_CUDA(cudaMemcpyAsync(out.data(), dy.get(), nt * 16, cudaMemcpyDeviceToHost, stream));
+        QMBED_CUDA(cudaStreamSynchronize(stream));
+        host.insert(host.end(), out.begin(), out.end());
+      }
+    } catch (...) {
+      cudaStreamDestroy(stream);
+      throw;
+    }
+    cudaStreamDestroy(stream);
+    Value out = Value::object();
+    out.set("kind", Value::string("vectors"));
+    out.set("dimension", Value::integer(static_cast<long long>(nt)));
+    out.set("vectors", vectors_value(host, nt, vectors.size()));
+    return out;
+  }
   if (operation == "lanczos_operator") {
     // command_lanczos_operator (bindings/capi/src/lib.rs:4046-4075); tolerance
     // default 1e-13 (default_lanczos_tolerance, lib.rs:2107-2109)

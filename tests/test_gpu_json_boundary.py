@@ -116,3 +116,44 @@ def test_operator_expression_commands(oracle):
         command({"operation": "apply_operator_expression", "vectors": xs,
                  "expression": {"kind": "matrix", "operator": {"shape": [1, 1], "entries": []}}})
     command({"operation": "release_model", "handle": handle})
+
+
+@pytest.mark.parametrize("sites", [20, 100])
+def test_apply_terms_between_models(oracle, sites):
+    """apply_terms_between_models (bindings/capi/src/lib.rs:4871-4915; anchor
+    6586-6626): sum_j S+_j from the k=0 all-down sector into the k=0 one-magnon
+    sector multiplies by sqrt(L)."""
+    from qmbed_b200 import QmbedError
+    from qmbed_b200._lib import command
+    src = command({"operation": "create_model", "basis": {"kind": "spin", "sites": sites, "up": 0, "momentum": 0},
+                   "terms": []})["handle"]
+    tgt = command({"operation": "create_model", "basis": {"kind": "spin", "sites": sites, "up": 1, "momentum": 0},
+                   "terms": []})["handle"]
+    raising = [{"product": {"local": ["raising"]},
+                "couplings": [{"coefficient": [1.0, 0.0], "sites": [j]} for j in range(sites)]}]
+    out = command({"operation": "apply_terms_between_models", "source_handle": src, "target_handle": tgt,
+                   "terms": raising, "vectors": [[[1.0, 0.0]]]})
+    assert out["kind"] == "vectors" and out["dimension"] == 1
+    assert abs(out["vectors"][0][0][0] - np.sqrt(sites)) < 1e-12 and abs(out["vectors"][0][0][1]) < 1e-12
+    if sites == 20:
+        # a momentum-changing shift on larger sectors against the oracle
+        a = command({"operation": "create_model", "basis": {"kind": "spin", "sites": 12, "up": 6, "momentum": 1},
+                     "terms": []})["handle"]
+        b = command({"operation": "create_model", "basis": {"kind": "spin", "sites": 12, "up": 5, "momentum": 4},
+                     "terms": []})["handle"]
+        coeff = [np.exp(-2j * np.pi * 3 * j / 12) for j in range(12)]
+        lowering = [{"product": {"local": ["lowering"]},
+                     "couplings": [{"coefficient": [c.real, c.imag], "sites": [j]} for j, c in enumerate(coeff)]}]
+        ob_s, ob_t = oracle.Basis(12, up=6, momentum=1), oracle.Basis(12, up=5, momentum=4)
+        x = np.random.default_rng(1).standard_normal(len(ob_s))
+        out = command({"operation": "apply_terms_between_models", "source_handle": a, "target_handle": b,
+                       "terms": lowering, "vectors": [[[float(v), 0.0] for v in x]]})
+        ref = oracle.sector_shift(ob_s, ob_t, [("-", [(c, (j,)) for j, c in enumerate(coeff)])], x)
+        np.testing.assert_allclose([complex(*p) for p in out["vectors"][0]], ref, atol=1e-13)
+        with pytest.raises(QmbedError, match="^dimension mismatch"):
+            command({"operation": "apply_terms_between_models", "source_handle": a, "target_handle": b,
+                     "terms": lowering, "vectors": [[[1.0, 0.0]]]})
+        for m in (a, b):
+            command({"operation": "release_model", "handle": m})
+    for m in (src, tgt):
+        command({"operation": "release_model", "handle": m})
