@@ -448,14 +448,16 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
   BlockSolver solver(op, o, ops, nb);
 
   // Start columns: the caller's vectors (real parts), then reference
-  // deterministic starts with seeds o.seed + j * 0x9e3779b9.
+  // deterministic starts with seeds o.seed + j * 0x9e3779b9 for the remaining
+  // column positions j (a caller's vector equal to the default start of
+  // column 0 is then not repeated).
   // Workspace slots of the handle: 0 start columns, 1-3 FP32 blocks, 4-6 FP64 blocks.
   const size_t block32 = static_cast<size_t>(n) * nb * 4, block64 = static_cast<size_t>(n) * nb * 8;
   double* cols = static_cast<double*>(ops.workspace(0, block64));
   auto col = [&](int j) { return cols + static_cast<size_t>(j) * n; };
   const int used = std::min(n_initial, nb);
   for (int j = 0; j < used; ++j) ops.import_complex(staged_initial + 2 * static_cast<size_t>(j) * n, col(j), n, 64, false);
-  for (int j = used; j < nb; ++j) ops.lcg_start(col(j), n, o.seed + static_cast<uint64_t>(j - used) * 0x9e3779b9ULL, 64, false);
+  for (int j = used; j < nb; ++j) ops.lcg_start(col(j), n, o.seed + static_cast<uint64_t>(j) * 0x9e3779b9ULL, 64, false);
 
   // QMBED_FILTER_TRACE=1 prints one line per outer iteration to stderr
   const char* trace_env = std::getenv("QMBED_FILTER_TRACE");

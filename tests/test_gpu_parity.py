@@ -280,6 +280,20 @@ def test_filtered_eigsh_warm_start(engine, oracle):
     np.testing.assert_allclose(second.eigenvalues, first.eigenvalues, rtol=1e-12)
 
 
+def test_filtered_eigsh_with_the_default_start_as_initial_vector(engine, oracle):
+    """A caller's vector equal to the solver's own first start column (the
+    deterministic start of the seed) must not be repeated in the start block:
+    the solve costs what the solve without an initial vector costs."""
+    terms = oracle.heisenberg_terms(20, delta=0.9)
+    g = engine.GpuOperator(engine.GpuBasis(20, up=10, momentum=0, parity=1), terms)
+    plain = g.eigsh(4, tolerance=1e-10, seed=0, mode="filtered")
+    v0 = engine.deterministic_start(g.dim, 0)
+    seeded = g.eigsh(4, tolerance=1e-10, seed=0, mode="filtered", initial=v0[None, :])
+    np.testing.assert_allclose(seeded.eigenvalues, plain.eigenvalues, rtol=1e-12)
+    assert seeded.operator_applications <= 1.25 * plain.operator_applications
+    assert seeded.fp32_iterations > 0  # the random start is not taken for a converged subspace
+
+
 @pytest.mark.parametrize("shape", ["0", "1", "2", "3"])
 @pytest.mark.parametrize("sites,up,momentum,parity,nb,precision", [
     (16, 8, 0, 1, 8, 64), (16, 8, 0, 1, 16, 64), (16, 8, 0, 1, 8, 32), (14, 7, None, None, 16, 32),
