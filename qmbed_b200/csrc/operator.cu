@@ -680,6 +680,70 @@ __global__ void __launch_bounds__(256) spmm_packed_kernel(uint64_t n, const IDX*
   }
 }
 
+// Block action on the fly (matrix-free storage, real operators): one thread
+// per row expands the adjoint products once and applies each transition to
+// all NB columns of the row-major block, so the integer work of the expansion
+// is shared by the NB vectors. In coordinates z = x / sqrt(R) the orbit ratio
+// cancels: (S^-1 H S)[r, c] = conj(coefficient * amplitude) * phase.
+// Epilogue as spmm_packed_kernel: out = alpha (S^-1 H S z) + beta z + gamma p.
+template <typename S, typename T, int NB, bool HAS_P>
+__global__ void __launch_bounds__(128) spmm_matrix_free_kernel(OpView<S> v, const T* __restrict__ z, const T* p,
+                                                               T* out, T alpha, T beta, T gamma) {
+  constexpr int VEC = 16 / sizeof(T);
+  constexpr int PARTS = NB / VEC;
+  extern __shared__ Instance shared_inst[];
+  const bool in_smem = v.n_inst <= kSmemInstances;
+  if (in_smem)
+    for (int k = threadIdx.x; k < v.n_inst; k += blockDim.x) shared_inst[k] = v.inst[k];
+  __syncthreads();
+  const Instance* inst = in_smem ? shared_inst : v.inst;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < v.dim; r += stride) {
+    const S s = row_state(v, r);
+    T acc[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) acc[j] = 0;
+    double diag = 0.0;
+    for (int k = 0; k < v.n_inst; ++k) {
+      S t;
+      double ar, ai;
+      if (!apply_instance(inst[k], s, v.f, t, ar, ai)) continue;
+      // real operators: conj(coefficient * amplitude) is real
+      const double w = inst[k].cr * ar - inst[k].ci * ai;
+      if (t == s) {
+        diag += w;
+        continue;
+      }
+      const Located L = locate(v, t);
+      if (L.col < 0) continue;
+      const T c = static_cast<T>(w * L.pr);
+      const T* row = z + static_cast<uint64_t>(L.col) * NB;
+#pragma unroll
+      for (int q = 0; q < PARTS; ++q) {
+        T g[VEC];
+        load16(row + q * VEC, g);
+#pragma unroll
+        for (int u = 0; u < VEC; ++u) acc[q * VEC + u] += c * g[u];
+      }
+    }
+    const T d = static_cast<T>(diag);
+#pragma unroll
+    for (int q = 0; q < PARTS; ++q) {
+      T self[VEC], o[VEC];
+      load16(z + r * NB + q * VEC, self);
+#pragma unroll
+      for (int u = 0; u < VEC; ++u) o[u] = alpha * (acc[q * VEC + u] + d * self[u]) + beta * self[u];
+      if (HAS_P) {
+        T pv[VEC];
+        load16_rw(p + r * NB + q * VEC, pv);
+#pragma unroll
+        for (int u = 0; u < VEC; ++u) o[u] += gamma * pv[u];
+      }
+      store16(out + r * NB + q * VEC, o);
+    }
+  }
+}
+
 // Shapes of the block action tried by the autotuner: (ES, KB).
 constexpr int kBlockShapes = 4;
 constexpr int kBlockShapeES[kBlockShapes] = {1, 1, 2, 4};
@@ -1304,7 +1368,40 @@ SpinOperator::ExplicitRows SpinOperator::explicit_rows() const {
   return r;
 }
 
-bool SpinOperator::supports_block() const { return real_ && storage_ == kStoragePacked; }
+bool SpinOperator::supports_block() const {
+  return real_ && (storage_ == kStoragePacked || storage_ == kStorageMatrixFree);
+}
+
+void SpinOperator::launch_block_matrix_free(int precision, int nb, const void* z, const void* p, void* out,
+                                            double alpha, double beta, double gamma, cudaStream_t stream) const {
+  const int grid = grid_for(dim(), 128, 16);
+  const size_t smem = n_inst_ <= kSmemInstances ? static_cast<size_t>(n_inst_) * sizeof(Instance) : 0;
+  auto launch = [&](auto stag, auto ttag, auto nbtag, auto ptag) {
+    using S = decltype(stag);
+    using T = decltype(ttag);
+    constexpr int NB = decltype(nbtag)::value;
+    constexpr bool HP = decltype(ptag)::value;
+    auto v = make_view<S>(*basis_, inst_adj_, n_inst_, factors_, inv_sqrt_);
+    spmm_matrix_free_kernel<S, T, NB, HP><<<grid, 128, smem, stream>>>(
+        v, static_cast<const T*>(z), static_cast<const T*>(p), static_cast<T*>(out), static_cast<T>(alpha),
+        static_cast<T>(beta), static_cast<T>(gamma));
+  };
+  auto by_p = [&](auto stag, auto ttag, auto nbtag) {
+    if (p) launch(stag, ttag, nbtag, std::true_type{});
+    else launch(stag, ttag, nbtag, std::false_type{});
+  };
+  auto by_nb = [&](auto stag, auto ttag) {
+    if (nb == 8) by_p(stag, ttag, std::integral_constant<int, 8>{});
+    else by_p(stag, ttag, std::integral_constant<int, 16>{});
+  };
+  auto by_t = [&](auto stag) {
+    if (precision == kFP64) by_nb(stag, double{});
+    else by_nb(stag, float{});
+  };
+  if (basis_->words() == 1) by_t(uint64_t{});
+  else by_t(u128{});
+  QMBED_LAUNCH_CHECK();
+}
 
 void SpinOperator::launch_block(int shape, int precision, int nb, const void* z, const void* p, void* out,
                                 double alpha, double beta, double gamma, cudaStream_t stream) const {
@@ -1402,9 +1499,13 @@ int SpinOperator::tuned_block_shape(int precision, int nb, bool with_p) const {
 void SpinOperator::apply_block(int precision, int nb, const void* z, const void* p, void* out, double alpha,
                                double beta, double gamma, cudaStream_t stream) const {
   QMBED_CUDA(cudaSetDevice(basis_->device()));
-  if (!supports_block()) raise(QMBED_UNSUPPORTED_BACKEND, "block action needs real packed rows");
+  if (!supports_block()) raise(QMBED_UNSUPPORTED_BACKEND, "block action needs a real operator with packed rows or matrix-free storage");
   if (nb != 8 && nb != 16) raise(QMBED_INVALID_OPTIONS, "block width must be 8 or 16");
   if (dim() == 0) return;
+  if (storage_ == kStorageMatrixFree) {
+    launch_block_matrix_free(precision, nb, z, p, out, alpha, beta, gamma, stream);
+    return;
+  }
   const int shape = block_shape(precision, nb, z, p, alpha, beta, gamma, stream);
   launch_block(shape, precision, nb, z, p, out, alpha, beta, gamma, stream);
 }

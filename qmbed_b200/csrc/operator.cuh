@@ -91,6 +91,8 @@ class SpinOperator {
   // Available for real operators with packed rows (supports_block()).
   // The kernel shape (entry split across lanes, entry batch depth) is chosen
   // per (precision, nb, p given) by timing on the first call (autotuner).
+  // Real operators with packed rows (autotuned gather kernel) or matrix-free
+  // storage (the expansion shared by the block's columns).
   bool supports_block() const;
   void apply_block(int precision, int nb, const void* z, const void* p, void* out, double alpha, double beta,
                    double gamma, cudaStream_t stream) const;
@@ -139,6 +141,8 @@ class SpinOperator {
   void build_instances(const std::vector<TermDesc>& terms, const OperatorChecks& checks);
   void assemble();
   void ensure_scratch(int precision, bool complex_vectors) const;
+  void launch_block_matrix_free(int precision, int nb, const void* z, const void* p, void* out, double alpha,
+                                double beta, double gamma, cudaStream_t stream) const;
   void launch_block(int shape, int precision, int nb, const void* z, const void* p, void* out, double alpha,
                     double beta, double gamma, cudaStream_t stream) const;
   int block_shape(int precision, int nb, const void* z, const void* p, double alpha, double beta, double gamma,

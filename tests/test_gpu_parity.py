@@ -244,16 +244,18 @@ def test_eigsh_matches_oracle(engine, oracle, sites, up, momentum, parity, krylo
         assert r.fp32_iterations > 0
 
 
-@pytest.mark.parametrize("sites,up,momentum,parity,k,delta", [
-    (20, 10, 0, 1, 4, 1.0),       # symmetry sector: weighted block coordinates, 8-wide block
-    (18, 9, None, None, 4, 0.8),  # no symmetry: unit weights
-    (20, 10, 0, None, 7, 0.7),    # 16-wide block
-    (22, 11, 11, -1, 2, 1.2),     # k = pi sector
+@pytest.mark.parametrize("sites,up,momentum,parity,k,delta,storage", [
+    (20, 10, 0, 1, 4, 1.0, "packed"),        # symmetry sector: weighted block coordinates, 8-wide block
+    (18, 9, None, None, 4, 0.8, "packed"),   # no symmetry: unit weights
+    (20, 10, 0, None, 7, 0.7, "packed"),     # 16-wide block
+    (22, 11, 11, -1, 2, 1.2, "packed"),      # k = pi sector
+    (20, 10, 0, 1, 6, 1.3, "matrix_free"),   # block action expanded on the fly
+    (18, 9, None, None, 4, 0.8, "matrix_free"),
 ])
-def test_filtered_eigsh_matches_oracle(engine, oracle, sites, up, momentum, parity, k, delta):
+def test_filtered_eigsh_matches_oracle(engine, oracle, sites, up, momentum, parity, k, delta, storage):
     terms = oracle.heisenberg_terms(sites, delta=delta)
     o = oracle.Operator.build(oracle.Basis(sites, up=up, momentum=momentum, parity=parity), terms)
-    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity), terms)
+    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity), terms, storage=storage)
     ro = o.eigsh(k, tolerance=1e-12, seed=3)
     r = g.eigsh(k, tolerance=1e-10, seed=3, mode="filtered", eigenvectors=True)
     # the block method ran (it makes no Gram-Schmidt passes) in both precisions
@@ -294,7 +296,7 @@ def test_filtered_eigsh_with_the_default_start_as_initial_vector(engine, oracle)
     assert seeded.fp32_iterations > 0  # the random start is not taken for a converged subspace
 
 
-@pytest.mark.parametrize("shape", ["0", "1", "2", "3"])
+@pytest.mark.parametrize("shape", ["0", "1", "2", "3", "matrix_free"])
 @pytest.mark.parametrize("sites,up,momentum,parity,nb,precision", [
     (16, 8, 0, 1, 8, 64), (16, 8, 0, 1, 16, 64), (16, 8, 0, 1, 8, 32), (14, 7, None, None, 16, 32),
     (18, 9, 9, 1, 8, 64),
@@ -302,11 +304,13 @@ def test_filtered_eigsh_with_the_default_start_as_initial_vector(engine, oracle)
 def test_block_action_matches_columnwise_apply(engine, oracle, monkeypatch, sites, up, momentum, parity, nb,
                                                precision, shape):
     import torch
-    monkeypatch.setenv("QMBED_BLOCK_SHAPE", shape)  # every kernel shape the autotuner may pick
+    storage = "matrix_free" if shape == "matrix_free" else "packed"
+    if storage == "packed":
+        monkeypatch.setenv("QMBED_BLOCK_SHAPE", shape)  # every kernel shape the autotuner may pick
     terms = oracle.heisenberg_terms(sites, delta=0.85)
     ob = oracle.Basis(sites, up=up, momentum=momentum, parity=parity)
     o = oracle.Operator.build(ob, terms)
-    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity), terms)
+    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity), terms, storage=storage)
     n = g.dim
     _, orbits = ob.states()
     s = np.sqrt(np.asarray(orbits, np.float64)) if momentum is not None or parity is not None else np.ones(n)
