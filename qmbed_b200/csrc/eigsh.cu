@@ -124,7 +124,16 @@ Ortho orthonormalize(Ctx& c, const Panel& Q, int ncols, int projection_from, con
   Ortho out{false, 1, 0, {}};
   std::vector<C64> h(std::max(ncols, 1));
   double before, norm;
-  if (ncols > 0) {
+  const bool fused = c.prec == 64 && Q.n == c.n;
+  if (ncols > 0 && fused) {
+    // overlaps, subtraction and both norms in two sweeps and one synchronisation
+    double before_sq = 0.0, norm_sq = 0.0;
+    c.ops.project_out(static_cast<const double*>(Q.col(0)), c.n, ncols, static_cast<const double*>(src),
+                      static_cast<double*>(w), c.cplx, h.data(), &before_sq, &norm_sq);
+    before = std::sqrt(std::max(before_sq, 0.0));
+    norm = std::sqrt(std::max(norm_sq, 0.0));
+    out.projection.assign(h.begin() + projection_from, h.begin() + ncols);
+  } else if (ncols > 0) {
     double before_sq = 0.0;
     c.ops.dots(Q.col(0), Q.n, ncols, src, c.n, c.prec, c.cplx, h.data(), &before_sq);
     before = std::sqrt(std::max(before_sq, 0.0));
@@ -137,7 +146,12 @@ Ortho orthonormalize(Ctx& c, const Panel& Q, int ncols, int projection_from, con
   }
   const bool second = before > kEps && norm <= kDgks * before;
   if (second) {
-    if (ncols > 0) {
+    if (ncols > 0 && fused) {
+      double unused_sq = 0.0, norm_sq = 0.0;
+      c.ops.project_out(static_cast<const double*>(Q.col(0)), c.n, ncols, static_cast<const double*>(w),
+                        static_cast<double*>(w), c.cplx, h.data(), &unused_sq, &norm_sq);
+      norm = std::sqrt(std::max(norm_sq, 0.0));
+    } else if (ncols > 0) {
       c.ops.dots(Q.col(0), Q.n, ncols, w, c.n, c.prec, c.cplx, h.data());
       norm = c.ops.subtract(Q.col(0), Q.n, ncols, h.data(), w, c.n, c.prec, c.cplx, true);
     }
@@ -229,52 +243,67 @@ EigshResult lanczos_window(Ctx& c, const EigshOptions& o, const void* initial_de
   size_t passes = 0, seconds = 0, size = 0;
   for (size_t it = 0; it < krylov; ++it) {
     c.apply(V.col(static_cast<int>(it)), out);
-    C64 a;
-    c.ops.dots(V.col(static_cast<int>(it)), n, 1, out, n, c.prec, c.cplx, &a);
-    const double alpha = a.real();
-    alphas.push_back(alpha);
-    double before;
-    if (it > 0) {
-      const C64 h[2] = {C64(betas[it - 1], 0.0), C64(alpha, 0.0)};
-      before = c.ops.subtract(V.col(static_cast<int>(it - 1)), n, 2, h, out, n, c.prec, c.cplx, true);
-    } else {
-      const C64 h[1] = {C64(alpha, 0.0)};
-      before = c.ops.subtract(V.col(0), n, 1, h, out, n, c.prec, c.cplx, true);
-    }
-    // dgks_reorthogonalize over the whole basis (src/solve/mod.rs:1050-1099)
     const int m = static_cast<int>(it + 1);
-    std::vector<C64> h(m);
-    c.ops.dots(V.col(0), n, m, out, n, c.prec, c.cplx, h.data());
-    double beta = c.ops.subtract(V.col(0), n, m, h.data(), out, n, c.prec, c.cplx, true);
-    passes += 1;
-    if (before > kEps && beta <= kDgks * before) {
+    double alpha, before, beta;
+    if (c.prec == 64) {
+      // FP64: alpha, the three-term residual norm and one classical pass over
+      // the whole basis come from two sweeps and one host synchronisation;
+      // dgks_reorthogonalize (src/solve/mod.rs:1050-1099) repeats the pass
+      double before_sq, after_sq;
+      C64 a;
+      c.ops.gram_schmidt_pass(static_cast<const double*>(V.col(0)), n, m, it > 0 ? betas[it - 1] : 0.0, true,
+                              static_cast<double*>(out), c.cplx, &before_sq, &after_sq, &a);
+      alpha = a.real();
+      before = std::sqrt(std::max(before_sq, 0.0));
+      beta = std::sqrt(std::max(after_sq, 0.0));
+      passes += 1;
+      if (before > kEps && beta <= kDgks * before) {
+        c.ops.gram_schmidt_pass(static_cast<const double*>(V.col(0)), n, m, 0.0, false, static_cast<double*>(out),
+                                c.cplx, &before_sq, &after_sq, nullptr);
+        beta = std::sqrt(std::max(after_sq, 0.0));
+        passes += 1;
+        seconds += 1;
+      }
+    } else {
+      C64 a;
+      c.ops.dots(V.col(static_cast<int>(it)), n, 1, out, n, c.prec, c.cplx, &a);
+      alpha = a.real();
+      if (it > 0) {
+        const C64 h[2] = {C64(betas[it - 1], 0.0), C64(alpha, 0.0)};
+        before = c.ops.subtract(V.col(static_cast<int>(it - 1)), n, 2, h, out, n, c.prec, c.cplx, true);
+      } else {
+        const C64 h[1] = {C64(alpha, 0.0)};
+        before = c.ops.subtract(V.col(0), n, 1, h, out, n, c.prec, c.cplx, true);
+      }
+      // dgks_reorthogonalize over the whole basis (src/solve/mod.rs:1050-1099)
+      std::vector<C64> h(m);
       c.ops.dots(V.col(0), n, m, out, n, c.prec, c.cplx, h.data());
       beta = c.ops.subtract(V.col(0), n, m, h.data(), out, n, c.prec, c.cplx, true);
       passes += 1;
-      seconds += 1;
+      if (before > kEps && beta <= kDgks * before) {
+        c.ops.dots(V.col(0), n, m, out, n, c.prec, c.cplx, h.data());
+        beta = c.ops.subtract(V.col(0), n, m, h.data(), out, n, c.prec, c.cplx, true);
+        passes += 1;
+        seconds += 1;
+      }
     }
+    alphas.push_back(alpha);
     size = it + 1;
     if (it + 1 == krylov || beta <= 1.0e-14) break;
     betas.push_back(beta);
     c.ops.scale_into(out, V.col(static_cast<int>(it + 1)), n, beta, c.prec, c.cplx);
   }
   if (size <= o.eigenpairs) nonconvergence(size, std::numeric_limits<double>::infinity());
-  std::vector<C64> T(size * size, C64(0.0, 0.0));
-  for (size_t i = 0; i < size; ++i) {
-    T[i * size + i] = C64(alphas[i], 0.0);
-    if (i + 1 < size) {
-      T[i * size + i + 1] = C64(betas[i], 0.0);
-      T[(i + 1) * size + i] = C64(betas[i], 0.0);
-    }
-  }
-  std::vector<double> values;
-  std::vector<C64> vectors;
-  device_hermitian_eigen(static_cast<int>(size), T, values, vectors, c.ops.stream());
+  // the tridiagonal eigenproblem (nalgebra SymmetricEigen in the reference) on the host
+  std::vector<double> values, vectors;  // vectors row-major: column j belongs to values[j]
+  tridiagonal_eigen(std::vector<double>(alphas.begin(), alphas.begin() + static_cast<long>(size)),
+                    std::vector<double>(betas.begin(), betas.begin() + static_cast<long>(size - 1)), false, values,
+                    vectors);
   const std::vector<size_t> indices = select_indices(values, o.target, o.eigenpairs);
   const int K = static_cast<int>(indices.size());
   std::vector<C64> Y(size * K);
   for (int k = 0; k < K; ++k)
-    for (size_t j = 0; j < size; ++j) Y[static_cast<size_t>(k) * size + j] = C64(vectors[indices[k] * size + j].real(), 0.0);
+    for (size_t j = 0; j < size; ++j) Y[static_cast<size_t>(k) * size + j] = C64(vectors[j * size + indices[k]], 0.0);
   Panel R;
   R.alloc(n, K, c.prec, c.cplx);
   c.ops.combine(V.col(0), n, static_cast<int>(size), Y.data(), K, R.col(0), n, n, c.prec, c.cplx);
@@ -627,12 +656,8 @@ RitzExtremes lanczos_extremes(const LinearOperatorView& op, int steps, uint64_t 
     std::swap(prev, cur);
   }
   const int size = static_cast<int>(alpha.size());
-  std::vector<double> T(static_cast<size_t>(size) * size, 0.0), vals, vecs;
-  for (int i = 0; i < size; ++i) {
-    T[static_cast<size_t>(i) * size + i] = alpha[i];
-    if (i + 1 < size) T[static_cast<size_t>(i) * size + i + 1] = T[static_cast<size_t>(i + 1) * size + i] = beta[i];
-  }
-  device_symmetric_eigen(size, T, vals, vecs, ops.stream());
+  std::vector<double> vals, vecs;
+  tridiagonal_eigen(alpha, std::vector<double>(beta.begin(), beta.begin() + (size - 1)), false, vals, vecs);
   RitzExtremes r;
   r.steps = size;
   r.min = vals.front();

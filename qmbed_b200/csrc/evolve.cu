@@ -13,7 +13,7 @@
 // the a-posteriori error bound and the accept/halve/bisect step control are
 // the reference's. Basis vectors live in one column-major FP64 device panel;
 // alpha and beta come from fused dot/update kernels with FP64 fixed-tree
-// reductions; the tridiagonal eigenproblem runs on the GPU (device Jacobi);
+// reductions; the tridiagonal eigenproblem runs on the host (implicit QL);
 // the projected combination is one pass over the panel.
 #include <algorithm>
 #include <cmath>
@@ -140,12 +140,8 @@ class KrylovExp {
       ops_.scale_into(w_.get(), col(it + 1, cplx), n_, beta, 64, cplx);
     }
     p.size = static_cast<int>(alphas.size());
-    std::vector<double> T(static_cast<size_t>(p.size) * p.size, 0.0);
-    for (int i = 0; i < p.size; ++i) {
-      T[static_cast<size_t>(i) * p.size + i] = alphas[i];
-      if (i + 1 < p.size) T[static_cast<size_t>(i) * p.size + i + 1] = T[static_cast<size_t>(i + 1) * p.size + i] = betas[i];
-    }
-    device_symmetric_eigen(p.size, T, p.eigenvalues, p.V, ops_.stream());
+    tridiagonal_eigen(alphas, std::vector<double>(betas.begin(), betas.begin() + (p.size - 1)), false, p.eigenvalues,
+                      p.V);
     return p;
   }
 

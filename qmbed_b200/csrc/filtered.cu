@@ -422,12 +422,8 @@ Bounds lanczos_bounds(const LinearOperatorView& op, BlockOps& ops, const double*
     b_prev = norm;
   }
   const int size = static_cast<int>(alpha.size());
-  std::vector<double> T(static_cast<size_t>(size) * size, 0.0), vals, vecs;
-  for (int i = 0; i < size; ++i) {
-    T[static_cast<size_t>(i) * size + i] = alpha[i];
-    if (i + 1 < size) T[static_cast<size_t>(i) * size + i + 1] = T[static_cast<size_t>(i + 1) * size + i] = beta[i];
-  }
-  device_symmetric_eigen(size, T, vals, vecs, ops.stream());
+  std::vector<double> vals, vecs;
+  tridiagonal_eigen(alpha, std::vector<double>(beta.begin(), beta.begin() + (size - 1)), false, vals, vecs);
   // residual norm of the top Ritz pair: |beta_m| times the last component of its vector
   const double top_residual = std::fabs(beta.back() * vecs[static_cast<size_t>(size - 1) * size + (size - 1)]);
   return Bounds{vals, beta.back(), top_residual, size};

@@ -37,6 +37,18 @@ class BlockOps {
   // interleaved), with no host round trip.
   void dots_device(const void* A, uint64_t ld, int m, const void* w, uint64_t n, int precision, bool cplx,
                    double* out);
+  // One classical Gram-Schmidt pass of a Lanczos step over an FP64 panel A
+  // (m columns, leading dimension n): h = A^H w, then w -= A h, and from the
+  // same sweep |w'|^2 for the three-term residual w' = w - Re(h_{m-1}) A_{m-1}
+  // - beta A_{m-2} (when `three_term`) and |w - A h|^2; last_overlap = h_{m-1}.
+  // One host synchronisation.
+  void gram_schmidt_pass(const double* A, uint64_t n, int m, double beta, bool three_term, double* w, bool cplx,
+                         double* before_sq, double* after_sq, C64* last_overlap);
+  // w = src - A h with h = A^H src (FP64 panel, m columns, leading dimension
+  // n; src may equal w), returning h (m values), |src|^2 and |w|^2 with one
+  // host synchronisation.
+  void project_out(const double* A, uint64_t n, int m, const double* src, double* w, bool cplx, C64* h,
+                   double* src_norm_sq, double* out_norm_sq);
   double norm(const void* w, uint64_t n, int precision, bool cplx);
   // w = src - sum_j h_j A_j (src = w when null); returns ||w|| when `want_norm`.
   double subtract(const void* A, uint64_t ld, int m, const C64* h, void* w, uint64_t n, int precision, bool cplx,
@@ -79,6 +91,12 @@ class BlockOps {
   double* host_results_ = nullptr;  // pinned
   size_t host_results_doubles_ = 0;
 };
+
+// Symmetric tridiagonal eigenproblem on the host by implicit QL with
+// Wilkinson shifts: ascending values; V row-major n x n (V[row * n + col],
+// column col belongs to values[col]), or only its first row when first_row.
+void tridiagonal_eigen(std::vector<double> diag, std::vector<double> off, bool first_row, std::vector<double>& values,
+                       std::vector<double>& V);
 
 // Eigen-decomposition of a small dense Hermitian matrix (row-major, n <= 2048)
 // by parallel cyclic Jacobi in one CTA. Values are returned unsorted with

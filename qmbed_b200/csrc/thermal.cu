@@ -89,213 +89,6 @@ __global__ void random_start_kernel(double* __restrict__ out, uint64_t n, uint64
 }
 
 
-constexpr int kOrthoThreads = 256;
-constexpr int kOrthoChunk = 8;
-
-__device__ __forceinline__ double block_sum(double v, double* red) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double total = 0.0;
-  if (threadIdx.x == 0)
-    for (int k = 0; k < kOrthoThreads / 32; ++k) total += red[k];
-  __syncthreads();
-  return total;
-}
-
-// One Gram-Schmidt pass of the Lanczos step over the basis panel Q (m
-// columns, leading dimension n, FP64): w -= sum_k h_k q_k with the overlaps
-// h (device, interleaved complex). Per-block partial sums, in a fixed order:
-// partials[2b] = |w'|^2 for the three-term residual
-// w' = w - Re(h_{m-1}) q_{m-1} - beta q_{m-2} (when `three_term`),
-// partials[2b+1] = |w - sum_k h_k q_k|^2. Elements are complex values
-// (kComplex), pairs of real rows loaded as one 16-byte word (kRealPair, n
-// even), or single real rows (kReal).
-enum { kReal = 0, kRealPair = 1, kComplex = 2 };
-template <int MODE>
-__global__ void __launch_bounds__(kOrthoThreads, 4) orthogonalize_kernel(const double* __restrict__ Q, uint64_t n, int m,
-                                                                      const double* __restrict__ h, double beta,
-                                                                      int three_term, double* __restrict__ w,
-                                                                      double* __restrict__ partials) {
-  extern __shared__ double hs[];
-  __shared__ double red[kOrthoThreads / 32];
-  for (int t = threadIdx.x; t < 2 * m; t += blockDim.x) hs[t] = h[t];
-  __syncthreads();
-  const double alpha = hs[2 * (m - 1)];
-  // element count and the stride between columns, in elements
-  const uint64_t elems = MODE == kRealPair ? n / 2 : n;
-  const uint64_t col = MODE == kReal ? n : n / (MODE == kRealPair ? 2 : 1);
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  // columns loaded ahead per element: eight 8-byte or four 16-byte words
-  constexpr int CH = MODE == kReal ? kOrthoChunk : kOrthoChunk / 2;
-  double before = 0.0, after = 0.0;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < elems; i += stride) {
-    // (a, b): real and imaginary parts, or the two rows of a pair
-    double wa, wb = 0.0;
-    if (MODE == kReal) {
-      wa = w[i];
-    } else {
-      const double2 v = reinterpret_cast<const double2*>(w)[i];
-      wa = v.x;
-      wb = v.y;
-    }
-    double sa = 0.0, sb = 0.0, la = 0.0, lb = 0.0, pa = 0.0, pb = 0.0;
-    for (int j0 = 0; j0 < m; j0 += CH) {
-      double xa[CH], xb[CH];
-#pragma unroll
-      for (int jj = 0; jj < CH; ++jj) {
-        xa[jj] = xb[jj] = 0.0;
-        if (j0 + jj < m) {
-          if (MODE == kReal) {
-            xa[jj] = Q[static_cast<uint64_t>(j0 + jj) * col + i];
-          } else {
-            const double2 v = reinterpret_cast<const double2*>(Q)[static_cast<uint64_t>(j0 + jj) * col + i];
-            xa[jj] = v.x;
-            xb[jj] = v.y;
-          }
-        }
-      }
-#pragma unroll
-      for (int jj = 0; jj < CH; ++jj) {
-        const int k = j0 + jj;
-        if (k < m) {
-          const double hr = hs[2 * k], hi = hs[2 * k + 1];
-          if (MODE == kComplex) {
-            sa += hr * xa[jj] - hi * xb[jj];
-            sb += hr * xb[jj] + hi * xa[jj];
-          } else {  // real basis: the overlaps are real
-            sa += hr * xa[jj];
-            sb += hr * xb[jj];
-          }
-          if (k == m - 1) {
-            la = xa[jj];
-            lb = xb[jj];
-          }
-          if (k == m - 2) {
-            pa = xa[jj];
-            pb = xb[jj];
-          }
-        }
-      }
-    }
-    if (three_term) {
-      const double ba = wa - alpha * la - beta * pa, bb = wb - alpha * lb - beta * pb;
-      before += ba * ba + bb * bb;
-    }
-    const double ra = wa - sa, rb = wb - sb;
-    if (MODE == kReal) w[i] = ra;
-    else reinterpret_cast<double2*>(w)[i] = make_double2(ra, rb);
-    after += ra * ra + rb * rb;
-  }
-  before = block_sum(before, red);
-  after = block_sum(after, red);
-  if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = before;
-    partials[2 * blockIdx.x + 1] = after;
-  }
-}
-
-// out[0..1] = sums of the two partial columns over G blocks (fixed order);
-// out[2..3] = alpha (the last overlap) for the host's Hermiticity check.
-__global__ void __launch_bounds__(128) orthogonalize_finish_kernel(const double* __restrict__ partials, int G,
-                                                                   const double* __restrict__ alpha,
-                                                                   double* __restrict__ out) {
-  __shared__ double tree[2][128];
-  double b = 0.0, a = 0.0;
-  for (int k = threadIdx.x; k < G; k += 128) {
-    b += partials[2 * k];
-    a += partials[2 * k + 1];
-  }
-  tree[0][threadIdx.x] = b;
-  tree[1][threadIdx.x] = a;
-  __syncthreads();
-  for (int width = 64; width > 0; width >>= 1) {
-    if (threadIdx.x < width) {
-      tree[0][threadIdx.x] += tree[0][threadIdx.x + width];
-      tree[1][threadIdx.x] += tree[1][threadIdx.x + width];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    out[0] = tree[0][0];
-    out[1] = tree[1][0];
-    out[2] = alpha[0];
-    out[3] = alpha[1];
-  }
-}
-
-// Symmetric tridiagonal eigenproblem (diagonal d, off-diagonal e) by the
-// implicit QL method with Wilkinson shifts (Bowdler, Martin, Reinsch and
-// Wilkinson, Numer. Math. 11 (1968) 293-306). Rotations are accumulated into
-// Z (row-major n x n, Z[k * n + c]) or, with `first_row`, into its first
-// row only (all that the Boltzmann weights need). Returns ascending values
-// with the columns permuted alike.
-void tridiagonal_eigensystem(std::vector<double> d, std::vector<double> e, bool first_row,
-                             std::vector<double>& values, std::vector<double>& V) {
-  const int n = static_cast<int>(d.size());
-  const int rows = first_row ? 1 : n;
-  std::vector<double> Z(static_cast<size_t>(rows) * n, 0.0);
-  for (int k = 0; k < rows; ++k) Z[static_cast<size_t>(k) * n + k] = 1.0;
-  e.resize(static_cast<size_t>(n), 0.0);
-  for (int l = 0; l < n; ++l) {
-    for (int sweep = 0;; ++sweep) {
-      int m = l;
-      for (; m + 1 < n; ++m)
-        if (std::fabs(e[m]) <= kEps * (std::fabs(d[m]) + std::fabs(d[m + 1]))) break;
-      if (m == l) break;
-      if (sweep == 60) raise(QMBED_INTERNAL_STATE, "tridiagonal eigensolver did not converge");
-      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-      double r = std::hypot(g, 1.0);
-      g = d[m] - d[l] + e[l] / (g + std::copysign(r, g));
-      double s = 1.0, c = 1.0, p = 0.0;
-      bool deflated = false;
-      for (int i = m - 1; i >= l; --i) {
-        const double f = s * e[i], b = c * e[i];
-        r = std::hypot(f, g);
-        e[i + 1] = r;
-        if (r == 0.0) {  // underflow: split the matrix here and restart
-          d[i + 1] -= p;
-          e[m] = 0.0;
-          deflated = true;
-          break;
-        }
-        s = f / r;
-        c = g / r;
-        g = d[i + 1] - p;
-        r = (d[i] - g) * s + 2.0 * c * b;
-        p = s * r;
-        d[i + 1] = g + p;
-        g = c * r - b;
-        for (int k = 0; k < rows; ++k) {
-          double* z = Z.data() + static_cast<size_t>(k) * n;
-          const double t = z[i + 1];
-          z[i + 1] = s * z[i] + c * t;
-          z[i] = c * z[i] - s * t;
-        }
-      }
-      if (deflated) continue;
-      d[l] -= p;
-      e[l] = g;
-      e[m] = 0.0;
-    }
-  }
-  std::vector<int> order(static_cast<size_t>(n));
-  for (int i = 0; i < n; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return d[a] < d[b]; });
-  values.resize(static_cast<size_t>(n));
-  V.assign(static_cast<size_t>(rows) * n, 0.0);
-  for (int c = 0; c < n; ++c) {
-    values[c] = d[order[c]];
-    for (int k = 0; k < rows; ++k) V[static_cast<size_t>(k) * n + c] = Z[static_cast<size_t>(k) * n + order[c]];
-  }
-}
-
-struct PinnedResults {
-  double* p = nullptr;
-  PinnedResults() { QMBED_CUDA(cudaMallocHost(&p, 8 * sizeof(double))); }
-  ~PinnedResults() { cudaFreeHost(p); }
-};
 
 }  // namespace
 
@@ -320,35 +113,12 @@ void lanczos_ritz_device(const LinearOperatorView& op, const double* initial, bo
   const int capacity = static_cast<int>(wanted);
   const size_t panel_bytes = static_cast<size_t>(capacity) * n * width;
   if (d.basis.bytes() < panel_bytes) d.basis.allocate(panel_bytes);  // kept across repeated runs
-  const int G = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((n + kOrthoThreads - 1) / kOrthoThreads,
-                                                                          4ull * ops.sms())));
-  DeviceBuffer w(n * width), h(static_cast<size_t>(capacity) * 16), partials(static_cast<size_t>(G) * 16),
-      results(8 * sizeof(double));
-  PinnedResults host;
+  DeviceBuffer w(n * width);
   auto col = [&](int j) { return static_cast<char*>(d.basis.get()) + static_cast<size_t>(j) * n * width; };
-  const cudaStream_t stream = ops.stream();
-  const size_t smem = static_cast<size_t>(capacity) * 16;
-  // pairs of real rows move as 16-byte words when every column starts 16-byte aligned
-  const int mode = cplx ? kComplex : (n % 2 == 0 ? kRealPair : kReal);
-  auto kernel = mode == kComplex ? orthogonalize_kernel<kComplex>
-                                 : (mode == kRealPair ? orthogonalize_kernel<kRealPair> : orthogonalize_kernel<kReal>);
-  if (smem > 48 * 1024)
-    QMBED_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   // one Gram-Schmidt pass over q_0 .. q_{m-1}; returns (|w'|^2, |w''|^2, alpha)
   auto pass = [&](int m, double beta, bool three_term, double* before_sq, double* after_sq, C64* alpha) {
-    ops.dots_device(d.basis.get(), n, m, w.get(), n, 64, cplx, h.as<double>());
-    kernel<<<G, kOrthoThreads, static_cast<size_t>(m) * 16, stream>>>(d.basis.as<double>(), n, m, h.as<double>(), beta,
-                                                                      three_term ? 1 : 0, w.as<double>(),
-                                                                      partials.as<double>());
-    QMBED_LAUNCH_CHECK();
-    orthogonalize_finish_kernel<<<1, 128, 0, stream>>>(partials.as<double>(), G, h.as<double>() + 2 * (m - 1),
-                                                       results.as<double>());
-    QMBED_LAUNCH_CHECK();
-    QMBED_CUDA(cudaMemcpyAsync(host.p, results.get(), 4 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    QMBED_CUDA(cudaStreamSynchronize(stream));
-    *before_sq = host.p[0];
-    *after_sq = host.p[1];
-    *alpha = C64(host.p[2], host.p[3]);
+    ops.gram_schmidt_pass(d.basis.as<double>(), n, m, beta, three_term, w.as<double>(), cplx, before_sq, after_sq,
+                          alpha);
   };
 
   // normalize (src/solve/mod.rs:694-705) on the caller's vector
@@ -399,7 +169,7 @@ void lanczos_ritz_device(const LinearOperatorView& op, const double* initial, bo
   d.size = static_cast<int>(d.diagonal.size());
   d.off_diagonal.assign(betas.begin(), betas.end() - 1);
   d.full_vectors = full_vectors;
-  tridiagonal_eigensystem(d.diagonal, d.off_diagonal, !full_vectors, d.eigenvalues, d.V);
+  tridiagonal_eigen(d.diagonal, d.off_diagonal, !full_vectors, d.eigenvalues, d.V);
 }
 
 void lanczos_ritz(const LinearOperatorView& op, const double* initial, size_t krylov, double tolerance,
