@@ -395,9 +395,10 @@ struct Bounds {
 Bounds lanczos_bounds(const LinearOperatorView& op, BlockOps& ops, const double* start, size_t& applications) {
   const uint64_t n = op.dim;
   const int m = static_cast<int>(std::min<uint64_t>(kBoundSteps, n - 1));
-  DeviceBuffer a(n * 4), b(n * 4), w(n * 4);
-  void* prev = a.get();
-  void* cur = b.get();
+  // workspace slots 7-9 of the handle: the three FP32 Lanczos vectors
+  void* prev = ops.workspace(7, n * 4);
+  void* cur = ops.workspace(8, n * 4);
+  void* w_vec = ops.workspace(9, n * 4);
   ops.convert(start, 64, cur, 32, n);
   const double n0 = ops.norm(cur, n, 32, false);
   if (!(n0 > 0.0)) raise(QMBED_INVALID_OPTIONS, "eigsh start vector has zero norm");
@@ -405,20 +406,20 @@ Bounds lanczos_bounds(const LinearOperatorView& op, BlockOps& ops, const double*
   std::vector<double> alpha, beta;
   double b_prev = 0.0;
   for (int j = 0; j < m; ++j) {
-    op.apply(32, false, cur, w.get());
+    op.apply(32, false, cur, w_vec);
     ++applications;
     C64 h;
-    ops.dots(cur, n, 1, w.get(), n, 32, false, &h);
-    double norm = ops.subtract(cur, n, 1, &h, w.get(), n, 32, false, j == 0);
+    ops.dots(cur, n, 1, w_vec, n, 32, false, &h);
+    double norm = ops.subtract(cur, n, 1, &h, w_vec, n, 32, false, j == 0);
     if (j > 0) {
       const C64 hb(b_prev, 0.0);
-      norm = ops.subtract(prev, n, 1, &hb, w.get(), n, 32, false, true);
+      norm = ops.subtract(prev, n, 1, &hb, w_vec, n, 32, false, true);
     }
     alpha.push_back(h.real());
     beta.push_back(norm);
     if (!(norm > 1.0e-10 * std::max(1.0, std::fabs(h.real())))) break;
     std::swap(prev, cur);
-    ops.scale_into(w.get(), cur, n, norm, 32, false);
+    ops.scale_into(w_vec, cur, n, norm, 32, false);
     b_prev = norm;
   }
   const int size = static_cast<int>(alpha.size());
@@ -447,7 +448,8 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
   // deterministic starts with seeds o.seed + j * 0x9e3779b9 for the remaining
   // column positions j (a caller's vector equal to the default start of
   // column 0 is then not repeated).
-  // Workspace slots of the handle: 0 start columns, 1-3 FP32 blocks, 4-6 FP64 blocks.
+  // Workspace slots of the handle: 0 start columns, 1-3 FP32 blocks, 4-6 FP64
+  // blocks, 7-9 the bound estimate's Lanczos vectors.
   const size_t block32 = static_cast<size_t>(n) * nb * 4, block64 = static_cast<size_t>(n) * nb * 8;
   double* cols = static_cast<double*>(ops.workspace(0, block64));
   auto col = [&](int j) { return cols + static_cast<size_t>(j) * n; };

@@ -313,18 +313,25 @@ __device__ inline uint64_t lcg_jump(uint64_t x, uint64_t k) {
   return A * x + C;
 }
 
+// Element i takes the (i+1)-th LCG state. A block covers blockDim * per_thread
+// consecutive elements; thread t takes base + t, base + t + blockDim, ...,
+// advancing its state by the blockDim-step map (A, C) between them, so every
+// warp store is contiguous.
 template <typename T, bool CPLX>
 __global__ void lcg_start_kernel(T* __restrict__ out, uint64_t n, uint64_t seed, uint64_t per_thread) {
-  const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const uint64_t i0 = t * per_thread;
+  const uint64_t stride = blockDim.x;
+  const uint64_t base = static_cast<uint64_t>(blockIdx.x) * stride * per_thread;
+  const uint64_t i0 = base + threadIdx.x;
   if (i0 >= n) return;
-  const uint64_t i1 = min(i0 + per_thread, n);
-  uint64_t state = lcg_jump(seed | 1ULL, i0);
-  for (uint64_t i = i0; i < i1; ++i) {
-    state = state * 6364136223846793005ULL + 1442695040888963407ULL;
+  const uint64_t C = lcg_jump(0, stride);
+  const uint64_t A = lcg_jump(1, stride) - C;  // the jump is affine: jump(x) = A x + C
+  uint64_t state = lcg_jump(seed | 1ULL, i0 + 1);
+  const uint64_t end = min(base + stride * per_thread, n);
+  for (uint64_t i = i0; i < end; i += stride) {
     const uint64_t mantissa = state >> 11;
     const double value = static_cast<double>(mantissa) / 9007199254740992.0 - 0.5;
     store<T, CPLX>(out, i, value, 0.0);
+    state = A * state + C;
   }
 }
 
