@@ -78,7 +78,7 @@ def build(verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
         objects = list(pool.map(compile_one, sources()))
     if _stale(LIBRARY, objects):
-        cmd = [compiler, *ARCH, "-shared", "-cudart", "static", "-o", str(LIBRARY), *map(str, objects)]
+        cmd = [compiler, *ARCH, "-shared", "-cudart", "static", "-o", str(LIBRARY), *map(str, objects), "-lcusolver"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -17,6 +17,7 @@
 #include "../../include/qmbed_b200.h"
 #include "batched.cuh"
 #include "chebyshev.cuh"
+#include "dense.cuh"
 #include "eigsh.cuh"
 #include "evolve.cuh"
 #include "expm.cuh"
@@ -669,6 +670,60 @@ ExpmPlan expm_plan_from(const Value& request, qmbed_operator_s& op) {
   return make_expm_plan(*op.op, coefficient, max_degree, tolerance, substeps);
 }
 
+// command_eigh (bindings/capi/src/lib.rs:5290-5300) in the command_eigensystem layout.
+Value dense_eigh_value(qmbed_operator_s& h, bool want_vectors) {
+  std::lock_guard<std::mutex> lock(h.mu);
+  const DenseEigensystem r = dense_eigh(h.view(), want_vectors, h.block_ops());
+  const uint64_t n = h.op->dim();
+  Value out = Value::object();
+  out.set("kind", Value::string("eigensystem"));
+  out.set("dimension", Value::integer(static_cast<long long>(n)));
+  Value vals = Value::array(), res = Value::array();
+  for (double v : r.eigenvalues) vals.push(Value::number(v));
+  for (double v : r.residuals) res.push(Value::number(v));
+  out.set("eigenvalues", std::move(vals));
+  out.set("residuals", std::move(res));
+  out.set("iterations", Value::integer(n != 0 ? 1 : 0));
+  out.set("converged", Value::boolean(true));
+  if (want_vectors) {
+    std::vector<double> host(2 * r.vectors.size());
+    for (size_t i = 0; i < r.vectors.size(); ++i) {
+      host[2 * i] = r.vectors[i].real();
+      host[2 * i + 1] = r.vectors[i].imag();
+    }
+    out.set("eigenvectors", vectors_value(host, n, r.eigenvalues.size()));
+  }
+  return out;
+}
+
+// The assembled rows as the reference's operator payload: shape, format and
+// (row, column, value) entries in row order.
+Value operator_entries(qmbed_operator_s& h, const std::string& format) {
+  std::lock_guard<std::mutex> lock(h.mu);
+  std::vector<uint64_t> row_ptr;
+  std::vector<uint32_t> cols;
+  std::vector<C64> values;
+  h.op->export_csr(row_ptr, cols, values);
+  Value out = Value::object();
+  out.set("kind", Value::string("operator"));
+  Value shape = Value::array();
+  shape.push(Value::integer(static_cast<long long>(h.op->dim())));
+  shape.push(Value::integer(static_cast<long long>(h.op->dim())));
+  out.set("shape", std::move(shape));
+  out.set("format", Value::string(format));
+  Value entries = Value::array();
+  for (uint64_t r = 0; r + 1 < row_ptr.size(); ++r)
+    for (uint64_t p = row_ptr[r]; p < row_ptr[r + 1]; ++p) {
+      Value e = Value::object();
+      e.set("row", Value::integer(static_cast<long long>(r)));
+      e.set("column", Value::integer(static_cast<long long>(cols[p])));
+      e.set("value", complex_pair(values[p]));
+      entries.push(std::move(e));
+    }
+  out.set("entries", std::move(entries));
+  return out;
+}
+
 Value command(const Value& request) {
   const std::string operation = request.at("operation").as_string();
   if (operation == "describe_basis") return describe_basis(request);
@@ -680,28 +735,13 @@ Value command(const Value& request) {
   if (operation == "materialize") {
     auto model = build_model(request);
     auto op = model->materialize(nullptr, kStoragePacked, model->checks.hermiticity);
-    std::vector<uint64_t> row_ptr;
-    std::vector<uint32_t> cols;
-    std::vector<C64> values;
-    op->op->export_csr(row_ptr, cols, values);
-    Value out = Value::object();
-    out.set("kind", Value::string("operator"));
-    Value shape = Value::array();
-    shape.push(Value::integer(static_cast<long long>(op->op->dim())));
-    shape.push(Value::integer(static_cast<long long>(op->op->dim())));
-    out.set("shape", std::move(shape));
-    out.set("format", Value::string(request.has("format") ? request.at("format").as_string() : "csc"));
-    Value entries = Value::array();
-    for (uint64_t r = 0; r + 1 < row_ptr.size(); ++r)
-      for (uint64_t p = row_ptr[r]; p < row_ptr[r + 1]; ++p) {
-        Value e = Value::object();
-        e.set("row", Value::integer(static_cast<long long>(r)));
-        e.set("column", Value::integer(static_cast<long long>(cols[p])));
-        e.set("value", complex_pair(values[p]));
-        entries.push(std::move(e));
-      }
-    out.set("entries", std::move(entries));
-    return out;
+    return operator_entries(*op, request.has("format") ? request.at("format").as_string() : "csc");
+  }
+  if (operation == "materialize_model") {
+    // MaterializeModel -> command_operator (bindings/capi/src/lib.rs:5652-5659)
+    auto model = registered_model(request.at("handle").as_string());
+    auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
+    return operator_entries(*op, request.has("format") ? request.at("format").as_string() : "csc");
   }
   if (operation == "create_model") {
     auto model = build_model(request);
@@ -757,6 +797,16 @@ Value command(const Value& request) {
   if (operation == "apply_expm_action") {
     auto entry = registered_expm(request.at("expm_handle").as_string());
     return expm_vectors(*entry->op, entry->plan, parse_vectors(request.at("vectors")));
+  }
+  if (operation == "eigh_model") {
+    // command_eigh (bindings/capi/src/lib.rs:5290-5300)
+    auto model = registered_model(request.at("handle").as_string());
+    auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
+    return dense_eigh_value(*op, request.has("eigenvectors") && request.at("eigenvectors").as_bool());
+  }
+  if (operation == "eigh_operator_expression") {
+    auto op = expression_operator(request.at("expression"));
+    return dense_eigh_value(*op, request.has("eigenvectors") && request.at("eigenvectors").as_bool());
   }
   if (operation == "eigsh_operator_expression") {
     // command_eigsh_operator_expression (bindings/capi/src/lib.rs:4172-4190)

@@ -157,3 +157,75 @@ def test_apply_terms_between_models(oracle, sites):
             command({"operation": "release_model", "handle": m})
     for m in (src, tgt):
         command({"operation": "release_model", "handle": m})
+
+
+@pytest.mark.parametrize("momentum,parity", [(0, 1), (3, None)])
+def test_eigh_model_matches_dense_spectrum(oracle, momentum, parity):
+    """eigh_model / eigh_operator_expression (bindings/capi/src/lib.rs:5290-5300,
+    src/solve/mod.rs:585-605): every eigenpair, ascending, with residuals."""
+    from qmbed_b200._lib import command
+    sites = 10
+    basis = {"kind": "spin", "sites": sites, "up": 5, "momentum": momentum}
+    if parity is not None:
+        basis["parity"] = parity
+    handle = command({"operation": "create_model", "basis": basis,
+                      "terms": heisenberg_request_terms(sites, delta=0.6)})["handle"]
+    o = oracle.Operator.build(oracle.Basis(sites, up=5, momentum=momentum, parity=parity),
+                              oracle.heisenberg_terms(sites, delta=0.6))
+    w = np.linalg.eigvalsh(o.dense())
+    out = command({"operation": "eigh_model", "handle": handle, "eigenvectors": True})
+    assert out["kind"] == "eigensystem" and out["dimension"] == o.dim and out["converged"] is True
+    assert out["iterations"] == 1
+    np.testing.assert_allclose(out["eigenvalues"], w, atol=1e-12)
+    assert max(out["residuals"]) < 1e-11
+    vecs = np.array([[complex(*p) for p in v] for v in out["eigenvectors"]])
+    np.testing.assert_allclose(vecs.conj() @ vecs.T, np.eye(o.dim), atol=1e-11)
+    for lam, v in zip(out["eigenvalues"], vecs[:3]):
+        assert np.linalg.norm(o.apply(v) - lam * v) < 1e-11
+    expr = command({"operation": "eigh_operator_expression",
+                    "expression": {"kind": "model", "handle": handle, "action": "normal"}})
+    np.testing.assert_allclose(expr["eigenvalues"], w, atol=1e-12)
+    assert "eigenvectors" not in expr
+    command({"operation": "release_model", "handle": handle})
+
+
+def test_eigh_model_dimer_and_size_limit():
+    from qmbed_b200 import QmbedError
+    from qmbed_b200._lib import command
+    dimer = command({"operation": "create_model", "basis": {"kind": "spin", "sites": 2},
+                     "terms": heisenberg_request_terms(2, periodic=False)})["handle"]
+    out = command({"operation": "eigh_model", "handle": dimer})
+    np.testing.assert_allclose(out["eigenvalues"], [-0.75, 0.25, 0.25, 0.25], atol=1e-13)
+    # a sector of 3432 states through the dense solver, against the oracle's Lanczos
+    mid = command({"operation": "create_model", "basis": {"kind": "spin", "sites": 14, "up": 7},
+                   "terms": heisenberg_request_terms(14)})["handle"]
+    full = command({"operation": "eigh_model", "handle": mid})
+    assert full["dimension"] == 3432 and max(full["residuals"]) < 1e-10
+    lowest = command({"operation": "eigsh_model", "handle": mid,
+                      "solver": {"eigenpairs": 3, "target": {"kind": "smallest_algebraic"}, "tolerance": 1e-12}})
+    np.testing.assert_allclose(full["eigenvalues"][:3], lowest["eigenvalues"], atol=1e-10)
+    command({"operation": "release_model", "handle": mid})
+    big = command({"operation": "create_model", "basis": {"kind": "spin", "sites": 20, "up": 10},
+                   "terms": heisenberg_request_terms(20)})["handle"]
+    with pytest.raises(QmbedError, match="^unsupported backend: dense eigh"):
+        command({"operation": "eigh_model", "handle": big})
+    for h in (dimer, big):
+        command({"operation": "release_model", "handle": h})
+
+
+def test_materialize_model_matches_oracle(oracle):
+    """materialize_model (bindings/capi/src/lib.rs:5652-5659) with a component parameter."""
+    from qmbed_b200._lib import command
+    request = {"basis": {"kind": "spin", "sites": 8, "up": 4, "momentum": 0},
+               "terms": heisenberg_request_terms(8)[1:],
+               "components": [{"name": "delta", "terms": heisenberg_request_terms(8)[:1], "default": [1.0, 0.0]}]}
+    handle = command({"operation": "create_model", **request})["handle"]
+    out = command({"operation": "materialize_model", "handle": handle, "parameters": {"delta": [0.3, 0.0]}})
+    o = oracle.Operator.build(oracle.Basis(8, up=4, momentum=0), oracle.heisenberg_terms(8, delta=0.3))
+    n = o.dim
+    assert out["kind"] == "operator" and out["shape"] == [n, n]
+    dense = np.zeros((n, n), complex)
+    for e in out["entries"]:
+        dense[e["row"], e["column"]] += complex(*e["value"])
+    np.testing.assert_allclose(dense, o.dense(), atol=1e-13)
+    command({"operation": "release_model", "handle": handle})
