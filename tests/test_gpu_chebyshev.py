@@ -32,6 +32,7 @@ def _tfim(engine, sites, g=1.0, seed=0, periodic=False):
     (10, "pauli", False), (11, "pauli", True), (12, "angular_momentum", False),
     (16, "pauli", False),   # complex128 tiles of 12 bits: the top bits flip through global partner reads
     (18, "pauli", True),
+    (20, "angular_momentum", True),  # 7-8 high bits through global partner reads
 ])
 def test_flip_chain_action_matches_oracle(engine, oracle, sites, normalization, periodic):
     terms = _tfim(engine, sites, g=0.8, seed=sites, periodic=periodic)
