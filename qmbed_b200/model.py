@@ -167,6 +167,11 @@ class NativeModel:
         params = {k: [complex(v).real, complex(v).imag] for k, v in (parameters or {}).items()}
         return _eigensystem(self.execute("eigsh_model", solver=options.request(), parameters=params, format=format))
 
+    def eigh(self, eigenvectors: bool = False, parameters: dict[str, complex] | None = None) -> Eigensystem:
+        """Every eigenpair (the eigh_model command, bindings/capi/src/lib.rs:5290-5300)."""
+        params = {k: [complex(v).real, complex(v).imag] for k, v in (parameters or {}).items()}
+        return _eigensystem(self.execute("eigh_model", eigenvectors=eigenvectors, parameters=params))
+
     def apply(self, vectors, parameters: dict[str, complex] | None = None) -> np.ndarray:
         params = {k: [complex(v).real, complex(v).imag] for k, v in (parameters or {}).items()}
         return _vectors_result(self.execute("apply_model", vectors=_vectors_request(vectors), parameters=params))

@@ -229,3 +229,15 @@ def test_materialize_model_matches_oracle(oracle):
         dense[e["row"], e["column"]] += complex(*e["value"])
     np.testing.assert_allclose(dense, o.dense(), atol=1e-13)
     command({"operation": "release_model", "handle": handle})
+
+
+def test_native_model_eigh(oracle):
+    import qmbed_b200 as q
+    request = {"basis": {"kind": "spin", "sites": 10, "up": 5, "momentum": 0},
+               "terms": heisenberg_request_terms(10)[1:],
+               "components": [{"name": "delta", "terms": heisenberg_request_terms(10)[:1], "default": [1.0, 0.0]}]}
+    with q.NativeModel(request) as model:
+        r = model.eigh(eigenvectors=True, parameters={"delta": 0.4})
+    o = oracle.Operator.build(oracle.Basis(10, up=5, momentum=0), oracle.heisenberg_terms(10, delta=0.4))
+    np.testing.assert_allclose(r.eigenvalues, np.linalg.eigvalsh(o.dense()), atol=1e-12)
+    assert len(r.eigenvectors) == o.dim and max(r.residuals) < 1e-11
