@@ -382,7 +382,9 @@ Value solve(qmbed_operator_s& handle, const SolverRequest& request, bool tagged)
       initial.push_back(x.imag());
     }
   }
-  EigshResult r = eigsh(view, request.options, initial.data(), static_cast<int>(request.initial.size()), request.mode,
+  EigshOptions options = request.options;
+  options.want_vectors = request.eigenvectors;
+  EigshResult r = eigsh(view, options, initial.data(), static_cast<int>(request.initial.size()), request.mode,
                         handle.block_ops());
   Value out = Value::object();
   if (tagged) out.set("kind", Value::string("eigensystem"));
@@ -1313,6 +1315,7 @@ int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, const
     o.tolerance = options->tolerance;
     o.max_iterations = options->max_iterations;
     o.seed = options->seed;
+    o.want_vectors = eigenvectors != nullptr;
     const uint64_t n = op->op->dim();
     if (n_initial < 0 || (n_initial > 0 && !initial)) raise(QMBED_INVALID_OPTIONS, "invalid initial vectors");
     LinearOperatorView view = op->view();

@@ -22,6 +22,7 @@ struct EigshOptions {
   double tolerance = 1.0e-10;
   size_t max_iterations = 1000;
   uint64_t seed = 0;
+  bool want_vectors = true;  // false: the caller takes eigenvalues only (the filtered solver exports no vectors)
 };
 
 enum SolverMode : int {

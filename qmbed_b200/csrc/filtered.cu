@@ -585,8 +585,10 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
   r.fp64_iterations = static_cast<size_t>(iterations[1]);
   r.converged = true;
   r.complex_vectors = false;
-  r.vectors.allocate(static_cast<size_t>(n) * k * sizeof(double));
-  solver.export_columns(64, A64, k, r.vectors.as<double>());
+  if (o.want_vectors) {
+    r.vectors.allocate(static_cast<size_t>(n) * k * sizeof(double));
+    solver.export_columns(64, A64, k, r.vectors.as<double>());
+  }
   ops.sync();
   stamp("export");
   r.operator_applications = solver.applications + bound_applications;
