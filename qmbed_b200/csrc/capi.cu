@@ -11,6 +11,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -214,11 +215,103 @@ int default_device() {
   return env ? std::atoi(env) : 0;
 }
 
-SpinBasisDesc parse_basis(const Value& b) {
+// General lattice maps of the reference's SymmetryRequest
+// (bindings/capi/src/lib.rs:3103-3127; LatticeSymmetryMap,
+// src/basis/mod.rs:2967-3130) as the built-in chain group. A map moves the
+// digit at site i to destinations[i]; one generator step multiplies the orbit
+// coefficient by exp(-2 pi i sector / period) (trace_symmetry_orbit,
+// src/basis/mod.rs:3455-3538). A translation i -> i + t with gcd(t, L) = 1
+// generates every translation, and exp(-2 pi i sector / L) on T^t is the
+// built-in momentum k with k t = sector (mod L) (the built-in T moves site i to
+// i + 1 with character exp(-2 pi i k / L), src/basis/mod.rs:661-676, 786-790).
+// The reflection i -> L-1-i with sector s is the built-in parity (-1)^s. The
+// reduced vectors, gauge (the representative's coefficient) and orbit sizes
+// of both constructions agree (GeneralBasis::from_reducer_impl,
+// src/basis/mod.rs:4180-4306; spin_symmetry_sector, 715-848). Other maps
+// (sublattice translations, spin inversion, arbitrary permutations) are
+// reported as unsupported.
+void apply_lattice_maps(const Value& list, SpinBasisDesc& d) {
+  const int L = d.sites;
+  bool translation = false, reflection = false;
+  for (const Value& s : list.items()) {
+    const auto& items = s.at("destinations").items();
+    if (static_cast<int>(items.size()) != L)
+      raise(QMBED_INVALID_OPTIONS, "symmetry map has " + std::to_string(items.size()) + " sites, expected " +
+                                       std::to_string(L));
+    std::vector<int> dest(L);
+    std::vector<char> seen(L, 0);
+    for (int i = 0; i < L; ++i) {
+      const long long v = items[i].as_int();
+      if (v < 0 || v >= L || seen[v]) raise(QMBED_INCOMPATIBLE_SYMMETRY, "symmetry site destinations must be a bijection");
+      seen[v] = 1;
+      dest[i] = static_cast<int>(v);
+    }
+    if (const Value* local = s.find("local_permutations"); local && !local->is_null()) {
+      const auto& rows = local->items();
+      if (static_cast<int>(rows.size()) != L)
+        raise(QMBED_INCOMPATIBLE_SYMMETRY, "every local-state map must be a permutation");
+      for (const Value& row : rows) {
+        const auto& r = row.items();
+        const bool identity = r.size() == 2 && r[0].as_int() == 0 && r[1].as_int() == 1;
+        const bool swap = r.size() == 2 && r[0].as_int() == 1 && r[1].as_int() == 0;
+        if (!identity && !swap) raise(QMBED_INCOMPATIBLE_SYMMETRY, "every local-state map must be a permutation");
+        if (swap) raise(QMBED_UNSUPPORTED_BACKEND, "local spin-inversion maps are not supported by the GPU engine");
+      }
+    }
+    const long long sector = s.at("sector").as_int();
+    const int t = dest[0];
+    bool is_translation = true, is_reflection = true;
+    for (int i = 0; i < L; ++i) {
+      is_translation = is_translation && dest[i] == (i + t) % L;
+      is_reflection = is_reflection && dest[i] == L - 1 - i;
+    }
+    if (is_translation && t == 0) continue;  // the identity: period 1, every sector trivial
+    if (is_translation) {
+      if (std::gcd(t, L) != 1)
+        raise(QMBED_UNSUPPORTED_BACKEND, "a translation by " + std::to_string(t) + " of " + std::to_string(L) +
+                                             " sites generates a proper subgroup; the GPU engine implements the "
+                                             "full translation group");
+      if (translation) raise(QMBED_UNSUPPORTED_BACKEND, "more than one translation generator is not supported by the GPU engine");
+      translation = true;
+      long long inverse = 1;  // t^-1 mod L by trial: L is at most 128
+      while ((inverse * t) % L != 1 % L) ++inverse;
+      const long long canonical = ((sector % L) + L) % L;
+      d.has_momentum = 1;
+      d.momentum = static_cast<int>((canonical * inverse) % L);
+    } else if (is_reflection) {
+      if (reflection) raise(QMBED_UNSUPPORTED_BACKEND, "more than one reflection generator is not supported by the GPU engine");
+      reflection = true;
+      d.parity = ((sector % 2) + 2) % 2 == 0 ? 1 : -1;
+    } else {
+      raise(QMBED_UNSUPPORTED_BACKEND,
+            "lattice maps other than chain translations and the reflection site -> L-1-site are not supported "
+            "by the GPU engine");
+    }
+  }
+}
+
+// A spin basis request as the engine builds it. The reference's `reverse`
+// flag (bindings/capi/src/lib.rs:2849-2905, 3412-3423) reverses the public
+// row order and, for lattice-map sectors, takes the maximum orbit state as
+// the representative. Bitwise complement (the global spin flip C) reverses
+// the order of integers and commutes with every site permutation, so that
+// basis is, row for row and phase for phase, the complement of the ordinary
+// (minimum-representative, ascending) sector with up' = L - up. The engine
+// builds that sector (`flipped`) and acts with C H C: its local products
+// follow flip_terms below, and every vector, matrix entry and eigenvector
+// keeps the reference's row order without a permutation.
+struct BasisRequest {
+  SpinBasisDesc desc;
+  bool flipped = false;
+};
+
+BasisRequest parse_basis(const Value& b) {
   const std::string kind = b.at("kind").as_string();
   if (kind != "spin")
     raise(QMBED_UNSUPPORTED_BACKEND, "the GPU engine implements spin-1/2 chain bases; `" + kind + "` is not supported");
-  SpinBasisDesc d{};
+  BasisRequest r;
+  SpinBasisDesc& d = r.desc;
+  d = SpinBasisDesc{};
   d.sites = static_cast<int>(b.at("sites").as_int());
   if (b.has("spin_twice") && b.at("spin_twice").as_int() != 1)
     raise(QMBED_UNSUPPORTED_BACKEND, "the GPU engine implements spin one half (spin_twice = 1)");
@@ -233,6 +326,7 @@ SpinBasisDesc parse_basis(const Value& b) {
   d.has_momentum = b.has("momentum") ? 1 : 0;
   d.momentum = d.has_momentum ? static_cast<int>(b.at("momentum").as_int()) : 0;
   d.parity = b.has("parity") ? static_cast<int>(b.at("parity").as_int()) : 0;
+  const bool built_in = d.has_momentum || d.parity;
   d.normalization = (b.has("pauli") && b.at("pauli").as_bool()) ? kPauliCartesian : kAngularMomentum;
   if (b.has("normalization")) {
     const std::string n = b.at("normalization").as_string();
@@ -242,14 +336,21 @@ SpinBasisDesc parse_basis(const Value& b) {
     else raise(QMBED_INVALID_OPTIONS, "unknown spin normalization `" + n + "`");
   }
   if (b.has("symmetries") && !b.at("symmetries").items().empty()) {
-    if (d.has_momentum || d.parity) raise(QMBED_INVALID_OPTIONS, "built-in and general spin symmetries cannot be mixed");
-    raise(QMBED_UNSUPPORTED_BACKEND, "general symmetry maps are not supported by the GPU engine");
+    if (built_in) raise(QMBED_INVALID_OPTIONS, "built-in and general spin symmetries cannot be mixed");
+    if (d.sites <= 0) raise(QMBED_INVALID_SECTOR, "symmetry sectors require at least one site");
+    apply_lattice_maps(b.at("symmetries"), d);
   }
   if (b.has("matrix_symmetry"))
     raise(QMBED_INVALID_OPTIONS, "matrix-valued symmetry sectors materialize as projected operator models");
-  if (b.has("reverse") && b.at("reverse").as_bool())
-    raise(QMBED_UNSUPPORTED_BACKEND, "maximum-representative ordering is not supported by the GPU engine");
-  return d;
+  if (b.has("reverse") && b.at("reverse").as_bool()) {
+    if (built_in)
+      raise(QMBED_UNSUPPORTED_BACKEND, "the reversed order of built-in momentum or parity sectors is not supported by "
+                                       "the GPU engine (send the sector as lattice maps)");
+    if (d.up > d.sites) raise(QMBED_INVALID_SECTOR, "particle count exceeds site count");
+    if (d.up >= 0) d.up = d.sites - d.up;
+    r.flipped = true;
+  }
+  return r;
 }
 
 // typed_local_operator (bindings/capi/src/lib.rs:6053-6071)
@@ -286,6 +387,73 @@ std::vector<TermDesc> parse_terms(const Value& terms, C64 scale = C64(1.0, 0.0))
     out.push_back(std::move(term));
   }
   return out;
+}
+
+// Spin-flip image C P C of one local product: C z C = -z, C S+ C = S-,
+// C S- C = S+, C x C = x and C y C = -y in every normalisation of spin one
+// half. Other symbols pass through and are rejected when the operator is built.
+std::vector<TermDesc> flip_terms(std::vector<TermDesc> terms) {
+  for (TermDesc& t : terms) {
+    double sign = 1.0;
+    for (char& c : t.symbols) {
+      if (c == 'z' || c == 'y') sign = -sign;
+      else if (c == '+') c = '-';
+      else if (c == '-') c = '+';
+    }
+    for (auto& coupling : t.couplings) coupling.coefficient *= sign;
+  }
+  return terms;
+}
+
+// The site labels a frontend uses for one model: the reference's
+// site_permutation (OperatorSpec::with_site_permutation,
+// src/operator/mod.rs:264-300, applied to terms and components by
+// EdModel::with_site_permutation and to later term requests by
+// prepare_terms, src/interop.rs:682-707, 1285-1296), followed by the spin flip
+// of a reversed basis.
+struct SiteConvention {
+  std::vector<int> permutation;  // empty: identity
+  bool flipped = false;
+
+  bool same_sites(const SiteConvention& o) const { return permutation == o.permutation; }
+
+  std::vector<TermDesc> prepare(std::vector<TermDesc> terms) const {
+    if (!permutation.empty())
+      for (TermDesc& t : terms)
+        for (auto& coupling : t.couplings)
+          for (int& site : coupling.sites) {
+            if (site >= static_cast<int>(permutation.size()))
+              raise(QMBED_INVALID_SITE, "site " + std::to_string(site) + " is outside a lattice with " +
+                                            std::to_string(permutation.size()) + " sites");
+            site = permutation[site];
+          }
+    return flipped ? flip_terms(std::move(terms)) : terms;
+  }
+};
+
+// validate_site_permutation (src/interop.rs:1328-1344)
+SiteConvention parse_convention(const Value& request, bool flipped) {
+  SiteConvention c;
+  c.flipped = flipped;
+  if (const Value* p = request.find("site_permutation"); p && !p->is_null()) {
+    const auto& items = p->items();
+    const long long n = static_cast<long long>(items.size());
+    for (const Value& v : items) {
+      const long long site = v.as_int();
+      if (site < 0) raise(QMBED_INVALID_OPTIONS, "site permutation entries are non-negative integers");
+      if (site >= n)
+        raise(QMBED_INVALID_SITE, "site " + std::to_string(site) + " is outside a lattice with " + std::to_string(n) +
+                                      " sites");
+    }
+    std::vector<char> seen(items.size(), 0);
+    for (const Value& v : items) {
+      const long long site = v.as_int();
+      if (seen[site]) raise(QMBED_INVALID_OPTIONS, "site permutation must be bijective");
+      seen[site] = 1;
+      c.permutation.push_back(static_cast<int>(site));
+    }
+  }
+  return c;
 }
 
 OperatorChecks parse_checks(const Value& request) {
@@ -428,6 +596,7 @@ struct Component {
 
 struct Model {
   std::shared_ptr<SpinBasis> basis;
+  SiteConvention convention;
   std::vector<TermDesc> terms;
   std::vector<Component> components;
   OperatorChecks checks;
@@ -530,16 +699,16 @@ std::shared_ptr<qmbed_lanczos_s> registered_lanczos(const std::string& text) {
 
 std::shared_ptr<Model> build_model(const Value& request) {
   auto model = std::make_shared<Model>();
-  model->basis = std::make_shared<SpinBasis>(parse_basis(request.at("basis")), default_device());
-  model->terms = parse_terms(request.at("terms"));
+  const BasisRequest basis = parse_basis(request.at("basis"));
+  model->convention = parse_convention(request, basis.flipped);
+  model->terms = model->convention.prepare(parse_terms(request.at("terms")));
   model->checks = parse_checks(request);
-  if (request.has("site_permutation")) raise(QMBED_UNSUPPORTED_BACKEND, "site permutations are not supported by the GPU engine");
   if (const Value* comps = request.find("components"))
     if (comps->is_array())
       for (const Value& c : comps->items()) {
         Component comp;
         comp.name = c.at("name").as_string();
-        comp.terms = parse_terms(c.at("terms"));
+        comp.terms = model->convention.prepare(parse_terms(c.at("terms")));
         comp.has_default = c.has("default");
         if (comp.has_default) {
           const auto& d = c.at("default").items();
@@ -547,6 +716,7 @@ std::shared_ptr<Model> build_model(const Value& request) {
         }
         model->components.push_back(std::move(comp));
       }
+  model->basis = std::make_shared<SpinBasis>(basis.desc, default_device());
   return model;
 }
 
@@ -556,18 +726,18 @@ std::vector<std::vector<C64>> parse_vectors(const Value& v) {
   return out;
 }
 
-Value apply_vectors(qmbed_operator_s& handle, const std::vector<std::vector<C64>>& vectors) {
+// The operator applied to host columns, one GPU application per column.
+std::vector<std::vector<C64>> apply_columns(qmbed_operator_s& handle, const std::vector<std::vector<C64>>& vectors,
+                                            const char* mismatch) {
   std::lock_guard<std::mutex> lock(handle.mu);
   const uint64_t dim = handle.op->dim();
   BlockOps& ops = handle.block_ops();
   DeviceBuffer x(std::max<uint64_t>(dim, 1) * 16), y(std::max<uint64_t>(dim, 1) * 16);
   std::vector<double> host(2 * dim);
-  Value out = Value::object();
-  out.set("kind", Value::string("vectors"));
-  out.set("dimension", Value::integer(static_cast<long long>(vectors.empty() ? dim : vectors[0].size())));
-  Value vs = Value::array();
+  std::vector<std::vector<C64>> out;
+  out.reserve(vectors.size());
   for (const auto& v : vectors) {
-    if (v.size() != dim) raise(QMBED_DIMENSION_MISMATCH, "vector length does not match the model dimension");
+    if (v.size() != dim) raise(QMBED_DIMENSION_MISMATCH, mismatch);
     for (uint64_t i = 0; i < dim; ++i) {
       host[2 * i] = v[i].real();
       host[2 * i + 1] = v[i].imag();
@@ -576,12 +746,119 @@ Value apply_vectors(qmbed_operator_s& handle, const std::vector<std::vector<C64>
     handle.op->apply(64, true, x.get(), y.get(), ops.stream());
     QMBED_CUDA(cudaMemcpyAsync(host.data(), y.get(), 16 * dim, cudaMemcpyDeviceToHost, ops.stream()));
     ops.sync();
+    std::vector<C64> r(dim);
+    for (uint64_t i = 0; i < dim; ++i) r[i] = C64(host[2 * i], host[2 * i + 1]);
+    out.push_back(std::move(r));
+  }
+  return out;
+}
+
+Value apply_vectors(qmbed_operator_s& handle, const std::vector<std::vector<C64>>& vectors) {
+  const auto applied = apply_columns(handle, vectors, "vector length does not match the model dimension");
+  Value out = Value::object();
+  out.set("kind", Value::string("vectors"));
+  out.set("dimension", Value::integer(static_cast<long long>(vectors.empty() ? handle.op->dim() : vectors[0].size())));
+  Value vs = Value::array();
+  for (const auto& v : applied) {
     Value r = Value::array();
-    for (uint64_t i = 0; i < dim; ++i) r.push(complex_pair(C64(host[2 * i], host[2 * i + 1])));
+    for (const C64& e : v) r.push(complex_pair(e));
     vs.push(std::move(r));
   }
   out.set("vectors", std::move(vs));
   return out;
+}
+
+// inner (src/measure/mod.rs:68-73): conjugate-linear in the left argument
+C64 inner(const std::vector<C64>& left, const std::vector<C64>& right) {
+  C64 sum(0.0, 0.0);
+  for (size_t i = 0; i < left.size() && i < right.size(); ++i) sum += std::conj(left[i]) * right[i];
+  return sum;
+}
+
+Value measurements_value(std::vector<long long> shape, const std::vector<C64>& values) {
+  Value out = Value::object();
+  out.set("kind", Value::string("measurements"));
+  Value s = Value::array();
+  for (long long n : shape) s.push(Value::integer(n));
+  out.set("shape", std::move(s));
+  Value v = Value::array();
+  for (const C64& x : values) v.push(complex_pair(x));
+  out.set("values", std::move(v));
+  return out;
+}
+
+// command_matrix_elements (bindings/capi/src/lib.rs:4362-4396) with
+// matrix_element (src/measure/mod.rs:101-115): <left| H |right> for every
+// pair, or for matching pairs when `diagonal`.
+Value matrix_elements(Model& model, const Value& request) {
+  const auto left = parse_vectors(request.at("left_vectors"));
+  const auto right = parse_vectors(request.at("right_vectors"));
+  const bool diagonal = request.has("diagonal") && request.at("diagonal").as_bool();
+  if (diagonal && left.size() != right.size())
+    raise(QMBED_DIMENSION_MISMATCH, "diagonal matrix elements require equal vector batches");
+  auto op = model.materialize(request.find("parameters"), kStoragePacked, false);
+  const char* mismatch = "matrix-element vectors do not match the operator shape";
+  for (const auto& l : left)
+    if (l.size() != op->op->dim()) raise(QMBED_DIMENSION_MISMATCH, mismatch);
+  const auto applied = apply_columns(*op, right, mismatch);
+  std::vector<C64> values;
+  if (diagonal) {
+    for (size_t i = 0; i < left.size(); ++i) values.push_back(inner(left[i], applied[i]));
+    return measurements_value({static_cast<long long>(left.size())}, values);
+  }
+  for (const auto& l : left)
+    for (const auto& a : applied) values.push_back(inner(l, a));
+  return measurements_value({static_cast<long long>(left.size()), static_cast<long long>(right.size())}, values);
+}
+
+// command_measure_model (bindings/capi/src/lib.rs:4398-4432): per sample,
+// expectation <s|H|s> and raw fluctuation <s|H^2|s> - <s|H|s>^2 of a pure
+// state (src/measure/mod.rs:117-175), or Tr(rho H) and Tr(rho H^2) - Tr(rho H)^2
+// of a row-major density matrix (1336-1390); no normalisation is imposed.
+Value measure(Model& model, const Value& request) {
+  const std::string what = request.at("measurement").as_string();
+  const bool fluctuation = what == "quantum_fluctuation";
+  if (!fluctuation && what != "expectation")
+    raise(QMBED_INVALID_OPTIONS, "measurement must be `expectation` or `quantum_fluctuation`");
+  std::vector<C64> values;
+  for (const Value& sample : request.at("samples").items()) {
+    const std::string kind = sample.at("kind").as_string();
+    if (kind != "pure" && kind != "density") raise(QMBED_INVALID_OPTIONS, "measurement samples are `pure` or `density`");
+    const auto state = parse_vector(sample.at("values"));
+    auto op = model.materialize(sample.find("parameters"), kStoragePacked, false);
+    const uint64_t dim = op->op->dim();
+    if (kind == "pure") {
+      const char* mismatch = fluctuation ? "raw quantum fluctuation requires a square operator matching the state"
+                                         : "matrix-element vectors do not match the operator shape";
+      const auto once = apply_columns(*op, {state}, mismatch);
+      const C64 mean = inner(state, once[0]);
+      if (!fluctuation) {
+        values.push_back(mean);
+        continue;
+      }
+      const auto twice = apply_columns(*op, once, mismatch);
+      values.push_back(inner(state, twice[0]) - mean * mean);
+      continue;
+    }
+    if (state.size() != dim * dim)
+      raise(QMBED_DIMENSION_MISMATCH, fluctuation ? "density fluctuation requires a square operator and matching density"
+                                                  : "density expectation requires a square operator and matching density");
+    std::vector<std::vector<C64>> columns(dim, std::vector<C64>(dim));
+    for (uint64_t r = 0; r < dim; ++r)
+      for (uint64_t c = 0; c < dim; ++c) columns[c][r] = state[r * dim + c];
+    const auto once = apply_columns(*op, columns, "density expectation requires a square operator and matching density");
+    C64 mean(0.0, 0.0);
+    for (uint64_t c = 0; c < dim; ++c) mean += once[c][c];
+    if (!fluctuation) {
+      values.push_back(mean);
+      continue;
+    }
+    const auto twice = apply_columns(*op, once, "density fluctuation requires a square operator and matching density");
+    C64 second(0.0, 0.0);
+    for (uint64_t c = 0; c < dim; ++c) second += twice[c][c];
+    values.push_back(second - mean * mean);
+  }
+  return measurements_value({static_cast<long long>(values.size())}, values);
 }
 
 Value run_request(const Value& request) {
@@ -591,10 +868,20 @@ Value run_request(const Value& request) {
 }
 
 Value describe_basis(const Value& request) {
-  SpinBasis basis(parse_basis(request.at("basis")), default_device());
+  const BasisRequest request_basis = parse_basis(request.at("basis"));
+  SpinBasis basis(request_basis.desc, default_device());
   const uint64_t n = basis.dim();
   std::vector<uint64_t> lo(n), hi(n);
   basis.copy_states(0, n, lo.data(), hi.data(), nullptr);
+  if (request_basis.flipped) {  // the reversed basis lists the complements of the engine's states
+    const int L = request_basis.desc.sites;
+    const uint64_t lo_mask = L >= 64 ? ~0ull : (1ull << L) - 1;
+    const uint64_t hi_mask = L >= 128 ? ~0ull : (L > 64 ? (1ull << (L - 64)) - 1 : 0ull);
+    for (uint64_t i = 0; i < n; ++i) {
+      lo[i] = ~lo[i] & lo_mask;
+      hi[i] = ~hi[i] & hi_mask;
+    }
+  }
   Value out = Value::object();
   out.set("kind", Value::string("basis"));
   out.set("dimension", Value::integer(static_cast<long long>(n)));
@@ -779,6 +1066,8 @@ Value command(const Value& request) {
     auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
     return apply_vectors(*op, parse_vectors(request.at("vectors")));
   }
+  if (operation == "matrix_elements_model") return matrix_elements(*registered_model(request.at("handle").as_string()), request);
+  if (operation == "measure_model") return measure(*registered_model(request.at("handle").as_string()), request);
   if (operation == "create_expm_action") {
     auto model = registered_model(request.at("handle").as_string());
     auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
@@ -886,7 +1175,12 @@ Value command(const Value& request) {
     // two spin-sector models: apply_sector_shift of the request's terms
     auto source = registered_model(request.at("source_handle").as_string());
     auto target = registered_model(request.at("target_handle").as_string());
-    const auto terms = parse_terms(request.at("terms"));
+    if (!source->convention.same_sites(target->convention))
+      raise(QMBED_INVALID_OPTIONS, "models must use the same site permutation for cross-basis operations");
+    if (source->convention.flipped != target->convention.flipped)
+      raise(QMBED_UNSUPPORTED_BACKEND, "cross-sector actions between reversed and ordinary bases are not supported by "
+                                       "the GPU engine");
+    const auto terms = source->convention.prepare(parse_terms(request.at("terms")));
     const auto vectors = parse_vectors(request.at("vectors"));
     OperatorChecks checks;
     checks.hermiticity = false;

@@ -224,6 +224,38 @@ struct RowList {
   int overflow;
 };
 
+// Stable insertion sort by column, then equal columns added in the order they
+// were collected (so a row's sums do not depend on when this runs).
+__host__ __device__ inline void sort_coalesce(RowList& out) {
+  for (int i = 1; i < out.count; ++i) {
+    const uint32_t c = out.col[i];
+    const double a = out.re[i], b = out.im[i];
+    int j = i - 1;
+    while (j >= 0 && out.col[j] > c) {
+      out.col[j + 1] = out.col[j];
+      out.re[j + 1] = out.re[j];
+      out.im[j + 1] = out.im[j];
+      --j;
+    }
+    out.col[j + 1] = c;
+    out.re[j + 1] = a;
+    out.im[j + 1] = b;
+  }
+  int m = 0;
+  for (int i = 0; i < out.count; ++i) {
+    if (m > 0 && out.col[m - 1] == out.col[i]) {
+      out.re[m - 1] += out.re[i];
+      out.im[m - 1] += out.im[i];
+    } else {
+      out.col[m] = out.col[i];
+      out.re[m] = out.re[i];
+      out.im[m] = out.im[i];
+      ++m;
+    }
+  }
+  out.count = m;
+}
+
 // Expands `inst` on row r. With `with_ratio`, entries carry sqrt(R_r/R_c) and
 // the diagonal is kept as an ordinary entry; otherwise the ratio is left out
 // (the packed format applies it through the scaled input vector) and the
@@ -263,42 +295,18 @@ __host__ __device__ inline void collect_row(const OpView<S>& v, const Instance* 
       fi *= ratio;
     }
     if (out.count == kRowCap) {
-      out.overflow = 1;
-      continue;
+      sort_coalesce(out);  // the buffer holds kRowCap distinct columns at most
+      if (out.count == kRowCap) {
+        out.overflow = 1;
+        continue;
+      }
     }
     out.col[out.count] = static_cast<uint32_t>(L.col);
     out.re[out.count] = fr;
     out.im[out.count] = fi;
     ++out.count;
   }
-  // insertion sort by column, then coalesce equal columns
-  for (int i = 1; i < out.count; ++i) {
-    const uint32_t c = out.col[i];
-    const double a = out.re[i], b = out.im[i];
-    int j = i - 1;
-    while (j >= 0 && out.col[j] > c) {
-      out.col[j + 1] = out.col[j];
-      out.re[j + 1] = out.re[j];
-      out.im[j + 1] = out.im[j];
-      --j;
-    }
-    out.col[j + 1] = c;
-    out.re[j + 1] = a;
-    out.im[j + 1] = b;
-  }
-  int m = 0;
-  for (int i = 0; i < out.count; ++i) {
-    if (m > 0 && out.col[m - 1] == out.col[i]) {
-      out.re[m - 1] += out.re[i];
-      out.im[m - 1] += out.im[i];
-    } else {
-      out.col[m] = out.col[i];
-      out.re[m] = out.re[i];
-      out.im[m] = out.im[i];
-      ++m;
-    }
-  }
-  out.count = m;
+  sort_coalesce(out);
 }
 
 // |H[r,c]| <= eps entries are not stored (reference drop rule, mod.rs:2162-2164).

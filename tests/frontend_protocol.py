@@ -1,0 +1,173 @@
+"""Oracle answers to the reference's JSON protocol for spin chains (test infrastructure).
+
+``tests/golden/make_frontend_requests.py`` uses this interpreter as the
+stand-in native library while it records the requests that the reference's
+unmodified Python frontend sends (``qmbed._ffi._call_json``,
+bindings/python/src/qmbed/_ffi.py:189-207), and
+``tests/test_gpu_frontend_requests.py`` uses it for the expected answers when
+the same requests are replayed through ``libqmbed_b200.so``.
+
+Every operator is the dense reduced matrix of ``oracle.general.reduced_dense``
+(the reference's transition rule on lattice-map bases, with the model's site
+permutation), so the answers cover the request forms the frontend sends:
+``run`` (SolveRequest, bindings/capi/src/lib.rs:55-61) and the commands
+``create_model``, ``eigsh_model``, ``apply_model``, ``eigh_model``,
+``measure_model``, ``matrix_elements_model``, ``evolve_model`` and
+``release_model`` (lib.rs:64-410, 4362-4432, 5513-5990).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import scipy.linalg
+
+from oracle import general
+
+LOCAL = {"identity": "I", "z": "z", "raising": "+", "lowering": "-", "x": "x", "y": "y"}
+
+
+def oracle_terms(terms):
+    out = []
+    for t in terms:
+        symbols = "".join(LOCAL[name] for name in t["product"]["local"])
+        couplings = [(complex(*c["coefficient"]), tuple(c["sites"])) for c in t["couplings"]]
+        out.append((symbols, couplings))
+    return out
+
+
+def normalization(basis) -> str:
+    if basis.get("normalization"):
+        return basis["normalization"]
+    return "pauli_cartesian" if basis.get("pauli") else "angular_momentum"
+
+
+def oracle_basis(basis) -> general.GeneralSpinBasis:
+    """A spin basis request as lattice maps (built-in momentum k: i -> i+1 with sector k; parity p: i -> L-1-i)."""
+    sites = basis["sites"]
+    up = basis.get("up")
+    if basis.get("up_sectors") is not None:
+        (up,) = basis["up_sectors"]
+    maps = list(basis.get("symmetries") or [])
+    if basis.get("momentum") is not None:
+        maps.append({"destinations": [(i + 1) % sites for i in range(sites)], "sector": basis["momentum"]})
+    if basis.get("parity") is not None:
+        maps.append({"destinations": [sites - 1 - i for i in range(sites)], "sector": 0 if basis["parity"] == 1 else 1})
+    return general.GeneralSpinBasis(sites, up, maps, reverse=bool(basis.get("reverse")))
+
+
+def model_matrix(request) -> np.ndarray:
+    b = oracle_basis(request["basis"])
+    terms = oracle_terms(request["terms"])
+    for c in request.get("components") or []:
+        value = complex(*c["default"]) if c.get("default") is not None else 0.0
+        terms += [(s, [(value * k, sites) for k, sites in cs]) for s, cs in oracle_terms(c["terms"])]
+    return general.reduced_dense(b, terms, normalization(request["basis"]), request.get("site_permutation"))
+
+
+def complex_vectors(vectors):
+    return [np.array([complex(*v) for v in vec]) for vec in vectors]
+
+
+def pairs(vector):
+    return [[float(v.real), float(v.imag)] for v in np.asarray(vector, dtype=complex)]
+
+
+def selected(values, k, target):
+    kind = target["kind"]
+    order = {
+        "smallest_algebraic": np.argsort(values),
+        "largest_algebraic": np.argsort(-values),
+        "smallest_magnitude": np.argsort(np.abs(values)),
+        "largest_magnitude": np.argsort(-np.abs(values)),
+    }.get(kind)
+    if kind == "shift":
+        order = np.argsort(np.abs(values - target["value"]))
+    if order is None:
+        raise NotImplementedError(kind)
+    return order[:k]
+
+
+class OracleProtocol:
+    """Answers requests the way the reference library does, from dense oracle matrices."""
+
+    def __init__(self):
+        self.models = {}
+        self.next_handle = 1
+
+    def matrix(self, handle) -> np.ndarray:
+        return self.models[handle]
+
+    def eigensystem(self, h, solver):
+        values, vectors = np.linalg.eigh(h)
+        idx = selected(values, solver["eigenpairs"], solver["target"])
+        idx = sorted(idx, key=lambda i: values[i])
+        result = {"dimension": h.shape[0], "eigenvalues": [float(values[i]) for i in idx],
+                  "residuals": [0.0 for _ in idx], "iterations": 0, "converged": True}
+        if solver.get("eigenvectors"):
+            result["eigenvectors"] = [pairs(vectors[:, i]) for i in idx]
+        return result
+
+    def run(self, request):
+        return self.eigensystem(model_matrix(request), request["solver"])
+
+    def command(self, request):
+        op = request["operation"]
+        if op == "create_model":
+            handle = f"oracle-model-{self.next_handle}"
+            self.next_handle += 1
+            self.models[handle] = model_matrix(request)
+            return {"kind": "model", "handle": handle, "dimension": self.models[handle].shape[0]}
+        if op == "release_model":
+            self.models.pop(request["handle"], None)
+            return {"kind": "released"}
+        h = self.matrix(request["handle"])
+        if op == "eigsh_model":
+            return {"kind": "eigensystem", **self.eigensystem(h, request["solver"])}
+        if op == "apply_model":
+            return {"kind": "vectors", "dimension": h.shape[0],
+                    "vectors": [pairs(h @ v) for v in complex_vectors(request["vectors"])]}
+        if op == "eigh_model":
+            values, vectors = np.linalg.eigh(h)
+            out = {"kind": "eigensystem", "dimension": h.shape[0], "eigenvalues": values.tolist()}
+            if request.get("eigenvectors"):
+                out["eigenvectors"] = [pairs(vectors[:, i]) for i in range(h.shape[0])]
+            return out
+        if op == "matrix_elements_model":
+            left = complex_vectors(request["left_vectors"])
+            right = complex_vectors(request["right_vectors"])
+            if request.get("diagonal"):
+                values = [np.vdot(a, h @ b) for a, b in zip(left, right)]
+                shape = [len(left)]
+            else:
+                values = [np.vdot(a, h @ b) for a in left for b in right]
+                shape = [len(left), len(right)]
+            return {"kind": "measurements", "shape": shape, "values": pairs(values)}
+        if op == "measure_model":
+            fluct = request["measurement"] == "quantum_fluctuation"
+            values = []
+            for sample in request["samples"]:
+                s = np.array([complex(*v) for v in sample["values"]])
+                if sample["kind"] == "pure":
+                    mean = np.vdot(s, h @ s)
+                    values.append(np.vdot(s, h @ (h @ s)) - mean * mean if fluct else mean)
+                else:
+                    rho = s.reshape(h.shape)
+                    mean = np.trace(h @ rho)
+                    values.append(np.trace(h @ h @ rho) - mean * mean if fluct else mean)
+            return {"kind": "measurements", "shape": [len(values)], "values": pairs(values)}
+        if op == "evolve_model":
+            ev = request["evolution"]
+            times = ev["times"]
+            states = []
+            for t in times:
+                u = scipy.linalg.expm(-1j * t * h)
+                states.append([pairs(u @ v) for v in complex_vectors(request["vectors"])])
+            return {"kind": "evolution", "times": times, "states": states}
+        raise NotImplementedError(op)
+
+    def call(self, symbol, request):
+        if symbol == "qmbed_run_json":
+            return self.run(request)
+        if symbol == "qmbed_command_json":
+            return self.command(request)
+        raise NotImplementedError(symbol)

@@ -1,0 +1,171 @@
+"""Requests of the reference's unmodified Python frontend, replayed on the GPU.
+
+``tests/golden/frontend_requests.json`` holds, in order, the JSON requests that
+the reference's ``qmbed`` package and its QuSpin-compatible ``quspin`` package
+send for a few ordinary user scripts (recorded by
+``tests/golden/make_frontend_requests.py``): the native ``qmbed.eigsh`` and
+QuSpin ``hamiltonian`` objects on ``spin_basis_1d`` with ``kblock``/``pblock``
+lattice maps, reversed row order and the reversed site labelling, with
+``eigsh``, ``dot``, ``expt_value``, ``quant_fluct``, ``matrix_ele``,
+``eigvalsh`` and the Krylov ``evolve``. Each request goes unchanged through
+``qmbed_run_json`` / ``qmbed_command_json`` of ``libqmbed_b200.so`` (model
+handles are mapped to the ones this library returned) and each answer is
+checked against the oracle's answer to the same request
+(``tests/frontend_protocol.py``).
+"""
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIXTURE = Path(__file__).resolve().parent / "golden" / "frontend_requests.json"
+SCENARIOS = json.loads(FIXTURE.read_text())
+
+
+def _complex(vectors):
+    return [np.array([complex(*v) for v in vec]) for vec in vectors]
+
+
+def _check_eigensystem(got, expected, h, solver):
+    scale = np.maximum(1.0, np.abs(expected["eigenvalues"]))
+    np.testing.assert_allclose(sorted(got["eigenvalues"]), sorted(expected["eigenvalues"]), atol=1e-8 * scale.max())
+    assert got["dimension"] == expected["dimension"]
+    if solver.get("eigenvectors"):
+        vectors = _complex(got["eigenvectors"])
+        assert len(vectors) == len(got["eigenvalues"])
+        for value, v in zip(got["eigenvalues"], vectors):
+            assert abs(np.linalg.norm(v) - 1.0) <= 1e-10
+            assert np.linalg.norm(h @ v - value * v) <= 1e-7 * max(1.0, abs(value))
+
+
+@pytest.mark.parametrize("scenario", sorted(SCENARIOS))
+def test_frontend_requests_replay(scenario):
+    from frontend_protocol import OracleProtocol, model_matrix
+    from qmbed_b200._lib import command, run
+
+    oracle = OracleProtocol()
+    handles = {}
+    for call in SCENARIOS[scenario]["calls"]:
+        request = call["request"]
+        expected = oracle.call(call["symbol"], request)
+        sent = dict(request)
+        if "handle" in sent:
+            sent["handle"] = handles[sent["handle"]]
+        got = run(sent) if call["symbol"] == "qmbed_run_json" else command(sent)
+        op = request.get("operation", "run")
+        if op == "run":
+            _check_eigensystem(got, expected, model_matrix(request), request["solver"])
+        elif op == "create_model":
+            handles[expected["handle"]] = got["handle"]
+            assert got["dimension"] == expected["dimension"]
+        elif op == "eigsh_model":
+            _check_eigensystem(got, expected, oracle.matrix(request["handle"]), request["solver"])
+        elif op in ("apply_model", "evolve_model"):
+            key = "vectors" if op == "apply_model" else "states"
+            a = np.array(got[key], dtype=float)
+            b = np.array(expected[key], dtype=float)
+            assert a.shape == b.shape
+            tol = 1e-12 if op == "apply_model" else 1e-8
+            assert np.abs(a - b).max() <= tol * max(1.0, np.abs(b).max())
+        elif op in ("measure_model", "matrix_elements_model"):
+            assert got["kind"] == "measurements" and got["shape"] == expected["shape"]
+            np.testing.assert_allclose(np.array(got["values"]), np.array(expected["values"]), rtol=1e-10, atol=1e-10)
+        elif op == "eigh_model":
+            np.testing.assert_allclose(got["eigenvalues"], expected["eigenvalues"], atol=1e-10)
+        elif op == "release_model":
+            pass
+        else:
+            raise AssertionError(f"unexpected request {op}")
+
+
+def _quspin_maps(sites, kblock=None, pblock=None):
+    """QuSpin's spin_basis_1d lattice maps: translation i -> i-1 and reflection i -> L-1-i."""
+    maps = []
+    if kblock is not None:
+        maps.append({"destinations": [(i - 1) % sites for i in range(sites)], "sector": kblock})
+    if pblock is not None:
+        maps.append({"destinations": [sites - 1 - i for i in range(sites)], "sector": 0 if pblock == 1 else 1})
+    return maps
+
+
+@pytest.mark.parametrize("sites,up,kblock,pblock,reverse", [
+    (10, 5, 0, 1, True), (10, 4, 3, None, True), (11, 5, 2, None, False), (9, None, 0, -1, True),
+    (8, 3, None, None, True), (8, None, None, None, True),
+])
+def test_lattice_map_bases_list_the_reference_states(sites, up, kblock, pblock, reverse):
+    """describe_basis on lattice-map sectors: representatives, order and count of the oracle's general basis."""
+    from oracle import general
+    from qmbed_b200._lib import command
+    maps = _quspin_maps(sites, kblock, pblock)
+    basis = {"kind": "spin", "sites": sites, "up": up, "symmetries": maps, "reverse": reverse}
+    got = command({"operation": "describe_basis", "basis": basis})
+    expected = general.GeneralSpinBasis(sites, up, maps, reverse=reverse)
+    assert got["dimension"] == len(expected)
+    assert [int(s) for s in got["states"]] == [int(s) for s in expected.states]
+
+
+def test_lattice_maps_and_site_labels_reject_what_the_engine_does_not_build():
+    from qmbed_b200 import QmbedError
+    from qmbed_b200._lib import command
+    L = 8
+    base = {"kind": "spin", "sites": L, "up": 4}
+    terms = [{"product": {"local": ["z", "z"]}, "couplings": [{"coefficient": [1.0, 0.0], "sites": [0, 1]}]}]
+    cases = [
+        ({**base, "symmetries": [{"destinations": [(i + 2) % L for i in range(L)], "sector": 0}]}, None,
+         "^unsupported backend"),
+        ({**base, "symmetries": [{"destinations": list(range(L)), "sector": 0,
+                                  "local_permutations": [[1, 0]] * L}]}, None, "^unsupported backend"),
+        ({**base, "symmetries": [{"destinations": [0] * L, "sector": 0}]}, None, "^incompatible symmetry request"),
+        ({**base, "momentum": 0, "reverse": True}, None, "^unsupported backend"),
+        ({**base, "momentum": 0, "symmetries": _quspin_maps(L, 0)}, None, "^invalid options"),
+        (base, [0, 1, 2, 3, 4, 5, 6, 8], "^site 8 is outside a lattice with 8 sites"),
+        (base, [0, 1, 2, 3, 4, 5, 6, 6], "^invalid options: site permutation must be bijective"),
+    ]
+    for basis, permutation, message in cases:
+        request = {"operation": "create_model", "basis": basis, "terms": terms}
+        if permutation is not None:
+            request["site_permutation"] = permutation
+        with pytest.raises(QmbedError, match=message):
+            command(request)
+
+
+def test_reversed_models_match_the_oracle_for_every_local_symbol():
+    """C H C on the complemented sector: every local symbol, complex couplings and a site permutation.
+
+    The couplings are translation invariant and symmetric under exchanging the
+    two factors, so the operator commutes with the chain's lattice maps (for an
+    operator that does not, the reduced matrix depends on how it is assembled).
+    """
+    from frontend_protocol import model_matrix
+    from qmbed_b200._lib import command
+    L = 10
+    rng = np.random.default_rng(5)
+    names = ["identity", "z", "raising", "lowering", "x", "y"]
+    coefficients = rng.standard_normal((6, 6)) + 1j * rng.standard_normal((6, 6))
+    coefficients = coefficients + coefficients.T
+    terms = []
+    for i_a, a in enumerate(names):
+        for i_b, b in enumerate(names):
+            c = coefficients[i_a, i_b]
+            terms.append({"product": {"local": [a, b]},
+                          "couplings": [{"coefficient": [c.real, c.imag], "sites": [i, (i + 3) % L]} for i in range(L)]})
+    for up, maps in [(None, []), (None, _quspin_maps(L, 0, 1)), (None, _quspin_maps(L, 3))]:
+        request = {"operation": "create_model",
+                   "basis": {"kind": "spin", "sites": L, "up": up, "normalization": "pauli", "symmetries": maps,
+                             "reverse": True},
+                   "terms": terms, "site_permutation": list(range(L))[::-1],
+                   "checks": {"hermiticity": False, "particle_conservation": False}}
+        h = model_matrix(request)
+        model = command(request)
+        try:
+            x = rng.standard_normal((2, h.shape[0])) + 1j * rng.standard_normal((2, h.shape[0]))
+            got = command({"operation": "apply_model", "handle": model["handle"],
+                           "vectors": [[[v.real, v.imag] for v in col] for col in x]})
+            y = np.array([[complex(*v) for v in col] for col in got["vectors"]])
+            assert np.abs(y - x @ h.T).max() <= 1e-12 * max(1.0, np.abs(h).max() * h.shape[0])
+        finally:
+            command({"operation": "release_model", "handle": model["handle"]})
