@@ -87,6 +87,16 @@ __device__ inline bool is_orbit_minimum(S s, const SectorParams& p, S mask) {
     for (int sh = 0; sh < translations; ++sh)
       if (rotate_state(u, sh, p.sites, mask) < s) return false;
   }
+  if (p.inversion != 0) {
+    const S c = static_cast<S>(~s & mask);
+    for (int sh = 0; sh < translations; ++sh)
+      if (rotate_state(c, sh, p.sites, mask) < s) return false;
+    if (p.parity != 0) {
+      S u = reflect_state(c, p.sites);
+      for (int sh = 0; sh < translations; ++sh)
+        if (rotate_state(u, sh, p.sites, mask) < s) return false;
+    }
+  }
   return true;
 }
 
@@ -174,6 +184,7 @@ __global__ void images_kernel(SectorParams p, const S* states, const uint16_t* o
         pr = phase_table[2 * c.shift];
         pi = phase_table[2 * c.shift + 1];
         if (c.reflected) { pr *= p.parity; pi *= p.parity; }
+        if (c.inverted) { pr *= p.inversion; pi *= p.inversion; }
         orbit = orbits[idx];
       }
     }
@@ -212,7 +223,15 @@ SpinBasis::SpinBasis(const SpinBasisDesc& desc, int device) : device_(device), n
   p.has_momentum = desc.has_momentum ? 1 : 0;
   p.momentum = p.has_momentum ? ((desc.momentum % desc.sites) + desc.sites) % desc.sites : 0;
   p.parity = desc.parity;
-  p.symmetric = (p.has_momentum || p.parity != 0) ? 1 : 0;
+  if (desc.inversion != 0 && desc.inversion != 1 && desc.inversion != -1)
+    raise(QMBED_INVALID_SECTOR, "spin inversion must be either -1 or +1");
+  if (desc.inversion != 0 && desc.up >= 0 && 2 * desc.up != desc.sites)
+    raise(QMBED_UNSUPPORTED_BACKEND, "spin inversion of a magnetisation sector other than up = L/2 mixes two sectors, "
+                                     "which the GPU engine does not build");
+  if (desc.inversion != 0 && desc.sites > 64)
+    raise(QMBED_UNSUPPORTED_BACKEND, "spin inversion sectors are built for chains of at most 64 sites");
+  p.inversion = desc.inversion;
+  p.symmetric = (p.has_momentum || p.parity != 0 || p.inversion != 0) ? 1 : 0;
   if (p.parity != 0 && p.has_momentum && p.momentum != 0 && 2 * p.momentum != p.sites)
     raise(QMBED_INCOMPATIBLE_SYMMETRY, "parity can share a one-dimensional sector with momentum only at k=0 or k=pi");
   p.n_divisors = 0;

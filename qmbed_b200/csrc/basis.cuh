@@ -14,6 +14,7 @@ struct SpinBasisDesc {
   int momentum;      // any integer; canonicalised modulo L
   int parity;        // 0 none, +-1
   int normalization; // Normalization
+  int inversion;     // 0 none, +-1: global spin-flip sector (up = L/2 or the full space, L <= 64)
 };
 
 // Layout in HBM:

@@ -224,15 +224,17 @@ int default_device() {
 // generates every translation, and exp(-2 pi i sector / L) on T^t is the
 // built-in momentum k with k t = sector (mod L) (the built-in T moves site i to
 // i + 1 with character exp(-2 pi i k / L), src/basis/mod.rs:661-676, 786-790).
-// The reflection i -> L-1-i with sector s is the built-in parity (-1)^s. The
-// reduced vectors, gauge (the representative's coefficient) and orbit sizes
-// of both constructions agree (GeneralBasis::from_reducer_impl,
+// The reflection i -> L-1-i with sector s is the built-in parity (-1)^s, and
+// the global spin flip (identity destinations, every local map [1, 0]) with
+// sector s is the engine's spin-inversion sector (-1)^s. The reduced vectors,
+// gauge (the representative's coefficient) and orbit sizes of both
+// constructions agree (GeneralBasis::from_reducer_impl,
 // src/basis/mod.rs:4180-4306; spin_symmetry_sector, 715-848). Other maps
-// (sublattice translations, spin inversion, arbitrary permutations) are
+// (sublattice translations, partial spin flips, arbitrary permutations) are
 // reported as unsupported.
 void apply_lattice_maps(const Value& list, SpinBasisDesc& d) {
   const int L = d.sites;
-  bool translation = false, reflection = false;
+  bool translation = false, reflection = false, inversion = false;
   for (const Value& s : list.items()) {
     const auto& items = s.at("destinations").items();
     if (static_cast<int>(items.size()) != L)
@@ -246,6 +248,7 @@ void apply_lattice_maps(const Value& list, SpinBasisDesc& d) {
       seen[v] = 1;
       dest[i] = static_cast<int>(v);
     }
+    int swaps = 0;
     if (const Value* local = s.find("local_permutations"); local && !local->is_null()) {
       const auto& rows = local->items();
       if (static_cast<int>(rows.size()) != L)
@@ -255,7 +258,7 @@ void apply_lattice_maps(const Value& list, SpinBasisDesc& d) {
         const bool identity = r.size() == 2 && r[0].as_int() == 0 && r[1].as_int() == 1;
         const bool swap = r.size() == 2 && r[0].as_int() == 1 && r[1].as_int() == 0;
         if (!identity && !swap) raise(QMBED_INCOMPATIBLE_SYMMETRY, "every local-state map must be a permutation");
-        if (swap) raise(QMBED_UNSUPPORTED_BACKEND, "local spin-inversion maps are not supported by the GPU engine");
+        swaps += swap ? 1 : 0;
       }
     }
     const long long sector = s.at("sector").as_int();
@@ -264,6 +267,16 @@ void apply_lattice_maps(const Value& list, SpinBasisDesc& d) {
     for (int i = 0; i < L; ++i) {
       is_translation = is_translation && dest[i] == (i + t) % L;
       is_reflection = is_reflection && dest[i] == L - 1 - i;
+    }
+    if (swaps != 0) {
+      // the global spin flip (QuSpin's zblock): every digit swapped, no site moved; period 2
+      if (swaps != L || !is_translation || t != 0)
+        raise(QMBED_UNSUPPORTED_BACKEND, "local spin maps other than the global spin flip are not supported by the "
+                                         "GPU engine");
+      if (inversion) raise(QMBED_UNSUPPORTED_BACKEND, "more than one spin-flip generator is not supported by the GPU engine");
+      inversion = true;
+      d.inversion = ((sector % 2) + 2) % 2 == 0 ? 1 : -1;
+      continue;
     }
     if (is_translation && t == 0) continue;  // the identity: period 1, every sector trivial
     if (is_translation) {
@@ -595,6 +608,7 @@ struct Component {
 };
 
 struct Model {
+  uint64_t id = 0;  // registry id (never reused), 0 for unregistered models
   std::shared_ptr<SpinBasis> basis;
   SiteConvention convention;
   std::vector<TermDesc> terms;
@@ -603,7 +617,9 @@ struct Model {
   std::mutex mu;
   std::map<std::string, std::shared_ptr<qmbed_operator_s>> cache;  // parameters+storage -> operator
 
-  std::shared_ptr<qmbed_operator_s> materialize(const Value* parameters, int storage, bool hermitian_check) {
+  // The model's terms with every component scaled by its parameter value
+  // (supplied, else the default); `key` receives the parameter values.
+  std::vector<TermDesc> resolved_terms(const Value* parameters, std::string& key) const {
     std::map<std::string, C64> values;
     if (parameters && parameters->is_object())
       for (auto& kv : parameters->members()) {
@@ -614,7 +630,6 @@ struct Model {
         values[kv.first] = C64(p.at(0).as_double(), p.at(1).as_double());
       }
     std::vector<TermDesc> all = terms;
-    std::string key = std::to_string(storage) + (hermitian_check ? "h" : "n");
     for (auto& c : components) {
       C64 v;
       auto it = values.find(c.name);
@@ -630,14 +645,26 @@ struct Model {
         all.push_back(std::move(scaled));
       }
     }
+    return all;
+  }
+
+  // One operator per distinct key, built on first use.
+  std::shared_ptr<qmbed_operator_s> cached(const std::string& key, const std::vector<TermDesc>& all, OperatorChecks c,
+                                           int storage) {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
-    OperatorChecks c = checks;
-    c.hermiticity = hermitian_check && checks.hermiticity;
     auto op = make_operator(basis, all, c, storage);
     cache[key] = op;
     return op;
+  }
+
+  std::shared_ptr<qmbed_operator_s> materialize(const Value* parameters, int storage, bool hermitian_check) {
+    std::string key = std::to_string(storage) + (hermitian_check ? "h" : "n");
+    const std::vector<TermDesc> all = resolved_terms(parameters, key);
+    OperatorChecks c = checks;
+    c.hermiticity = hermitian_check && checks.hermiticity;
+    return cached(key, all, c, storage);
   }
 };
 
@@ -906,13 +933,71 @@ Value describe_basis(const Value& request) {
 // actions are not built).
 // Matrix, scale, transform and binary expressions build operator algebra
 // outside the GPU engine.
-std::shared_ptr<qmbed_operator_s> expression_operator(const Value& e, int storage = kStoragePacked) {
+// A linear operator expression flattened to (model, parameters, coefficient)
+// parts: Model, Scale and Binary add/subtract of OperatorExpressionRequest
+// (bindings/capi/src/lib.rs:789-818) with the normal action.
+struct ExpressionPart {
+  std::shared_ptr<Model> model;
+  const Value* parameters;
+  C64 coefficient;
+};
+
+void flatten_expression(const Value& e, C64 scale, std::vector<ExpressionPart>& parts) {
   const std::string kind = e.at("kind").as_string();
-  if (kind != "model") raise(QMBED_UNSUPPORTED_BACKEND, "operator expressions of kind `" + kind + "` are outside the GPU engine");
-  if (e.has("action") && e.at("action").as_string() != "normal")
-    raise(QMBED_UNSUPPORTED_BACKEND, "only the normal action is supported by the GPU engine");
-  auto model = registered_model(e.at("handle").as_string());
-  return model->materialize(e.find("parameters"), storage, false);
+  if (kind == "model") {
+    if (e.has("action") && e.at("action").as_string() != "normal")
+      raise(QMBED_UNSUPPORTED_BACKEND, "only the normal action is supported by the GPU engine");
+    parts.push_back({registered_model(e.at("handle").as_string()), e.find("parameters"), scale});
+    return;
+  }
+  if (kind == "scale") {
+    const auto& c = e.at("coefficient").items();
+    if (c.size() != 2) raise(QMBED_INVALID_OPTIONS, "coefficients are [re, im] pairs");
+    flatten_expression(e.at("operand"), scale * C64(c[0].as_double(), c[1].as_double()), parts);
+    return;
+  }
+  if (kind == "binary") {
+    const std::string op = e.at("operation").as_string();
+    if (op != "add" && op != "subtract")
+      raise(QMBED_UNSUPPORTED_BACKEND, "operator products are outside the GPU engine");
+    flatten_expression(e.at("left"), scale, parts);
+    flatten_expression(e.at("right"), op == "add" ? scale : -scale, parts);
+    return;
+  }
+  raise(QMBED_UNSUPPORTED_BACKEND, "operator expressions of kind `" + kind + "` are outside the GPU engine");
+}
+
+bool same_space(const Model& a, const Model& b) {
+  const SectorParams& x = a.basis->params();
+  const SectorParams& y = b.basis->params();
+  return x.sites == y.sites && x.up == y.up && x.has_momentum == y.has_momentum && x.momentum == y.momentum &&
+         x.parity == y.parity && x.inversion == y.inversion && a.basis->normalization() == b.basis->normalization() &&
+         a.convention.same_sites(b.convention) && a.convention.flipped == b.convention.flipped;
+}
+
+std::shared_ptr<qmbed_operator_s> expression_operator(const Value& e, int storage = kStoragePacked) {
+  std::vector<ExpressionPart> parts;
+  flatten_expression(e, C64(1.0, 0.0), parts);
+  if (parts.size() == 1 && parts[0].coefficient == C64(1.0, 0.0))
+    return parts[0].model->materialize(parts[0].parameters, storage, false);
+  Model& first = *parts[0].model;
+  std::string key = "expression|" + std::to_string(storage);
+  std::vector<TermDesc> all;
+  for (const ExpressionPart& part : parts) {
+    if (!same_space(first, *part.model))
+      raise(QMBED_DIMENSION_MISMATCH, "operator expression terms act on different spaces");
+    char buffer[160];
+    std::snprintf(buffer, sizeof(buffer), "|%llu*%.17g,%.17g", static_cast<unsigned long long>(part.model->id),
+                  part.coefficient.real(), part.coefficient.imag());
+    key += buffer;
+    for (TermDesc t : part.model->resolved_terms(part.parameters, key)) {
+      for (auto& coupling : t.couplings) coupling.coefficient *= part.coefficient;
+      all.push_back(std::move(t));
+    }
+  }
+  OperatorChecks c = first.checks;
+  c.hermiticity = false;
+  return first.cached(key, all, c, storage);
 }
 
 // ExpmActionPlan applied to a host column batch (the apply step of
@@ -1032,9 +1117,15 @@ Value command(const Value& request) {
     auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
     return operator_entries(*op, request.has("format") ? request.at("format").as_string() : "csc");
   }
+  if (operation == "evaluate_operator_expression") {
+    // EvaluateOperatorExpression -> command_operator_value (bindings/capi/src/lib.rs:5660-5663)
+    auto op = expression_operator(request.at("expression"), kStoragePacked);
+    return operator_entries(*op, request.has("format") ? request.at("format").as_string() : "csc");
+  }
   if (operation == "create_model") {
     auto model = build_model(request);
     const uint64_t id = g_next_model.fetch_add(1);
+    model->id = id;
     {
       std::lock_guard<std::mutex> lock(g_registry_mu);
       g_models[id] = model;
@@ -2124,7 +2215,7 @@ int qmbed_gpu_spectral_function(qmbed_operator target, qmbed_shift probe, uint64
     const SectorParams& a = probe->target->params();
     const SectorParams& b = target->op->basis().params();
     const bool same = a.sites == b.sites && a.up == b.up && a.has_momentum == b.has_momentum &&
-                      a.momentum == b.momentum && a.parity == b.parity &&
+                      a.momentum == b.momentum && a.parity == b.parity && a.inversion == b.inversion &&
                       probe->target->normalization() == target->op->basis().normalization();
     if (!same || probe->target->dim() != nt || n_source != ns)
       raise(QMBED_DIMENSION_MISMATCH, "target Hamiltonian, source, and probe shapes are incompatible");

@@ -160,7 +160,8 @@ struct SectorParams {
   int has_momentum;   // translation sector selected
   int momentum;       // canonical k in [0, L)
   int parity;         // 0 none, else +-1
-  int symmetric;      // has_momentum || parity
+  int inversion;      // 0 none, else +-1: character of the global spin flip (every bit inverted)
+  int symmetric;      // has_momentum || parity || inversion
   int n_divisors;     // proper divisors of L in increasing order (periods)
   int divisors[32];
 };
@@ -169,28 +170,39 @@ struct SectorParams {
 template <typename S>
 struct Canonical {
   S rep;          // minimum of the orbit (reference rep = min, mod.rs:785-788)
-  int shift;      // rotate(t or reflect(t), shift) == rep
+  int shift;      // rotate(t' or reflect(t'), shift) == rep, t' = t or its spin flip
   int reflected;  // 1 if the minimum came from the reflected state
+  int inverted;   // 1 if the minimum came from the spin-flipped state
 };
 
-// Minimum over translations (and reflections) of `t`, with the translation
-// and reflection that reach it. Translation-only sectors use shifts 0..L-1;
-// parity-only sectors use {t, reflect(t)}.
+// Folds the translations (and reflections) of `t` into `best`, starting at
+// shift `first_shift`.
 template <typename S>
-__host__ __device__ inline Canonical<S> canonicalize(S t, const SectorParams& p, S mask) {
-  Canonical<S> best{t, 0, 0};
+__host__ __device__ inline void scan_orbit(S t, const SectorParams& p, S mask, int first_shift, int inverted,
+                                           Canonical<S>& best) {
   const int translations = p.has_momentum ? p.sites : 1;
-  for (int s = 1; s < translations; ++s) {
+  for (int s = first_shift; s < translations; ++s) {
     S r = rotate_state(t, s, p.sites, mask);
-    if (r < best.rep) { best.rep = r; best.shift = s; }
+    if (r < best.rep) best = Canonical<S>{r, s, 0, inverted};
   }
   if (p.parity != 0) {
     S u = reflect_state(t, p.sites);
     for (int s = 0; s < translations; ++s) {
       S r = rotate_state(u, s, p.sites, mask);
-      if (r < best.rep) { best.rep = r; best.shift = s; best.reflected = 1; }
+      if (r < best.rep) best = Canonical<S>{r, s, 1, inverted};
     }
   }
+}
+
+// Minimum over translations (and reflections, and the global spin flip) of
+// `t`, with the group element that reaches it. Translation-only sectors use
+// shifts 0..L-1; parity-only sectors use {t, reflect(t)}; the spin flip
+// doubles the scan with ~t (it commutes with every site permutation).
+template <typename S>
+__host__ __device__ inline Canonical<S> canonicalize(S t, const SectorParams& p, S mask) {
+  Canonical<S> best{t, 0, 0, 0};
+  scan_orbit(t, p, mask, 1, 0, best);
+  if (p.inversion != 0) scan_orbit(static_cast<S>(~t & mask), p, mask, 0, 1, best);
   return best;
 }
 
@@ -209,7 +221,7 @@ __host__ __device__ inline int translation_period(S rep, const SectorParams& p, 
 // one-dimensional projection rules of spin_symmetry_sector (mod.rs:785-841):
 // an orbit belongs to the sector iff its projected coefficients are nonzero.
 template <typename S>
-__host__ __device__ inline int orbit_size_if_compatible(S rep, const SectorParams& p, S mask) {
+__host__ __device__ inline int lattice_orbit_size_if_compatible(S rep, const SectorParams& p, S mask) {
   int period = translation_period(rep, p, mask);
   if (p.has_momentum && (static_cast<long long>(p.momentum) * period) % p.sites != 0) return 0;
   if (p.parity == 0) return period;
@@ -225,6 +237,41 @@ __host__ __device__ inline int orbit_size_if_compatible(S rep, const SectorParam
   int sign = 1;
   if (p.has_momentum && 2 * p.momentum == p.sites && (self_shift & 1)) sign = -1;
   return (p.parity * sign == 1) ? period : 0;
+}
+
+// Character exp(-2 pi i k s / L) of T^s when it is real (+-1); 2 otherwise.
+__host__ __device__ inline int real_translation_character(int s, const SectorParams& p) {
+  if (!p.has_momentum) return 1;
+  const long long m = (static_cast<long long>(p.momentum) * s) % p.sites;
+  if (m == 0) return 1;
+  return 2 * m == p.sites ? -1 : 2;
+}
+
+// Orbit size and compatibility with the spin flip Z (character z) added to
+// the lattice group G: if Z rep = g rep for some g in G, the stabiliser holds
+// g^-1 Z and the orbit belongs to the sector iff chi(g) = z (then its size is
+// that of the G orbit); otherwise Z doubles the orbit. This is the
+// one-dimensional orbit rule of the reference's general reducer
+// (trace_symmetry_orbit, src/basis/mod.rs:3455-3538) for these generators.
+template <typename S>
+__host__ __device__ inline int orbit_size_if_compatible(S rep, const SectorParams& p, S mask) {
+  const int base = lattice_orbit_size_if_compatible(rep, p, mask);
+  if (base == 0 || p.inversion == 0) return base;
+  const S flipped = static_cast<S>(~rep & mask);
+  const int translations = p.has_momentum ? p.sites : 1;
+  int character = 0;
+  for (int s = 0; s < translations && character == 0; ++s)
+    if (rotate_state(rep, s, p.sites, mask) == flipped) character = real_translation_character(s, p);
+  if (character == 0 && p.parity != 0) {
+    const S u = reflect_state(rep, p.sites);
+    for (int s = 0; s < translations && character == 0; ++s)
+      if (rotate_state(u, s, p.sites, mask) == flipped) {
+        character = real_translation_character(s, p);
+        if (character != 2) character *= p.parity;
+      }
+  }
+  if (character == 0) return 2 * base;
+  return character == p.inversion ? base : 0;
 }
 
 }  // namespace qmbed

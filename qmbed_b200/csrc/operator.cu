@@ -134,7 +134,7 @@ __host__ __device__ inline Located locate(const OpView<S>& v, S t) {
   if (out.col >= 0) {
     out.pr = v.phase[2 * c.shift];
     out.pi = v.phase[2 * c.shift + 1];
-    if (c.reflected && v.p.parity < 0) {
+    if ((c.reflected && v.p.parity < 0) != (c.inverted && v.p.inversion < 0)) {
       out.pr = -out.pr;
       out.pi = -out.pi;
     }

@@ -11,9 +11,10 @@ Every operator is the dense reduced matrix of ``oracle.general.reduced_dense``
 (the reference's transition rule on lattice-map bases, with the model's site
 permutation), so the answers cover the request forms the frontend sends:
 ``run`` (SolveRequest, bindings/capi/src/lib.rs:55-61) and the commands
-``create_model``, ``eigsh_model``, ``apply_model``, ``eigh_model``,
-``measure_model``, ``matrix_elements_model``, ``evolve_model`` and
-``release_model`` (lib.rs:64-410, 4362-4432, 5513-5990).
+``describe_basis``, ``create_model``, ``eigsh_model``, ``apply_model``,
+``eigh_model``, ``measure_model``, ``matrix_elements_model``,
+``evolve_model``, ``release_model`` and the Lanczos resource commands on
+linear model expressions (lib.rs:64-410, 4046-4212, 4362-4432, 5513-5990).
 """
 
 from __future__ import annotations
@@ -22,6 +23,12 @@ import numpy as np
 import scipy.linalg
 
 from oracle import general
+
+def _oracle_module():
+    from oracle import oracle
+    oracle.build()
+    return oracle
+
 
 LOCAL = {"identity": "I", "z": "z", "raising": "+", "lowering": "-", "x": "x", "y": "y"}
 
@@ -92,7 +99,50 @@ class OracleProtocol:
 
     def __init__(self):
         self.models = {}
+        self.lanczos = {}
         self.next_handle = 1
+
+    def expression_matrix(self, e) -> np.ndarray:
+        """OperatorExpressionRequest (bindings/capi/src/lib.rs:789-818) for models without parameters."""
+        kind = e["kind"]
+        if kind == "model":
+            if e.get("action", "normal") != "normal" or e.get("parameters"):
+                raise NotImplementedError("model expression with an action or parameters")
+            return self.models[e["handle"]]
+        if kind == "scale":
+            return complex(*e["coefficient"]) * self.expression_matrix(e["operand"])
+        if kind == "binary":
+            left, right = self.expression_matrix(e["left"]), self.expression_matrix(e["right"])
+            return {"add": left + right, "subtract": left - right, "product": left @ right}[e["operation"]]
+        raise NotImplementedError(kind)
+
+    def lanczos_command(self, op, request):
+        """command_lanczos_* (bindings/capi/src/lib.rs:4046-4212) with the C++ oracle's lanczos_ritz."""
+        if op == "lanczos_operator":
+            h = self.expression_matrix(request["expression"])
+            rows, cols = np.nonzero(h)
+            operator = _oracle_module().Operator.from_triplets(h.shape[0], rows, cols, h[rows, cols])
+            d = operator.lanczos_ritz(np.array([complex(*v) for v in request["initial"]]),
+                                      request["krylov_dimension"], request.get("tolerance", 1e-13))
+            handle = f"oracle-lanczos-{self.next_handle}"
+            self.next_handle += 1
+            self.lanczos[handle] = d
+            return {"kind": "lanczos", "handle": handle, "dimension": h.shape[0],
+                    "krylov_dimension": len(d["values"]), "initial_norm": d["initial_norm"],
+                    "eigenvalues": d["values"].tolist(), "eigenvectors": d["vectors"].T.tolist()}
+        d = self.lanczos[request["lanczos_handle"]]
+        if op == "lanczos_combine":
+            c = np.array([complex(*v) for v in request["coefficients"]])
+        elif op == "lanczos_exponential":
+            a = complex(*request["coefficient"])
+            v = d["vectors"]
+            c = v @ (v[0, :] * np.exp(a * d["values"]) * d["initial_norm"])
+        elif op == "release_lanczos":
+            self.lanczos.pop(request["lanczos_handle"])
+            return {"kind": "released"}
+        else:
+            raise NotImplementedError(op)
+        return {"kind": "vectors", "dimension": d["basis"].shape[1], "vectors": [pairs(c @ d["basis"])]}
 
     def matrix(self, handle) -> np.ndarray:
         return self.models[handle]
@@ -117,9 +167,28 @@ class OracleProtocol:
             self.next_handle += 1
             self.models[handle] = model_matrix(request)
             return {"kind": "model", "handle": handle, "dimension": self.models[handle].shape[0]}
+        if op == "describe_basis":
+            b = oracle_basis(request["basis"])
+            return {"kind": "basis", "dimension": len(b), "states": [str(int(x)) for x in b.states]}
         if op == "release_model":
             self.models.pop(request["handle"], None)
             return {"kind": "released"}
+        if op.startswith("lanczos_") or op == "release_lanczos":
+            return self.lanczos_command(op, request)
+        if op == "eigsh_operator_expression":
+            return {"kind": "eigensystem", **self.eigensystem(self.expression_matrix(request["expression"]),
+                                                              request["solver"])}
+        if op == "apply_operator_expression":
+            h = self.expression_matrix(request["expression"])
+            return {"kind": "vectors", "dimension": h.shape[0],
+                    "vectors": [pairs(h @ v) for v in complex_vectors(request["vectors"])]}
+        if op in ("materialize_model", "evaluate_operator_expression"):
+            h = self.matrix(request["handle"]) if op == "materialize_model" else \
+                self.expression_matrix(request["expression"])
+            rows, cols = np.nonzero(h)
+            return {"kind": "operator", "shape": list(h.shape), "format": request.get("format", "csc"),
+                    "entries": [{"row": int(r), "column": int(c), "value": pairs([h[r, c]])[0]}
+                                for r, c in zip(rows, cols)]}
         h = self.matrix(request["handle"])
         if op == "eigsh_model":
             return {"kind": "eigensystem", **self.eigensystem(h, request["solver"])}

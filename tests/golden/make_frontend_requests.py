@@ -125,6 +125,24 @@ def scenarios(qmbed):
         H.expt_value(rho)
         H.quant_fluct(rho)
 
+    def quspin_lanczos_tools():
+        """QuSpin's Lanczos tools on -H in a kblock=0, pblock=1, zblock=1 sector (the compat test_Lanczos flow)."""
+        from quspin.tools.lanczos import expm_lanczos, lanczos_full, lanczos_iter, lin_comb_Q_T
+        L = 16
+        basis = spin_basis_1d(L, m=0, kblock=0, pblock=1, zblock=1)
+        J = [[1.0, i, (i + 1) % L] for i in range(L)]
+        H = -hamiltonian([[op, J] for op in ["xx", "yy", "zz"]], [], basis=basis, dtype=np.float64)
+        v0 = rng.normal(0, 1, size=basis.Ns)
+        v0 /= np.linalg.norm(v0)
+        E1, V1, lv1 = lanczos_full(H, v0, 20)
+        E2, V2, lv2 = lanczos_iter(H, v0, 20)
+        expm_lanczos(E1, V1, lv1, a=-0.1j)
+        expm_lanczos(E2, V2, lv2, a=-0.1j)
+        H.eigsh(k=1, which="LA")
+        E, V, Q = lanczos_full(H, v0, 30, full_ortho=False)
+        lin_comb_Q_T(V[:, -1], Q)
+        H.static
+
     def quspin_fixed_magnetisation():
         """spin_basis_1d(L, Nup) without lattice maps: reversed order and site permutation only."""
         L = 10
@@ -135,7 +153,8 @@ def scenarios(qmbed):
         H.dot(rng.standard_normal(H.Ns))
 
     return {f.__name__: f for f in (native_eigsh, quspin_real_sector, quspin_complex_sector,
-                                     quspin_transverse_field, quspin_density_matrix, quspin_fixed_magnetisation)}
+                                     quspin_transverse_field, quspin_density_matrix, quspin_lanczos_tools,
+                                     quspin_fixed_magnetisation)}
 
 
 def main() -> None:

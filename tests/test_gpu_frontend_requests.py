@@ -42,6 +42,24 @@ def _check_eigensystem(got, expected, h, solver):
             assert np.linalg.norm(h @ v - value * v) <= 1e-7 * max(1.0, abs(value))
 
 
+def _substitute(value, handles):
+    """The request with every recorded handle (model or Lanczos, at any depth) replaced by this library's."""
+    if isinstance(value, dict):
+        return {k: _substitute(v, handles) for k, v in value.items()}
+    if isinstance(value, list):
+        return [_substitute(v, handles) for v in value]
+    if isinstance(value, str) and value in handles:
+        return handles[value]
+    return value
+
+
+def _dense(result):
+    h = np.zeros(result["shape"], dtype=complex)
+    for e in result["entries"]:
+        h[e["row"], e["column"]] += complex(*e["value"])
+    return h
+
+
 @pytest.mark.parametrize("scenario", sorted(SCENARIOS))
 def test_frontend_requests_replay(scenario):
     from frontend_protocol import OracleProtocol, model_matrix
@@ -52,9 +70,7 @@ def test_frontend_requests_replay(scenario):
     for call in SCENARIOS[scenario]["calls"]:
         request = call["request"]
         expected = oracle.call(call["symbol"], request)
-        sent = dict(request)
-        if "handle" in sent:
-            sent["handle"] = handles[sent["handle"]]
+        sent = _substitute(request, handles)
         got = run(sent) if call["symbol"] == "qmbed_run_json" else command(sent)
         op = request.get("operation", "run")
         if op == "run":
@@ -62,8 +78,30 @@ def test_frontend_requests_replay(scenario):
         elif op == "create_model":
             handles[expected["handle"]] = got["handle"]
             assert got["dimension"] == expected["dimension"]
+        elif op == "describe_basis":
+            assert got["dimension"] == expected["dimension"] and got["states"] == expected["states"]
         elif op == "eigsh_model":
             _check_eigensystem(got, expected, oracle.matrix(request["handle"]), request["solver"])
+        elif op == "eigsh_operator_expression":
+            _check_eigensystem(got, expected, oracle.expression_matrix(request["expression"]), request["solver"])
+        elif op == "lanczos_operator":
+            handles[expected["handle"]] = got["handle"]
+            assert got["krylov_dimension"] == expected["krylov_dimension"]
+            assert abs(got["initial_norm"] - expected["initial_norm"]) <= 1e-12 * expected["initial_norm"]
+            scale = max(1.0, np.abs(expected["eigenvalues"]).max())
+            np.testing.assert_allclose(got["eigenvalues"], expected["eigenvalues"], atol=1e-10 * scale)
+            for a, b in zip(got["eigenvectors"], expected["eigenvectors"]):  # columns up to sign
+                a, b = np.array(a), np.array(b)
+                assert min(np.abs(a - b).max(), np.abs(a + b).max()) <= 1e-8
+        elif op in ("materialize_model", "evaluate_operator_expression"):
+            assert got["shape"] == expected["shape"]
+            assert np.abs(_dense(got) - _dense(expected)).max() <= 1e-12 * max(1.0, np.abs(_dense(expected)).max())
+        elif op in ("lanczos_combine", "lanczos_exponential"):
+            a = np.array(got["vectors"], dtype=float)
+            b = np.array(expected["vectors"], dtype=float)
+            assert a.shape == b.shape and np.abs(a - b).max() <= 1e-10 * max(1.0, np.abs(b).max())
+        elif op in ("release_lanczos",):
+            pass
         elif op in ("apply_model", "evolve_model"):
             key = "vectors" if op == "apply_model" else "states"
             a = np.array(got[key], dtype=float)
@@ -82,25 +120,30 @@ def test_frontend_requests_replay(scenario):
             raise AssertionError(f"unexpected request {op}")
 
 
-def _quspin_maps(sites, kblock=None, pblock=None):
-    """QuSpin's spin_basis_1d lattice maps: translation i -> i-1 and reflection i -> L-1-i."""
+def _quspin_maps(sites, kblock=None, pblock=None, zblock=None):
+    """QuSpin's spin_basis_1d lattice maps: translation i -> i-1, reflection i -> L-1-i, global spin flip."""
     maps = []
     if kblock is not None:
         maps.append({"destinations": [(i - 1) % sites for i in range(sites)], "sector": kblock})
     if pblock is not None:
         maps.append({"destinations": [sites - 1 - i for i in range(sites)], "sector": 0 if pblock == 1 else 1})
+    if zblock is not None:
+        maps.append({"destinations": list(range(sites)), "sector": 0 if zblock == 1 else 1,
+                     "local_permutations": [[1, 0]] * sites})
     return maps
 
 
-@pytest.mark.parametrize("sites,up,kblock,pblock,reverse", [
-    (10, 5, 0, 1, True), (10, 4, 3, None, True), (11, 5, 2, None, False), (9, None, 0, -1, True),
-    (8, 3, None, None, True), (8, None, None, None, True),
+@pytest.mark.parametrize("sites,up,kblock,pblock,zblock,reverse", [
+    (10, 5, 0, 1, None, True), (10, 4, 3, None, None, True), (11, 5, 2, None, None, False),
+    (9, None, 0, -1, None, True), (8, 3, None, None, None, True), (8, None, None, None, None, True),
+    (10, 5, 0, 1, 1, True), (10, 5, 0, 1, -1, True), (12, 6, 6, -1, 1, True), (12, 6, 3, None, -1, True),
+    (8, None, None, None, -1, True), (9, None, 0, 1, 1, False), (14, 7, 0, None, 1, False),
 ])
-def test_lattice_map_bases_list_the_reference_states(sites, up, kblock, pblock, reverse):
+def test_lattice_map_bases_list_the_reference_states(sites, up, kblock, pblock, zblock, reverse):
     """describe_basis on lattice-map sectors: representatives, order and count of the oracle's general basis."""
     from oracle import general
     from qmbed_b200._lib import command
-    maps = _quspin_maps(sites, kblock, pblock)
+    maps = _quspin_maps(sites, kblock, pblock, zblock)
     basis = {"kind": "spin", "sites": sites, "up": up, "symmetries": maps, "reverse": reverse}
     got = command({"operation": "describe_basis", "basis": basis})
     expected = general.GeneralSpinBasis(sites, up, maps, reverse=reverse)
@@ -118,6 +161,9 @@ def test_lattice_maps_and_site_labels_reject_what_the_engine_does_not_build():
         ({**base, "symmetries": [{"destinations": [(i + 2) % L for i in range(L)], "sector": 0}]}, None,
          "^unsupported backend"),
         ({**base, "symmetries": [{"destinations": list(range(L)), "sector": 0,
+                                  "local_permutations": [[1, 0]] * (L - 1) + [[0, 1]]}]}, None, "^unsupported backend"),
+        ({**base, "up": 3, "symmetries": _quspin_maps(L, zblock=1)}, None, "^unsupported backend"),
+        ({**base, "symmetries": [{"destinations": [(i + 1) % L for i in range(L)], "sector": 0,
                                   "local_permutations": [[1, 0]] * L}]}, None, "^unsupported backend"),
         ({**base, "symmetries": [{"destinations": [0] * L, "sector": 0}]}, None, "^incompatible symmetry request"),
         ({**base, "momentum": 0, "reverse": True}, None, "^unsupported backend"),
@@ -162,6 +208,50 @@ def test_reversed_models_match_the_oracle_for_every_local_symbol():
         h = model_matrix(request)
         model = command(request)
         try:
+            x = rng.standard_normal((2, h.shape[0])) + 1j * rng.standard_normal((2, h.shape[0]))
+            got = command({"operation": "apply_model", "handle": model["handle"],
+                           "vectors": [[[v.real, v.imag] for v in col] for col in x]})
+            y = np.array([[complex(*v) for v in col] for col in got["vectors"]])
+            assert np.abs(y - x @ h.T).max() <= 1e-12 * max(1.0, np.abs(h).max() * h.shape[0])
+        finally:
+            command({"operation": "release_model", "handle": model["handle"]})
+
+
+@pytest.mark.parametrize("kblock,pblock,zblock", [(0, 1, 1), (0, 1, -1), (5, -1, 1), (3, None, -1), (None, None, 1)])
+def test_spin_flip_sectors_match_the_oracle(kblock, pblock, zblock):
+    """Operators that commute with the spin flip on zblock sectors (full space and up = L/2), reversed order."""
+    from frontend_protocol import model_matrix
+    from qmbed_b200._lib import command
+    L = 10
+    rng = np.random.default_rng(11)
+
+    def term(local, coefficient, offset):
+        return {"product": {"local": local},
+                "couplings": [{"coefficient": [coefficient, 0.0], "sites": [(i + k) % L for k in offset]}
+                              for i in range(L)]}
+
+    flip_even = [
+        (["x"], (0,)), (["x", "x"], (0, 1)), (["y", "y"], (0, 1)), (["z", "z"], (0, 2)),
+        (["raising", "lowering"], (0, 1)),
+    ]
+    # y z is flip-even; with z y of the same coefficient it is also reflection-even
+    c_yz = float(rng.standard_normal())
+    for up in (None, 5):
+        terms = [term(local, float(rng.standard_normal()), offset) for local, offset in flip_even]
+        terms.append(dict(terms[-1], product={"local": ["lowering", "raising"]}))  # S+S- + S-S+, one coefficient
+        terms += [term(["y", "z"], c_yz, (0, 3)), term(["z", "y"], c_yz, (0, 3))]
+        if up is not None:
+            terms = [t for t in terms if t["product"]["local"] not in (["x"],)]
+            terms = [t for t in terms if "y" not in t["product"]["local"] and t["product"]["local"] != ["x", "x"]]
+        request = {"operation": "create_model",
+                   "basis": {"kind": "spin", "sites": L, "up": up, "normalization": "pauli",
+                             "symmetries": _quspin_maps(L, kblock, pblock, zblock), "reverse": True},
+                   "terms": terms, "site_permutation": list(range(L))[::-1],
+                   "checks": {"hermiticity": True, "particle_conservation": up is not None}}
+        h = model_matrix(request)
+        model = command(request)
+        try:
+            assert model["dimension"] == h.shape[0]
             x = rng.standard_normal((2, h.shape[0])) + 1j * rng.standard_normal((2, h.shape[0]))
             got = command({"operation": "apply_model", "handle": model["handle"],
                            "vectors": [[[v.real, v.imag] for v in col] for col in x]})
