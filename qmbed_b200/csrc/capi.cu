@@ -23,6 +23,7 @@
 #include "evolve.cuh"
 #include "expm.cuh"
 #include "json.hpp"
+#include "matrix.cuh"
 #include "mlp.cuh"
 #include "operator.cuh"
 #include "spectrum.cuh"
@@ -552,9 +553,7 @@ Value vectors_value(const std::vector<double>& host, uint64_t dim, size_t count)
 }
 
 // Runs eigsh and returns the SolveResult / Eigensystem JSON fields.
-Value solve(qmbed_operator_s& handle, const SolverRequest& request, bool tagged) {
-  std::lock_guard<std::mutex> lock(handle.mu);
-  LinearOperatorView view = handle.view();
+Value solve_view(const LinearOperatorView& view, BlockOps& ops, const SolverRequest& request, bool tagged) {
   std::vector<double> initial;
   for (const auto& v : request.initial) {
     if (v.size() != view.dim) raise(QMBED_DIMENSION_MISMATCH, "eigsh initial vector does not match the operator");
@@ -565,8 +564,7 @@ Value solve(qmbed_operator_s& handle, const SolverRequest& request, bool tagged)
   }
   EigshOptions options = request.options;
   options.want_vectors = request.eigenvectors;
-  EigshResult r = eigsh(view, options, initial.data(), static_cast<int>(request.initial.size()), request.mode,
-                        handle.block_ops());
+  EigshResult r = eigsh(view, options, initial.data(), static_cast<int>(request.initial.size()), request.mode, ops);
   Value out = Value::object();
   if (tagged) out.set("kind", Value::string("eigensystem"));
   const uint64_t dim = view.dim;
@@ -591,6 +589,11 @@ Value solve(qmbed_operator_s& handle, const SolverRequest& request, bool tagged)
     out.set("eigenvectors", vectors_value(host, dim, k));
   }
   return out;
+}
+
+Value solve(qmbed_operator_s& handle, const SolverRequest& request, bool tagged) {
+  std::lock_guard<std::mutex> lock(handle.mu);
+  return solve_view(handle.view(), handle.block_ops(), request, tagged);
 }
 
 std::shared_ptr<qmbed_operator_s> make_operator(std::shared_ptr<SpinBasis> basis, const std::vector<TermDesc>& terms,
@@ -668,8 +671,40 @@ struct Model {
   }
 };
 
+// An operator model given by explicit matrix entries: create_operator_model
+// with a static operator and neither components nor a basis
+// (build_operator_model, bindings/capi/src/lib.rs:5605-5622). Its handle
+// shares the model handle sequence.
+struct MatrixModel {
+  std::shared_ptr<CsrMatrix> matrix;
+  cudaStream_t stream = nullptr;
+  std::unique_ptr<BlockOps> ops;
+  std::mutex mu;
+  ~MatrixModel() {
+    ops.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
+  BlockOps& block_ops() {
+    if (!ops) {
+      QMBED_CUDA(cudaSetDevice(matrix->device()));
+      QMBED_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+      ops = std::make_unique<BlockOps>(matrix->device(), stream);
+    }
+    return *ops;
+  }
+  LinearOperatorView view() {
+    BlockOps& b = block_ops();
+    const CsrMatrix* raw = matrix.get();
+    cudaStream_t s = b.stream();
+    return LinearOperatorView{raw->dim(), raw->is_real(), [raw, s](int prec, bool cplx, const void* x, void* y) {
+                                raw->apply(prec, cplx, x, y, s);
+                              }};
+  }
+};
+
 struct ExpmEntry {
   std::shared_ptr<qmbed_operator_s> op;
+  std::shared_ptr<MatrixModel> matrix;  // set instead of `op` for explicit-matrix models
   ExpmPlan plan;
 };
 
@@ -686,6 +721,37 @@ uint64_t parse_handle(const std::string& text, const char* what) {
   if (text.empty() || !end || *end != '\0' || value == 0)
     raise(QMBED_INVALID_OPTIONS, std::string(what) + " handle \"" + text + "\" is not a positive integer");
   return value;
+}
+
+std::map<uint64_t, std::shared_ptr<MatrixModel>> g_matrix_models;
+
+// The explicit-matrix model behind a model handle, or null for a term model.
+std::shared_ptr<MatrixModel> matrix_model(const std::string& text) {
+  const uint64_t id = parse_handle(text, "model");
+  std::lock_guard<std::mutex> lock(g_registry_mu);
+  auto it = g_matrix_models.find(id);
+  return it == g_matrix_models.end() ? nullptr : it->second;
+}
+
+// MatrixRequest (bindings/capi/src/lib.rs:744-754): shape and entries.
+std::shared_ptr<CsrMatrix> parse_matrix(const Value& m) {
+  const auto& shape = m.at("shape").items();
+  if (shape.size() != 2) raise(QMBED_INVALID_OPTIONS, "matrix shape is a [rows, columns] pair");
+  const long long rows = shape[0].as_int(), cols = shape[1].as_int();
+  if (rows < 0 || cols < 0) raise(QMBED_INVALID_OPTIONS, "matrix shape entries are non-negative");
+  if (rows != cols) raise(QMBED_DIMENSION_MISMATCH, "an operator model requires a square matrix");
+  std::vector<uint64_t> r, c;
+  std::vector<C64> v;
+  for (const Value& e : m.at("entries").items()) {
+    const long long row = e.at("row").as_int(), column = e.at("column").as_int();
+    if (row < 0 || column < 0) raise(QMBED_INVALID_OPTIONS, "matrix entry indices are non-negative");
+    const auto& value = e.at("value").items();
+    if (value.size() != 2) raise(QMBED_INVALID_OPTIONS, "matrix values are [re, im] pairs");
+    r.push_back(static_cast<uint64_t>(row));
+    c.push_back(static_cast<uint64_t>(column));
+    v.emplace_back(value[0].as_double(), value[1].as_double());
+  }
+  return std::make_shared<CsrMatrix>(default_device(), static_cast<uint64_t>(rows), r, c, v);
 }
 
 std::shared_ptr<Model> registered_model(const std::string& text) {
@@ -754,11 +820,9 @@ std::vector<std::vector<C64>> parse_vectors(const Value& v) {
 }
 
 // The operator applied to host columns, one GPU application per column.
-std::vector<std::vector<C64>> apply_columns(qmbed_operator_s& handle, const std::vector<std::vector<C64>>& vectors,
-                                            const char* mismatch) {
-  std::lock_guard<std::mutex> lock(handle.mu);
-  const uint64_t dim = handle.op->dim();
-  BlockOps& ops = handle.block_ops();
+std::vector<std::vector<C64>> apply_columns(const LinearOperatorView& view, BlockOps& ops,
+                                            const std::vector<std::vector<C64>>& vectors, const char* mismatch) {
+  const uint64_t dim = view.dim;
   DeviceBuffer x(std::max<uint64_t>(dim, 1) * 16), y(std::max<uint64_t>(dim, 1) * 16);
   std::vector<double> host(2 * dim);
   std::vector<std::vector<C64>> out;
@@ -770,7 +834,7 @@ std::vector<std::vector<C64>> apply_columns(qmbed_operator_s& handle, const std:
       host[2 * i + 1] = v[i].imag();
     }
     QMBED_CUDA(cudaMemcpyAsync(x.get(), host.data(), 16 * dim, cudaMemcpyHostToDevice, ops.stream()));
-    handle.op->apply(64, true, x.get(), y.get(), ops.stream());
+    view.apply(64, true, x.get(), y.get());
     QMBED_CUDA(cudaMemcpyAsync(host.data(), y.get(), 16 * dim, cudaMemcpyDeviceToHost, ops.stream()));
     ops.sync();
     std::vector<C64> r(dim);
@@ -780,11 +844,16 @@ std::vector<std::vector<C64>> apply_columns(qmbed_operator_s& handle, const std:
   return out;
 }
 
-Value apply_vectors(qmbed_operator_s& handle, const std::vector<std::vector<C64>>& vectors) {
-  const auto applied = apply_columns(handle, vectors, "vector length does not match the model dimension");
+std::vector<std::vector<C64>> apply_columns(qmbed_operator_s& handle, const std::vector<std::vector<C64>>& vectors,
+                                            const char* mismatch) {
+  std::lock_guard<std::mutex> lock(handle.mu);
+  return apply_columns(handle.view(), handle.block_ops(), vectors, mismatch);
+}
+
+Value vectors_result(const std::vector<std::vector<C64>>& applied, uint64_t dim) {
   Value out = Value::object();
   out.set("kind", Value::string("vectors"));
-  out.set("dimension", Value::integer(static_cast<long long>(vectors.empty() ? handle.op->dim() : vectors[0].size())));
+  out.set("dimension", Value::integer(static_cast<long long>(dim)));
   Value vs = Value::array();
   for (const auto& v : applied) {
     Value r = Value::array();
@@ -793,6 +862,11 @@ Value apply_vectors(qmbed_operator_s& handle, const std::vector<std::vector<C64>
   }
   out.set("vectors", std::move(vs));
   return out;
+}
+
+Value apply_vectors(qmbed_operator_s& handle, const std::vector<std::vector<C64>>& vectors) {
+  const auto applied = apply_columns(handle, vectors, "vector length does not match the model dimension");
+  return vectors_result(applied, handle.op->dim());
 }
 
 // inner (src/measure/mod.rs:68-73): conjugate-linear in the left argument
@@ -1002,13 +1076,9 @@ std::shared_ptr<qmbed_operator_s> expression_operator(const Value& e, int storag
 
 // ExpmActionPlan applied to a host column batch (the apply step of
 // ExpmMultiplyParallel, src/solve/mod.rs:252-326), one column at a time.
-Value expm_vectors(qmbed_operator_s& h, const ExpmPlan& plan, const std::vector<std::vector<C64>>& vectors) {
-  std::lock_guard<std::mutex> lock(h.mu);
-  const uint64_t dim = h.op->dim();
-  BlockOps& ops = h.block_ops();
-  LinearOperatorView view{dim, h.op->is_real(), [&h, &ops](int prec, bool cplx, const void* x, void* y) {
-                            h.op->apply(prec, cplx, x, y, ops.stream());
-                          }};
+Value expm_vectors(const LinearOperatorView& view, BlockOps& ops, const ExpmPlan& plan,
+                   const std::vector<std::vector<C64>>& vectors) {
+  const uint64_t dim = view.dim;
   DeviceBuffer state(std::max<uint64_t>(dim, 1) * 16);
   std::vector<double> host(2 * dim);
   Value out = Value::object();
@@ -1030,6 +1100,11 @@ Value expm_vectors(qmbed_operator_s& h, const ExpmPlan& plan, const std::vector<
   }
   out.set("vectors", std::move(vs));
   return out;
+}
+
+Value expm_vectors(qmbed_operator_s& h, const ExpmPlan& plan, const std::vector<std::vector<C64>>& vectors) {
+  std::lock_guard<std::mutex> lock(h.mu);
+  return expm_vectors(h.view(), h.block_ops(), plan, vectors);
 }
 
 // create_expm_action / expm_operator_expression options: ExpmMultiplyParallel
@@ -1101,6 +1176,58 @@ Value operator_entries(qmbed_operator_s& h, const std::string& format) {
 Value command(const Value& request) {
   const std::string operation = request.at("operation").as_string();
   if (operation == "describe_basis") return describe_basis(request);
+  if (operation == "create_operator_model") {
+    if (request.has("basis")) raise(QMBED_UNSUPPORTED_BACKEND, "basis-embedded operator models are not supported by the GPU engine");
+    if (const Value* c = request.find("components"); c && c->is_array() && !c->items().empty())
+      raise(QMBED_UNSUPPORTED_BACKEND, "operator models with matrix components are not supported by the GPU engine");
+    if (!request.has("static_operator")) raise(QMBED_INVALID_OPTIONS, "an operator model needs a static operator");
+    auto model = std::make_shared<MatrixModel>();
+    model->matrix = parse_matrix(request.at("static_operator"));
+    const uint64_t id = g_next_model.fetch_add(1);
+    {
+      std::lock_guard<std::mutex> lock(g_registry_mu);
+      g_matrix_models[id] = model;
+    }
+    Value out = Value::object();
+    out.set("kind", Value::string("model"));
+    out.set("handle", Value::string(std::to_string(id)));
+    out.set("dimension", Value::integer(static_cast<long long>(model->matrix->dim())));
+    return out;
+  }
+  if (operation == "create_expm_action" || operation == "apply_model" || operation == "eigsh_model") {
+    if (auto mm = matrix_model(request.at("handle").as_string())) {
+      if (request.has("parameters") && request.at("parameters").is_object() && !request.at("parameters").members().empty())
+        raise(QMBED_INVALID_OPTIONS, "this operator model has no parameters");
+      std::lock_guard<std::mutex> lock(mm->mu);
+      if (operation == "apply_model") {
+        if (request.has("action") && request.at("action").as_string() != "normal")
+          raise(QMBED_UNSUPPORTED_BACKEND, "only the normal action is supported by the GPU engine");
+        return vectors_result(apply_columns(mm->view(), mm->block_ops(), parse_vectors(request.at("vectors")),
+                                            "vector length does not match the model dimension"),
+                              mm->matrix->dim());
+      }
+      if (operation == "eigsh_model") return solve_view(mm->view(), mm->block_ops(), parse_solver(request.at("solver")), true);
+      auto entry = std::make_shared<ExpmEntry>();
+      entry->matrix = mm;
+      const auto& c = request.at("coefficient").items();
+      if (c.size() != 2) raise(QMBED_INVALID_OPTIONS, "coefficient is a [re, im] pair");
+      const size_t max_degree = request.has("max_degree") ? static_cast<size_t>(request.at("max_degree").as_int()) : 55;
+      const double tolerance = request.has("tolerance") ? request.at("tolerance").as_double() : 0.5 * 2.220446049250313e-16;
+      const size_t substeps = request.has("max_substeps") ? static_cast<size_t>(request.at("max_substeps").as_int()) : 10000;
+      entry->plan = make_expm_plan(mm->matrix->dim(), mm->matrix->shift(), mm->matrix->one_norm(),
+                                   C64(c[0].as_double(), c[1].as_double()), max_degree, tolerance, substeps);
+      const uint64_t id = g_next_expm.fetch_add(1);
+      {
+        std::lock_guard<std::mutex> registry(g_registry_mu);
+        g_expm[id] = entry;
+      }
+      Value out = Value::object();
+      out.set("kind", Value::string("expm_plan"));
+      out.set("handle", Value::string(std::to_string(id)));
+      out.set("dimension", Value::integer(static_cast<long long>(mm->matrix->dim())));
+      return out;
+    }
+  }
   if (operation == "eigsh") {
     auto model = build_model(request);
     auto op = model->materialize(nullptr, parse_storage(request), true);
@@ -1178,6 +1305,11 @@ Value command(const Value& request) {
   }
   if (operation == "apply_expm_action") {
     auto entry = registered_expm(request.at("expm_handle").as_string());
+    if (entry->matrix) {
+      std::lock_guard<std::mutex> lock(entry->matrix->mu);
+      return expm_vectors(entry->matrix->view(), entry->matrix->block_ops(), entry->plan,
+                          parse_vectors(request.at("vectors")));
+    }
     return expm_vectors(*entry->op, entry->plan, parse_vectors(request.at("vectors")));
   }
   if (operation == "eigh_model") {
@@ -1484,7 +1616,8 @@ Value command(const Value& request) {
     const std::string text = request.at("handle").as_string();
     const uint64_t id = parse_handle(text, "model");
     std::lock_guard<std::mutex> lock(g_registry_mu);
-    if (!g_models.erase(id)) raise(QMBED_INVALID_OPTIONS, "model handle " + text + " is not registered");
+    if (!g_models.erase(id) && !g_matrix_models.erase(id))
+      raise(QMBED_INVALID_OPTIONS, "model handle " + text + " is not registered");
     Value out = Value::object();
     out.set("kind", Value::string("released"));
     out.set("handle", Value::string(text));

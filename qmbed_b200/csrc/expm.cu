@@ -103,11 +103,23 @@ ExpmPlan make_expm_plan(const SpinOperator& op, C64 coefficient, size_t max_degr
   if (!std::isfinite(coefficient.real()) || !std::isfinite(coefficient.imag()) || max_degree == 0 ||
       !std::isfinite(tolerance) || tolerance <= 0.0 || max_substeps == 0)
     raise(QMBED_INVALID_OPTIONS, "invalid exponential coefficient or numerical controls");
+  C64 shift;
+  double one_norm;
+  op.trace_and_one_norm(&shift, &one_norm);
+  return make_expm_plan(op.dim(), shift, one_norm, coefficient, max_degree, tolerance, max_substeps);
+}
+
+ExpmPlan make_expm_plan(uint64_t dim, C64 shift, double one_norm, C64 coefficient, size_t max_degree,
+                        double tolerance, size_t max_substeps) {
+  if (!std::isfinite(coefficient.real()) || !std::isfinite(coefficient.imag()) || max_degree == 0 ||
+      !std::isfinite(tolerance) || tolerance <= 0.0 || max_substeps == 0)
+    raise(QMBED_INVALID_OPTIONS, "invalid exponential coefficient or numerical controls");
   ExpmPlan plan;
-  plan.dim = op.dim();
+  plan.dim = dim;
   plan.coefficient = coefficient;
   plan.tolerance = tolerance;
-  op.trace_and_one_norm(&plan.shift, &plan.one_norm);
+  plan.shift = shift;
+  plan.one_norm = one_norm;
   const double scaled = std::abs(coefficient) * plan.one_norm;
   if (scaled != 0.0) {
     bool found = false;

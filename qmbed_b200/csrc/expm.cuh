@@ -21,6 +21,10 @@ struct ExpmPlan {
 ExpmPlan make_expm_plan(const SpinOperator& op, C64 coefficient, size_t max_degree, double tolerance,
                         size_t max_substeps);
 
+// The same plan from an operator's dimension, trace shift and shifted 1-norm.
+ExpmPlan make_expm_plan(uint64_t dim, C64 shift, double one_norm, C64 coefficient, size_t max_degree,
+                        double tolerance, size_t max_substeps);
+
 // In-place state <- exp(c A) state for an interleaved complex device vector
 // of the given precision (64: complex128, 32: complex64).
 // Returns the number of operator applications.

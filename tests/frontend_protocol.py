@@ -100,6 +100,7 @@ class OracleProtocol:
     def __init__(self):
         self.models = {}
         self.lanczos = {}
+        self.plans = {}
         self.next_handle = 1
 
     def expression_matrix(self, e) -> np.ndarray:
@@ -170,6 +171,33 @@ class OracleProtocol:
         if op == "describe_basis":
             b = oracle_basis(request["basis"])
             return {"kind": "basis", "dimension": len(b), "states": [str(int(x)) for x in b.states]}
+        if op == "create_operator_model":
+            m = request["static_operator"]
+            h = np.zeros(m["shape"], dtype=complex)
+            for e in m["entries"]:
+                h[e["row"], e["column"]] += complex(*e["value"])
+            handle = f"oracle-model-{self.next_handle}"
+            self.next_handle += 1
+            self.models[handle] = h
+            return {"kind": "model", "handle": handle, "dimension": h.shape[0]}
+        if op == "create_expm_action":
+            # ExpmActionPlan (src/solve/mod.rs:116-248) as restated by the C++ oracle
+            h = self.matrix(request["handle"])
+            rows, cols = np.nonzero(h)
+            operator = _oracle_module().Operator.from_triplets(h.shape[0], rows, cols, h[rows, cols])
+            handle = f"oracle-expm-{self.next_handle}"
+            self.next_handle += 1
+            self.plans[handle] = (operator, complex(*request["coefficient"]), request.get("max_degree", 55),
+                                  request.get("tolerance", 0.5 * np.finfo(float).eps))
+            return {"kind": "expm_plan", "handle": handle, "dimension": h.shape[0]}
+        if op == "apply_expm_action":
+            operator, c, degree, tolerance = self.plans[request["expm_handle"]]
+            return {"kind": "vectors", "dimension": operator.dim,
+                    "vectors": [pairs(operator.expm_apply(c, v, max_degree=degree, tolerance=tolerance))
+                                for v in complex_vectors(request["vectors"])]}
+        if op == "release_expm_action":
+            self.plans.pop(request["expm_handle"], None)
+            return {"kind": "released"}
         if op == "release_model":
             self.models.pop(request["handle"], None)
             return {"kind": "released"}

@@ -143,6 +143,31 @@ def scenarios(qmbed):
         lin_comb_Q_T(V[:, -1], Q)
         H.static
 
+    def quspin_expm_multiply_parallel():
+        """expm_multiply_parallel on -(H - E) of a zblock sector (the compat test_imag_time flow) and on a
+        random complex sparse matrix: explicit-matrix operator models and their exponential-action plans."""
+        import scipy.sparse as sp
+        from quspin.tools.evolution import expm_multiply_parallel
+        L = 12
+        basis = spin_basis_1d(L, m=0, kblock=0, pblock=1, zblock=1)
+        J = [[1.0, i, (i + 1) % L] for i in range(L)]
+        H = hamiltonian([["xx", J], ["yy", J], ["zz", J]], [], basis=basis, dtype=np.float64)
+        (E,), _ = H.eigsh(k=1, which="SA")
+        A = -(H.tocsr() - E * sp.eye(H.Ns, format="csr", dtype=np.float64))
+        U = expm_multiply_parallel(A)
+        v = rng.uniform(-1, 1, size=H.Ns)
+        v /= np.linalg.norm(v)
+        for _ in range(3):
+            v = U.dot(v)
+            v /= np.linalg.norm(v)
+        n = 120
+        B = (sp.random(n, n, density=np.log(n) / n, random_state=1)
+             + 1j * sp.random(n, n, density=np.log(n) / n, random_state=2)).tocsr()
+        w = rng.normal(0, 1, size=n) + 1j * rng.normal(0, 1, size=n)
+        w /= np.linalg.norm(w)
+        expm_multiply_parallel(B).dot(w)
+        expm_multiply_parallel(B, a=-0.01j, dtype=np.complex128).dot(w)
+
     def quspin_fixed_magnetisation():
         """spin_basis_1d(L, Nup) without lattice maps: reversed order and site permutation only."""
         L = 10
@@ -154,7 +179,7 @@ def scenarios(qmbed):
 
     return {f.__name__: f for f in (native_eigsh, quspin_real_sector, quspin_complex_sector,
                                      quspin_transverse_field, quspin_density_matrix, quspin_lanczos_tools,
-                                     quspin_fixed_magnetisation)}
+                                     quspin_expm_multiply_parallel, quspin_fixed_magnetisation)}
 
 
 def main() -> None:

@@ -7,7 +7,9 @@ send for a few ordinary user scripts (recorded by
 QuSpin ``hamiltonian`` objects on ``spin_basis_1d`` with ``kblock``/``pblock``
 lattice maps, reversed row order and the reversed site labelling, with
 ``eigsh``, ``dot``, ``expt_value``, ``quant_fluct``, ``matrix_ele``,
-``eigvalsh`` and the Krylov ``evolve``. Each request goes unchanged through
+``eigvalsh``, the Krylov ``evolve``, the Lanczos tools on a ``zblock``
+sector and ``expm_multiply_parallel`` on explicit sparse matrices. Each
+request goes unchanged through
 ``qmbed_run_json`` / ``qmbed_command_json`` of ``libqmbed_b200.so`` (model
 handles are mapped to the ones this library returned) and each answer is
 checked against the oracle's answer to the same request
@@ -75,7 +77,7 @@ def test_frontend_requests_replay(scenario):
         op = request.get("operation", "run")
         if op == "run":
             _check_eigensystem(got, expected, model_matrix(request), request["solver"])
-        elif op == "create_model":
+        elif op in ("create_model", "create_operator_model", "create_expm_action"):
             handles[expected["handle"]] = got["handle"]
             assert got["dimension"] == expected["dimension"]
         elif op == "describe_basis":
@@ -100,14 +102,14 @@ def test_frontend_requests_replay(scenario):
             a = np.array(got["vectors"], dtype=float)
             b = np.array(expected["vectors"], dtype=float)
             assert a.shape == b.shape and np.abs(a - b).max() <= 1e-10 * max(1.0, np.abs(b).max())
-        elif op in ("release_lanczos",):
+        elif op in ("release_lanczos", "release_expm_action"):
             pass
-        elif op in ("apply_model", "evolve_model"):
-            key = "vectors" if op == "apply_model" else "states"
+        elif op in ("apply_model", "evolve_model", "apply_expm_action"):
+            key = "states" if op == "evolve_model" else "vectors"
             a = np.array(got[key], dtype=float)
             b = np.array(expected[key], dtype=float)
             assert a.shape == b.shape
-            tol = 1e-12 if op == "apply_model" else 1e-8
+            tol = {"apply_model": 1e-12, "evolve_model": 1e-8, "apply_expm_action": 1e-12}[op]
             assert np.abs(a - b).max() <= tol * max(1.0, np.abs(b).max())
         elif op in ("measure_model", "matrix_elements_model"):
             assert got["kind"] == "measurements" and got["shape"] == expected["shape"]
@@ -259,3 +261,58 @@ def test_spin_flip_sectors_match_the_oracle(kblock, pblock, zblock):
             assert np.abs(y - x @ h.T).max() <= 1e-12 * max(1.0, np.abs(h).max() * h.shape[0])
         finally:
             command({"operation": "release_model", "handle": model["handle"]})
+
+
+def _matrix_request(a):
+    rows, cols = np.nonzero(a)
+    return {"shape": list(a.shape),
+            "entries": [{"row": int(r), "column": int(c), "value": [a[r, c].real, a[r, c].imag]}
+                        for r, c in zip(rows, cols)]}
+
+
+@pytest.mark.parametrize("complex_matrix", [False, True])
+def test_explicit_matrix_models_apply_solve_and_exponentiate(complex_matrix):
+    """create_operator_model with a static matrix: CSR action, eigsh and the Taylor plan against dense numpy."""
+    import scipy.linalg
+    from qmbed_b200._lib import command
+    rng = np.random.default_rng(3)
+    n = 300
+    a = np.where(rng.random((n, n)) < 0.02, rng.standard_normal((n, n)), 0.0).astype(complex)
+    if complex_matrix:
+        a += 1j * np.where(rng.random((n, n)) < 0.02, rng.standard_normal((n, n)), 0.0)
+    a = a + a.conj().T + np.diag(rng.standard_normal(n))
+    model = command({"operation": "create_operator_model", "static_operator": _matrix_request(a)})
+    try:
+        assert model["dimension"] == n
+        x = rng.standard_normal((2, n)) + 1j * rng.standard_normal((2, n))
+        got = command({"operation": "apply_model", "handle": model["handle"],
+                       "vectors": [[[v.real, v.imag] for v in col] for col in x]})
+        y = np.array([[complex(*v) for v in col] for col in got["vectors"]])
+        assert np.abs(y - x @ a.T).max() <= 1e-13 * np.abs(a).sum(axis=1).max()
+        solved = command({"operation": "eigsh_model", "handle": model["handle"],
+                          "solver": {"eigenpairs": 3, "target": {"kind": "smallest_algebraic"}, "tolerance": 1e-12}})
+        np.testing.assert_allclose(solved["eigenvalues"], np.linalg.eigvalsh(a)[:3], atol=1e-9)
+        plan = command({"operation": "create_expm_action", "handle": model["handle"], "coefficient": [0.0, -0.3]})
+        out = command({"operation": "apply_expm_action", "expm_handle": plan["handle"],
+                       "vectors": [[[v.real, v.imag] for v in x[0]]]})
+        z = np.array([complex(*v) for v in out["vectors"][0]])
+        assert np.linalg.norm(z - scipy.linalg.expm(-0.3j * a) @ x[0]) <= 1e-12 * np.linalg.norm(x[0])
+        command({"operation": "release_expm_action", "expm_handle": plan["handle"]})
+    finally:
+        command({"operation": "release_model", "handle": model["handle"]})
+
+
+def test_explicit_matrix_models_reject_bad_requests():
+    from qmbed_b200 import QmbedError
+    from qmbed_b200._lib import command
+    square = {"shape": [2, 2], "entries": [{"row": 0, "column": 1, "value": [1.0, 0.0]}]}
+    cases = [
+        ({"static_operator": {"shape": [2, 3], "entries": []}}, "^dimension mismatch"),
+        ({"static_operator": {"shape": [2, 2], "entries": [{"row": 2, "column": 0, "value": [1.0, 0.0]}]}},
+         "^dimension mismatch"),
+        ({"static_operator": square, "components": [{"name": "g", "operator": square}]}, "^unsupported backend"),
+        ({}, "^invalid options"),
+    ]
+    for request, message in cases:
+        with pytest.raises(QmbedError, match=message):
+            command({"operation": "create_operator_model", **request})
