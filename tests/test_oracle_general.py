@@ -107,3 +107,22 @@ def test_recorded_frontend_requests_are_answered_by_the_oracle():
             operations.add(call["request"].get("operation", "run"))
     assert {"run", "create_model", "eigsh_model", "apply_model", "measure_model", "matrix_elements_model",
             "eigh_model", "evolve_model", "release_model"} <= operations
+
+
+def test_reference_frontend_binds_every_symbol_of_the_library():
+    """The reference's own ctypes loader (bindings/python/src/qmbed/_ffi.py:154-186) binds all six JSON
+    symbols of libqmbed_b200.so; skipped when the frontend is not installed in baseline/_ref."""
+    import ctypes
+    import importlib.util
+    root = Path(__file__).resolve().parents[1]
+    ffi_path = root / "baseline" / "_ref" / "qmbed" / "_ffi.py"
+    library = root / "qmbed_b200" / "libqmbed_b200.so"
+    if not ffi_path.is_file() or not library.is_file():
+        pytest.skip("reference frontend or library not present")
+    spec = importlib.util.spec_from_file_location("reference_qmbed_ffi", ffi_path)
+    ffi = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(ffi)
+    lib = ffi._load_library(str(library))
+    for symbol in ("qmbed_run_json", "qmbed_command_json", "qmbed_string_free", "qmbed_evolve_model_with_drive_json",
+                   "qmbed_register_user_basis_32_json", "qmbed_register_user_basis_64_json"):
+        assert isinstance(getattr(lib, symbol), ctypes._CFuncPtr)
