@@ -1244,6 +1244,21 @@ Value command(const Value& request) {
     auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
     return operator_entries(*op, request.has("format") ? request.at("format").as_string() : "csc");
   }
+  if (operation == "materialize_component_model") {
+    // MaterializeComponentModel -> component_operator (bindings/capi/src/lib.rs:5797-5805,
+    // src/interop.rs:185-190): one named component with coefficient 1
+    auto model = registered_model(request.at("handle").as_string());
+    const std::string name = request.at("name").as_string();
+    if (model->components.empty()) raise(QMBED_INVALID_OPTIONS, "fixed operator model has no component \"" + name + "\"");
+    const Component* found = nullptr;
+    for (const Component& c : model->components)
+      if (c.name == name) found = &c;
+    if (!found) raise(QMBED_INVALID_OPTIONS, "unknown operator component \"" + name + "\"");
+    OperatorChecks checks = model->checks;
+    checks.hermiticity = false;
+    auto op = model->cached("component|" + name, found->terms, checks, kStoragePacked);
+    return operator_entries(*op, request.has("format") ? request.at("format").as_string() : "csc");
+  }
   if (operation == "evaluate_operator_expression") {
     // EvaluateOperatorExpression -> command_operator_value (bindings/capi/src/lib.rs:5660-5663)
     auto op = expression_operator(request.at("expression"), kStoragePacked);

@@ -62,13 +62,32 @@ def oracle_basis(basis) -> general.GeneralSpinBasis:
     return general.GeneralSpinBasis(sites, up, maps, reverse=bool(basis.get("reverse")))
 
 
-def model_matrix(request) -> np.ndarray:
+def model_parts(request):
+    """(static matrix, {component name: (matrix with coefficient 1, default or None)}) of a model request."""
     b = oracle_basis(request["basis"])
-    terms = oracle_terms(request["terms"])
+    norm, perm = normalization(request["basis"]), request.get("site_permutation")
+    static = general.reduced_dense(b, oracle_terms(request["terms"]), norm, perm)
+    components = {}
     for c in request.get("components") or []:
-        value = complex(*c["default"]) if c.get("default") is not None else 0.0
-        terms += [(s, [(value * k, sites) for k, sites in cs]) for s, cs in oracle_terms(c["terms"])]
-    return general.reduced_dense(b, terms, normalization(request["basis"]), request.get("site_permutation"))
+        default = complex(*c["default"]) if c.get("default") is not None else None
+        components[c["name"]] = (general.reduced_dense(b, oracle_terms(c["terms"]), norm, perm), default)
+    return static, components
+
+
+def evaluate(parts, parameters=None) -> np.ndarray:
+    """The model at the given parameter values (defaults for the rest), like EdModel::materialize."""
+    static, components = parts
+    h = static.copy()
+    for name, (matrix, default) in components.items():
+        value = complex(*parameters[name]) if parameters and name in parameters else default
+        if value is None:
+            raise ValueError(f"operator parameter {name!r} has no default and was not supplied")
+        h = h + value * matrix
+    return h
+
+
+def model_matrix(request) -> np.ndarray:
+    return evaluate(model_parts(request))
 
 
 def complex_vectors(vectors):
@@ -107,9 +126,9 @@ class OracleProtocol:
         """OperatorExpressionRequest (bindings/capi/src/lib.rs:789-818) for models without parameters."""
         kind = e["kind"]
         if kind == "model":
-            if e.get("action", "normal") != "normal" or e.get("parameters"):
-                raise NotImplementedError("model expression with an action or parameters")
-            return self.models[e["handle"]]
+            if e.get("action", "normal") != "normal":
+                raise NotImplementedError("model expression with an action")
+            return self.matrix(e["handle"], e.get("parameters"))
         if kind == "scale":
             return complex(*e["coefficient"]) * self.expression_matrix(e["operand"])
         if kind == "binary":
@@ -145,8 +164,16 @@ class OracleProtocol:
             raise NotImplementedError(op)
         return {"kind": "vectors", "dimension": d["basis"].shape[1], "vectors": [pairs(c @ d["basis"])]}
 
-    def matrix(self, handle) -> np.ndarray:
-        return self.models[handle]
+    def matrix(self, handle, parameters=None) -> np.ndarray:
+        model = self.models[handle]
+        return evaluate(model, parameters) if isinstance(model, tuple) else model
+
+    @staticmethod
+    def entries(h, format):
+        rows, cols = np.nonzero(h)
+        return {"kind": "operator", "shape": list(h.shape), "format": format,
+                "entries": [{"row": int(r), "column": int(c), "value": pairs([h[r, c]])[0]}
+                            for r, c in zip(rows, cols)]}
 
     def eigensystem(self, h, solver):
         values, vectors = np.linalg.eigh(h)
@@ -166,8 +193,8 @@ class OracleProtocol:
         if op == "create_model":
             handle = f"oracle-model-{self.next_handle}"
             self.next_handle += 1
-            self.models[handle] = model_matrix(request)
-            return {"kind": "model", "handle": handle, "dimension": self.models[handle].shape[0]}
+            self.models[handle] = model_parts(request)
+            return {"kind": "model", "handle": handle, "dimension": self.models[handle][0].shape[0]}
         if op == "describe_basis":
             b = oracle_basis(request["basis"])
             return {"kind": "basis", "dimension": len(b), "states": [str(int(x)) for x in b.states]}
@@ -211,13 +238,13 @@ class OracleProtocol:
             return {"kind": "vectors", "dimension": h.shape[0],
                     "vectors": [pairs(h @ v) for v in complex_vectors(request["vectors"])]}
         if op in ("materialize_model", "evaluate_operator_expression"):
-            h = self.matrix(request["handle"]) if op == "materialize_model" else \
+            h = self.matrix(request["handle"], request.get("parameters")) if op == "materialize_model" else \
                 self.expression_matrix(request["expression"])
-            rows, cols = np.nonzero(h)
-            return {"kind": "operator", "shape": list(h.shape), "format": request.get("format", "csc"),
-                    "entries": [{"row": int(r), "column": int(c), "value": pairs([h[r, c]])[0]}
-                                for r, c in zip(rows, cols)]}
-        h = self.matrix(request["handle"])
+            return self.entries(h, request.get("format", "csc"))
+        if op == "materialize_component_model":
+            matrix, _ = self.models[request["handle"]][1][request["name"]]
+            return self.entries(matrix, request.get("format", "csc"))
+        h = self.matrix(request["handle"], request.get("parameters"))
         if op == "eigsh_model":
             return {"kind": "eigensystem", **self.eigensystem(h, request["solver"])}
         if op == "apply_model":

@@ -168,6 +168,20 @@ def scenarios(qmbed):
         expm_multiply_parallel(B).dot(w)
         expm_multiply_parallel(B, a=-0.01j, dtype=np.complex128).dot(w)
 
+    def quspin_driven_hamiltonian():
+        """A driven chain: the dynamic term becomes a named component; dot, eigsh and the matrix at given times."""
+        L = 10
+        basis = spin_basis_1d(L, Nup=5, kblock=0, pblock=1, pauli=False)
+
+        def drive(t, omega):
+            return np.cos(omega * t)
+
+        dynamic = [["zz", [[0.4, i, (i + 2) % L] for i in range(L)], drive, [2.0]]]
+        H = hamiltonian(heisenberg_static(L, 1.0), dynamic, basis=basis, dtype=np.float64)
+        H.dot(rng.standard_normal(H.Ns), time=0.3)
+        H.eigsh(k=2, which="SA", time=0.7)
+        H.tocsr(time=1.1)
+
     def quspin_fixed_magnetisation():
         """spin_basis_1d(L, Nup) without lattice maps: reversed order and site permutation only."""
         L = 10
@@ -179,7 +193,8 @@ def scenarios(qmbed):
 
     return {f.__name__: f for f in (native_eigsh, quspin_real_sector, quspin_complex_sector,
                                      quspin_transverse_field, quspin_density_matrix, quspin_lanczos_tools,
-                                     quspin_expm_multiply_parallel, quspin_fixed_magnetisation)}
+                                     quspin_expm_multiply_parallel, quspin_driven_hamiltonian,
+                                     quspin_fixed_magnetisation)}
 
 
 def main() -> None:

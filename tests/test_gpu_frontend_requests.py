@@ -83,7 +83,8 @@ def test_frontend_requests_replay(scenario):
         elif op == "describe_basis":
             assert got["dimension"] == expected["dimension"] and got["states"] == expected["states"]
         elif op == "eigsh_model":
-            _check_eigensystem(got, expected, oracle.matrix(request["handle"]), request["solver"])
+            _check_eigensystem(got, expected, oracle.matrix(request["handle"], request.get("parameters")),
+                               request["solver"])
         elif op == "eigsh_operator_expression":
             _check_eigensystem(got, expected, oracle.expression_matrix(request["expression"]), request["solver"])
         elif op == "lanczos_operator":
@@ -95,7 +96,7 @@ def test_frontend_requests_replay(scenario):
             for a, b in zip(got["eigenvectors"], expected["eigenvectors"]):  # columns up to sign
                 a, b = np.array(a), np.array(b)
                 assert min(np.abs(a - b).max(), np.abs(a + b).max()) <= 1e-8
-        elif op in ("materialize_model", "evaluate_operator_expression"):
+        elif op in ("materialize_model", "evaluate_operator_expression", "materialize_component_model"):
             assert got["shape"] == expected["shape"]
             assert np.abs(_dense(got) - _dense(expected)).max() <= 1e-12 * max(1.0, np.abs(_dense(expected)).max())
         elif op in ("lanczos_combine", "lanczos_exponential"):
