@@ -392,8 +392,11 @@ QMBED_API char* qmbed_run_json(const char* request);
 QMBED_API char* qmbed_command_json(const char* request);
 /* qmbed_string_free (bindings/capi/src/lib.rs:6290-6296) */
 QMBED_API void qmbed_string_free(char* response);
-/* qmbed_evolve_model_with_drive_json (bindings/capi/src/lib.rs:6153-6190):
- * present for load-time binding; answers an unsupported-backend error. */
+/* qmbed_evolve_model_with_drive_json (bindings/capi/src/lib.rs:6153-6190,
+ * 2206-2225, 4695-4746): evolves a registered model's columns under
+ * H(t) = H_0 + sum_j c_j(t) H_j with adaptive RK4 step doubling on the GPU;
+ * `callback` is int (*)(void* context, double time, {double re, im}* c,
+ * size_t count), called at every internal time, 0 on success. */
 QMBED_API char* qmbed_evolve_model_with_drive_json(const char* request, void* callback, void* context);
 /* qmbed_register_user_basis_{32,64}_json (bindings/capi/src/lib.rs:6192-6282):
  * present for load-time binding; answer an unsupported-backend error. */

@@ -1651,7 +1651,8 @@ Value command(const Value& request) {
   raise(QMBED_UNSUPPORTED_BACKEND, "operation `" + operation + "` is outside the GPU engine");
 }
 
-std::string respond(const char* request, bool command_api) {
+std::string respond_with(const char* request, const std::string& invalid,
+                         const std::function<Value(const Value&)>& handler) {
   if (!request) return R"({"status":"error","error":"request pointer is null"})";
   Value response = Value::object();
   try {
@@ -1659,13 +1660,13 @@ std::string respond(const char* request, bool command_api) {
     try {
       parsed = json::parse(request);
     } catch (const json::ParseError& e) {
-      raise(QMBED_INVALID_OPTIONS, std::string(command_api ? "invalid binding command: " : "invalid binding request: ") + e.what());
+      raise(QMBED_INVALID_OPTIONS, invalid + e.what());
     }
     Value result;
     try {
-      result = command_api ? command(parsed) : run_request(parsed);
+      result = handler(parsed);
     } catch (const json::ParseError& e) {
-      raise(QMBED_INVALID_OPTIONS, std::string(command_api ? "invalid binding command: " : "invalid binding request: ") + e.what());
+      raise(QMBED_INVALID_OPTIONS, invalid + e.what());
     }
     response.set("status", Value::string("ok"));
     response.set("result", std::move(result));
@@ -1679,6 +1680,122 @@ std::string respond(const char* request, bool command_api) {
     response.set("error", Value::string(std::string("internal state error: ") + e.what()));
   }
   return response.dump();
+}
+
+std::string respond(const char* request, bool command_api) {
+  return respond_with(request, command_api ? "invalid binding command: " : "invalid binding request: ",
+                      [command_api](const Value& r) { return command_api ? command(r) : run_request(r); });
+}
+
+// QmbedComplex64 and the drive callback of qmbed_evolve_model_with_drive_json
+// (bindings/capi/src/lib.rs:452-470): fill `count` coefficients at `time`,
+// return 0 on success.
+struct DriveComplex {
+  double real, imaginary;
+};
+using DriveCallbackFn = int (*)(void*, double, DriveComplex*, size_t);
+
+std::string debug_names(const std::vector<std::string>& names) {
+  std::string out = "[";
+  for (size_t i = 0; i < names.size(); ++i) out += (i ? ", \"" : "\"") + names[i] + "\"";
+  return out + "]";
+}
+
+Value drive_evolution(const Value& request, void* callback, void* context) {
+  auto model = registered_model(request.at("handle").as_string());
+  std::vector<std::string> names, expected;
+  for (const Value& v : request.at("component_names").items()) names.push_back(v.as_string());
+  for (const Component& c : model->components) expected.push_back(c.name);
+  if (names != expected)
+    raise(QMBED_INVALID_OPTIONS, "drive component order mismatch: expected " + debug_names(expected) + ", received " +
+                                     debug_names(names));
+  if (expected.empty()) raise(QMBED_INVALID_OPTIONS, "time-dependent evolution requires at least one operator component");
+  const Value& ev = request.at("evolution");
+  EvolutionOptions o;
+  for (const Value& t : ev.at("times").items()) o.times.push_back(t.as_double());
+  o.krylov_dimension = ev.has("krylov_dimension") ? static_cast<size_t>(ev.at("krylov_dimension").as_int()) : 64;
+  o.tolerance = ev.has("tolerance") ? ev.at("tolerance").as_double() : 1.0e-10;
+  o.max_substeps = ev.has("max_substeps") ? static_cast<size_t>(ev.at("max_substeps").as_int()) : 10000;
+  const bool imaginary = ev.has("imaginary_time") && ev.at("imaginary_time").as_bool();
+  const double initial_time = request.at("initial_time").as_double();
+  const auto vectors = parse_vectors(request.at("vectors"));
+  if (vectors.empty()) raise(QMBED_INVALID_OPTIONS, "a state batch must contain at least one column");
+
+  OperatorChecks checks = model->checks;
+  checks.hermiticity = false;
+  std::vector<std::shared_ptr<qmbed_operator_s>> parts;
+  parts.push_back(model->terms.empty() ? nullptr : model->cached("static", model->terms, checks, kStoragePacked));
+  for (const Component& c : model->components)
+    parts.push_back(model->cached("component|" + c.name, c.terms, checks, kStoragePacked));
+  std::vector<std::unique_lock<std::mutex>> locks;
+  for (auto& part : parts)
+    if (part) locks.emplace_back(part->mu);
+  qmbed_operator_s& first = parts[0] ? *parts[0] : *parts[1];
+  BlockOps& ops = first.block_ops();
+  const cudaStream_t stream = ops.stream();
+  const uint64_t dim = first.op->dim();
+
+  TimeDependentOperator td;
+  td.dim = dim;
+  for (auto& part : parts) {
+    if (!part) {  // no static terms: the zero operator
+      td.parts.push_back(LinearOperatorView{dim, true, [stream, dim](int, bool cplx, const void*, void* y) {
+                                              QMBED_CUDA(cudaMemsetAsync(y, 0, dim * (cplx ? 16 : 8), stream));
+                                            }});
+      continue;
+    }
+    SpinOperator* raw = part->op.get();
+    td.parts.push_back(LinearOperatorView{dim, raw->is_real(), [raw, stream](int prec, bool cplx, const void* x, void* y) {
+                                            raw->apply(prec, cplx, x, y, stream);
+                                          }});
+  }
+  auto fn = reinterpret_cast<DriveCallbackFn>(callback);
+  td.coefficients = [fn, context](double t, std::vector<C64>& c) {
+    std::vector<DriveComplex> buffer(c.size(), DriveComplex{std::nan(""), std::nan("")});
+    const int status = fn(context, t, buffer.data(), buffer.size());
+    if (status != 0) {
+      char text[64];
+      std::snprintf(text, sizeof(text), "%.17g", t);
+      raise(QMBED_INVALID_OPTIONS, "drive callback returned status " + std::to_string(status) + " at time " + text);
+    }
+    for (size_t i = 0; i < c.size(); ++i) c[i] = C64(buffer[i].real, buffer[i].imaginary);
+  };
+  td.scale = imaginary ? C64(0.0, -1.0) : C64(1.0, 0.0);
+
+  std::vector<std::vector<double>> per_column;
+  for (const auto& v : vectors) {
+    if (v.size() != dim) raise(QMBED_DIMENSION_MISMATCH, "time-dependent operator and initial state do not match");
+    std::vector<double> host(2 * dim), states(2 * dim * o.times.size());
+    for (uint64_t i = 0; i < dim; ++i) {
+      host[2 * i] = v[i].real();
+      host[2 * i + 1] = v[i].imag();
+    }
+    evolve_time_dependent(td, host.data(), initial_time, o, states.data(), ops);
+    per_column.push_back(std::move(states));
+  }
+  Value out = Value::object();
+  out.set("kind", Value::string("trajectory"));
+  out.set("dimension", Value::integer(static_cast<long long>(dim)));
+  Value times = Value::array();
+  for (double t : o.times) times.push(Value::number(t));
+  out.set("times", std::move(times));
+  Value states = Value::array();
+  for (size_t t = 0; t < o.times.size(); ++t) {
+    Value columns = Value::array();
+    for (const auto& col : per_column) {
+      Value r = Value::array();
+      for (uint64_t i = 0; i < dim; ++i) r.push(complex_pair(C64(col[2 * (t * dim + i)], col[2 * (t * dim + i) + 1])));
+      columns.push(std::move(r));
+    }
+    states.push(std::move(columns));
+  }
+  out.set("states", std::move(states));
+  return out;
+}
+
+template <typename F>
+char* json_call(const char* request, F handler) {
+  return to_c_string(respond_with(request, "invalid drive evolution request: ", handler));
 }
 
 }  // namespace
@@ -2401,11 +2518,13 @@ char* qmbed_command_json(const char* request) { return to_c_string(respond(reque
 
 void qmbed_string_free(char* response) { std::free(response); }
 
+// run_drive_evolution_json / execute_drive_evolution (bindings/capi/src/lib.rs:2206-2225, 4695-4746):
+// the model's static part and components, coefficients from the caller's
+// callback at every internal time, the adaptive RK4 of evolve_time_dependent.
 char* qmbed_evolve_model_with_drive_json(const char* request, void* callback, void* context) {
-  (void)request;
-  (void)callback;
-  (void)context;
-  return to_c_string(R"({"status":"error","error":"unsupported backend: driven evolution is outside the GPU engine"})");
+  if (!request) return to_c_string(R"({"status":"error","error":"request pointer is null"})");
+  if (!callback) return to_c_string(R"({"status":"error","error":"drive callback is null"})");
+  return json_call(request, [callback, context](const Value& r) { return drive_evolution(r, callback, context); });
 }
 
 char* qmbed_register_user_basis_32_json(const char* request, void* op, void* next_state, void* pre_check, void* maps,

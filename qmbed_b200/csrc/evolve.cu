@@ -328,4 +328,90 @@ void expm_lanczos(const LinearOperatorView& op, const double* initial, double ti
   ops.sync();
 }
 
+void evolve_time_dependent(const TimeDependentOperator& op, const double* initial, double initial_time,
+                           const EvolutionOptions& o, double* states, BlockOps& ops) {
+  validate_evolution(o);
+  if (!std::isfinite(initial_time) || o.times[0] < initial_time)
+    raise(QMBED_INVALID_OPTIONS, "initial time must be finite and no later than the first output time");
+  if (op.parts.empty()) raise(QMBED_INVALID_OPTIONS, "time-dependent evolution requires a static part");
+  const uint64_t n = op.dim;
+  const cudaStream_t s = ops.stream();
+  const size_t parts = op.parts.size();
+  const size_t column = std::max<uint64_t>(n, 1) * 16;
+  // columns: rk block [in, k1, k2, k3, k4]; x; part outputs; state; [full, two]; half; error
+  DeviceBuffer rk(5 * column), x(column), outputs(parts * column), state(column), pair(2 * column), half(column),
+      error(column);
+  auto col = [&](const DeviceBuffer& b, size_t j) { return b.as<double>() + 2 * std::max<uint64_t>(n, 1) * j; };
+  const uint64_t ld = std::max<uint64_t>(n, 1);
+  std::vector<C64> c(parts - 1), weights(parts);
+  // derivative -i H(t) x into `out`
+  auto derivative = [&](double t, const double* in, double* out) {
+    c.assign(parts - 1, C64(std::nan(""), std::nan("")));
+    op.coefficients(t, c);
+    for (const C64& v : c)
+      if (!std::isfinite(v.real()) || !std::isfinite(v.imag()))
+        raise(QMBED_INVALID_OPTIONS, "time-dependent coefficient callback did not return " + std::to_string(c.size()) +
+                                         " finite values");
+    for (size_t j = 0; j < parts; ++j) op.parts[j].apply(64, true, in, col(outputs, j));
+    const C64 factor = C64(0.0, -1.0) * op.scale;
+    weights[0] = factor;
+    for (size_t j = 1; j < parts; ++j) weights[j] = factor * c[j - 1];
+    ops.combine(outputs.get(), ld, static_cast<int>(parts), weights.data(), 1, out, ld, n, 64, true);
+  };
+  auto rk4 = [&](double t, const double* in, double h, double* out) {
+    ops.copy(in, col(rk, 0), n * 16);
+    derivative(t, col(rk, 0), col(rk, 1));
+    const C64 stages[3][4] = {{1.0, 0.5 * h, 0.0, 0.0}, {1.0, 0.0, 0.5 * h, 0.0}, {1.0, 0.0, 0.0, h}};
+    const double times[3] = {t + 0.5 * h, t + 0.5 * h, t + h};
+    for (int k = 0; k < 3; ++k) {
+      ops.combine(rk.get(), ld, k + 2, stages[k], 1, x.get(), ld, n, 64, true);
+      derivative(times[k], x.as<double>(), col(rk, k + 2));
+    }
+    const C64 final_weights[5] = {1.0, h / 6.0, h / 3.0, h / 3.0, h / 6.0};
+    ops.combine(rk.get(), ld, 5, final_weights, 1, out, ld, n, 64, true);
+  };
+  QMBED_CUDA(cudaMemcpyAsync(state.get(), initial, n * 16, cudaMemcpyHostToDevice, s));
+  const double requested_norm = ops.norm(state.get(), n, 64, true);
+  double previous = initial_time;
+  for (size_t output = 0; output < o.times.size(); ++output) {
+    const double target = o.times[output];
+    const double interval = target - previous;
+    if (interval != 0.0) {
+      const double direction = interval > 0.0 ? 1.0 : -1.0;
+      double h = direction * std::min(std::fabs(interval), 0.1);
+      double t = previous;
+      size_t steps = 0;
+      const double interval_scale = std::max(std::fabs(interval), 1.0);
+      while (direction * (target - t) > 16.0 * kEps * std::max(std::fabs(target), 1.0)) {
+        if (steps >= o.max_substeps) raise_nonconvergence(steps, std::fabs(target - t));
+        if (direction * (t + h - target) > 0.0) h = target - t;
+        rk4(t, state.as<double>(), h, col(pair, 0));
+        rk4(t, state.as<double>(), 0.5 * h, half.as<double>());
+        rk4(t + 0.5 * h, half.as<double>(), 0.5 * h, col(pair, 1));
+        const C64 difference[2] = {1.0, -1.0};
+        ops.combine(pair.get(), ld, 2, difference, 1, error.get(), ld, n, 64, true);
+        const double err = ops.norm(error.get(), n, 64, true);
+        const double scale = std::max(ops.norm(col(pair, 1), n, 64, true), 1.0);
+        const double threshold = o.tolerance * scale * std::clamp(std::fabs(h) / interval_scale, kEps, 1.0);
+        if (err <= threshold || std::fabs(h) <= kEps * std::max(std::fabs(t), 1.0)) {
+          ops.copy(col(pair, 1), state.get(), n * 16);
+          t += h;
+          ++steps;
+          h *= err <= kEps ? 2.0 : std::clamp(0.9 * std::pow(threshold / err, 0.2), 1.0, 2.0);
+        } else {
+          h *= std::clamp(0.9 * std::pow(threshold / err, 0.2), 0.1, 0.8);
+        }
+      }
+    }
+    if (requested_norm > kEps) {
+      const double norm = ops.norm(state.get(), n, 64, true);
+      if (norm <= kEps || !std::isfinite(norm)) raise_nonconvergence(o.max_substeps, norm);
+      ops.scale(state.get(), n, norm / requested_norm, 64, true);  // divides by its argument
+    }
+    QMBED_CUDA(cudaMemcpyAsync(states + 2 * output * n, state.get(), n * 16, cudaMemcpyDeviceToHost, s));
+    previous = target;
+  }
+  ops.sync();
+}
+
 }  // namespace qmbed

@@ -3,6 +3,7 @@
 // reference evolve.
 #pragma once
 
+#include <functional>
 #include <vector>
 
 #include "eigsh.cuh"
@@ -35,6 +36,25 @@ void validate_evolution(const EvolutionOptions& o);
 // at times[t] is written to states + 2 * t * op.dim (host, interleaved).
 void evolve(const LinearOperatorView& op, const double* initial, const EvolutionOptions& o, double* states,
             EvolutionDiagnostics& diagnostics, BlockOps& ops);
+
+// A time-dependent operator H(t) = scale * (A_0 + sum_j c_j(t) A_{j+1}):
+// `parts` act on the integrator's stream; `coefficients(t, c)` fills the
+// c_j (the reference's apply_coefficients / time_operator_scaled,
+// src/interop.rs:477-551).
+struct TimeDependentOperator {
+  uint64_t dim = 0;
+  std::vector<LinearOperatorView> parts;  // static part first, then one per component
+  std::function<void(double, std::vector<C64>&)> coefficients;
+  C64 scale{1.0, 0.0};
+};
+
+// evolve_time_dependent_from (src/solve/mod.rs:4086-4138) with
+// hamiltonian = true: adaptive RK4 with step doubling between output times
+// (adaptive_time_interval, 3998-4066; rk4_step, 3960-3996; derivative
+// -i H(t) x, 3941-3958), the state rescaled to the initial norm at every
+// output time. Host vectors as in `evolve`.
+void evolve_time_dependent(const TimeDependentOperator& op, const double* initial, double initial_time,
+                           const EvolutionOptions& o, double* states, BlockOps& ops);
 
 // expm_lanczos (src/solve/mod.rs:3432-3454): one projection of dimension
 // `krylov`, host vectors in and out (interleaved complex).

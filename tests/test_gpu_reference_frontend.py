@@ -117,3 +117,27 @@ def test_random_sparse_matrices(quspin, seed):
     np.testing.assert_allclose(got, expm_multiply(A, v), rtol=0, atol=1e-15)
     got = quspin.tools.evolution.expm_multiply_parallel(A, a=-0.01j, dtype=np.complex128).dot(v)
     np.testing.assert_allclose(got, expm_multiply(-0.01j * A, v), rtol=0, atol=1e-15)
+
+
+def test_driven_evolution_through_the_drive_callback(quspin):
+    """hamiltonian.evolve(solver_name="qmbed") with a dynamic term calls qmbed_evolve_model_with_drive_json with
+    the frontend's own coefficient callback; it must agree with the frontend's SciPy integration, which
+    applies the same model through apply_model at every right-hand-side evaluation."""
+    L = 10
+    basis = quspin.basis.spin_basis_1d(L, Nup=L // 2, kblock=0, pblock=1, pauli=False)
+    bonds = [[1.0, i, (i + 1) % L] for i in range(L)]
+
+    def drive(t, omega):
+        return np.cos(omega * t)
+
+    dynamic = [["zz", [[0.4, i, (i + 2) % L] for i in range(L)], drive, [2.0]]]
+    H = quspin.operators.hamiltonian([[op, bonds] for op in ("xx", "yy", "zz")], dynamic, basis=basis,
+                                     dtype=np.float64)
+    rng = np.random.default_rng(2)
+    psi = rng.standard_normal(H.Ns) + 1j * rng.standard_normal(H.Ns)
+    psi /= np.linalg.norm(psi)
+    times = np.array([0.5, 1.0, 1.5])
+    ours = H.evolve(psi, 0.0, times, solver_name="qmbed")
+    scipy_path = H.evolve(psi, 0.0, times, atol=1e-12, rtol=1e-12)
+    assert ours.shape == scipy_path.shape
+    assert np.abs(ours - scipy_path).max() <= 1e-8
