@@ -64,9 +64,18 @@ def test_malformed_requests_are_errors_not_crashes(library):
     library.qmbed_string_free(pointer)
 
 
-def test_placeholder_exports_answer_unsupported(library):
+def test_callback_exports_validate_their_arguments(library):
+    """Null pointers give the reference's fixed errors (bindings/capi/src/lib.rs:6159-6165); user bases are
+    outside the engine."""
     library.qmbed_evolve_model_with_drive_json.restype = ctypes.c_void_p
     pointer = library.qmbed_evolve_model_with_drive_json(b"{}", None, None)
+    assert b"drive callback is null" in ctypes.string_at(pointer)
+    library.qmbed_string_free(pointer)
+    pointer = library.qmbed_evolve_model_with_drive_json(None, None, None)
+    assert b"request pointer is null" in ctypes.string_at(pointer)
+    library.qmbed_string_free(pointer)
+    library.qmbed_register_user_basis_32_json.restype = ctypes.c_void_p
+    pointer = library.qmbed_register_user_basis_32_json(b"{}", None, None, None, None, 0)
     assert b"unsupported backend" in ctypes.string_at(pointer)
     library.qmbed_string_free(pointer)
 
