@@ -603,6 +603,43 @@ std::shared_ptr<qmbed_operator_s> make_operator(std::shared_ptr<SpinBasis> basis
   return h;
 }
 
+// The adjoint of local products: each product reversed with S+ <-> S- and the
+// coupling sites in the same reversed order, coefficients conjugated
+// (z, x, y and the identity are Hermitian).
+std::vector<TermDesc> adjoint_terms(const std::vector<TermDesc>& terms) {
+  std::vector<TermDesc> out;
+  for (const TermDesc& t : terms) {
+    TermDesc a;
+    a.symbols.assign(t.symbols.rbegin(), t.symbols.rend());
+    for (char& c : a.symbols) c = c == '+' ? '-' : (c == '-' ? '+' : c);
+    for (const CouplingDesc& coupling : t.couplings) {
+      CouplingDesc d;
+      d.coefficient = std::conj(coupling.coefficient);
+      d.sites.assign(coupling.sites.rbegin(), coupling.sites.rend());
+      a.couplings.push_back(std::move(d));
+    }
+    out.push_back(std::move(a));
+  }
+  return out;
+}
+
+// OperatorActionRequest (bindings/capi/src/lib.rs:937-945). Conjugate and
+// transpose are applied as conj(H conj(x)) and conj(H^dagger conj(x)).
+enum class Action { kNormal, kTranspose, kConjugate, kAdjoint };
+
+Action parse_action(const Value& owner) {
+  if (!owner.has("action")) return Action::kNormal;
+  const std::string a = owner.at("action").as_string();
+  if (a == "normal") return Action::kNormal;
+  if (a == "transpose") return Action::kTranspose;
+  if (a == "conjugate") return Action::kConjugate;
+  if (a == "adjoint") return Action::kAdjoint;
+  raise(QMBED_INVALID_OPTIONS, "unknown operator action `" + a + "`");
+}
+
+bool uses_adjoint(Action a) { return a == Action::kTranspose || a == Action::kAdjoint; }
+bool conjugates(Action a) { return a == Action::kTranspose || a == Action::kConjugate; }
+
 struct Component {
   std::string name;
   std::vector<TermDesc> terms;
@@ -660,6 +697,16 @@ struct Model {
     auto op = make_operator(basis, all, c, storage);
     cache[key] = op;
     return op;
+  }
+
+  // H (normal, conjugate) or H^dagger (adjoint, transpose) at the parameters
+  std::shared_ptr<qmbed_operator_s> materialize_action(const Value* parameters, int storage, Action action) {
+    if (!uses_adjoint(action)) return materialize(parameters, storage, false);
+    std::string key = "adjoint|" + std::to_string(storage);
+    const std::vector<TermDesc> all = adjoint_terms(resolved_terms(parameters, key));
+    OperatorChecks c = checks;
+    c.hermiticity = false;
+    return cached(key, all, c, storage);
   }
 
   std::shared_ptr<qmbed_operator_s> materialize(const Value* parameters, int storage, bool hermitian_check) {
@@ -869,6 +916,17 @@ Value apply_vectors(qmbed_operator_s& handle, const std::vector<std::vector<C64>
   return vectors_result(applied, handle.op->dim());
 }
 
+// A x, or conj(A conj(x)) for the conjugating actions.
+Value apply_with_action(qmbed_operator_s& handle, std::vector<std::vector<C64>> vectors, bool conjugate) {
+  if (!conjugate) return apply_vectors(handle, vectors);
+  for (auto& v : vectors)
+    for (C64& x : v) x = std::conj(x);
+  auto applied = apply_columns(handle, vectors, "vector length does not match the model dimension");
+  for (auto& v : applied)
+    for (C64& x : v) x = std::conj(x);
+  return vectors_result(applied, handle.op->dim());
+}
+
 // inner (src/measure/mod.rs:68-73): conjugate-linear in the left argument
 C64 inner(const std::vector<C64>& left, const std::vector<C64>& right) {
   C64 sum(0.0, 0.0);
@@ -1014,28 +1072,44 @@ struct ExpressionPart {
   std::shared_ptr<Model> model;
   const Value* parameters;
   C64 coefficient;
+  Action action;
 };
 
-void flatten_expression(const Value& e, C64 scale, std::vector<ExpressionPart>& parts) {
+Action compose(Action a, Action b) {  // actions as (adjoint, conjugate) bits; composition is XOR
+  const bool adj = uses_adjoint(a) != uses_adjoint(b), conj = conjugates(a) != conjugates(b);
+  if (adj && conj) return Action::kTranspose;
+  if (adj) return Action::kAdjoint;
+  return conj ? Action::kConjugate : Action::kNormal;
+}
+
+// `outer` is the action applied to this subexpression. Adjoints are taken term
+// by term, so they conjugate scale coefficients; the conjugating actions are
+// applied to the whole result by the caller (conj(c A) keeps c inside).
+void flatten_expression(const Value& e, C64 scale, std::vector<ExpressionPart>& parts, Action outer = Action::kNormal) {
   const std::string kind = e.at("kind").as_string();
   if (kind == "model") {
-    if (e.has("action") && e.at("action").as_string() != "normal")
-      raise(QMBED_UNSUPPORTED_BACKEND, "only the normal action is supported by the GPU engine");
-    parts.push_back({registered_model(e.at("handle").as_string()), e.find("parameters"), scale});
+    parts.push_back({registered_model(e.at("handle").as_string()), e.find("parameters"), scale,
+                     compose(outer, parse_action(e))});
+    return;
+  }
+  if (kind == "transform") {
+    flatten_expression(e.at("operand"), scale, parts, compose(outer, parse_action(e)));
     return;
   }
   if (kind == "scale") {
     const auto& c = e.at("coefficient").items();
     if (c.size() != 2) raise(QMBED_INVALID_OPTIONS, "coefficients are [re, im] pairs");
-    flatten_expression(e.at("operand"), scale * C64(c[0].as_double(), c[1].as_double()), parts);
+    C64 coefficient(c[0].as_double(), c[1].as_double());
+    if (uses_adjoint(outer)) coefficient = std::conj(coefficient);
+    flatten_expression(e.at("operand"), scale * coefficient, parts, outer);
     return;
   }
   if (kind == "binary") {
     const std::string op = e.at("operation").as_string();
     if (op != "add" && op != "subtract")
       raise(QMBED_UNSUPPORTED_BACKEND, "operator products are outside the GPU engine");
-    flatten_expression(e.at("left"), scale, parts);
-    flatten_expression(e.at("right"), op == "add" ? scale : -scale, parts);
+    flatten_expression(e.at("left"), scale, parts, outer);
+    flatten_expression(e.at("right"), op == "add" ? scale : -scale, parts, outer);
     return;
   }
   raise(QMBED_UNSUPPORTED_BACKEND, "operator expressions of kind `" + kind + "` are outside the GPU engine");
@@ -1049,11 +1123,24 @@ bool same_space(const Model& a, const Model& b) {
          a.convention.same_sites(b.convention) && a.convention.flipped == b.convention.flipped;
 }
 
-std::shared_ptr<qmbed_operator_s> expression_operator(const Value& e, int storage = kStoragePacked) {
+// The operator of a linear expression. Adjoints are built from adjoint
+// terms; a conjugating action (conjugate, transpose) is returned through
+// `conjugate` for the caller to apply as conj(A conj(x)) or to conjugate
+// entries, and is refused when the caller cannot (`conjugate` null) or when
+// parts disagree on it.
+std::shared_ptr<qmbed_operator_s> expression_operator(const Value& e, int storage = kStoragePacked,
+                                                      bool* conjugate = nullptr) {
   std::vector<ExpressionPart> parts;
   flatten_expression(e, C64(1.0, 0.0), parts);
+  const bool conj = conjugates(parts[0].action);
+  for (const ExpressionPart& part : parts)
+    if (conjugates(part.action) != conj)
+      raise(QMBED_UNSUPPORTED_BACKEND, "sums of conjugated and plain operators are outside the GPU engine");
+  if (conj && !conjugate)
+    raise(QMBED_UNSUPPORTED_BACKEND, "conjugate and transpose actions are applied or evaluated only");
+  if (conjugate) *conjugate = conj;
   if (parts.size() == 1 && parts[0].coefficient == C64(1.0, 0.0))
-    return parts[0].model->materialize(parts[0].parameters, storage, false);
+    return parts[0].model->materialize_action(parts[0].parameters, storage, parts[0].action);
   Model& first = *parts[0].model;
   std::string key = "expression|" + std::to_string(storage);
   std::vector<TermDesc> all;
@@ -1061,10 +1148,12 @@ std::shared_ptr<qmbed_operator_s> expression_operator(const Value& e, int storag
     if (!same_space(first, *part.model))
       raise(QMBED_DIMENSION_MISMATCH, "operator expression terms act on different spaces");
     char buffer[160];
-    std::snprintf(buffer, sizeof(buffer), "|%llu*%.17g,%.17g", static_cast<unsigned long long>(part.model->id),
-                  part.coefficient.real(), part.coefficient.imag());
+    std::snprintf(buffer, sizeof(buffer), "|%llu%s*%.17g,%.17g", static_cast<unsigned long long>(part.model->id),
+                  uses_adjoint(part.action) ? "^" : "", part.coefficient.real(), part.coefficient.imag());
     key += buffer;
-    for (TermDesc t : part.model->resolved_terms(part.parameters, key)) {
+    std::vector<TermDesc> terms = part.model->resolved_terms(part.parameters, key);
+    if (uses_adjoint(part.action)) terms = adjoint_terms(terms);
+    for (TermDesc t : terms) {
       for (auto& coupling : t.couplings) coupling.coefficient *= part.coefficient;
       all.push_back(std::move(t));
     }
@@ -1147,7 +1236,7 @@ Value dense_eigh_value(qmbed_operator_s& h, bool want_vectors) {
 
 // The assembled rows as the reference's operator payload: shape, format and
 // (row, column, value) entries in row order.
-Value operator_entries(qmbed_operator_s& h, const std::string& format) {
+Value operator_entries(qmbed_operator_s& h, const std::string& format, bool conjugate = false) {
   std::lock_guard<std::mutex> lock(h.mu);
   std::vector<uint64_t> row_ptr;
   std::vector<uint32_t> cols;
@@ -1166,7 +1255,7 @@ Value operator_entries(qmbed_operator_s& h, const std::string& format) {
       Value e = Value::object();
       e.set("row", Value::integer(static_cast<long long>(r)));
       e.set("column", Value::integer(static_cast<long long>(cols[p])));
-      e.set("value", complex_pair(values[p]));
+      e.set("value", complex_pair(conjugate ? std::conj(values[p]) : values[p]));
       entries.push(std::move(e));
     }
   out.set("entries", std::move(entries));
@@ -1261,8 +1350,9 @@ Value command(const Value& request) {
   }
   if (operation == "evaluate_operator_expression") {
     // EvaluateOperatorExpression -> command_operator_value (bindings/capi/src/lib.rs:5660-5663)
-    auto op = expression_operator(request.at("expression"), kStoragePacked);
-    return operator_entries(*op, request.has("format") ? request.at("format").as_string() : "csc");
+    bool conj = false;
+    auto op = expression_operator(request.at("expression"), kStoragePacked, &conj);
+    return operator_entries(*op, request.has("format") ? request.at("format").as_string() : "csc", conj);
   }
   if (operation == "create_model") {
     auto model = build_model(request);
@@ -1294,10 +1384,9 @@ Value command(const Value& request) {
   if (operation == "apply_model") {
     auto model = registered_model(request.at("handle").as_string());
     // OperatorActionRequest (bindings/capi/src/lib.rs:937-945): "normal" is the default
-    if (request.has("action") && request.at("action").as_string() != "normal")
-      raise(QMBED_UNSUPPORTED_BACKEND, "only the normal action is supported by the GPU engine");
-    auto op = model->materialize(request.find("parameters"), kStoragePacked, false);
-    return apply_vectors(*op, parse_vectors(request.at("vectors")));
+    const Action action = parse_action(request);
+    auto op = model->materialize_action(request.find("parameters"), kStoragePacked, action);
+    return apply_with_action(*op, parse_vectors(request.at("vectors")), conjugates(action));
   }
   if (operation == "matrix_elements_model") return matrix_elements(*registered_model(request.at("handle").as_string()), request);
   if (operation == "measure_model") return measure(*registered_model(request.at("handle").as_string()), request);
@@ -1344,12 +1433,13 @@ Value command(const Value& request) {
   }
   if (operation == "apply_operator_expression") {
     // command_apply_operator_expression (bindings/capi/src/lib.rs:4078-4105)
-    auto op = expression_operator(request.at("expression"));
+    bool conj = false;
+    auto op = expression_operator(request.at("expression"), kStoragePacked, &conj);
     const auto vectors = parse_vectors(request.at("vectors"));
     bool ok = !vectors.empty();
     for (const auto& v : vectors) ok = ok && v.size() == op->op->dim();
     if (!ok) raise(QMBED_DIMENSION_MISMATCH, "operator expression inputs must be a nonempty batch matching its columns");
-    return apply_vectors(*op, vectors);
+    return apply_with_action(*op, vectors, conj);
   }
   if (operation == "expm_operator_expression") {
     // command_expm_operator_expression (bindings/capi/src/lib.rs:4135-4170)

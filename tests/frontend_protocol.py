@@ -90,6 +90,11 @@ def model_matrix(request) -> np.ndarray:
     return evaluate(model_parts(request))
 
 
+def act(h, action):
+    """OperatorActionRequest (bindings/capi/src/lib.rs:937-945) on a dense matrix."""
+    return {"normal": h, "conjugate": h.conj(), "adjoint": h.conj().T, "transpose": h.T}[action]
+
+
 def complex_vectors(vectors):
     return [np.array([complex(*v) for v in vec]) for vec in vectors]
 
@@ -126,9 +131,9 @@ class OracleProtocol:
         """OperatorExpressionRequest (bindings/capi/src/lib.rs:789-818) for models without parameters."""
         kind = e["kind"]
         if kind == "model":
-            if e.get("action", "normal") != "normal":
-                raise NotImplementedError("model expression with an action")
-            return self.matrix(e["handle"], e.get("parameters"))
+            return act(self.matrix(e["handle"], e.get("parameters")), e.get("action", "normal"))
+        if kind == "transform":
+            return act(self.expression_matrix(e["operand"]), e.get("action", "normal"))
         if kind == "scale":
             return complex(*e["coefficient"]) * self.expression_matrix(e["operand"])
         if kind == "binary":
@@ -248,8 +253,9 @@ class OracleProtocol:
         if op == "eigsh_model":
             return {"kind": "eigensystem", **self.eigensystem(h, request["solver"])}
         if op == "apply_model":
+            a = act(h, request.get("action", "normal"))
             return {"kind": "vectors", "dimension": h.shape[0],
-                    "vectors": [pairs(h @ v) for v in complex_vectors(request["vectors"])]}
+                    "vectors": [pairs(a @ v) for v in complex_vectors(request["vectors"])]}
         if op == "eigh_model":
             values, vectors = np.linalg.eigh(h)
             out = {"kind": "eigensystem", "dimension": h.shape[0], "eigenvalues": values.tolist()}

@@ -317,3 +317,48 @@ def test_explicit_matrix_models_reject_bad_requests():
     for request, message in cases:
         with pytest.raises(QmbedError, match=message):
             command({"operation": "create_operator_model", **request})
+
+
+def test_operator_actions_match_the_oracle():
+    """Normal, conjugate, adjoint and transpose actions (OperatorActionRequest, bindings/capi/src/lib.rs:937-945)
+    of a non-Hermitian, translation-invariant model on a complex momentum sector: apply_model,
+    evaluate_operator_expression and apply_operator_expression of model and transform expressions."""
+    from frontend_protocol import OracleProtocol
+    from qmbed_b200._lib import command
+    L = 10
+    bonds = [[i, (i + 1) % L] for i in range(L)]
+    terms = [{"product": {"local": p}, "couplings": [{"coefficient": list(c), "sites": b} for b in bonds]}
+             for p, c in ((["raising", "lowering"], (0.7, 0.2)), (["lowering", "raising"], (0.3, -0.5)),
+                          (["z", "z"], (0.4, 0.1)))]
+    terms.append({"product": {"local": ["z"]}, "couplings": [{"coefficient": [0.2, 0.3], "sites": [i]} for i in range(L)]})
+    request = {"operation": "create_model", "basis": {"kind": "spin", "sites": L, "up": 4, "momentum": 3},
+               "terms": terms, "checks": {"hermiticity": False, "particle_conservation": True}}
+    oracle = OracleProtocol()
+    o_handle = oracle.call("qmbed_command_json", request)["handle"]
+    model = command(request)
+    try:
+        rng = np.random.default_rng(8)
+        x = rng.standard_normal((2, model["dimension"])) + 1j * rng.standard_normal((2, model["dimension"]))
+        vectors = [[[v.real, v.imag] for v in col] for col in x]
+        for action in ("normal", "conjugate", "adjoint", "transpose"):
+            for kind in ("model", "transform"):
+                expression = ({"kind": "model", "handle": model["handle"], "action": action} if kind == "model" else
+                              {"kind": "transform", "action": action,
+                               "operand": {"kind": "scale", "coefficient": [0.3, 0.4],
+                                           "operand": {"kind": "model", "handle": model["handle"]}}})
+                o_expression = json.loads(json.dumps(expression).replace(f'"{model["handle"]}"', f'"{o_handle}"'))
+                want = oracle.expression_matrix(o_expression)
+                got = _dense(command({"operation": "evaluate_operator_expression", "expression": expression}))
+                assert np.abs(got - want).max() <= 1e-13, (action, kind)
+                applied = command({"operation": "apply_operator_expression", "expression": expression,
+                                   "vectors": vectors})
+                y = np.array([[complex(*v) for v in col] for col in applied["vectors"]])
+                assert np.abs(y - x @ want.T).max() <= 1e-12, (action, kind)
+            applied = command({"operation": "apply_model", "handle": model["handle"], "action": action,
+                               "vectors": vectors})
+            y = np.array([[complex(*v) for v in col] for col in applied["vectors"]])
+            want = oracle.call("qmbed_command_json", {"operation": "apply_model", "handle": o_handle,
+                                                      "action": action, "vectors": vectors})
+            assert np.abs(y - np.array([[complex(*v) for v in col] for col in want["vectors"]])).max() <= 1e-12
+    finally:
+        command({"operation": "release_model", "handle": model["handle"]})

@@ -320,7 +320,7 @@ def test_lanczos_json_resource_anchor(anchors):
     with pytest.raises(QmbedError, match="exactly one expression"):
         _lib.command({"operation": "lanczos_thermal", "method": "ftlm", "eigenvalues": [0.0], "eigenvectors": [[1.0]],
                       "inverse_temperatures": [1.0], "observables": [{"name": "A"}]})
-    with pytest.raises(QmbedError, match="^unsupported backend: only the normal action"):
+    with pytest.raises(QmbedError, match="^unsupported backend: conjugate and transpose actions"):
         _lib.command({"operation": "lanczos_operator", "expression": {**expr, "action": "transpose"},
                       "initial": a["initial"], "krylov_dimension": 2})
     assert _lib.command({"operation": "release_lanczos", "lanczos_handle": handle})["kind"] == "released"
