@@ -126,3 +126,23 @@ def test_reference_frontend_binds_every_symbol_of_the_library():
     for symbol in ("qmbed_run_json", "qmbed_command_json", "qmbed_string_free", "qmbed_evolve_model_with_drive_json",
                    "qmbed_register_user_basis_32_json", "qmbed_register_user_basis_64_json"):
         assert isinstance(getattr(lib, symbol), ctypes._CFuncPtr)
+
+
+@pytest.mark.parametrize("k,p", [(0, 1), (0, -1), (5, None), (3, None)])
+def test_spin_flip_sectors_split_the_spectrum(oracle, k, p):
+    """The global spin flip (identity destinations, local maps [1, 0]) splits a sector at up = L/2 into
+    z = +1 and z = -1 blocks whose spectra together are the sector's, like the reference's parity
+    anchors (tests/full_api_foundation.rs:159-198)."""
+    from oracle import general
+    terms = oracle.heisenberg_terms(L10, delta=0.8)
+    maps = [{"destinations": _translation(L10, -1), "sector": k}]
+    if p is not None:
+        maps.append({"destinations": _reflection(L10), "sector": 0 if p == 1 else 1})
+    whole = np.linalg.eigvalsh(general.reduced_dense(general.GeneralSpinBasis(L10, 5, maps), terms))
+    flip = {"destinations": list(range(L10)), "local_permutations": [[1, 0]] * L10}
+    parts = []
+    for z in (0, 1):
+        b = general.GeneralSpinBasis(L10, 5, maps + [{**flip, "sector": z}], reverse=True)
+        parts.append(np.linalg.eigvalsh(general.reduced_dense(b, terms)))
+    assert len(parts[0]) + len(parts[1]) == len(whole) and min(len(parts[0]), len(parts[1])) > 0
+    np.testing.assert_allclose(np.sort(np.concatenate(parts)), whole, atol=1e-12)
