@@ -362,3 +362,26 @@ def test_operator_actions_match_the_oracle():
             assert np.abs(y - np.array([[complex(*v) for v in col] for col in want["vectors"]])).max() <= 1e-12
     finally:
         command({"operation": "release_model", "handle": model["handle"]})
+
+
+def test_spin_flip_sectors_split_the_spectrum_on_the_gpu():
+    """eigh_model on QuSpin's zblock = +1 and -1 sectors (kblock=0, pblock=1, reversed order, 12 sites) gives
+    together the spectrum of the sector without the spin flip."""
+    from qmbed_b200._lib import command
+    L = 12
+    bonds = [[i, (i + 1) % L] for i in range(L)]
+    terms = [{"product": {"local": p}, "couplings": [{"coefficient": [c, 0.0], "sites": b} for b in bonds]}
+             for p, c in ((["z", "z"], 0.8), (["raising", "lowering"], 0.5), (["lowering", "raising"], 0.5))]
+    spectra = {}
+    for z in (None, 1, -1):
+        request = {"operation": "create_model",
+                   "basis": {"kind": "spin", "sites": L, "up": L // 2, "normalization": "angular_momentum",
+                             "symmetries": _quspin_maps(L, 0, 1, z), "reverse": True},
+                   "terms": terms, "site_permutation": list(range(L))[::-1]}
+        model = command(request)
+        try:
+            spectra[z] = np.array(command({"operation": "eigh_model", "handle": model["handle"]})["eigenvalues"])
+        finally:
+            command({"operation": "release_model", "handle": model["handle"]})
+    assert len(spectra[1]) > 0 and len(spectra[-1]) > 0
+    np.testing.assert_allclose(np.sort(np.concatenate([spectra[1], spectra[-1]])), np.sort(spectra[None]), atol=1e-11)
