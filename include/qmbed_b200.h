@@ -104,6 +104,14 @@ QMBED_API int qmbed_gpu_basis_states(qmbed_basis basis, uint64_t offset, uint64_
 QMBED_API int qmbed_gpu_basis_images(qmbed_basis basis, const uint64_t* lo, const uint64_t* hi, uint64_t n,
                                      int64_t* index, double* phase, uint16_t* orbit);
 QMBED_API int qmbed_gpu_basis_build_seconds(qmbed_basis basis, double* seconds);
+/* The same images resolved through the sector's image table (one entry per
+ * parent state holding row, character and orbit class), built on first use:
+ * the lookup the matrix-free action uses. u64 states of symmetry sectors only
+ * (otherwise QMBED_STATUS_UNSUPPORTED_BACKEND). Replaces, like
+ * qmbed_gpu_basis_images, the HashMap probe of Basis::reduction_image /
+ * index_transition (src/basis/mod.rs:1536-1580), with the table in HBM. */
+QMBED_API int qmbed_gpu_basis_table_images(qmbed_basis basis, const uint64_t* lo, uint64_t n, int64_t* index,
+                                           double* phase, uint16_t* orbit);
 
 /* OperatorBuilder::on(&basis).terms(...).checks(...).build(format)
  * (src/operator/mod.rs:2040-2216). Terms are flattened: term t has arity[t]
@@ -126,8 +134,8 @@ QMBED_API int qmbed_gpu_operator_apply_device(qmbed_operator op, int precision, 
  * symmetry): out = alpha * (S^-1 H S) z + beta * z + gamma * p, S = diag(sqrt(R)).
  * p may be NULL; out may equal p but not z. One call is one step of a
  * three-term recurrence over nb vectors (the Chebyshev filter of the
- * QMBED_MODE_FILTERED solver). Real operators with packed storage only
- * (otherwise QMBED_STATUS_UNSUPPORTED_BACKEND). No counterpart in the
+ * QMBED_MODE_FILTERED solver). Real operators with packed or matrix-free
+ * storage (otherwise QMBED_STATUS_UNSUPPORTED_BACKEND). No counterpart in the
  * reference, whose operators act on one vector at a time
  * (LinearOperator::apply_real, src/operator/mod.rs:1414-1485). */
 QMBED_API int qmbed_gpu_operator_apply_block_device(qmbed_operator op, int precision, int nb, const void* z,
@@ -156,8 +164,28 @@ QMBED_API int qmbed_gpu_operator_apply_host(qmbed_operator op, int complex_vecto
  * with stored rows: first call with cols == NULL to get *nnz_total. */
 QMBED_API int qmbed_gpu_operator_export_csr(qmbed_operator op, uint64_t* nnz_total, uint64_t* row_ptr, uint32_t* cols,
                                             double* values);
-/* Operand-byte model of one application: D(b_state + s_y) + (D + nnz_off) s_x. */
+/* Operand-byte model of one application: D(b_state + s_y) + (D + nnz_off) s_x.
+ * Matrix-free operators count nnz_off (distinct off-diagonal columns per row)
+ * once, on the first call. */
 QMBED_API int qmbed_gpu_operator_operand_bytes(qmbed_operator op, int precision, int complex_vectors, double* bytes);
+/* Lookup of the matrix-free action (LinearOperator::apply with
+ * MatrixFormat::MatrixFree, src/operator/mod.rs:1414-1548, whose index
+ * transitions probe a HashMap, src/basis/mod.rs:1561-1580):
+ * QMBED_LOOKUP_AUTO (the image table when the basis holds one, else the
+ * representative search), QMBED_LOOKUP_TABLE (builds the table; error when it
+ * does not fit), QMBED_LOOKUP_SEARCH, QMBED_LOOKUP_LEGACY (one thread per row
+ * over every product, the form used for u128 states and products that repeat
+ * a site). */
+#define QMBED_LOOKUP_AUTO 0
+#define QMBED_LOOKUP_TABLE 1
+#define QMBED_LOOKUP_SEARCH 2
+#define QMBED_LOOKUP_LEGACY 3
+QMBED_API int qmbed_gpu_operator_set_lookup(qmbed_operator op, int mode);
+/* What the matrix-free action runs: 1 table, 2 search, 3 legacy, 4 no symmetry
+ * (direct or colex index); the basis's image table size and build time (0 when
+ * none). */
+QMBED_API int qmbed_gpu_operator_lookup_info(qmbed_operator op, int* in_use, uint64_t* table_bytes,
+                                             double* table_seconds);
 
 typedef struct {
   uint64_t eigenpairs;

@@ -282,6 +282,7 @@ SpinBasis::SpinBasis(const SpinBasisDesc& desc, int device) : device_(device), n
   } else {
     enumerate<u128>();
   }
+  prepare_lookup();
   QMBED_CUDA(cudaDeviceSynchronize());
   build_seconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
 }

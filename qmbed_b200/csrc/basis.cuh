@@ -1,6 +1,9 @@
 // Spin-1/2 chain sector basis resident in HBM.
 #pragma once
 
+#include <memory>
+#include <mutex>
+
 #include "common.cuh"
 
 namespace qmbed {
@@ -15,6 +18,25 @@ struct SpinBasisDesc {
   int parity;        // 0 none, +-1
   int normalization; // Normalization
   int inversion;     // 0 none, +-1: global spin-flip sector (up = L/2 or the full space, L <= 64)
+};
+
+// Image table of a symmetry sector: one entry per state of the parent space
+// (indexed by colex rank for fixed weight, by the state itself otherwise):
+//   entry = row | code << idx_bits,  code = sign | orbit class << 1 | m << (1 + rbits)
+// where row is the representative's index, sign and m give the character of
+// the group element mapping the state to its representative (m indexes
+// exp(-2 pi i m / L); m is absent for real characters) and the orbit class
+// indexes the sector's possible orbit sizes. States outside the sector hold
+// all ones. u32 entries when the fields fit 32 bits, u64 otherwise.
+struct ImageTable {
+  DeviceBuffer entries;
+  uint64_t length = 0, bytes = 0;
+  bool wide = false;
+  int idx_bits = 0, rbits = 0, mbits = 0;
+  DeviceBuffer class_inv_sqrt;  // per orbit class: 1/sqrt(R)
+  DeviceBuffer class_sizes;     // per orbit class: R (u16)
+  DeviceBuffer phase_m;         // 2L doubles
+  double build_seconds = 0.0;
 };
 
 // Layout in HBM:
@@ -51,9 +73,31 @@ class SpinBasis {
   double build_seconds() const { return build_seconds_; }
   uint64_t parent_dim() const { return parent_dim_; }
 
+  // Lookup structures of the warp-tile H.v (u64 states only). Colex chunk
+  // tables of fixed-weight spaces (4-bit chunks, stride up + 1; absent when
+  // larger than 40 KB) and fence keys (every fence_segment()-th
+  // representative, at most 4096) are built with the basis.
+  const uint64_t* rank_chunk_table() const { return rank_tab_.as<uint64_t>(); }
+  int rank_chunk_count() const { return rank_chunks_; }
+  int rank_chunk_stride() const { return rank_stride_; }
+  const uint64_t* fence_keys() const { return fences_.as<uint64_t>(); }
+  int fence_count() const { return n_fences_; }
+  uint64_t fence_segment() const { return fence_seg_; }
+  int fence_levels() const { return fence_levels_; }
+  // The image table when built, else null. build_image_table builds it once
+  // (thread-safe) when it fits QMBED_IMAGE_TABLE_MAX_BYTES (default 48 GiB)
+  // and 60% of the free device memory; otherwise it returns null, or raises
+  // when `required`.
+  const ImageTable* image_table() const;
+  const ImageTable* build_image_table(bool required) const;
+  // images() resolved through the image table (built here if absent): u64
+  // states of a symmetry sector only.
+  void table_images(const uint64_t* lo, uint64_t n, int64_t* index, double* phase, uint16_t* orbit) const;
+
  private:
   template <typename S>
   void enumerate();
+  void prepare_lookup();
 
   int device_;
   SectorParams params_{};
@@ -62,6 +106,11 @@ class SpinBasis {
   uint64_t dim_ = 0, parent_dim_ = 0;
   DeviceBuffer states_, orbits_, binom_, phase_;
   double build_seconds_ = 0.0;
+  DeviceBuffer rank_tab_, fences_;
+  int rank_chunks_ = 0, rank_stride_ = 0, n_fences_ = 0, fence_levels_ = 0;
+  uint64_t fence_seg_ = 0;
+  mutable std::mutex table_mu_;
+  mutable std::unique_ptr<ImageTable> table_;
 };
 
 }  // namespace qmbed

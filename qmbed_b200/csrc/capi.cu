@@ -1948,6 +1948,15 @@ int qmbed_gpu_basis_images(qmbed_basis basis, const uint64_t* lo, const uint64_t
   return guarded([&] { basis->basis->images(lo, hi, n, index, phase, orbit); });
 }
 
+int qmbed_gpu_basis_table_images(qmbed_basis basis, const uint64_t* lo, uint64_t n, int64_t* index, double* phase,
+                                 uint16_t* orbit) {
+  return guarded([&] {
+    if (basis->basis->words() != 1 || !basis->basis->symmetric())
+      raise(QMBED_UNSUPPORTED_BACKEND, "image tables serve symmetry sectors of at most 64 sites");
+    basis->basis->table_images(lo, n, index, phase, orbit);
+  });
+}
+
 int qmbed_gpu_basis_build_seconds(qmbed_basis basis, double* seconds) {
   return guarded([&] { *seconds = basis->basis->build_seconds(); });
 }
@@ -2040,7 +2049,26 @@ int qmbed_gpu_operator_export_csr(qmbed_operator op, uint64_t* nnz_total, uint64
 }
 
 int qmbed_gpu_operator_operand_bytes(qmbed_operator op, int precision, int complex_vectors, double* bytes) {
-  return guarded([&] { *bytes = op->op->operand_bytes(precision, complex_vectors != 0); });
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(op->mu);
+    *bytes = op->op->operand_bytes(precision, complex_vectors != 0);
+  });
+}
+
+int qmbed_gpu_operator_set_lookup(qmbed_operator op, int mode) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lock(op->mu);
+    op->op->set_lookup(mode);
+  });
+}
+
+int qmbed_gpu_operator_lookup_info(qmbed_operator op, int* in_use, uint64_t* table_bytes, double* table_seconds) {
+  return guarded([&] {
+    const ImageTable* t = op->op->basis().image_table();
+    if (in_use) *in_use = op->op->lookup_in_use();
+    if (table_bytes) *table_bytes = t ? t->bytes : 0;
+    if (table_seconds) *table_seconds = t ? t->build_seconds : 0.0;
+  });
 }
 
 int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, const double* initial, int n_initial,

@@ -892,6 +892,36 @@ SpinOperator::SpinOperator(std::shared_ptr<SpinBasis> basis, const std::vector<T
       assemble();
     }
   }
+  // Matrix-free operators on a symmetry sector resolve their targets through
+  // the basis's image table when it fits (built once, shared by every
+  // operator on the basis); otherwise through the representative search.
+  if (storage_ == kStorageMatrixFree && !flip_ && prog_.ok() && basis_->symmetric())
+    basis_->build_image_table(false);
+}
+
+bool SpinOperator::launch_tile_action(const TileLaunch& l) const {
+  if (lookup_mode_ == kLookupLegacy) return false;
+  TileLaunch a = l;
+  a.inv_sqrt = inv_sqrt_.as<double>();
+  return launch_tile(*basis_, prog_, lookup_mode_, a);
+}
+
+void SpinOperator::set_lookup(int mode) {
+  if (mode < kLookupAuto || mode > kLookupLegacy) raise(QMBED_INVALID_OPTIONS, "unknown lookup mode");
+  if (mode == kLookupTable) {
+    if (!prog_.ok() || !basis_->symmetric())
+      raise(QMBED_UNSUPPORTED_BACKEND, "image tables serve symmetry sectors of u64 states with a flip program");
+    QMBED_CUDA(cudaSetDevice(basis_->device()));
+    basis_->build_image_table(true);
+  }
+  lookup_mode_ = mode;
+}
+
+int SpinOperator::lookup_in_use() const {
+  if (lookup_mode_ == kLookupLegacy || !prog_.ok() || basis_->words() != 1) return 3;
+  if (!basis_->symmetric()) return 4;
+  if (lookup_mode_ != kLookupSearch && basis_->image_table()) return 1;
+  return 2;
 }
 
 void SpinOperator::build_instances(const std::vector<TermDesc>& terms, const OperatorChecks& checks) {
@@ -1034,6 +1064,7 @@ void SpinOperator::build_instances(const std::vector<TermDesc>& terms, const Ope
       nnz_off_ = flips * dim();
     }
   }
+  if (basis_->words() == 1) prog_.upload(compile_flip_program(adj, factors_, sites));
   inst_adj_.allocate(std::max<size_t>(adj.size(), 1) * sizeof(Instance));
   inst_fwd_.allocate(std::max<size_t>(fwd.size(), 1) * sizeof(Instance));
   if (!adj.empty()) {
@@ -1195,7 +1226,17 @@ void SpinOperator::apply(int precision, bool complex_vectors, const void* x, voi
     flip_->apply(precision, cplx, x, y, nullptr, nullptr, FlipStep{}, stream);
     return;
   }
+  // Wide rows of a real operator keep a real diagonal: complex vectors take the matrix-free path.
+  if (real_ && cplx && storage_ == kStorageWide) force_matrix_free = true;
   if (storage_ == kStorageMatrixFree || force_matrix_free) {
+    TileLaunch tl;
+    tl.precision = precision;
+    tl.nb = 1;
+    tl.complex_vectors = cplx;
+    tl.x = x;
+    tl.y = y;
+    tl.stream = stream;
+    if (launch_tile_action(tl)) return;
     const int grid = grid_for(n, 256, 8);
     const size_t smem = n_inst_ <= kSmemInstances ? static_cast<size_t>(n_inst_) * sizeof(Instance) : 0;
     auto launch = [&](auto stag, auto ttag, auto ctag) {
@@ -1262,11 +1303,6 @@ void SpinOperator::apply(int precision, bool complex_vectors, const void* x, voi
     QMBED_LAUNCH_CHECK();
     return;
   }
-  if (real_ && cplx) {
-    // Wide rows of a real operator keep a real diagonal: complex vectors take the matrix-free path.
-    apply(precision, complex_vectors, x, y, stream, true);
-    return;
-  }
   // Wide storage: explicit (interleaved complex) values.
   const void* xin = x;
   void* yout = y;
@@ -1304,17 +1340,20 @@ void SpinOperator::apply_with_scratch(int precision, bool complex_vectors, const
   const bool stored_symmetric = storage_ != kStorageMatrixFree && basis_->symmetric() &&
                                 !(real_ && cplx && storage_ == kStorageWide);
   if (!stored_symmetric) {
-    // these paths hold no scaled vector; flip chains take the on-the-fly
-    // expansion, whose kernels need no work buffer either
-    apply(precision, complex_vectors, x, y, stream, flip_ != nullptr);
+    // These paths hold no scaled vector. Flip chains and wide rows of a real
+    // operator with complex vectors take the on-the-fly expansion, whose
+    // kernels need no work buffer (the flip-chain kernels would allocate their
+    // diagonal tables on first use).
+    apply(precision, complex_vectors, x, y, stream, flip_ != nullptr || (real_ && cplx && storage_ == kStorageWide));
     return;
   }
   if (!real_ && !cplx) raise(QMBED_UNSUPPORTED_BACKEND, "real action requires an operator with real-valued storage");
   const int comps = cplx ? 2 : 1;
   const size_t need = static_cast<size_t>(n) * comps * (precision == kFP64 ? 8 : 4);
   if (need > scratch_bytes)
-    raise(QMBED_DIMENSION_MISMATCH, "the scaled input needs " + std::to_string(need) + " bytes of scratch, " +
-                                        std::to_string(scratch_bytes) + " available");
+    raise(QMBED_DIMENSION_MISMATCH, "symmetry sectors with stored rows take vectors of at most " +
+                                        std::to_string(scratch_bytes) + " bytes here; this one has " +
+                                        std::to_string(need));
   {
     const int grid = grid_for(n * comps, 256, 16);
     if (precision == kFP64)
@@ -1382,6 +1421,17 @@ bool SpinOperator::supports_block() const {
 
 void SpinOperator::launch_block_matrix_free(int precision, int nb, const void* z, const void* p, void* out,
                                             double alpha, double beta, double gamma, cudaStream_t stream) const {
+  TileLaunch tl;
+  tl.precision = precision;
+  tl.nb = nb;
+  tl.x = z;
+  tl.p = p;
+  tl.y = out;
+  tl.alpha = alpha;
+  tl.beta = beta;
+  tl.gamma = gamma;
+  tl.stream = stream;
+  if (launch_tile_action(tl)) return;
   const int grid = grid_for(dim(), 128, 16);
   const size_t smem = n_inst_ <= kSmemInstances ? static_cast<size_t>(n_inst_) * sizeof(Instance) : 0;
   auto launch = [&](auto stag, auto ttag, auto nbtag, auto ptag) {
@@ -1627,11 +1677,34 @@ void SpinOperator::trace_and_one_norm(C64* shift, double* one_norm) const {
   *one_norm = device_max_shifted_column(diag.as<double>(), offsum.as<double>(), n, *shift);
 }
 
+uint64_t SpinOperator::count_offdiag() const {
+  if (counted_nnz_ != ~0ull) return counted_nnz_;
+  QMBED_CUDA(cudaSetDevice(basis_->device()));
+  const uint64_t n = dim();
+  if (n == 0) return counted_nnz_ = 0;
+  DeviceBuffer row_nnz(n * sizeof(uint32_t)), diag(n * 2 * sizeof(double)), flags(sizeof(int));
+  QMBED_CUDA(cudaMemset(flags.get(), 0, sizeof(int)));
+  auto run = [&](auto tag) {
+    using S = decltype(tag);
+    auto v = make_view<S>(*basis_, inst_adj_, n_inst_, factors_, inv_sqrt_);
+    assemble_count_kernel<S><<<grid_for(n, 128, 16), 128>>>(v, row_nnz.as<uint32_t>(), diag.as<double>(), nullptr, 0,
+                                                             flags.as<int>());
+  };
+  if (basis_->words() == 1) run(uint64_t{});
+  else run(u128{});
+  QMBED_LAUNCH_CHECK();
+  DeviceBuffer row_ptr;
+  bool wide = false;
+  counted_nnz_ = exclusive_scan_counts(row_nnz.as<uint32_t>(), n, row_ptr, &wide);
+  return counted_nnz_;
+}
+
 double SpinOperator::operand_bytes(int precision, bool complex_vectors) const {
   const double s = (precision == kFP64 ? 8.0 : 4.0) * (complex_vectors ? 2.0 : 1.0);
   const double b_state = basis_->direct() ? 0.0 : 8.0 * basis_->words();
   const double n = static_cast<double>(dim());
   uint64_t nnz = nnz_off_;
+  if (storage_ == kStorageMatrixFree && !flip_) nnz = count_offdiag();
   return n * (b_state + s) + (n + static_cast<double>(nnz)) * s;
 }
 

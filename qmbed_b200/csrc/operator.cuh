@@ -11,6 +11,7 @@
 
 #include "basis.cuh"
 #include "flipchain.cuh"
+#include "hv_tile.cuh"
 
 namespace qmbed {
 
@@ -137,6 +138,17 @@ class SpinOperator {
   // Bytes per application in the operand model D(b_state + s_y) + (D + nnz_off) s_x.
   double operand_bytes(int precision, bool complex_vectors) const;
 
+  // Lookup used by the on-the-fly action (LookupMode): auto (the basis's
+  // image table when built, else the representative search), table (built
+  // here if absent; raises when it does not fit), search, or legacy (the
+  // one-thread-per-row expansion of every product, kept for u128 states and
+  // products that repeat a site).
+  void set_lookup(int mode);
+  int lookup_mode() const { return lookup_mode_; }
+  // What the on-the-fly action runs now: 1 table, 2 search, 3 legacy,
+  // 4 direct/colex (no symmetry).
+  int lookup_in_use() const;
+
  private:
   void build_instances(const std::vector<TermDesc>& terms, const OperatorChecks& checks);
   void assemble();
@@ -166,6 +178,14 @@ class SpinOperator {
   std::unique_ptr<FlipChain> flip_;
   mutable std::mutex tune_mu_;
   mutable std::map<int, int> block_shapes_;  // autotuned block-action shape per key
+  DeviceFlipProgram prog_;                   // flip form of the adjoint products (u64 states)
+  int lookup_mode_ = kLookupAuto;
+  // The warp-tile kernel with the current lookup; false when it does not apply.
+  bool launch_tile_action(const TileLaunch& l) const;
+  // Off-diagonal nonzeros after coalescing of a matrix-free operator, counted
+  // on the device on first use.
+  uint64_t count_offdiag() const;
+  mutable uint64_t counted_nnz_ = ~0ull;
 };
 
 }  // namespace qmbed

@@ -27,6 +27,8 @@ EVOLUTION_DIAGNOSTICS = ("lanczos_projections", "matrix_vector_products", "real_
                          "real_matrix_vector_products", "accepted_substeps", "rejected_trial_intervals",
                          "maximum_estimated_error")
 STORAGE = {"matrix_free": 0, "packed": 1, "explicit": 2}
+LOOKUPS = {"auto": 0, "table": 1, "search": 2, "legacy": 3}
+LOOKUPS_IN_USE = {1: "table", 2: "search", 3: "legacy", 4: "index"}
 
 
 def _ptr(array):
@@ -91,6 +93,16 @@ class GpuBasis:
         phase = np.zeros(n, np.complex128)
         orbit = np.zeros(n, np.uint16)
         check(lib().qmbed_gpu_basis_images(self.handle, _ptr(lo), _ptr(hi), n, _ptr(index), _ptr(phase), _ptr(orbit)))
+        return index, phase, orbit
+
+    def table_images(self, lo):
+        """images() resolved through the sector's image table (u64 symmetry sectors)."""
+        lo = np.ascontiguousarray(lo, np.uint64)
+        n = len(lo)
+        index = np.zeros(n, np.int64)
+        phase = np.zeros(n, np.complex128)
+        orbit = np.zeros(n, np.uint16)
+        check(lib().qmbed_gpu_basis_table_images(self.handle, _ptr(lo), n, _ptr(index), _ptr(phase), _ptr(orbit)))
         return index, phase, orbit
 
 
@@ -196,7 +208,7 @@ class GpuOperator:
         """out = alpha (S^-1 H S) z + beta z + gamma p on row-major n x nb device blocks.
 
         Coordinates are orbit-scaled (z = x / sqrt(R) in symmetry sectors); real
-        operators with packed storage only.
+        operators with packed or matrix-free storage.
         """
         check(lib().qmbed_gpu_operator_apply_block_device(self.handle, precision, nb, _ptr(z), _ptr(p), _ptr(out),
                                                           alpha, beta, gamma,
@@ -211,6 +223,17 @@ class GpuOperator:
         """
         check(lib().qmbed_gpu_operator_apply_device_noalloc(self.handle, precision, int(complex_vectors), _ptr(x),
                                                             _ptr(y), None if stream is None else ctypes.c_void_p(stream)))
+
+    def set_lookup(self, mode: str) -> None:
+        """Lookup of the matrix-free action: "auto", "table", "search" or "legacy"."""
+        check(lib().qmbed_gpu_operator_set_lookup(self.handle, LOOKUPS[mode]))
+
+    def lookup_info(self) -> dict:
+        in_use, nbytes, seconds = ctypes.c_int(), ctypes.c_uint64(), ctypes.c_double()
+        check(lib().qmbed_gpu_operator_lookup_info(self.handle, ctypes.byref(in_use), ctypes.byref(nbytes),
+                                                   ctypes.byref(seconds)))
+        return {"lookup": LOOKUPS_IN_USE.get(in_use.value, "none"), "table_bytes": nbytes.value,
+                "table_seconds": seconds.value}
 
     def operand_bytes(self, precision: int = 64, complex_vectors: bool = False) -> float:
         value = ctypes.c_double()
