@@ -148,9 +148,13 @@ QMBED_API int qmbed_gpu_operator_apply_block_device(qmbed_operator op, int preci
  * reference: it is an addition of this library. It allocates nothing; the
  * x / sqrt(R) vector of symmetry sectors with stored rows goes to a fixed
  * 32 MiB array in device global memory, reserved on every GPU where the
- * library's device code is loaded and held until the process exits. Vectors
- * are limited to 32 MiB (dimension x (2 if complex) x (8 FP64 | 4 FP32) bytes);
- * larger ones return QMBED_STATUS_DIMENSION_MISMATCH. The first call on a
+ * library's device code is loaded and held until the process exits. For those
+ * operators vectors are limited to 32 MiB (dimension x (2 if complex) x
+ * (8 FP64 | 4 FP32) bytes); larger ones return QMBED_STATUS_DIMENSION_MISMATCH.
+ * Other operators (matrix-free storage, no symmetry, flip chains) use no
+ * scratch and have no limit; flip chains run the matrix-free tile kernel here,
+ * because their structured kernels allocate diagonal tables on first use.
+ * The first call on a
  * device looks up the array's device address (once per device, cached); make
  * that first call before any stream capture. All calls share the array and it
  * keeps the last call's contents (each call overwrites the part it reads), so

@@ -24,8 +24,8 @@ namespace {
 
 // 32 MiB of scratch, reserved in global memory of every GPU on which this
 // library's device code is loaded, and held until the process exits. It
-// bounds the input vector: dimension x (2 if complex) x (8 for FP64, 4 for
-// FP32) bytes.
+// bounds the input vector of symmetry sectors with stored rows: dimension x
+// (2 if complex) x (8 for FP64, 4 for FP32) bytes.
 constexpr size_t kNoAllocScratchBytes = size_t{1} << 25;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -62,11 +62,8 @@ extern "C" int qmbed_gpu_operator_apply_device_noalloc(qmbed_operator op, int pr
   return qmbed::noalloc_guarded([&] {
     if (precision != 64 && precision != 32) qmbed::raise(qmbed::QMBED_INVALID_OPTIONS, "precision must be 64 or 32");
     const qmbed::SpinOperator& H = qmbed::operator_of(op);
-    const size_t need = static_cast<size_t>(H.dim()) * (complex_vectors ? 2 : 1) * (precision == 64 ? 8 : 4);
-    if (need > kNoAllocScratchBytes)
-      qmbed::raise(qmbed::QMBED_DIMENSION_MISMATCH,
-                   "qmbed_gpu_operator_apply_device_noalloc accepts vectors of at most " +
-                       std::to_string(kNoAllocScratchBytes) + " bytes; this one has " + std::to_string(need));
+    // The size limit applies where the scratch is used (symmetry sectors with
+    // stored rows); apply_with_scratch checks it there.
     void* scratch = scratch_address(H.basis().device());
     H.apply_with_scratch(precision, complex_vectors != 0, x, y, static_cast<cudaStream_t>(stream), scratch,
                          kNoAllocScratchBytes);
