@@ -27,6 +27,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -35,7 +36,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "eigsh time to 1e-10 (L=34 Heisenberg k=0 p=+1, 4 lowest, Krylov 40)"
+METRIC = "eigsh time to 1e-10 (L=34 Heisenberg k=0 p=+1, 4 lowest)"
 UNIT = "s/solve"
 
 
@@ -61,9 +62,89 @@ def parse():
                    help="XXZ plain/mixed/filtered comparison size (0 skips it)")
     p.add_argument("--ftlm-sites", type=int, default=28,
                    help="finite-temperature Lanczos size: 8 vectors x 100 steps (0 skips it)")
+    p.add_argument("--matrix-free-sites", type=int, default=34,
+                   help="on-the-fly (matrix-free) H.v, block action and solves at this size (0 skips it)")
     p.add_argument("--scan-sites", type=int, default=26,
                    help="batched J1-J2 scan size: every momentum sector x 64 points (0 skips it)")
     return p.parse_args()
+
+
+def timed_launches(fn, count: int) -> float:
+    """Seconds per call of `fn` over `count` back-to-back calls (CUDA events, after 3 warm-up calls)."""
+    import torch
+    for _ in range(3):
+        fn()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(count):
+        fn()
+    stop.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(stop) / 1000.0 / count
+
+
+def matrix_free_section(sites: int, rank: int, local_rank: int, peak: float, launches: int,
+                        eigenpairs: int, krylov: int, tolerance: float) -> dict:
+    """The L=34 sector with the terms expanded on every application (no stored
+    rows): the warp-tile kernel resolving targets through the image table,
+    H.v and 8-vector block action timed against the operand-byte model, the
+    representative search timed beside it, and the filtered and plain FP64
+    solves on this storage."""
+    import torch
+    from qmbed_b200 import engine
+
+    basis = engine.GpuBasis(sites, up=sites // 2, momentum=0, parity=1, device=local_rank)
+    t0 = time.perf_counter()
+    op = engine.GpuOperator(basis, engine.heisenberg_terms(sites), storage="matrix_free")
+    setup = time.perf_counter() - t0
+    info = op.lookup_info()
+    dim = len(basis)
+    b32, b64 = op.operand_bytes(32), op.operand_bytes(64)
+    x32 = torch.rand(dim, dtype=torch.float32, device="cuda")
+    y32 = torch.empty_like(x32)
+    x64 = x32.double()
+    y64 = torch.empty_like(x64)
+    out = {"workload": f"heisenberg L={sites} k=0 p=+1 dim={dim}, terms expanded per application",
+           "lookup": info["lookup"], "chain_form": info["chain_form"], "image_table_bytes": info["table_bytes"],
+           "image_table_build_s": info["table_seconds"], "setup_s": setup, "operand_bytes_fp32": b32,
+           "operand_bytes_fp64": b64}
+    hv32 = timed_launches(lambda: op.apply_device(x32, y32, precision=32), launches)
+    hv64 = timed_launches(lambda: op.apply_device(x64, y64, precision=64), launches)
+    zb = torch.rand((dim, 8), dtype=torch.float32, device="cuda")
+    pb = torch.rand_like(zb)
+    blk = timed_launches(lambda: op.apply_block_device(zb, pb, 8, precision=32, alpha=1.0 / 16, gamma=0.5, p=pb),
+                         launches)
+    block_bytes = 8 * b32 + dim * 8 * 4
+    out["hv"] = {"fp32_ms": hv32 * 1e3, "fp64_ms": hv64 * 1e3, "fp32_gbs": b32 / hv32 / 1e9,
+                 "fp64_gbs": b64 / hv64 / 1e9, "fp32_frac": b32 / hv32 / 1e9 / peak}
+    out["block_action"] = {"nb": 8, "ms": blk * 1e3, "operand_bytes": block_bytes, "gbs": block_bytes / blk / 1e9,
+                           "frac": block_bytes / blk / 1e9 / peak}
+    del zb, pb
+    op.set_lookup("search")
+    search32 = timed_launches(lambda: op.apply_device(x32, y32, precision=32), max(2, launches // 10))
+    op.set_lookup("auto")
+    out["search_hv_fp32_ms"] = search32 * 1e3
+    del x32, y32, x64, y64
+    solves = {}
+    for mode in ("filtered", "fp64"):
+        kw = dict(krylov_dimension=krylov, tolerance=tolerance, seed=rank, mode=mode)
+        if mode == "filtered":
+            op.eigsh(eigenpairs, **kw)  # warm-up: autotuning and workspaces
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        r = op.eigsh(eigenpairs, **kw)
+        stop.record()
+        torch.cuda.synchronize()
+        solves[mode] = {"s": start.elapsed_time(stop) / 1000.0, "iterations": r.iterations,
+                        "applications": r.operator_applications, "eigenvalues": r.eigenvalues.tolist(),
+                        "max_residual": float(np.max(r.residuals))}
+    ref = np.asarray(solves["fp64"]["eigenvalues"])
+    got = np.asarray(solves["filtered"]["eigenvalues"])
+    solves["filtered"]["max_rel_diff_vs_fp64"] = float(np.max(np.abs(got - ref) / np.abs(ref)))
+    solves["speedup_filtered_vs_fp64"] = solves["fp64"]["s"] / solves["filtered"]["s"]
+    out["eigsh"] = solves
+    return out
 
 
 def xxz_section(sites: int, rank: int, local_rank: int) -> dict:
@@ -290,7 +371,7 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{device}.csv"
+        self.path = Path(tempfile.gettempdir()) / f"qmbed_clocks_{os.getpid()}_rank{device}.csv"
 
     def __enter__(self):
         try:
@@ -558,6 +639,12 @@ def main():
                          f"{sample['iterations']} H.v, {sample['solve_s']:.2f} s) scaled by rows and by "
                          f"{iterations_target} iterations to D={dim}"}
 
+    # the packed rows are released before the on-the-fly section builds its image table
+    matrix_free_result = None
+    if args.matrix_free_sites > 0:
+        matrix_free_result = matrix_free_section(args.matrix_free_sites, rank, local_rank, peak, args.hv_launches,
+                                                 args.eigenpairs, args.krylov, args.tolerance)
+
     quench_result = None
     if args.quench_sites > 0:
         quench_result = quench(args.quench_sites, args.quench_bounds, rank, local_rank)
@@ -576,7 +663,12 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.mode == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": {"workload": f"heisenberg L={sites} k=0 p=+1 up={sites // 2} dim={dim}, {args.eigenpairs} "
-                                   f"lowest, krylov {args.krylov}, tol {args.tolerance:g}, mode {args.mode}",
+                                   f"lowest, tol {args.tolerance:g}, mode {args.mode}"
+                                   + (" (block Chebyshev-filtered subspace iteration)" if args.mode == "filtered"
+                                      else f" (thick-restart Lanczos, krylov {args.krylov})")
+                                   + ", storage packed rows (4 B per stored entry)",
+                       "plain_fp64": f"thick-restart Lanczos, krylov {args.krylov}, reference algorithms in FP64,"
+                                     " same storage",
                        "l2": "working set (GBs of vectors and packed rows) exceeds the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
             "eigenvalues": last.eigenvalues.tolist(), "residuals": last.residuals.tolist(),
@@ -590,6 +682,7 @@ def main():
                    "operand_bytes_fp64": op.operand_bytes(64), "fp32_gbs": achieved,
                    "fp64_gbs": op.operand_bytes(64) / hv64_s / 1e9},
             "block_action": block,
+            "matrix_free": matrix_free_result,
             "quench": quench_result,
             "scan": scan_result,
             "xxz": xxz_result,

@@ -186,9 +186,11 @@ QMBED_API int qmbed_gpu_operator_operand_bytes(qmbed_operator op, int precision,
 #define QMBED_LOOKUP_LEGACY 3
 QMBED_API int qmbed_gpu_operator_set_lookup(qmbed_operator op, int mode);
 /* What the matrix-free action runs: 1 table, 2 search, 3 legacy, 4 no symmetry
- * (direct or colex index); the basis's image table size and build time (0 when
- * none). */
-QMBED_API int qmbed_gpu_operator_lookup_info(qmbed_operator op, int* in_use, uint64_t* table_bytes,
+ * (direct or colex index); whether it expands the products in their
+ * translation-structured form (uniform couplings per bond displacement: one
+ * activity mask per displacement from word operations); the basis's image
+ * table size and build time (0 when none). */
+QMBED_API int qmbed_gpu_operator_lookup_info(qmbed_operator op, int* in_use, int* chain_form, uint64_t* table_bytes,
                                              double* table_seconds);
 
 typedef struct {

@@ -97,7 +97,7 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_basis_build_seconds.argtypes = [vp, P(d)]
     L.qmbed_gpu_basis_table_images.argtypes = [vp, vp, u64, vp, vp, vp]
     L.qmbed_gpu_operator_set_lookup.argtypes = [vp, i]
-    L.qmbed_gpu_operator_lookup_info.argtypes = [vp, P(i), P(u64), P(d)]
+    L.qmbed_gpu_operator_lookup_info.argtypes = [vp, P(i), P(i), P(u64), P(d)]
     L.qmbed_gpu_operator_create.argtypes = [vp, i, vp, ctypes.c_char_p, vp, vp, vp, i, i, i, P(vp)]
     L.qmbed_gpu_operator_destroy.argtypes = [vp]
     L.qmbed_gpu_operator_info.argtypes = [vp, P(u64), P(i), P(i), P(u64), P(i), P(d)]

@@ -158,8 +158,29 @@ namespace {
 
 thread_local std::string g_last_error;
 
+// Every entry point leaves the calling thread's current device as it found
+// it: the library selects the device of the handle it works on, and an
+// embedding host (a framework with its own current device) must not see that.
+struct CallerDevice {
+  int device = -1;
+  CallerDevice() {
+    if (cudaGetDevice(&device) != cudaSuccess) {
+      device = -1;
+      (void)cudaGetLastError();
+    }
+  }
+  ~CallerDevice() {
+    int now = -1;
+    if (device >= 0 && cudaGetDevice(&now) == cudaSuccess && now != device && cudaSetDevice(device) != cudaSuccess)
+      (void)cudaGetLastError();
+  }
+  CallerDevice(const CallerDevice&) = delete;
+  CallerDevice& operator=(const CallerDevice&) = delete;
+};
+
 template <typename F>
 int guarded(F&& body) {
+  CallerDevice restore;
   try {
     body();
     return QMBED_STATUS_OK;
@@ -1744,6 +1765,7 @@ Value command(const Value& request) {
 std::string respond_with(const char* request, const std::string& invalid,
                          const std::function<Value(const Value&)>& handler) {
   if (!request) return R"({"status":"error","error":"request pointer is null"})";
+  CallerDevice restore;
   Value response = Value::object();
   try {
     Value parsed;
@@ -2062,10 +2084,12 @@ int qmbed_gpu_operator_set_lookup(qmbed_operator op, int mode) {
   });
 }
 
-int qmbed_gpu_operator_lookup_info(qmbed_operator op, int* in_use, uint64_t* table_bytes, double* table_seconds) {
+int qmbed_gpu_operator_lookup_info(qmbed_operator op, int* in_use, int* chain_form, uint64_t* table_bytes,
+                                   double* table_seconds) {
   return guarded([&] {
     const ImageTable* t = op->op->basis().image_table();
     if (in_use) *in_use = op->op->lookup_in_use();
+    if (chain_form) *chain_form = op->op->chain_form() && op->op->lookup_in_use() != 3 ? 1 : 0;
     if (table_bytes) *table_bytes = t ? t->bytes : 0;
     if (table_seconds) *table_seconds = t ? t->build_seconds : 0.0;
   });

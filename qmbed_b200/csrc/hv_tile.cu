@@ -22,16 +22,102 @@
 
 namespace qmbed {
 
+namespace {
+
+constexpr int kRankChunkBits = 4;
+constexpr int kRankChunkValues = 1 << kRankChunkBits;
+constexpr size_t kRankTableMaxBytes = 40 * 1024;
+constexpr int kMaxFences = 4096;
+constexpr size_t kProgramSmemMax = 32 * 1024;
+constexpr int kTileThreads = 256;
+constexpr uint64_t kAllOnes = ~0ull;
+
+using TermKey = std::tuple<uint64_t, uint64_t, uint64_t>;  // req_mask, req_val, sign_mask
+
+// Amplitude of one term on the state whose bits at sites i, j are (v & 1, v >> 1).
+double term_sign(const TermKey& key, int i, int j, int v, bool* allowed) {
+  const auto& [req_mask, req_val, sign_mask] = key;
+  auto bit_of = [&](int site) -> uint64_t {
+    if (site == i) return static_cast<uint64_t>(v & 1);
+    return static_cast<uint64_t>((v >> 1) & 1);
+  };
+  uint64_t state = 0;
+  for (int site : {i, j}) state |= bit_of(site) << site;
+  *allowed = (state & req_mask) == req_val;
+  const int zeros = __builtin_popcountll(~state & sign_mask & ((1ull << i) | (1ull << j)));
+  return (zeros & 1) ? -1.0 : 1.0;
+}
+
+// Sites (i <= j) carrying every bit of `u`, when u has at most two bits.
+bool two_sites(uint64_t u, int* i, int* j) {
+  const int n = __builtin_popcountll(u);
+  if (n > 2) return false;
+  if (n == 0) {
+    *i = *j = 0;
+    return true;
+  }
+  *i = __builtin_ctzll(u);
+  *j = 63 - __builtin_clzll(u);
+  return true;
+}
+
+}  // namespace
+
 // ---------------------------------------------------------------------------
 // Flip programs (host)
 // ---------------------------------------------------------------------------
 
-FlipProgram compile_flip_program(const std::vector<Instance>& adjoint, const LocalFactors& f, int sites) {
+namespace {
+
+// Chain classes from pair tables: bond (i, i + d mod L), digits v = d_i | d_{i+d} << 1.
+struct ChainBuilder {
+  int sites;
+  bool ok = true;
+  std::vector<ChainClass> classes;
+
+  void add(int a, int b, const double* re, const double* im, int nz) {
+    // a < b: orient the bond as (i, i + d) with d <= L / 2
+    int i = a, d = b - a;
+    bool swap = false;
+    if (d > sites - d) {
+      i = b;
+      d = sites - d;
+      swap = true;  // the table's first digit is then the bond's second site
+    }
+    double r[4], m[4];
+    int z = 0;
+    for (int v = 0; v < 4; ++v) {
+      const int w = swap ? (((v & 1) << 1) | (v >> 1)) : v;
+      r[v] = re[w];
+      m[v] = im[w];
+      if ((nz >> w) & 1) z |= 1 << v;
+    }
+    for (ChainClass& c : classes) {
+      if (c.d != d) continue;
+      if (c.nz != z || std::memcmp(c.re, r, sizeof r) != 0 || std::memcmp(c.im, m, sizeof m) != 0) ok = false;
+      if (c.bonds & (1ull << i)) ok = false;
+      c.bonds |= 1ull << i;
+      return;
+    }
+    ChainClass c{};
+    c.bonds = 1ull << i;
+    c.d = d;
+    c.nz = z;
+    std::memcpy(c.re, r, sizeof r);
+    std::memcpy(c.im, m, sizeof m);
+    classes.push_back(c);
+  }
+};
+
+}  // namespace
+
+FlipProgram compile_flip_program(const std::vector<Instance>& adjoint, const LocalFactors& f, int sites,
+                                 bool fixed_weight) {
   FlipProgram prog;
   if (sites > 64) return prog;
   // spin-1/2 factors: z(d) = z1 * (+1 | -1), ladder factors independent of d
   if (f.z[0] != -f.z[1] || f.raise != f.lower) return prog;
-  std::map<uint64_t, std::map<std::tuple<uint64_t, uint64_t, uint64_t>, C64>> by_flip;
+  std::map<uint64_t, std::map<TermKey, C64>> by_flip;
   for (const Instance& a : adjoint) {
     uint64_t seen = 0, flip = 0, req_mask = 0, req_val = 0, sign_mask = 0;
     C64 k(a.cr, a.ci);
@@ -75,24 +161,132 @@ FlipProgram compile_flip_program(const std::vector<Instance>& adjoint, const Loc
     // the row entry is conj(coefficient * amplitude)
     by_flip[flip][{req_mask, req_val, sign_mask}] += std::conj(k);
   }
-  for (const auto& [flip, terms] : by_flip) {
-    std::vector<FlipTerm> list;
-    for (const auto& [key, k] : terms) {
+  // Products whose amplitude depends on at most two sites (those they flip
+  // included) become 4-entry amplitude tables indexed by the two digits.
+  auto add_slot = [&](const std::map<TermKey, C64>& terms, int i, int j, uint8_t* nz) {
+    C64 amp[4];
+    for (int v = 0; v < 4; ++v)
+      for (const auto& [key, k] : terms) {
+        bool allowed = false;
+        const double sign = term_sign(key, i, j, v, &allowed);
+        if (allowed) amp[v] += sign * k;
+      }
+    *nz = 0;
+    for (int v = 0; v < 4; ++v) {
+      prog.amp_re.push_back(amp[v].real());
+      prog.amp_im.push_back(amp[v].imag());
+      if (amp[v].imag() != 0.0) prog.complex_coefs = true;
+      if (amp[v] != C64(0.0, 0.0)) *nz |= static_cast<uint8_t>(1u << v);
+    }
+  };
+  // diagonal products: grouped by the (at most two) sites they read
+  if (by_flip.count(0)) {
+    std::map<std::pair<int, int>, std::map<TermKey, C64>> pairs;
+    for (const auto& [key, k] : by_flip[0]) {
       if (k == C64(0.0, 0.0)) continue;
-      FlipTerm t{std::get<0>(key), std::get<1>(key), std::get<2>(key), k.real(), k.imag()};
-      if (t.ki != 0.0) prog.complex_coefs = true;
-      list.push_back(t);
+      int i = 0, j = 0;
+      if (two_sites(std::get<0>(key) | std::get<2>(key), &i, &j)) {
+        pairs[{i, j}][key] += k;
+      } else {
+        FlipTerm t{std::get<0>(key), std::get<1>(key), std::get<2>(key), k.real(), k.imag()};
+        if (t.ki != 0.0) prog.complex_coefs = true;
+        prog.diag_terms.push_back(t);
+      }
     }
-    if (list.empty()) continue;
-    if (flip == 0) {
-      prog.diag = list;
-      continue;
+    for (const auto& [sites_ij, terms] : pairs) {
+      uint8_t nz = 0;
+      add_slot(terms, sites_ij.first, sites_ij.second, &nz);
+      prog.diag_pairs.push_back(static_cast<uint32_t>(sites_ij.first) | (static_cast<uint32_t>(sites_ij.second) << 8));
     }
-    FlipGroup g{flip, static_cast<uint32_t>(prog.terms.size()), static_cast<uint32_t>(list.size())};
+  }
+  for (const auto& [flip, terms] : by_flip) {
+    if (flip == 0) continue;
+    std::map<TermKey, C64> live;
+    uint64_t reads = flip;
+    for (const auto& [key, k] : terms)
+      if (k != C64(0.0, 0.0)) {
+        live[key] = k;
+        reads |= std::get<0>(key) | std::get<2>(key);
+      }
+    if (live.empty()) continue;
+    FlipGroup g{};
+    g.flip = flip;
+    g.chunk_lo = static_cast<uint8_t>(__builtin_ctzll(flip) / 4);
+    g.chunk_hi = static_cast<uint8_t>((63 - __builtin_clzll(flip)) / 4);
+    int i = 0, j = 0;
+    if (two_sites(reads, &i, &j)) {
+      g.kind = kGroupPair;
+      g.site_i = static_cast<uint8_t>(i);
+      g.site_j = static_cast<uint8_t>(j);
+      g.first = static_cast<uint32_t>(prog.amp_re.size() / 4);
+      add_slot(live, i, j, &g.nz);
+      if (fixed_weight) {
+        // a flip keeps the weight only when it moves one up spin: two flipped
+        // sites with different digits (v = 1, 2)
+        g.nz &= (__builtin_popcountll(flip) == 2) ? 0x6 : 0x0;
+      }
+      if (g.nz == 0) {  // every amplitude cancels, or every target leaves the space
+        prog.amp_re.resize(prog.amp_re.size() - 4);
+        prog.amp_im.resize(prog.amp_im.size() - 4);
+        continue;
+      }
+    } else {
+      g.kind = kGroupGeneric;
+      g.first = static_cast<uint32_t>(prog.terms.size());
+      for (const auto& [key, k] : live) {
+        FlipTerm t{std::get<0>(key), std::get<1>(key), std::get<2>(key), k.real(), k.imag()};
+        if (t.ki != 0.0) prog.complex_coefs = true;
+        prog.terms.push_back(t);
+      }
+      g.count = static_cast<uint16_t>(prog.terms.size() - g.first);
+    }
     prog.groups.push_back(g);
-    prog.terms.insert(prog.terms.end(), list.begin(), list.end());
   }
   prog.ok = true;
+  // Translation-structured form: every group a two-site flip, every diagonal
+  // part a site pair or a uniform single-site field, uniform per displacement.
+  ChainBuilder off{sites}, diag{sites};
+  bool chain = prog.terms.empty() && prog.diag_terms.empty();
+  for (const FlipGroup& g : prog.groups) {
+    if (!chain) break;
+    if (g.kind != kGroupPair || g.site_i == g.site_j) {
+      chain = false;
+      break;
+    }
+    off.add(g.site_i, g.site_j, &prog.amp_re[4 * g.first], &prog.amp_im[4 * g.first], g.nz);
+  }
+  ChainProgram cp{};
+  for (size_t q = 0; q < prog.diag_pairs.size() && chain; ++q) {
+    const int i = prog.diag_pairs[q] & 0xff, j = prog.diag_pairs[q] >> 8;
+    const double* re = &prog.amp_re[4 * q];
+    const double* im = &prog.amp_im[4 * q];
+    if (i != j) {
+      diag.add(i, j, re, im, 0xf);
+      continue;
+    }
+    // one site: digits 0 and 1 sit at v = 0 and v = 3
+    if (cp.has_field && (cp.field_re[0] != re[0] || cp.field_re[1] != re[3] || cp.field_im[0] != im[0] ||
+                         cp.field_im[1] != im[3] || (cp.field_mask & (1ull << i)))) {
+      chain = false;
+      break;
+    }
+    cp.has_field = 1;
+    cp.field_mask |= 1ull << i;
+    cp.field_re[0] = re[0];
+    cp.field_re[1] = re[3];
+    cp.field_im[0] = im[0];
+    cp.field_im[1] = im[3];
+  }
+  chain = chain && off.ok && diag.ok && off.classes.size() <= static_cast<size_t>(kChainMaxOff) &&
+          diag.classes.size() <= static_cast<size_t>(kChainMaxDiag);
+  if (chain) {
+    cp.n_off = static_cast<int>(off.classes.size());
+    cp.n_diag = static_cast<int>(diag.classes.size());
+    for (int c = 0; c < cp.n_off; ++c) cp.off[c] = off.classes[static_cast<size_t>(c)];
+    for (int c = 0; c < cp.n_diag; ++c) cp.diag[c] = diag.classes[static_cast<size_t>(c)];
+    prog.chain = cp;
+    prog.chain_ok = true;
+  }
   return prog;
 }
 
@@ -100,32 +294,39 @@ void DeviceFlipProgram::upload(const FlipProgram& prog) {
   ok_ = prog.ok;
   if (!ok_) return;
   complex_ = prog.complex_coefs;
-  n_diag_ = static_cast<int>(prog.diag.size());
-  n_terms_ = n_diag_ + static_cast<int>(prog.terms.size());
+  chain_ok_ = prog.chain_ok;
+  chain_ = prog.chain;
+  n_dterms_ = static_cast<int>(prog.diag_terms.size());
+  n_terms_ = n_dterms_ + static_cast<int>(prog.terms.size());
   n_groups_ = static_cast<int>(prog.groups.size());
-  std::vector<FlipTerm> all(prog.diag);
+  n_slots_ = static_cast<int>(prog.amp_re.size() / 4);
+  n_dpairs_ = static_cast<int>(prog.diag_pairs.size());
+  std::vector<FlipTerm> all(prog.diag_terms);
   all.insert(all.end(), prog.terms.begin(), prog.terms.end());
-  // group term offsets are relative to the diagonal-free list: shift them
+  // generic group terms follow the generic diagonal terms
   std::vector<FlipGroup> groups(prog.groups);
-  for (FlipGroup& g : groups) g.first += static_cast<uint32_t>(n_diag_);
+  for (FlipGroup& g : groups)
+    if (g.kind == kGroupGeneric) g.first += static_cast<uint32_t>(n_dterms_);
+  // [terms][groups][amp_re][amp_im][diag pair sites], every part 8-byte aligned
   groups_offset_ = all.size() * sizeof(FlipTerm);
-  bytes_ = groups_offset_ + groups.size() * sizeof(FlipGroup);
-  buf_.allocate(std::max<size_t>(bytes_, 16));
-  if (!all.empty()) QMBED_CUDA(cudaMemcpy(buf_.get(), all.data(), groups_offset_, cudaMemcpyHostToDevice));
-  if (!groups.empty())
-    QMBED_CUDA(cudaMemcpy(buf_.as<char>() + groups_offset_, groups.data(), groups.size() * sizeof(FlipGroup),
-                          cudaMemcpyHostToDevice));
+  amp_offset_ = groups_offset_ + groups.size() * sizeof(FlipGroup);
+  pairs_offset_ = amp_offset_ + 2 * prog.amp_re.size() * sizeof(double);
+  bytes_ = pairs_offset_ + ((prog.diag_pairs.size() + 1) / 2) * 8;
+  std::vector<char> host(std::max<size_t>(bytes_, 16), 0);
+  if (!all.empty()) std::memcpy(host.data(), all.data(), groups_offset_);
+  if (!groups.empty()) std::memcpy(host.data() + groups_offset_, groups.data(), groups.size() * sizeof(FlipGroup));
+  if (!prog.amp_re.empty()) {
+    std::memcpy(host.data() + amp_offset_, prog.amp_re.data(), prog.amp_re.size() * sizeof(double));
+    std::memcpy(host.data() + amp_offset_ + prog.amp_re.size() * sizeof(double), prog.amp_im.data(),
+                prog.amp_im.size() * sizeof(double));
+  }
+  if (!prog.diag_pairs.empty())
+    std::memcpy(host.data() + pairs_offset_, prog.diag_pairs.data(), prog.diag_pairs.size() * sizeof(uint32_t));
+  buf_.allocate(host.size());
+  QMBED_CUDA(cudaMemcpy(buf_.get(), host.data(), host.size(), cudaMemcpyHostToDevice));
 }
 
 namespace {
-
-constexpr int kRankChunkBits = 4;
-constexpr int kRankChunkValues = 1 << kRankChunkBits;
-constexpr size_t kRankTableMaxBytes = 40 * 1024;
-constexpr int kMaxFences = 4096;
-constexpr size_t kProgramSmemMax = 32 * 1024;
-constexpr int kTileThreads = 256;
-constexpr uint64_t kAllOnes = ~0ull;
 
 // ---------------------------------------------------------------------------
 // Device helpers
@@ -134,17 +335,40 @@ constexpr uint64_t kAllOnes = ~0ull;
 // Colex rank from 4-bit chunk tables: tab[(c * 16 + v) * stride + k] is the
 // rank contribution of the set bits v of chunk c when k set bits lie below
 // it (fixed_weight_state_index, src/basis/mod.rs:640-659, summed per chunk).
+// The set bits below each chunk come from a masked popcount, so the chunk
+// reads do not wait on one another.
 __device__ __forceinline__ uint64_t rank_chunked(uint64_t t, const uint64_t* __restrict__ tab, int chunks,
                                                  int stride) {
   uint64_t r = 0;
-  int ones = 0;
 #pragma unroll 4
   for (int c = 0; c < chunks; ++c) {
     const unsigned v = static_cast<unsigned>(t >> (kRankChunkBits * c)) & (kRankChunkValues - 1);
+    const int ones = __popcll(t & ((1ull << (kRankChunkBits * c)) - 1));
     r += tab[(c * kRankChunkValues + v) * stride + ones];
-    ones += __popc(v);
   }
   return r;
+}
+
+// Rank of t = s ^ flip from the rank of s when both have the same weight:
+// only chunks lo..hi (those holding flipped bits, and the ones between them)
+// change their contribution.
+__device__ __forceinline__ uint64_t rank_delta(uint64_t s, uint64_t t, uint64_t rank_s, int lo, int hi,
+                                               const uint64_t* __restrict__ tab, int stride) {
+  uint64_t r = rank_s;
+  const uint64_t below = (1ull << (kRankChunkBits * lo)) - 1;
+  int ones_s = __popcll(s & below), ones_t = ones_s;
+  for (int c = lo; c <= hi; ++c) {
+    const unsigned vs = static_cast<unsigned>(s >> (kRankChunkBits * c)) & (kRankChunkValues - 1);
+    const unsigned vt = static_cast<unsigned>(t >> (kRankChunkBits * c)) & (kRankChunkValues - 1);
+    r += tab[(c * kRankChunkValues + vt) * stride + ones_t] - tab[(c * kRankChunkValues + vs) * stride + ones_s];
+    ones_s += __popc(vs);
+    ones_t += __popc(vt);
+  }
+  return r;
+}
+
+__device__ __forceinline__ int digit_pair(uint64_t s, uint32_t i, uint32_t j) {
+  return static_cast<int>((s >> i) & 1) | (static_cast<int>((s >> j) & 1) << 1);
 }
 
 struct TileArgs {
@@ -153,11 +377,11 @@ struct TileArgs {
   uint64_t dim;
   const uint64_t* states;
   const uint16_t* orbits;
-  // program
-  const FlipTerm* terms;
-  const FlipGroup* groups;
-  int n_diag, n_terms, n_groups;
-  int prog_smem;
+  // program (copied to shared memory by every block)
+  const unsigned long long* program;
+  int program_words;
+  int n_dterms, n_terms, n_groups, n_slots, n_dpairs;
+  int groups_offset, amp_offset, pairs_offset;  // bytes
   // lookups
   const uint64_t* rank_tab;  // chunk tables (shared memory copy in the kernel)
   int rank_chunks, rank_stride;
@@ -178,17 +402,25 @@ struct TileArgs {
   const void* pv;
   void* y;
   double alpha, beta, gamma;
+  ChainProgram chain;
+  int binom_rows;  // chain path: C(n, k), n < binom_rows, k <= up, staged in shared memory
 };
 
 enum TileMode : int { kModeDirect = 0, kModeColex = 1, kModeTable = 2, kModeSearch = 3 };
 
-// Amplitude of group g (or of the diagonal when `first`..`count` span the
-// diagonal terms) on state s: sum_k [s & req == val] k (-1)^popc(~s & sign).
+// Shared-memory view of a flip program.
+struct Program {
+  const FlipTerm* terms;
+  const FlipGroup* groups;
+  const double* amp_re;
+  const double* amp_im;
+  const uint32_t* pairs;
+};
+
+// Sum over generic terms [first, first + count) of [s & req == val] k (-1)^popc(~s & sign).
 template <bool CPLX>
-__device__ __forceinline__ void group_amplitude(const FlipTerm* __restrict__ terms, uint32_t first, uint32_t count,
+__device__ __forceinline__ void terms_amplitude(const FlipTerm* __restrict__ terms, uint32_t first, uint32_t count,
                                                 uint64_t s, double& ar, double& ai) {
-  ar = 0.0;
-  ai = 0.0;
   for (uint32_t i = first; i < first + count; ++i) {
     const FlipTerm& t = terms[i];
     if ((s & t.req_mask) != t.req_val) continue;
@@ -198,10 +430,24 @@ __device__ __forceinline__ void group_amplitude(const FlipTerm* __restrict__ ter
   }
 }
 
-__device__ __forceinline__ bool group_active(const FlipTerm* __restrict__ terms, uint32_t first, uint32_t count,
-                                             uint64_t s) {
+template <bool CPLX>
+__device__ __forceinline__ void group_amplitude(const Program& pg, const FlipGroup& g, uint64_t s, double& ar,
+                                                double& ai) {
+  ar = 0.0;
+  ai = 0.0;
+  if (g.kind == kGroupPair) {
+    const int v = digit_pair(s, g.site_i, g.site_j);
+    ar = pg.amp_re[4 * g.first + v];
+    if (CPLX) ai = pg.amp_im[4 * g.first + v];
+  } else {
+    terms_amplitude<CPLX>(pg.terms, g.first, g.count, s, ar, ai);
+  }
+}
+
+__device__ __forceinline__ bool group_active(const Program& pg, const FlipGroup& g, uint64_t s) {
+  if (g.kind == kGroupPair) return (g.nz >> digit_pair(s, g.site_i, g.site_j)) & 1;
   bool any = false;
-  for (uint32_t i = first; i < first + count; ++i) any |= (s & terms[i].req_mask) == terms[i].req_val;
+  for (uint32_t i = g.first; i < g.first + g.count; ++i) any |= (s & pg.terms[i].req_mask) == pg.terms[i].req_val;
   return any;
 }
 
@@ -213,10 +459,19 @@ struct Hit {
   double inv_sqrt_rc;
 };
 
+// Rank of target t (same weight as the row state s): incremental over the
+// chunks the flip touches when they are few, else from scratch.
+__device__ __forceinline__ uint64_t target_rank(const TileArgs& a, const uint64_t* __restrict__ s_rank, uint64_t s,
+                                                uint64_t t, uint64_t rank_s, int lo, int hi) {
+  return hi - lo <= 2 ? rank_delta(s, t, rank_s, lo, hi, s_rank, a.rank_stride)
+                      : rank_chunked(t, s_rank, a.rank_chunks, a.rank_stride);
+}
+
 template <int U, int MODE, bool NEED_R>
 __device__ __forceinline__ void lookup_batch(const TileArgs& a, const uint64_t* __restrict__ s_rank,
-                                             const uint64_t* __restrict__ s_fence, const bool (&act)[U],
-                                             const uint64_t (&t)[U], Hit (&h)[U]) {
+                                             const uint64_t* __restrict__ s_fence, uint64_t s, uint64_t rank_s,
+                                             const bool (&act)[U], const uint64_t (&t)[U], const int (&lo)[U],
+                                             const int (&hi)[U], const uint64_t (&rank_t)[U], Hit (&h)[U]) {
 #pragma unroll
   for (int u = 0; u < U; ++u) h[u] = Hit{-1, 1.0, 0.0, 1.0};
   if (MODE == kModeDirect) {
@@ -227,8 +482,9 @@ __device__ __forceinline__ void lookup_batch(const TileArgs& a, const uint64_t* 
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (!act[u] || __popcll(t[u]) != a.p.up) continue;
-      h[u].col = a.rank_chunks > 0 ? static_cast<int64_t>(rank_chunked(t[u], s_rank, a.rank_chunks, a.rank_stride))
-                                   : colex_rank_checked(t[u], a.p.sites, a.p.up, a.binom);
+      if (rank_t[u] != kAllOnes) h[u].col = static_cast<int64_t>(rank_t[u]);
+      else h[u].col = a.rank_chunks > 0 ? static_cast<int64_t>(target_rank(a, s_rank, s, t[u], rank_s, lo[u], hi[u]))
+                                        : colex_rank_checked(t[u], a.p.sites, a.p.up, a.binom);
     }
   } else if (MODE == kModeTable) {
     uint64_t e[U];
@@ -237,8 +493,10 @@ __device__ __forceinline__ void lookup_batch(const TileArgs& a, const uint64_t* 
     for (int u = 0; u < U; ++u) {
       e[u] = kAllOnes;
       if (!act[u]) continue;
-      if (a.p.up >= 0 && __popcll(t[u]) != a.p.up) continue;
-      const uint64_t rank = a.p.up >= 0 ? rank_chunked(t[u], s_rank, a.rank_chunks, a.rank_stride) : t[u];
+      if (a.p.up >= 0 && rank_t[u] == kAllOnes && __popcll(t[u]) != a.p.up) continue;
+      const uint64_t rank = a.p.up < 0 ? t[u]
+                            : rank_t[u] != kAllOnes ? rank_t[u]
+                                                    : target_rank(a, s_rank, s, t[u], rank_s, lo[u], hi[u]);
       if (a.table_wide) {
         e[u] = __ldg(static_cast<const unsigned long long*>(a.table) + rank);
       } else {
@@ -325,142 +583,260 @@ __device__ __forceinline__ void lookup_batch(const TileArgs& a, const uint64_t* 
   }
 }
 
-// Gathers per target: U entries in flight per lane.
+// Targets per lane per round: U lookups (and gathers) in flight per lane.
 template <typename T, int NB, bool CPLX>
 struct TileShape {
-  static constexpr int U = NB == 1 ? 8 : (NB * sizeof(T) <= 32 ? 4 : (NB * sizeof(T) <= 64 ? 2 : 1));
+  static constexpr int U = NB == 1 ? 4 : (NB * sizeof(T) <= 32 ? 4 : (NB * sizeof(T) <= 64 ? 2 : 1));
+  static constexpr int MIN_BLOCKS = NB == 1 ? 3 : 2;
 };
 
-// One warp per tile of 32 consecutive rows, one lane per row. Each lane
-// marks its row's active flip groups in a bit mask; the warp then pops U
-// groups per lane per round, so every lane stays busy until the row with the
-// most transitions in the tile is done. NB = 1 computes y = H x (orbit ratio
-// sqrt(R_r / R_c) applied, x real or interleaved complex); NB = 8/16 computes
-// the block action in orbit-scaled coordinates with the three-term epilogue.
-template <typename T, int NB, bool CPLX, int MODE, bool HAS_P>
-__global__ void __launch_bounds__(kTileThreads, 2) hv_tile_kernel(const TileArgs a) {
-  constexpr int U = TileShape<T, NB, CPLX>::U;
+// Resolves a round of U targets and accumulates their contributions:
+// acc += w chi / sqrt(R_c) x[c] (NB = 1) or acc[:] += w chi z[c][:] (blocks).
+template <typename T, int NB, bool CPLX, int MODE, int U>
+__device__ __forceinline__ void consume_round(const TileArgs& a, const uint64_t* __restrict__ s_rank,
+                                              const uint64_t* __restrict__ s_fence, uint64_t s, uint64_t rank_s,
+                                              const bool (&act)[U], const uint64_t (&t)[U], const int (&lo)[U],
+                                              const int (&hi)[U], const double (&wr)[U], const double (&wi)[U],
+                                              const T* __restrict__ x, T (&acc)[NB], T& acc_i,
+                                              const uint64_t (&rank_t)[U]) {
   constexpr bool NEED_R = NB == 1;
   constexpr int VEC = 16 / sizeof(T);
   constexpr int PARTS = NB >= VEC ? NB / VEC : 1;
-  extern __shared__ __align__(16) unsigned char smem[];
-  // shared memory: [program terms][groups][rank chunk table][fence keys]
-  const size_t prog_bytes = a.prog_smem ? a.n_terms * sizeof(FlipTerm) + a.n_groups * sizeof(FlipGroup) : 0;
-  const size_t rank_words = (MODE == kModeColex || MODE == kModeTable) && a.rank_chunks > 0
-                                ? static_cast<size_t>(a.rank_chunks) * kRankChunkValues * a.rank_stride
-                                : 0;
-  unsigned long long* words = reinterpret_cast<unsigned long long*>(smem);
-  if (a.prog_smem) {
-    const unsigned long long* src_t = reinterpret_cast<const unsigned long long*>(a.terms);
-    const size_t tw = a.n_terms * sizeof(FlipTerm) / 8;
-    for (size_t i = threadIdx.x; i < tw; i += blockDim.x) words[i] = src_t[i];
-    const unsigned long long* src_g = reinterpret_cast<const unsigned long long*>(a.groups);
-    const size_t gw = a.n_groups * sizeof(FlipGroup) / 8;
-    for (size_t i = threadIdx.x; i < gw; i += blockDim.x) words[tw + i] = src_g[i];
+  Hit h[U];
+  lookup_batch<U, MODE, NEED_R>(a, s_rank, s_fence, s, rank_s, act, t, lo, hi, rank_t, h);
+  if (NB == 1) {
+    T gr[U], gi[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      gr[u] = 0;
+      gi[u] = 0;
+      if (h[u].col < 0) continue;
+      if (CPLX) {
+        gr[u] = __ldg(x + 2 * h[u].col);
+        gi[u] = __ldg(x + 2 * h[u].col + 1);
+      } else {
+        gr[u] = __ldg(x + h[u].col);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (h[u].col < 0) continue;
+      if (CPLX) {
+        // w * chi / sqrt(R_c)
+        const double fr = (wr[u] * h[u].cr - wi[u] * h[u].ci) * h[u].inv_sqrt_rc;
+        const double fi = (wr[u] * h[u].ci + wi[u] * h[u].cr) * h[u].inv_sqrt_rc;
+        acc[0] += static_cast<T>(fr) * gr[u] - static_cast<T>(fi) * gi[u];
+        acc_i += static_cast<T>(fr) * gi[u] + static_cast<T>(fi) * gr[u];
+      } else {
+        // real operators: chi = +-1
+        acc[0] += static_cast<T>(wr[u] * h[u].cr * h[u].inv_sqrt_rc) * gr[u];
+      }
+    }
+  } else {
+    T g[U][NB];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (h[u].col < 0) {
+#pragma unroll
+        for (int j = 0; j < NB; ++j) g[u][j] = 0;
+        continue;
+      }
+      const T* row = x + static_cast<uint64_t>(h[u].col) * NB;
+#pragma unroll
+      for (int q = 0; q < PARTS; ++q) {
+        T v[VEC];
+        load16(row + q * VEC, v);
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) g[u][q * VEC + j] = v[j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      // real operators: the entry is w * chi, chi = +-1
+      const T c = h[u].col < 0 ? static_cast<T>(0) : static_cast<T>(wr[u] * h[u].cr);
+#pragma unroll
+      for (int j = 0; j < NB; ++j) acc[j] += c * g[u][j];
+    }
   }
-  uint64_t* s_rank = reinterpret_cast<uint64_t*>(smem + prog_bytes);
+}
+
+// State rotated so that bit i holds digit (i + d) mod L.
+__device__ __forceinline__ uint64_t digits_ahead(uint64_t s, int d, int sites, uint64_t mask) {
+  return ((s >> d) | (s << (sites - d))) & mask;
+}
+
+// One warp per tile of 32 consecutive rows, one lane per row. Each lane
+// marks its row's active transitions in a bit mask; the warp then pops U of
+// them per lane per round, so every lane stays busy until the row with the
+// most transitions in the tile is done. CHAIN programs take their masks and
+// diagonal from word operations per bond class; others visit their groups.
+// NB = 1 computes y = H x (orbit ratio sqrt(R_r / R_c) applied, x real or
+// interleaved complex); NB = 8/16 computes the block action in orbit-scaled
+// coordinates with the three-term epilogue.
+template <typename T, int NB, bool CPLX, int MODE, bool HAS_P, bool CHAIN>
+__global__ void __launch_bounds__(kTileThreads, TileShape<T, NB, CPLX>::MIN_BLOCKS)
+    hv_tile_kernel(const __grid_constant__ TileArgs a) {
+  constexpr int U = TileShape<T, NB, CPLX>::U;
+  constexpr int VEC = 16 / sizeof(T);
+  constexpr int PARTS = NB >= VEC ? NB / VEC : 1;
+  constexpr bool RANKED = MODE == kModeColex || MODE == kModeTable;
+  extern __shared__ __align__(16) unsigned char smem[];
+  // shared memory: [flip program][rank chunk table][fence keys]
+  unsigned long long* words = reinterpret_cast<unsigned long long*>(smem);
+  for (int i = threadIdx.x; i < a.program_words; i += blockDim.x) words[i] = a.program[i];
+  const size_t rank_words =
+      RANKED && a.rank_chunks > 0 ? static_cast<size_t>(a.rank_chunks) * kRankChunkValues * a.rank_stride : 0;
+  uint64_t* s_rank = reinterpret_cast<uint64_t*>(words + a.program_words);
   for (size_t i = threadIdx.x; i < rank_words; i += blockDim.x) s_rank[i] = a.rank_tab[i];
   uint64_t* s_fence = s_rank + rank_words;
   if (MODE == kModeSearch)
     for (int i = threadIdx.x; i < a.n_fences; i += blockDim.x) s_fence[i] = a.fences[i];
+  // chain path of ranked lookups: binomials for the nearest-neighbour rank step
+  uint64_t* s_binom = s_fence + (MODE == kModeSearch ? a.n_fences : 0);
+  const int binom_stride = a.p.up + 1;
+  if (CHAIN && RANKED)
+    for (int i = threadIdx.x; i < a.binom_rows * binom_stride; i += blockDim.x)
+      s_binom[i] = a.binom[(i / binom_stride) * kBinomStride + i % binom_stride];
   __syncthreads();
-  const FlipTerm* terms = a.prog_smem ? reinterpret_cast<const FlipTerm*>(smem) : a.terms;
-  const FlipGroup* groups =
-      a.prog_smem ? reinterpret_cast<const FlipGroup*>(smem + a.n_terms * sizeof(FlipTerm)) : a.groups;
+  Program pg;
+  pg.terms = reinterpret_cast<const FlipTerm*>(smem);
+  pg.groups = reinterpret_cast<const FlipGroup*>(smem + a.groups_offset);
+  pg.amp_re = reinterpret_cast<const double*>(smem + a.amp_offset);
+  pg.amp_im = pg.amp_re + 4 * a.n_slots;
+  pg.pairs = reinterpret_cast<const uint32_t*>(smem + a.pairs_offset);
 
   const int lane = threadIdx.x & 31;
+  const int L = a.p.sites;
   const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
   const T* x = static_cast<const T*>(a.x);
+  const bool ranked_rows = RANKED && a.p.up >= 0 && a.rank_chunks > 0;
   for (uint64_t tile = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 32 < a.dim;
        tile += warps) {
     const uint64_t r = tile * 32 + lane;
     const bool valid = r < a.dim;
     uint64_t s = 0;
     if (valid) s = MODE == kModeDirect ? r : __ldcs(a.states + r);
+    const uint64_t rank_s = ranked_rows ? rank_chunked(s, s_rank, a.rank_chunks, a.rank_stride) : 0;
     double dr = 0.0, di = 0.0;
-    if (valid) group_amplitude<CPLX>(terms, 0, a.n_diag, s, dr, di);
     T acc[NB], acc_i = 0;
 #pragma unroll
     for (int j = 0; j < NB; ++j) acc[j] = 0;
-    for (int g0 = 0; g0 < a.n_groups; g0 += 64) {
-      const int gn = min(64, a.n_groups - g0);
-      uint64_t active = 0;
-      if (valid)
-        for (int g = 0; g < gn; ++g) {
-          const FlipGroup grp = groups[g0 + g];
-          if (group_active(terms, grp.first, grp.count, s)) active |= 1ull << g;
+    if (CHAIN) {
+      const ChainProgram& ch = a.chain;
+      if (valid) {
+        if (ch.has_field) {
+          const int ones = __popcll(s & ch.field_mask), zeros = __popcll(~s & ch.field_mask);
+          dr += zeros * ch.field_re[0] + ones * ch.field_re[1];
+          if (CPLX) di += zeros * ch.field_im[0] + ones * ch.field_im[1];
         }
-      while (__any_sync(0xffffffffu, active != 0)) {
-        bool act[U];
-        uint64_t t[U];
-        double wr[U], wi[U];
+        for (int c = 0; c < ch.n_diag; ++c) {
+          const ChainClass& cl = ch.diag[c];
+          const uint64_t b = digits_ahead(s, cl.d, L, a.mask);
+          const int n[4] = {__popcll(~s & ~b & cl.bonds), __popcll(s & ~b & cl.bonds), __popcll(~s & b & cl.bonds),
+                            __popcll(s & b & cl.bonds)};
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          act[u] = active != 0;
-          t[u] = 0;
-          wr[u] = 0.0;
-          wi[u] = 0.0;
-          if (!act[u]) continue;
-          const int g = __ffsll(static_cast<long long>(active)) - 1;
-          active &= active - 1;
-          const FlipGroup grp = groups[g0 + g];
-          group_amplitude<CPLX>(terms, grp.first, grp.count, s, wr[u], wi[u]);
-          t[u] = s ^ grp.flip;
+          for (int v = 0; v < 4; ++v) {
+            dr += n[v] * cl.re[v];
+            if (CPLX) di += n[v] * cl.im[v];
+          }
         }
-        Hit h[U];
-        lookup_batch<U, MODE, NEED_R>(a, s_rank, s_fence, act, t, h);
-        if (NB == 1) {
-          T gr[U], gi[U];
+      }
+      for (int c = 0; c < ch.n_off; ++c) {
+        const ChainClass& cl = ch.off[c];
+        const uint64_t b = digits_ahead(s, cl.d, L, a.mask);
+        uint64_t active = 0;
+        if (valid) {
+          if (cl.nz & 1) active |= ~s & ~b;
+          if (cl.nz & 2) active |= s & ~b;
+          if (cl.nz & 4) active |= ~s & b;
+          if (cl.nz & 8) active |= s & b;
+          active &= cl.bonds;
+        }
+        while (__any_sync(0xffffffffu, active != 0)) {
+          bool act[U];
+          uint64_t t[U];
+          int lo[U], hi[U];
+          double wr[U], wi[U];
+#pragma unroll
+          uint64_t rank_t[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
-            gr[u] = 0;
-            gi[u] = 0;
-            if (h[u].col < 0) continue;
-            if (CPLX) {
-              gr[u] = __ldg(x + 2 * h[u].col);
-              gi[u] = __ldg(x + 2 * h[u].col + 1);
-            } else {
-              gr[u] = __ldg(x + h[u].col);
+            act[u] = active != 0;
+            t[u] = 0;
+            lo[u] = 0;
+            hi[u] = 0;
+            wr[u] = 0.0;
+            wi[u] = 0.0;
+            rank_t[u] = kAllOnes;
+            if (!act[u]) continue;
+            // the bond's first site as a one-bit mask, its partner d sites ahead
+            const uint64_t first = active & (0ull - active);
+            active ^= first;
+            const uint64_t partner = ((first << cl.d) | (first >> (L - cl.d))) & a.mask;
+            const bool d0 = (s & first) != 0, d1 = (s & partner) != 0;
+            const int v = (d0 ? 1 : 0) | (d1 ? 2 : 0);
+            wr[u] = cl.re[v];
+            if (CPLX) wi[u] = cl.im[v];
+            t[u] = s ^ first ^ partner;
+            const uint64_t below = first - 1;
+            const int i = __popcll(below);
+            const int j = partner > first ? i + cl.d : i + cl.d - L;
+            lo[u] = min(i, j) >> 2;
+            hi[u] = max(i, j) >> 2;
+            if (RANKED && ranked_rows && cl.d == 1 && partner > first) {
+              // one up spin hops between neighbours i, i+1 with k up spins below:
+              // the colex rank moves by C(i, k) (up) or -C(i, k) (down)
+              const uint64_t step = s_binom[i * binom_stride + __popcll(s & below)];
+              rank_t[u] = d0 ? rank_s + step : rank_s - step;
             }
           }
+          consume_round<T, NB, CPLX, MODE, U>(a, s_rank, s_fence, s, rank_s, act, t, lo, hi, wr, wi, x, acc, acc_i,
+                                              rank_t);
+        }
+      }
+    } else {
+      if (valid) {
+        for (int q = 0; q < a.n_dpairs; ++q) {
+          const uint32_t ij = pg.pairs[q];
+          const int v = digit_pair(s, ij & 0xff, ij >> 8);
+          dr += pg.amp_re[4 * q + v];
+          if (CPLX) di += pg.amp_im[4 * q + v];
+        }
+        terms_amplitude<CPLX>(pg.terms, 0, a.n_dterms, s, dr, di);
+      }
+      for (int g0 = 0; g0 < a.n_groups; g0 += 64) {
+        const int gn = min(64, a.n_groups - g0);
+        uint64_t active = 0;
+        if (valid)
+          for (int g = 0; g < gn; ++g)
+            if (group_active(pg, pg.groups[g0 + g], s)) active |= 1ull << g;
+        while (__any_sync(0xffffffffu, active != 0)) {
+          bool act[U];
+          uint64_t t[U];
+          int lo[U], hi[U];
+          double wr[U], wi[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
-            if (h[u].col < 0) continue;
-            // w * chi / sqrt(R_c)
-            const double fr = (wr[u] * h[u].cr - wi[u] * h[u].ci) * h[u].inv_sqrt_rc;
-            const double fi = (wr[u] * h[u].ci + wi[u] * h[u].cr) * h[u].inv_sqrt_rc;
-            if (CPLX) {
-              acc[0] += static_cast<T>(fr) * gr[u] - static_cast<T>(fi) * gi[u];
-              acc_i += static_cast<T>(fr) * gi[u] + static_cast<T>(fi) * gr[u];
-            } else {
-              acc[0] += static_cast<T>(fr) * gr[u];
-            }
+            act[u] = active != 0;
+            t[u] = 0;
+            lo[u] = 0;
+            hi[u] = 0;
+            wr[u] = 0.0;
+            wi[u] = 0.0;
+            if (!act[u]) continue;
+            const int g = __ffsll(static_cast<long long>(active)) - 1;
+            active &= active - 1;
+            const FlipGroup& grp = pg.groups[g0 + g];
+            group_amplitude<CPLX>(pg, grp, s, wr[u], wi[u]);
+            t[u] = s ^ grp.flip;
+            lo[u] = grp.chunk_lo;
+            hi[u] = grp.chunk_hi;
           }
-        } else {
-          T g[U][NB];
+          uint64_t rank_t[U];
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            if (h[u].col < 0) {
-#pragma unroll
-              for (int j = 0; j < NB; ++j) g[u][j] = 0;
-              continue;
-            }
-            const T* row = x + static_cast<uint64_t>(h[u].col) * NB;
-#pragma unroll
-            for (int q = 0; q < PARTS; ++q) {
-              T v[VEC];
-              load16(row + q * VEC, v);
-#pragma unroll
-              for (int j = 0; j < VEC; ++j) g[u][q * VEC + j] = v[j];
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            // real operators: the entry is w * chi, chi = +-1
-            const T c = h[u].col < 0 ? static_cast<T>(0) : static_cast<T>(wr[u] * h[u].cr);
-#pragma unroll
-            for (int j = 0; j < NB; ++j) acc[j] += c * g[u][j];
-          }
+          for (int u = 0; u < U; ++u) rank_t[u] = kAllOnes;
+          consume_round<T, NB, CPLX, MODE, U>(a, s_rank, s_fence, s, rank_s, act, t, lo, hi, wr, wi, x, acc, acc_i,
+                                              rank_t);
         }
       }
     }
@@ -837,9 +1213,9 @@ void SpinBasis::table_images(const uint64_t* lo, uint64_t n, int64_t* index, dou
 
 namespace {
 
-template <typename T, int NB, bool CPLX, int MODE, bool HAS_P>
-void launch_one(const TileArgs& a, size_t smem, cudaStream_t stream) {
-  auto kernel = hv_tile_kernel<T, NB, CPLX, MODE, HAS_P>;
+template <typename T, int NB, bool CPLX, int MODE, bool HAS_P, bool CHAIN>
+void launch_chain(const TileArgs& a, size_t smem, cudaStream_t stream) {
+  auto kernel = hv_tile_kernel<T, NB, CPLX, MODE, HAS_P, CHAIN>;
   // resident blocks per SM for this instantiation, cached per (device, smem)
   static thread_local int cached_device = -1;
   static thread_local size_t cached_smem = 0;
@@ -863,29 +1239,35 @@ void launch_one(const TileArgs& a, size_t smem, cudaStream_t stream) {
   QMBED_LAUNCH_CHECK();
 }
 
+template <typename T, int NB, bool CPLX, int MODE, bool HAS_P>
+void launch_one(const TileArgs& a, size_t smem, cudaStream_t stream, bool chain) {
+  if (chain) launch_chain<T, NB, CPLX, MODE, HAS_P, true>(a, smem, stream);
+  else launch_chain<T, NB, CPLX, MODE, HAS_P, false>(a, smem, stream);
+}
+
 template <int MODE>
-void dispatch_mode(const TileArgs& a, size_t smem, const TileLaunch& l) {
+void dispatch_mode(const TileArgs& a, size_t smem, const TileLaunch& l, bool chain) {
   const bool hp = l.p != nullptr;
   if (l.nb == 1) {
     if (l.precision == 64) {
-      if (l.complex_vectors) launch_one<double, 1, true, MODE, false>(a, smem, l.stream);
-      else launch_one<double, 1, false, MODE, false>(a, smem, l.stream);
+      if (l.complex_vectors) launch_one<double, 1, true, MODE, false>(a, smem, l.stream, chain);
+      else launch_one<double, 1, false, MODE, false>(a, smem, l.stream, chain);
     } else {
-      if (l.complex_vectors) launch_one<float, 1, true, MODE, false>(a, smem, l.stream);
-      else launch_one<float, 1, false, MODE, false>(a, smem, l.stream);
+      if (l.complex_vectors) launch_one<float, 1, true, MODE, false>(a, smem, l.stream, chain);
+      else launch_one<float, 1, false, MODE, false>(a, smem, l.stream, chain);
     }
     return;
   }
   if (l.precision == 64) {
-    if (l.nb == 8) hp ? launch_one<double, 8, false, MODE, true>(a, smem, l.stream)
-                      : launch_one<double, 8, false, MODE, false>(a, smem, l.stream);
-    else hp ? launch_one<double, 16, false, MODE, true>(a, smem, l.stream)
-            : launch_one<double, 16, false, MODE, false>(a, smem, l.stream);
+    if (l.nb == 8) hp ? launch_one<double, 8, false, MODE, true>(a, smem, l.stream, chain)
+                      : launch_one<double, 8, false, MODE, false>(a, smem, l.stream, chain);
+    else hp ? launch_one<double, 16, false, MODE, true>(a, smem, l.stream, chain)
+            : launch_one<double, 16, false, MODE, false>(a, smem, l.stream, chain);
   } else {
-    if (l.nb == 8) hp ? launch_one<float, 8, false, MODE, true>(a, smem, l.stream)
-                      : launch_one<float, 8, false, MODE, false>(a, smem, l.stream);
-    else hp ? launch_one<float, 16, false, MODE, true>(a, smem, l.stream)
-            : launch_one<float, 16, false, MODE, false>(a, smem, l.stream);
+    if (l.nb == 8) hp ? launch_one<float, 8, false, MODE, true>(a, smem, l.stream, chain)
+                      : launch_one<float, 8, false, MODE, false>(a, smem, l.stream, chain);
+    else hp ? launch_one<float, 16, false, MODE, true>(a, smem, l.stream, chain)
+            : launch_one<float, 16, false, MODE, false>(a, smem, l.stream, chain);
   }
 }
 
@@ -903,12 +1285,17 @@ bool launch_tile(const SpinBasis& basis, const DeviceFlipProgram& prog, int mode
   a.dim = basis.dim();
   a.states = static_cast<const uint64_t*>(basis.states());
   a.orbits = basis.orbits();
-  a.terms = prog.terms();
-  a.groups = prog.groups();
-  a.n_diag = prog.n_diag();
+  if (prog.bytes() > kProgramSmemMax) return false;
+  a.program = static_cast<const unsigned long long*>(prog.data());
+  a.program_words = static_cast<int>((prog.bytes() + 7) / 8);
+  a.n_dterms = prog.n_dterms();
   a.n_terms = prog.n_terms();
   a.n_groups = prog.n_groups();
-  a.prog_smem = prog.bytes() <= kProgramSmemMax ? 1 : 0;
+  a.n_slots = prog.n_slots();
+  a.n_dpairs = prog.n_dpairs();
+  a.groups_offset = static_cast<int>(prog.groups_offset());
+  a.amp_offset = static_cast<int>(prog.amp_offset());
+  a.pairs_offset = static_cast<int>(prog.pairs_offset());
   a.rank_tab = basis.rank_chunk_table();
   a.rank_chunks = basis.rank_chunk_count();
   a.rank_stride = basis.rank_chunk_stride();
@@ -925,7 +1312,7 @@ bool launch_tile(const SpinBasis& basis, const DeviceFlipProgram& prog, int mode
   a.alpha = l.alpha;
   a.beta = l.beta;
   a.gamma = l.gamma;
-  size_t smem = a.prog_smem ? prog.bytes() : 0;
+  size_t smem = static_cast<size_t>(a.program_words) * 8;
   int tile_mode;
   if (basis.direct()) {
     tile_mode = kModeDirect;
@@ -952,11 +1339,20 @@ bool launch_tile(const SpinBasis& basis, const DeviceFlipProgram& prog, int mode
     }
   }
   if (smem > 96 * 1024) return false;
+  const bool chain = prog.chain_ok();
+  if (chain) {
+    a.chain = prog.chain();
+    if ((tile_mode == kModeColex || tile_mode == kModeTable) && p.up >= 0 && a.rank_chunks > 0) {
+      a.binom_rows = p.sites;
+      smem += static_cast<size_t>(p.sites) * (p.up + 1) * 8;
+      if (smem > 96 * 1024) return false;
+    }
+  }
   switch (tile_mode) {
-    case kModeDirect: dispatch_mode<kModeDirect>(a, smem, l); break;
-    case kModeColex: dispatch_mode<kModeColex>(a, smem, l); break;
-    case kModeTable: dispatch_mode<kModeTable>(a, smem, l); break;
-    default: dispatch_mode<kModeSearch>(a, smem, l); break;
+    case kModeDirect: dispatch_mode<kModeDirect>(a, smem, l, chain); break;
+    case kModeColex: dispatch_mode<kModeColex>(a, smem, l, chain); break;
+    case kModeTable: dispatch_mode<kModeTable>(a, smem, l, chain); break;
+    default: dispatch_mode<kModeSearch>(a, smem, l, chain); break;
   }
   return true;
 }

@@ -41,9 +41,43 @@ struct FlipTerm {
   double kr, ki;
 };
 
+enum GroupKind : uint8_t { kGroupGeneric = 0, kGroupPair = 1 };
+
+// Products sharing one flip mask. A pair group's amplitude depends on the
+// digits of two sites only (i <= j, i == j for one site), so it is a 4-entry
+// table indexed by d_i | d_j << 1; generic groups keep their terms.
 struct FlipGroup {
   uint64_t flip;
-  uint32_t first, count;  // terms[first, first + count)
+  uint32_t first;      // generic: first term; pair: amplitude slot
+  uint16_t count;      // generic: term count
+  uint8_t kind;        // GroupKind
+  uint8_t nz;          // pair: bit v set when the amplitude at digits v is nonzero
+  uint8_t site_i, site_j;
+  uint8_t chunk_lo, chunk_hi;  // 4-bit chunks holding the lowest / highest flipped bit
+  uint8_t pad[4];
+};
+static_assert(sizeof(FlipGroup) == 24, "FlipGroup is packed for shared memory");
+
+// Translation-structured form of a program whose products all act on bonds
+// (i, i + d mod L) with the same amplitude table for every bond of one
+// displacement d (uniform chains: Heisenberg, XXZ, J1-J2, XY, DM, ...).
+// For a class, B = state rotated so that bit i of B is digit i + d; the
+// digits of every bond at once are (bit i of s, bit i of B), so activity
+// masks and diagonal sums take a few word operations per class.
+constexpr int kChainMaxOff = 4;
+constexpr int kChainMaxDiag = 6;
+struct ChainClass {
+  uint64_t bonds;  // bit i: bond (i, i + d mod L) present
+  int d;
+  int nz;          // off-diagonal: digit patterns v = d_i | d_{i+d} << 1 with nonzero amplitude
+  double re[4], im[4];
+};
+struct ChainProgram {
+  int n_off = 0, n_diag = 0, has_field = 0, pad = 0;
+  uint64_t field_mask = 0;          // single-site diagonal terms, the same on every site listed
+  double field_re[2] = {0, 0}, field_im[2] = {0, 0};
+  ChainClass off[kChainMaxOff];
+  ChainClass diag[kChainMaxDiag];
 };
 
 // Host-side compiled program; `ok` is false when some product repeats a site
@@ -51,32 +85,47 @@ struct FlipGroup {
 struct FlipProgram {
   bool ok = false;
   bool complex_coefs = false;
-  std::vector<FlipTerm> diag;      // flip == 0
-  std::vector<FlipGroup> groups;   // off-diagonal, ascending flip mask
-  std::vector<FlipTerm> terms;     // terms of the groups
+  std::vector<FlipTerm> diag_terms;   // diagonal products reading three or more sites
+  std::vector<uint32_t> diag_pairs;   // site_i | site_j << 8; amplitude slot = position
+  std::vector<FlipGroup> groups;      // off-diagonal, ascending flip mask
+  std::vector<FlipTerm> terms;        // terms of the generic groups
+  std::vector<double> amp_re, amp_im; // 4 per slot: diagonal pairs first, then pair groups
+  bool chain_ok = false;
+  ChainProgram chain;
 };
 
-FlipProgram compile_flip_program(const std::vector<Instance>& adjoint, const LocalFactors& f, int sites);
+// `fixed_weight`: the basis holds states of one weight, so flips that change
+// the weight are dropped from the activity masks.
+FlipProgram compile_flip_program(const std::vector<Instance>& adjoint, const LocalFactors& f, int sites,
+                                 bool fixed_weight);
 
 enum LookupMode : int { kLookupAuto = 0, kLookupTable = 1, kLookupSearch = 2, kLookupLegacy = 3 };
 
-// Device copy of a flip program: [diag terms][group terms] then the groups.
+// Device copy of a flip program, one buffer the kernel stages in shared
+// memory: [generic terms][groups][amp_re][amp_im][diagonal pair sites].
 class DeviceFlipProgram {
  public:
   void upload(const FlipProgram& prog);
   bool ok() const { return ok_; }
   bool complex_coefs() const { return complex_; }
-  const FlipTerm* terms() const { return buf_.as<FlipTerm>(); }
-  const FlipGroup* groups() const { return reinterpret_cast<const FlipGroup*>(buf_.as<char>() + groups_offset_); }
-  int n_diag() const { return n_diag_; }
+  const void* data() const { return buf_.get(); }
+  size_t bytes() const { return bytes_; }
+  int n_dterms() const { return n_dterms_; }
   int n_terms() const { return n_terms_; }
   int n_groups() const { return n_groups_; }
-  size_t bytes() const { return bytes_; }
+  int n_slots() const { return n_slots_; }
+  int n_dpairs() const { return n_dpairs_; }
+  size_t groups_offset() const { return groups_offset_; }
+  size_t amp_offset() const { return amp_offset_; }
+  size_t pairs_offset() const { return pairs_offset_; }
+  bool chain_ok() const { return chain_ok_; }
+  const ChainProgram& chain() const { return chain_; }
 
  private:
-  bool ok_ = false, complex_ = false;
-  int n_diag_ = 0, n_terms_ = 0, n_groups_ = 0;
-  size_t groups_offset_ = 0, bytes_ = 0;
+  bool ok_ = false, complex_ = false, chain_ok_ = false;
+  ChainProgram chain_;
+  int n_dterms_ = 0, n_terms_ = 0, n_groups_ = 0, n_slots_ = 0, n_dpairs_ = 0;
+  size_t groups_offset_ = 0, amp_offset_ = 0, pairs_offset_ = 0, bytes_ = 0;
   DeviceBuffer buf_;
 };
 

@@ -1064,7 +1064,7 @@ void SpinOperator::build_instances(const std::vector<TermDesc>& terms, const Ope
       nnz_off_ = flips * dim();
     }
   }
-  if (basis_->words() == 1) prog_.upload(compile_flip_program(adj, factors_, sites));
+  if (basis_->words() == 1) prog_.upload(compile_flip_program(adj, factors_, sites, basis_->params().up >= 0));
   inst_adj_.allocate(std::max<size_t>(adj.size(), 1) * sizeof(Instance));
   inst_fwd_.allocate(std::max<size_t>(fwd.size(), 1) * sizeof(Instance));
   if (!adj.empty()) {

@@ -148,6 +148,9 @@ class SpinOperator {
   // What the on-the-fly action runs now: 1 table, 2 search, 3 legacy,
   // 4 direct/colex (no symmetry).
   int lookup_in_use() const;
+  // True when the on-the-fly action takes the translation-structured (chain)
+  // form of its flip program.
+  bool chain_form() const { return prog_.ok() && prog_.chain_ok(); }
 
  private:
   void build_instances(const std::vector<TermDesc>& terms, const OperatorChecks& checks);

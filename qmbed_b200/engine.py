@@ -229,11 +229,11 @@ class GpuOperator:
         check(lib().qmbed_gpu_operator_set_lookup(self.handle, LOOKUPS[mode]))
 
     def lookup_info(self) -> dict:
-        in_use, nbytes, seconds = ctypes.c_int(), ctypes.c_uint64(), ctypes.c_double()
-        check(lib().qmbed_gpu_operator_lookup_info(self.handle, ctypes.byref(in_use), ctypes.byref(nbytes),
-                                                   ctypes.byref(seconds)))
-        return {"lookup": LOOKUPS_IN_USE.get(in_use.value, "none"), "table_bytes": nbytes.value,
-                "table_seconds": seconds.value}
+        in_use, chain, nbytes, seconds = ctypes.c_int(), ctypes.c_int(), ctypes.c_uint64(), ctypes.c_double()
+        check(lib().qmbed_gpu_operator_lookup_info(self.handle, ctypes.byref(in_use), ctypes.byref(chain),
+                                                   ctypes.byref(nbytes), ctypes.byref(seconds)))
+        return {"lookup": LOOKUPS_IN_USE.get(in_use.value, "none"), "chain_form": bool(chain.value),
+                "table_bytes": nbytes.value, "table_seconds": seconds.value}
 
     def operand_bytes(self, precision: int = 64, complex_vectors: bool = False) -> float:
         value = ctypes.c_double()

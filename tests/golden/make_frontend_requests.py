@@ -10,9 +10,10 @@ scripts, and writes every request, in order, to
 replays the file through ``libqmbed_b200.so`` and checks each answer against
 the oracle, so the GPU tests need neither the reference nor its frontend.
 
-    python tests/golden/make_frontend_requests.py [reference checkout]
+    python tests/golden/make_frontend_requests.py <reference checkout>
 
-The checkout defaults to ``$QMBED_REFERENCE`` or ``/root/reference``.
+The checkout may instead be given as ``$QMBED_REFERENCE``; one of the two is
+required.
 """
 
 from __future__ import annotations
@@ -198,7 +199,10 @@ def scenarios(qmbed):
 
 
 def main() -> None:
-    checkout = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("QMBED_REFERENCE", "/root/reference"))
+    location = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("QMBED_REFERENCE")
+    if not location:
+        sys.exit("usage: make_frontend_requests.py <reference checkout>  (or set QMBED_REFERENCE)")
+    checkout = Path(location)
     qmbed, ffi = reference_frontend(checkout)
     out = {}
     for name, scenario in scenarios(qmbed).items():

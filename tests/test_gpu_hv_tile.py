@@ -163,7 +163,7 @@ def test_table_images_equal_canonical_images(engine, sites, up, momentum, parity
     tindex, tphase, torbit = basis.table_images(states)
     assert np.array_equal(index, tindex)
     assert np.array_equal(orbit, torbit)
-    assert np.max(np.abs(phase - tphase)) <= 1e-15
+    assert np.max(np.abs(phase - tphase)) <= 4e-15
 
 
 def test_repeated_site_products_take_the_legacy_expansion(engine, oracle):
@@ -173,6 +173,33 @@ def test_repeated_site_products_take_the_legacy_expansion(engine, oracle):
     g = engine.GpuOperator(engine.GpuBasis(sites, up=6, momentum=0, parity=1), terms, storage="matrix_free")
     assert g.lookup_info()["lookup"] == "legacy"
     x = np.random.default_rng(1).normal(size=o.dim)
+    expected = o.apply(x).real
+    assert np.linalg.norm(g.apply(x) - expected) <= 1e-13 * np.linalg.norm(expected)
+
+
+@pytest.mark.parametrize("model,chain", [("heisenberg", True), ("j1j2", True), ("xy_y", True), ("dm", True),
+                                         ("tfim_uniform", False), ("tfim_fields", False)])
+def test_chain_form_detection(engine, model, chain):
+    """Uniform bond models take the translation-structured expansion; single-site
+    flips and non-uniform couplings keep the per-group expansion."""
+    sites = 12
+    up = None if model.startswith("tfim") else 6
+    norm = "pauli_cartesian" if model.startswith("tfim") else "angular_momentum"
+    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, normalization=norm), _models(sites)[model],
+                           storage="matrix_free", check_particles=not model.startswith("tfim"))
+    assert g.lookup_info()["chain_form"] is chain
+
+
+def test_open_chain_with_uniform_fields_matches_oracle(engine, oracle):
+    """Open boundary (a partial bond mask) and a uniform longitudinal field in the chain form."""
+    sites = 14
+    bonds = [(i, i + 1) for i in range(sites - 1)]
+    terms = [("zz", [(0.9, b) for b in bonds]), ("+-", [(0.5, b) for b in bonds]), ("-+", [(0.5, b) for b in bonds]),
+             ("z", [(0.37, (i,)) for i in range(sites)])]
+    o = oracle.Operator.build(oracle.Basis(sites, up=7), terms)
+    g = engine.GpuOperator(engine.GpuBasis(sites, up=7), terms, storage="matrix_free")
+    assert g.lookup_info()["chain_form"]
+    x = np.random.default_rng(2).normal(size=o.dim)
     expected = o.apply(x).real
     assert np.linalg.norm(g.apply(x) - expected) <= 1e-13 * np.linalg.norm(expected)
 
