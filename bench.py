@@ -185,6 +185,16 @@ def xxz_section(sites: int, rank: int, local_rank: int) -> dict:
                      "max_rel_error_vs_fp64": float(np.max(np.abs(r.eigenvalues - ref) / np.abs(ref))),
                      "max_residual": float(np.max(r.residuals))}
     out["eigenvalues_fp64"] = ref.tolist()
+    # the oracle's eigenvalues of this workload, computed off line (tests/golden/config_fixtures.json)
+    fixture = ROOT / "tests" / "golden" / "config_fixtures.json"
+    if fixture.exists():
+        xxz = json.loads(fixture.read_text()).get("xxz", {})
+        if xxz.get("sites") == sites and xxz.get("seed") == seed and abs(xxz.get("delta", 0.0) - delta) < 1e-15:
+            oracle_values = np.asarray(xxz["eigenvalues"])
+            for mode in runs:
+                out[mode]["max_rel_error_vs_oracle"] = float(np.max(np.abs(runs[mode][1].eigenvalues - oracle_values)
+                                                                    / np.abs(oracle_values)))
+            out["eigenvalues_oracle"] = oracle_values.tolist()
     return out
 
 

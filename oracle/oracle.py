@@ -11,6 +11,7 @@ exponential-action plan.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 from dataclasses import dataclass
@@ -63,6 +64,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_basis_dim.restype = ll
         L.oracle_basis_states.argtypes = [vp, vp, vp, vp]
         L.oracle_basis_image.argtypes = [vp, u64, u64, P(u64), P(u64), P(d), P(u64)]
+        L.oracle_orbit_images.argtypes = [i, i, i, i, ctypes.c_longlong, vp, vp, vp, vp, vp, vp]
         L.oracle_operator_build.argtypes = [vp, i, vp, ctypes.c_char_p, vp, vp, vp, i, i, P(vp)]
         L.oracle_operator_from_triplets.argtypes = [ll, ll, vp, vp, vp, P(vp)]
         L.oracle_operator_free.argtypes = [vp]
@@ -144,6 +146,69 @@ class Basis:
         if not found:
             return None
         return (rep_hi.value << 64) | rep_lo.value, complex(phase[0], phase[1]), orbit.value
+
+
+def orbit_images(sites: int, states, momentum: int | None = None, parity: int | None = None):
+    """Reduction images of physical states by the reference's per-orbit rule
+    (spin_symmetry_sector, src/basis/mod.rs:760-841, one orbit at a time):
+    (representative, phase, orbit size); orbit size 0 when the state's orbit
+    is not in the sector. For sectors too large for the full lookup."""
+    states = np.ascontiguousarray(states, np.uint64)
+    n = len(states)
+    rep_lo = np.zeros(n, np.uint64)
+    rep_hi = np.zeros(n, np.uint64)
+    phase = np.zeros(n, np.complex128)
+    orbit = np.zeros(n, np.uint64)
+    _check(lib().oracle_orbit_images(sites, 0 if momentum is None else 1, 0 if momentum is None else momentum,
+                                     0 if parity is None else parity, n, _ptr(states), None, _ptr(rep_lo),
+                                     _ptr(rep_hi), _ptr(phase), _ptr(orbit)))
+    return rep_lo, phase, orbit
+
+
+def _fixed_weight_count(cycles, weight):
+    """States of the given weight fixed by a site permutation with these cycle lengths."""
+    poly = [1] + [0] * weight
+    for c in cycles:
+        nxt = poly[:]
+        for w in range(weight - c + 1):
+            nxt[w + c] += poly[w]
+        poly = nxt
+    return poly[weight]
+
+
+def _cycles(perm):
+    seen, out = set(), []
+    for start in range(len(perm)):
+        if start in seen:
+            continue
+        n, i = 0, start
+        while i not in seen:
+            seen.add(i)
+            i = perm[i]
+            n += 1
+        out.append(n)
+    return out
+
+
+def sector_dimension(sites: int, up: int, momentum: int, parity: int | None) -> int:
+    """Dimension of a momentum (and parity) sector without enumerating it:
+    the multiplicity of the sector's character in the permutation action on
+    weight-`up` states: (1/|G|) sum_g conj(chi(g)) fix(g), over translations T^a
+    (chi = exp(-2 pi i k a / L)) and, with parity p, reflections R T^a (chi = p
+    exp(-2 pi i k a / L))."""
+    total = 0j
+    for a in range(sites):
+        chi = complex(math.cos(2 * math.pi * momentum * a / sites), -math.sin(2 * math.pi * momentum * a / sites))
+        rot = [(i + a) % sites for i in range(sites)]
+        total += chi.conjugate() * _fixed_weight_count(_cycles(rot), up)
+        if parity:
+            refl = [sites - 1 - rot[i] for i in range(sites)]
+            total += parity * chi.conjugate() * _fixed_weight_count(_cycles(refl), up)
+    order = sites * (2 if parity else 1)
+    value = total / order
+    assert abs(value.imag) < 1e-6
+    return int(round(value.real))
+
 
 
 def encode_terms(terms):

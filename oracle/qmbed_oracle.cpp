@@ -347,6 +347,52 @@ struct SpinBasis {
   }
 };
 
+// The per-orbit part of spin_symmetry_sector (src/basis/mod.rs:790-841):
+// projection coefficients of the orbit of `representative` (its minimum),
+// the drop of |c| <= 1e-12, the gauge by the representative's coefficient,
+// the normalisation check and the SymmetryImage of every member. Returns
+// false when the projection vanishes (the orbit is not in the sector).
+template <typename Lookup>
+bool project_orbit(u128 representative, size_t sites, size_t translations, long normalized, int parity,
+                   bool has_momentum, Lookup& lookup, size_t* orbit_size_out) {
+  std::unordered_map<u128, C64, U128Hash> coefficients;
+  for (size_t shift = 0; shift < translations; ++shift) {
+    double angle = has_momentum ? -(2.0 * M_PI) * static_cast<double>(normalized * shift) /
+                                      static_cast<double>(sites)
+                                : 0.0;
+    C64 character = std::polar(1.0, angle);
+    u128 translated = rotate_lattice_state(representative, shift, sites);
+    coefficients[translated] += character;
+    if (parity != 0) {
+      u128 reflected = reflect_lattice_state(translated, sites);
+      coefficients[reflected] += static_cast<double>(parity) * character;
+    }
+  }
+  for (auto it = coefficients.begin(); it != coefficients.end();) {
+    if (std::abs(it->second) > 1.0e-12) ++it; else it = coefficients.erase(it);
+  }
+  if (coefficients.empty()) return false;
+  auto rep_it = coefficients.find(representative);
+  if (rep_it == coefficients.end())
+    fail(ERR_INCOMPATIBLE_SYMMETRY, "symmetry projection removed its orbit representative");
+  C64 representative_coefficient = rep_it->second;
+  C64 gauge = representative_coefficient / std::abs(representative_coefficient);
+  double norm_sq = 0.0;
+  for (auto& entry : coefficients) norm_sq += std::norm(entry.second);
+  double norm = std::sqrt(norm_sq);
+  size_t orbit_size = coefficients.size();
+  double expected = 1.0 / std::sqrt(static_cast<double>(orbit_size));
+  for (auto& entry : coefficients) {
+    C64 normalized_value = entry.second / (gauge * norm);
+    if (std::abs(std::abs(normalized_value) - expected) > 1.0e-10)
+      fail(ERR_INCOMPATIBLE_SYMMETRY,
+           "symmetry projection does not define a one-dimensional orbit sector");
+    lookup[entry.first] = {representative, normalized_value / expected, orbit_size};
+  }
+  *orbit_size_out = orbit_size;
+  return true;
+}
+
 // spin_symmetry_sector (src/basis/mod.rs:715-848)
 void spin_symmetry_sector(SpinBasis& basis, std::vector<u128> parent_states, bool has_momentum,
                           long momentum, int parity) {
@@ -392,41 +438,10 @@ void spin_symmetry_sector(SpinBasis& basis, std::vector<u128> parent_states, boo
         fail(ERR_INCOMPATIBLE_SYMMETRY, "symmetry map leaves the selected magnetization sector");
     visited.insert(orbit.begin(), orbit.end());
     u128 representative = *std::min_element(orbit.begin(), orbit.end());
-
-    std::unordered_map<u128, C64, U128Hash> coefficients;
-    for (size_t shift = 0; shift < translations; ++shift) {
-      double angle = has_momentum ? -(2.0 * M_PI) * static_cast<double>(normalized * shift) /
-                                        static_cast<double>(sites)
-                                  : 0.0;
-      C64 character = std::polar(1.0, angle);
-      u128 translated = rotate_lattice_state(representative, shift, sites);
-      coefficients[translated] += character;
-      if (parity != 0) {
-        u128 reflected = reflect_lattice_state(translated, sites);
-        coefficients[reflected] += static_cast<double>(parity) * character;
-      }
-    }
-    for (auto it = coefficients.begin(); it != coefficients.end();) {
-      if (std::abs(it->second) > 1.0e-12) ++it; else it = coefficients.erase(it);
-    }
-    if (coefficients.empty()) continue;
-    auto rep_it = coefficients.find(representative);
-    if (rep_it == coefficients.end())
-      fail(ERR_INCOMPATIBLE_SYMMETRY, "symmetry projection removed its orbit representative");
-    C64 representative_coefficient = rep_it->second;
-    C64 gauge = representative_coefficient / std::abs(representative_coefficient);
-    double norm_sq = 0.0;
-    for (auto& entry : coefficients) norm_sq += std::norm(entry.second);
-    double norm = std::sqrt(norm_sq);
-    size_t orbit_size = coefficients.size();
-    double expected = 1.0 / std::sqrt(static_cast<double>(orbit_size));
-    for (auto& entry : coefficients) {
-      C64 normalized_value = entry.second / (gauge * norm);
-      if (std::abs(std::abs(normalized_value) - expected) > 1.0e-10)
-        fail(ERR_INCOMPATIBLE_SYMMETRY,
-             "symmetry projection does not define a one-dimensional orbit sector");
-      basis.lookup[entry.first] = {representative, normalized_value / expected, orbit_size};
-    }
+    size_t orbit_size = 0;
+    if (!project_orbit(representative, sites, translations, normalized, parity, has_momentum, basis.lookup,
+                       &orbit_size))
+      continue;
     sectors.push_back({representative, orbit_size});
   }
   std::sort(sectors.begin(), sectors.end(),
@@ -2158,6 +2173,45 @@ int oracle_basis_image(void* handle, uint64_t lo, uint64_t hi, uint64_t* rep_lo,
   phase[1] = it->second.phase.imag();
   *orbit = it->second.orbit_size;
   return 1;
+}
+
+// Reduction images of physical states by the reference's per-orbit rule
+// alone: the orbit of each state, its minimum, and the projection of that
+// orbit (project_orbit), without building the sector. For sectors too large
+// for the full lookup. Outputs per state: representative (lo/hi words),
+// phase (2 doubles) and orbit size (0 when the orbit is not in the sector).
+int oracle_orbit_images(int sites, int has_momentum, int momentum, int parity, long long n, const uint64_t* lo,
+                        const uint64_t* hi, uint64_t* rep_lo, uint64_t* rep_hi, double* phase, uint64_t* orbit) {
+  return guarded([&] {
+    const size_t L = static_cast<size_t>(sites);
+    const long normalized = has_momentum ? ((momentum % sites) + sites) % sites : 0;
+    const size_t translations = has_momentum ? L : 1;
+    for (long long i = 0; i < n; ++i) {
+      const u128 state = (static_cast<u128>(hi ? hi[i] : 0) << 64) | lo[i];
+      u128 representative = state;
+      for (size_t shift = 0; shift < translations; ++shift) {
+        u128 translated = rotate_lattice_state(state, shift, L);
+        representative = std::min(representative, translated);
+        if (parity != 0) representative = std::min(representative, reflect_lattice_state(translated, L));
+      }
+      std::unordered_map<u128, SymmetryImage, U128Hash> images;
+      size_t orbit_size = 0;
+      const bool kept = project_orbit(representative, L, translations, normalized, parity, has_momentum != 0,
+                                      images, &orbit_size);
+      auto it = images.find(state);
+      if (!kept || it == images.end()) {
+        rep_lo[i] = rep_hi[i] = 0;
+        phase[2 * i] = phase[2 * i + 1] = 0.0;
+        orbit[i] = 0;
+        continue;
+      }
+      rep_lo[i] = static_cast<uint64_t>(it->second.representative);
+      rep_hi[i] = static_cast<uint64_t>(it->second.representative >> 64);
+      phase[2 * i] = it->second.phase.real();
+      phase[2 * i + 1] = it->second.phase.imag();
+      orbit[i] = it->second.orbit_size;
+    }
+  });
 }
 
 int oracle_operator_build(void* basis, int n_terms, const int* arity, const char* symbols, const int* n_couplings,
