@@ -62,6 +62,8 @@ def parse():
                    help="XXZ plain/mixed/filtered comparison size (0 skips it)")
     p.add_argument("--ftlm-sites", type=int, default=28,
                    help="finite-temperature Lanczos size: 8 vectors x 100 steps (0 skips it)")
+    p.add_argument("--only", default="all", choices=["all", "matrix_free"],
+                   help="matrix_free: run only the on-the-fly section at --sites (a small case for profilers)")
     p.add_argument("--matrix-free-sites", type=int, default=34,
                    help="on-the-fly (matrix-free) H.v, block action and solves at this size (0 skips it)")
     p.add_argument("--scan-sites", type=int, default=26,
@@ -84,7 +86,7 @@ def timed_launches(fn, count: int) -> float:
 
 
 def matrix_free_section(sites: int, rank: int, local_rank: int, peak: float, launches: int,
-                        eigenpairs: int, krylov: int, tolerance: float) -> dict:
+                        eigenpairs: int, krylov: int, tolerance: float, solves: bool = True) -> dict:
     """The L=34 sector with the terms expanded on every application (no stored
     rows): the warp-tile kernel resolving targets through the image table,
     H.v and 8-vector block action timed against the operand-byte model, the
@@ -125,6 +127,8 @@ def matrix_free_section(sites: int, rank: int, local_rank: int, peak: float, lau
     op.set_lookup("auto")
     out["search_hv_fp32_ms"] = search32 * 1e3
     del x32, y32, x64, y64
+    if not solves:
+        return out
     solves = {}
     for mode in ("filtered", "fp64"):
         kw = dict(krylov_dimension=krylov, tolerance=tolerance, seed=rank, mode=mode)
@@ -498,6 +502,12 @@ def main():
     from qmbed_b200._lib import EigshInfoC, EigshOptionsC, check, lib
 
     sites = args.sites
+    if args.only == "matrix_free":
+        section = matrix_free_section(sites, rank, local_rank, float(measured_peaks()["hbm_gbs"]), args.hv_launches,
+                                      args.eigenpairs, args.krylov, args.tolerance, solves=not args.no_plain)
+        if rank == 0:
+            print(json.dumps({"matrix_free": section}), flush=True)
+        return
     t0 = time.perf_counter()
     basis = engine.GpuBasis(sites, up=sites // 2, momentum=0, parity=1, device=local_rank)
     build_s = basis.build_seconds

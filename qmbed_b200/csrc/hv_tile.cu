@@ -587,7 +587,7 @@ __device__ __forceinline__ void lookup_batch(const TileArgs& a, const uint64_t* 
 template <typename T, int NB, bool CPLX>
 struct TileShape {
   static constexpr int U = NB == 1 ? 4 : (NB * sizeof(T) <= 32 ? 4 : (NB * sizeof(T) <= 64 ? 2 : 1));
-  static constexpr int MIN_BLOCKS = NB == 1 ? 3 : 2;
+  static constexpr int MIN_BLOCKS = (NB == 1 || NB * sizeof(T) <= 32) ? 3 : 2;
 };
 
 // Resolves a round of U targets and accumulates their contributions:
