@@ -262,6 +262,14 @@ QMBED_API int qmbed_gpu_expm_lanczos(qmbed_operator op, const double* initial, d
 QMBED_API int qmbed_gpu_chebyshev_evolve(qmbed_operator op, const double* initial, int n_times, const double* times,
                                          double e_min, double e_max, double tolerance, int precision, int final_only,
                                          double* states, double* info);
+/* The same propagation on a device state: `state` (interleaved complex128,
+ * dimension x 2 doubles, device memory) holds the initial state and receives
+ * the state at the last time; intermediate times are propagated through but
+ * not returned, and nothing crosses to the host. Runs on the operator's
+ * stream and returns after it completes. Addition of this library. */
+QMBED_API int qmbed_gpu_chebyshev_evolve_device(qmbed_operator op, double* state, int n_times, const double* times,
+                                                double e_min, double e_max, double tolerance, int precision,
+                                                double* info);
 
 /* Lowest eigenvalues of every H(s, p) = sum_k coefficients[p][k] A_k(s) for
  * n_sectors sectors s and n_points scan points p (<= 64), in one batched

@@ -114,6 +114,7 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_evolve.argtypes = [vp, vp, i, vp, u64, d, u64, vp, vp]
     L.qmbed_gpu_expm_lanczos.argtypes = [vp, vp, d, u64, vp]
     L.qmbed_gpu_chebyshev_evolve.argtypes = [vp, vp, i, vp, d, d, d, i, i, vp, vp]
+    L.qmbed_gpu_chebyshev_evolve_device.argtypes = [vp, vp, i, vp, d, d, d, i, vp]
     L.qmbed_gpu_lanczos_extremes.argtypes = [vp, i, u64, vp]
     L.qmbed_gpu_scan_lowest.argtypes = [i, i, vp, i, vp, i, d, i, u64, vp, vp, vp]
     L.qmbed_gpu_lanczos_create.argtypes = [vp, vp, u64, d, P(vp)]

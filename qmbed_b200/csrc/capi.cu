@@ -2213,6 +2213,26 @@ int qmbed_gpu_expm_lanczos(qmbed_operator op, const double* initial, double time
   });
 }
 
+int qmbed_gpu_chebyshev_evolve_device(qmbed_operator op, double* state, int n_times, const double* times,
+                                      double e_min, double e_max, double tolerance, int precision, double* info) {
+  return guarded([&] {
+    if (!state || n_times <= 0 || !times)
+      raise(QMBED_INVALID_OPTIONS, "evolution needs a device state and a time grid");
+    std::lock_guard<std::mutex> lock(op->mu);
+    if (std::isnan(e_min) && std::isnan(e_max)) flip_chain_norm_bounds(*op->op, &e_min, &e_max);
+    ChebyshevInfo ci;
+    chebyshev_evolve_device(*op->op, state, std::vector<double>(times, times + n_times), e_min, e_max, tolerance,
+                            precision, ci, op->block_ops());
+    if (info) {
+      info[0] = static_cast<double>(ci.applications);
+      info[1] = static_cast<double>(ci.intervals);
+      info[2] = ci.e_min;
+      info[3] = ci.e_max;
+      info[4] = ci.max_norm_drift;
+    }
+  });
+}
+
 int qmbed_gpu_chebyshev_evolve(qmbed_operator op, const double* initial, int n_times, const double* times,
                                double e_min, double e_max, double tolerance, int precision, int final_only,
                                double* states, double* info) {

@@ -49,9 +49,15 @@ void flip_chain_norm_bounds(const SpinOperator& op, double* e_min, double* e_max
   *e_max = b;
 }
 
-void chebyshev_evolve(const SpinOperator& op, const double* initial, const std::vector<double>& times, double e_min,
-                      double e_max, double tolerance, int precision, bool final_only, double* states,
-                      ChebyshevInfo& info, BlockOps& ops) {
+namespace {
+
+// The propagation itself: `initial` (interleaved complex128, host or device
+// memory per `initial_kind`) evolved over `times`; `output(t, psi, staging)`
+// runs after time t with the working-precision state on the device.
+template <typename Output>
+void chebyshev_run(const SpinOperator& op, const double* initial, cudaMemcpyKind initial_kind,
+                   const std::vector<double>& times, double e_min, double e_max, double tolerance, int precision,
+                   ChebyshevInfo& info, BlockOps& ops, Output&& output) {
   const FlipChain* fc = op.flip_chain();
   if (!fc)
     raise(QMBED_UNSUPPORTED_BACKEND,
@@ -71,7 +77,7 @@ void chebyshev_evolve(const SpinOperator& op, const double* initial, const std::
   void* psi = buf_psi.get();
   void* b1 = buf_a.get();
   void* b2 = buf_b.get();
-  QMBED_CUDA(cudaMemcpyAsync(staging.get(), initial, n * 16, cudaMemcpyHostToDevice, s));
+  QMBED_CUDA(cudaMemcpyAsync(staging.get(), initial, n * 16, initial_kind, s));
   ops.convert(staging.get(), 64, psi, precision, 2 * n);
   const double norm0 = ops.norm(psi, n, precision, true);
   const double a = 0.5 * (e_max - e_min), c = 0.5 * (e_max + e_min);
@@ -88,11 +94,7 @@ void chebyshev_evolve(const SpinOperator& op, const double* initial, const std::
     QMBED_LAUNCH_CHECK();
   };
   auto emit = [&](size_t t) {
-    if (!final_only || t + 1 == times.size()) {
-      ops.convert(psi, precision, staging.get(), 64, 2 * n);
-      QMBED_CUDA(cudaMemcpyAsync(states + (final_only ? 0 : 2 * t * n), staging.get(), n * 16, cudaMemcpyDeviceToHost,
-                                 s));
-    }
+    output(t, static_cast<const void*>(psi), staging.get());
     const double norm = ops.norm(psi, n, precision, true);
     info.max_norm_drift = std::max(info.max_norm_drift, std::fabs(norm - norm0));
   };
@@ -146,6 +148,31 @@ void chebyshev_evolve(const SpinOperator& op, const double* initial, const std::
     emit(t);
   }
   ops.sync();
+}
+
+}  // namespace
+
+void chebyshev_evolve(const SpinOperator& op, const double* initial, const std::vector<double>& times, double e_min,
+                      double e_max, double tolerance, int precision, bool final_only, double* states,
+                      ChebyshevInfo& info, BlockOps& ops) {
+  const uint64_t n = op.dim();
+  const cudaStream_t s = ops.stream();
+  chebyshev_run(op, initial, cudaMemcpyHostToDevice, times, e_min, e_max, tolerance, precision, info, ops,
+                [&](size_t t, const void* psi, void* staging) {
+                  if (final_only && t + 1 != times.size()) return;
+                  ops.convert(psi, precision, staging, 64, 2 * n);
+                  QMBED_CUDA(cudaMemcpyAsync(states + (final_only ? 0 : 2 * t * n), staging, n * 16,
+                                             cudaMemcpyDeviceToHost, s));
+                });
+}
+
+void chebyshev_evolve_device(const SpinOperator& op, double* state, const std::vector<double>& times, double e_min,
+                             double e_max, double tolerance, int precision, ChebyshevInfo& info, BlockOps& ops) {
+  const uint64_t n = op.dim();
+  chebyshev_run(op, state, cudaMemcpyDeviceToDevice, times, e_min, e_max, tolerance, precision, info, ops,
+                [&](size_t t, const void* psi, void*) {
+                  if (t + 1 == times.size()) ops.convert(psi, precision, state, 64, 2 * n);
+                });
 }
 
 }  // namespace qmbed

@@ -29,6 +29,11 @@ void chebyshev_evolve(const SpinOperator& op, const double* initial, const std::
                       double e_max, double tolerance, int precision, bool final_only, double* states,
                       ChebyshevInfo& info, BlockOps& ops);
 
+// The same propagation on a device state (interleaved complex128, n
+// elements) overwritten with the state at the last time; no host transfers.
+void chebyshev_evolve_device(const SpinOperator& op, double* state, const std::vector<double>& times, double e_min,
+                             double e_max, double tolerance, int precision, ChebyshevInfo& info, BlockOps& ops);
+
 // Spectral interval guaranteed to contain the spectrum of a flip chain
 // (sum of the absolute coefficients on either side of zero).
 void flip_chain_norm_bounds(const SpinOperator& op, double* e_min, double* e_max);

@@ -313,6 +313,17 @@ class GpuOperator:
         return states, {"applications": int(info[0]), "intervals": int(info[1]), "e_min": float(info[2]),
                         "e_max": float(info[3]), "max_norm_drift": float(info[4])}
 
+    def chebyshev_evolve_device(self, state, times, e_min: float = float("nan"), e_max: float = float("nan"),
+                                tolerance: float = 1e-10, precision: int = 64) -> dict:
+        """In place on a device complex128 tensor (``data_ptr()``): state <- exp(-i H t_last) state,
+        stepping through `times`. Returns the info dict of chebyshev_evolve."""
+        t = np.ascontiguousarray(np.asarray(times, np.float64))
+        info = np.zeros(5)
+        check(lib().qmbed_gpu_chebyshev_evolve_device(self.handle, _ptr(state), len(t), _ptr(t), e_min, e_max,
+                                                      tolerance, precision, _ptr(info)))
+        return {"applications": int(info[0]), "intervals": int(info[1]), "e_min": float(info[2]),
+                "e_max": float(info[3]), "max_norm_drift": float(info[4])}
+
     def expm_plan(self, coefficient: complex, max_degree: int = 55, tolerance: float = 0.5 * np.finfo(float).eps,
                   max_substeps: int = 10_000):
         degree, scaling, one_norm = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_double()

@@ -195,6 +195,24 @@ def lanczos_interval(op: GpuOperator, steps: int = 40, seed: int = 0, margin: fl
     return Interval(lo - pad, hi + pad, "lanczos", steps)
 
 
+def propagate_device(op: GpuOperator, state, times, interval: Interval, precision: int = 64,
+                     tolerance: float = 1e-10, drift_limit: float | None = None) -> dict:
+    """propagate() in place on a device complex128 tensor (no host copies of the state)."""
+    import torch
+    if drift_limit is None:
+        drift_limit = 1e-8 if precision == 64 else 1e-4
+    initial = state.clone()
+    info = op.chebyshev_evolve_device(state, times, interval.e_min, interval.e_max, tolerance=tolerance,
+                                      precision=precision)
+    info["source"] = interval.source
+    norm0 = max(1.0, float(torch.linalg.vector_norm(initial)))
+    if info["max_norm_drift"] > drift_limit * norm0:
+        state.copy_(initial)
+        info = op.chebyshev_evolve_device(state, times, tolerance=tolerance, precision=precision)
+        info["source"] = "norm bound (after drift)"
+    return info
+
+
 def propagate(op: GpuOperator, psi0, times, interval: Interval, precision: int = 64, tolerance: float = 1e-10,
               final_only: bool = False, drift_limit: float | None = None):
     """Chebyshev propagation on `interval`; repeats on the guaranteed bound if the norm drifts.
