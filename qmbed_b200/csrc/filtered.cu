@@ -37,6 +37,8 @@
 #include <vector>
 
 #include "device_util.cuh"
+#include <string>
+
 #include "filtered.cuh"
 
 namespace qmbed {
@@ -94,6 +96,74 @@ __global__ void __launch_bounds__(kThreads) block_gram_kernel(uint64_t n, const 
     double s = 0.0;
     for (int q = 0; q < kSplit; ++q) s += red[q * kPairs + threadIdx.x];
     partial[static_cast<uint64_t>(blockIdx.x) * kPairs + threadIdx.x] = s;
+  }
+}
+
+// D = A B + C on the FP64 tensor cores: one m8n8k4 MMA per warp, A 8 x 4
+// (row major), B 4 x 8 (column major). Per lane: a = A[lane / 4][lane % 4],
+// b = B[lane % 4][lane / 4], c/d = C[lane / 4][2 (lane % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_8x8x4(double a, double b, double& c0, double& c1) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// The same weighted Gram on the tensor cores. The contraction runs over the
+// rows: every MMA takes 4 consecutive rows of the row-major n x NB blocks, so
+// the 32 lanes' operand loads are the 4 x 8 sub-block of a and of b (one
+// contiguous 256-byte (FP64) or 128-byte (FP32) span per operand). A warp
+// keeps the (NB / 8)^2 output tiles of the NB x NB Gram in registers, strides
+// over groups of 4 rows, and the block reduces its warps in a fixed order.
+template <typename T, int NB>
+__global__ void __launch_bounds__(kThreads) block_gram_mma_kernel(uint64_t n, const T* __restrict__ a,
+                                                                   const T* __restrict__ b,
+                                                                   const uint16_t* __restrict__ weights,
+                                                                   double* __restrict__ partial) {
+  constexpr int TILES = NB / 8;
+  constexpr int kWarps = kThreads / 32;
+  constexpr int kUnroll = 4;  // row groups whose operands are loaded before their MMAs
+  __shared__ double red[kWarps][NB * NB];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int kr = lane & 3, col = lane >> 2;  // operand row within the group, column within a tile
+  double c[TILES][TILES][2];
+#pragma unroll
+  for (int p = 0; p < TILES; ++p)
+#pragma unroll
+    for (int q = 0; q < TILES; ++q) c[p][q][0] = c[p][q][1] = 0.0;
+  const uint64_t groups = (n + 3) / 4;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * kWarps;
+  for (uint64_t g0 = static_cast<uint64_t>(blockIdx.x) * kWarps + warp; g0 < groups; g0 += stride * kUnroll) {
+    double va[kUnroll][TILES], vb[kUnroll][TILES];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const uint64_t g = g0 + u * stride;
+      const uint64_t r = g * 4 + kr;
+      const bool in = g < groups && r < n;
+      const double w = in ? (weights ? static_cast<double>(__ldg(weights + r)) : 1.0) : 0.0;
+#pragma unroll
+      for (int t = 0; t < TILES; ++t) {
+        va[u][t] = in ? w * static_cast<double>(__ldg(a + r * NB + t * 8 + col)) : 0.0;
+        vb[u][t] = in ? static_cast<double>(__ldg(b + r * NB + t * 8 + col)) : 0.0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+#pragma unroll
+      for (int p = 0; p < TILES; ++p)
+#pragma unroll
+        for (int q = 0; q < TILES; ++q) dmma_8x8x4(va[u][p], vb[u][q], c[p][q][0], c[p][q][1]);
+  }
+#pragma unroll
+  for (int p = 0; p < TILES; ++p)
+#pragma unroll
+    for (int q = 0; q < TILES; ++q)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) red[warp][(p * 8 + col) * NB + q * 8 + 2 * kr + h] = c[p][q][h];
+  __syncthreads();
+  for (int t = threadIdx.x; t < NB * NB; t += kThreads) {
+    double s = 0.0;
+    for (int w8 = 0; w8 < kWarps; ++w8) s += red[w8][t];
+    partial[static_cast<uint64_t>(blockIdx.x) * NB * NB + t] = s;
   }
 }
 
@@ -255,14 +325,20 @@ class BlockSolver {
     ++block_actions;
   }
 
-  // G[i][j] = sum_r R_r a[r][i] b[r][j]
+  // G[i][j] = sum_r R_r a[r][i] b[r][j], on the FP64 tensor cores unless
+  // QMBED_DENSE=scalar selects the CUDA-core kernel.
   std::vector<double> gram(int prec, const void* a, const void* b) {
     const cudaStream_t s = ops_.stream();
+    const bool scalar = !dense_on_tensor_cores();
     dispatch_block(prec, nb_, [&](auto ttag, auto nbtag) {
       using T = decltype(ttag);
       constexpr int NB = decltype(nbtag)::value;
-      block_gram_kernel<T, NB><<<blocks_, kThreads, 0, s>>>(n_, static_cast<const T*>(a), static_cast<const T*>(b),
-                                                            op_.weights, partial_.as<double>());
+      if (scalar)
+        block_gram_kernel<T, NB><<<blocks_, kThreads, 0, s>>>(n_, static_cast<const T*>(a), static_cast<const T*>(b),
+                                                              op_.weights, partial_.as<double>());
+      else
+        block_gram_mma_kernel<T, NB><<<blocks_, kThreads, 0, s>>>(
+            n_, static_cast<const T*>(a), static_cast<const T*>(b), op_.weights, partial_.as<double>());
     });
     QMBED_LAUNCH_CHECK();
     return reduce(nb_ * nb_);

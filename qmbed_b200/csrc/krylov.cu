@@ -8,9 +8,21 @@
 #include <numeric>
 
 #include "device_util.cuh"
+#include <cstdlib>
+#include <string>
+
 #include "krylov.cuh"
 
 namespace qmbed {
+
+bool dense_on_tensor_cores() {
+  static const bool on = [] {
+    const char* env = std::getenv("QMBED_DENSE");
+    return !(env && std::string(env) == "scalar");
+  }();
+  return on;
+}
+
 
 namespace {
 
@@ -258,6 +270,51 @@ __global__ void __launch_bounds__(kThreads) combine_kernel(const T* __restrict__
 #pragma unroll
     for (int kk = 0; kk < kCombine; ++kk)
       if (kk < cnt) store<T, CPLX>(out + (k0 + kk) * ld_out * (CPLX ? 2 : 1), i, ar[kk], ai[kk]);
+  }
+}
+
+// Real combinations on the FP64 tensor cores: out[:, k0 + q] = sum_j Re(Y[j, k0 + q]) A[:, j] for
+// q < 8, one m8n8k4 DMMA per 8 rows x 4 basis columns. A warp takes tiles of
+// 8 consecutive rows; lane l holds A[row 8t + l / 4][column j0 + l % 4] (four
+// 64-byte column segments per MMA) and the block's Y columns come from shared
+// memory (y[j][q]); D[l / 4][2 (l % 4) + h] is row 8t + l / 4 of output
+// column k0 + 2 (l % 4) + h.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) combine_mma_kernel(const T* __restrict__ A, uint64_t ld, int m,
+                                                                const double* __restrict__ Y, int K, int k0,
+                                                                T* __restrict__ out, uint64_t ld_out, uint64_t n) {
+  extern __shared__ double ys[];  // ys[j * 8 + q] = Re Y[j, k0 + q], zero-padded to a multiple of 4 rows
+  const int m4 = (m + 3) & ~3;
+  for (int t = threadIdx.x; t < m4 * 8; t += blockDim.x) {
+    const int j = t / 8, q = t % 8;
+    ys[t] = (j < m && k0 + q < K) ? Y[(static_cast<uint64_t>(k0 + q) * m + j) * 2] : 0.0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int r = lane >> 2, kq = lane & 3;
+  const uint64_t tiles = (n + 7) / 8;
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); t < tiles; t += warps) {
+    const uint64_t row = t * 8 + r;
+    const bool in = row < n;
+    double c0 = 0.0, c1 = 0.0;
+    for (int j0 = 0; j0 < m4; j0 += 16) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int j = j0 + 4 * u + kq;
+        a[u] = (in && j < m) ? static_cast<double>(A[static_cast<uint64_t>(j) * ld + row]) : 0.0;
+        b[u] = j < m4 ? ys[j * 8 + r] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                     : "+d"(c0), "+d"(c1)
+                     : "d"(a[u]), "d"(b[u]));
+    }
+    const int q0 = k0 + 2 * kq;
+    if (in && q0 < K) out[static_cast<uint64_t>(q0) * ld_out + row] = static_cast<T>(c0);
+    if (in && q0 + 1 < K) out[static_cast<uint64_t>(q0 + 1) * ld_out + row] = static_cast<T>(c1);
   }
 }
 
@@ -955,6 +1012,25 @@ void BlockOps::combine(const void* A, uint64_t ld, int m, const C64* Y, int K, v
   ensure_coeffs(static_cast<size_t>(m) * K * 16);
   QMBED_CUDA(cudaMemcpyAsync(coeffs_.get(), Y, static_cast<size_t>(m) * K * 16, cudaMemcpyHostToDevice, stream_));
   const int G = stream_grid(n, sms_);
+  // real data with real coefficients: the tensor-core kernel, 8 columns per launch
+  bool real_y = !cplx;
+  for (int i = 0; i < m * K && real_y; ++i) real_y = Y[i].imag() == 0.0;
+  const size_t ys_bytes = static_cast<size_t>((m + 3) & ~3) * 8 * sizeof(double);
+  if (real_y && dense_on_tensor_cores() && ys_bytes <= 48 * 1024) {
+    for (int k0 = 0; k0 < K; k0 += 8) {
+      if (precision == 64)
+        combine_mma_kernel<double><<<G, kThreads, ys_bytes, stream_>>>(static_cast<const double*>(A), ld, m,
+                                                                       coeffs_.as<double>(), K, k0,
+                                                                       static_cast<double*>(out), ld_out, n);
+      else
+        combine_mma_kernel<float><<<G, kThreads, ys_bytes, stream_>>>(static_cast<const float*>(A), ld, m,
+                                                                      coeffs_.as<double>(), K, k0,
+                                                                      static_cast<float*>(out), ld_out, n);
+      QMBED_LAUNCH_CHECK();
+    }
+    sync();
+    return;
+  }
   for (int k0 = 0; k0 < K; k0 += kCombine) {
     QMBED_DISPATCH(precision, cplx,
                    (combine_kernel<T, C><<<G, kThreads, 0, stream_>>>(static_cast<const T*>(A), ld, m,

@@ -13,6 +13,10 @@ namespace qmbed {
 using C64 = std::complex<double>;
 
 // row_ptr = exclusive scan of per-row counts (u32 when the total fits).
+// False when QMBED_DENSE=scalar selects the CUDA-core kernels for the dense
+// contractions (block Gram, Ritz combinations) instead of the FP64 tensor cores.
+bool dense_on_tensor_cores();
+
 uint64_t exclusive_scan_counts(const uint32_t* counts, uint64_t n, DeviceBuffer& row_ptr, bool* is64);
 C64 device_sum_complex(const double* interleaved, uint64_t n);
 double device_max_shifted_column(const double* diag, const double* offsum, uint64_t n, C64 shift);

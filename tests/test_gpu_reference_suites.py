@@ -13,9 +13,9 @@ library, so every numeric call of the reference frontend goes through the
 GPU engine. The compatibility files must pass whole. test_qmbed.py also
 covers families this library leaves to the reference (fermion and photon
 bases, archives, Floquet and density workflows), which answer "unsupported
-backend"; the tests of the eigsh / expm / evolution / thermal / sector-shift
-path listed in NATIVE_IN_SCOPE must pass, and the outcome of every test is
-printed. The tests skip when baseline/_ref is absent.
+backend"; the tests of the eigsh / expm / evolution / sector-shift path
+listed in NATIVE_IN_SCOPE must pass, and the outcome and failure reason of
+every test is printed. The tests skip when baseline/_ref is absent.
 """
 
 import os
@@ -41,8 +41,11 @@ pytestmark = [
 NATIVE_IN_SCOPE = [
     "test_native_and_compatibility_paths_share_the_rust_solver",
     "test_quspin_static_adapter",
-    "test_all_operator_paths_pass_eigsh_v0_to_the_rust_solver",
+    "test_quspin_hamiltonian_reuses_and_releases_one_native_model",
+    "test_reusable_nonnormal_exponential_action_supports_column_batches",
+    "test_sector_shift_runs_directly_between_persistent_models",
     "test_static_hamiltonian_evolution_uses_the_registered_rust_model",
+    "test_basis_dynamic_hamiltonian_groups_equal_drives_in_rust",
 ]
 
 
@@ -73,6 +76,10 @@ def test_native_suite_in_scope_tests_pass_verbatim():
     proc, outcomes = _run(SUITES / "native" / "test_qmbed.py")
     for name, outcome in sorted(outcomes.items()):
         print(f"{outcome:7s} {name}")
+    # the reason of every failure, as pytest's short summary gives it
+    for line in proc.stdout.splitlines():
+        if line.startswith("FAILED"):
+            print(line[:400])
     assert outcomes, proc.stdout[-3000:] + proc.stderr[-2000:]
     missing = [t for t in NATIVE_IN_SCOPE if outcomes.get(t) != "PASSED"]
     assert not missing, (missing, proc.stdout[-4000:])
