@@ -288,7 +288,13 @@ def scan_section(sites: int, rank: int, local_rank: int, with_cpu: bool) -> dict
                        f"(J2 in [0,0.5], Delta~U[0.8,1.2] seed {sites + rank}), 2 lowest, tol 1e-10",
            "solves": solves, "sector_dims": [min(dims), max(dims)], "setup_s": setup, "s": seconds,
            "ms_per_solve": 1e3 * seconds / solves, "lanczos_steps": [int(steps.min()), int(steps.max())],
-           "applications": info["applications"], "precision": "fp64 vectors and recurrences"}
+           "applications": info["applications"], "verification_applications": info["verification_applications"],
+           "first_pass_s": info["pass1_seconds"], "cuda_graph": info["graph"],
+           "max_relative_residual": info["max_relative_residual"], "merged_ritz_copies": info["merged_copies"],
+           "residuals_verified": int(np.isfinite(info["residuals"]).sum()),
+           "e_max_range": [float(np.nanmin(info["e_max"])), float(np.nanmax(info["e_max"]))],
+           "precision": "fp64 vectors and recurrences; every reported pair's residual recomputed in FP64 "
+                        "from its Ritz vector (second pass)"}
     if with_cpu:
         # the oracle's eigsh on one (sector, point) pair at full size: parity and the CPU time per solve
         sys.path.insert(0, str(ROOT))

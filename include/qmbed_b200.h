@@ -287,6 +287,24 @@ QMBED_API int qmbed_gpu_chebyshev_evolve_device(qmbed_operator op, double* state
 QMBED_API int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
                                     const double* coefficients, int eigenpairs, double tolerance, int max_steps,
                                     uint64_t seed, double* eigenvalues, int* steps, double* info);
+/* The same scan with its verification outputs: residuals[s][p][i] =
+ * ||H v - theta v|| / ||v|| of each reported Ritz pair, computed in FP64 from
+ * its Ritz vector (the reference's acceptance test r <= tol max(|theta|, 1),
+ * src/solve/mod.rs:1252-1263, holds for every reported pair, otherwise
+ * QMBED_STATUS_NON_CONVERGENCE); e_max[s][p] = the largest Ritz value at
+ * convergence (an inner estimate of the top of the spectrum); info (8
+ * doubles): first-pass steps of the longest pair, first-pass applications,
+ * verification applications, CUDA graph used (1/0), first-pass seconds,
+ * total seconds, largest relative residual, Ritz copies merged.
+ * residuals and e_max may be NULL. */
+QMBED_API int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
+                                   const double* coefficients, int eigenpairs, double tolerance, int max_steps,
+                                   uint64_t seed, double* eigenvalues, double* residuals, double* e_max, int* steps,
+                                   double* info);
+/* Test of the persistent scan kernel's grid barrier: launches it with one
+ * block fewer than it waits for; *status receives 1 when the bounded spin
+ * ended in the time-out status (the kernel returns instead of hanging). */
+QMBED_API int qmbed_gpu_scan_barrier_selftest(int device, int* status);
 
 /* Extreme Ritz values of a steps-step FP64 Lanczos run without
  * reorthogonalisation from deterministic_start(seed) (src/solve/mod.rs:

@@ -117,6 +117,8 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_chebyshev_evolve_device.argtypes = [vp, vp, i, vp, d, d, d, i, vp]
     L.qmbed_gpu_lanczos_extremes.argtypes = [vp, i, u64, vp]
     L.qmbed_gpu_scan_lowest.argtypes = [i, i, vp, i, vp, i, d, i, u64, vp, vp, vp]
+    L.qmbed_gpu_scan_solve.argtypes = [i, i, vp, i, vp, i, d, i, u64, vp, vp, vp, vp, vp]
+    L.qmbed_gpu_scan_barrier_selftest.argtypes = [i, P(i)]
     L.qmbed_gpu_lanczos_create.argtypes = [vp, vp, u64, d, P(vp)]
     L.qmbed_gpu_lanczos_destroy.argtypes = [vp]
     L.qmbed_gpu_lanczos_info.argtypes = [vp, P(u64), P(u64), P(d), P(i), P(u64)]

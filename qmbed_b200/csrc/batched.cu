@@ -1,25 +1,35 @@
-// Batched Lanczos over sectors x scan points.
+// Batched Lanczos over sectors x scan points in one persistent launch.
 //
 // Every (sector s, point p) pair is an independent Hermitian problem
 // H(s, p) = sum_k c_k(p) A_k(s) whose lowest eigenvalues are wanted (the
-// reference would call eigsh once per pair, src/solve/mod.rs:2335-2350). Here
-// all pairs advance together: one column per pair in row-major blocks
-// (rows of sector s) x (points), so one launch applies every sector's
-// operator to every point, and the gather of a column reads all points of
-// that row as one contiguous 512-byte or 1-KB line. The rows of all sectors are
-// concatenated and each warp finds its sector by binary search, so sectors of
-// uneven dimension share the launch.
+// reference calls eigsh once per pair, src/solve/mod.rs:2335-2350). Here all
+// pairs advance together: one column per pair in row-major blocks (rows of
+// sector s) x (points), so one pass applies every sector's operator to every
+// point, and the gather of a column reads all points of that row as one
+// contiguous 512-byte or 1-KB line. The rows of all sectors are concatenated
+// and each warp finds its sector by binary search, so sectors of uneven
+// dimension share the launch.
 //
-// Method: the plain three-term Lanczos recurrence without reorthogonalisation
-// (each column its own alpha, beta in FP64, all vectors FP64), in the
-// orbit-scaled coordinates z = x / sqrt(R) with R-weighted inner products.
-// Loss of orthogonality only adds copies of converged Ritz values; the
-// lowest distinct Ritz values are taken after merging copies closer than
-// 1e-8 max(|theta|, 1), and a pair is converged when its wanted values move
-// by less than 1e-3 tol max(|theta|, 1) over `kCheck` steps. The tridiagonal
-// eigenvalues come from Sturm-sequence bisection on the GPU, one thread per
-// pair, from the alpha/beta histories kept in device memory.
+// Execution: a cooperative kernel runs a chunk of Lanczos steps; its phases
+// (apply, alpha, update, beta, scale) are separated by a grid barrier whose
+// spin is bounded (on time-out every block records the error and returns).
+// A chunk is [persistent kernel, convergence check, status copy]; it is
+// captured once in a CUDA graph and replayed until every pair has converged.
+// The step counter lives in device memory, so the graph's arguments never
+// change.
+//
+// Method: plain three-term Lanczos without reorthogonalisation, FP64 vectors
+// and recurrences, orbit-scaled coordinates z = x / sqrt(R) with R-weighted
+// inner products. A pair stops when the residual estimates |beta_m s_m| of
+// its lowest Ritz values (copies from lost orthogonality counted once) are
+// below 0.1 tol max(|theta|, 1). A second pass repeats the identical
+// recurrence and accumulates the Ritz vectors of the lowest candidates; one
+// FP64 application then gives every candidate's true residual
+// ||H v - theta v|| / ||v|| (the reference's acceptance test, src/solve/mod.rs:
+// 1252-1263) and the overlaps that decide which close Ritz values are copies
+// of one eigenvector (overlap > 1/2) and which are distinct eigenvalues.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -31,9 +41,13 @@ namespace {
 
 constexpr int kMaxComp = 8;
 constexpr int kMaxSectors = 128;
-constexpr int kRowsPerBlock = 256;  // reduction blocks: 8 warps x 32 rows
-constexpr int kCheck = 10;
-constexpr int kLowest = 8;  // Ritz values computed per pair at a check
+constexpr int kMaxCand = 6;          // Ritz candidates kept per pair (eigenpairs + 2)
+constexpr int kRowsPerItem = 256;    // rows of one reduction item: 8 warps x 32 rows
+constexpr int kThreads = 256;
+constexpr int kChunkSteps = 10;      // Lanczos steps per persistent launch (one graph replay)
+constexpr unsigned kSpinLimit = 1u << 22;  // barrier polls (with 64 ns sleeps: about a quarter second)
+
+enum ScanStatus : int { kStatusRunning = 0, kStatusBarrierTimeout = 1 };
 
 struct CompRows {
   const void* row_ptr;
@@ -45,10 +59,40 @@ struct CompRows {
 };
 
 struct SectorDesc {
-  uint64_t row0, n, block0, blocks;
+  uint64_t row0, n, item0, items;
   const uint16_t* weights;
-  double* buf[3];
+  double* buf[3];            // Lanczos vectors (roles rotate with the step)
+  double* ritz[kMaxCand];    // second pass: Ritz vector accumulators
   CompRows comp[kMaxComp];
+};
+
+// Device state shared by the persistent kernel, the check kernel and the host.
+struct ScanState {
+  unsigned barrier_count, barrier_gen;
+  int status;                // ScanStatus
+  int step;                  // steps completed in this pass
+  int pass;                  // 1: search, 2: Ritz vectors
+  int active;                // pairs not yet converged (pass 1)
+  int target_steps;          // pass 2: steps to run (max over pairs of m_p)
+  int pad;
+};
+
+struct ScanArgs {
+  const SectorDesc* sec;
+  int ns, P, K, cols, points, eigenpairs, max_steps, ncand;
+  uint64_t total_rows, total_items;
+  const double* coef;        // K x P
+  double* partial;           // total_items x P
+  double* alpha;             // max_steps x cols
+  double* beta;              // (max_steps + 1) x cols; row max_steps: start-vector norms
+  int* length;               // step at which beta vanished (Krylov space exhausted), -1 before
+  int* stop;                 // pass-1 step count at convergence per pair (-1: running)
+  double* cand_s;            // cols x ncand x max_steps: eigenvectors of T_m for the candidates
+  double* cand_theta;        // cols x ncand
+  double* top;               // cols: largest Ritz value at convergence
+  double tolerance;
+  uint64_t seed;
+  ScanState* state;
 };
 
 __device__ __forceinline__ int find_sector(const uint64_t* starts, int ns, uint64_t g) {
@@ -65,12 +109,476 @@ __device__ __forceinline__ uint64_t row_begin(const CompRows& c, uint64_t r) {
   return c.row_ptr64 ? static_cast<const uint64_t*>(c.row_ptr)[r] : static_cast<const uint32_t*>(c.row_ptr)[r];
 }
 
-// out = H(s, p) cur - beta_prev(s, p) prev, one warp per row, lane owns PPL points
+// Grid-wide barrier with a bounded spin. Returns false when any block timed
+// out (then every block leaves the kernel at its next barrier).
+__device__ bool grid_sync(ScanState* st, unsigned blocks) {
+  __syncthreads();
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile int* status = &st->status;
+    if (*status != kStatusRunning) {
+      ok = 0;
+    } else {
+      volatile unsigned* gen = &st->barrier_gen;
+      const unsigned g = *gen;
+      __threadfence();
+      const unsigned arrived = atomicAdd(&st->barrier_count, 1u);
+      if (arrived == blocks - 1) {
+        st->barrier_count = 0;
+        __threadfence();
+        atomicAdd(&st->barrier_gen, 1u);
+      } else {
+        unsigned polls = 0;
+        while (*gen == g) {
+          if (++polls > kSpinLimit || *status != kStatusRunning) {
+            atomicExch(&st->status, kStatusBarrierTimeout);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// The vector roles at step j: z_j (current), z_{j-1} (previous), work.
+__device__ __forceinline__ void roles(int j, int& cur, int& prev, int& work) {
+  cur = j % 3;
+  prev = (j + 2) % 3;
+  work = (j + 1) % 3;
+}
+
+// One warp per row of all sectors: work = H(s, p) cur - beta_{j-1} prev, and
+// in the second pass ritz_i += s_i[j] cur for the pairs still inside m_p.
+template <int PPL, bool PASS2>
+__device__ void phase_apply(const ScanArgs& a, const uint64_t* starts, const double* c, int j) {
+  constexpr int P = 32 * PPL;
+  int cur, prev, work;
+  roles(j, cur, prev, work);
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (uint64_t g = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; g < a.total_rows;
+       g += warps) {
+    const int s = find_sector(starts, a.ns, g);
+    const SectorDesc& d = a.sec[s];
+    const uint64_t r = g - d.row0;
+    const double* z = d.buf[cur];
+    double are[PPL], aim[PPL], dsum[PPL];
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) are[q] = aim[q] = dsum[q] = 0.0;
+    for (int k = 0; k < a.K; ++k) {
+      const CompRows& cr = d.comp[k];
+      double ck[PPL];
+#pragma unroll
+      for (int q = 0; q < PPL; ++q) ck[q] = c[k * P + lane * PPL + q];
+      const uint64_t begin = row_begin(cr, r), end = row_begin(cr, r + 1);
+      for (uint64_t e = begin; e < end; ++e) {
+        const uint64_t col = cr.cols[e];
+        const double vr = cr.vals[2 * e], vi = cr.vals[2 * e + 1];
+        const double2* zc = reinterpret_cast<const double2*>(z) + col * P + lane * PPL;
+#pragma unroll
+        for (int q = 0; q < PPL; ++q) {
+          const double2 x = zc[q];
+          are[q] = fma(ck[q], vr * x.x - vi * x.y, are[q]);
+          aim[q] = fma(ck[q], vr * x.y + vi * x.x, aim[q]);
+        }
+      }
+      const double dr = cr.diag_complex ? cr.diag[2 * r] : cr.diag[r];
+#pragma unroll
+      for (int q = 0; q < PPL; ++q) dsum[q] = fma(ck[q], dr, dsum[q]);
+    }
+    const double2* zs = reinterpret_cast<const double2*>(z) + r * P + lane * PPL;
+    const double2* pv = reinterpret_cast<const double2*>(d.buf[prev]) + r * P + lane * PPL;
+    double2* o = reinterpret_cast<double2*>(d.buf[work]) + r * P + lane * PPL;
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) {
+      const double2 x = zs[q];
+      double wr = are[q] + dsum[q] * x.x, wi = aim[q] + dsum[q] * x.y;
+      const int colidx = s * P + lane * PPL + q;
+      if (j > 0) {
+        const double b = a.beta[static_cast<uint64_t>(j - 1) * a.cols + colidx];
+        const double2 y = pv[q];
+        wr -= b * y.x;
+        wi -= b * y.y;
+      }
+      o[q] = make_double2(wr, wi);
+      if (PASS2 && j < a.stop[colidx]) {
+        for (int i = 0; i < a.ncand; ++i) {
+          const double si = a.cand_s[(static_cast<uint64_t>(colidx) * a.ncand + i) * a.max_steps + j];
+          double2* acc = reinterpret_cast<double2*>(d.ritz[i]) + r * P + lane * PPL + q;
+          double2 v = *acc;
+          v.x = fma(si, x.x, v.x);
+          v.y = fma(si, x.y, v.y);
+          *acc = v;
+        }
+      }
+    }
+  }
+}
+
+// Reduction items (256 rows of one sector each). MODE 0: partial = sum_r R_r
+// Re(conj(cur) work) (alpha); MODE 1: work -= alpha cur and partial =
+// sum_r R_r |work|^2 (beta^2; alpha null for the start vector's norm).
+template <int PPL, int MODE>
+__device__ void phase_reduce(const ScanArgs& a, const uint64_t* item_starts, int ia, int ib, const double* alpha) {
+  constexpr int P = 32 * PPL;
+  __shared__ double red[kThreads / 32][P];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint64_t item = blockIdx.x; item < a.total_items; item += gridDim.x) {
+    const int s = find_sector(item_starts, a.ns, item);
+    const SectorDesc& d = a.sec[s];
+    const uint64_t local = item - d.item0;
+    double acc[PPL];
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) acc[q] = 0.0;
+    double al[PPL];
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) al[q] = (MODE == 1 && alpha) ? alpha[static_cast<uint64_t>(s) * P + lane * PPL + q] : 0.0;
+    const uint64_t r0 = local * kRowsPerItem;
+    for (int i = warp; i < kRowsPerItem; i += kThreads / 32) {
+      const uint64_t r = r0 + i;
+      if (r >= d.n) break;
+      const double w = d.weights ? static_cast<double>(d.weights[r]) : 1.0;
+      double2* x = reinterpret_cast<double2*>(d.buf[ia]) + r * P + lane * PPL;
+      const double2* y = reinterpret_cast<const double2*>(d.buf[ib]) + r * P + lane * PPL;
+#pragma unroll
+      for (int q = 0; q < PPL; ++q) {
+        double2 u = x[q];
+        const double2 v = y[q];
+        if (MODE == 0) {
+          acc[q] = fma(w, u.x * v.x + u.y * v.y, acc[q]);
+        } else {
+          u.x -= al[q] * v.x;
+          u.y -= al[q] * v.y;
+          if (alpha) x[q] = u;
+          acc[q] = fma(w, u.x * u.x + u.y * u.y, acc[q]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) red[warp][lane * PPL + q] = acc[q];
+    __syncthreads();
+    if (threadIdx.x < P) {
+      double t = 0.0;
+      for (int w8 = 0; w8 < kThreads / 32; ++w8) t += red[w8][threadIdx.x];
+      a.partial[item * P + threadIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// out[c] = sum over the sector's items of partial (in item order); SQRT: the
+// square root, and the first step whose beta falls below 1e-12 (scale) is
+// recorded as the exhausted Krylov length.
+__device__ void phase_finish(const ScanArgs& a, double* out, bool sqrt_mode, int step, const double* alpha) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < static_cast<uint64_t>(a.cols);
+       t += stride) {
+    const int s = static_cast<int>(t / a.P), p = static_cast<int>(t % a.P);
+    double v = 0.0;
+    for (uint64_t b = a.sec[s].item0; b < a.sec[s].item0 + a.sec[s].items; ++b) v += a.partial[b * a.P + p];
+    if (sqrt_mode) {
+      v = sqrt(fmax(v, 0.0));
+      const double scale = alpha ? fmax(fabs(alpha[t]), 1.0) : 1.0;
+      if (step >= 0 && a.length[t] < 0 && v <= 1.0e-12 * scale) a.length[t] = step + 1;
+    }
+    out[t] = v;
+  }
+}
+
+// dst = src / beta (0 where beta vanished), one warp per row.
 template <int PPL>
-__global__ void __launch_bounds__(256) scan_apply_kernel(const SectorDesc* __restrict__ sec, int ns,
-                                                         uint64_t total_rows, int K, const double* __restrict__ coef,
-                                                         int cur, int prev, int out,
-                                                         const double* __restrict__ beta_prev) {
+__device__ void phase_scale(const ScanArgs& a, const uint64_t* starts, int isrc, int idst, const double* beta) {
+  constexpr int P = 32 * PPL;
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (uint64_t g = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; g < a.total_rows;
+       g += warps) {
+    const int s = find_sector(starts, a.ns, g);
+    const SectorDesc& d = a.sec[s];
+    const uint64_t r = g - d.row0;
+    const double2* x = reinterpret_cast<const double2*>(d.buf[isrc]) + r * P + lane * PPL;
+    double2* o = reinterpret_cast<double2*>(d.buf[idst]) + r * P + lane * PPL;
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) {
+      const double b = beta[static_cast<uint64_t>(s) * P + lane * PPL + q];
+      const double inv = b > 1.0e-300 ? 1.0 / b : 0.0;
+      const double2 v = x[q];
+      o[q] = make_double2(v.x * inv, v.y * inv);
+    }
+  }
+}
+
+// Start vectors: real parts uniform in [-0.5, 0.5) from a SplitMix64 hash of
+// (seed, sector, point, row), written to `idst`.
+template <int PPL>
+__device__ void phase_init(const ScanArgs& a, const uint64_t* starts, int idst) {
+  constexpr int P = 32 * PPL;
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (uint64_t g = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; g < a.total_rows;
+       g += warps) {
+    const int s = find_sector(starts, a.ns, g);
+    const SectorDesc& d = a.sec[s];
+    const uint64_t r = g - d.row0;
+    double2* o = reinterpret_cast<double2*>(d.buf[idst]) + r * P + lane * PPL;
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) {
+      uint64_t z = a.seed ^ (0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(s) * 4096 + lane * PPL + q + 1)) ^
+                   (r * 0xd1b54a32d192ed03ULL);
+      z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+      z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+      z ^= z >> 31;
+      o[q] = make_double2(static_cast<double>(z >> 11) * (1.0 / 9007199254740992.0) - 0.5, 0.0);
+    }
+  }
+}
+
+// The persistent kernel: (when step == 0) the normalised start vectors, then
+// up to kChunkSteps Lanczos steps of the current pass; the step counter in
+// `state` advances once per completed step.
+template <int PPL, bool PASS2>
+__global__ void __launch_bounds__(kThreads) scan_chunk_kernel(const ScanArgs a) {
+  constexpr int P = 32 * PPL;
+  __shared__ double c[kMaxComp * P];
+  __shared__ uint64_t starts[kMaxSectors], item_starts[kMaxSectors];
+  for (int i = threadIdx.x; i < a.K * P; i += blockDim.x) c[i] = a.coef[i];
+  for (int i = threadIdx.x; i < a.ns; i += blockDim.x) {
+    starts[i] = a.sec[i].row0;
+    item_starts[i] = a.sec[i].item0;
+  }
+  __syncthreads();
+  const unsigned blocks = gridDim.x;
+  ScanState* st = a.state;
+  volatile int* vstep = &st->step;
+  int j = *vstep;
+  const int limit = PASS2 ? st->target_steps : a.max_steps;
+  if (PASS2 ? j >= limit : (st->active == 0 || j >= limit)) return;
+  double* beta0 = a.beta + static_cast<uint64_t>(a.max_steps) * a.cols;
+  if (j == 0) {
+    // z_0 = random / ||random||_R, built in the `work` role of step 0 then scaled into `cur`
+    int cur, prev, work;
+    roles(0, cur, prev, work);
+    phase_init<PPL>(a, starts, work);
+    if (!grid_sync(st, blocks)) return;
+    phase_reduce<PPL, 1>(a, item_starts, work, work, nullptr);
+    if (!grid_sync(st, blocks)) return;
+    phase_finish(a, beta0, true, -1, nullptr);
+    if (!grid_sync(st, blocks)) return;
+    phase_scale<PPL>(a, starts, work, cur, beta0);
+    if (!grid_sync(st, blocks)) return;
+  }
+  for (int n = 0; n < kChunkSteps && j < limit; ++n, ++j) {
+    int cur, prev, work;
+    roles(j, cur, prev, work);
+    double* alpha_j = a.alpha + static_cast<uint64_t>(j) * a.cols;
+    double* beta_j = a.beta + static_cast<uint64_t>(j) * a.cols;
+    phase_apply<PPL, PASS2>(a, starts, c, j);
+    if (!grid_sync(st, blocks)) return;
+    phase_reduce<PPL, 0>(a, item_starts, cur, work, nullptr);
+    if (!grid_sync(st, blocks)) return;
+    phase_finish(a, alpha_j, false, j, nullptr);
+    if (!grid_sync(st, blocks)) return;
+    phase_reduce<PPL, 1>(a, item_starts, work, cur, alpha_j);
+    if (!grid_sync(st, blocks)) return;
+    phase_finish(a, beta_j, true, PASS2 ? -1 : j, alpha_j);
+    if (!grid_sync(st, blocks)) return;
+    // z_{j+1} goes to the role of z_{j-1}, which step j+1 sees as `cur`
+    phase_scale<PPL>(a, starts, work, prev, beta_j);
+    if (!grid_sync(st, blocks)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *vstep = j + 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tridiagonal work per pair (one thread each)
+// ---------------------------------------------------------------------------
+
+struct Tri {
+  const double* alpha;
+  const double* beta;
+  int cols, t, m;
+  __device__ double a(int j) const { return alpha[static_cast<size_t>(j) * cols + t]; }
+  __device__ double b(int j) const { return beta[static_cast<size_t>(j) * cols + t]; }
+};
+
+__device__ int count_below(const Tri& T, double x) {
+  int c = 0;
+  double q = T.a(0) - x;
+  if (q < 0) ++c;
+  for (int j = 1; j < T.m; ++j) {
+    if (q == 0.0) q = 1e-300;
+    const double bb = T.b(j - 1);
+    q = T.a(j) - x - bb * bb / q;
+    if (q < 0) ++c;
+  }
+  return c;
+}
+
+// i-th smallest eigenvalue of T by Sturm bisection (Gershgorin start).
+__device__ double tri_eigenvalue(const Tri& T, int i, double lo, double hi) {
+  double l = lo, h = hi;
+  for (int it = 0; it < 200 && h - l > 2.0e-16 * fmax(fabs(l), fabs(h)) + 1e-300; ++it) {
+    const double mid = 0.5 * (l + h);
+    if (count_below(T, mid) > i) h = mid;
+    else l = mid;
+  }
+  return 0.5 * (l + h);
+}
+
+// Eigenvector of T for the eigenvalue theta by two steps of inverse
+// iteration (LU of T - theta' I without pivoting, theta' nudged off theta);
+// written to s[0..m) with unit norm. Returns its last component.
+__device__ double tri_vector(const Tri& T, double theta, double* s, double* work) {
+  const int m = T.m;
+  const double shift = theta + 1.0e-13 * fmax(fabs(theta), 1.0);
+  for (int j = 0; j < m; ++j) s[j] = 1.0 / sqrt(static_cast<double>(m));
+  for (int sweep = 0; sweep < 2; ++sweep) {
+    // forward elimination: d_j = a_j - shift - b_{j-1}^2 / d_{j-1}; rhs likewise
+    double d = T.a(0) - shift;
+    if (d == 0.0) d = 1e-300;
+    work[0] = d;
+    double y = s[0];
+    s[0] = y;
+    for (int j = 1; j < m; ++j) {
+      const double l = T.b(j - 1) / d;
+      d = T.a(j) - shift - l * T.b(j - 1);
+      if (d == 0.0) d = 1e-300;
+      work[j] = d;
+      s[j] = s[j] - l * s[j - 1];
+    }
+    // back substitution
+    s[m - 1] /= work[m - 1];
+    for (int j = m - 2; j >= 0; --j) s[j] = (s[j] - T.b(j) * s[j + 1]) / work[j];
+    double norm = 0.0;
+    for (int j = 0; j < m; ++j) norm += s[j] * s[j];
+    norm = sqrt(norm);
+    for (int j = 0; j < m; ++j) s[j] /= norm;
+  }
+  return s[m - 1];
+}
+
+// Pass-1 convergence check after `step` steps, for every pair still running:
+// the lowest Ritz values, copies within 1e-8 max(|theta|, 1) counted once,
+// converge when |beta_m s_m| <= 0.1 tol max(|theta|, 1) for the wanted ones
+// (and, when copies were merged, for one more distinct value). Converged
+// pairs record m, the top Ritz value, and the first ncand Ritz values with
+// their T eigenvectors for the second pass.
+__global__ void scan_check_kernel(const ScanArgs a, double* work_all) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int step = a.state->step;
+  if (t >= a.cols || a.stop[t] >= 0 || step == 0) return;
+  int m = step;
+  const bool exhausted = a.length[t] > 0 && a.length[t] <= step;
+  if (exhausted) m = a.length[t];
+  const bool check = exhausted || step % kChunkSteps == 0 || step >= a.max_steps;
+  if (!check) return;
+  Tri T{a.alpha, a.beta, a.cols, t, m};
+  double lo = 1e300, hi = -1e300;
+  for (int j = 0; j < m; ++j) {
+    const double off = (j > 0 ? fabs(T.b(j - 1)) : 0.0) + (j + 1 < m ? fabs(T.b(j)) : 0.0);
+    lo = fmin(lo, T.a(j) - off);
+    hi = fmax(hi, T.a(j) + off);
+  }
+  double* s = a.cand_s + static_cast<size_t>(t) * a.ncand * a.max_steps;
+  double* work = work_all + static_cast<size_t>(t) * a.max_steps;
+  const double beta_m = exhausted ? 0.0 : T.b(m - 1);
+  const int n = min(a.ncand, m);
+  double theta[kMaxCand];
+  bool converged = true;
+  int distinct = 0, merged = 0;
+  double last = 0.0;
+  for (int i = 0; i < n; ++i) {
+    theta[i] = tri_eigenvalue(T, i, lo, hi);
+    const double scale = fmax(fabs(theta[i]), 1.0);
+    const bool copy = i > 0 && theta[i] - last <= 1.0e-8 * scale;
+    const bool needed = distinct < a.eigenpairs || (merged > 0 && distinct < a.eigenpairs + 1);
+    if (!copy) last = theta[i];
+    if (copy) ++merged;
+    if (!needed && !copy) break;
+    const double last_component = tri_vector(T, theta[i], s + static_cast<size_t>(i) * a.max_steps, work);
+    if (!(fabs(beta_m * last_component) <= 0.1 * a.tolerance * scale)) converged = false;
+    if (!copy) ++distinct;
+  }
+  if (!converged && !exhausted && step < a.max_steps) return;
+  // record the candidates (vectors of the ones not computed above)
+  for (int i = 0; i < n; ++i) {
+    theta[i] = tri_eigenvalue(T, i, lo, hi);
+    tri_vector(T, theta[i], s + static_cast<size_t>(i) * a.max_steps, work);
+    a.cand_theta[static_cast<size_t>(t) * a.ncand + i] = theta[i];
+  }
+  for (int i = n; i < a.ncand; ++i) a.cand_theta[static_cast<size_t>(t) * a.ncand + i] = NAN;
+  a.top[t] = tri_eigenvalue(T, m - 1, lo, hi);
+  a.stop[t] = converged ? m : -2 - m;  // -2 - m: stopped at max_steps without convergence
+  atomicSub(&a.state->active, 1);
+}
+
+// Second-pass results: for candidate i of every pair, sums over the rows of
+// R |v|^2, R Re(conj(v) H v), R |H v - theta v|^2 and the overlaps R Re(conj(v_i) v_k).
+template <int PPL>
+__global__ void __launch_bounds__(kThreads) scan_verify_kernel(const SectorDesc* __restrict__ sec, int ns, int P,
+                                                               int ncand, int cand, const double* __restrict__ theta,
+                                                               int hv_buf, double* __restrict__ partial) {
+  // partial[item][c][q]: q = 0 |v|^2, 1 v.Hv, 2 |Hv - theta v|^2, 3 + k overlap with candidate k
+  const int s_count = ns;
+  __shared__ uint64_t item_starts[kMaxSectors];
+  for (int i = threadIdx.x; i < s_count; i += blockDim.x) item_starts[i] = sec[i].item0;
+  __syncthreads();
+  const int s = find_sector(item_starts, s_count, blockIdx.x);
+  const SectorDesc& d = sec[s];
+  const uint64_t local = blockIdx.x - d.item0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int Q = 3 + kMaxCand;
+  double acc[PPL][Q];
+#pragma unroll
+  for (int q = 0; q < PPL; ++q)
+#pragma unroll
+    for (int u = 0; u < Q; ++u) acc[q][u] = 0.0;
+  const uint64_t r0 = local * kRowsPerItem;
+  for (int i = warp; i < kRowsPerItem; i += kThreads / 32) {
+    const uint64_t r = r0 + i;
+    if (r >= d.n) break;
+    const double w = d.weights ? static_cast<double>(d.weights[r]) : 1.0;
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) {
+      const uint64_t off = r * P + lane * PPL + q;
+      const int colidx = s * P + lane * PPL + q;
+      const double2 v = reinterpret_cast<const double2*>(d.ritz[cand])[off];
+      const double2 h = reinterpret_cast<const double2*>(d.buf[hv_buf])[off];
+      const double th = theta[static_cast<size_t>(colidx) * ncand + cand];
+      const double rr = h.x - th * v.x, ri = h.y - th * v.y;
+      acc[q][0] = fma(w, v.x * v.x + v.y * v.y, acc[q][0]);
+      acc[q][1] = fma(w, v.x * h.x + v.y * h.y, acc[q][1]);
+      acc[q][2] = fma(w, rr * rr + ri * ri, acc[q][2]);
+      for (int k = 0; k < ncand; ++k) {
+        const double2 u = reinterpret_cast<const double2*>(d.ritz[k])[off];
+        acc[q][3 + k] = fma(w, v.x * u.x + v.y * u.y, acc[q][3 + k]);
+      }
+    }
+  }
+  __shared__ double red[kThreads / 32][64 * 2][1];
+  for (int u = 0; u < Q; ++u) {
+#pragma unroll
+    for (int q = 0; q < PPL; ++q) red[warp][lane * PPL + q][0] = acc[q][u];
+    __syncthreads();
+    if (threadIdx.x < P) {
+      double t = 0.0;
+      for (int w8 = 0; w8 < kThreads / 32; ++w8) t += red[w8][threadIdx.x][0];
+      partial[(static_cast<uint64_t>(blockIdx.x) * P + threadIdx.x) * Q + u] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Applies H(s, p) to a Ritz accumulator (second-pass verification): one warp per row.
+template <int PPL>
+__global__ void __launch_bounds__(kThreads) scan_hv_kernel(const SectorDesc* __restrict__ sec, int ns, uint64_t total_rows,
+                                                           int K, const double* __restrict__ coef, int cand, int out_buf) {
   constexpr int P = 32 * PPL;
   __shared__ double c[kMaxComp * P];
   __shared__ uint64_t starts[kMaxSectors];
@@ -83,7 +591,7 @@ __global__ void __launch_bounds__(256) scan_apply_kernel(const SectorDesc* __res
     const int s = find_sector(starts, ns, g);
     const SectorDesc& d = sec[s];
     const uint64_t r = g - d.row0;
-    const double* z = d.buf[cur];
+    const double* z = d.ritz[cand];
     double are[PPL], aim[PPL], dsum[PPL];
 #pragma unroll
     for (int q = 0; q < PPL; ++q) are[q] = aim[q] = dsum[q] = 0.0;
@@ -109,189 +617,19 @@ __global__ void __launch_bounds__(256) scan_apply_kernel(const SectorDesc* __res
       for (int q = 0; q < PPL; ++q) dsum[q] = fma(ck[q], dr, dsum[q]);
     }
     const double2* zs = reinterpret_cast<const double2*>(z) + r * P + lane * PPL;
-    const double2* pv = reinterpret_cast<const double2*>(d.buf[prev]) + r * P + lane * PPL;
-    double2* o = reinterpret_cast<double2*>(d.buf[out]) + r * P + lane * PPL;
+    double2* o = reinterpret_cast<double2*>(d.buf[out_buf]) + r * P + lane * PPL;
 #pragma unroll
     for (int q = 0; q < PPL; ++q) {
       const double2 x = zs[q];
-      double wr = are[q] + dsum[q] * x.x, wi = aim[q] + dsum[q] * x.y;
-      if (beta_prev) {
-        const double b = beta_prev[static_cast<uint64_t>(s) * P + lane * PPL + q];
-        const double2 y = pv[q];
-        wr -= b * y.x;
-        wi -= b * y.y;
-      }
-      o[q] = make_double2(wr, wi);
+      o[q] = make_double2(are[q] + dsum[q] * x.x, aim[q] + dsum[q] * x.y);
     }
   }
 }
 
-// Reduction blocks: rows [b * kRowsPerBlock, ...) of one sector.
-// MODE 0: partial[b][p] = sum_r R_r Re(conj(a) b)        (alpha)
-// MODE 1: a -= alpha(s, p) b; partial = sum_r R_r |a|^2  (update + beta^2; alpha may be null)
-template <int PPL, int MODE>
-__global__ void __launch_bounds__(256) scan_reduce_kernel(const SectorDesc* __restrict__ sec, int ns, int ia, int ib,
-                                                          const double* __restrict__ alpha,
-                                                          double* __restrict__ partial) {
-  constexpr int P = 32 * PPL;
-  __shared__ uint64_t bstarts[kMaxSectors];
-  __shared__ double red[8][P];
-  for (int i = threadIdx.x; i < ns; i += blockDim.x) bstarts[i] = sec[i].block0;
-  __syncthreads();
-  const int s = find_sector(bstarts, ns, blockIdx.x);
-  const SectorDesc& d = sec[s];
-  const uint64_t local_block = blockIdx.x - d.block0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double acc[PPL];
-#pragma unroll
-  for (int q = 0; q < PPL; ++q) acc[q] = 0.0;
-  double al[PPL];
-#pragma unroll
-  for (int q = 0; q < PPL; ++q) al[q] = (MODE == 1 && alpha) ? alpha[static_cast<uint64_t>(s) * P + lane * PPL + q] : 0.0;
-  const uint64_t r0 = local_block * kRowsPerBlock;
-  for (int i = warp; i < kRowsPerBlock; i += 8) {
-    const uint64_t r = r0 + i;
-    if (r >= d.n) break;
-    const double w = d.weights ? static_cast<double>(d.weights[r]) : 1.0;
-    double2* a = reinterpret_cast<double2*>(d.buf[ia]) + r * P + lane * PPL;
-    const double2* b = reinterpret_cast<const double2*>(d.buf[ib]) + r * P + lane * PPL;
-#pragma unroll
-    for (int q = 0; q < PPL; ++q) {
-      double2 x = a[q];
-      const double2 y = b[q];
-      if (MODE == 0) {
-        acc[q] = fma(w, x.x * y.x + x.y * y.y, acc[q]);
-      } else {
-        x.x -= al[q] * y.x;
-        x.y -= al[q] * y.y;
-        if (alpha) a[q] = x;
-        acc[q] = fma(w, x.x * x.x + x.y * x.y, acc[q]);
-      }
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < PPL; ++q) red[warp][lane * PPL + q] = acc[q];
-  __syncthreads();
-  if (threadIdx.x < P) {
-    double t = 0.0;
-    for (int w8 = 0; w8 < 8; ++w8) t += red[w8][threadIdx.x];
-    partial[static_cast<uint64_t>(blockIdx.x) * P + threadIdx.x] = t;
-  }
-}
-
-// out[s][p] = sum over sector s's blocks of partial (in block order); SQRT: sqrt
-// of it, and the first step whose beta falls below 1e-12 (scale) is recorded.
-__global__ void scan_finish_kernel(const SectorDesc* __restrict__ sec, int ns, int P, const double* __restrict__ partial,
-                                   double* __restrict__ out, int sqrt_mode, int* __restrict__ length, int step,
-                                   const double* __restrict__ alpha) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ns * P) return;
-  const int s = t / P, p = t % P;
-  double v = 0.0;
-  for (uint64_t b = sec[s].block0; b < sec[s].block0 + sec[s].blocks; ++b) v += partial[b * P + p];
-  if (sqrt_mode) {
-    v = sqrt(fmax(v, 0.0));
-    const double scale = alpha ? fmax(fabs(alpha[t]), 1.0) : 1.0;
-    if (length && length[t] < 0 && v <= 1.0e-12 * scale) length[t] = step + 1;
-  }
-  out[t] = v;
-}
-
-// dst = src / beta(s, p) (0 where beta is 0)
-template <int PPL>
-__global__ void scan_scale_kernel(const SectorDesc* __restrict__ sec, int ns, uint64_t total_rows, int isrc, int idst,
-                                  const double* __restrict__ beta) {
-  constexpr int P = 32 * PPL;
-  __shared__ uint64_t starts[kMaxSectors];
-  for (int i = threadIdx.x; i < ns; i += blockDim.x) starts[i] = sec[i].row0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
-  for (uint64_t g = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; g < total_rows; g += warps) {
-    const int s = find_sector(starts, ns, g);
-    const SectorDesc& d = sec[s];
-    const uint64_t r = g - d.row0;
-    const double2* a = reinterpret_cast<const double2*>(d.buf[isrc]) + r * P + lane * PPL;
-    double2* o = reinterpret_cast<double2*>(d.buf[idst]) + r * P + lane * PPL;
-#pragma unroll
-    for (int q = 0; q < PPL; ++q) {
-      const double b = beta[static_cast<uint64_t>(s) * P + lane * PPL + q];
-      const double inv = b > 1.0e-300 ? 1.0 / b : 0.0;
-      const double2 x = a[q];
-      o[q] = make_double2(x.x * inv, x.y * inv);
-    }
-  }
-}
-
-// start vectors: real parts uniform in [-0.5, 0.5) from a splitmix64 hash of (seed, sector, point, row)
-template <int PPL>
-__global__ void scan_init_kernel(const SectorDesc* __restrict__ sec, int ns, uint64_t total_rows, int idst,
-                                 uint64_t seed) {
-  constexpr int P = 32 * PPL;
-  __shared__ uint64_t starts[kMaxSectors];
-  for (int i = threadIdx.x; i < ns; i += blockDim.x) starts[i] = sec[i].row0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
-  for (uint64_t g = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; g < total_rows; g += warps) {
-    const int s = find_sector(starts, ns, g);
-    const SectorDesc& d = sec[s];
-    const uint64_t r = g - d.row0;
-    double2* o = reinterpret_cast<double2*>(d.buf[idst]) + r * P + lane * PPL;
-#pragma unroll
-    for (int q = 0; q < PPL; ++q) {
-      uint64_t z = seed ^ (0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(s) * 4096 + lane * PPL + q + 1)) ^ (r * 0xd1b54a32d192ed03ULL);
-      z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
-      z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
-      z ^= z >> 31;
-      o[q] = make_double2(static_cast<double>(z >> 11) * (1.0 / 9007199254740992.0) - 0.5, 0.0);
-    }
-  }
-}
-
-// Lowest `m_out` eigenvalues of each pair's tridiagonal T (alpha_j, beta_j for
-// j < length) by Sturm bisection; one thread per pair.
-__global__ void scan_tridiagonal_kernel(int cols, int steps, const double* __restrict__ alpha_hist,
-                                        const double* __restrict__ beta_hist, const int* __restrict__ length,
-                                        int m_out, double* __restrict__ values) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= cols) return;
-  int m = steps;
-  if (length[t] > 0 && length[t] < m) m = length[t];
-  auto a = [&](int j) { return alpha_hist[static_cast<size_t>(j) * cols + t]; };
-  auto b = [&](int j) { return beta_hist[static_cast<size_t>(j) * cols + t]; };
-  double lo = 1e300, hi = -1e300;
-  for (int j = 0; j < m; ++j) {
-    const double off = (j > 0 ? fabs(b(j - 1)) : 0.0) + (j + 1 < m ? fabs(b(j)) : 0.0);
-    lo = fmin(lo, a(j) - off);
-    hi = fmax(hi, a(j) + off);
-  }
-  auto count_below = [&](double x) {
-    int c = 0;
-    double q = a(0) - x;
-    if (q < 0) ++c;
-    for (int j = 1; j < m; ++j) {
-      if (q == 0.0) q = 1e-300;
-      const double bb = b(j - 1);
-      q = a(j) - x - bb * bb / q;
-      if (q < 0) ++c;
-    }
-    return c;
-  };
-  for (int i = 0; i < m_out; ++i) {
-    if (i >= m) {
-      values[static_cast<size_t>(t) * m_out + i] = NAN;
-      continue;
-    }
-    double l = lo, h = hi;
-    for (int it = 0; it < 200 && h - l > 4.0e-16 * fmax(fabs(l), fabs(h)) + 1e-300; ++it) {
-      const double mid = 0.5 * (l + h);
-      if (count_below(mid) > i) h = mid;
-      else l = mid;
-    }
-    values[static_cast<size_t>(t) * m_out + i] = 0.5 * (l + h);
-  }
-}
+// A kernel that waits at the grid barrier for one more block than it has:
+// the bounded spin must end with kStatusBarrierTimeout (used by the test of
+// the time-out path).
+__global__ void barrier_selftest_kernel(ScanState* st) { grid_sync(st, gridDim.x + 1); }
 
 template <typename F>
 void by_points(int P, F&& f) {
@@ -300,6 +638,25 @@ void by_points(int P, F&& f) {
 }
 
 }  // namespace
+
+int scan_barrier_selftest(int device) {
+  QMBED_CUDA(cudaSetDevice(device));
+  DeviceBuffer state(sizeof(ScanState));
+  QMBED_CUDA(cudaMemset(state.get(), 0, sizeof(ScanState)));
+  int sms = 148, per_sm = 0;
+  QMBED_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  QMBED_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, barrier_selftest_kernel, 32, 0));
+  ScanState* st = state.as<ScanState>();
+  void* args[] = {&st};
+  const unsigned grid = static_cast<unsigned>(std::max(1, std::min(2, per_sm)) * sms);
+  QMBED_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(barrier_selftest_kernel), dim3(grid), dim3(32), args,
+                                         0, nullptr));
+  QMBED_LAUNCH_CHECK();
+  QMBED_CUDA(cudaDeviceSynchronize());
+  ScanState host{};
+  QMBED_CUDA(cudaMemcpy(&host, state.get(), sizeof(ScanState), cudaMemcpyDeviceToHost));
+  return host.status;
+}
 
 ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& components,
                        const std::vector<double>& coefficients, int points, int eigenpairs, double tolerance,
@@ -312,15 +669,19 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
   if (eigenpairs < 1 || eigenpairs > 4) raise(QMBED_INVALID_OPTIONS, "a scan returns 1 to 4 eigenvalues per pair");
   if (!(tolerance > 0.0) || max_steps < 1) raise(QMBED_INVALID_OPTIONS, "tolerance and steps must be positive");
   if (static_cast<int>(coefficients.size()) != points * K) raise(QMBED_DIMENSION_MISMATCH, "coefficients must be points x components");
+  const auto t_start = std::chrono::steady_clock::now();
   const int P = points <= 32 ? 32 : 64;
+  const int ncand = eigenpairs + 2;
   const cudaStream_t stream = ops.stream();
+  int device = 0;
+  QMBED_CUDA(cudaGetDevice(&device));
   // coefficients padded to P columns by repeating the last point
   std::vector<double> coef(static_cast<size_t>(K) * P);
   for (int k = 0; k < K; ++k)
     for (int p = 0; p < P; ++p) coef[static_cast<size_t>(k) * P + p] = coefficients[static_cast<size_t>(std::min(p, points - 1)) * K + k];
   std::vector<SectorDesc> desc(ns);
-  uint64_t rows = 0, blocks = 0;
-  size_t block_bytes_total = 0;
+  uint64_t rows = 0, items = 0;
+  size_t set_bytes = 0;  // one vector set (every sector's rows x P complex FP64)
   for (int s = 0; s < ns; ++s) {
     if (static_cast<int>(components[s].size()) != K) raise(QMBED_DIMENSION_MISMATCH, "every sector needs the same components");
     const SpinOperator* first = components[s][0];
@@ -328,12 +689,12 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
     std::memset(&d, 0, sizeof(d));
     d.n = first->dim();
     d.row0 = rows;
-    d.block0 = blocks;
-    d.blocks = (d.n + kRowsPerBlock - 1) / kRowsPerBlock;
+    d.item0 = items;
+    d.items = (d.n + kRowsPerItem - 1) / kRowsPerItem;
     d.weights = first->basis().symmetric() ? first->basis().orbits() : nullptr;
     rows += d.n;
-    blocks += d.blocks;
-    block_bytes_total += 3 * d.n * P * 16;
+    items += d.items;
+    set_bytes += d.n * P * 16;
     for (int k = 0; k < K; ++k) {
       const SpinOperator* op = components[s][k];
       if (op->dim() != d.n || &op->basis() != &first->basis())
@@ -343,95 +704,232 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
     }
   }
   const int cols = ns * P;
-  DeviceBuffer blocks_mem(block_bytes_total), desc_dev(ns * sizeof(SectorDesc)), coef_dev(coef.size() * sizeof(double));
-  DeviceBuffer partial(std::max<uint64_t>(blocks, 1) * P * sizeof(double));
+  DeviceBuffer lanczos_mem(3 * set_bytes), ritz_mem(static_cast<size_t>(ncand) * set_bytes);
+  DeviceBuffer desc_dev(ns * sizeof(SectorDesc)), coef_dev(coef.size() * sizeof(double));
+  constexpr int Q = 3 + kMaxCand;
+  DeviceBuffer partial(std::max<uint64_t>(items, 1) * P * Q * sizeof(double));
   DeviceBuffer alpha_hist(static_cast<size_t>(max_steps) * cols * sizeof(double));
   DeviceBuffer beta_hist(static_cast<size_t>(max_steps + 1) * cols * sizeof(double));
-  DeviceBuffer length(cols * sizeof(int)), ritz(static_cast<size_t>(cols) * kLowest * sizeof(double));
-  size_t offset = 0;
-  for (int s = 0; s < ns; ++s)
+  DeviceBuffer length(cols * sizeof(int)), stop(cols * sizeof(int));
+  DeviceBuffer cand_s(static_cast<size_t>(cols) * ncand * max_steps * sizeof(double));
+  DeviceBuffer cand_theta(static_cast<size_t>(cols) * ncand * sizeof(double)), top(cols * sizeof(double));
+  DeviceBuffer tri_work(static_cast<size_t>(cols) * max_steps * sizeof(double));
+  DeviceBuffer state(sizeof(ScanState));
+  size_t offset = 0, roffset = 0;
+  for (int s = 0; s < ns; ++s) {
     for (int b = 0; b < 3; ++b) {
-      desc[s].buf[b] = reinterpret_cast<double*>(static_cast<char*>(blocks_mem.get()) + offset);
+      desc[s].buf[b] = reinterpret_cast<double*>(lanczos_mem.as<char>() + offset);
       offset += desc[s].n * P * 16;
     }
+    for (int i = 0; i < ncand; ++i) {
+      desc[s].ritz[i] = reinterpret_cast<double*>(ritz_mem.as<char>() + roffset);
+      roffset += desc[s].n * P * 16;
+    }
+  }
   QMBED_CUDA(cudaMemcpyAsync(desc_dev.get(), desc.data(), ns * sizeof(SectorDesc), cudaMemcpyHostToDevice, stream));
   QMBED_CUDA(cudaMemcpyAsync(coef_dev.get(), coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-  QMBED_CUDA(cudaMemsetAsync(length.get(), 0xff, cols * sizeof(int), stream));  // -1: no breakdown yet
-  const SectorDesc* sd = desc_dev.as<SectorDesc>();
-  const int row_grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((rows * 32 + 255) / 256, 16ull * ops.sms())));
-  const int red_grid = static_cast<int>(blocks);
-  const int fin_grid = (cols + 127) / 128;
-  double* beta0 = beta_hist.as<double>() + static_cast<size_t>(max_steps) * cols;  // start-vector norms
+  QMBED_CUDA(cudaMemsetAsync(length.get(), 0xff, cols * sizeof(int), stream));  // -1: not exhausted
+  QMBED_CUDA(cudaMemsetAsync(stop.get(), 0xff, cols * sizeof(int), stream));    // -1: running
+  QMBED_CUDA(cudaMemsetAsync(ritz_mem.get(), 0, static_cast<size_t>(ncand) * set_bytes, stream));
+  ScanState init{};
+  init.pass = 1;
+  init.active = cols;
+  QMBED_CUDA(cudaMemcpyAsync(state.get(), &init, sizeof(ScanState), cudaMemcpyHostToDevice, stream));
+
+  ScanArgs a{};
+  a.sec = desc_dev.as<SectorDesc>();
+  a.ns = ns;
+  a.P = P;
+  a.K = K;
+  a.cols = cols;
+  a.points = points;
+  a.eigenpairs = eigenpairs;
+  a.max_steps = max_steps;
+  a.ncand = ncand;
+  a.total_rows = rows;
+  a.total_items = items;
+  a.coef = coef_dev.as<double>();
+  a.partial = partial.as<double>();
+  a.alpha = alpha_hist.as<double>();
+  a.beta = beta_hist.as<double>();
+  a.length = length.as<int>();
+  a.stop = stop.as<int>();
+  a.cand_s = cand_s.as<double>();
+  a.cand_theta = cand_theta.as<double>();
+  a.top = top.as<double>();
+  a.tolerance = tolerance;
+  a.seed = seed;
+  a.state = state.as<ScanState>();
 
   ScanResult result;
-  result.eigenvalues.assign(static_cast<size_t>(ns) * points * eigenpairs, std::nan(""));
-  result.steps.assign(static_cast<size_t>(ns) * points, -1);
+  ScanState* host_state = nullptr;
+  QMBED_CUDA(cudaMallocHost(&host_state, sizeof(ScanState)));
+  struct PinnedFree {
+    ScanState* p;
+    ~PinnedFree() { cudaFreeHost(p); }
+  } pinned_guard{host_state};
+  auto read_state = [&] {
+    QMBED_CUDA(cudaMemcpyAsync(host_state, state.get(), sizeof(ScanState), cudaMemcpyDeviceToHost, stream));
+    QMBED_CUDA(cudaStreamSynchronize(stream));
+    if (host_state->status == kStatusBarrierTimeout)
+      raise(QMBED_DEVICE_TIMEOUT, "batched scan: a grid barrier timed out (not every block of the persistent "
+                                  "launch was resident)");
+  };
+
   by_points(P, [&](auto ptag) {
     constexpr int PPL = decltype(ptag)::value;
-    int cur = 0, prev = 1, work = 2;
-    // normalised start vectors in buffer `cur`
-    scan_init_kernel<PPL><<<row_grid, 256, 0, stream>>>(sd, ns, rows, work, seed);
-    scan_reduce_kernel<PPL, 1><<<red_grid, 256, 0, stream>>>(sd, ns, work, work, nullptr, partial.as<double>());
-    scan_finish_kernel<<<fin_grid, 128, 0, stream>>>(sd, ns, P, partial.as<double>(), beta0, 1, nullptr, 0, nullptr);
-    scan_scale_kernel<PPL><<<row_grid, 256, 0, stream>>>(sd, ns, rows, work, cur, beta0);
-    QMBED_LAUNCH_CHECK();
-    std::vector<double> previous(static_cast<size_t>(cols) * eigenpairs, std::nan("")), host(static_cast<size_t>(cols) * kLowest);
-    std::vector<int> host_len(cols);
-    std::vector<char> done(cols, 0);
-    int active = cols;
-    for (int j = 0; j < max_steps && active > 0; ++j) {
-      double* alpha_j = alpha_hist.as<double>() + static_cast<size_t>(j) * cols;
-      double* beta_j = beta_hist.as<double>() + static_cast<size_t>(j) * cols;
-      const double* beta_prev = j > 0 ? beta_hist.as<double>() + static_cast<size_t>(j - 1) * cols : nullptr;
-      scan_apply_kernel<PPL><<<row_grid, 256, 0, stream>>>(sd, ns, rows, K, coef_dev.as<double>(), cur, prev, work, beta_prev);
-      scan_reduce_kernel<PPL, 0><<<red_grid, 256, 0, stream>>>(sd, ns, cur, work, nullptr, partial.as<double>());
-      scan_finish_kernel<<<fin_grid, 128, 0, stream>>>(sd, ns, P, partial.as<double>(), alpha_j, 0, nullptr, j, nullptr);
-      scan_reduce_kernel<PPL, 1><<<red_grid, 256, 0, stream>>>(sd, ns, work, cur, alpha_j, partial.as<double>());
-      scan_finish_kernel<<<fin_grid, 128, 0, stream>>>(sd, ns, P, partial.as<double>(), beta_j, 1, length.as<int>(), j, alpha_j);
-      scan_scale_kernel<PPL><<<row_grid, 256, 0, stream>>>(sd, ns, rows, work, prev, beta_j);
+    auto grid_of = [&](const void* kernel) {
+      int per_sm = 0;
+      QMBED_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0));
+      if (per_sm < 1) raise(QMBED_UNSUPPORTED_BACKEND, "the persistent scan kernel does not fit on an SM");
+      return static_cast<unsigned>(per_sm * ops.sms());
+    };
+    const void* k1 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false>);
+    const void* k2 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true>);
+    const unsigned grid1 = grid_of(k1), grid2 = grid_of(k2);
+    const int check_grid = (cols + 127) / 128;
+    double* tri = tri_work.as<double>();
+    ScanArgs args = a;
+    void* kargs[] = {&args};
+    auto chunk = [&](bool pass2) {
+      QMBED_CUDA(cudaLaunchCooperativeKernel(pass2 ? k2 : k1, dim3(pass2 ? grid2 : grid1), dim3(kThreads), kargs, 0,
+                                             stream));
       QMBED_LAUNCH_CHECK();
-      std::swap(cur, prev);  // the new vector went to the old prev buffer
-      result.total_steps = j + 1;
-      if ((j + 1) % kCheck != 0 && j + 1 != max_steps) continue;
-      scan_tridiagonal_kernel<<<fin_grid, 128, 0, stream>>>(cols, j + 1, alpha_hist.as<double>(), beta_hist.as<double>(),
-                                                            length.as<int>(), kLowest, ritz.as<double>());
-      QMBED_LAUNCH_CHECK();
-      QMBED_CUDA(cudaMemcpyAsync(host.data(), ritz.get(), host.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
-      QMBED_CUDA(cudaMemcpyAsync(host_len.data(), length.get(), cols * sizeof(int), cudaMemcpyDeviceToHost, stream));
-      QMBED_CUDA(cudaStreamSynchronize(stream));
-      for (int c = 0; c < cols; ++c) {
-        if (done[c]) continue;
-        // lowest distinct Ritz values (copies from lost orthogonality merged)
-        std::vector<double> distinct;
-        for (int i = 0; i < kLowest && static_cast<int>(distinct.size()) < eigenpairs; ++i) {
-          const double v = host[static_cast<size_t>(c) * kLowest + i];
-          if (std::isnan(v)) break;
-          if (distinct.empty() || v - distinct.back() > 1.0e-8 * std::max(std::fabs(v), 1.0)) distinct.push_back(v);
-        }
-        const bool exhausted = host_len[c] > 0;
-        bool converged = static_cast<int>(distinct.size()) == eigenpairs || exhausted;
-        for (int i = 0; i < eigenpairs && converged; ++i) {
-          if (i >= static_cast<int>(distinct.size())) break;
-          const double old = previous[static_cast<size_t>(c) * eigenpairs + i];
-          if (!exhausted && !(std::fabs(distinct[i] - old) <= 1.0e-3 * tolerance * std::max(std::fabs(distinct[i]), 1.0)))
-            converged = false;
-        }
-        for (int i = 0; i < eigenpairs; ++i)
-          previous[static_cast<size_t>(c) * eigenpairs + i] = i < static_cast<int>(distinct.size()) ? distinct[i] : std::nan("");
-        if (!converged) continue;
-        done[c] = 1;
-        --active;
-        const int s = c / P, p = c % P;
-        if (p >= points) continue;
-        result.steps[static_cast<size_t>(s) * points + p] = exhausted ? std::min(j + 1, host_len[c]) : j + 1;
-        result.applications += static_cast<size_t>(j + 1);
-        for (int i = 0; i < eigenpairs && i < static_cast<int>(distinct.size()); ++i)
-          result.eigenvalues[(static_cast<size_t>(s) * points + p) * eigenpairs + i] = distinct[i];
+      if (!pass2) {
+        scan_check_kernel<<<check_grid, 128, 0, stream>>>(args, tri);
+        QMBED_LAUNCH_CHECK();
       }
+      QMBED_CUDA(cudaMemcpyAsync(host_state, state.get(), sizeof(ScanState), cudaMemcpyDeviceToHost, stream));
+    };
+    // Pass 1: one chunk captured in a graph, replayed until every pair stopped.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool graph_ok = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (graph_ok) {
+      chunk(false);
+      graph_ok = cudaStreamEndCapture(stream, &graph) == cudaSuccess && graph &&
+                 cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
     }
+    if (!graph_ok) {
+      (void)cudaGetLastError();  // capture not available: launch the chunks directly
+      cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(stream, &capture) == cudaSuccess && capture != cudaStreamCaptureStatusNone) {
+        cudaGraph_t discarded = nullptr;
+        cudaStreamEndCapture(stream, &discarded);
+        if (discarded) cudaGraphDestroy(discarded);
+      }
+      if (graph) cudaGraphDestroy(graph);
+      graph = nullptr;
+      exec = nullptr;
+    }
+    result.graph = graph_ok;
+    const int max_chunks = (max_steps + kChunkSteps - 1) / kChunkSteps + 1;
+    for (int c = 0; c < max_chunks; ++c) {
+      if (exec) QMBED_CUDA(cudaGraphLaunch(exec, stream));
+      else chunk(false);
+      QMBED_CUDA(cudaStreamSynchronize(stream));
+      if (host_state->status == kStatusBarrierTimeout) break;
+      if (host_state->active == 0 || host_state->step >= max_steps) break;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    read_state();
+    result.total_steps = host_state->step;
+    result.pass1_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+
+    std::vector<int> host_stop(cols);
+    QMBED_CUDA(cudaMemcpy(host_stop.data(), stop.get(), cols * sizeof(int), cudaMemcpyDeviceToHost));
+    int target = 0;
+    for (int c = 0; c < cols; ++c) {
+      const int m = host_stop[c] >= 0 ? host_stop[c] : (host_stop[c] <= -2 ? -2 - host_stop[c] : 0);
+      target = std::max(target, m);
+      if ((c % P) < points) result.applications += static_cast<size_t>(m);
+    }
+    // Pass 2: the same recurrence from the same start vectors, accumulating
+    // the candidates' Ritz vectors (the stop array now bounds each pair's steps).
+    std::vector<int> bounded(cols);
+    for (int c = 0; c < cols; ++c) bounded[c] = host_stop[c] >= 0 ? host_stop[c] : (host_stop[c] <= -2 ? -2 - host_stop[c] : 0);
+    QMBED_CUDA(cudaMemcpyAsync(stop.get(), bounded.data(), cols * sizeof(int), cudaMemcpyHostToDevice, stream));
+    ScanState second{};
+    second.pass = 2;
+    second.target_steps = target;
+    QMBED_CUDA(cudaMemcpyAsync(state.get(), &second, sizeof(ScanState), cudaMemcpyHostToDevice, stream));
+    for (int c = 0; c * kChunkSteps < target + kChunkSteps; ++c) {
+      chunk(true);
+      QMBED_CUDA(cudaStreamSynchronize(stream));
+      if (host_state->status == kStatusBarrierTimeout || host_state->step >= target) break;
+    }
+    read_state();
+    result.pass2_steps = target;
+    // Verification: H v for every candidate, then the per-pair sums.
+    const int row_grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((rows * 32 + 255) / 256, 16ull * ops.sms())));
+    std::vector<double> sums(static_cast<size_t>(cols) * ncand * Q, 0.0), host_partial;
+    for (int i = 0; i < ncand; ++i) {
+      scan_hv_kernel<PPL><<<row_grid, kThreads, 0, stream>>>(a.sec, ns, rows, K, a.coef, i, 0);
+      QMBED_LAUNCH_CHECK();
+      scan_verify_kernel<PPL><<<static_cast<unsigned>(items), kThreads, 0, stream>>>(a.sec, ns, P, ncand, i,
+                                                                                     a.cand_theta, 0, a.partial);
+      QMBED_LAUNCH_CHECK();
+      host_partial.resize(static_cast<size_t>(items) * P * Q);
+      QMBED_CUDA(cudaMemcpyAsync(host_partial.data(), a.partial, host_partial.size() * sizeof(double),
+                                 cudaMemcpyDeviceToHost, stream));
+      QMBED_CUDA(cudaStreamSynchronize(stream));
+      for (int s = 0; s < ns; ++s)
+        for (uint64_t b = desc[s].item0; b < desc[s].item0 + desc[s].items; ++b)
+          for (int p = 0; p < P; ++p)
+            for (int u = 0; u < Q; ++u)
+              sums[((static_cast<size_t>(s) * P + p) * ncand + i) * Q + u] += host_partial[(b * P + p) * Q + u];
+    }
+    result.applications_verification = static_cast<size_t>(target) * points * ns + static_cast<size_t>(ncand) * points * ns;
+    std::vector<double> theta(static_cast<size_t>(cols) * ncand), host_top(cols);
+    QMBED_CUDA(cudaMemcpy(theta.data(), cand_theta.get(), theta.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    QMBED_CUDA(cudaMemcpy(host_top.data(), top.get(), cols * sizeof(double), cudaMemcpyDeviceToHost));
+    result.eigenvalues.assign(static_cast<size_t>(ns) * points * eigenpairs, std::nan(""));
+    result.residuals.assign(static_cast<size_t>(ns) * points * eigenpairs, std::nan(""));
+    result.e_max.assign(static_cast<size_t>(ns) * points, std::nan(""));
+    result.steps.assign(static_cast<size_t>(ns) * points, -1);
+    bool all_ok = true;
+    for (int s = 0; s < ns; ++s)
+      for (int p = 0; p < points; ++p) {
+        const int c = s * P + p;
+        const size_t out = static_cast<size_t>(s) * points + p;
+        result.steps[out] = host_stop[c] >= 0 ? host_stop[c] : -1;
+        result.e_max[out] = host_top[c];
+        auto S = [&](int i, int u) { return sums[(static_cast<size_t>(c) * ncand + i) * Q + u]; };
+        // accept candidates in ascending order; a close candidate whose vector
+        // overlaps an accepted one by more than 1/2 is a copy of it
+        std::vector<int> accepted;
+        for (int i = 0; i < ncand && static_cast<int>(accepted.size()) < eigenpairs; ++i) {
+          const double th = theta[static_cast<size_t>(c) * ncand + i];
+          if (std::isnan(th) || !(S(i, 0) > 0.0)) continue;
+          bool copy = false;
+          for (int k : accepted) {
+            const double overlap = std::fabs(S(i, 3 + k)) / std::sqrt(S(i, 0) * S(k, 0));
+            const double thk = theta[static_cast<size_t>(c) * ncand + k];
+            if (std::fabs(th - thk) <= 1.0e-6 * std::max(std::fabs(th), 1.0) && overlap > 0.5) copy = true;
+          }
+          if (copy) {
+            ++result.merged_copies;
+            continue;
+          }
+          accepted.push_back(i);
+        }
+        for (size_t q = 0; q < accepted.size(); ++q) {
+          const int i = accepted[q];
+          const double th = theta[static_cast<size_t>(c) * ncand + i];
+          const double res = std::sqrt(std::max(S(i, 2), 0.0) / S(i, 0));
+          result.eigenvalues[out * eigenpairs + q] = th;
+          result.residuals[out * eigenpairs + q] = res;
+          const double rel = res / std::max(std::fabs(th), 1.0);
+          result.max_relative_residual = std::max(result.max_relative_residual, rel);
+          if (!(rel <= tolerance)) all_ok = false;
+        }
+        if (static_cast<int>(accepted.size()) < eigenpairs || host_stop[c] < 0) all_ok = false;
+      }
+    result.verified = all_ok;
   });
-  for (size_t i = 0; i < result.steps.size(); ++i)
-    if (result.steps[i] < 0) raise_nonconvergence(static_cast<size_t>(result.total_steps), std::nan(""));
+  result.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  if (!result.verified) raise_nonconvergence(static_cast<size_t>(result.total_steps), result.max_relative_residual);
   return result;
 }
 

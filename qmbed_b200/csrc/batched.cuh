@@ -1,6 +1,6 @@
 // Batched lowest eigenvalues of many independent Hamiltonians H(s, p) =
 // sum_k c_k(p) A_k(s): every sector s of a basis family times every point p of
-// a parameter scan, in one launch per Lanczos step.
+// a parameter scan, in one persistent launch per chunk of Lanczos steps.
 #pragma once
 
 #include <vector>
@@ -12,16 +12,31 @@ namespace qmbed {
 
 struct ScanResult {
   std::vector<double> eigenvalues;  // [sector][point][eigenpairs]
+  std::vector<double> residuals;    // [sector][point][eigenpairs]: ||H v - theta v|| / ||v|| in FP64
+  std::vector<double> e_max;        // [sector][point]: largest Ritz value at convergence
   std::vector<int> steps;           // [sector][point]: Lanczos steps at convergence (-1: not converged)
-  int total_steps = 0;
-  size_t applications = 0;          // operator applications summed over all columns
+  int total_steps = 0;              // first-pass steps of the longest pair
+  int pass2_steps = 0;              // steps repeated by the Ritz-vector pass
+  size_t applications = 0;          // first-pass operator applications summed over the pairs
+  size_t applications_verification = 0;  // second pass and residual applications
+  double max_relative_residual = 0.0;    // max over reported pairs of residual / max(|theta|, 1)
+  int merged_copies = 0;            // close Ritz values found to be copies of one eigenvector
+  bool verified = false;            // every reported pair met residual <= tol max(|theta|, 1)
+  bool graph = false;               // first pass replayed from a CUDA graph
+  double pass1_seconds = 0.0, seconds = 0.0;
 };
 
 // components[s][k] holds A_k of sector s (explicit-value rows, all on sector
 // s's basis); coefficients[p * K + k] = c_k(p) (real). Up to 64 points (padded
 // to 32 or 64 columns internally), up to 8 components, eigenpairs <= 4.
+// Raises NonConvergence unless every pair's reported eigenvalues pass the
+// FP64 residual test.
 ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& components,
                        const std::vector<double>& coefficients, int points, int eigenpairs, double tolerance,
                        int max_steps, uint64_t seed, BlockOps& ops);
+
+// Runs the persistent kernel's grid barrier with one block too few on
+// `device`; returns the status it ended with (1: the bounded spin timed out).
+int scan_barrier_selftest(int device);
 
 }  // namespace qmbed

@@ -2254,9 +2254,9 @@ int qmbed_gpu_chebyshev_evolve(qmbed_operator op, const double* initial, int n_t
   });
 }
 
-int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
-                          const double* coefficients, int eigenpairs, double tolerance, int max_steps, uint64_t seed,
-                          double* eigenvalues, int* steps, double* info) {
+int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
+                         const double* coefficients, int eigenpairs, double tolerance, int max_steps, uint64_t seed,
+                         double* eigenvalues, double* residuals, double* e_max, int* steps, double* info) {
   return guarded([&] {
     if (n_sectors < 1 || n_components < 1 || !components || !coefficients || !eigenvalues || !steps)
       raise(QMBED_INVALID_OPTIONS, "a scan needs sectors, components, coefficients and outputs");
@@ -2270,11 +2270,36 @@ int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed_operator*
                                      n_points, eigenpairs, tolerance, max_steps, seed, first.block_ops());
     std::copy(r.eigenvalues.begin(), r.eigenvalues.end(), eigenvalues);
     std::copy(r.steps.begin(), r.steps.end(), steps);
+    if (residuals) std::copy(r.residuals.begin(), r.residuals.end(), residuals);
+    if (e_max) std::copy(r.e_max.begin(), r.e_max.end(), e_max);
     if (info) {
       info[0] = static_cast<double>(r.total_steps);
       info[1] = static_cast<double>(r.applications);
+      info[2] = static_cast<double>(r.applications_verification);
+      info[3] = r.graph ? 1.0 : 0.0;
+      info[4] = r.pass1_seconds;
+      info[5] = r.seconds;
+      info[6] = r.max_relative_residual;
+      info[7] = static_cast<double>(r.merged_copies);
     }
   });
+}
+
+int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
+                          const double* coefficients, int eigenpairs, double tolerance, int max_steps, uint64_t seed,
+                          double* eigenvalues, int* steps, double* info) {
+  double full[8] = {0};
+  const int rc = qmbed_gpu_scan_solve(n_sectors, n_components, components, n_points, coefficients, eigenpairs,
+                                      tolerance, max_steps, seed, eigenvalues, nullptr, nullptr, steps, full);
+  if (rc == QMBED_STATUS_OK && info) {
+    info[0] = full[0];
+    info[1] = full[1];
+  }
+  return rc;
+}
+
+int qmbed_gpu_scan_barrier_selftest(int device, int* status) {
+  return guarded([&] { *status = scan_barrier_selftest(device); });
 }
 
 int qmbed_gpu_lanczos_extremes(qmbed_operator op, int steps, uint64_t seed, double* out) {

@@ -20,20 +20,34 @@ from .engine import GpuBasis, GpuOperator
 def scan_lowest(components, coefficients, eigenpairs: int = 2, tolerance: float = 1e-10, max_steps: int = 600,
                 seed: int = 0):
     """components[s][k]: GpuOperator A_k of sector s (explicit storage, one basis per sector);
-    coefficients: points x components. Returns (eigenvalues[s, p, eigenpairs], steps[s, p], info)."""
+    coefficients: points x components. Returns (eigenvalues[s, p, eigenpairs], steps[s, p], info);
+    info also holds the FP64 residual of every reported pair and the top Ritz value of every pair."""
     sectors, k = len(components), len(components[0])
     coef = np.ascontiguousarray(coefficients, np.float64)
     points = coef.shape[0]
     assert coef.shape == (points, k)
     handles = (ctypes.c_void_p * (sectors * k))(*[op.handle.value for row in components for op in row])
     values = np.full((sectors, points, eigenpairs), np.nan)
+    residuals = np.full((sectors, points, eigenpairs), np.nan)
+    e_max = np.full((sectors, points), np.nan)
     steps = np.zeros((sectors, points), np.int32)
-    info = np.zeros(2)
-    check(lib().qmbed_gpu_scan_lowest(sectors, k, ctypes.cast(handles, ctypes.c_void_p), points,
-                                      coef.ctypes.data_as(ctypes.c_void_p), eigenpairs, tolerance, max_steps, seed,
-                                      values.ctypes.data_as(ctypes.c_void_p), steps.ctypes.data_as(ctypes.c_void_p),
-                                      info.ctypes.data_as(ctypes.c_void_p)))
-    return values, steps, {"total_steps": int(info[0]), "applications": int(info[1])}
+    info = np.zeros(8)
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    check(lib().qmbed_gpu_scan_solve(sectors, k, ctypes.cast(handles, ctypes.c_void_p), points, ptr(coef),
+                                     eigenpairs, tolerance, max_steps, seed, ptr(values), ptr(residuals), ptr(e_max),
+                                     ptr(steps), ptr(info)))
+    return values, steps, {"total_steps": int(info[0]), "applications": int(info[1]),
+                           "verification_applications": int(info[2]), "graph": bool(info[3]),
+                           "pass1_seconds": float(info[4]), "seconds": float(info[5]),
+                           "max_relative_residual": float(info[6]), "merged_copies": int(info[7]),
+                           "residuals": residuals, "e_max": e_max}
+
+
+def barrier_selftest(device: int = 0) -> int:
+    """Status of the persistent scan kernel's barrier run one block short (1: timed out as designed)."""
+    status = ctypes.c_int(-1)
+    check(lib().qmbed_gpu_scan_barrier_selftest(device, ctypes.byref(status)))
+    return status.value
 
 
 def j1j2_component_terms(sites: int):

@@ -3,7 +3,11 @@
 Each (sector, point) pair is an independent Hamiltonian of the J1-J2 chain;
 the batched Lanczos must return the same lowest eigenvalues as the oracle's
 eigsh on that pair (1e-10 relative), in real (k = 0, pi) and complex sectors,
-and exactly on sectors small enough to exhaust their Krylov space.
+and exactly on sectors small enough to exhaust their Krylov space. Every
+reported pair carries its FP64 residual ||H v - theta v|| / ||v||, which must
+meet the reference acceptance test; the top Ritz value lies inside the
+spectrum next to its top; the persistent kernel's barrier returns a time-out
+status instead of hanging when a block is missing.
 """
 
 import numpy as np
@@ -36,6 +40,50 @@ def test_scan_matches_oracle(oracle, sites, points):
             ref = _oracle_pair(oracle, scan, sites, k, coefs[p], 2)
             got = values[k, p]
             assert np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1.0)) <= 1e-10, (k, p, got, ref)
+
+
+def _oracle_top(oracle, scan, sites, k, coefs):
+    basis = oracle.Basis(sites, up=sites // 2, momentum=k)
+    terms = []
+    for c, component in zip(coefs, scan.j1j2_component_terms(sites)):
+        for symbols, couplings in component:
+            terms.append((symbols, [(c * v, b) for v, b in couplings]))
+    op = oracle.Operator.build(basis, terms)
+    return op.eigsh(1, target="largest_algebraic", tolerance=1e-12, seed=2).eigenvalues[0]
+
+
+def test_scan_residuals_top_values_and_graph(oracle):
+    from qmbed_b200 import scan
+    sites, points, tol = 18, 16, 1e-10
+    sectors = scan.j1j2_sectors(sites)
+    coefs = scan.j1j2_scan_points(points, seed=3)
+    values, steps, info = scan.scan_lowest(sectors, coefs, eigenpairs=2, tolerance=tol)
+    assert info["graph"]
+    residuals = info["residuals"]
+    assert np.all(np.isfinite(residuals))
+    assert np.all(residuals <= tol * np.maximum(np.abs(values), 1.0))
+    assert info["max_relative_residual"] <= tol
+    assert info["verification_applications"] > 0
+    for k, p in ((0, 0), (5, points - 1), (9, 7)):
+        top = _oracle_top(oracle, scan, sites, k, coefs[p])
+        got = info["e_max"][k, p]
+        assert got <= top + 1e-9 * abs(top) and got >= top - 1e-3 * (top - values[k, p, 0])
+
+
+def test_scan_at_22_sites_matches_oracle(oracle):
+    from qmbed_b200 import scan
+    sites, points = 22, 8
+    sectors = scan.j1j2_sectors(sites)
+    coefs = scan.j1j2_scan_points(points, seed=22)
+    values, steps, info = scan.scan_lowest(sectors, coefs, eigenpairs=2, tolerance=1e-10)
+    for k, p in ((0, 0), (11, 3), (7, points - 1), (15, 5)):
+        ref = _oracle_pair(oracle, scan, sites, k, coefs[p], 2)
+        assert np.max(np.abs(values[k, p] - ref) / np.maximum(np.abs(ref), 1.0)) <= 1e-10, (k, p)
+
+
+def test_scan_barrier_times_out_instead_of_hanging():
+    from qmbed_b200 import scan
+    assert scan.barrier_selftest(0) == 1
 
 
 def test_scan_exhausts_small_sectors_exactly(oracle):
