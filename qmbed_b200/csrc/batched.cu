@@ -22,7 +22,8 @@
 // and recurrences, orbit-scaled coordinates z = x / sqrt(R) with R-weighted
 // inner products. A pair stops when the residual estimates |beta_m s_m| of
 // its lowest Ritz values (copies from lost orthogonality counted once) are
-// below 0.1 tol max(|theta|, 1). A second pass repeats the identical
+// below 0.5 tol max(|theta|, 1); a sector's rows leave the recurrence once all
+// its pairs have stopped. A second pass repeats the identical
 // recurrence and accumulates the Ritz vectors of the lowest candidates; one
 // FP64 application then gives every candidate's true residual
 // ||H v - theta v|| / ||v|| (the reference's acceptance test, src/solve/mod.rs:
@@ -41,7 +42,7 @@ namespace {
 
 constexpr int kMaxComp = 8;
 constexpr int kMaxSectors = 128;
-constexpr int kMaxCand = 6;          // Ritz candidates kept per pair (eigenpairs + 2)
+constexpr int kMaxCand = 8;          // Ritz candidates kept per pair (two per wanted eigenvalue)
 constexpr int kRowsPerItem = 256;    // rows of one reduction item: 8 warps x 32 rows
 constexpr int kThreads = 256;
 constexpr int kChunkSteps = 10;      // Lanczos steps per persistent launch (one graph replay)
@@ -90,6 +91,8 @@ struct ScanArgs {
   double* cand_s;            // cols x ncand x max_steps: eigenvectors of T_m for the candidates
   double* cand_theta;        // cols x ncand
   double* top;               // cols: largest Ritz value at convergence
+  int* sector_gate;          // rows of sector s take part in step j only while j < sector_gate[s]
+  int* sector_running;       // pass 1: columns of sector s still running
   double tolerance;
   uint64_t seed;
   ScanState* state;
@@ -165,6 +168,7 @@ __device__ void phase_apply(const ScanArgs& a, const uint64_t* starts, const dou
   for (uint64_t g = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; g < a.total_rows;
        g += warps) {
     const int s = find_sector(starts, a.ns, g);
+    if (j >= a.sector_gate[s]) continue;  // every column of the sector is done
     const SectorDesc& d = a.sec[s];
     const uint64_t r = g - d.row0;
     const double* z = d.buf[cur];
@@ -225,12 +229,14 @@ __device__ void phase_apply(const ScanArgs& a, const uint64_t* starts, const dou
 // Re(conj(cur) work) (alpha); MODE 1: work -= alpha cur and partial =
 // sum_r R_r |work|^2 (beta^2; alpha null for the start vector's norm).
 template <int PPL, int MODE>
-__device__ void phase_reduce(const ScanArgs& a, const uint64_t* item_starts, int ia, int ib, const double* alpha) {
+__device__ void phase_reduce(const ScanArgs& a, const uint64_t* item_starts, int ia, int ib, const double* alpha,
+                             int j) {
   constexpr int P = 32 * PPL;
   __shared__ double red[kThreads / 32][P];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (uint64_t item = blockIdx.x; item < a.total_items; item += gridDim.x) {
     const int s = find_sector(item_starts, a.ns, item);
+    if (j >= a.sector_gate[s]) continue;  // block-uniform: one item per block iteration
     const SectorDesc& d = a.sec[s];
     const uint64_t local = item - d.item0;
     double acc[PPL];
@@ -293,13 +299,14 @@ __device__ void phase_finish(const ScanArgs& a, double* out, bool sqrt_mode, int
 
 // dst = src / beta (0 where beta vanished), one warp per row.
 template <int PPL>
-__device__ void phase_scale(const ScanArgs& a, const uint64_t* starts, int isrc, int idst, const double* beta) {
+__device__ void phase_scale(const ScanArgs& a, const uint64_t* starts, int isrc, int idst, const double* beta, int j) {
   constexpr int P = 32 * PPL;
   const int lane = threadIdx.x & 31;
   const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
   for (uint64_t g = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; g < a.total_rows;
        g += warps) {
     const int s = find_sector(starts, a.ns, g);
+    if (j >= a.sector_gate[s]) continue;
     const SectorDesc& d = a.sec[s];
     const uint64_t r = g - d.row0;
     const double2* x = reinterpret_cast<const double2*>(d.buf[isrc]) + r * P + lane * PPL;
@@ -343,7 +350,7 @@ __device__ void phase_init(const ScanArgs& a, const uint64_t* starts, int idst) 
 // up to kChunkSteps Lanczos steps of the current pass; the step counter in
 // `state` advances once per completed step.
 template <int PPL, bool PASS2>
-__global__ void __launch_bounds__(kThreads) scan_chunk_kernel(const ScanArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) scan_chunk_kernel(const ScanArgs a) {
   constexpr int P = 32 * PPL;
   __shared__ double c[kMaxComp * P];
   __shared__ uint64_t starts[kMaxSectors], item_starts[kMaxSectors];
@@ -366,11 +373,11 @@ __global__ void __launch_bounds__(kThreads) scan_chunk_kernel(const ScanArgs a) 
     roles(0, cur, prev, work);
     phase_init<PPL>(a, starts, work);
     if (!grid_sync(st, blocks)) return;
-    phase_reduce<PPL, 1>(a, item_starts, work, work, nullptr);
+    phase_reduce<PPL, 1>(a, item_starts, work, work, nullptr, 0);
     if (!grid_sync(st, blocks)) return;
     phase_finish(a, beta0, true, -1, nullptr);
     if (!grid_sync(st, blocks)) return;
-    phase_scale<PPL>(a, starts, work, cur, beta0);
+    phase_scale<PPL>(a, starts, work, cur, beta0, 0);
     if (!grid_sync(st, blocks)) return;
   }
   for (int n = 0; n < kChunkSteps && j < limit; ++n, ++j) {
@@ -380,16 +387,16 @@ __global__ void __launch_bounds__(kThreads) scan_chunk_kernel(const ScanArgs a) 
     double* beta_j = a.beta + static_cast<uint64_t>(j) * a.cols;
     phase_apply<PPL, PASS2>(a, starts, c, j);
     if (!grid_sync(st, blocks)) return;
-    phase_reduce<PPL, 0>(a, item_starts, cur, work, nullptr);
+    phase_reduce<PPL, 0>(a, item_starts, cur, work, nullptr, j);
     if (!grid_sync(st, blocks)) return;
     phase_finish(a, alpha_j, false, j, nullptr);
     if (!grid_sync(st, blocks)) return;
-    phase_reduce<PPL, 1>(a, item_starts, work, cur, alpha_j);
+    phase_reduce<PPL, 1>(a, item_starts, work, cur, alpha_j, j);
     if (!grid_sync(st, blocks)) return;
     phase_finish(a, beta_j, true, PASS2 ? -1 : j, alpha_j);
     if (!grid_sync(st, blocks)) return;
-    // z_{j+1} goes to the role of z_{j-1}, which step j+1 sees as `cur`
-    phase_scale<PPL>(a, starts, work, prev, beta_j);
+    // z_{j+1} = work / beta_j in place: step j+1 sees this buffer as `cur` and z_j as `prev`
+    phase_scale<PPL>(a, starts, work, work, beta_j, j);
     if (!grid_sync(st, blocks)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) *vstep = j + 1;
   }
@@ -463,16 +470,22 @@ __device__ double tri_vector(const Tri& T, double theta, double* s, double* work
   return s[m - 1];
 }
 
-// Pass-1 convergence check after `step` steps, for every pair still running:
-// the lowest Ritz values, copies within 1e-8 max(|theta|, 1) counted once,
-// converge when |beta_m s_m| <= 0.1 tol max(|theta|, 1) for the wanted ones
-// (and, when copies were merged, for one more distinct value). Converged
-// pairs record m, the top Ritz value, and the first ncand Ritz values with
-// their T eigenvectors for the second pass.
+// Pass-1 convergence check after `step` steps, for every pair still running.
+// The Ritz values are grouped into clusters (values within 1e-8 max(|theta|,
+// 1) of the cluster's first); copies of one eigenvalue from lost
+// orthogonality form such clusters, and so would two genuinely close
+// eigenvalues. A pair converges when the first member of each of its lowest
+// `eigenpairs` clusters has a residual estimate |beta_m s_m| of at most
+// 0.5 tol max(|theta|, 1). The candidates kept for the second pass are these
+// first members and, where its estimate is as small, each cluster's second
+// member; the second pass decides from the Ritz vectors whether a second
+// member is a copy (overlap above 1/2) or a distinct eigenvalue. Also
+// recorded: m and the top Ritz value. When the last column of a sector stops,
+// the sector's rows leave the recurrence.
 __global__ void scan_check_kernel(const ScanArgs a, double* work_all) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int step = a.state->step;
-  if (t >= a.cols || a.stop[t] >= 0 || step == 0) return;
+  if (t >= a.cols || a.stop[t] >= 0 || a.stop[t] <= -2 || step == 0) return;
   int m = step;
   const bool exhausted = a.length[t] > 0 && a.length[t] <= step;
   if (exhausted) m = a.length[t];
@@ -488,34 +501,38 @@ __global__ void scan_check_kernel(const ScanArgs a, double* work_all) {
   double* s = a.cand_s + static_cast<size_t>(t) * a.ncand * a.max_steps;
   double* work = work_all + static_cast<size_t>(t) * a.max_steps;
   const double beta_m = exhausted ? 0.0 : T.b(m - 1);
-  const int n = min(a.ncand, m);
-  double theta[kMaxCand];
+  int nc = 0, clusters = 0, members = 0;
+  double cluster_value = 0.0;
   bool converged = true;
-  int distinct = 0, merged = 0;
-  double last = 0.0;
-  for (int i = 0; i < n; ++i) {
-    theta[i] = tri_eigenvalue(T, i, lo, hi);
-    const double scale = fmax(fabs(theta[i]), 1.0);
-    const bool copy = i > 0 && theta[i] - last <= 1.0e-8 * scale;
-    const bool needed = distinct < a.eigenpairs || (merged > 0 && distinct < a.eigenpairs + 1);
-    if (!copy) last = theta[i];
-    if (copy) ++merged;
-    if (!needed && !copy) break;
-    const double last_component = tri_vector(T, theta[i], s + static_cast<size_t>(i) * a.max_steps, work);
-    if (!(fabs(beta_m * last_component) <= 0.1 * a.tolerance * scale)) converged = false;
-    if (!copy) ++distinct;
+  for (int i = 0; i < m && nc < a.ncand; ++i) {
+    const double theta = tri_eigenvalue(T, i, lo, hi);
+    const double scale = fmax(fabs(theta), 1.0);
+    if (clusters == 0 || theta - cluster_value > 1.0e-8 * scale) {
+      if (clusters == a.eigenpairs) break;
+      ++clusters;
+      cluster_value = theta;
+      members = 0;
+    }
+    if (members == 2) continue;
+    ++members;
+    double* v = s + static_cast<size_t>(nc) * a.max_steps;
+    const bool small = fabs(beta_m * tri_vector(T, theta, v, work)) <= 0.5 * a.tolerance * scale;
+    if (members == 1) {
+      if (!small) converged = false;
+    } else if (!small) {
+      continue;  // a copy still forming: not a candidate
+    }
+    a.cand_theta[static_cast<size_t>(t) * a.ncand + nc] = theta;
+    ++nc;
   }
+  if (clusters < a.eigenpairs && m > nc) converged = false;
   if (!converged && !exhausted && step < a.max_steps) return;
-  // record the candidates (vectors of the ones not computed above)
-  for (int i = 0; i < n; ++i) {
-    theta[i] = tri_eigenvalue(T, i, lo, hi);
-    tri_vector(T, theta[i], s + static_cast<size_t>(i) * a.max_steps, work);
-    a.cand_theta[static_cast<size_t>(t) * a.ncand + i] = theta[i];
-  }
-  for (int i = n; i < a.ncand; ++i) a.cand_theta[static_cast<size_t>(t) * a.ncand + i] = NAN;
+  for (int i = nc; i < a.ncand; ++i) a.cand_theta[static_cast<size_t>(t) * a.ncand + i] = NAN;
   a.top[t] = tri_eigenvalue(T, m - 1, lo, hi);
   a.stop[t] = converged ? m : -2 - m;  // -2 - m: stopped at max_steps without convergence
   atomicSub(&a.state->active, 1);
+  const int sector = t / a.P;
+  if (atomicSub(&a.sector_running[sector], 1) == 1) a.sector_gate[sector] = step;  // the sector's last column
 }
 
 // Second-pass results: for candidate i of every pair, sums over the rows of
@@ -671,7 +688,7 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
   if (static_cast<int>(coefficients.size()) != points * K) raise(QMBED_DIMENSION_MISMATCH, "coefficients must be points x components");
   const auto t_start = std::chrono::steady_clock::now();
   const int P = points <= 32 ? 32 : 64;
-  const int ncand = eigenpairs + 2;
+  const int ncand = 2 * eigenpairs;
   const cudaStream_t stream = ops.stream();
   int device = 0;
   QMBED_CUDA(cudaGetDevice(&device));
@@ -715,6 +732,7 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
   DeviceBuffer cand_theta(static_cast<size_t>(cols) * ncand * sizeof(double)), top(cols * sizeof(double));
   DeviceBuffer tri_work(static_cast<size_t>(cols) * max_steps * sizeof(double));
   DeviceBuffer state(sizeof(ScanState));
+  DeviceBuffer gate(ns * sizeof(int)), running(ns * sizeof(int));
   size_t offset = 0, roffset = 0;
   for (int s = 0; s < ns; ++s) {
     for (int b = 0; b < 3; ++b) {
@@ -731,6 +749,11 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
   QMBED_CUDA(cudaMemsetAsync(length.get(), 0xff, cols * sizeof(int), stream));  // -1: not exhausted
   QMBED_CUDA(cudaMemsetAsync(stop.get(), 0xff, cols * sizeof(int), stream));    // -1: running
   QMBED_CUDA(cudaMemsetAsync(ritz_mem.get(), 0, static_cast<size_t>(ncand) * set_bytes, stream));
+  {
+    const std::vector<int> gates(ns, max_steps), counts(ns, P);
+    QMBED_CUDA(cudaMemcpyAsync(gate.get(), gates.data(), ns * sizeof(int), cudaMemcpyHostToDevice, stream));
+    QMBED_CUDA(cudaMemcpyAsync(running.get(), counts.data(), ns * sizeof(int), cudaMemcpyHostToDevice, stream));
+  }
   ScanState init{};
   init.pass = 1;
   init.active = cols;
@@ -757,6 +780,8 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
   a.cand_s = cand_s.as<double>();
   a.cand_theta = cand_theta.as<double>();
   a.top = top.as<double>();
+  a.sector_gate = gate.as<int>();
+  a.sector_running = running.as<int>();
   a.tolerance = tolerance;
   a.seed = seed;
   a.state = state.as<ScanState>();
@@ -850,6 +875,10 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
     std::vector<int> bounded(cols);
     for (int c = 0; c < cols; ++c) bounded[c] = host_stop[c] >= 0 ? host_stop[c] : (host_stop[c] <= -2 ? -2 - host_stop[c] : 0);
     QMBED_CUDA(cudaMemcpyAsync(stop.get(), bounded.data(), cols * sizeof(int), cudaMemcpyHostToDevice, stream));
+    // pass 2: a sector's rows take part while any of its columns needs the step
+    std::vector<int> gates(ns, 0);
+    for (int c = 0; c < cols; ++c) gates[c / P] = std::max(gates[c / P], bounded[c]);
+    QMBED_CUDA(cudaMemcpyAsync(gate.get(), gates.data(), ns * sizeof(int), cudaMemcpyHostToDevice, stream));
     ScanState second{};
     second.pass = 2;
     second.target_steps = target;
@@ -906,7 +935,7 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
           for (int k : accepted) {
             const double overlap = std::fabs(S(i, 3 + k)) / std::sqrt(S(i, 0) * S(k, 0));
             const double thk = theta[static_cast<size_t>(c) * ncand + k];
-            if (std::fabs(th - thk) <= 1.0e-6 * std::max(std::fabs(th), 1.0) && overlap > 0.5) copy = true;
+            if (std::fabs(th - thk) <= 1.0e-8 * std::max(std::fabs(th), 1.0) && overlap > 0.5) copy = true;
           }
           if (copy) {
             ++result.merged_copies;
@@ -924,12 +953,19 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
           result.max_relative_residual = std::max(result.max_relative_residual, rel);
           if (!(rel <= tolerance)) all_ok = false;
         }
-        if (static_cast<int>(accepted.size()) < eigenpairs || host_stop[c] < 0) all_ok = false;
+        if (static_cast<int>(accepted.size()) < eigenpairs || host_stop[c] < 0) {
+          all_ok = false;
+          ++result.failed_pairs;
+        }
       }
     result.verified = all_ok;
   });
   result.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-  if (!result.verified) raise_nonconvergence(static_cast<size_t>(result.total_steps), result.max_relative_residual);
+  if (!result.verified)
+    raise(QMBED_NON_CONVERGENCE, "solver did not converge after " + std::to_string(result.total_steps) +
+                                     " iterations; " + std::to_string(result.failed_pairs) +
+                                     " scan pairs without verified eigenpairs, largest relative residual " +
+                                     std::to_string(result.max_relative_residual));
   return result;
 }
 

@@ -21,6 +21,7 @@ struct ScanResult {
   size_t applications_verification = 0;  // second pass and residual applications
   double max_relative_residual = 0.0;    // max over reported pairs of residual / max(|theta|, 1)
   int merged_copies = 0;            // close Ritz values found to be copies of one eigenvector
+  int failed_pairs = 0;             // pairs without `eigenpairs` verified values
   bool verified = false;            // every reported pair met residual <= tol max(|theta|, 1)
   bool graph = false;               // first pass replayed from a CUDA graph
   double pass1_seconds = 0.0, seconds = 0.0;
