@@ -129,6 +129,14 @@ QMBED_API int qmbed_gpu_operator_info(qmbed_operator op, uint64_t* dimension, in
  * interleaved complex vectors. stream may be NULL (default stream). */
 QMBED_API int qmbed_gpu_operator_apply_device(qmbed_operator op, int precision, int complex_vectors, const void* x,
                                               void* y, void* stream, int force_matrix_free);
+/* Rows row0 .. row0 + rows - 1 of y = H x for a matrix-free real operator:
+ * x is the full device vector (dimension entries), y receives `rows` entries.
+ * The slab of a row-partitioned operator whose x is all-gathered across
+ * devices (the reference's distributed profile is rejected,
+ * src/runtime.rs:224-228; its GPU slot is RuntimeLinearOperator::apply_on,
+ * src/runtime.rs:119-175). */
+QMBED_API int qmbed_gpu_operator_apply_rows_device(qmbed_operator op, int precision, uint64_t row0, uint64_t rows,
+                                                   const void* x, void* y, void* stream);
 /* Block action on row-major n x nb device blocks (nb = 8 or 16), in the
  * orbit-scaled coordinates z = x / sqrt(R) of symmetry sectors (z = x without
  * symmetry): out = alpha * (S^-1 H S) z + beta * z + gamma * p, S = diag(sqrt(R)).
@@ -179,14 +187,16 @@ QMBED_API int qmbed_gpu_operator_operand_bytes(qmbed_operator op, int precision,
  * representative search), QMBED_LOOKUP_TABLE (builds the table; error when it
  * does not fit), QMBED_LOOKUP_SEARCH, QMBED_LOOKUP_LEGACY (one thread per row
  * over every product, the form used for u128 states and products that repeat
- * a site). */
+ * a site), QMBED_LOOKUP_TABLE_GENERIC (the table with the general tile kernel
+ * even where the nearest-neighbour hop kernel applies). */
 #define QMBED_LOOKUP_AUTO 0
 #define QMBED_LOOKUP_TABLE 1
 #define QMBED_LOOKUP_SEARCH 2
 #define QMBED_LOOKUP_LEGACY 3
+#define QMBED_LOOKUP_TABLE_GENERIC 4
 QMBED_API int qmbed_gpu_operator_set_lookup(qmbed_operator op, int mode);
 /* What the matrix-free action runs: 1 table, 2 search, 3 legacy, 4 no symmetry
- * (direct or colex index); whether it expands the products in their
+ * (direct or colex index), 5 table with the nearest-neighbour hop kernel; whether it expands the products in their
  * translation-structured form (uniform couplings per bond displacement: one
  * activity mask per displacement from word operations); the basis's image
  * table size and build time (0 when none). */
@@ -221,6 +231,32 @@ typedef struct {
 QMBED_API int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, const double* initial,
                               int n_initial, double* eigenvalues, double* residuals, double* eigenvectors,
                               qmbed_eigsh_info* info);
+
+/* Spectral hint for eigsh (no reference counterpart: the reference estimates
+ * nothing before a solve). lower/upper: an interval believed to hold the
+ * spectrum (for example the learned bound network's prediction, padded);
+ * gap: the predicted gap above the lowest eigenvalue; restart_keep: Ritz
+ * vectors the thick restart keeps per cycle (0: the reference's
+ * min(needed, krylov / 2), src/solve/mod.rs:1799); check_steps: Lanczos steps
+ * of the check that the filtered mode runs before it trusts the interval (its
+ * Ritz values must lie inside it, else the solver's own bound estimate is
+ * used). On return, used = 1 when the interval passed the check and set the
+ * filter, and bound_applications counts the operator applications spent on
+ * spectral bounds. */
+typedef struct {
+  double lower;
+  double upper;
+  double gap;
+  uint64_t restart_keep;
+  int check_steps;
+  int used;
+  uint64_t bound_applications;
+} qmbed_eigsh_hint;
+
+/* qmbed_gpu_eigsh with a spectral hint (no reference counterpart). */
+QMBED_API int qmbed_gpu_eigsh_hinted(qmbed_operator op, const qmbed_eigsh_options* options, qmbed_eigsh_hint* hint,
+                                     const double* initial, int n_initial, double* eigenvalues, double* residuals,
+                                     double* eigenvectors, qmbed_eigsh_info* info);
 
 /* ExpmActionPlan::new (src/solve/mod.rs:126-184): degree, scaling, trace
  * shift (complex) and the exact stored 1-norm of A - shift. */

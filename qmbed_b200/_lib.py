@@ -71,6 +71,18 @@ class EigshInfoC(ctypes.Structure):
     ]
 
 
+class EigshHintC(ctypes.Structure):
+    _fields_ = [
+        ("lower", ctypes.c_double),
+        ("upper", ctypes.c_double),
+        ("gap", ctypes.c_double),
+        ("restart_keep", ctypes.c_uint64),
+        ("check_steps", ctypes.c_int),
+        ("used", ctypes.c_int),
+        ("bound_applications", ctypes.c_uint64),
+    ]
+
+
 def library_path() -> Path:
     configured = os.environ.get("QMBED_B200_LIBRARY")
     return Path(configured) if configured else LIBRARY
@@ -97,6 +109,7 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_basis_build_seconds.argtypes = [vp, P(d)]
     L.qmbed_gpu_basis_table_images.argtypes = [vp, vp, u64, vp, vp, vp]
     L.qmbed_gpu_operator_set_lookup.argtypes = [vp, i]
+    L.qmbed_gpu_operator_apply_rows_device.argtypes = [vp, i, ctypes.c_uint64, ctypes.c_uint64, vp, vp, vp]
     L.qmbed_gpu_operator_lookup_info.argtypes = [vp, P(i), P(i), P(u64), P(d)]
     L.qmbed_gpu_operator_create.argtypes = [vp, i, vp, ctypes.c_char_p, vp, vp, vp, i, i, i, P(vp)]
     L.qmbed_gpu_operator_destroy.argtypes = [vp]
@@ -108,6 +121,7 @@ def lib() -> ctypes.CDLL:
     L.qmbed_gpu_operator_export_csr.argtypes = [vp, P(u64), vp, vp, vp]
     L.qmbed_gpu_operator_operand_bytes.argtypes = [vp, i, i, P(d)]
     L.qmbed_gpu_eigsh.argtypes = [vp, P(EigshOptionsC), vp, i, vp, vp, vp, P(EigshInfoC)]
+    L.qmbed_gpu_eigsh_hinted.argtypes = [vp, P(EigshOptionsC), P(EigshHintC), vp, i, vp, vp, vp, P(EigshInfoC)]
     L.qmbed_gpu_expm_plan.argtypes = [vp, d, d, u64, d, u64, P(u64), P(u64), vp, P(d)]
     L.qmbed_gpu_expm_apply_host.argtypes = [vp, d, d, u64, d, u64, i, vp, vp, u64]
     L.qmbed_gpu_deterministic_start.argtypes = [i, u64, u64, vp]

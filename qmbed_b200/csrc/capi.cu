@@ -2027,6 +2027,15 @@ int qmbed_gpu_operator_apply_device(qmbed_operator op, int precision, int comple
   });
 }
 
+int qmbed_gpu_operator_apply_rows_device(qmbed_operator op, int precision, uint64_t row0, uint64_t rows,
+                                         const void* x, void* y, void* stream) {
+  return guarded([&] {
+    if (precision != 64 && precision != 32) raise(QMBED_INVALID_OPTIONS, "precision must be 64 or 32");
+    if (!x || !y || x == y) raise(QMBED_INVALID_OPTIONS, "row slabs need distinct input and output vectors");
+    op->op->apply_rows(precision, row0, rows, x, y, static_cast<cudaStream_t>(stream));
+  });
+}
+
 int qmbed_gpu_operator_apply_block_device(qmbed_operator op, int precision, int nb, const void* z, const void* p,
                                           void* out, double alpha, double beta, double gamma, void* stream) {
   return guarded([&] {
@@ -2095,11 +2104,24 @@ int qmbed_gpu_operator_lookup_info(qmbed_operator op, int* in_use, int* chain_fo
   });
 }
 
-int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, const double* initial, int n_initial,
-                    double* eigenvalues, double* residuals, double* eigenvectors, qmbed_eigsh_info* info) {
+namespace {
+
+int run_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, qmbed_eigsh_hint* hint, const double* initial,
+              int n_initial, double* eigenvalues, double* residuals, double* eigenvectors, qmbed_eigsh_info* info) {
   return guarded([&] {
+    if (!op || !options) raise(QMBED_INVALID_OPTIONS, "null operator or options");
     std::lock_guard<std::mutex> lock(op->mu);
     EigshOptions o;
+    if (hint) {
+      if (!std::isfinite(hint->lower) || !std::isfinite(hint->upper) || !std::isfinite(hint->gap))
+        raise(QMBED_INVALID_OPTIONS, "eigsh hint must be finite");
+      o.hint = true;
+      o.hint_lower = hint->lower;
+      o.hint_upper = hint->upper;
+      o.hint_gap = hint->gap;
+      o.hint_check_steps = hint->check_steps > 0 ? hint->check_steps : 8;
+      o.restart_keep = hint->restart_keep;
+    }
     o.eigenpairs = options->eigenpairs;
     o.target = options->target;
     o.shift = options->shift;
@@ -2140,7 +2162,24 @@ int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, const
       info->converged = r.converged ? 1 : 0;
       info->complex_vectors = r.complex_vectors ? 1 : 0;
     }
+    if (hint) {
+      hint->used = r.hint_used;
+      hint->bound_applications = r.bound_applications;
+    }
   });
+}
+
+}  // namespace
+
+int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, const double* initial, int n_initial,
+                    double* eigenvalues, double* residuals, double* eigenvectors, qmbed_eigsh_info* info) {
+  return run_eigsh(op, options, nullptr, initial, n_initial, eigenvalues, residuals, eigenvectors, info);
+}
+
+int qmbed_gpu_eigsh_hinted(qmbed_operator op, const qmbed_eigsh_options* options, qmbed_eigsh_hint* hint,
+                           const double* initial, int n_initial, double* eigenvalues, double* residuals,
+                           double* eigenvectors, qmbed_eigsh_info* info) {
+  return run_eigsh(op, options, hint, initial, n_initial, eigenvalues, residuals, eigenvectors, info);
 }
 
 int qmbed_gpu_expm_plan(qmbed_operator op, double coef_re, double coef_im, uint64_t max_degree, double tolerance,

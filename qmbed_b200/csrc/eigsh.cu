@@ -351,7 +351,12 @@ EigshResult thick_restart(Ctx& c, const EigshOptions& o, const Panel* initial, i
   const int m = static_cast<int>(thick_restart_dimension(o, n));
   const int k = static_cast<int>(o.eigenpairs);
   if (m <= k) raise(QMBED_INVALID_OPTIONS, "the effective Krylov dimension must exceed eigenpairs");
-  const int keep_cap = std::max(std::min(k, m / 2), 1);  // candidates per cycle never exceed this
+  // Ritz vectors kept per cycle: the reference keeps the unconverged wanted
+  // ones (src/solve/mod.rs:1799); a restart_keep hint keeps more of the
+  // lowest ones, up to half the Krylov dimension.
+  const int wider = static_cast<int>(std::min<size_t>(o.restart_keep, static_cast<size_t>(m)));
+  auto keep_for = [&](int active) { return std::max(std::min(std::max(active, wider), m / 2), 1); };
+  const int keep_cap = keep_for(k);  // candidates per cycle never exceed this
   Panel Q, W, C, CA, RC, RCA, work;
   Q.alloc(n, k + m, c.prec, c.cplx);  // [locked | basis]
   W.alloc(n, m, c.prec, c.cplx);      // applied actions of the basis
@@ -440,7 +445,7 @@ EigshResult thick_restart(Ctx& c, const EigshOptions& o, const Panel* initial, i
     std::vector<C64> vectors;
     device_hermitian_eigen(size, P, values, vectors, c.ops.stream());
     const int active = k - l;
-    const int keep = std::max(std::min(active, m / 2), 1);
+    const int keep = keep_for(active);
     const std::vector<size_t> indices = select_indices(values, o.target, std::min(keep, size));
     const int K = static_cast<int>(indices.size());
     std::vector<C64> Y(static_cast<size_t>(size) * K);

@@ -23,6 +23,18 @@ struct EigshOptions {
   size_t max_iterations = 1000;
   uint64_t seed = 0;
   bool want_vectors = true;  // false: the caller takes eigenvalues only (the filtered solver exports no vectors)
+  // Spectral hint (for example from the learned bound network): an interval
+  // [hint_lower, hint_upper] believed to hold the spectrum and the gap above
+  // the lowest eigenvalue. The filtered solver uses the interval only after a
+  // hint_check_steps Lanczos run whose Ritz values it must contain; otherwise
+  // it takes its own Lanczos bounds. restart_keep > 0 sets how many Ritz
+  // vectors the thick restart keeps per cycle (at least the unconverged
+  // wanted ones, at most half the Krylov dimension); 0 keeps the reference's
+  // min(needed, m / 2) (src/solve/mod.rs:1799).
+  bool hint = false;
+  double hint_lower = 0.0, hint_upper = 0.0, hint_gap = 0.0;
+  int hint_check_steps = 8;
+  size_t restart_keep = 0;
 };
 
 enum SolverMode : int {
@@ -45,6 +57,8 @@ struct EigshResult {
   size_t fp32_iterations = 0;
   size_t fp64_iterations = 0;
   size_t operator_applications = 0;
+  int hint_used = 0;               // 1: the hint's interval passed its check and set the filter
+  size_t bound_applications = 0;   // operator applications spent on spectral bounds
 };
 
 // y = A x on device vectors for the given precision (64/32) and complex flag.

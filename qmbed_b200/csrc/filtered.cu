@@ -468,9 +468,10 @@ struct Bounds {
 
 // Spectral bounds from a short Lanczos run in FP32 without reorthogonalisation
 // (only the extreme Ritz values are used). `start` is an FP64 real vector.
-Bounds lanczos_bounds(const LinearOperatorView& op, BlockOps& ops, const double* start, size_t& applications) {
+Bounds lanczos_bounds(const LinearOperatorView& op, BlockOps& ops, const double* start, size_t& applications,
+                      int steps = kBoundSteps) {
   const uint64_t n = op.dim;
-  const int m = static_cast<int>(std::min<uint64_t>(kBoundSteps, n - 1));
+  const int m = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(std::max(steps, 2)), n - 1));
   // workspace slots 7-9 of the handle: the three FP32 Lanczos vectors
   void* prev = ops.workspace(7, n * 4);
   void* cur = ops.workspace(8, n * 4);
@@ -544,11 +545,26 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
                  std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - started).count());
   };
   size_t bound_applications = 0;
-  const Bounds bd = lanczos_bounds(op, ops, col(0), bound_applications);
-  // Upper end of the damped interval: the top Ritz value plus its residual
-  // norm and 1% of the Ritz range. Components a little above it grow only
-  // like exp(d sqrt(2 delta)), far below the amplification of the wanted end.
-  const double upper = bd.theta.back() + bd.top_residual + 0.01 * (bd.theta.back() - bd.theta.front());
+  // A spectral hint replaces the bound estimate when the Ritz values of a
+  // short check run lie inside its interval (Ritz values lie inside the
+  // spectrum, so an interval that misses one is wrong).
+  bool hint_used = false;
+  Bounds bd;
+  if (o.hint && o.hint_upper > o.hint_lower) {
+    bd = lanczos_bounds(op, ops, col(0), bound_applications, o.hint_check_steps);
+    hint_used = bd.theta.front() >= o.hint_lower && bd.theta.back() <= o.hint_upper;
+  }
+  if (!hint_used) {
+    size_t more = 0;
+    bd = lanczos_bounds(op, ops, col(0), more);
+    bound_applications += more;
+  }
+  // Upper end of the damped interval: the hint's upper end, or the top Ritz
+  // value plus its residual norm and 1% of the Ritz range. Components a little
+  // above it grow only like exp(d sqrt(2 delta)), far below the amplification
+  // of the wanted end.
+  const double upper = hint_used ? o.hint_upper
+                                 : bd.theta.back() + bd.top_residual + 0.01 * (bd.theta.back() - bd.theta.front());
   double lower = bd.theta.front();
   // First cut: the k-th Ritz value, which lies at or above the k-th eigenvalue.
   double cut = bd.theta[std::min<size_t>(k, bd.theta.size()) - 1];
@@ -668,6 +684,8 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
   ops.sync();
   stamp("export");
   r.operator_applications = solver.applications + bound_applications;
+  r.bound_applications = bound_applications;
+  r.hint_used = hint_used ? 1 : 0;
   return r;
 }
 

@@ -375,6 +375,7 @@ struct TileArgs {
   SectorParams p;
   uint64_t mask;
   uint64_t dim;
+  uint64_t row0, rows;  // rows computed: row0 .. row0 + rows - 1 (outputs indexed from row0)
   const uint64_t* states;
   const uint16_t* orbits;
   // program (copied to shared memory by every block)
@@ -710,10 +711,12 @@ __global__ void __launch_bounds__(kTileThreads, TileShape<T, NB, CPLX>::MIN_BLOC
   const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
   const T* x = static_cast<const T*>(a.x);
   const bool ranked_rows = RANKED && a.p.up >= 0 && a.rank_chunks > 0;
-  for (uint64_t tile = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 32 < a.dim;
+  for (uint64_t tile = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 32 < a.rows;
        tile += warps) {
-    const uint64_t r = tile * 32 + lane;
-    const bool valid = r < a.dim;
+    // row r of the operator; `slot` indexes the outputs (rows row0 .. row0 + rows - 1)
+    const uint64_t slot = tile * 32 + lane;
+    const uint64_t r = a.row0 + slot;
+    const bool valid = slot < a.rows;
     uint64_t s = 0;
     if (valid) s = MODE == kModeDirect ? r : __ldcs(a.states + r);
     const uint64_t rank_s = ranked_rows ? rank_chunked(s, s_rank, a.rank_chunks, a.rank_stride) : 0;
@@ -847,10 +850,10 @@ __global__ void __launch_bounds__(kTileThreads, TileShape<T, NB, CPLX>::MIN_BLOC
       if (CPLX) {
         const T xr = __ldcs(x + 2 * r), xi = __ldcs(x + 2 * r + 1);
         const T d_r = static_cast<T>(dr), d_i = static_cast<T>(di);
-        __stcs(y + 2 * r, scale * acc[0] + d_r * xr - d_i * xi);
-        __stcs(y + 2 * r + 1, scale * acc_i + d_r * xi + d_i * xr);
+        __stcs(y + 2 * slot, scale * acc[0] + d_r * xr - d_i * xi);
+        __stcs(y + 2 * slot + 1, scale * acc_i + d_r * xi + d_i * xr);
       } else {
-        __stcs(y + r, scale * acc[0] + static_cast<T>(dr) * __ldcs(x + r));
+        __stcs(y + slot, scale * acc[0] + static_cast<T>(dr) * __ldcs(x + r));
       }
     } else {
       const T d = static_cast<T>(dr);
@@ -865,11 +868,223 @@ __global__ void __launch_bounds__(kTileThreads, TileShape<T, NB, CPLX>::MIN_BLOC
         for (int j = 0; j < VEC; ++j) o[j] = al * (acc[q * VEC + j] + d * self[j]) + be * self[j];
         if (HAS_P) {
           T pq[VEC];
-          load16_rw(pv + r * NB + q * VEC, pq);
+          load16_rw(pv + slot * NB + q * VEC, pq);
 #pragma unroll
           for (int j = 0; j < VEC; ++j) o[j] += ga * pq[j];
         }
-        store16(out + r * NB + q * VEC, o);
+        store16(out + slot * NB + q * VEC, o);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Nearest-neighbour hop kernel
+// ---------------------------------------------------------------------------
+
+// Arguments of the hop kernel: a chain program whose only off-diagonal class
+// is the nearest-neighbour bond (d = 1), on a real fixed-weight sector with a
+// 32-bit image table (Heisenberg and XXZ chains in their k = 0, pi sectors).
+struct HopArgs {
+  uint64_t dim;
+  uint64_t row0, rows;  // rows computed: row0 .. row0 + rows - 1 (outputs indexed from row0)
+  int sites, up;
+  const uint64_t* states;
+  const uint16_t* orbits;
+  const uint64_t* rank_tab;
+  int rank_chunks, rank_stride;
+  const uint64_t* binom;      // [n][k] with row stride kBinomStride
+  const uint32_t* table;
+  int idx_bits, rbits, n_classes;
+  const double* class_inv_sqrt;  // orbit class -> 1/sqrt(R)
+  const double* inv_sqrt;        // [257 + R] sqrt(R)
+  uint64_t bonds_inner;          // bonds (i, i + 1) with i < L - 1
+  int wrap;                      // bond (L - 1, 0) present
+  double w_down, w_up;           // entries of the hops from digits (1, 0) and (0, 1) of a bond
+  ChainProgram chain;            // diagonal classes and field
+  const void* x;
+  const void* pv;
+  void* y;
+  double alpha, beta, gamma;
+};
+
+constexpr int kHopMaxClasses = 64;
+
+template <typename T, int NB>
+struct HopShape {
+  static constexpr int U = NB == 1 ? 4 : (NB * sizeof(T) <= 32 ? 4 : 2);
+  static constexpr int MIN_BLOCKS = NB == 1 ? 4 : (NB * sizeof(T) <= 32 ? 3 : 2);
+};
+
+// One warp per tile of 32 consecutive rows, one lane per row. A bond
+// (i, i + 1) with different digits moves one up spin between neighbours, so
+// the target's colex rank is the row's rank +- C(i, k), k = up spins below
+// site i (fixed_weight_state_index, src/basis/mod.rs:640-659): one shared-
+// memory read per transition. The target's image-table entry gives its
+// column, character sign and orbit class. The wrapping bond (L - 1, 0)
+// renumbers every up spin, so its rank comes from the chunk tables in a step
+// of its own after the inner bonds. Contributions (index_transition,
+// src/basis/mod.rs:1561-1580, apply_real src/operator/mod.rs:1414-1485):
+// NB = 1 accumulates w chi x[c] / sqrt(R_c) and scales by sqrt(R_r); blocks
+// accumulate w chi z[c][:] in orbit-scaled coordinates with the three-term
+// epilogue out = alpha (acc + d z_r) + beta z_r + gamma p_r.
+template <typename T, int NB, bool HAS_P>
+__global__ void __launch_bounds__(kTileThreads, HopShape<T, NB>::MIN_BLOCKS)
+    hop_tile_kernel(const __grid_constant__ HopArgs a) {
+  constexpr int U = HopShape<T, NB>::U;
+  constexpr int VEC = 16 / sizeof(T);
+  constexpr int PARTS = NB >= VEC ? NB / VEC : 1;
+  extern __shared__ __align__(16) unsigned char smem[];
+  // shared memory: [rank chunk table][binomials C(i, k), i < L, k <= up][1/sqrt(R) per class]
+  uint64_t* s_rank = reinterpret_cast<uint64_t*>(smem);
+  const int rank_words = a.rank_chunks * kRankChunkValues * a.rank_stride;
+  for (int i = threadIdx.x; i < rank_words; i += blockDim.x) s_rank[i] = a.rank_tab[i];
+  uint64_t* s_binom = s_rank + rank_words;
+  const int bstride = a.up + 1;
+  for (int i = threadIdx.x; i < a.sites * bstride; i += blockDim.x)
+    s_binom[i] = a.binom[(i / bstride) * kBinomStride + i % bstride];
+  T* s_cls = reinterpret_cast<T*>(s_binom + a.sites * bstride);
+  for (int i = threadIdx.x; i < a.n_classes; i += blockDim.x) s_cls[i] = static_cast<T>(a.class_inv_sqrt[i]);
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const int L = a.sites;
+  const uint64_t idx_mask = (1ull << a.idx_bits) - 1;
+  const uint32_t cls_mask = (1u << a.rbits) - 1;
+  const int cls_shift = a.idx_bits + 1;
+  const T w_down = static_cast<T>(a.w_down), w_up = static_cast<T>(a.w_up);
+  const T* x = static_cast<const T*>(a.x);
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  const uint64_t mask = L == 64 ? ~0ull : (1ull << L) - 1;
+
+  // Adds the contributions of up to U targets whose table entries are e[u]
+  // (0xffffffff: outside the sector) with hop amplitudes w[u].
+  auto consume = [&](const uint32_t (&e)[U], const T (&w)[U], T (&acc)[NB]) {
+    if (NB == 1) {
+      T g[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) g[u] = e[u] != 0xffffffffu ? __ldg(x + (e[u] & idx_mask)) : static_cast<T>(0);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (e[u] == 0xffffffffu) continue;
+        T f = w[u] * s_cls[(e[u] >> cls_shift) & cls_mask];
+        if ((e[u] >> a.idx_bits) & 1) f = -f;
+        acc[0] += f * g[u];
+      }
+    } else {
+      T g[U][NB];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (e[u] == 0xffffffffu) {
+#pragma unroll
+          for (int j = 0; j < NB; ++j) g[u][j] = 0;
+          continue;
+        }
+        const T* row = x + static_cast<uint64_t>(e[u] & idx_mask) * NB;
+#pragma unroll
+        for (int q = 0; q < PARTS; ++q) {
+          T v[VEC];
+          load16(row + q * VEC, v);
+#pragma unroll
+          for (int j = 0; j < VEC; ++j) g[u][q * VEC + j] = v[j];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        T c = e[u] == 0xffffffffu ? static_cast<T>(0) : w[u];
+        if ((e[u] >> a.idx_bits) & 1) c = -c;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) acc[j] += c * g[u][j];
+      }
+    }
+  };
+
+  for (uint64_t tile = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); tile * 32 < a.rows;
+       tile += warps) {
+    // row r of the operator; `slot` indexes the outputs (rows row0 .. row0 + rows - 1)
+    const uint64_t slot = tile * 32 + lane;
+    const uint64_t r = a.row0 + slot;
+    const bool valid = slot < a.rows;
+    const uint64_t s = valid ? __ldcs(a.states + r) : 0;
+    const uint64_t rank_s = rank_chunked(s, s_rank, a.rank_chunks, a.rank_stride);
+    double dr = 0.0;
+    const ChainProgram& ch = a.chain;
+    if (valid) {
+      if (ch.has_field) dr += __popcll(~s & ch.field_mask) * ch.field_re[0] + __popcll(s & ch.field_mask) * ch.field_re[1];
+      for (int c = 0; c < ch.n_diag; ++c) {
+        const ChainClass& cl = ch.diag[c];
+        const uint64_t b = digits_ahead(s, cl.d, L, mask);
+        dr += __popcll(~s & ~b & cl.bonds) * cl.re[0] + __popcll(s & ~b & cl.bonds) * cl.re[1] +
+              __popcll(~s & b & cl.bonds) * cl.re[2] + __popcll(s & b & cl.bonds) * cl.re[3];
+      }
+    }
+    T acc[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) acc[j] = 0;
+    // bit i: digits of sites i and i + 1 differ (one up spin can hop)
+    uint64_t hop = valid ? ((s ^ (s >> 1)) & a.bonds_inner) : 0;
+    while (__any_sync(0xffffffffu, hop != 0)) {
+      uint32_t e[U];
+      T w[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        e[u] = 0xffffffffu;
+        w[u] = 0;
+        if (hop == 0) continue;
+        const int i = __ffsll(static_cast<long long>(hop)) - 1;
+        hop &= hop - 1;
+        const uint64_t below = (1ull << i) - 1;
+        const bool down = (s >> i) & 1;  // the up spin sits at i and moves to i + 1
+        const uint64_t step = s_binom[i * bstride + __popcll(s & below)];
+        const uint64_t rank_t = down ? rank_s + step : rank_s - step;
+        w[u] = down ? w_down : w_up;
+        e[u] = __ldg(a.table + rank_t);
+      }
+      consume(e, w, acc);
+    }
+    if (a.wrap) {
+      // bond (L - 1, 0): digit L - 1 differs from digit 0
+      const bool on = valid && (((s >> (L - 1)) ^ s) & 1);
+      if (__any_sync(0xffffffffu, on)) {
+        uint32_t e[U];
+        T w[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          e[u] = 0xffffffffu;
+          w[u] = 0;
+        }
+        if (on) {
+          const uint64_t t = s ^ (1ull << (L - 1)) ^ 1ull;
+          const bool down = (s >> (L - 1)) & 1;
+          w[0] = down ? w_down : w_up;
+          e[0] = __ldg(a.table + rank_chunked(t, s_rank, a.rank_chunks, a.rank_stride));
+        }
+        consume(e, w, acc);
+      }
+    }
+    if (!valid) continue;
+    if (NB == 1) {
+      const T scale = static_cast<T>(__ldg(a.inv_sqrt + 257 + __ldcs(a.orbits + r)));
+      T* y = static_cast<T*>(a.y);
+      __stcs(y + slot, scale * acc[0] + static_cast<T>(dr) * __ldcs(x + r));
+    } else {
+      const T d = static_cast<T>(dr);
+      const T al = static_cast<T>(a.alpha), be = static_cast<T>(a.beta), ga = static_cast<T>(a.gamma);
+      T* out = static_cast<T*>(a.y);
+      const T* pv = static_cast<const T*>(a.pv);
+#pragma unroll
+      for (int q = 0; q < PARTS; ++q) {
+        T self[VEC], o[VEC];
+        load16(x + r * NB + q * VEC, self);
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) o[j] = al * (acc[q * VEC + j] + d * self[j]) + be * self[j];
+        if (HAS_P) {
+          T pq[VEC];
+          load16_rw(pv + slot * NB + q * VEC, pq);
+#pragma unroll
+          for (int j = 0; j < VEC; ++j) o[j] += ga * pq[j];
+        }
+        store16(out + slot * NB + q * VEC, o);
       }
     }
   }
@@ -1231,7 +1446,7 @@ void launch_chain(const TileArgs& a, size_t smem, cudaStream_t stream) {
     cached_smem = smem;
   }
   const int sms = cached_sms, per_sm = cached_per_sm;
-  const uint64_t tiles = (a.dim + 31) / 32;
+  const uint64_t tiles = (a.rows + 31) / 32;
   const uint64_t blocks_needed = (tiles + kTileThreads / 32 - 1) / (kTileThreads / 32);
   const uint64_t cap = static_cast<uint64_t>(sms) * std::max(per_sm, 1);
   const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min(blocks_needed, cap)));
@@ -1243,6 +1458,98 @@ template <typename T, int NB, bool CPLX, int MODE, bool HAS_P>
 void launch_one(const TileArgs& a, size_t smem, cudaStream_t stream, bool chain) {
   if (chain) launch_chain<T, NB, CPLX, MODE, HAS_P, true>(a, smem, stream);
   else launch_chain<T, NB, CPLX, MODE, HAS_P, false>(a, smem, stream);
+}
+
+template <typename T, int NB, bool HAS_P>
+void launch_hop_kernel(const HopArgs& a, size_t smem, cudaStream_t stream) {
+  auto kernel = hop_tile_kernel<T, NB, HAS_P>;
+  static thread_local int cached_device = -1;
+  static thread_local size_t cached_smem = 0;
+  static thread_local int cached_per_sm = 0, cached_sms = 0;
+  int device = 0;
+  QMBED_CUDA(cudaGetDevice(&device));
+  if (cached_device != device || cached_smem != smem) {
+    if (smem > 48 * 1024)
+      QMBED_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    QMBED_CUDA(cudaDeviceGetAttribute(&cached_sms, cudaDevAttrMultiProcessorCount, device));
+    QMBED_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached_per_sm, kernel, kTileThreads, smem));
+    cached_device = device;
+    cached_smem = smem;
+  }
+  const uint64_t tiles = (a.rows + 31) / 32;
+  const uint64_t blocks_needed = (tiles + kTileThreads / 32 - 1) / (kTileThreads / 32);
+  const uint64_t cap = static_cast<uint64_t>(cached_sms) * std::max(cached_per_sm, 1);
+  const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min(blocks_needed, cap)));
+  kernel<<<grid, kTileThreads, smem, stream>>>(a);
+  QMBED_LAUNCH_CHECK();
+}
+
+// The hop kernel serves chain programs whose only off-diagonal class is the
+// nearest-neighbour bond, on real fixed-weight sectors whose image table has
+// 32-bit entries without a phase index.
+bool hop_form(const SpinBasis& basis, const DeviceFlipProgram& prog, const ImageTable* table) {
+  const SectorParams& p = basis.params();
+  if (!table || table->wide || table->mbits != 0 || !basis.real_phases()) return false;
+  if (!prog.ok() || !prog.chain_ok() || prog.complex_coefs()) return false;
+  if (p.up < 0 || basis.rank_chunk_count() == 0 || p.sites < 3 || p.sites > 64) return false;
+  const ChainProgram& ch = prog.chain();
+  if (ch.n_off != 1 || ch.off[0].d != 1 || (ch.off[0].nz & ~0x6) != 0) return false;
+  return orbit_size_classes(p).size() <= static_cast<size_t>(kHopMaxClasses);
+}
+
+bool launch_hop(const SpinBasis& basis, const DeviceFlipProgram& prog, const ImageTable& table, const TileLaunch& l) {
+  const SectorParams& p = basis.params();
+  const ChainProgram& ch = prog.chain();
+  HopArgs a{};
+  a.dim = basis.dim();
+  a.row0 = l.row0;
+  a.rows = std::min(l.rows, a.dim - std::min(l.row0, a.dim));
+  a.sites = p.sites;
+  a.up = p.up;
+  a.states = static_cast<const uint64_t*>(basis.states());
+  a.orbits = basis.orbits();
+  a.rank_tab = basis.rank_chunk_table();
+  a.rank_chunks = basis.rank_chunk_count();
+  a.rank_stride = basis.rank_chunk_stride();
+  a.binom = basis.binomials();
+  a.table = static_cast<const uint32_t*>(table.entries.get());
+  a.idx_bits = table.idx_bits;
+  a.rbits = table.rbits;
+  a.n_classes = static_cast<int>(orbit_size_classes(p).size());
+  a.class_inv_sqrt = table.class_inv_sqrt.as<double>();
+  a.inv_sqrt = l.inv_sqrt;
+  const uint64_t inner = p.sites == 64 ? ~0ull >> 1 : (1ull << (p.sites - 1)) - 1;
+  a.bonds_inner = ch.off[0].bonds & inner;
+  a.wrap = static_cast<int>((ch.off[0].bonds >> (p.sites - 1)) & 1);
+  a.w_down = ch.off[0].re[1];
+  a.w_up = ch.off[0].re[2];
+  a.chain = ch;
+  a.x = l.x;
+  a.pv = l.p;
+  a.y = l.y;
+  a.alpha = l.alpha;
+  a.beta = l.beta;
+  a.gamma = l.gamma;
+  const size_t elem = l.precision == 64 ? 8 : 4;
+  const size_t smem = static_cast<size_t>(a.rank_chunks) * kRankChunkValues * a.rank_stride * 8 +
+                      static_cast<size_t>(p.sites) * (p.up + 1) * 8 + static_cast<size_t>(a.n_classes) * elem;
+  if (smem > 96 * 1024) return false;
+  const bool hp = l.p != nullptr;
+  if (l.nb == 1) {
+    if (l.precision == 64) launch_hop_kernel<double, 1, false>(a, smem, l.stream);
+    else launch_hop_kernel<float, 1, false>(a, smem, l.stream);
+  } else if (l.precision == 64) {
+    if (l.nb == 8) hp ? launch_hop_kernel<double, 8, true>(a, smem, l.stream)
+                      : launch_hop_kernel<double, 8, false>(a, smem, l.stream);
+    else hp ? launch_hop_kernel<double, 16, true>(a, smem, l.stream)
+            : launch_hop_kernel<double, 16, false>(a, smem, l.stream);
+  } else {
+    if (l.nb == 8) hp ? launch_hop_kernel<float, 8, true>(a, smem, l.stream)
+                      : launch_hop_kernel<float, 8, false>(a, smem, l.stream);
+    else hp ? launch_hop_kernel<float, 16, true>(a, smem, l.stream)
+            : launch_hop_kernel<float, 16, false>(a, smem, l.stream);
+  }
+  return true;
 }
 
 template <int MODE>
@@ -1273,6 +1580,10 @@ void dispatch_mode(const TileArgs& a, size_t smem, const TileLaunch& l, bool cha
 
 }  // namespace
 
+bool hop_kernel_applies(const SpinBasis& basis, const DeviceFlipProgram& prog) {
+  return hop_form(basis, prog, basis.image_table());
+}
+
 bool launch_tile(const SpinBasis& basis, const DeviceFlipProgram& prog, int mode, const TileLaunch& l) {
   if (basis.words() != 1 || !prog.ok()) return false;
   if (l.nb != 1 && l.nb != 8 && l.nb != 16) return false;
@@ -1283,6 +1594,8 @@ bool launch_tile(const SpinBasis& basis, const DeviceFlipProgram& prog, int mode
   a.p = p;
   a.mask = low_mask<uint64_t>(p.sites);
   a.dim = basis.dim();
+  a.row0 = l.row0;
+  a.rows = std::min(l.rows, a.dim - std::min(l.row0, a.dim));
   a.states = static_cast<const uint64_t*>(basis.states());
   a.orbits = basis.orbits();
   if (prog.bytes() > kProgramSmemMax) return false;
@@ -1321,7 +1634,10 @@ bool launch_tile(const SpinBasis& basis, const DeviceFlipProgram& prog, int mode
     if (a.rank_chunks > 0) smem += static_cast<size_t>(a.rank_chunks) * kRankChunkValues * a.rank_stride * 8;
   } else {
     const ImageTable* table = mode == kLookupSearch ? nullptr : basis.image_table();
-    if (mode == kLookupTable && !table) return false;
+    if ((mode == kLookupTable || mode == kLookupTableGeneric) && !table) return false;
+    if (mode != kLookupTableGeneric && !l.complex_vectors && hop_form(basis, prog, table) &&
+        launch_hop(basis, prog, *table, l))
+      return true;
     if (table) {
       tile_mode = kModeTable;
       a.table = table->entries.get();

@@ -99,7 +99,11 @@ struct FlipProgram {
 FlipProgram compile_flip_program(const std::vector<Instance>& adjoint, const LocalFactors& f, int sites,
                                  bool fixed_weight);
 
-enum LookupMode : int { kLookupAuto = 0, kLookupTable = 1, kLookupSearch = 2, kLookupLegacy = 3 };
+// kLookupTableGeneric: the image table with the general tile kernel even
+// where the nearest-neighbour hop kernel applies (kept for comparisons).
+enum LookupMode : int { kLookupAuto = 0, kLookupTable = 1, kLookupSearch = 2, kLookupLegacy = 3,
+                        kLookupTableGeneric = 4 };
+
 
 // Device copy of a flip program, one buffer the kernel stages in shared
 // memory: [generic terms][groups][amp_re][amp_im][diagonal pair sites].
@@ -142,6 +146,9 @@ struct TileLaunch {
   double alpha = 1.0, beta = 0.0, gamma = 0.0;
   const double* inv_sqrt = nullptr;  // [R] 1/sqrt(R), [257 + R] sqrt(R), R <= 256
   cudaStream_t stream = nullptr;
+  // Rows computed: row0 .. row0 + rows - 1 (clipped to the dimension). x (or
+  // z) is the full vector; y, p and the output block hold these rows only.
+  uint64_t row0 = 0, rows = ~0ull;
 };
 
 // Runs the tile kernel with the lookup `mode` (auto: the table when the
@@ -149,6 +156,11 @@ struct TileLaunch {
 // outside the kernel's scope (u128 states, no flip program, requested table
 // absent), in which case nothing was launched.
 bool launch_tile(const SpinBasis& basis, const DeviceFlipProgram& prog, int mode, const TileLaunch& a);
+
+// True when the nearest-neighbour hop kernel serves this operator on this
+// basis: a chain program whose only off-diagonal class is the bond (i, i + 1),
+// a real fixed-weight sector and a 32-bit image table without phase index.
+bool hop_kernel_applies(const SpinBasis& basis, const DeviceFlipProgram& prog);
 
 // True when this basis can hold an image table within `limit_bytes`.
 bool image_table_feasible(const SpinBasis& basis, uint64_t limit_bytes, uint64_t* bytes_out);

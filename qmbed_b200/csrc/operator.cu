@@ -906,9 +906,29 @@ bool SpinOperator::launch_tile_action(const TileLaunch& l) const {
   return launch_tile(*basis_, prog_, lookup_mode_, a);
 }
 
+void SpinOperator::apply_rows(int precision, uint64_t row0, uint64_t rows, const void* x, void* y,
+                              cudaStream_t stream) const {
+  QMBED_CUDA(cudaSetDevice(basis_->device()));
+  const uint64_t n = dim();
+  if (row0 > n || rows > n - row0) raise(QMBED_INVALID_OPTIONS, "row range outside the operator");
+  if (!real_) raise(QMBED_UNSUPPORTED_BACKEND, "row slabs take real vectors of a real operator");
+  if (storage_ != kStorageMatrixFree) raise(QMBED_UNSUPPORTED_BACKEND, "row slabs need matrix-free storage");
+  if (rows == 0) return;
+  TileLaunch tl;
+  tl.precision = precision;
+  tl.nb = 1;
+  tl.x = x;
+  tl.y = y;
+  tl.stream = stream;
+  tl.row0 = row0;
+  tl.rows = rows;
+  if (!launch_tile_action(tl))
+    raise(QMBED_UNSUPPORTED_BACKEND, "row slabs need the tile kernel (u64 states, products on distinct sites)");
+}
+
 void SpinOperator::set_lookup(int mode) {
-  if (mode < kLookupAuto || mode > kLookupLegacy) raise(QMBED_INVALID_OPTIONS, "unknown lookup mode");
-  if (mode == kLookupTable) {
+  if (mode < kLookupAuto || mode > kLookupTableGeneric) raise(QMBED_INVALID_OPTIONS, "unknown lookup mode");
+  if (mode == kLookupTable || mode == kLookupTableGeneric) {
     if (!prog_.ok() || !basis_->symmetric())
       raise(QMBED_UNSUPPORTED_BACKEND, "image tables serve symmetry sectors of u64 states with a flip program");
     QMBED_CUDA(cudaSetDevice(basis_->device()));
@@ -920,7 +940,8 @@ void SpinOperator::set_lookup(int mode) {
 int SpinOperator::lookup_in_use() const {
   if (lookup_mode_ == kLookupLegacy || !prog_.ok() || basis_->words() != 1) return 3;
   if (!basis_->symmetric()) return 4;
-  if (lookup_mode_ != kLookupSearch && basis_->image_table()) return 1;
+  if (lookup_mode_ != kLookupSearch && basis_->image_table())
+    return lookup_mode_ != kLookupTableGeneric && hop_kernel_applies(*basis_, prog_) ? 5 : 1;
   return 2;
 }
 

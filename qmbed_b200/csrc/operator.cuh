@@ -79,6 +79,11 @@ class SpinOperator {
   void apply(int precision, bool complex_vectors, const void* x, void* y, cudaStream_t stream,
              bool force_matrix_free = false) const;
 
+  // Rows row0 .. row0 + rows - 1 of y = H x (real vectors, terms expanded on
+  // the fly by the tile kernels): x is the full vector, y holds those rows
+  // only. The slab form of a row-partitioned operator across devices.
+  void apply_rows(int precision, uint64_t row0, uint64_t rows, const void* x, void* y, cudaStream_t stream) const;
+
   // The same action with the x / sqrt(R) vector of symmetric stored rows
   // written to caller-provided device memory (`scratch`, `scratch_bytes`)
   // instead of a buffer this object allocates. Paths that need no such

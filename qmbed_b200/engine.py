@@ -11,7 +11,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import EigshInfoC, EigshOptionsC, QmbedError, check, lib
+from ._lib import EigshHintC, EigshInfoC, EigshOptionsC, QmbedError, check, lib
 
 NORMALIZATIONS = {"angular_momentum": 0, "pauli": 1, "pauli_cartesian": 2}
 TARGETS = {
@@ -27,8 +27,8 @@ EVOLUTION_DIAGNOSTICS = ("lanczos_projections", "matrix_vector_products", "real_
                          "real_matrix_vector_products", "accepted_substeps", "rejected_trial_intervals",
                          "maximum_estimated_error")
 STORAGE = {"matrix_free": 0, "packed": 1, "explicit": 2}
-LOOKUPS = {"auto": 0, "table": 1, "search": 2, "legacy": 3}
-LOOKUPS_IN_USE = {1: "table", 2: "search", 3: "legacy", 4: "index"}
+LOOKUPS = {"auto": 0, "table": 1, "search": 2, "legacy": 3, "table_generic": 4}
+LOOKUPS_IN_USE = {1: "table", 2: "search", 3: "legacy", 4: "index", 5: "table_hop"}
 
 
 def _ptr(array):
@@ -140,6 +140,8 @@ class EigshResult:
     fp64_iterations: int
     operator_applications: int
     converged: bool
+    hint_used: bool = False
+    bound_applications: int = 0
 
 
 class GpuOperator:
@@ -225,7 +227,7 @@ class GpuOperator:
                                                             _ptr(y), None if stream is None else ctypes.c_void_p(stream)))
 
     def set_lookup(self, mode: str) -> None:
-        """Lookup of the matrix-free action: "auto", "table", "search" or "legacy"."""
+        """Lookup of the matrix-free action: "auto", "table", "search", "legacy" or "table_generic"."""
         check(lib().qmbed_gpu_operator_set_lookup(self.handle, LOOKUPS[mode]))
 
     def lookup_info(self) -> dict:
@@ -259,7 +261,13 @@ class GpuOperator:
 
     def eigsh(self, eigenpairs: int, target: str = "smallest_algebraic", shift: float = 0.0,
               krylov_dimension: int | None = None, tolerance: float = 1e-10, max_iterations: int = 1000,
-              seed: int = 0, initial=None, eigenvectors: bool = False, mode: str = "fp64") -> EigshResult:
+              seed: int = 0, initial=None, eigenvectors: bool = False, mode: str = "fp64",
+              hint: dict | None = None) -> EigshResult:
+        """Reference eigsh (mode "fp64") or the mixed / filtered GPU modes.
+
+        `hint` (optional): {"lower", "upper", "gap", "restart_keep", "check_steps"}, a
+        predicted spectral interval and gap (qmbed_gpu_eigsh_hinted); the result
+        then says whether the interval passed its Lanczos check."""
         n = self.dim
         options = EigshOptionsC(eigenpairs, TARGETS[target], shift, krylov_dimension or 0, tolerance, max_iterations,
                                 seed, MODES[mode])
@@ -272,11 +280,20 @@ class GpuOperator:
         residuals = np.zeros(eigenpairs)
         vectors = np.zeros((eigenpairs, n), np.complex128) if eigenvectors else None
         info = EigshInfoC()
-        check(lib().qmbed_gpu_eigsh(self.handle, ctypes.byref(options), _ptr(initial), n_initial, _ptr(values),
-                                    _ptr(residuals), _ptr(vectors), ctypes.byref(info)))
+        if hint is None:
+            check(lib().qmbed_gpu_eigsh(self.handle, ctypes.byref(options), _ptr(initial), n_initial, _ptr(values),
+                                        _ptr(residuals), _ptr(vectors), ctypes.byref(info)))
+            used, bound = False, 0
+        else:
+            h = EigshHintC(float(hint.get("lower", 0.0)), float(hint.get("upper", 0.0)), float(hint.get("gap", 0.0)),
+                           int(hint.get("restart_keep", 0)), int(hint.get("check_steps", 8)), 0, 0)
+            check(lib().qmbed_gpu_eigsh_hinted(self.handle, ctypes.byref(options), ctypes.byref(h), _ptr(initial),
+                                               n_initial, _ptr(values), _ptr(residuals), _ptr(vectors),
+                                               ctypes.byref(info)))
+            used, bound = bool(h.used), int(h.bound_applications)
         return EigshResult(values, residuals, vectors, info.iterations, info.reorthogonalization_passes,
                            info.conditional_second_passes, info.fp32_iterations, info.fp64_iterations,
-                           info.operator_applications, bool(info.converged))
+                           info.operator_applications, bool(info.converged), used, bound)
 
     def evolve(self, initial, times, krylov_dimension: int = 30, tolerance: float = 1e-10,
                max_substeps: int = 10_000):

@@ -1,4 +1,4 @@
-"""Learned spectral bounds for the Chebyshev propagator.
+"""Learned spectral bounds: the Chebyshev propagator and the eigsh hint.
 
 A small ReLU network (4 hidden layers of 128 by default) maps the parameters
 of a transverse-field Ising chain with random longitudinal fields (size L,
@@ -13,6 +13,15 @@ that fails to contain them is wrong and the plain Lanczos bound estimate is
 used instead. The norm of the propagated state is the second check: if it
 drifts, the interval missed part of the spectrum and the propagation is
 repeated with the guaranteed bound +-sum|coefficients|.
+
+The second network (ChainSpectrum) maps the couplings, size and momentum of a
+J1-J2 / XXZ chain sector to its lowest eigenvalue, its largest eigenvalue and
+the gap above the lowest one. Its training set is what the batched scan
+solver (qmbed_gpu_scan_solve) returns for every sector and scan point. Its
+prediction becomes an eigsh hint: the padded interval replaces the filtered
+solver's own Lanczos bound estimate once a short Lanczos check finds the
+interval holding its Ritz values, and the predicted relative gap sets how
+many Ritz vectors the thick restart keeps per cycle.
 """
 
 from __future__ import annotations
@@ -233,3 +242,79 @@ def propagate(op: GpuOperator, psi0, times, interval: Interval, precision: int =
         info["source"] = "norm bound (after drift)"
         info["bound_applications"] = interval.applications
     return states, info
+
+
+# ---------------------------------------------------------------------------
+# Chain spectra for the eigsh hint
+# ---------------------------------------------------------------------------
+
+CHAIN_FEATURES = ("inverse_sites", "j2", "delta", "cos_momentum", "momentum_zero", "sites_mod_4")
+CHAIN_TARGETS = ("e0_per_site", "e_max_per_site", "gap_times_sites")
+
+
+def chain_features(sites: int, j2: float, delta: float, momentum: int) -> np.ndarray:
+    """Network inputs of a momentum sector of H = Delta (zz1 + J2 zz2) + flips1 + J2 flips2
+    at half filling: 1/L, J2, Delta, cos(2 pi k / L), [k = 0] and [L = 0 mod 4] (the
+    sector holding the ground state alternates with L mod 4 by the Marshall sign rule)."""
+    return np.array([1.0 / sites, j2, delta, np.cos(2.0 * np.pi * momentum / sites), 1.0 if momentum == 0 else 0.0,
+                     1.0 if sites % 4 == 0 else 0.0], np.float32)
+
+
+def scan_training_set(sizes=(12, 14, 16, 18, 20), points: int = 16, seed: int = 0, j2_max: float = 0.5,
+                      delta_range=(0.5, 1.5), device: int = 0, tolerance: float = 1e-10):
+    """Training set from the batched scan solver: for every size, every momentum
+    sector at half filling times `points` scan points (J2 on a grid, Delta drawn),
+    the scan's lowest two eigenvalues and largest Ritz value give the targets
+    (E0 / L, E_max / L, (E1 - E0) L). Returns (x, y, info)."""
+    from . import scan
+    xs, ys = [], []
+    solves = 0
+    for sites in sizes:
+        components = scan.j1j2_sectors(sites, device=device)
+        coef = scan.j1j2_scan_points(points, seed=seed + sites, j2_max=j2_max, delta_range=delta_range)
+        values, steps, info = scan.scan_lowest(components, coef, eigenpairs=2, tolerance=tolerance, seed=seed)
+        e_max = info["e_max"]
+        for k in range(sites):
+            for p in range(points):
+                delta, j2 = float(coef[p, 0]), float(coef[p, 3])
+                e0, e1 = float(values[k, p, 0]), float(values[k, p, 1])
+                xs.append(chain_features(sites, j2, delta, k))
+                ys.append([e0 / sites, float(e_max[k, p]) / sites, (e1 - e0) * sites])
+        solves += sites * points
+        del components
+    return np.array(xs, np.float32), np.array(ys, np.float32), {"solves": solves, "sizes": list(sizes)}
+
+
+class ChainSpectrum:
+    """Lowest and largest eigenvalue and the gap of chain sectors from a GPU network."""
+
+    def __init__(self, mlp: GpuMlp | None = None, margin: float = 0.03, check_steps: int = 8, device: int = 0):
+        self.mlp = mlp or GpuMlp(len(CHAIN_FEATURES), len(CHAIN_TARGETS), device=device)
+        self.margin = margin
+        self.check_steps = check_steps
+
+    def fit(self, x, y, epochs: int = 400, batch: int = 64, learning_rate: float = 2e-3, seed: int = 0) -> float:
+        return self.mlp.train(x, y, epochs=epochs, batch=batch, learning_rate=learning_rate, seed=seed)
+
+    def predict(self, sites: int, j2: float, delta: float, momentum: int):
+        """(E0, E_max, gap) of the momentum sector (half filling)."""
+        e0, emax, gap = self.mlp.predict(chain_features(sites, j2, delta, momentum))[0]
+        return float(e0) * sites, float(emax) * sites, max(float(gap), 0.0) / sites
+
+    def hint(self, sites: int, j2: float, delta: float, momentum: int, eigenpairs: int,
+             krylov_dimension: int = 40) -> dict:
+        """eigsh hint for a sector of these couplings (a parity subsector of momentum
+        sector k has its spectrum inside sector k's, so the interval still holds it).
+
+        Interval: [E0, E_max] padded by `margin` of its width on both sides.
+        Restart size: with a small predicted relative gap (E1 - E0) / (E_max - E0) the
+        thick restart keeps half the Krylov dimension, otherwise the wanted pairs and
+        four more."""
+        e0, emax, gap = self.predict(sites, j2, delta, momentum)
+        width = max(emax - e0, 1e-12)
+        relative_gap = gap / width
+        half = krylov_dimension // 2
+        keep = half if relative_gap < 0.02 else min(half, eigenpairs + 4)
+        return {"lower": e0 - self.margin * width, "upper": emax + self.margin * width, "gap": gap,
+                "restart_keep": keep, "check_steps": self.check_steps, "relative_gap": relative_gap,
+                "e0": e0, "e_max": emax}

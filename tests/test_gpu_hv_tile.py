@@ -76,7 +76,17 @@ def engine():
 
 def _lookups(case):
     symmetric = case[3] is not None or case[4] is not None
-    return ["table", "search", "legacy"] if symmetric else ["auto", "legacy"]
+    return ["table", "table_generic", "search", "legacy"] if symmetric else ["auto", "legacy"]
+
+
+def _expected_in_use(lookup, info):
+    """The lookup that lookup_info reports for a requested one: "table" runs the
+    nearest-neighbour hop kernel where it applies."""
+    if lookup == "table":
+        return info["lookup"] in ("table", "table_hop")
+    if lookup == "table_generic":
+        return info["lookup"] == "table"
+    return info["lookup"] == lookup
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(map(str, c)))
@@ -91,8 +101,8 @@ def test_tile_hv_fp64_matches_oracle(engine, oracle, case):
     for lookup in _lookups(case):
         g.set_lookup(lookup)
         info = g.lookup_info()
-        if lookup in ("table", "search", "legacy"):
-            assert info["lookup"] == lookup
+        if lookup in ("table", "table_generic", "search", "legacy"):
+            assert _expected_in_use(lookup, info), (lookup, info)
         got = g.apply(xc)
         assert np.linalg.norm(got - expected_c) <= 1e-13 * max(np.linalg.norm(expected_c), 1.0), lookup
         if expected_r is not None:
@@ -140,7 +150,7 @@ def test_tile_block_action_matches_packed(engine, sites, momentum, parity, preci
     ref = torch.empty_like(z)
     packed.apply_block_device(z, ref, nb, precision=precision, alpha=0.7, beta=-0.2, gamma=0.4, p=p)
     tol = 1e-13 if precision == 64 else 2e-5
-    for lookup in ("table", "search", "legacy"):
+    for lookup in ("table", "table_generic", "search", "legacy"):
         free.set_lookup(lookup)
         out = torch.full_like(z, float("nan"))
         free.apply_block_device(z, out, nb, precision=precision, alpha=0.7, beta=-0.2, gamma=0.4, p=p)
@@ -209,7 +219,7 @@ def test_matrix_free_defaults_to_the_image_table(engine):
     g = engine.GpuOperator(engine.GpuBasis(20, up=10, momentum=0, parity=1), heisenberg_terms(20),
                            storage="matrix_free")
     info = g.lookup_info()
-    assert info["lookup"] == "table"
+    assert info["lookup"] == "table_hop"
     assert info["table_bytes"] == 184756 * 4  # C(20, 10) u32 entries
 
 
@@ -229,9 +239,83 @@ def test_tile_lookups_agree_at_26_sites(engine):
                         generator=torch.Generator(device="cuda").manual_seed(momentum))
         ref = torch.empty_like(x)
         packed.apply_device(x, ref, precision=64, complex_vectors=cplx)
-        for lookup in ("table", "search", "legacy"):
+        for lookup in ("table", "table_generic", "search", "legacy"):
             free.set_lookup(lookup)
             y = torch.full_like(x, float("nan"))
             free.apply_device(x, y, precision=64, complex_vectors=cplx)
             torch.cuda.synchronize()
             assert float(torch.linalg.vector_norm(y - ref)) <= 1e-13 * float(torch.linalg.vector_norm(ref)), lookup
+
+
+# (sites, up, momentum, parity, delta, periodic): real sectors of nearest-neighbour chains
+HOP_CASES = [(16, 8, 0, 1, 1.0, True), (18, 9, 9, -1, 0.73, True), (17, 8, 0, None, 1.2, True),
+             (16, 7, 8, 1, 0.5, True), (14, 7, None, 1, 0.9, False), (15, 7, None, -1, 1.0, False),
+             (20, 10, 0, -1, 1.35, True)]
+
+
+def _hop_terms(sites, delta, periodic):
+    bonds = [(i, (i + 1) % sites) for i in range(sites if periodic else sites - 1)]
+    return [("zz", [(delta, b) for b in bonds]), ("+-", [(0.5, b) for b in bonds]), ("-+", [(0.5, b) for b in bonds])]
+
+
+@pytest.mark.parametrize("case", HOP_CASES, ids=lambda c: "-".join(map(str, c)))
+def test_hop_kernel_matches_oracle(engine, oracle, case):
+    """The nearest-neighbour hop kernel (rank steps by one binomial, the wrapping
+    bond from the chunk tables) against the oracle: FP64 1e-13, FP32 5e-6."""
+    import torch
+    sites, up, momentum, parity, delta, periodic = case
+    terms = _hop_terms(sites, delta, periodic)
+    o = oracle.Operator.build(oracle.Basis(sites, up=up, momentum=momentum, parity=parity), terms)
+    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity), terms,
+                           storage="matrix_free")
+    assert g.lookup_info()["lookup"] == "table_hop"
+    x = np.random.default_rng(sites).normal(size=o.dim)
+    expected = o.apply(x).real
+    assert np.linalg.norm(g.apply(x) - expected) <= 1e-13 * np.linalg.norm(expected)
+    xd = torch.tensor(x, dtype=torch.float32, device="cuda")
+    yd = torch.full_like(xd, float("nan"))
+    g.apply_device(xd, yd, precision=32)
+    torch.cuda.synchronize()
+    assert np.linalg.norm(yd.double().cpu().numpy() - expected) <= 5e-6 * np.linalg.norm(expected)
+
+
+@pytest.mark.parametrize("case", HOP_CASES[:4], ids=lambda c: "-".join(map(str, c)))
+@pytest.mark.parametrize("precision,nb", [(64, 8), (64, 16), (32, 8), (32, 16)])
+def test_hop_block_action_matches_generic_tile(engine, case, precision, nb):
+    """Block action of the hop kernel against the general tile kernel on the same table."""
+    import torch
+    sites, up, momentum, parity, delta, periodic = case
+    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity),
+                           _hop_terms(sites, delta, periodic), storage="matrix_free")
+    n = g.dim
+    dtype = torch.float64 if precision == 64 else torch.float32
+    gen = torch.Generator(device="cuda").manual_seed(nb + sites)
+    z = torch.randn(n, nb, dtype=dtype, device="cuda", generator=gen)
+    p = torch.randn(n, nb, dtype=dtype, device="cuda", generator=gen)
+    g.set_lookup("table_generic")
+    ref = torch.full_like(z, float("nan"))
+    g.apply_block_device(z, ref, nb, precision=precision, alpha=0.6, beta=0.3, gamma=-0.5, p=p)
+    g.set_lookup("table")
+    out = torch.full_like(z, float("nan"))
+    g.apply_block_device(z, out, nb, precision=precision, alpha=0.6, beta=0.3, gamma=-0.5, p=p)
+    torch.cuda.synchronize()
+    tol = 1e-13 if precision == 64 else 2e-6
+    err = float(torch.linalg.vector_norm((out - ref).double()))
+    assert err <= tol * float(torch.linalg.vector_norm(ref.double())), err
+
+
+def test_hop_kernel_agrees_with_packed_rows_at_28_sites(engine):
+    """Size-independent check at the XXZ benchmark size: hop kernel against the
+    packed rows in FP64 (L=28, k=0, p=+1, D = 718,146)."""
+    import torch
+    terms = _hop_terms(28, 1.35, True)
+    basis = engine.GpuBasis(28, up=14, momentum=0, parity=1)
+    packed = engine.GpuOperator(basis, terms, storage="packed")
+    free = engine.GpuOperator(basis, terms, storage="matrix_free")
+    assert free.lookup_info()["lookup"] == "table_hop"
+    x = torch.randn(packed.dim, dtype=torch.float64, device="cuda", generator=torch.Generator(device="cuda").manual_seed(1))
+    ref, y = torch.empty_like(x), torch.full_like(x, float("nan"))
+    packed.apply_device(x, ref, precision=64)
+    free.apply_device(x, y, precision=64)
+    torch.cuda.synchronize()
+    assert float(torch.linalg.vector_norm(y - ref)) <= 1e-13 * float(torch.linalg.vector_norm(ref))
