@@ -10,10 +10,13 @@ before timing (their times are reported). Synthetic: the Hamiltonian is the
 model itself, no dataset.
 
 Arms:
-  default           mixed-precision GPU solve (FP32 vectors/H.v, FP64
-                    recurrences and FP64 refinement to 1e-10)
+  default           block Chebyshev-filtered GPU solve on packed rows (FP32
+                    blocks, then FP64 to 1e-10 with every residual verified),
+                    with the spectral hint predicted by the network trained
+                    on the batched scan's outputs (--no-learned: without it)
   --impl reference  the CPU oracle (restatement of the reference eigsh) on a
-                    bounded sample (L=24 sector solve), scaled to L=34
+                    bounded sample (40 thick-restart steps at L=28), scaled to
+                    L=34
 
 One JSON line on rank 0. Under torchrun each rank solves its own replica.
 """
@@ -68,7 +71,63 @@ def parse():
                    help="on-the-fly (matrix-free) H.v, block action and solves at this size (0 skips it)")
     p.add_argument("--scan-sites", type=int, default=26,
                    help="batched J1-J2 scan size: every momentum sector x 64 points (0 skips it)")
+    p.add_argument("--no-learned", action="store_true",
+                   help="solve without the learned spectral hint (the network trained on the batched scan)")
+    p.add_argument("--row-partition", action="store_true",
+                   help="under torchrun: also solve the sector once row-partitioned across the ranks")
     return p.parse_args()
+
+
+def learned_hint(sites: int, eigenpairs: int, krylov: int, local_rank: int) -> tuple[dict, dict]:
+    """Train the chain-spectrum network on the batched scan's outputs at 12-20
+    sites (every momentum sector x 16 points) and predict the eigsh hint of
+    the benchmark sector (Heisenberg: J2 = 0, Delta = 1, k = 0)."""
+    import torch
+    from qmbed_b200 import learned
+
+    t0 = time.perf_counter()
+    x, y, info = learned.scan_training_set(sizes=(12, 14, 16, 18, 20), points=16, seed=0, device=local_rank)
+    t1 = time.perf_counter()
+    model = learned.ChainSpectrum(device=local_rank)
+    loss = model.fit(x, y, epochs=300, seed=1)
+    torch.cuda.synchronize()
+    hint = model.hint(sites, 0.0, 1.0, 0, eigenpairs=eigenpairs, krylov_dimension=krylov)
+    return hint, {"training_solves": info["solves"], "training_sizes": info["sizes"], "scan_s": t1 - t0,
+                  "train_s": time.perf_counter() - t1, "final_loss": loss,
+                  "prediction": {"e0": hint["e0"], "e_max": hint["e_max"], "gap": hint["gap"]},
+                  "hint": {k: hint[k] for k in ("lower", "upper", "restart_keep", "check_steps")}}
+
+
+def row_partition_section(sites: int, eigenpairs: int, krylov: int, tolerance: float, rank: int, world: int,
+                          local_rank: int) -> dict:
+    """One solve of the sector row-partitioned across the ranks: matrix-free slab
+    kernel per rank, NCCL all-gather of x per application, all-reduced
+    Gram-Schmidt (qmbed_b200.distributed). Device time, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from qmbed_b200 import engine
+    from qmbed_b200.distributed import RowPartition, distributed_eigsh, gpu_slab
+
+    basis = engine.GpuBasis(sites, up=sites // 2, momentum=0, parity=1, device=local_rank)
+    op = engine.GpuOperator(basis, engine.heisenberg_terms(sites), storage="matrix_free")
+    part = RowPartition(op.dim, world)
+    row0, rows = part.range(rank)
+    start = torch.as_tensor(engine.deterministic_start(op.dim, 0, device=local_rank)[row0:row0 + rows],
+                            device="cuda")
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    r = distributed_eigsh(gpu_slab(op, part, rank), part, eigenpairs, krylov_dimension=krylov, tolerance=tolerance,
+                          start=start, restart_keep=krylov // 2, device="cuda")
+    t1.record()
+    torch.cuda.synchronize()
+    t = torch.tensor([t0.elapsed_time(t1) / 1000.0], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return {"workload": f"heisenberg L={sites} k=0 p=+1 dim={op.dim}, matrix-free rows split over {world} ranks",
+            "s": float(t.item()), "applications": r.applications, "restarts": r.restarts,
+            "converged": r.converged, "eigenvalues": r.eigenvalues.tolist(),
+            "max_residual": float(np.max(r.residuals))}
 
 
 def timed_launches(fn, count: int) -> float:
@@ -573,7 +632,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(minutes=5), device_id=torch.device("cuda", local_rank))
 
     from qmbed_b200 import engine
-    from qmbed_b200._lib import EigshInfoC, EigshOptionsC, check, lib
+    from qmbed_b200._lib import EigshHintC, EigshInfoC, EigshOptionsC, check, lib
 
     sites = args.sites
     if args.only == "matrix_free":
@@ -591,6 +650,9 @@ def main():
     dim = info["dimension"]
 
     solve_kw = dict(krylov_dimension=args.krylov, tolerance=args.tolerance, seed=rank)
+    hint, learned_info = None, None
+    if not args.no_learned:
+        hint, learned_info = learned_hint(sites, args.eigenpairs, args.krylov, local_rank)
 
     def barrier():
         torch.cuda.synchronize()
@@ -600,14 +662,14 @@ def main():
     # --- warm-up and timed solves (inputs resident) ---
     results = []
     for _ in range(args.warmup):
-        op.eigsh(args.eigenpairs, mode=args.mode, **solve_kw)
+        op.eigsh(args.eigenpairs, mode=args.mode, hint=hint, **solve_kw)
     launches_before = engine.launch_count()
     barrier()
     with ClockSampler(local_rank) as clocks:
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
         for _ in range(args.steps):
-            results.append(op.eigsh(args.eigenpairs, mode=args.mode, **solve_kw))
+            results.append(op.eigsh(args.eigenpairs, mode=args.mode, hint=hint, **solve_kw))
         stop.record()
         barrier()
     launches = engine.launch_count() - launches_before
@@ -618,6 +680,22 @@ def main():
         elapsed = float(t.item())
     value = elapsed / (args.steps * world)
     last = results[-1]
+
+    # --- the same solve without the learned hint, once (what the network gains) ---
+    if learned_info is not None:
+        barrier()
+        u_start, u_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        u_start.record()
+        ru = op.eigsh(args.eigenpairs, mode=args.mode, **solve_kw)
+        u_stop.record()
+        barrier()
+        learned_info.update({
+            "hint_used": bool(last.hint_used), "bound_applications": last.bound_applications,
+            "applications": last.operator_applications,
+            "without_hint": {"s": u_start.elapsed_time(u_stop) / 1000.0, "applications": ru.operator_applications,
+                             "bound_applications": ru.bound_applications, "iterations": ru.iterations},
+            "max_rel_diff_vs_without": float(np.max(np.abs(ru.eigenvalues - last.eigenvalues)
+                                                    / np.abs(ru.eigenvalues)))})
 
     # --- plain FP64 path (the reference algorithms in FP64), once ---
     plain = None
@@ -707,15 +785,20 @@ def main():
     options = EigshOptionsC(args.eigenpairs, 0, 0.0, args.krylov, args.tolerance, 1000, rank,
                             engine.MODES[args.mode])
     e2e_info = EigshInfoC()
+    e2e_hint = None if hint is None else EigshHintC(hint["lower"], hint["upper"], hint["gap"], hint["restart_keep"],
+                                                    hint["check_steps"], 0, 0)
     h2d = v0.nbytes
     d2h = vectors.nbytes + values.nbytes + residuals.nbytes
     barrier()
     e2e_times = []
     for _ in range(0 if args.no_e2e else max(1, min(args.steps, 2))):
         t_e2e = time.perf_counter()
-        check(lib().qmbed_gpu_eigsh(op.handle, ctypes.byref(options), v0.ctypes.data_as(ctypes.c_void_p), 1,
-                                    values.ctypes.data_as(ctypes.c_void_p), residuals.ctypes.data_as(ctypes.c_void_p),
-                                    vectors.ctypes.data_as(ctypes.c_void_p), ctypes.byref(e2e_info)))
+        check(lib().qmbed_gpu_eigsh_hinted(op.handle, ctypes.byref(options),
+                                           None if e2e_hint is None else ctypes.byref(e2e_hint),
+                                           v0.ctypes.data_as(ctypes.c_void_p), 1,
+                                           values.ctypes.data_as(ctypes.c_void_p),
+                                           residuals.ctypes.data_as(ctypes.c_void_p),
+                                           vectors.ctypes.data_as(ctypes.c_void_p), ctypes.byref(e2e_info)))
         e2e_times.append(time.perf_counter() - t_e2e)
     e2e_value = statistics.median(e2e_times) if e2e_times else None
     if world > 1 and e2e_value is not None:
@@ -748,6 +831,10 @@ def main():
     if args.scan_sites > 0:
         scan_result = scan_section(args.scan_sites, rank, local_rank, rank == 0 and world == 1 and not args.no_cpu)
 
+    row_result = None
+    if args.row_partition and world > 1:
+        row_result = row_partition_section(sites, args.eigenpairs, args.krylov, args.tolerance, rank, world, local_rank)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -758,7 +845,9 @@ def main():
                                    f"lowest, tol {args.tolerance:g}, mode {args.mode}"
                                    + (" (block Chebyshev-filtered subspace iteration)" if args.mode == "filtered"
                                       else f" (thick-restart Lanczos, krylov {args.krylov})")
-                                   + ", storage packed rows (4 B per stored entry)",
+                                   + ", storage packed rows (4 B per stored entry)"
+                                   + (", spectral hint from the network trained on the batched scan"
+                                      if learned_info is not None else ""),
                        "plain_fp64": f"thick-restart Lanczos, krylov {args.krylov}, reference algorithms in FP64,"
                                      " same storage",
                        "l2": "working set (GBs of vectors and packed rows) exceeds the 126 MB L2",
@@ -766,6 +855,8 @@ def main():
             "eigenvalues": last.eigenvalues.tolist(), "residuals": last.residuals.tolist(),
             "iterations": last.iterations, "fp32_iterations": last.fp32_iterations,
             "fp64_iterations": last.fp64_iterations,
+            "learned": learned_info,
+            "row_partition": row_result,
             "plain_fp64": plain,
             "speedup_vs_plain_fp64": (plain["s"] / value) if plain else None,
             "setup": {"basis_build_s": build_s, "assembly_s": info["assembly_seconds"], "total_s": setup_s,
@@ -784,7 +875,7 @@ def main():
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "_fallback" not in peaks
                          else "fallback 6650 GB/s"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "path": "qmbed_gpu_eigsh C ABI, host v0 in, host eigenvectors out"},
+                    "path": "qmbed_gpu_eigsh_hinted C ABI (the learned hint), host v0 in, host eigenvectors out"},
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "gpu_launches": launches,
