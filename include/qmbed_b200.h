@@ -242,7 +242,12 @@ QMBED_API int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* opti
  * Ritz values must lie inside it, else the solver's own bound estimate is
  * used). On return, used = 1 when the interval passed the check and set the
  * filter, and bound_applications counts the operator applications spent on
- * spectral bounds. */
+ * spectral bounds. An accepted hint with gap > 0 also places the filter's first
+ * cut at lower + nb * gap when that is below the check's Ritz value (nb = 8 or
+ * 16, the block width). upper <= lower and restart_keep = 0 give an empty
+ * hint: the solve is that of qmbed_gpu_eigsh and the outputs are still set.
+ * restart_keep applies to FP64 thick restarts (the mixed mode's FP32 phase
+ * keeps the reference's size). */
 typedef struct {
   double lower;
   double upper;

@@ -735,6 +735,10 @@ EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options, con
   Ctx c32{op, ops, 32, cplx, n};
   EigshOptions first = options;
   first.tolerance = std::max(options.tolerance, kMixedHandover);
+  // The FP32 phase keeps the reference's restart size: Ritz vectors kept
+  // beyond the wanted ones carry FP32 actions whose residual directions are
+  // rounding noise, and the phase then stalls short of its handover.
+  first.restart_keep = 0;
   Panel init32;
   const int n_init32 = upload_initial(c32, init32);
   EigshResult phase1;

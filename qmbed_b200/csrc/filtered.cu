@@ -567,7 +567,12 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
                                  : bd.theta.back() + bd.top_residual + 0.01 * (bd.theta.back() - bd.theta.front());
   double lower = bd.theta.front();
   // First cut: the k-th Ritz value, which lies at or above the k-th eigenvalue.
+  // With an accepted hint, the predicted gap places it nb gaps above the
+  // interval's lower end when that is lower (the level density grows with
+  // energy, so nb gaps lie above the block's share of the spectrum); a cut
+  // near the wanted end lets the first filters take a high degree.
   double cut = bd.theta[std::min<size_t>(k, bd.theta.size()) - 1];
+  if (hint_used && o.hint_gap > 0.0) cut = std::min(cut, o.hint_lower + nb * o.hint_gap);
   if (!(cut > lower)) cut = lower + 0.1 * (upper - lower);
 
   std::vector<double> theta, res;

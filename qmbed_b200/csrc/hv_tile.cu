@@ -912,7 +912,7 @@ constexpr int kHopMaxClasses = 64;
 
 template <typename T, int NB>
 struct HopShape {
-  static constexpr int U = NB == 1 ? 4 : (NB * sizeof(T) <= 32 ? 4 : 2);
+  static constexpr int U = NB == 1 ? 4 : (NB * sizeof(T) <= 64 ? 4 : 2);
   static constexpr int MIN_BLOCKS = NB == 1 ? 4 : (NB * sizeof(T) <= 32 ? 3 : 2);
 };
 

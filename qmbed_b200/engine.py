@@ -280,17 +280,14 @@ class GpuOperator:
         residuals = np.zeros(eigenpairs)
         vectors = np.zeros((eigenpairs, n), np.complex128) if eigenvectors else None
         info = EigshInfoC()
-        if hint is None:
-            check(lib().qmbed_gpu_eigsh(self.handle, ctypes.byref(options), _ptr(initial), n_initial, _ptr(values),
-                                        _ptr(residuals), _ptr(vectors), ctypes.byref(info)))
-            used, bound = False, 0
-        else:
-            h = EigshHintC(float(hint.get("lower", 0.0)), float(hint.get("upper", 0.0)), float(hint.get("gap", 0.0)),
-                           int(hint.get("restart_keep", 0)), int(hint.get("check_steps", 8)), 0, 0)
-            check(lib().qmbed_gpu_eigsh_hinted(self.handle, ctypes.byref(options), ctypes.byref(h), _ptr(initial),
-                                               n_initial, _ptr(values), _ptr(residuals), _ptr(vectors),
-                                               ctypes.byref(info)))
-            used, bound = bool(h.used), int(h.bound_applications)
+        # an empty hint (upper <= lower, restart_keep 0) changes nothing and reports the bound work
+        hint = hint or {}
+        h = EigshHintC(float(hint.get("lower", 0.0)), float(hint.get("upper", 0.0)), float(hint.get("gap", 0.0)),
+                       int(hint.get("restart_keep", 0)), int(hint.get("check_steps", 8)), 0, 0)
+        check(lib().qmbed_gpu_eigsh_hinted(self.handle, ctypes.byref(options), ctypes.byref(h), _ptr(initial),
+                                           n_initial, _ptr(values), _ptr(residuals), _ptr(vectors),
+                                           ctypes.byref(info)))
+        used, bound = bool(h.used), int(h.bound_applications)
         return EigshResult(values, residuals, vectors, info.iterations, info.reorthogonalization_passes,
                            info.conditional_second_passes, info.fp32_iterations, info.fp64_iterations,
                            info.operator_applications, bool(info.converged), used, bound)
