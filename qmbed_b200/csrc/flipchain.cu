@@ -11,8 +11,15 @@
 // D(s) = D_low(j) + D_high(t) + D_cross(s): terms inside the low bits come from
 // a 2^tb table computed once, terms inside the high bits once per tile, and
 // only the terms spanning both are evaluated per element.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
 
 #include "device_util.cuh"
 #include "flipchain.cuh"
@@ -178,6 +185,246 @@ int log2_int(int v) {
   return r;
 }
 
+// ---------------------------------------------------------------------------
+// Multi-pass action for chains whose vectors exceed the L2 (TMA-staged boxes)
+// ---------------------------------------------------------------------------
+//
+// Pass A applies the diagonal and the flips of the low TB bits to contiguous
+// boxes of 2^TB elements and writes the whole epilogue
+//   out = alpha (D x + sum_{i < TB} c_i x[s ^ 2^i]) + beta x + gamma p + kappa q.
+// Each later pass takes a group of G higher bits [b0, b0 + G): a box holds the
+// 2^G elements that differ only in those bits, for a 64-byte run of the lowest
+// bits and a batch of the bits above the run, so every flip of the group is a
+// read of the box in shared memory; it adds alpha sum_{i in group} c_i x[s ^ 2^i]
+// to out. Boxes come in by TMA (cp.async.bulk for pass A, cp.async.bulk.tensor
+// for the strided group boxes) into two shared-memory stages, so the next box
+// loads while the current one is used. Every wait on a stage's mbarrier is
+// bounded: on time-out the block records the failure in `status` and stops.
+
+constexpr int kPassThreads = 512;
+constexpr int kBoxBytes = 32 * 1024;
+constexpr int kStages = 2;
+constexpr unsigned kWaitPolls = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait for the phase `parity` of a stage barrier; false on time-out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (unsigned polls = 0; polls < kWaitPolls; ++polls)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tensor_load5(void* dst, const CUtensorMap* map, int c1, int c4, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(c1), "r"(0), "r"(0), "r"(c4), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// One pass of the multi-pass action. GROUP = false: pass A over contiguous
+// boxes; GROUP = true: the group [b0, b0 + G) from tensor-map boxes.
+struct PassArgs {
+  int sites, b0, G, bb;  // group pass: box = run (R bits) x batch (bb bits) x group (G bits)
+  int nd;
+  const uint64_t* masks;
+  const double* coefs;
+  const void* low_table;
+  const double* xcoef;
+  const void* x;
+  void* out;
+  const void* p;
+  const void* q;
+  double alpha, beta, gamma, kr, ki;
+  int* status;
+};
+
+template <typename T, bool CPLX, int TB, int R, bool GROUP>
+__global__ void __launch_bounds__(kPassThreads) flip_pass_kernel(const __grid_constant__ CUtensorMap map,
+                                                                 const PassArgs a) {
+  using E = typename Elem<T, CPLX>::type;
+  constexpr int kBox = 1 << TB;
+  constexpr int kPer = kBox / kPassThreads;
+  static_assert(kBox % kPassThreads == 0, "box elements must divide among the threads");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  E* stage_buf = reinterpret_cast<E*>(smem_raw);
+  __shared__ __align__(8) uint64_t full[kStages];
+  __shared__ T cx[64];
+  __shared__ uint64_t cross_mask[kMaxDiagTerms];
+  __shared__ T cross_coef[kMaxDiagTerms];
+  __shared__ int n_cross;
+  __shared__ T d_high;
+  __shared__ int abort_flag;
+  __shared__ unsigned long long failed_box;
+  const int L = a.sites;
+  if (threadIdx.x < L) cx[threadIdx.x] = static_cast<T>(a.xcoef[threadIdx.x]);
+  const uint64_t low = (1ull << TB) - 1ull;
+  if (threadIdx.x == 0) {
+    int c = 0;
+    if (!GROUP)
+      for (int k = 0; k < a.nd; ++k)
+        if ((a.masks[k] & low) != 0 && (a.masks[k] & ~low) != 0) {
+          cross_mask[c] = a.masks[k];
+          cross_coef[c] = static_cast<T>(a.coefs[k]);
+          ++c;
+        }
+    n_cross = c;
+    abort_flag = 0;
+    for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const uint64_t boxes = 1ull << (L - TB);
+  const uint64_t mine = boxes > blockIdx.x ? (boxes - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const E* x = static_cast<const E*>(a.x);
+  // global index of box position 0 and the box's load coordinates
+  const int batch_shift = GROUP ? a.b0 - R - a.bb : 0;  // bits of the batch coordinate above the box's batch
+  auto box_id = [&](uint64_t k) { return blockIdx.x + k * gridDim.x; };
+  auto issue = [&](uint64_t k) {
+    const uint64_t id = box_id(k);
+    E* dst = stage_buf + static_cast<size_t>(k % kStages) * kBox;
+    mbar_expect_tx(&full[k % kStages], kBox * static_cast<uint32_t>(sizeof(E)));
+    if (GROUP) {
+      // id = batch block (low b0 - R - bb bits) | above-group index
+      const uint64_t blk = id & ((1ull << batch_shift) - 1);
+      const uint64_t above = id >> batch_shift;
+      tensor_load5(dst, &map, static_cast<int>(blk << a.bb), static_cast<int>(above), &full[k % kStages]);
+    } else {
+      bulk_load(dst, x + (id << TB), kBox * static_cast<uint32_t>(sizeof(E)), &full[k % kStages]);
+    }
+  };
+  if (threadIdx.x == 0)
+    for (uint64_t k = 0; k < mine && k < static_cast<uint64_t>(kStages); ++k) issue(k);
+  const T alpha = static_cast<T>(a.alpha), beta = static_cast<T>(a.beta), gamma = static_cast<T>(a.gamma);
+  const T kr = static_cast<T>(a.kr), ki = static_cast<T>(a.ki);
+  E* out = static_cast<E*>(a.out);
+  const E* pv = static_cast<const E*>(a.p);
+  const E* qv = static_cast<const E*>(a.q);
+  const T* low_table = static_cast<const T*>(a.low_table);
+  for (uint64_t k = 0; k < mine; ++k) {
+    const uint64_t id = box_id(k);
+    E* box = stage_buf + static_cast<size_t>(k % kStages) * kBox;
+    if (!GROUP && threadIdx.x == 0) {
+      double d = 0.0;
+      const uint64_t base = id << TB;
+      for (int t = 0; t < a.nd; ++t)
+        if (a.masks[t] != 0 && (a.masks[t] & low) == 0) d += (__popcll(~base & a.masks[t]) & 1) ? -a.coefs[t] : a.coefs[t];
+      d_high = static_cast<T>(d);
+    }
+    if (threadIdx.x == 0 && !mbar_wait(&full[k % kStages], static_cast<uint32_t>((k / kStages) & 1))) {
+      atomicExch(a.status, 1);
+      abort_flag = 1;
+      failed_box = k;
+    }
+    __syncthreads();
+    if (abort_flag) break;
+    if (GROUP) {
+      const uint64_t blk = id & ((1ull << batch_shift) - 1);
+      const uint64_t above = id >> batch_shift;
+      const uint64_t base = (blk << (a.bb + R)) | (above << (a.b0 + a.G));
+      const int pos_shift = R + a.bb;  // box position bit of group bit 0
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int e = threadIdx.x + u * kPassThreads;
+        const int lowpart = e & ((1 << pos_shift) - 1);
+        const uint64_t g = static_cast<uint64_t>(e >> pos_shift);
+        const uint64_t s = base | static_cast<uint64_t>(lowpart) | (g << a.b0);
+        E acc = zero_elem<E>();
+        for (int i = 0; i < a.G; ++i) acc = scale_add(acc, cx[a.b0 + i], box[e ^ (1 << (pos_shift + i))]);
+        out[s] = add(out[s], scaled(alpha, acc));
+      }
+    } else {
+      const uint64_t base = id << TB;
+      const T dh = d_high;
+      const int nc = n_cross;
+#pragma unroll 2
+      for (int u = 0; u < kPer; ++u) {
+        const int j = threadIdx.x + u * kPassThreads;
+        const uint64_t s = base + j;
+        T d = dh + __ldg(low_table + j);
+        for (int c = 0; c < nc; ++c) d += (__popcll(~s & cross_mask[c]) & 1) ? -cross_coef[c] : cross_coef[c];
+        const E xs = box[j];
+        E acc = scaled(d, xs);
+#pragma unroll
+        for (int i = 0; i < TB; ++i) acc = scale_add(acc, cx[i], box[j ^ (1 << i)]);
+        out[s] = epilogue(acc, xs, pv, qv, s, alpha, beta, gamma, kr, ki);
+      }
+    }
+    __syncthreads();  // every thread is done with this stage
+    if (threadIdx.x == 0 && k + kStages < mine) issue(k + kStages);
+  }
+  // after a time-out, wait (bounded) for the copies still in flight (the box
+  // that timed out and the one issued after it) before leaving
+  if (threadIdx.x == 0 && abort_flag)
+    for (uint64_t k = failed_box; k < mine && k < failed_box + kStages; ++k)
+      mbar_wait(&full[k % kStages], static_cast<uint32_t>((k / kStages) & 1));
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  if (!fn) raise(QMBED_CUDA_ERROR, "cuTensorMapEncodeTiled is not available");
+  return fn;
+}
+
+// Tensor map of the group boxes over x (4-byte units): d0 the 64-byte run
+// (R bits), d1 the bits between the run and the group (box: bb of them),
+// d2 / d3 the group's bits (at most 8 per dimension), d4 the bits above.
+CUtensorMap group_map(const void* x, int sites, int esize, int r, int b0, int G, int bb) {
+  const int g1 = std::min(G, 8), g2 = G - g1;
+  const cuuint64_t dims[5] = {static_cast<cuuint64_t>((esize << r) / 4), 1ull << (b0 - r), 1ull << g1, 1ull << g2,
+                              1ull << (sites - b0 - G)};
+  const cuuint64_t strides[4] = {static_cast<cuuint64_t>(esize) << r, static_cast<cuuint64_t>(esize) << b0,
+                                 static_cast<cuuint64_t>(esize) << (b0 + g1), static_cast<cuuint64_t>(esize) << (b0 + G)};
+  const cuuint32_t box[5] = {static_cast<cuuint32_t>((esize << r) / 4), 1u << bb, 1u << g1, 1u << g2, 1u};
+  const cuuint32_t elem[5] = {1, 1, 1, 1, 1};
+  CUtensorMap map;
+  const CUresult rc = tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 5, const_cast<void*>(x), dims, strides,
+                                           box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (rc != CUDA_SUCCESS) raise(QMBED_CUDA_ERROR, "cuTensorMapEncodeTiled failed with code " + std::to_string(rc));
+  return map;
+}
+
+// Chooses between the one-pass kernel and the multi-pass action: QMBED_FLIP_PASSES=single|multi
+// forces one (tests); otherwise vectors beyond 256 MB take the multi-pass action.
+bool use_multipass(uint64_t n, int esize, int sites, int tb) {
+  if (const char* env = std::getenv("QMBED_FLIP_PASSES")) {
+    if (std::strcmp(env, "single") == 0) return false;
+    if (std::strcmp(env, "multi") == 0) return sites > tb;
+  }
+  return sites > tb && n * static_cast<uint64_t>(esize) >= (256ull << 20);
+}
+
 }  // namespace
 
 FlipChain::FlipChain(const FlipChainDesc& d) : sites_(d.sites), n_diag_(static_cast<int>(d.z_masks.size())) {
@@ -186,6 +433,8 @@ FlipChain::FlipChain(const FlipChainDesc& d) : sites_(d.sites), n_diag_(static_c
   diag_masks_.allocate(std::max(n_diag_, 1) * sizeof(uint64_t));
   diag_coefs_.allocate(std::max(n_diag_, 1) * sizeof(double));
   x_coefs_.allocate(64 * sizeof(double));
+  status_.allocate(sizeof(int));
+  QMBED_CUDA(cudaMemset(status_.get(), 0, sizeof(int)));
   std::vector<double> x(64, 0.0);
   for (int i = 0; i < sites_; ++i) x[i] = d.x_coefs[i];
   if (n_diag_ > 0) {
@@ -235,6 +484,10 @@ void FlipChain::apply(int precision, bool cplx, const void* x, void* out, const 
     tables_ready_ |= table_slot;
     table_tb_[table_slot - 1] = tb;
   }
+  if (use_multipass(n, esize, sites_, log2_int(kBoxBytes / esize))) {
+    apply_multipass(precision, cplx, x, out, p, q, step, stream, sms);
+    return;
+  }
   const size_t smem = static_cast<size_t>(esize) << tb;
   const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(n >> tb, 3ull * sms)));
   auto run = [&](auto ttag, auto ctag) {
@@ -255,6 +508,98 @@ void FlipChain::apply(int precision, bool cplx, const void* x, void* out, const 
   };
   if (precision == 64) cplx ? run(double{}, std::true_type{}) : run(double{}, std::false_type{});
   else cplx ? run(float{}, std::true_type{}) : run(float{}, std::false_type{});
+}
+
+}  // namespace qmbed
+
+namespace qmbed {
+
+namespace {
+
+template <typename T, bool C, int TB, int R>
+void run_passes(int sites, const PassArgs& base, int esize, cudaStream_t stream, int sms) {
+  const size_t smem = static_cast<size_t>(kStages) * kBoxBytes;
+  auto pass_a = flip_pass_kernel<T, C, TB, R, false>;
+  auto pass_g = flip_pass_kernel<T, C, TB, R, true>;
+  QMBED_CUDA(cudaFuncSetAttribute(pass_a, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  QMBED_CUDA(cudaFuncSetAttribute(pass_g, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  int per_sm = 1;
+  QMBED_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_a, kPassThreads, smem));
+  const uint64_t boxes = 1ull << (sites - TB);
+  const unsigned grid =
+      static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(boxes, static_cast<uint64_t>(sms) * std::max(per_sm, 1))));
+  CUtensorMap unused{};
+  pass_a<<<grid, kPassThreads, smem, stream>>>(unused, base);
+  QMBED_LAUNCH_CHECK();
+  for (int b0 = TB; b0 < sites;) {
+    const int G = std::min(TB - R, sites - b0);
+    PassArgs g = base;
+    g.b0 = b0;
+    g.G = G;
+    g.bb = TB - R - G;
+    const CUtensorMap map = group_map(base.x, sites, esize, R, b0, G, g.bb);
+    pass_g<<<grid, kPassThreads, smem, stream>>>(map, g);
+    QMBED_LAUNCH_CHECK();
+    b0 += G;
+  }
+}
+
+}  // namespace
+
+void FlipChain::apply_multipass(int precision, bool cplx, const void* x, void* out, const void* p, const void* q,
+                                const FlipStep& step, cudaStream_t stream, int sms) const {
+  if (x == out || (q && q == out)) raise(QMBED_INVALID_OPTIONS, "the flip-chain action cannot write over x or q");
+  const int esize = (precision == 64 ? 8 : 4) * (cplx ? 2 : 1);
+  const int tb = log2_int(kBoxBytes / esize);
+  // the low-bit diagonal table of this box width
+  const size_t need = static_cast<size_t>(esize / (cplx ? 2 : 1)) << tb;
+  const int slot = precision == 64 ? 0 : 1;
+  if (pass_table_bytes_[slot] < need || pass_table_tb_[slot] != tb) {
+    pass_tables_[slot].allocate(need);
+    pass_table_bytes_[slot] = need;
+    pass_table_tb_[slot] = tb;
+    const int blocks = static_cast<int>(std::min<uint64_t>(((1ull << tb) + 255) / 256, 1024));
+    if (precision == 64)
+      diag_low_table_kernel<double><<<blocks, 256, 0, stream>>>(tb, n_diag_, diag_masks_.as<uint64_t>(),
+                                                                diag_coefs_.as<double>(), pass_tables_[slot].as<double>());
+    else
+      diag_low_table_kernel<float><<<blocks, 256, 0, stream>>>(tb, n_diag_, diag_masks_.as<uint64_t>(),
+                                                               diag_coefs_.as<double>(), pass_tables_[slot].as<float>());
+    QMBED_LAUNCH_CHECK();
+  }
+  PassArgs a{};
+  a.sites = sites_;
+  a.nd = n_diag_;
+  a.masks = diag_masks_.as<uint64_t>();
+  a.coefs = diag_coefs_.as<double>();
+  a.low_table = pass_tables_[slot].get();
+  a.xcoef = x_coefs_.as<double>();
+  a.x = x;
+  a.out = out;
+  a.p = p;
+  a.q = q;
+  a.alpha = step.alpha;
+  a.beta = step.beta;
+  a.gamma = step.gamma;
+  a.kr = step.kappa_re;
+  a.ki = step.kappa_im;
+  a.status = status_.as<int>();
+  if (precision == 64) {
+    if (cplx) run_passes<double, true, 11, 2>(sites_, a, esize, stream, sms);
+    else run_passes<double, false, 12, 3>(sites_, a, esize, stream, sms);
+  } else {
+    if (cplx) run_passes<float, true, 12, 3>(sites_, a, esize, stream, sms);
+    else run_passes<float, false, 13, 4>(sites_, a, esize, stream, sms);
+  }
+}
+
+void FlipChain::check_status() const {
+  int host = 0;
+  QMBED_CUDA(cudaMemcpy(&host, status_.get(), sizeof(int), cudaMemcpyDeviceToHost));
+  if (host != 0) {
+    QMBED_CUDA(cudaMemset(status_.get(), 0, sizeof(int)));
+    raise(QMBED_CUDA_ERROR, "a flip-chain pass timed out waiting for its tile copy");
+  }
 }
 
 }  // namespace qmbed

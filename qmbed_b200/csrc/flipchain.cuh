@@ -40,6 +40,8 @@ class FlipChain {
              cudaStream_t stream) const;
   // Gershgorin-type bounds: |D| max over the diagonal terms plus sum |x|.
   double norm_bound() const;
+  // Raises when a multi-pass launch recorded a timed-out tile wait (and clears it).
+  void check_status() const;
 
  private:
   int sites_;
@@ -49,6 +51,13 @@ class FlipChain {
   mutable size_t tables_bytes_ = 0;
   mutable int tables_ready_ = 0;  // bit 1: FP64 table, bit 2: FP32 table
   mutable int table_tb_[2] = {0, 0};
+  // multi-pass action (vectors beyond the L2): low-bit tables of its box width, time-out status
+  void apply_multipass(int precision, bool cplx, const void* x, void* out, const void* p, const void* q,
+                       const FlipStep& step, cudaStream_t stream, int sms) const;
+  mutable DeviceBuffer pass_tables_[2];
+  mutable size_t pass_table_bytes_[2] = {0, 0};
+  mutable int pass_table_tb_[2] = {0, 0};
+  DeviceBuffer status_;
   std::vector<double> host_diag_coefs_, host_x_;
 };
 
