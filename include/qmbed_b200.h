@@ -246,8 +246,9 @@ QMBED_API int qmbed_gpu_eigsh(qmbed_operator op, const qmbed_eigsh_options* opti
  * cut at lower + nb * gap when that is below the check's Ritz value (nb = 8 or
  * 16, the block width). upper <= lower and restart_keep = 0 give an empty
  * hint: the solve is that of qmbed_gpu_eigsh and the outputs are still set.
- * restart_keep applies to FP64 thick restarts (the mixed mode's FP32 phase
- * keeps the reference's size). */
+ * restart_keep applies to the plain FP64 thick restart (mode
+ * QMBED_MODE_FP64); the mixed mode keeps the reference's size in both of its
+ * phases. */
 typedef struct {
   double lower;
   double upper;
@@ -333,10 +334,12 @@ QMBED_API int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed
  * its Ritz vector (the reference's acceptance test r <= tol max(|theta|, 1),
  * src/solve/mod.rs:1252-1263, holds for every reported pair, otherwise
  * QMBED_STATUS_NON_CONVERGENCE); e_max[s][p] = the largest Ritz value at
- * convergence (an inner estimate of the top of the spectrum); info (8
+ * convergence (an inner estimate of the top of the spectrum); info (10
  * doubles): first-pass steps of the longest pair, first-pass applications,
  * verification applications, CUDA graph used (1/0), first-pass seconds,
- * total seconds, largest relative residual, Ritz copies merged.
+ * total seconds, largest relative residual, Ritz copies merged, the
+ * autotuned resident blocks per SM of the persistent launch and the fastest
+ * tuning chunk's milliseconds (0 when not tuned).
  * residuals and e_max may be NULL. */
 QMBED_API int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
                                    const double* coefficients, int eigenpairs, double tolerance, int max_steps,

@@ -33,6 +33,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <limits>
 
 #include "batched.cuh"
 
@@ -789,6 +790,8 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
   ScanResult result;
   ScanState* host_state = nullptr;
   QMBED_CUDA(cudaMallocHost(&host_state, sizeof(ScanState)));
+  *host_state = ScanState{};
+  host_state->active = 1;  // until the first chunk's copy arrives
   struct PinnedFree {
     ScanState* p;
     ~PinnedFree() { cudaFreeHost(p); }
@@ -811,7 +814,8 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
     };
     const void* k1 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false>);
     const void* k2 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true>);
-    const unsigned grid1 = grid_of(k1), grid2 = grid_of(k2);
+    unsigned grid1 = grid_of(k1), grid2 = grid_of(k2);
+    const int max_per_sm1 = static_cast<int>(grid1 / ops.sms()), max_per_sm2 = static_cast<int>(grid2 / ops.sms());
     const int check_grid = (cols + 127) / 128;
     double* tri = tri_work.as<double>();
     ScanArgs args = a;
@@ -826,6 +830,38 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
       }
       QMBED_CUDA(cudaMemcpyAsync(host_state, state.get(), sizeof(ScanState), cudaMemcpyDeviceToHost, stream));
     };
+    // Autotuner: the persistent launch's resident blocks per SM. More blocks
+    // hide more gather latency, fewer make every grid barrier cheaper; the
+    // first chunks of pass 1 (real work, all pairs active) run once per
+    // candidate under CUDA events and the fastest shape is captured below
+    // and kept for pass 2.
+    result.tuned_blocks_per_sm = max_per_sm1;
+    if (max_per_sm1 > 1 && rows >= (1ull << 16) && max_steps >= 6 * kChunkSteps) {
+      cudaEvent_t e0, e1;
+      QMBED_CUDA(cudaEventCreate(&e0));
+      QMBED_CUDA(cudaEventCreate(&e1));
+      double best = std::numeric_limits<double>::infinity();
+      for (int per_sm = max_per_sm1; per_sm >= 1 && per_sm > max_per_sm1 - 4; --per_sm) {
+        grid1 = static_cast<unsigned>(per_sm * ops.sms());
+        QMBED_CUDA(cudaEventRecord(e0, stream));
+        chunk(false);
+        QMBED_CUDA(cudaEventRecord(e1, stream));
+        QMBED_CUDA(cudaStreamSynchronize(stream));
+        float ms = 0.0f;
+        QMBED_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        result.tuning_ms.push_back(ms);
+        if (ms < best) {
+          best = ms;
+          result.tuned_blocks_per_sm = per_sm;
+        }
+        if (host_state->status == kStatusBarrierTimeout || host_state->active == 0 || host_state->step >= max_steps)
+          break;
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      grid1 = static_cast<unsigned>(result.tuned_blocks_per_sm * ops.sms());
+      grid2 = static_cast<unsigned>(std::min(result.tuned_blocks_per_sm, max_per_sm2) * ops.sms());
+    }
     // Pass 1: one chunk captured in a graph, replayed until every pair stopped.
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -850,6 +886,9 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
     result.graph = graph_ok;
     const int max_chunks = (max_steps + kChunkSteps - 1) / kChunkSteps + 1;
     for (int c = 0; c < max_chunks; ++c) {
+      if (host_state->status == kStatusBarrierTimeout || host_state->active == 0 ||
+          host_state->step >= max_steps)
+        break;  // the tuning chunks may already have finished
       if (exec) QMBED_CUDA(cudaGraphLaunch(exec, stream));
       else chunk(false);
       QMBED_CUDA(cudaStreamSynchronize(stream));

@@ -4,6 +4,7 @@
 // entry point converts failures into a status code (typed API) or an error
 // response (JSON API), like the reference's catch_unwind wrappers
 // (lib.rs:6090-6104).
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -2320,6 +2321,8 @@ int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_operator* 
       info[5] = r.seconds;
       info[6] = r.max_relative_residual;
       info[7] = static_cast<double>(r.merged_copies);
+      info[8] = static_cast<double>(r.tuned_blocks_per_sm);
+      info[9] = r.tuning_ms.empty() ? 0.0 : *std::min_element(r.tuning_ms.begin(), r.tuning_ms.end());
     }
   });
 }
@@ -2327,7 +2330,7 @@ int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_operator* 
 int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
                           const double* coefficients, int eigenpairs, double tolerance, int max_steps, uint64_t seed,
                           double* eigenvalues, int* steps, double* info) {
-  double full[8] = {0};
+  double full[10] = {0};
   const int rc = qmbed_gpu_scan_solve(n_sectors, n_components, components, n_points, coefficients, eigenpairs,
                                       tolerance, max_steps, seed, eigenvalues, nullptr, nullptr, steps, full);
   if (rc == QMBED_STATUS_OK && info) {

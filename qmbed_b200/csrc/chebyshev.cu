@@ -148,6 +148,7 @@ void chebyshev_run(const SpinOperator& op, const double* initial, cudaMemcpyKind
     emit(t);
   }
   ops.sync();
+  fc->check_status();  // a multi-pass box wait that timed out
 }
 
 }  // namespace

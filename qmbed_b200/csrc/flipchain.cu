@@ -203,7 +203,7 @@ int log2_int(int v) {
 
 constexpr int kPassThreads = 512;
 constexpr int kBoxBytes = 32 * 1024;
-constexpr int kStages = 2;
+constexpr int kStages = 3;
 constexpr unsigned kWaitPolls = 1u << 22;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -323,15 +323,44 @@ __global__ void __launch_bounds__(kPassThreads) flip_pass_kernel(const __grid_co
   const E* pv = static_cast<const E*>(a.p);
   const E* qv = static_cast<const E*>(a.q);
   const T* low_table = static_cast<const T*>(a.low_table);
+  const int pos_shift = R + a.bb;  // group pass: box position bit of group bit 0
   for (uint64_t k = 0; k < mine; ++k) {
     const uint64_t id = box_id(k);
     E* box = stage_buf + static_cast<size_t>(k % kStages) * kBox;
-    if (!GROUP && threadIdx.x == 0) {
-      double d = 0.0;
+    // Global index of each of this thread's elements, and the operands that
+    // come from global memory, loaded before the wait on the box so that
+    // their latency overlaps the copy.
+    uint64_t sidx[kPer];
+    E pre0[kPer], pre1[kPer];
+    T lowv[kPer];
+    if (GROUP) {
+      const uint64_t blk = id & ((1ull << batch_shift) - 1);
+      const uint64_t above = id >> batch_shift;
+      const uint64_t base = (blk << (a.bb + R)) | (above << (a.b0 + a.G));
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int e = threadIdx.x + u * kPassThreads;
+        sidx[u] = base | static_cast<uint64_t>(e & ((1 << pos_shift) - 1)) |
+                  (static_cast<uint64_t>(e >> pos_shift) << a.b0);
+        pre0[u] = out[sidx[u]];
+      }
+    } else {
       const uint64_t base = id << TB;
-      for (int t = 0; t < a.nd; ++t)
-        if (a.masks[t] != 0 && (a.masks[t] & low) == 0) d += (__popcll(~base & a.masks[t]) & 1) ? -a.coefs[t] : a.coefs[t];
-      d_high = static_cast<T>(d);
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int j = threadIdx.x + u * kPassThreads;
+        sidx[u] = base + j;
+        lowv[u] = __ldg(low_table + j);
+        pre0[u] = pv ? pv[sidx[u]] : zero_elem<E>();
+        pre1[u] = qv ? qv[sidx[u]] : zero_elem<E>();
+      }
+      if (threadIdx.x == 0) {
+        double d = 0.0;
+        for (int t = 0; t < a.nd; ++t)
+          if (a.masks[t] != 0 && (a.masks[t] & low) == 0)
+            d += (__popcll(~base & a.masks[t]) & 1) ? -a.coefs[t] : a.coefs[t];
+        d_high = static_cast<T>(d);
+      }
     }
     if (threadIdx.x == 0 && !mbar_wait(&full[k % kStages], static_cast<uint32_t>((k / kStages) & 1))) {
       atomicExch(a.status, 1);
@@ -341,38 +370,33 @@ __global__ void __launch_bounds__(kPassThreads) flip_pass_kernel(const __grid_co
     __syncthreads();
     if (abort_flag) break;
     if (GROUP) {
-      const uint64_t blk = id & ((1ull << batch_shift) - 1);
-      const uint64_t above = id >> batch_shift;
-      const uint64_t base = (blk << (a.bb + R)) | (above << (a.b0 + a.G));
-      const int pos_shift = R + a.bb;  // box position bit of group bit 0
 #pragma unroll
       for (int u = 0; u < kPer; ++u) {
         const int e = threadIdx.x + u * kPassThreads;
-        const int lowpart = e & ((1 << pos_shift) - 1);
-        const uint64_t g = static_cast<uint64_t>(e >> pos_shift);
-        const uint64_t s = base | static_cast<uint64_t>(lowpart) | (g << a.b0);
         E acc = zero_elem<E>();
         for (int i = 0; i < a.G; ++i) acc = scale_add(acc, cx[a.b0 + i], box[e ^ (1 << (pos_shift + i))]);
-        out[s] = add(out[s], scaled(alpha, acc));
+        out[sidx[u]] = add(pre0[u], scaled(alpha, acc));
       }
     } else {
-      const uint64_t base = id << TB;
       const T dh = d_high;
       const int nc = n_cross;
-#pragma unroll 2
+#pragma unroll
       for (int u = 0; u < kPer; ++u) {
         const int j = threadIdx.x + u * kPassThreads;
-        const uint64_t s = base + j;
-        T d = dh + __ldg(low_table + j);
+        const uint64_t s = sidx[u];
+        T d = dh + lowv[u];
         for (int c = 0; c < nc; ++c) d += (__popcll(~s & cross_mask[c]) & 1) ? -cross_coef[c] : cross_coef[c];
         const E xs = box[j];
         E acc = scaled(d, xs);
 #pragma unroll
         for (int i = 0; i < TB; ++i) acc = scale_add(acc, cx[i], box[j ^ (1 << i)]);
-        out[s] = epilogue(acc, xs, pv, qv, s, alpha, beta, gamma, kr, ki);
+        E o = add(scaled(alpha, acc), scaled(beta, xs));
+        if (pv) o = add(o, scaled(gamma, pre0[u]));
+        if (qv) o = add(o, kappa_times(kr, ki, pre1[u]));
+        out[s] = o;
       }
     }
-    __syncthreads();  // every thread is done with this stage
+    __syncthreads();  // every thread is done with this stage (and with d_high)
     if (threadIdx.x == 0 && k + kStages < mine) issue(k + kStages);
   }
   // after a time-out, wait (bounded) for the copies still in flight (the box

@@ -6,8 +6,8 @@ point of J1-J2 / XXZ chains at 12-20 sites: the lowest eigenvalue, the
 largest Ritz value and the gap. Its prediction for a held-out 28-site XXZ
 sector becomes an eigsh hint. The filtered solver must accept the interval
 after its short Lanczos check and spend fewer operator applications on
-bounds than without the network; the thick restart takes the predicted
-restart size. Eigenvalues must agree with the un-hinted solves within 1e-10
+bounds than without the network; the plain thick restart takes the
+predicted restart size and needs fewer operator applications. Eigenvalues must agree with the un-hinted solves within 1e-10
 relative, every residual verified. A hint that contradicts the check is
 rejected and the solver falls back to its own bounds.
 """
@@ -66,12 +66,16 @@ def test_learned_hint_cuts_bound_applications_with_identical_eigenvalues(trained
     assert np.all(hinted.residuals <= 1e-10 * np.maximum(np.abs(hinted.eigenvalues), 1.0))
 
 
-def test_learned_restart_size_in_the_thick_restart(trained, xxz28):
+def test_learned_restart_size_cuts_thick_restart_steps(trained, xxz28):
+    """The plain FP64 thick restart (Krylov 40) with the predicted restart size
+    against the reference's size: fewer operator applications, the same
+    eigenvalues within 1e-10, every residual verified."""
     model = trained[0]
     hint = model.hint(SITES, 0.0, DELTA, 0, eigenpairs=6)
-    assert 6 <= hint["restart_keep"] <= 20
-    base = xxz28.eigsh(6, krylov_dimension=40, tolerance=1e-10, seed=0, mode="mixed")
-    hinted = xxz28.eigsh(6, krylov_dimension=40, tolerance=1e-10, seed=0, mode="mixed", hint=hint)
+    assert hint["restart_keep"] == 8  # small relative gap: the wanted pairs and two more
+    base = xxz28.eigsh(6, krylov_dimension=40, tolerance=1e-10, seed=0, mode="fp64")
+    hinted = xxz28.eigsh(6, krylov_dimension=40, tolerance=1e-10, seed=0, mode="fp64", hint=hint)
+    assert hinted.operator_applications < base.operator_applications
     assert np.max(np.abs(hinted.eigenvalues - base.eigenvalues) / np.abs(base.eigenvalues)) <= 1e-10
     assert np.all(hinted.residuals <= 1e-10 * np.maximum(np.abs(hinted.eigenvalues), 1.0))
 
