@@ -102,6 +102,22 @@ __global__ void diag_low_table_kernel(int tb, int nd, const uint64_t* __restrict
   }
 }
 
+// D_high[t] = sum over terms with mask inside the bits >= tb of c (-1)^popcount(~(t << tb) & mask)
+template <typename T>
+__global__ void diag_high_table_kernel(int tb, int sites, int nd, const uint64_t* __restrict__ masks,
+                                       const double* __restrict__ coefs, T* __restrict__ table) {
+  const uint64_t low = (1ull << tb) - 1ull;
+  const uint64_t count = 1ull << (sites - tb);
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < count;
+       t += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t base = t << tb;
+    double d = 0.0;
+    for (int k = 0; k < nd; ++k)
+      if (masks[k] != 0 && (masks[k] & low) == 0) d += (__popcll(~base & masks[k]) & 1) ? -coefs[k] : coefs[k];
+    table[t] = static_cast<T>(d);
+  }
+}
+
 // One pass: tile flips, global-partner flips, diagonal and the epilogue.
 // TB > 0 fixes the tile bits at compile time (the tile loop unrolls); TB = 0
 // takes them from `tb` (chains shorter than a tile).
@@ -252,6 +268,7 @@ struct PassArgs {
   const uint64_t* masks;
   const double* coefs;
   const void* low_table;
+  const void* high_table;  // pass A: the diagonal part of the bits above the box, per box
   const double* xcoef;
   const void* x;
   void* out;
@@ -262,7 +279,7 @@ struct PassArgs {
 };
 
 template <typename T, bool CPLX, int TB, int R, bool GROUP>
-__global__ void __launch_bounds__(kPassThreads) flip_pass_kernel(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid_constant__ CUtensorMap map,
                                                                  const PassArgs a) {
   using E = typename Elem<T, CPLX>::type;
   constexpr int kBox = 1 << TB;
@@ -354,13 +371,7 @@ __global__ void __launch_bounds__(kPassThreads) flip_pass_kernel(const __grid_co
         pre0[u] = pv ? pv[sidx[u]] : zero_elem<E>();
         pre1[u] = qv ? qv[sidx[u]] : zero_elem<E>();
       }
-      if (threadIdx.x == 0) {
-        double d = 0.0;
-        for (int t = 0; t < a.nd; ++t)
-          if (a.masks[t] != 0 && (a.masks[t] & low) == 0)
-            d += (__popcll(~base & a.masks[t]) & 1) ? -a.coefs[t] : a.coefs[t];
-        d_high = static_cast<T>(d);
-      }
+      if (threadIdx.x == 0) d_high = static_cast<const T*>(a.high_table)[id];
     }
     if (threadIdx.x == 0 && !mbar_wait(&full[k % kStages], static_cast<uint32_t>((k / kStages) & 1))) {
       atomicExch(a.status, 1);
@@ -374,7 +385,9 @@ __global__ void __launch_bounds__(kPassThreads) flip_pass_kernel(const __grid_co
       for (int u = 0; u < kPer; ++u) {
         const int e = threadIdx.x + u * kPassThreads;
         E acc = zero_elem<E>();
-        for (int i = 0; i < a.G; ++i) acc = scale_add(acc, cx[a.b0 + i], box[e ^ (1 << (pos_shift + i))]);
+#pragma unroll
+        for (int i = 0; i < TB - R; ++i)
+          if (i < a.G) acc = scale_add(acc, cx[a.b0 + i], box[e ^ (1 << (pos_shift + i))]);
         out[sidx[u]] = add(pre0[u], scaled(alpha, acc));
       }
     } else {
@@ -578,17 +591,27 @@ void FlipChain::apply_multipass(int precision, bool cplx, const void* x, void* o
   // the low-bit diagonal table of this box width
   const size_t need = static_cast<size_t>(esize / (cplx ? 2 : 1)) << tb;
   const int slot = precision == 64 ? 0 : 1;
+  const size_t high_need = static_cast<size_t>(esize / (cplx ? 2 : 1)) << (sites_ - tb);
   if (pass_table_bytes_[slot] < need || pass_table_tb_[slot] != tb) {
     pass_tables_[slot].allocate(need);
+    pass_high_tables_[slot].allocate(high_need);
     pass_table_bytes_[slot] = need;
     pass_table_tb_[slot] = tb;
     const int blocks = static_cast<int>(std::min<uint64_t>(((1ull << tb) + 255) / 256, 1024));
-    if (precision == 64)
+    const int hblocks = static_cast<int>(std::min<uint64_t>(((1ull << (sites_ - tb)) + 255) / 256, 4096));
+    if (precision == 64) {
       diag_low_table_kernel<double><<<blocks, 256, 0, stream>>>(tb, n_diag_, diag_masks_.as<uint64_t>(),
                                                                 diag_coefs_.as<double>(), pass_tables_[slot].as<double>());
-    else
+      diag_high_table_kernel<double><<<hblocks, 256, 0, stream>>>(tb, sites_, n_diag_, diag_masks_.as<uint64_t>(),
+                                                                  diag_coefs_.as<double>(),
+                                                                  pass_high_tables_[slot].as<double>());
+    } else {
       diag_low_table_kernel<float><<<blocks, 256, 0, stream>>>(tb, n_diag_, diag_masks_.as<uint64_t>(),
                                                                diag_coefs_.as<double>(), pass_tables_[slot].as<float>());
+      diag_high_table_kernel<float><<<hblocks, 256, 0, stream>>>(tb, sites_, n_diag_, diag_masks_.as<uint64_t>(),
+                                                                 diag_coefs_.as<double>(),
+                                                                 pass_high_tables_[slot].as<float>());
+    }
     QMBED_LAUNCH_CHECK();
   }
   PassArgs a{};
@@ -597,6 +620,7 @@ void FlipChain::apply_multipass(int precision, bool cplx, const void* x, void* o
   a.masks = diag_masks_.as<uint64_t>();
   a.coefs = diag_coefs_.as<double>();
   a.low_table = pass_tables_[slot].get();
+  a.high_table = pass_high_tables_[slot].get();
   a.xcoef = x_coefs_.as<double>();
   a.x = x;
   a.out = out;

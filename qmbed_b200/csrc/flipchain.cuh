@@ -54,7 +54,7 @@ class FlipChain {
   // multi-pass action (vectors beyond the L2): low-bit tables of its box width, time-out status
   void apply_multipass(int precision, bool cplx, const void* x, void* out, const void* p, const void* q,
                        const FlipStep& step, cudaStream_t stream, int sms) const;
-  mutable DeviceBuffer pass_tables_[2];
+  mutable DeviceBuffer pass_tables_[2], pass_high_tables_[2];
   mutable size_t pass_table_bytes_[2] = {0, 0};
   mutable int pass_table_tb_[2] = {0, 0};
   DeviceBuffer status_;
