@@ -341,6 +341,11 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
   const E* qv = static_cast<const E*>(a.q);
   const T* low_table = static_cast<const T*>(a.low_table);
   const int pos_shift = R + a.bb;  // group pass: box position bit of group bit 0
+  // flip coefficients of this pass in registers (TB low bits, or the group's bits)
+  constexpr int kFlips = GROUP ? TB - R : TB;
+  T coef[kFlips];
+#pragma unroll
+  for (int i = 0; i < kFlips; ++i) coef[i] = GROUP ? (i < a.G ? cx[a.b0 + i] : static_cast<T>(0)) : cx[i];
   for (uint64_t k = 0; k < mine; ++k) {
     const uint64_t id = box_id(k);
     E* box = stage_buf + static_cast<size_t>(k % kStages) * kBox;
@@ -386,8 +391,8 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
         const int e = threadIdx.x + u * kPassThreads;
         E acc = zero_elem<E>();
 #pragma unroll
-        for (int i = 0; i < TB - R; ++i)
-          if (i < a.G) acc = scale_add(acc, cx[a.b0 + i], box[e ^ (1 << (pos_shift + i))]);
+        for (int i = 0; i < kFlips; ++i)
+          if (i < a.G) acc = scale_add(acc, coef[i], box[e ^ (1 << (pos_shift + i))]);
         out[sidx[u]] = add(pre0[u], scaled(alpha, acc));
       }
     } else {
@@ -402,7 +407,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
         const E xs = box[j];
         E acc = scaled(d, xs);
 #pragma unroll
-        for (int i = 0; i < TB; ++i) acc = scale_add(acc, cx[i], box[j ^ (1 << i)]);
+        for (int i = 0; i < kFlips; ++i) acc = scale_add(acc, coef[i], box[j ^ (1 << i)]);
         E o = add(scaled(alpha, acc), scaled(beta, xs));
         if (pv) o = add(o, scaled(gamma, pre0[u]));
         if (qv) o = add(o, kappa_times(kr, ki, pre1[u]));
