@@ -73,3 +73,18 @@ def test_chebyshev_propagation_multipass_equals_one_pass(precision, tol, monkeyp
     multi, info = op.chebyshev_evolve(psi0, times, precision=precision)
     assert info["applications"] > 0
     assert np.max(np.linalg.norm(multi - one, axis=1)) <= tol
+
+
+def test_unaligned_vectors_take_the_one_pass_kernel(monkeypatch):
+    """Views that do not start on a 32-byte boundary cannot use the 32-byte
+    chunks and TMA boxes; the action falls back to the one-pass kernel."""
+    import torch
+    op, _ = _operator(16, seed=2)
+    n = op.dim
+    storage = torch.randn(2 * n + 2, dtype=torch.float32, device="cuda",
+                          generator=torch.Generator(device="cuda").manual_seed(9))
+    x = storage[2:]  # one complex64 element (8 bytes) past the allocation
+    assert x.data_ptr() % 32 != 0
+    ref = _apply(op, x.clone(), 32, True, "single", monkeypatch)
+    got = _apply(op, x, 32, True, "multi", monkeypatch)
+    assert float(torch.linalg.vector_norm(got - ref)) <= 2e-6 * float(torch.linalg.vector_norm(ref))
