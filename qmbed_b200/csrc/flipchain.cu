@@ -295,6 +295,20 @@ __device__ __forceinline__ Chunk<E> load_chunk(const E* p) {
   c.q[1] = q[1];
   return c;
 }
+// Shared-memory form: a 16-byte load serves 8 lanes per wavefront, and lanes
+// 32 bytes apart would meet in the same banks; lanes whose bit 2 is set take
+// their second half first, so every quarter-warp covers all 32 banks for any
+// partner distance.
+template <typename E>
+__device__ __forceinline__ Chunk<E> load_chunk_shared(const E* p) {
+  Chunk<E> c;
+  const float4* q = reinterpret_cast<const float4*>(p);
+  const int sw = (threadIdx.x >> 2) & 1;
+  const float4 first = q[sw], second = q[sw ^ 1];
+  c.q[0] = sw ? second : first;
+  c.q[1] = sw ? first : second;
+  return c;
+}
 template <typename E>
 __device__ __forceinline__ void store_chunk(E* p, const Chunk<E>& c) {
   float4* q = reinterpret_cast<float4*>(p);
@@ -420,7 +434,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
 #pragma unroll
         for (int i = 0; i < kFlips; ++i) {
           if (i >= a.G) break;
-          const Chunk<E> y = load_chunk(box + static_cast<size_t>(c ^ (1 << (pos_shift - LV + i))) * V);
+          const Chunk<E> y = load_chunk_shared(box + static_cast<size_t>(c ^ (1 << (pos_shift - LV + i))) * V);
 #pragma unroll
           for (int v = 0; v < V; ++v) acc[v] = scale_add(acc[v], coef[i], y.e[v]);
         }
@@ -435,7 +449,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
 #pragma unroll
       for (int u = 0; u < kPerC; ++u) {
         const int c = threadIdx.x + u * kPassThreads;
-        const Chunk<E> xs = load_chunk(box + static_cast<size_t>(c) * V);
+        const Chunk<E> xs = load_chunk_shared(box + static_cast<size_t>(c) * V);
         E acc[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
@@ -450,7 +464,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
           for (int v = 0; v < V; ++v) acc[v] = scale_add(acc[v], coef[i], xs.e[v ^ (1 << i)]);
 #pragma unroll
         for (int i = LV; i < TB; ++i) {
-          const Chunk<E> y = load_chunk(box + static_cast<size_t>(c ^ (1 << (i - LV))) * V);
+          const Chunk<E> y = load_chunk_shared(box + static_cast<size_t>(c ^ (1 << (i - LV))) * V);
 #pragma unroll
           for (int v = 0; v < V; ++v) acc[v] = scale_add(acc[v], coef[i], y.e[v]);
         }
