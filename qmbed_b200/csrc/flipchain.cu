@@ -278,57 +278,13 @@ struct PassArgs {
   int* status;
 };
 
-// 32 bytes of consecutive elements: loaded and stored as two 16-byte words.
-template <typename E>
-struct Chunk {
-  static constexpr int V = 32 / static_cast<int>(sizeof(E));
-  union {
-    E e[V];
-    float4 q[2];
-  };
-};
-template <typename E>
-__device__ __forceinline__ Chunk<E> load_chunk(const E* p) {
-  Chunk<E> c;
-  const float4* q = reinterpret_cast<const float4*>(p);
-  c.q[0] = q[0];
-  c.q[1] = q[1];
-  return c;
-}
-// Shared-memory form: a 16-byte load serves 8 lanes per wavefront, and lanes
-// 32 bytes apart would meet in the same banks; lanes whose bit 2 is set take
-// their second half first, so every quarter-warp covers all 32 banks for any
-// partner distance.
-template <typename E>
-__device__ __forceinline__ Chunk<E> load_chunk_shared(const E* p) {
-  Chunk<E> c;
-  const float4* q = reinterpret_cast<const float4*>(p);
-  const int sw = (threadIdx.x >> 2) & 1;
-  const float4 first = q[sw], second = q[sw ^ 1];
-  c.q[0] = sw ? second : first;
-  c.q[1] = sw ? first : second;
-  return c;
-}
-template <typename E>
-__device__ __forceinline__ void store_chunk(E* p, const Chunk<E>& c) {
-  float4* q = reinterpret_cast<float4*>(p);
-  q[0] = c.q[0];
-  q[1] = c.q[1];
-}
-
-// Each thread owns chunks of V = 32 / sizeof(E) consecutive elements (two
-// per box): the flips of the lowest log2(V) bits stay in registers, and every
-// other flip reads its partner chunk with two 16-byte shared-memory loads.
 template <typename T, bool CPLX, int TB, int R, bool GROUP>
 __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid_constant__ CUtensorMap map,
-                                                                    const PassArgs a) {
+                                                                 const PassArgs a) {
   using E = typename Elem<T, CPLX>::type;
   constexpr int kBox = 1 << TB;
-  constexpr int V = Chunk<E>::V;
-  constexpr int LV = V == 8 ? 3 : (V == 4 ? 2 : (V == 2 ? 1 : 0));
-  constexpr int kChunks = kBox / V;
-  constexpr int kPerC = kChunks / kPassThreads;
-  static_assert(kChunks % kPassThreads == 0 && R >= LV, "box chunks must divide among the threads");
+  constexpr int kPer = kBox / kPassThreads;
+  static_assert(kBox % kPassThreads == 0, "box elements must divide among the threads");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   E* stage_buf = reinterpret_cast<E*>(smem_raw);
   __shared__ __align__(8) uint64_t full[kStages];
@@ -360,6 +316,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
   const uint64_t boxes = 1ull << (L - TB);
   const uint64_t mine = boxes > blockIdx.x ? (boxes - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const E* x = static_cast<const E*>(a.x);
+  // global index of box position 0 and the box's load coordinates
   const int batch_shift = GROUP ? a.b0 - R - a.bb : 0;  // bits of the batch coordinate above the box's batch
   auto box_id = [&](uint64_t k) { return blockIdx.x + k * gridDim.x; };
   auto issue = [&](uint64_t k) {
@@ -367,6 +324,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
     E* dst = stage_buf + static_cast<size_t>(k % kStages) * kBox;
     mbar_expect_tx(&full[k % kStages], kBox * static_cast<uint32_t>(sizeof(E)));
     if (GROUP) {
+      // id = batch block (low b0 - R - bb bits) | above-group index
       const uint64_t blk = id & ((1ull << batch_shift) - 1);
       const uint64_t above = id >> batch_shift;
       tensor_load5(dst, &map, static_cast<int>(blk << a.bb), static_cast<int>(above), &full[k % kStages]);
@@ -391,29 +349,32 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
   for (uint64_t k = 0; k < mine; ++k) {
     const uint64_t id = box_id(k);
     E* box = stage_buf + static_cast<size_t>(k % kStages) * kBox;
-    // Global index of each chunk's first element, and the operands that come
-    // from global memory, loaded before the wait on the box so that their
-    // latency overlaps the copy.
-    uint64_t sidx[kPerC];
-    Chunk<E> pre0[kPerC], pre1[kPerC];
+    // Global index of each of this thread's elements, and the operands that
+    // come from global memory, loaded before the wait on the box so that
+    // their latency overlaps the copy.
+    uint64_t sidx[kPer];
+    E pre0[kPer], pre1[kPer];
+    T lowv[kPer];
     if (GROUP) {
       const uint64_t blk = id & ((1ull << batch_shift) - 1);
       const uint64_t above = id >> batch_shift;
       const uint64_t base = (blk << (a.bb + R)) | (above << (a.b0 + a.G));
 #pragma unroll
-      for (int u = 0; u < kPerC; ++u) {
-        const int e = (threadIdx.x + u * kPassThreads) * V;
+      for (int u = 0; u < kPer; ++u) {
+        const int e = threadIdx.x + u * kPassThreads;
         sidx[u] = base | static_cast<uint64_t>(e & ((1 << pos_shift) - 1)) |
                   (static_cast<uint64_t>(e >> pos_shift) << a.b0);
-        pre0[u] = load_chunk(out + sidx[u]);
+        pre0[u] = out[sidx[u]];
       }
     } else {
       const uint64_t base = id << TB;
 #pragma unroll
-      for (int u = 0; u < kPerC; ++u) {
-        sidx[u] = base + static_cast<uint64_t>(threadIdx.x + u * kPassThreads) * V;
-        if (pv) pre0[u] = load_chunk(pv + sidx[u]);
-        if (qv) pre1[u] = load_chunk(qv + sidx[u]);
+      for (int u = 0; u < kPer; ++u) {
+        const int j = threadIdx.x + u * kPassThreads;
+        sidx[u] = base + j;
+        lowv[u] = __ldg(low_table + j);
+        pre0[u] = pv ? pv[sidx[u]] : zero_elem<E>();
+        pre1[u] = qv ? qv[sidx[u]] : zero_elem<E>();
       }
       if (threadIdx.x == 0) d_high = static_cast<const T*>(a.high_table)[id];
     }
@@ -426,57 +387,31 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
     if (abort_flag) break;
     if (GROUP) {
 #pragma unroll
-      for (int u = 0; u < kPerC; ++u) {
-        const int c = threadIdx.x + u * kPassThreads;
-        E acc[V];
+      for (int u = 0; u < kPer; ++u) {
+        const int e = threadIdx.x + u * kPassThreads;
+        E acc = zero_elem<E>();
 #pragma unroll
-        for (int v = 0; v < V; ++v) acc[v] = zero_elem<E>();
-#pragma unroll
-        for (int i = 0; i < kFlips; ++i) {
-          if (i >= a.G) break;
-          const Chunk<E> y = load_chunk_shared(box + static_cast<size_t>(c ^ (1 << (pos_shift - LV + i))) * V);
-#pragma unroll
-          for (int v = 0; v < V; ++v) acc[v] = scale_add(acc[v], coef[i], y.e[v]);
-        }
-        Chunk<E> o;
-#pragma unroll
-        for (int v = 0; v < V; ++v) o.e[v] = add(pre0[u].e[v], scaled(alpha, acc[v]));
-        store_chunk(out + sidx[u], o);
+        for (int i = 0; i < kFlips; ++i)
+          if (i < a.G) acc = scale_add(acc, coef[i], box[e ^ (1 << (pos_shift + i))]);
+        out[sidx[u]] = add(pre0[u], scaled(alpha, acc));
       }
     } else {
       const T dh = d_high;
       const int nc = n_cross;
 #pragma unroll
-      for (int u = 0; u < kPerC; ++u) {
-        const int c = threadIdx.x + u * kPassThreads;
-        const Chunk<E> xs = load_chunk_shared(box + static_cast<size_t>(c) * V);
-        E acc[V];
+      for (int u = 0; u < kPer; ++u) {
+        const int j = threadIdx.x + u * kPassThreads;
+        const uint64_t s = sidx[u];
+        T d = dh + lowv[u];
+        for (int c = 0; c < nc; ++c) d += (__popcll(~s & cross_mask[c]) & 1) ? -cross_coef[c] : cross_coef[c];
+        const E xs = box[j];
+        E acc = scaled(d, xs);
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const uint64_t s = sidx[u] + v;
-          T d = dh + __ldg(low_table + c * V + v);
-          for (int t = 0; t < nc; ++t) d += (__popcll(~s & cross_mask[t]) & 1) ? -cross_coef[t] : cross_coef[t];
-          acc[v] = scaled(d, xs.e[v]);
-        }
-#pragma unroll
-        for (int i = 0; i < LV; ++i)
-#pragma unroll
-          for (int v = 0; v < V; ++v) acc[v] = scale_add(acc[v], coef[i], xs.e[v ^ (1 << i)]);
-#pragma unroll
-        for (int i = LV; i < TB; ++i) {
-          const Chunk<E> y = load_chunk_shared(box + static_cast<size_t>(c ^ (1 << (i - LV))) * V);
-#pragma unroll
-          for (int v = 0; v < V; ++v) acc[v] = scale_add(acc[v], coef[i], y.e[v]);
-        }
-        Chunk<E> o;
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          E r = add(scaled(alpha, acc[v]), scaled(beta, xs.e[v]));
-          if (pv) r = add(r, scaled(gamma, pre0[u].e[v]));
-          if (qv) r = add(r, kappa_times(kr, ki, pre1[u].e[v]));
-          o.e[v] = r;
-        }
-        store_chunk(out + sidx[u], o);
+        for (int i = 0; i < kFlips; ++i) acc = scale_add(acc, coef[i], box[j ^ (1 << i)]);
+        E o = add(scaled(alpha, acc), scaled(beta, xs));
+        if (pv) o = add(o, scaled(gamma, pre0[u]));
+        if (qv) o = add(o, kappa_times(kr, ki, pre1[u]));
+        out[s] = o;
       }
     }
     __syncthreads();  // every thread is done with this stage (and with d_high)
@@ -591,7 +526,9 @@ void FlipChain::apply(int precision, bool cplx, const void* x, void* out, const 
     tables_ready_ |= table_slot;
     table_tb_[table_slot - 1] = tb;
   }
-  // the passes move 32-byte chunks and TMA boxes: every vector 32-byte aligned
+  // TMA boxes (cp.async.bulk needs 16-byte aligned sources; tensor maps
+  // 16-byte aligned bases): vectors that start elsewhere, such as offset
+  // views, take the one-pass kernel
   auto aligned = [](const void* ptr) { return ptr == nullptr || (reinterpret_cast<uintptr_t>(ptr) & 31) == 0; };
   if (aligned(x) && aligned(out) && aligned(p) && aligned(q) &&
       use_multipass(n, esize, sites_, log2_int(kBoxBytes / esize))) {

@@ -76,8 +76,8 @@ def test_chebyshev_propagation_multipass_equals_one_pass(precision, tol, monkeyp
 
 
 def test_unaligned_vectors_take_the_one_pass_kernel(monkeypatch):
-    """Views that do not start on a 32-byte boundary cannot use the 32-byte
-    chunks and TMA boxes; the action falls back to the one-pass kernel."""
+    """Views that do not start on a 32-byte boundary cannot be the source of
+    TMA boxes; the action falls back to the one-pass kernel."""
     import torch
     op, _ = _operator(16, seed=2)
     n = op.dim
