@@ -712,6 +712,19 @@ def main():
                  "eigenvalues": rp.eigenvalues.tolist(),
                  "max_rel_diff_vs_mixed": float(np.max(np.abs(rp.eigenvalues - last.eigenvalues)
                                                        / np.abs(rp.eigenvalues)))}
+        if hint is not None and hint.get("restart_keep", 0) > 0:
+            # the same reference algorithm (Krylov 40 thick restart, FP64) with the
+            # network's restart size
+            barrier()
+            t_start.record()
+            rk = op.eigsh(args.eigenpairs, mode="fp64", hint=hint, **solve_kw)
+            t_stop.record()
+            barrier()
+            plain["with_learned_restart_size"] = {
+                "s": t_start.elapsed_time(t_stop) / 1000.0, "iterations": rk.iterations,
+                "restart_keep": hint["restart_keep"],
+                "max_rel_diff": float(np.max(np.abs(rk.eigenvalues - rp.eigenvalues) / np.abs(rp.eigenvalues))),
+                "max_residual": float(np.max(rk.residuals))}
 
     # --- H.v roofline (FP32 packed SpMV, the operator inside the mixed solve) ---
     stream = torch.cuda.current_stream().cuda_stream
