@@ -122,6 +122,19 @@ def test_two_ranks_match_the_oracle_and_one_rank():
         assert applications == out[0][5]  # every rank applies its slab the same number of times
 
 
+def test_three_ranks_with_a_short_last_slab():
+    """Three ranks on a dimension that does not divide by three: the last slab
+    is shorter, and the gathered layout still puts every row in place."""
+    op, _, _ = _problem()
+    part = RowPartition(op.dim, 3)
+    assert part.range(2)[1] < part.block
+    expected = op.eigsh(4, tolerance=1e-12, seed=1).eigenvalues
+    out = _run(3)
+    for rank, status, values, residuals, converged, applications in out:
+        assert status == "ok" and converged
+        assert np.max(np.abs(np.array(values) - expected) / np.abs(expected)) <= 1e-10
+
+
 def test_failed_rank_ends_the_other_ranks_solve():
     out = _run(2, fail_rank=1)
     assert out[1][1] == "error" and "planted slab failure" in out[1][2]
