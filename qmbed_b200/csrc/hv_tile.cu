@@ -760,7 +760,6 @@ __global__ void __launch_bounds__(kTileThreads, TileShape<T, NB, CPLX>::MIN_BLOC
           uint64_t t[U];
           int lo[U], hi[U];
           double wr[U], wi[U];
-#pragma unroll
           uint64_t rank_t[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
