@@ -602,10 +602,15 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
       }
       if (it >= kMaxOuter) return false;
       lower = std::min(lower, theta.front());
-      // the first filter of a start block uses the Lanczos cut when it is lower
+      // The first filter of a start block uses the Lanczos (or hinted) cut
+      // when it is lower. A random start block's Ritz values all sit near the
+      // middle of the spectrum; a hinted cut below them is kept (it only has
+      // to stay above the spectrum's lower estimate), every other cut stays
+      // above the block's lowest Ritz value.
+      const bool hinted_first = first_filter && hint_used && o.hint_gap > 0.0;
       cut = first_filter ? std::min(theta.back(), cut) : theta.back();
       first_filter = false;
-      if (!(cut > theta.front())) cut = theta.front() + 1.0e-3 * (upper - theta.front());
+      if (!(cut > (hinted_first ? lower : theta.front()))) cut = theta.front() + 1.0e-3 * (upper - theta.front());
       const double e = 0.5 * (upper - cut), c = 0.5 * (upper + cut);
       if (!(e > 0.0)) return false;
       double need = 1.0;
