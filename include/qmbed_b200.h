@@ -349,6 +349,11 @@ QMBED_API int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_
  * block fewer than it waits for; *status receives 1 when the bounded spin
  * ended in the time-out status (the kernel returns instead of hanging). */
 QMBED_API int qmbed_gpu_scan_barrier_selftest(int device, int* status);
+/* Test of the multi-pass flip-chain action's bounded wait on its box copies
+ * (no reference counterpart): a barrier armed for bytes that no copy
+ * delivers is polled 1024 times; *status receives 1 when the wait gave up
+ * (the kernel returns instead of hanging). */
+QMBED_API int qmbed_gpu_flip_wait_selftest(int device, int* status);
 
 /* Extreme Ritz values of a steps-step FP64 Lanczos run without
  * reorthogonalisation from deterministic_start(seed) (src/solve/mod.rs:

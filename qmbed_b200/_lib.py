@@ -100,6 +100,7 @@ def lib() -> ctypes.CDLL:
     P = ctypes.POINTER
     L.qmbed_gpu_last_error.restype = ctypes.c_char_p
     L.qmbed_gpu_device_count.argtypes = [P(i)]
+    L.qmbed_gpu_flip_wait_selftest.argtypes = [i, P(i)]
     L.qmbed_gpu_launch_count.argtypes = [P(u64)]
     L.qmbed_gpu_spin_basis_create.argtypes = [i, i, i, i, i, i, i, P(vp)]
     L.qmbed_gpu_basis_destroy.argtypes = [vp]

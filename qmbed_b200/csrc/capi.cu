@@ -2340,6 +2340,13 @@ int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed_operator*
   return rc;
 }
 
+int qmbed_gpu_flip_wait_selftest(int device, int* status) {
+  return guarded([&] {
+    if (!status) raise(QMBED_INVALID_OPTIONS, "null status");
+    *status = flip_stage_wait_selftest(device);
+  });
+}
+
 int qmbed_gpu_scan_barrier_selftest(int device, int* status) {
   return guarded([&] { *status = scan_barrier_selftest(device); });
 }

@@ -424,6 +424,20 @@ __global__ void __launch_bounds__(kPassThreads, 2) flip_pass_kernel(const __grid
       mbar_wait(&full[k % kStages], static_cast<uint32_t>((k / kStages) & 1));
 }
 
+// Self-test of the bounded stage wait: one thread arms an mbarrier for bytes
+// that no copy will deliver and waits `polls` times; status receives 1 when
+// the wait gave up (the kernel then returns as the passes do).
+__global__ void stage_wait_selftest_kernel(unsigned polls, int* status) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  mbar_expect_tx(&bar, 16);
+  bool done = false;
+  for (unsigned i = 0; i < polls && !done; ++i) done = mbar_try_wait(&bar, 0);
+  *status = done ? 0 : 1;
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
@@ -658,6 +672,21 @@ void FlipChain::check_status() const {
     QMBED_CUDA(cudaMemset(status_.get(), 0, sizeof(int)));
     raise(QMBED_CUDA_ERROR, "a flip-chain pass timed out waiting for its tile copy");
   }
+}
+
+}  // namespace qmbed
+
+namespace qmbed {
+
+int flip_stage_wait_selftest(int device) {
+  QMBED_CUDA(cudaSetDevice(device));
+  DeviceBuffer status(sizeof(int));
+  QMBED_CUDA(cudaMemset(status.get(), 0xff, sizeof(int)));
+  stage_wait_selftest_kernel<<<1, 32>>>(1u << 10, status.as<int>());
+  QMBED_LAUNCH_CHECK();
+  int host = -1;
+  QMBED_CUDA(cudaMemcpy(&host, status.get(), sizeof(int), cudaMemcpyDeviceToHost));
+  return host;
 }
 
 }  // namespace qmbed

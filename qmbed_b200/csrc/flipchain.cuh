@@ -30,6 +30,10 @@ struct FlipStep {
   double kappa_re = 0.0, kappa_im = 0.0;
 };
 
+// Runs the multi-pass action's bounded stage wait on a barrier that no copy
+// completes (1024 polls) on `device`; returns 1 when it gave up as designed.
+int flip_stage_wait_selftest(int device);
+
 class FlipChain {
  public:
   explicit FlipChain(const FlipChainDesc& d);

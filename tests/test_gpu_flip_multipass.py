@@ -88,3 +88,15 @@ def test_unaligned_vectors_take_the_one_pass_kernel(monkeypatch):
     ref = _apply(op, x.clone(), 32, True, "single", monkeypatch)
     got = _apply(op, x, 32, True, "multi", monkeypatch)
     assert float(torch.linalg.vector_norm(got - ref)) <= 2e-6 * float(torch.linalg.vector_norm(ref))
+
+
+def test_stage_wait_times_out_instead_of_hanging():
+    """The passes' wait on a box copy is bounded: a barrier armed for bytes that
+    never arrive gives up and reports it, and the context stays usable."""
+    import ctypes
+    from qmbed_b200._lib import check, lib
+    status = ctypes.c_int(-1)
+    check(lib().qmbed_gpu_flip_wait_selftest(0, ctypes.byref(status)))
+    assert status.value == 1
+    op, _ = _operator(12, seed=4)
+    assert op.apply(np.ones(op.dim)).shape == (op.dim,)
