@@ -350,8 +350,11 @@ __device__ void phase_init(const ScanArgs& a, const uint64_t* starts, int idst) 
 // The persistent kernel: (when step == 0) the normalised start vectors, then
 // up to kChunkSteps Lanczos steps of the current pass; the step counter in
 // `state` advances once per completed step.
-template <int PPL, bool PASS2>
-__global__ void __launch_bounds__(kThreads, 3) scan_chunk_kernel(const ScanArgs a) {
+// MINB: the resident blocks per SM the register budget is compiled for (3:
+// no spills; 4: 64 registers, more warps to hide the gathers' latency, a few
+// spills); the autotuner picks between them.
+template <int PPL, bool PASS2, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) scan_chunk_kernel(const ScanArgs a) {
   constexpr int P = 32 * PPL;
   __shared__ double c[kMaxComp * P];
   __shared__ uint64_t starts[kMaxSectors], item_starts[kMaxSectors];
@@ -812,10 +815,14 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
       if (per_sm < 1) raise(QMBED_UNSUPPORTED_BACKEND, "the persistent scan kernel does not fit on an SM");
       return static_cast<unsigned>(per_sm * ops.sms());
     };
-    const void* k1 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false>);
-    const void* k2 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true>);
+    const void* k1 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 3>);
+    const void* k2 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true, 3>);
+    const void* k1_wide = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 4>);
+    const void* k2_wide = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true, 4>);
     unsigned grid1 = grid_of(k1), grid2 = grid_of(k2);
     const int max_per_sm1 = static_cast<int>(grid1 / ops.sms()), max_per_sm2 = static_cast<int>(grid2 / ops.sms());
+    const int wide_per_sm1 = static_cast<int>(grid_of(k1_wide) / ops.sms());
+    const int wide_per_sm2 = static_cast<int>(grid_of(k2_wide) / ops.sms());
     const int check_grid = (cols + 127) / 128;
     double* tri = tri_work.as<double>();
     ScanArgs args = a;
@@ -837,12 +844,22 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
     // and kept for pass 2.
     result.tuned_blocks_per_sm = max_per_sm1;
     if (max_per_sm1 > 1 && rows >= (1ull << 16) && max_steps >= 6 * kChunkSteps) {
+      // candidates: (register budget, blocks per SM), most warps first
+      struct Shape {
+        bool wide;
+        int per_sm;
+      };
+      std::vector<Shape> shapes;
+      if (wide_per_sm1 > max_per_sm1) shapes.push_back({true, wide_per_sm1});
+      for (int per_sm = max_per_sm1; per_sm >= 1 && shapes.size() < 4; --per_sm) shapes.push_back({false, per_sm});
       cudaEvent_t e0, e1;
       QMBED_CUDA(cudaEventCreate(&e0));
       QMBED_CUDA(cudaEventCreate(&e1));
       double best = std::numeric_limits<double>::infinity();
-      for (int per_sm = max_per_sm1; per_sm >= 1 && per_sm > max_per_sm1 - 4; --per_sm) {
-        grid1 = static_cast<unsigned>(per_sm * ops.sms());
+      bool best_wide = false;
+      for (const Shape& shape : shapes) {
+        k1 = shape.wide ? k1_wide : reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 3>);
+        grid1 = static_cast<unsigned>(shape.per_sm * ops.sms());
         QMBED_CUDA(cudaEventRecord(e0, stream));
         chunk(false);
         QMBED_CUDA(cudaEventRecord(e1, stream));
@@ -852,15 +869,19 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
         result.tuning_ms.push_back(ms);
         if (ms < best) {
           best = ms;
-          result.tuned_blocks_per_sm = per_sm;
+          best_wide = shape.wide;
+          result.tuned_blocks_per_sm = shape.per_sm;
         }
         if (host_state->status == kStatusBarrierTimeout || host_state->active == 0 || host_state->step >= max_steps)
           break;
       }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
+      k1 = best_wide ? k1_wide : reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 3>);
+      k2 = best_wide ? k2_wide : k2;
       grid1 = static_cast<unsigned>(result.tuned_blocks_per_sm * ops.sms());
-      grid2 = static_cast<unsigned>(std::min(result.tuned_blocks_per_sm, max_per_sm2) * ops.sms());
+      grid2 = static_cast<unsigned>(std::min(result.tuned_blocks_per_sm, best_wide ? wide_per_sm2 : max_per_sm2) *
+                                    ops.sms());
     }
     // Pass 1: one chunk captured in a graph, replayed until every pair stopped.
     cudaGraph_t graph = nullptr;
