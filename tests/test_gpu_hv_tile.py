@@ -319,3 +319,18 @@ def test_hop_kernel_agrees_with_packed_rows_at_28_sites(engine):
     free.apply_device(x, y, precision=64)
     torch.cuda.synchronize()
     assert float(torch.linalg.vector_norm(y - ref)) <= 1e-13 * float(torch.linalg.vector_norm(ref))
+
+
+@pytest.mark.parametrize("sites,up,momentum,parity", [(16, 1, 0, 1), (16, 15, 0, None), (18, 2, 9, -1),
+                                                       (5, 2, 0, 1), (6, 3, 3, None), (22, 11, 0, 1)])
+def test_hop_kernel_extreme_fillings_match_oracle(engine, oracle, sites, up, momentum, parity):
+    """One or two up spins (few hops), one down spin, the smallest chains, and a
+    half-filled 22-site sector, through the hop kernel against the oracle."""
+    terms = _hop_terms(sites, 0.8, True)
+    o = oracle.Operator.build(oracle.Basis(sites, up=up, momentum=momentum, parity=parity), terms)
+    g = engine.GpuOperator(engine.GpuBasis(sites, up=up, momentum=momentum, parity=parity), terms,
+                           storage="matrix_free")
+    assert g.lookup_info()["lookup"] == "table_hop"
+    x = np.random.default_rng(up).normal(size=o.dim)
+    expected = o.apply(x).real
+    assert np.linalg.norm(g.apply(x) - expected) <= 1e-13 * max(np.linalg.norm(expected), 1e-300)
