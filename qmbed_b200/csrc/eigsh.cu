@@ -771,6 +771,28 @@ EigshResult eigsh(const LinearOperatorView& op, const EigshOptions& options, con
     return r;
   }
   const int k = static_cast<int>(phase1.eigenvalues.size());
+  // FP64 refinement of the FP32 Ritz vectors. Real operators with a block
+  // action refine them as one block through the filtered solver's FP64 phase
+  // (its start subspace already holds the wanted pairs to the FP32 level, so it
+  // skips its FP32 phase and filters in FP64 to the tolerance); every other
+  // operator, or a refinement that does not converge, takes the FP64 thick
+  // restart seeded with them.
+  if (!cplx && filtered_applicable(op, options, false)) {
+    DeviceBuffer wide(static_cast<size_t>(k) * n * 16);
+    ops.widen_real(phase1.vectors.as<double>(), wide.as<double>(), static_cast<uint64_t>(k) * n);
+    try {
+      EigshResult r = filtered_eigsh(op, options, wide.as<double>(), k, ops);
+      r.fp32_iterations = phase1.iterations;
+      r.fp64_iterations = r.iterations;
+      r.iterations += phase1.iterations;
+      r.reorthogonalization_passes += phase1.reorthogonalization_passes;
+      r.conditional_second_passes += phase1.conditional_second_passes;
+      r.operator_applications += c32.applications;
+      return r;
+    } catch (const Error& e) {
+      if (e.code != QMBED_NON_CONVERGENCE) throw;
+    }
+  }
   Panel seed;
   seed.alloc(n, k, 64, cplx);
   ops.copy(phase1.vectors.get(), seed.col(0), static_cast<size_t>(k) * n * (cplx ? 16 : 8));

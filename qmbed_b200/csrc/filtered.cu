@@ -545,18 +545,22 @@ EigshResult filtered_eigsh(const LinearOperatorView& op, const EigshOptions& o, 
                  std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - started).count());
   };
   size_t bound_applications = 0;
+  // The bound runs start from a deterministic start column: a caller's
+  // vectors may be near eigenvectors (a refinement), from which a short
+  // Lanczos run sees little of the spectrum.
+  const double* bound_start = col(used < nb ? used : 0);
   // A spectral hint replaces the bound estimate when the Ritz values of a
   // short check run lie inside its interval (Ritz values lie inside the
   // spectrum, so an interval that misses one is wrong).
   bool hint_used = false;
   Bounds bd;
   if (o.hint && o.hint_upper > o.hint_lower) {
-    bd = lanczos_bounds(op, ops, col(0), bound_applications, o.hint_check_steps);
+    bd = lanczos_bounds(op, ops, bound_start, bound_applications, o.hint_check_steps);
     hint_used = bd.theta.front() >= o.hint_lower && bd.theta.back() <= o.hint_upper;
   }
   if (!hint_used) {
     size_t more = 0;
-    bd = lanczos_bounds(op, ops, col(0), more);
+    bd = lanczos_bounds(op, ops, bound_start, more);
     bound_applications += more;
   }
   // Upper end of the damped interval: the hint's upper end, or the top Ritz
