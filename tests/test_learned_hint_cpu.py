@@ -1,0 +1,47 @@
+"""Host logic of the learned eigsh hint, without a GPU.
+
+The network is replaced by a stand-in with fixed outputs, so the features,
+the padding of the predicted interval and the restart-size rule are checked
+on their own: the interval is [E0, E_max] widened by the margin on both
+sides, the gap is returned in energy units, and the restart keeps the wanted
+pairs and two more only when the predicted relative gap is small.
+"""
+
+import numpy as np
+import pytest
+
+from qmbed_b200 import learned
+
+
+class _FixedNetwork:
+    def __init__(self, e0_per_site, emax_per_site, gap_times_sites):
+        self.out = np.array([[e0_per_site, emax_per_site, gap_times_sites]], np.float32)
+
+    def predict(self, x):
+        assert np.asarray(x).shape[-1] == len(learned.CHAIN_FEATURES)
+        return self.out
+
+
+def test_chain_features():
+    f = learned.chain_features(28, 0.25, 1.1, 0)
+    assert f.dtype == np.float32 and f.shape == (len(learned.CHAIN_FEATURES),)
+    assert np.allclose(f, [1 / 28, 0.25, 1.1, 1.0, 1.0, 1.0])
+    g = learned.chain_features(26, 0.0, 0.9, 13)
+    assert np.allclose(g, [1 / 26, 0.0, 0.9, -1.0, 0.0, 0.0])
+
+
+@pytest.mark.parametrize("gap_times_sites,expected_keep", [(4.0, 6), (40.0, 0)])
+def test_hint_interval_and_restart_rule(gap_times_sites, expected_keep):
+    model = learned.ChainSpectrum(mlp=_FixedNetwork(-0.44, 0.25, gap_times_sites), margin=0.03)
+    hint = model.hint(34, 0.0, 1.0, 0, eigenpairs=4, krylov_dimension=40)
+    e0, emax, width = -0.44 * 34, 0.25 * 34, (0.25 + 0.44) * 34
+    assert hint["lower"] == pytest.approx(e0 - 0.03 * width, rel=1e-6)
+    assert hint["upper"] == pytest.approx(emax + 0.03 * width, rel=1e-6)
+    assert hint["gap"] == pytest.approx(gap_times_sites / 34, rel=1e-6)
+    assert hint["restart_keep"] == expected_keep
+    assert hint["check_steps"] == 8
+
+
+def test_negative_gap_predictions_are_clipped():
+    model = learned.ChainSpectrum(mlp=_FixedNetwork(-0.44, 0.25, -1.0))
+    assert model.predict(20, 0.1, 1.0, 0)[2] == 0.0

@@ -81,9 +81,10 @@ def test_callback_exports_validate_their_arguments(library):
 
 
 def test_struct_layouts_match_the_header(library):
-    from qmbed_b200._lib import EigshInfoC, EigshOptionsC
+    from qmbed_b200._lib import EigshHintC, EigshInfoC, EigshOptionsC
     assert ctypes.sizeof(EigshOptionsC) == 64
     assert ctypes.sizeof(EigshInfoC) == 56
+    assert ctypes.sizeof(EigshHintC) == 48  # qmbed_eigsh_hint: 3 doubles, u64, 2 ints, u64
 
 
 def test_missing_library_fails_loudly(tmp_path):
