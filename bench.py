@@ -350,6 +350,7 @@ def scan_section(sites: int, rank: int, local_rank: int, with_cpu: bool) -> dict
            "applications": info["applications"], "verification_applications": info["verification_applications"],
            "first_pass_s": info["pass1_seconds"], "cuda_graph": info["graph"],
            "autotuned_blocks_per_sm": info["tuned_blocks_per_sm"], "tuning_chunk_ms": info["tuning_chunk_ms"],
+           "autotuned_rows_per_warp": info["tuned_rows_per_warp"],
            "max_relative_residual": info["max_relative_residual"], "merged_ritz_copies": info["merged_copies"],
            "residuals_verified": int(np.isfinite(info["residuals"]).sum()),
            "e_max_range": [float(np.nanmin(info["e_max"])), float(np.nanmax(info["e_max"]))],

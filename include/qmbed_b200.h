@@ -334,12 +334,13 @@ QMBED_API int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed
  * its Ritz vector (the reference's acceptance test r <= tol max(|theta|, 1),
  * src/solve/mod.rs:1252-1263, holds for every reported pair, otherwise
  * QMBED_STATUS_NON_CONVERGENCE); e_max[s][p] = the largest Ritz value at
- * convergence (an inner estimate of the top of the spectrum); info (10
+ * convergence (an inner estimate of the top of the spectrum); info (11
  * doubles): first-pass steps of the longest pair, first-pass applications,
  * verification applications, CUDA graph used (1/0), first-pass seconds,
  * total seconds, largest relative residual, Ritz copies merged, the
- * autotuned resident blocks per SM of the persistent launch and the fastest
- * tuning chunk's milliseconds (0 when not tuned).
+ * autotuned resident blocks per SM of the persistent launch, the fastest
+ * tuning chunk's milliseconds (0 when not tuned) and the autotuned rows per
+ * warp of its apply phase.
  * residuals and e_max may be NULL. */
 QMBED_API int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
                                    const double* coefficients, int eigenpairs, double tolerance, int max_steps,

@@ -157,37 +157,43 @@ __device__ __forceinline__ void roles(int j, int& cur, int& prev, int& work) {
   work = (j + 1) % 3;
 }
 
-// One warp per row of all sectors: work = H(s, p) cur - beta_{j-1} prev, and
-// in the second pass ritz_i += s_i[j] cur for the pairs still inside m_p.
-template <int PPL, bool PASS2>
+// RPW rows per warp (1: a warp per row, 2: a half-warp per row with twice
+// the points per lane) of all sectors: work = H(s, p) cur - beta_{j-1} prev,
+// and in the second pass ritz_i += s_i[j] cur for the pairs still inside m_p.
+template <int PPL, bool PASS2, int RPW>
 __device__ void phase_apply(const ScanArgs& a, const uint64_t* starts, const double* c, int j) {
   constexpr int P = 32 * PPL;
+  constexpr int LPR = 32 / RPW;   // lanes per row
+  constexpr int PL = PPL * RPW;   // points per lane
   int cur, prev, work;
   roles(j, cur, prev, work);
   const int lane = threadIdx.x & 31;
+  const int sl = lane % LPR;
   const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
-  for (uint64_t g = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; g < a.total_rows;
-       g += warps) {
+  for (uint64_t gw = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; gw * RPW < a.total_rows;
+       gw += warps) {
+    const uint64_t g = gw * RPW + static_cast<uint64_t>(lane / LPR);
+    if (g >= a.total_rows) continue;
     const int s = find_sector(starts, a.ns, g);
     if (j >= a.sector_gate[s]) continue;  // every column of the sector is done
     const SectorDesc& d = a.sec[s];
     const uint64_t r = g - d.row0;
     const double* z = d.buf[cur];
-    double are[PPL], aim[PPL], dsum[PPL];
+    double are[PL], aim[PL], dsum[PL];
 #pragma unroll
-    for (int q = 0; q < PPL; ++q) are[q] = aim[q] = dsum[q] = 0.0;
+    for (int q = 0; q < PL; ++q) are[q] = aim[q] = dsum[q] = 0.0;
     for (int k = 0; k < a.K; ++k) {
       const CompRows& cr = d.comp[k];
-      double ck[PPL];
+      double ck[PL];
 #pragma unroll
-      for (int q = 0; q < PPL; ++q) ck[q] = c[k * P + lane * PPL + q];
+      for (int q = 0; q < PL; ++q) ck[q] = c[k * P + sl * PL + q];
       const uint64_t begin = row_begin(cr, r), end = row_begin(cr, r + 1);
       for (uint64_t e = begin; e < end; ++e) {
         const uint64_t col = cr.cols[e];
         const double vr = cr.vals[2 * e], vi = cr.vals[2 * e + 1];
-        const double2* zc = reinterpret_cast<const double2*>(z) + col * P + lane * PPL;
+        const double2* zc = reinterpret_cast<const double2*>(z) + col * P + sl * PL;
 #pragma unroll
-        for (int q = 0; q < PPL; ++q) {
+        for (int q = 0; q < PL; ++q) {
           const double2 x = zc[q];
           are[q] = fma(ck[q], vr * x.x - vi * x.y, are[q]);
           aim[q] = fma(ck[q], vr * x.y + vi * x.x, aim[q]);
@@ -195,16 +201,16 @@ __device__ void phase_apply(const ScanArgs& a, const uint64_t* starts, const dou
       }
       const double dr = cr.diag_complex ? cr.diag[2 * r] : cr.diag[r];
 #pragma unroll
-      for (int q = 0; q < PPL; ++q) dsum[q] = fma(ck[q], dr, dsum[q]);
+      for (int q = 0; q < PL; ++q) dsum[q] = fma(ck[q], dr, dsum[q]);
     }
-    const double2* zs = reinterpret_cast<const double2*>(z) + r * P + lane * PPL;
-    const double2* pv = reinterpret_cast<const double2*>(d.buf[prev]) + r * P + lane * PPL;
-    double2* o = reinterpret_cast<double2*>(d.buf[work]) + r * P + lane * PPL;
+    const double2* zs = reinterpret_cast<const double2*>(z) + r * P + sl * PL;
+    const double2* pv = reinterpret_cast<const double2*>(d.buf[prev]) + r * P + sl * PL;
+    double2* o = reinterpret_cast<double2*>(d.buf[work]) + r * P + sl * PL;
 #pragma unroll
-    for (int q = 0; q < PPL; ++q) {
+    for (int q = 0; q < PL; ++q) {
       const double2 x = zs[q];
       double wr = are[q] + dsum[q] * x.x, wi = aim[q] + dsum[q] * x.y;
-      const int colidx = s * P + lane * PPL + q;
+      const int colidx = s * P + sl * PL + q;
       if (j > 0) {
         const double b = a.beta[static_cast<uint64_t>(j - 1) * a.cols + colidx];
         const double2 y = pv[q];
@@ -215,7 +221,7 @@ __device__ void phase_apply(const ScanArgs& a, const uint64_t* starts, const dou
       if (PASS2 && j < a.stop[colidx]) {
         for (int i = 0; i < a.ncand; ++i) {
           const double si = a.cand_s[(static_cast<uint64_t>(colidx) * a.ncand + i) * a.max_steps + j];
-          double2* acc = reinterpret_cast<double2*>(d.ritz[i]) + r * P + lane * PPL + q;
+          double2* acc = reinterpret_cast<double2*>(d.ritz[i]) + r * P + sl * PL + q;
           double2 v = *acc;
           v.x = fma(si, x.x, v.x);
           v.y = fma(si, x.y, v.y);
@@ -353,7 +359,9 @@ __device__ void phase_init(const ScanArgs& a, const uint64_t* starts, int idst) 
 // MINB: the resident blocks per SM the register budget is compiled for (3:
 // no spills; 4: 64 registers, more warps to hide the gathers' latency, a few
 // spills); the autotuner picks between them.
-template <int PPL, bool PASS2, int MINB>
+// RPW: rows per warp in the apply phase (1 or 2), the other shape the
+// autotuner chooses.
+template <int PPL, bool PASS2, int MINB, int RPW>
 __global__ void __launch_bounds__(kThreads, MINB) scan_chunk_kernel(const ScanArgs a) {
   constexpr int P = 32 * PPL;
   __shared__ double c[kMaxComp * P];
@@ -389,7 +397,7 @@ __global__ void __launch_bounds__(kThreads, MINB) scan_chunk_kernel(const ScanAr
     roles(j, cur, prev, work);
     double* alpha_j = a.alpha + static_cast<uint64_t>(j) * a.cols;
     double* beta_j = a.beta + static_cast<uint64_t>(j) * a.cols;
-    phase_apply<PPL, PASS2>(a, starts, c, j);
+    phase_apply<PPL, PASS2, RPW>(a, starts, c, j);
     if (!grid_sync(st, blocks)) return;
     phase_reduce<PPL, 0>(a, item_starts, cur, work, nullptr, j);
     if (!grid_sync(st, blocks)) return;
@@ -815,12 +823,14 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
       if (per_sm < 1) raise(QMBED_UNSUPPORTED_BACKEND, "the persistent scan kernel does not fit on an SM");
       return static_cast<unsigned>(per_sm * ops.sms());
     };
-    const void* k1 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 3>);
-    const void* k2 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true, 3>);
-    const void* k1_wide = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 4>);
-    const void* k2_wide = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true, 4>);
+    const void* k1 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 3, 1>);
+    const void* k2 = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true, 3, 1>);
+    const void* k1_wide = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 4, 1>);
+    const void* k2_wide = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true, 4, 1>);
+    const void* k1_pair = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 3, 2>);
+    const void* k2_pair = reinterpret_cast<const void*>(scan_chunk_kernel<PPL, true, 3, 2>);
     unsigned grid1 = grid_of(k1), grid2 = grid_of(k2);
-    const int max_per_sm1 = static_cast<int>(grid1 / ops.sms()), max_per_sm2 = static_cast<int>(grid2 / ops.sms());
+    const int max_per_sm1 = static_cast<int>(grid1 / ops.sms());
     const int wide_per_sm1 = static_cast<int>(grid_of(k1_wide) / ops.sms());
     const int wide_per_sm2 = static_cast<int>(grid_of(k2_wide) / ops.sms());
     const int check_grid = (cols + 127) / 128;
@@ -844,21 +854,24 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
     // and kept for pass 2.
     result.tuned_blocks_per_sm = max_per_sm1;
     if (max_per_sm1 > 1 && rows >= (1ull << 16) && max_steps >= 6 * kChunkSteps) {
-      // candidates: (register budget, blocks per SM), most warps first
+      // candidates: (register budget, rows per warp, blocks per SM)
       struct Shape {
         bool wide;
+        int rpw;
         int per_sm;
       };
-      std::vector<Shape> shapes;
-      if (wide_per_sm1 > max_per_sm1) shapes.push_back({true, wide_per_sm1});
-      for (int per_sm = max_per_sm1; per_sm >= 1 && shapes.size() < 4; --per_sm) shapes.push_back({false, per_sm});
+      const int pair_per_sm1 = static_cast<int>(grid_of(k1_pair) / ops.sms());
+      std::vector<Shape> shapes{{false, 1, max_per_sm1}, {false, 2, pair_per_sm1}};
+      if (wide_per_sm1 > max_per_sm1) shapes.push_back({true, 1, wide_per_sm1});
+      if (max_per_sm1 > 1) shapes.push_back({false, 1, max_per_sm1 - 1});
       cudaEvent_t e0, e1;
       QMBED_CUDA(cudaEventCreate(&e0));
       QMBED_CUDA(cudaEventCreate(&e1));
       double best = std::numeric_limits<double>::infinity();
-      bool best_wide = false;
+      Shape chosen = shapes.front();
+      const void* k1_plain = k1;
       for (const Shape& shape : shapes) {
-        k1 = shape.wide ? k1_wide : reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 3>);
+        k1 = shape.wide ? k1_wide : (shape.rpw == 2 ? k1_pair : k1_plain);
         grid1 = static_cast<unsigned>(shape.per_sm * ops.sms());
         QMBED_CUDA(cudaEventRecord(e0, stream));
         chunk(false);
@@ -869,19 +882,21 @@ ScanResult scan_lowest(const std::vector<std::vector<const SpinOperator*>>& comp
         result.tuning_ms.push_back(ms);
         if (ms < best) {
           best = ms;
-          best_wide = shape.wide;
+          chosen = shape;
           result.tuned_blocks_per_sm = shape.per_sm;
+          result.tuned_rows_per_warp = shape.rpw;
         }
         if (host_state->status == kStatusBarrierTimeout || host_state->active == 0 || host_state->step >= max_steps)
           break;
       }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
-      k1 = best_wide ? k1_wide : reinterpret_cast<const void*>(scan_chunk_kernel<PPL, false, 3>);
-      k2 = best_wide ? k2_wide : k2;
-      grid1 = static_cast<unsigned>(result.tuned_blocks_per_sm * ops.sms());
-      grid2 = static_cast<unsigned>(std::min(result.tuned_blocks_per_sm, best_wide ? wide_per_sm2 : max_per_sm2) *
-                                    ops.sms());
+      k1 = chosen.wide ? k1_wide : (chosen.rpw == 2 ? k1_pair : k1_plain);
+      k2 = chosen.wide ? k2_wide : (chosen.rpw == 2 ? k2_pair : k2);
+      const int per_sm2 = chosen.wide ? wide_per_sm2
+                                      : static_cast<int>(grid_of(chosen.rpw == 2 ? k2_pair : k2) / ops.sms());
+      grid1 = static_cast<unsigned>(chosen.per_sm * ops.sms());
+      grid2 = static_cast<unsigned>(std::min(chosen.per_sm, per_sm2) * ops.sms());
     }
     // Pass 1: one chunk captured in a graph, replayed until every pair stopped.
     cudaGraph_t graph = nullptr;

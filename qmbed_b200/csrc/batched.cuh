@@ -25,6 +25,7 @@ struct ScanResult {
   bool verified = false;            // every reported pair met residual <= tol max(|theta|, 1)
   bool graph = false;               // first pass replayed from a CUDA graph
   int tuned_blocks_per_sm = 0;      // autotuned resident blocks per SM of the persistent launch
+  int tuned_rows_per_warp = 1;      // autotuned rows per warp of its apply phase
   std::vector<double> tuning_ms;    // chunk times of the candidates, most blocks first
   double pass1_seconds = 0.0, seconds = 0.0;
 };

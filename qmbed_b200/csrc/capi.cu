@@ -2323,6 +2323,7 @@ int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_operator* 
       info[7] = static_cast<double>(r.merged_copies);
       info[8] = static_cast<double>(r.tuned_blocks_per_sm);
       info[9] = r.tuning_ms.empty() ? 0.0 : *std::min_element(r.tuning_ms.begin(), r.tuning_ms.end());
+      info[10] = static_cast<double>(r.tuned_rows_per_warp);
     }
   });
 }
@@ -2330,7 +2331,7 @@ int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_operator* 
 int qmbed_gpu_scan_lowest(int n_sectors, int n_components, const qmbed_operator* components, int n_points,
                           const double* coefficients, int eigenpairs, double tolerance, int max_steps, uint64_t seed,
                           double* eigenvalues, int* steps, double* info) {
-  double full[10] = {0};
+  double full[11] = {0};
   const int rc = qmbed_gpu_scan_solve(n_sectors, n_components, components, n_points, coefficients, eigenpairs,
                                       tolerance, max_steps, seed, eigenvalues, nullptr, nullptr, steps, full);
   if (rc == QMBED_STATUS_OK && info) {

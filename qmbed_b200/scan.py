@@ -31,7 +31,7 @@ def scan_lowest(components, coefficients, eigenpairs: int = 2, tolerance: float 
     residuals = np.full((sectors, points, eigenpairs), np.nan)
     e_max = np.full((sectors, points), np.nan)
     steps = np.zeros((sectors, points), np.int32)
-    info = np.zeros(10)
+    info = np.zeros(11)
     ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
     check(lib().qmbed_gpu_scan_solve(sectors, k, ctypes.cast(handles, ctypes.c_void_p), points, ptr(coef),
                                      eigenpairs, tolerance, max_steps, seed, ptr(values), ptr(residuals), ptr(e_max),
@@ -41,6 +41,7 @@ def scan_lowest(components, coefficients, eigenpairs: int = 2, tolerance: float 
                            "pass1_seconds": float(info[4]), "seconds": float(info[5]),
                            "max_relative_residual": float(info[6]), "merged_copies": int(info[7]),
                            "tuned_blocks_per_sm": int(info[8]), "tuning_chunk_ms": float(info[9]),
+                           "tuned_rows_per_warp": int(info[10]),
                            "residuals": residuals, "e_max": e_max}
 
 

@@ -77,7 +77,7 @@ def test_scan_at_22_sites_matches_oracle(oracle):
     coefs = scan.j1j2_scan_points(points, seed=22)
     values, steps, info = scan.scan_lowest(sectors, coefs, eigenpairs=2, tolerance=1e-10)
     # 705,432 rows: the autotuner timed the persistent launch's shapes on the first chunks
-    assert info["tuned_blocks_per_sm"] >= 1 and info["graph"]
+    assert info["tuned_blocks_per_sm"] >= 1 and info["tuned_rows_per_warp"] in (1, 2) and info["graph"]
     for k, p in ((0, 0), (11, 3), (7, points - 1), (15, 5)):
         ref = _oracle_pair(oracle, scan, sites, k, coefs[p], 2)
         assert np.max(np.abs(values[k, p] - ref) / np.maximum(np.abs(ref), 1.0)) <= 1e-10, (k, p)
