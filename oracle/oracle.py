@@ -112,6 +112,7 @@ class Basis:
             0 if momentum is None else momentum, 0 if parity is None else parity,
             NORMALIZATIONS[normalization], ctypes.byref(handle)))
         self.handle = handle
+        self._free = lib().oracle_basis_free  # held so the destructor works during interpreter shutdown
         self.sites = sites
         self.up = up
         self.momentum = momentum
@@ -120,7 +121,7 @@ class Basis:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            lib().oracle_basis_free(self.handle)
+            self._free(self.handle)
             self.handle = None
 
     def __len__(self) -> int:
@@ -242,6 +243,7 @@ class Operator:
 
     def __init__(self, handle):
         self.handle = handle
+        self._free = lib().oracle_operator_free  # held so the destructor works during interpreter shutdown
 
     @classmethod
     def build(cls, basis: Basis, terms, check_hermitian=True, check_particles=True) -> "Operator":
@@ -271,7 +273,7 @@ class Operator:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            lib().oracle_operator_free(self.handle)
+            self._free(self.handle)
             self.handle = None
 
     @property
