@@ -2111,6 +2111,7 @@ int run_eigsh(qmbed_operator op, const qmbed_eigsh_options* options, qmbed_eigsh
               int n_initial, double* eigenvalues, double* residuals, double* eigenvectors, qmbed_eigsh_info* info) {
   return guarded([&] {
     if (!op || !options) raise(QMBED_INVALID_OPTIONS, "null operator or options");
+    if (!eigenvalues || !residuals) raise(QMBED_INVALID_OPTIONS, "null eigenvalue or residual buffer");
     std::lock_guard<std::mutex> lock(op->mu);
     EigshOptions o;
     if (hint) {
@@ -2302,7 +2303,11 @@ int qmbed_gpu_scan_solve(int n_sectors, int n_components, const qmbed_operator* 
       raise(QMBED_INVALID_OPTIONS, "a scan needs sectors, components, coefficients and outputs");
     std::vector<std::vector<const SpinOperator*>> comps(static_cast<size_t>(n_sectors));
     for (int s = 0; s < n_sectors; ++s)
-      for (int k = 0; k < n_components; ++k) comps[s].push_back(components[s * n_components + k]->op.get());
+      for (int k = 0; k < n_components; ++k) {
+        const qmbed_operator c = components[s * n_components + k];
+        if (!c) raise(QMBED_INVALID_OPTIONS, "null scan component");
+        comps[s].push_back(c->op.get());
+      }
     qmbed_operator_s& first = *components[0];
     std::lock_guard<std::mutex> lock(first.mu);
     QMBED_CUDA(cudaSetDevice(first.op->basis().device()));
@@ -2349,11 +2354,15 @@ int qmbed_gpu_flip_wait_selftest(int device, int* status) {
 }
 
 int qmbed_gpu_scan_barrier_selftest(int device, int* status) {
-  return guarded([&] { *status = scan_barrier_selftest(device); });
+  return guarded([&] {
+    if (!status) raise(QMBED_INVALID_OPTIONS, "null status");
+    *status = scan_barrier_selftest(device);
+  });
 }
 
 int qmbed_gpu_lanczos_extremes(qmbed_operator op, int steps, uint64_t seed, double* out) {
   return guarded([&] {
+    if (!op || !out) raise(QMBED_INVALID_OPTIONS, "null operator or output");
     std::lock_guard<std::mutex> lock(op->mu);
     const RitzExtremes r = lanczos_extremes(op->view(), steps, seed, op->block_ops());
     out[0] = r.min;

@@ -176,6 +176,22 @@ def test_operator_errors_match_reference_categories(engine):
     assert e.value.code == 6
 
 
+def test_eigsh_rejects_null_outputs(engine):
+    """Null eigenvalue/residual buffers are QMBED_STATUS_INVALID_OPTIONS, and the operator stays usable."""
+    import ctypes
+    from qmbed_b200._lib import EigshOptionsC, lib
+    op = engine.GpuOperator(engine.GpuBasis(8, up=4), engine.heisenberg_terms(8))
+    options = EigshOptionsC()
+    values = np.zeros(2)
+    assert lib().qmbed_gpu_eigsh_hinted(op.handle, ctypes.byref(options), None, None, 0, None, None, None, None) == 8
+    assert lib().qmbed_gpu_eigsh(op.handle, ctypes.byref(options), None, 0,
+                                 values.ctypes.data_as(ctypes.c_void_p), None, None, None) == 8
+    assert b"null eigenvalue or residual buffer" in lib().qmbed_gpu_last_error()
+    r = op.eigsh(2, tolerance=1e-12)
+    dense = np.linalg.eigvalsh(op.to_scipy().toarray())[:2]
+    assert r.converged and np.allclose(r.eigenvalues, dense, rtol=1e-10, atol=1e-10)
+
+
 def test_deterministic_start_matches_oracle(engine, oracle):
     for n, seed in ((1000, 31), (123457, 0), (5, 2**63 + 11)):
         np.testing.assert_allclose(engine.deterministic_start(n, seed), oracle.deterministic_start(n, seed),

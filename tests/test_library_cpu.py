@@ -80,6 +80,34 @@ def test_callback_exports_validate_their_arguments(library):
     library.qmbed_string_free(pointer)
 
 
+def test_typed_entries_reject_null_arguments_before_cuda(library):
+    """Null handles, components and output pointers are argument errors
+    (QMBED_STATUS_INVALID_OPTIONS = 8), raised before any device work."""
+    import numpy as np
+    from qmbed_b200._lib import EigshOptionsC
+    invalid = 8
+
+    def ptr(a):
+        return a.ctypes.data_as(ctypes.c_void_p)
+
+    values, residuals = np.zeros(4), np.zeros(4)
+    options = EigshOptionsC()
+    assert library.qmbed_gpu_eigsh_hinted(None, ctypes.byref(options), None, None, 0, ptr(values), ptr(residuals),
+                                          None, None) == invalid
+    assert b"null operator" in library.qmbed_gpu_last_error()
+    components = (ctypes.c_void_p * 1)(None)
+    coefficients, steps = np.ones(1), np.zeros(1, np.int32)
+    assert library.qmbed_gpu_scan_solve(1, 1, components, 1, ptr(coefficients), 1, 1e-10, 10, 0, ptr(values), None,
+                                        None, ptr(steps), None) == invalid
+    assert b"null scan component" in library.qmbed_gpu_last_error()
+    assert library.qmbed_gpu_scan_solve(0, 1, components, 1, ptr(coefficients), 1, 1e-10, 10, 0, ptr(values), None,
+                                        None, ptr(steps), None) == invalid
+    assert library.qmbed_gpu_scan_barrier_selftest(0, None) == invalid
+    assert library.qmbed_gpu_flip_wait_selftest(0, None) == invalid
+    assert library.qmbed_gpu_lanczos_extremes(None, 8, 0, None) == invalid
+    assert b"null operator" in library.qmbed_gpu_last_error()
+
+
 def test_struct_layouts_match_the_header(library):
     from qmbed_b200._lib import EigshHintC, EigshInfoC, EigshOptionsC
     assert ctypes.sizeof(EigshOptionsC) == 64
