@@ -59,13 +59,25 @@ def _slab_apply(matrix, part, rank, fail_after=None):
     return apply
 
 
-def _solve(rank, world, fail_rank=None):
-    _, matrix, start = _problem()
+def _tiny():
+    """A 4 x 4 symmetric matrix: with three ranks the last slab is empty."""
+    import scipy.sparse as sp
+    a = np.random.default_rng(5).normal(size=(4, 4))
+    return sp.csr_matrix(a + a.T), np.ones(4)
+
+
+def _solve(rank, world, fail_rank=None, case="sector"):
+    if case == "tiny":
+        matrix, start = _tiny()
+        eigenpairs, krylov = 1, 3
+    else:
+        _, matrix, start = _problem()
+        eigenpairs, krylov = 4, 24
     part = RowPartition(matrix.shape[0], world)
     row0, rows = part.range(rank)
     apply = _slab_apply(matrix, part, rank, fail_after=3 if rank == fail_rank else None)
-    return distributed_eigsh(apply, part, 4, krylov_dimension=24, tolerance=1e-10, start=start[row0:row0 + rows],
-                             restart_keep=8)
+    return distributed_eigsh(apply, part, eigenpairs, krylov_dimension=krylov, tolerance=1e-10,
+                             start=start[row0:row0 + rows], restart_keep=0 if case == "tiny" else 8)
 
 
 def _free_port():
@@ -74,14 +86,14 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, fail_rank, queue):
+def _worker(rank, world, port, fail_rank, queue, case="sector"):
     import torch.distributed as dist
     from datetime import timedelta
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=20))
     try:
-        r = _solve(rank, world, fail_rank)
+        r = _solve(rank, world, fail_rank, case)
         queue.put((rank, "ok", r.eigenvalues.tolist(), r.residuals.tolist(), r.converged, r.applications))
     except Exception as exc:  # the planted failure, or the collective that ends because of it
         queue.put((rank, "error", f"{type(exc).__name__}: {exc}", None, None, None))
@@ -90,11 +102,11 @@ def _worker(rank, world, port, fail_rank, queue):
             dist.destroy_process_group()
 
 
-def _run(world, fail_rank=None):
+def _run(world, fail_rank=None, case="sector"):
     ctx = mp.get_context("spawn")
     queue = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, fail_rank, queue)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, fail_rank, queue, case)) for r in range(world)]
     for p in procs:
         p.start()
     out = sorted(queue.get(timeout=240) for _ in range(world))
@@ -139,3 +151,17 @@ def test_failed_rank_ends_the_other_ranks_solve():
     out = _run(2, fail_rank=1)
     assert out[1][1] == "error" and "planted slab failure" in out[1][2]
     assert out[0][1] == "error"  # the next collective fails instead of waiting forever
+
+
+def test_rank_with_an_empty_slab():
+    """Four rows over three ranks: blocks of two, so rank 2 owns no rows but
+    still takes part in every gather and reduction."""
+    part = RowPartition(4, 3)
+    assert part.range(2) == (4, 0)
+    matrix, _ = _tiny()
+    expected = np.linalg.eigvalsh(matrix.toarray())[0]
+    out = _run(3, case="tiny")
+    for rank, status, values, residuals, converged, applications in out:
+        assert status == "ok" and converged, (rank, status, values)
+        assert abs(values[0] - expected) <= 1e-10 * max(abs(expected), 1.0)
+        assert applications == out[0][5]
