@@ -310,11 +310,20 @@ class ChainSpectrum:
         Restart size: with a small predicted relative gap (E1 - E0) / (E_max - E0),
         where the thick restart converges slowly, it keeps two Ritz vectors beyond
         the wanted ones (measured at 28 sites, 6 wanted, Krylov 40: 466 -> 173
-        steps; keeping more cost time), otherwise the reference's size."""
+        steps; keeping more cost time), otherwise the reference's size.
+
+        A prediction that is not finite, or whose E_max is not above E0, gives
+        the empty hint (lower = upper = 0, no restart change, "usable" False):
+        the solver then takes its own Lanczos bounds and the reference's
+        restart size instead of failing on the prediction."""
         e0, emax, gap = self.predict(sites, j2, delta, momentum)
+        if not (np.isfinite(e0) and np.isfinite(emax) and np.isfinite(gap)) or not emax > e0:
+            return {"lower": 0.0, "upper": 0.0, "gap": 0.0, "restart_keep": 0, "check_steps": self.check_steps,
+                    "relative_gap": None, "e0": e0 if np.isfinite(e0) else None,
+                    "e_max": emax if np.isfinite(emax) else None, "usable": False}
         width = max(emax - e0, 1e-12)
         relative_gap = gap / width
         keep = min(krylov_dimension // 2, eigenpairs + 2) if relative_gap < 0.05 else 0
         return {"lower": e0 - self.margin * width, "upper": emax + self.margin * width, "gap": gap,
                 "restart_keep": keep, "check_steps": self.check_steps, "relative_gap": relative_gap,
-                "e0": e0, "e_max": emax}
+                "e0": e0, "e_max": emax, "usable": True}

@@ -45,3 +45,22 @@ def test_hint_interval_and_restart_rule(gap_times_sites, expected_keep):
 def test_negative_gap_predictions_are_clipped():
     model = learned.ChainSpectrum(mlp=_FixedNetwork(-0.44, 0.25, -1.0))
     assert model.predict(20, 0.1, 1.0, 0)[2] == 0.0
+
+
+@pytest.mark.parametrize("e0,emax,gap", [(float("nan"), 0.25, 4.0), (-0.44, float("inf"), 4.0),
+                                         (-0.44, 0.25, float("nan")), (0.3, 0.25, 4.0)])
+def test_unusable_predictions_give_the_empty_hint(e0, emax, gap):
+    """A non-finite prediction or an inverted interval must not reach the solver
+    as an interval: the hint is empty (lower = upper = 0), so the solver takes
+    its own Lanczos bounds and the reference restart size."""
+    import json
+    model = learned.ChainSpectrum(mlp=_FixedNetwork(e0, emax, gap))
+    hint = model.hint(28, 0.0, 1.0, 0, eigenpairs=6, krylov_dimension=40)
+    assert hint["usable"] is False
+    assert hint["lower"] == hint["upper"] == 0.0 and hint["gap"] == 0.0 and hint["restart_keep"] == 0
+    json.dumps(hint, allow_nan=False)  # reported values stay valid JSON
+
+
+def test_usable_prediction_is_marked():
+    model = learned.ChainSpectrum(mlp=_FixedNetwork(-0.44, 0.25, 4.0))
+    assert model.hint(28, 0.0, 1.0, 0, eigenpairs=6)["usable"] is True
