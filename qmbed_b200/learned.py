@@ -190,7 +190,7 @@ class LearnedBounds:
         pad = self.margin * (hi - lo)
         lo, hi = lo - pad, hi + pad
         ritz = lanczos_extremes(op, self.check_steps, seed)
-        if hi > lo and lo <= ritz[0] and hi >= ritz[1]:
+        if np.isfinite(lo) and np.isfinite(hi) and hi > lo and lo <= ritz[0] and hi >= ritz[1]:
             return Interval(lo, hi, "learned", self.check_steps)
         fallback = lanczos_interval(op, seed=seed)
         return Interval(fallback.e_min, fallback.e_max, "lanczos", fallback.applications + self.check_steps)

@@ -64,3 +64,33 @@ def test_unusable_predictions_give_the_empty_hint(e0, emax, gap):
 def test_usable_prediction_is_marked():
     model = learned.ChainSpectrum(mlp=_FixedNetwork(-0.44, 0.25, 4.0))
     assert model.hint(28, 0.0, 1.0, 0, eigenpairs=6)["usable"] is True
+
+
+class _FixedBoundsNetwork:
+    def __init__(self, lo_per_site, hi_per_site):
+        self.out = np.array([[lo_per_site, hi_per_site]], np.float32)
+
+    def predict(self, x):
+        assert np.asarray(x).shape[-1] == len(learned.FEATURES)
+        return self.out
+
+
+@pytest.mark.parametrize("lo,hi,source", [(-1.9, 1.9, "learned"), (-1.0, 1.0, "lanczos"),
+                                          (float("-inf"), float("inf"), "lanczos"),
+                                          (float("nan"), 1.9, "lanczos"), (1.9, -1.9, "lanczos")])
+def test_quench_interval_check(monkeypatch, lo, hi, source):
+    """The Chebyshev interval is the network's only when it is finite, ordered
+    and holds the short Lanczos run's Ritz extremes; otherwise the plain
+    Lanczos estimate replaces it."""
+    sites = 10
+    monkeypatch.setattr(learned, "lanczos_extremes", lambda op, steps, seed=0: np.array([-15.0, 15.0, 0.1, 0.1]))
+    monkeypatch.setattr(learned, "lanczos_interval",
+                        lambda op, seed=0: learned.Interval(-16.0, 16.0, "lanczos", 40))
+    bounds = learned.LearnedBounds(mlp=_FixedBoundsNetwork(lo, hi), margin=0.03, check_steps=8)
+    interval = bounds.interval(None, sites, 1.0, 1.0, np.zeros(sites))
+    assert interval.source == source
+    assert np.isfinite(interval.e_min) and np.isfinite(interval.e_max) and interval.e_min < interval.e_max
+    if source == "learned":
+        assert interval.e_min <= -15.0 and interval.e_max >= 15.0 and interval.applications == 8
+    else:
+        assert (interval.e_min, interval.e_max, interval.applications) == (-16.0, 16.0, 48)
