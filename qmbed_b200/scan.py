@@ -22,10 +22,16 @@ def scan_lowest(components, coefficients, eigenpairs: int = 2, tolerance: float 
     """components[s][k]: GpuOperator A_k of sector s (explicit storage, one basis per sector);
     coefficients: points x components. Returns (eigenvalues[s, p, eigenpairs], steps[s, p], info);
     info also holds the FP64 residual of every reported pair and the top Ritz value of every pair."""
-    sectors, k = len(components), len(components[0])
+    sectors = len(components)
+    k = len(components[0]) if sectors else 0
+    if sectors < 1 or k < 1 or any(len(row) != k for row in components):
+        raise ValueError("a scan needs at least one sector, each with the same (nonzero) number of components")
     coef = np.ascontiguousarray(coefficients, np.float64)
+    if coef.ndim != 2 or coef.shape[0] < 1 or coef.shape[1] != k:
+        raise ValueError(f"coefficients must be a (points x {k}) array; got shape {coef.shape}")
+    if eigenpairs < 1:
+        raise ValueError("eigenpairs must be at least 1")
     points = coef.shape[0]
-    assert coef.shape == (points, k)
     handles = (ctypes.c_void_p * (sectors * k))(*[op.handle.value for row in components for op in row])
     values = np.full((sectors, points, eigenpairs), np.nan)
     residuals = np.full((sectors, points, eigenpairs), np.nan)
