@@ -70,8 +70,9 @@ class GpuMlp:
         return out
 
     def set_parameters(self, params) -> None:
-        p = np.ascontiguousarray(params, np.float32)
-        assert p.size == self.parameter_count
+        p = np.ascontiguousarray(params, np.float32).ravel()
+        if p.size != self.parameter_count:
+            raise ValueError(f"expected {self.parameter_count} parameters, got {p.size}")
         check(lib().qmbed_gpu_mlp_set_parameters(self.handle, _ptr(p)))
 
     def scaling(self):
@@ -80,10 +81,23 @@ class GpuMlp:
         check(lib().qmbed_gpu_mlp_get_scaling(self.handle, *[_ptr(a) for a in arrays]))
         return arrays
 
+    def _inputs(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(np.atleast_2d(x), np.float32)
+        if x.ndim != 2 or x.shape[1] != self.inputs:
+            raise ValueError(f"inputs must be (rows x {self.inputs}); got shape {x.shape}")
+        return x
+
+    def _samples(self, x, y):
+        """(x, y) as contiguous float32 rows whose widths match the network (the library reads rows x width)."""
+        x = self._inputs(x)
+        y = np.ascontiguousarray(np.atleast_2d(y), np.float32)
+        if y.shape != (x.shape[0], self.outputs):
+            raise ValueError(f"targets must be ({x.shape[0]} x {self.outputs}); got shape {y.shape}")
+        return x, y
+
     def gradients(self, x, y):
         """Loss and parameter gradient of the unscaled network on (x, y)."""
-        x = np.ascontiguousarray(x, np.float32)
-        y = np.ascontiguousarray(y, np.float32)
+        x, y = self._samples(x, y)
         grads = np.zeros(self.parameter_count, np.float32)
         loss = ctypes.c_float()
         check(lib().qmbed_gpu_mlp_gradients(self.handle, _ptr(x), _ptr(y), x.shape[0], _ptr(grads),
@@ -91,15 +105,14 @@ class GpuMlp:
         return loss.value, grads
 
     def train(self, x, y, epochs: int = 400, batch: int = 32, learning_rate: float = 2e-3, seed: int = 0) -> float:
-        x = np.ascontiguousarray(x, np.float32)
-        y = np.ascontiguousarray(y, np.float32)
+        x, y = self._samples(x, y)
         loss = ctypes.c_float()
         check(lib().qmbed_gpu_mlp_train(self.handle, _ptr(x), _ptr(y), x.shape[0], epochs, batch, learning_rate,
                                         seed, ctypes.byref(loss)))
         return loss.value
 
     def predict(self, x) -> np.ndarray:
-        x = np.ascontiguousarray(np.atleast_2d(x), np.float32)
+        x = self._inputs(x)
         y = np.zeros((x.shape[0], self.outputs), np.float32)
         check(lib().qmbed_gpu_mlp_predict(self.handle, _ptr(x), x.shape[0], _ptr(y)))
         return y

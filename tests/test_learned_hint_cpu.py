@@ -94,3 +94,22 @@ def test_quench_interval_check(monkeypatch, lo, hi, source):
         assert interval.e_min <= -15.0 and interval.e_max >= 15.0 and interval.applications == 8
     else:
         assert (interval.e_min, interval.e_max, interval.applications) == (-16.0, 16.0, 48)
+
+
+def test_network_calls_check_shapes_before_the_library():
+    """The library reads rows x width floats from the arrays it is given, so a
+    wrong width is refused in Python before any call (a network shell without
+    a device handle is enough to show it)."""
+    net = object.__new__(learned.GpuMlp)
+    net.inputs, net.outputs, net.handle = 6, 3, None
+    good_x, good_y = np.zeros((4, 6), np.float32), np.zeros((4, 3), np.float32)
+    with pytest.raises(ValueError):
+        net.predict(np.zeros((4, 5)))
+    with pytest.raises(ValueError):
+        net.train(np.zeros((4, 7)), good_y)
+    with pytest.raises(ValueError):
+        net.train(good_x, np.zeros((4, 2)))
+    with pytest.raises(ValueError):
+        net.gradients(good_x, np.zeros((5, 3)))
+    x, y = net._samples(good_x[0], good_y[0])  # one sample as 1-D rows
+    assert x.shape == (1, 6) and y.shape == (1, 3)
