@@ -11,7 +11,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import EigshHintC, EigshInfoC, EigshOptionsC, QmbedError, check, lib
+from ._lib import STATUS, EigshHintC, EigshInfoC, EigshOptionsC, QmbedError, check, lib
 
 NORMALIZATIONS = {"angular_momentum": 0, "pauli": 1, "pauli_cartesian": 2}
 TARGETS = {
@@ -29,6 +29,18 @@ EVOLUTION_DIAGNOSTICS = ("lanczos_projections", "matrix_vector_products", "real_
 STORAGE = {"matrix_free": 0, "packed": 1, "explicit": 2}
 LOOKUPS = {"auto": 0, "table": 1, "search": 2, "legacy": 3, "table_generic": 4}
 LOOKUPS_IN_USE = {1: "table", 2: "search", 3: "legacy", 4: "index", 5: "table_hop"}
+
+
+def _sector_vectors(x, dim: int, dtype, what: str, batch: bool = False) -> np.ndarray:
+    """x as contiguous `dtype` vectors of the sector's length (one vector, or rows
+    of vectors with `batch`). The host entries read `dim` values per vector from
+    the buffer they are given, so another length is refused here with the
+    library's dimension-mismatch error instead of being read past its end."""
+    arr = np.ascontiguousarray(np.atleast_2d(x) if batch else np.asarray(x), dtype)
+    if arr.ndim != (2 if batch else 1) or arr.shape[-1] != dim:
+        raise QmbedError(f"dimension mismatch: {what} has shape {tuple(np.shape(x))}, the sector dimension is {dim}",
+                         STATUS["dimension_mismatch"])
+    return arr
 
 
 def _ptr(array):
@@ -188,12 +200,8 @@ class GpuOperator:
         """y = H x on host vectors (FP64). Real input uses the real action when possible."""
         x = np.asarray(x)
         complex_vectors = np.iscomplexobj(x) or not self.is_real
-        if complex_vectors:
-            xin = np.ascontiguousarray(x, np.complex128)
-            y = np.zeros_like(xin)
-        else:
-            xin = np.ascontiguousarray(x, np.float64)
-            y = np.zeros_like(xin)
+        xin = _sector_vectors(x, self.dim, np.complex128 if complex_vectors else np.float64, "the input vector")
+        y = np.zeros_like(xin)
         check(lib().qmbed_gpu_operator_apply_host(self.handle, int(complex_vectors), _ptr(xin), _ptr(y),
                                                   int(force_matrix_free)))
         return y
@@ -272,7 +280,7 @@ class GpuOperator:
         options = EigshOptionsC(eigenpairs, TARGETS[target], shift, krylov_dimension or 0, tolerance, max_iterations,
                                 seed, MODES[mode])
         if initial is not None:
-            initial = np.ascontiguousarray(np.atleast_2d(np.asarray(initial, np.complex128)))
+            initial = _sector_vectors(initial, n, np.complex128, "the initial vectors", batch=True)
             n_initial = initial.shape[0]
         else:
             n_initial = 0
@@ -297,7 +305,7 @@ class GpuOperator:
         """exp(-i H t) initial on a nondecreasing time grid (reference evolve).
 
         Returns (states[n_times, dim], diagnostics dict)."""
-        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        x = _sector_vectors(initial, self.dim, np.complex128, "the initial state")
         t = np.ascontiguousarray(np.asarray(times, np.float64))
         states = np.zeros((len(t), self.dim), np.complex128)
         diag = np.zeros(7)
@@ -307,7 +315,7 @@ class GpuOperator:
 
     def expm_lanczos(self, initial, time: float, krylov_dimension: int = 30) -> np.ndarray:
         """exp(-i H time) initial from one Lanczos projection (reference expm_lanczos)."""
-        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        x = _sector_vectors(initial, self.dim, np.complex128, "the initial state")
         y = np.zeros(self.dim, np.complex128)
         check(lib().qmbed_gpu_expm_lanczos(self.handle, _ptr(x), time, krylov_dimension, _ptr(y)))
         return y
@@ -318,7 +326,7 @@ class GpuOperator:
 
         [e_min, e_max] must contain the spectrum; NaN uses the guaranteed
         +-sum|coefficients| bound. Returns (states[n_times or 1, dim], info dict)."""
-        x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+        x = _sector_vectors(initial, self.dim, np.complex128, "the initial state")
         t = np.ascontiguousarray(np.asarray(times, np.float64))
         states = np.zeros((1 if final_only else len(t), self.dim), np.complex128)
         info = np.zeros(5)
@@ -351,7 +359,7 @@ class GpuOperator:
     def expm_apply(self, coefficient: complex, vectors, max_degree: int = 55,
                    tolerance: float = 0.5 * np.finfo(float).eps, max_substeps: int = 10_000,
                    precision: int = 64) -> np.ndarray:
-        x = np.ascontiguousarray(np.atleast_2d(np.asarray(vectors, np.complex128)))
+        x = _sector_vectors(vectors, self.dim, np.complex128, "the input vectors", batch=True)
         y = np.zeros_like(x)
         coefficient = complex(coefficient)
         check(lib().qmbed_gpu_expm_apply_host(self.handle, coefficient.real, coefficient.imag, max_degree, tolerance,
