@@ -43,6 +43,27 @@ def _sector_vectors(x, dim: int, dtype, what: str, batch: bool = False) -> np.nd
     return arr
 
 
+def _device_operands(need_bytes: int, *operands) -> None:
+    """Refuses torch tensors that the kernels cannot use: one smaller than
+    `need_bytes`, one that is not contiguous (the kernels read and write the
+    dense span from data_ptr()), or one off the GPU. `operands` are
+    (description, tensor) pairs; sizes and layouts are checked for all of them
+    before devices. Objects without these attributes (any other holder of a
+    device pointer) are the caller's to size."""
+    tensors = [(what, t) for what, t in operands
+               if t is not None and hasattr(t, "numel") and hasattr(t, "element_size")]
+    for what, t in tensors:
+        have = int(t.numel()) * int(t.element_size())
+        if have < need_bytes:
+            raise QmbedError(f"dimension mismatch: {what} holds {have} bytes, the action needs {need_bytes}",
+                             STATUS["dimension_mismatch"])
+        if hasattr(t, "is_contiguous") and not t.is_contiguous():
+            raise QmbedError(f"invalid options: {what} must be contiguous", STATUS["invalid_options"])
+    for what, t in tensors:
+        if getattr(t, "is_cuda", True) is False:
+            raise QmbedError(f"invalid options: {what} must be a CUDA tensor", STATUS["invalid_options"])
+
+
 def _ptr(array):
     if array is None:
         return None
@@ -192,6 +213,16 @@ class GpuOperator:
     def dim(self) -> int:
         return self.info()["dimension"]
 
+    def _rows(self) -> int:
+        """The sector dimension, read once (it never changes for an operator)."""
+        n = self.__dict__.get("_rows_cache")
+        if n is None:
+            n = self._rows_cache = int(self.dim)
+        return n
+
+    def _vector_bytes(self, precision: int, complex_vectors: bool, columns: int = 1) -> int:
+        return self._rows() * columns * (8 if precision == 64 else 4) * (2 if complex_vectors else 1)
+
     @property
     def is_real(self) -> bool:
         return self.info()["is_real"]
@@ -209,6 +240,8 @@ class GpuOperator:
     def apply_device(self, x, y, precision: int = 64, complex_vectors: bool = False, stream=None,
                      force_matrix_free: bool = False) -> None:
         """y = H x on device tensors (``data_ptr()``), FP64 or FP32."""
+        _device_operands(self._vector_bytes(precision, complex_vectors), ("the input vector", x),
+                         ("the output vector", y))
         check(lib().qmbed_gpu_operator_apply_device(self.handle, precision, int(complex_vectors), _ptr(x), _ptr(y),
                                                     None if stream is None else ctypes.c_void_p(stream),
                                                     int(force_matrix_free)))
@@ -220,6 +253,8 @@ class GpuOperator:
         Coordinates are orbit-scaled (z = x / sqrt(R) in symmetry sectors); real
         operators with packed or matrix-free storage.
         """
+        _device_operands(self._vector_bytes(precision, False, nb), ("the input block", z), ("the output block", out),
+                         ("the third block", p))
         check(lib().qmbed_gpu_operator_apply_block_device(self.handle, precision, nb, _ptr(z), _ptr(p), _ptr(out),
                                                           alpha, beta, gamma,
                                                           None if stream is None else ctypes.c_void_p(stream)))
@@ -231,6 +266,8 @@ class GpuOperator:
         symmetry sectors goes to a fixed 32 MiB device array shared by all
         calls, so vectors are limited to 32 MiB and concurrent calls race.
         """
+        _device_operands(self._vector_bytes(precision, complex_vectors), ("the input vector", x),
+                         ("the output vector", y))
         check(lib().qmbed_gpu_operator_apply_device_noalloc(self.handle, precision, int(complex_vectors), _ptr(x),
                                                             _ptr(y), None if stream is None else ctypes.c_void_p(stream)))
 
@@ -339,6 +376,7 @@ class GpuOperator:
                                 tolerance: float = 1e-10, precision: int = 64) -> dict:
         """In place on a device complex128 tensor (``data_ptr()``): state <- exp(-i H t_last) state,
         stepping through `times`. Returns the info dict of chebyshev_evolve."""
+        _device_operands(self._vector_bytes(64, True), ("the state", state))
         t = np.ascontiguousarray(np.asarray(times, np.float64))
         info = np.zeros(5)
         check(lib().qmbed_gpu_chebyshev_evolve_device(self.handle, _ptr(state), len(t), _ptr(t), e_min, e_max,

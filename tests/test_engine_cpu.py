@@ -44,3 +44,32 @@ def test_sector_vectors_shapes():
     assert rows.shape == (1, 3)
     rows = engine._sector_vectors(np.ones((4, 3)), 3, np.float64, "x", batch=True)
     assert rows.shape == (4, 3)
+
+
+@pytest.mark.parametrize("call,code", [
+    (lambda op, t: op.apply_device(t.zeros(5, dtype=t.float64), t.zeros(6, dtype=t.float64)), 9),
+    (lambda op, t: op.apply_device(t.zeros(6, dtype=t.float32), t.zeros(6, dtype=t.float32), precision=64), 9),
+    (lambda op, t: op.apply_device(t.zeros(6, dtype=t.float64), t.zeros(6, dtype=t.float64),
+                                   complex_vectors=True), 9),
+    (lambda op, t: op.apply_device(t.zeros(24, dtype=t.float64)[::2], t.zeros(6, dtype=t.float64)), 8),
+    (lambda op, t: op.apply_device_noalloc(t.zeros(6, dtype=t.float64), t.zeros(5, dtype=t.float64)), 9),
+    (lambda op, t: op.apply_block_device(t.zeros(48), t.zeros(47), nb=8, precision=32), 9),
+    (lambda op, t: op.apply_block_device(t.zeros(48), t.zeros(48), nb=8, precision=32, p=t.zeros(40)), 9),
+    (lambda op, t: op.chebyshev_evolve_device(t.zeros(6, dtype=t.complex64), [1.0]), 9),
+])
+def test_device_operands_are_checked_before_the_library(call, code):
+    """Device entries refuse tensors smaller than the action's span (status 9)
+    and strided views (status 8) before looking at the device, so CPU tensors
+    show both checks here."""
+    import torch
+    with pytest.raises(QmbedError) as e:
+        call(_Operator(), torch)
+    assert e.value.code == code, str(e.value)
+    assert "CUDA tensor" not in str(e.value)
+
+
+def test_host_tensors_are_refused_by_device_entries():
+    import torch
+    with pytest.raises(QmbedError) as e:
+        _Operator().apply_device(torch.zeros(6, dtype=torch.float64), torch.zeros(6, dtype=torch.float64))
+    assert e.value.code == 8 and "CUDA tensor" in str(e.value)
