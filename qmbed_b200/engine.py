@@ -43,23 +43,23 @@ def _sector_vectors(x, dim: int, dtype, what: str, batch: bool = False) -> np.nd
     return arr
 
 
-def _device_operands(need_bytes: int, *operands) -> None:
-    """Refuses torch tensors that the kernels cannot use: one smaller than
-    `need_bytes`, one that is not contiguous (the kernels read and write the
-    dense span from data_ptr()), or one off the GPU. `operands` are
-    (description, tensor) pairs; sizes and layouts are checked for all of them
-    before devices. Objects without these attributes (any other holder of a
-    device pointer) are the caller's to size."""
-    tensors = [(what, t) for what, t in operands
+def _device_operands(*operands) -> None:
+    """Refuses torch tensors that the kernels cannot use: one smaller than the
+    bytes the action reads or writes through it, one that is not contiguous
+    (the kernels use the dense span from data_ptr()), or one off the GPU.
+    `operands` are (description, tensor, bytes) triples; sizes and layouts are
+    checked for all of them before devices. Objects without these attributes
+    (any other holder of a device pointer) are the caller's to size."""
+    tensors = [(what, t, need) for what, t, need in operands
                if t is not None and hasattr(t, "numel") and hasattr(t, "element_size")]
-    for what, t in tensors:
+    for what, t, need in tensors:
         have = int(t.numel()) * int(t.element_size())
-        if have < need_bytes:
-            raise QmbedError(f"dimension mismatch: {what} holds {have} bytes, the action needs {need_bytes}",
+        if have < need:
+            raise QmbedError(f"dimension mismatch: {what} holds {have} bytes, the action needs {need}",
                              STATUS["dimension_mismatch"])
         if hasattr(t, "is_contiguous") and not t.is_contiguous():
             raise QmbedError(f"invalid options: {what} must be contiguous", STATUS["invalid_options"])
-    for what, t in tensors:
+    for what, t, _ in tensors:
         if getattr(t, "is_cuda", True) is False:
             raise QmbedError(f"invalid options: {what} must be a CUDA tensor", STATUS["invalid_options"])
 
@@ -240,8 +240,8 @@ class GpuOperator:
     def apply_device(self, x, y, precision: int = 64, complex_vectors: bool = False, stream=None,
                      force_matrix_free: bool = False) -> None:
         """y = H x on device tensors (``data_ptr()``), FP64 or FP32."""
-        _device_operands(self._vector_bytes(precision, complex_vectors), ("the input vector", x),
-                         ("the output vector", y))
+        need = self._vector_bytes(precision, complex_vectors)
+        _device_operands(("the input vector", x, need), ("the output vector", y, need))
         check(lib().qmbed_gpu_operator_apply_device(self.handle, precision, int(complex_vectors), _ptr(x), _ptr(y),
                                                     None if stream is None else ctypes.c_void_p(stream),
                                                     int(force_matrix_free)))
@@ -253,8 +253,8 @@ class GpuOperator:
         Coordinates are orbit-scaled (z = x / sqrt(R) in symmetry sectors); real
         operators with packed or matrix-free storage.
         """
-        _device_operands(self._vector_bytes(precision, False, nb), ("the input block", z), ("the output block", out),
-                         ("the third block", p))
+        need = self._vector_bytes(precision, False, nb)
+        _device_operands(("the input block", z, need), ("the output block", out, need), ("the third block", p, need))
         check(lib().qmbed_gpu_operator_apply_block_device(self.handle, precision, nb, _ptr(z), _ptr(p), _ptr(out),
                                                           alpha, beta, gamma,
                                                           None if stream is None else ctypes.c_void_p(stream)))
@@ -266,8 +266,8 @@ class GpuOperator:
         symmetry sectors goes to a fixed 32 MiB device array shared by all
         calls, so vectors are limited to 32 MiB and concurrent calls race.
         """
-        _device_operands(self._vector_bytes(precision, complex_vectors), ("the input vector", x),
-                         ("the output vector", y))
+        need = self._vector_bytes(precision, complex_vectors)
+        _device_operands(("the input vector", x, need), ("the output vector", y, need))
         check(lib().qmbed_gpu_operator_apply_device_noalloc(self.handle, precision, int(complex_vectors), _ptr(x),
                                                             _ptr(y), None if stream is None else ctypes.c_void_p(stream)))
 
@@ -376,7 +376,7 @@ class GpuOperator:
                                 tolerance: float = 1e-10, precision: int = 64) -> dict:
         """In place on a device complex128 tensor (``data_ptr()``): state <- exp(-i H t_last) state,
         stepping through `times`. Returns the info dict of chebyshev_evolve."""
-        _device_operands(self._vector_bytes(64, True), ("the state", state))
+        _device_operands(("the state", state, self._vector_bytes(64, True)))
         t = np.ascontiguousarray(np.asarray(times, np.float64))
         info = np.zeros(5)
         check(lib().qmbed_gpu_chebyshev_evolve_device(self.handle, _ptr(state), len(t), _ptr(t), e_min, e_max,

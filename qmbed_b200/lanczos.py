@@ -22,7 +22,7 @@ import ctypes
 import numpy as np
 
 from ._lib import check, lib
-from .engine import GpuOperator, _ptr
+from .engine import GpuOperator, _ptr, _sector_vectors
 
 METHODS = {"ftlm": 0, "ltlm": 1}
 
@@ -31,9 +31,7 @@ class LanczosBasis:
     """Device-resident Lanczos decomposition (the reference's LanczosRitzDecomposition)."""
 
     def __init__(self, op: GpuOperator, v0, m: int, eps: float = 1e-13):
-        x = np.ascontiguousarray(np.asarray(v0, np.complex128))
-        if x.ndim != 1:
-            raise ValueError("v0 must be one-dimensional")
+        x = _sector_vectors(v0, op.dim, np.complex128, "v0")
         handle = ctypes.c_void_p()
         check(lib().qmbed_gpu_lanczos_create(op.handle, _ptr(x), int(m), float(eps), ctypes.byref(handle)))
         self._handle = handle
@@ -221,7 +219,7 @@ def LTLM_static_iteration(O_dict, E, V, Q_T, beta=0):
 def thermal_iteration(op: GpuOperator, initial, inverse_temperatures, krylov_dimension: int,
                       tolerance: float = 1e-12):
     """ftlm_static_iteration (src/solve/mod.rs:3543-3554): (log_partition, mean_energy, krylov_dimension)."""
-    x = np.ascontiguousarray(np.asarray(initial, np.complex128))
+    x = _sector_vectors(initial, op.dim, np.complex128, "the initial vector")
     b = np.ascontiguousarray(np.atleast_1d(np.asarray(inverse_temperatures, np.float64)))
     lz, e = np.zeros(max(b.size, 1)), np.zeros(max(b.size, 1))
     size = ctypes.c_uint64()

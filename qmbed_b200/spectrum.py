@@ -16,7 +16,7 @@ import ctypes
 import numpy as np
 
 from ._lib import check, lib
-from .engine import GpuBasis, GpuOperator, _ptr, encode_terms
+from .engine import GpuBasis, GpuOperator, _device_operands, _ptr, encode_terms
 
 
 class SectorShift:
@@ -49,6 +49,8 @@ class SectorShift:
 
     def apply_device(self, x, y, stream=None) -> None:
         """y = shift(x) on device tensors (complex128 ``data_ptr()``)."""
+        _device_operands(("the source-sector vector", x, 16 * len(self.source)),
+                         ("the target-sector vector", y, 16 * len(self.target)))
         check(lib().qmbed_gpu_shift_apply_device(self.handle, _ptr(x), _ptr(y),
                                                  None if stream is None else ctypes.c_void_p(stream)))
 

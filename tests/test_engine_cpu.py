@@ -73,3 +73,34 @@ def test_host_tensors_are_refused_by_device_entries():
     with pytest.raises(QmbedError) as e:
         _Operator().apply_device(torch.zeros(6, dtype=torch.float64), torch.zeros(6, dtype=torch.float64))
     assert e.value.code == 8 and "CUDA tensor" in str(e.value)
+
+
+def test_lanczos_entries_check_the_vector_length():
+    from qmbed_b200 import lanczos
+    for call in (lambda: lanczos.LanczosBasis(_Operator(), np.zeros(5), 4),
+                 lambda: lanczos.thermal_iteration(_Operator(), np.zeros(7), [1.0], 4)):
+        with pytest.raises(QmbedError) as e:
+            call()
+        assert e.value.code == 9
+
+
+def test_sector_shift_and_row_slab_device_operands():
+    import torch
+    from qmbed_b200 import spectrum
+    from qmbed_b200.distributed import RowPartition, gpu_slab
+    shift = object.__new__(spectrum.SectorShift)
+    shift.handle, shift.source, shift.target = None, [0] * 6, [0] * 4
+    with pytest.raises(QmbedError) as e:
+        shift.apply_device(torch.zeros(5, dtype=torch.complex128), torch.zeros(4, dtype=torch.complex128))
+    assert e.value.code == 9 and "source-sector" in str(e.value)
+    with pytest.raises(QmbedError) as e:
+        shift.apply_device(torch.zeros(6, dtype=torch.complex128), torch.zeros(3, dtype=torch.complex128))
+    assert e.value.code == 9 and "target-sector" in str(e.value)
+    part = RowPartition(10, 3)  # blocks of 4: rank 1 owns rows 4..7
+    slab = gpu_slab(_Operator(), part, 1, precision=64)
+    with pytest.raises(QmbedError) as e:
+        slab(torch.zeros(9, dtype=torch.float64), torch.zeros(4, dtype=torch.float64))
+    assert e.value.code == 9 and "gathered" in str(e.value)
+    with pytest.raises(QmbedError) as e:
+        slab(torch.zeros(12, dtype=torch.float64), torch.zeros(3, dtype=torch.float64))
+    assert e.value.code == 9 and "slab output" in str(e.value)
