@@ -119,9 +119,12 @@ class GpuBasis:
         return lo, hi, orbit
 
     def images(self, lo, hi=None):
-        lo = np.ascontiguousarray(lo, np.uint64)
-        hi = None if hi is None else np.ascontiguousarray(hi, np.uint64)
+        lo = np.ascontiguousarray(np.atleast_1d(lo), np.uint64)
+        hi = None if hi is None else np.ascontiguousarray(np.atleast_1d(hi), np.uint64)
         n = len(lo)
+        if lo.ndim != 1 or (hi is not None and hi.shape != lo.shape):
+            raise QmbedError("dimension mismatch: the high state words must match the low ones one to one",
+                             STATUS["dimension_mismatch"])
         index = np.zeros(n, np.int64)
         phase = np.zeros(n, np.complex128)
         orbit = np.zeros(n, np.uint16)

@@ -104,3 +104,11 @@ def test_sector_shift_and_row_slab_device_operands():
     with pytest.raises(QmbedError) as e:
         slab(torch.zeros(12, dtype=torch.float64), torch.zeros(3, dtype=torch.float64))
     assert e.value.code == 9 and "slab output" in str(e.value)
+
+
+def test_images_need_matching_state_words():
+    basis = object.__new__(engine.GpuBasis)
+    basis.handle = None
+    with pytest.raises(QmbedError) as e:
+        basis.images(np.arange(4), np.zeros(3))
+    assert e.value.code == 9
