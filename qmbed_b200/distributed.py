@@ -66,7 +66,8 @@ def gpu_slab(op, part: RowPartition, rank: int, precision: int = 64):
     scalar = 8 if precision == 64 else 4
 
     def apply(x_full, y_slab):
-        _device_operands(("the gathered vector", x_full, part.dim * scalar), ("the slab output", y_slab, rows * scalar))
+        _device_operands(("the gathered vector", x_full, part.dim * scalar), ("the slab output", y_slab, rows * scalar),
+                         device=getattr(getattr(op, "basis", None), "device", None))
         stream = torch.cuda.current_stream(x_full.device).cuda_stream
         check(lib().qmbed_gpu_operator_apply_rows_device(op.handle, precision, row0, rows,
                                                          ctypes.c_void_p(x_full.data_ptr()),

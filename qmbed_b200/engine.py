@@ -43,13 +43,14 @@ def _sector_vectors(x, dim: int, dtype, what: str, batch: bool = False) -> np.nd
     return arr
 
 
-def _device_operands(*operands) -> None:
+def _device_operands(*operands, device: int | None = None) -> None:
     """Refuses torch tensors that the kernels cannot use: one smaller than the
     bytes the action reads or writes through it, one that is not contiguous
-    (the kernels use the dense span from data_ptr()), or one off the GPU.
-    `operands` are (description, tensor, bytes) triples; sizes and layouts are
-    checked for all of them before devices. Objects without these attributes
-    (any other holder of a device pointer) are the caller's to size."""
+    (the kernels use the dense span from data_ptr()), one off the GPU, or one
+    on another GPU than `device` (the operator's). `operands` are
+    (description, tensor, bytes) triples; sizes and layouts are checked for
+    all of them before devices. Objects without these attributes (any other
+    holder of a device pointer) are the caller's to size."""
     tensors = [(what, t, need) for what, t, need in operands
                if t is not None and hasattr(t, "numel") and hasattr(t, "element_size")]
     for what, t, need in tensors:
@@ -62,6 +63,10 @@ def _device_operands(*operands) -> None:
     for what, t, _ in tensors:
         if getattr(t, "is_cuda", True) is False:
             raise QmbedError(f"invalid options: {what} must be a CUDA tensor", STATUS["invalid_options"])
+        index = getattr(getattr(t, "device", None), "index", None)
+        if device is not None and index is not None and index != device:
+            raise QmbedError(f"invalid options: {what} is on cuda:{index}, the operator on cuda:{device}",
+                             STATUS["invalid_options"])
 
 
 def _ptr(array):
@@ -223,6 +228,9 @@ class GpuOperator:
             n = self._rows_cache = int(self.dim)
         return n
 
+    def _device(self) -> int | None:
+        return getattr(getattr(self, "basis", None), "device", None)
+
     def _vector_bytes(self, precision: int, complex_vectors: bool, columns: int = 1) -> int:
         return self._rows() * columns * (8 if precision == 64 else 4) * (2 if complex_vectors else 1)
 
@@ -244,7 +252,7 @@ class GpuOperator:
                      force_matrix_free: bool = False) -> None:
         """y = H x on device tensors (``data_ptr()``), FP64 or FP32."""
         need = self._vector_bytes(precision, complex_vectors)
-        _device_operands(("the input vector", x, need), ("the output vector", y, need))
+        _device_operands(("the input vector", x, need), ("the output vector", y, need), device=self._device())
         check(lib().qmbed_gpu_operator_apply_device(self.handle, precision, int(complex_vectors), _ptr(x), _ptr(y),
                                                     None if stream is None else ctypes.c_void_p(stream),
                                                     int(force_matrix_free)))
@@ -257,7 +265,8 @@ class GpuOperator:
         operators with packed or matrix-free storage.
         """
         need = self._vector_bytes(precision, False, nb)
-        _device_operands(("the input block", z, need), ("the output block", out, need), ("the third block", p, need))
+        _device_operands(("the input block", z, need), ("the output block", out, need), ("the third block", p, need),
+                         device=self._device())
         check(lib().qmbed_gpu_operator_apply_block_device(self.handle, precision, nb, _ptr(z), _ptr(p), _ptr(out),
                                                           alpha, beta, gamma,
                                                           None if stream is None else ctypes.c_void_p(stream)))
@@ -270,7 +279,7 @@ class GpuOperator:
         calls, so vectors are limited to 32 MiB and concurrent calls race.
         """
         need = self._vector_bytes(precision, complex_vectors)
-        _device_operands(("the input vector", x, need), ("the output vector", y, need))
+        _device_operands(("the input vector", x, need), ("the output vector", y, need), device=self._device())
         check(lib().qmbed_gpu_operator_apply_device_noalloc(self.handle, precision, int(complex_vectors), _ptr(x),
                                                             _ptr(y), None if stream is None else ctypes.c_void_p(stream)))
 
@@ -379,7 +388,7 @@ class GpuOperator:
                                 tolerance: float = 1e-10, precision: int = 64) -> dict:
         """In place on a device complex128 tensor (``data_ptr()``): state <- exp(-i H t_last) state,
         stepping through `times`. Returns the info dict of chebyshev_evolve."""
-        _device_operands(("the state", state, self._vector_bytes(64, True)))
+        _device_operands(("the state", state, self._vector_bytes(64, True)), device=self._device())
         t = np.ascontiguousarray(np.asarray(times, np.float64))
         info = np.zeros(5)
         check(lib().qmbed_gpu_chebyshev_evolve_device(self.handle, _ptr(state), len(t), _ptr(t), e_min, e_max,

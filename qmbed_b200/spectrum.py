@@ -50,7 +50,8 @@ class SectorShift:
     def apply_device(self, x, y, stream=None) -> None:
         """y = shift(x) on device tensors (complex128 ``data_ptr()``)."""
         _device_operands(("the source-sector vector", x, 16 * len(self.source)),
-                         ("the target-sector vector", y, 16 * len(self.target)))
+                         ("the target-sector vector", y, 16 * len(self.target)),
+                         device=getattr(self.source, "device", None))
         check(lib().qmbed_gpu_shift_apply_device(self.handle, _ptr(x), _ptr(y),
                                                  None if stream is None else ctypes.c_void_p(stream)))
 

@@ -112,3 +112,32 @@ def test_images_need_matching_state_words():
     with pytest.raises(QmbedError) as e:
         basis.images(np.arange(4), np.zeros(3))
     assert e.value.code == 9
+
+
+class _FakeCudaTensor:
+    """A CUDA tensor's size, layout and device attributes, for the host checks."""
+
+    def __init__(self, numel, element_size, index):
+        self._numel, self._element_size = numel, element_size
+        self.is_cuda = True
+        self.device = type("Device", (), {"index": index})()
+
+    def numel(self):
+        return self._numel
+
+    def element_size(self):
+        return self._element_size
+
+    def is_contiguous(self):
+        return True
+
+    def data_ptr(self):
+        return 0
+
+
+def test_tensors_on_another_gpu_are_refused():
+    op = _Operator()
+    op.basis = type("Basis", (), {"device": 0})()
+    with pytest.raises(QmbedError) as e:
+        op.apply_device(_FakeCudaTensor(6, 8, 0), _FakeCudaTensor(6, 8, 1))
+    assert e.value.code == 8 and "cuda:1" in str(e.value)
