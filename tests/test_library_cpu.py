@@ -122,3 +122,24 @@ def test_missing_library_fails_loudly(tmp_path):
     out = subprocess.run(["python", "-c", code, str(tmp_path / "missing.so")], capture_output=True, text=True,
                          cwd=ROOT)
     assert "raised" in out.stdout and "not found" in out.stdout
+
+
+def test_ctypes_bindings_match_the_header(library):
+    """Every function the header declares is bound in qmbed_b200._lib with as
+    many argument types as the declaration has parameters (a drifted binding
+    would pass arguments in the wrong slots). The three callback exports are
+    bound by the reference's own frontend, not by this package."""
+    text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "qmbed_b200.h").read_text(), flags=re.S)
+    declared = {}
+    for m in re.finditer(r"QMBED_API\s+[\w\s\*]+?\b(qmbed_\w+)\s*\((.*?)\)\s*;", text, flags=re.S):
+        params = m.group(2).strip()
+        declared[m.group(1)] = 0 if params in ("", "void") else len(params.split(","))
+    assert len(declared) == len(declared_symbols())
+    frontend_only = {"qmbed_evolve_model_with_drive_json", "qmbed_register_user_basis_32_json",
+                     "qmbed_register_user_basis_64_json"}
+    for name, count in declared.items():
+        argtypes = getattr(getattr(library, name), "argtypes", None)
+        if name in frontend_only or (argtypes is None and count == 0):
+            continue
+        assert argtypes is not None, f"{name} has no argtypes"
+        assert len(argtypes) == count, (name, len(argtypes), count)
