@@ -143,3 +143,27 @@ def test_ctypes_bindings_match_the_header(library):
             continue
         assert argtypes is not None, f"{name} has no argtypes"
         assert len(argtypes) == count, (name, len(argtypes), count)
+
+
+def test_header_is_plain_c_with_the_binding_layouts(tmp_path):
+    """The boundary header compiles as strict C99, and its structs have the
+    sizes and field offsets the ctypes binding uses."""
+    from qmbed_b200._lib import EigshHintC, EigshInfoC, EigshOptionsC
+    fields = {"qmbed_eigsh_options": EigshOptionsC, "qmbed_eigsh_info": EigshInfoC, "qmbed_eigsh_hint": EigshHintC}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "qmbed_b200.h"', "int main(void) {"]
+    for struct, binding in fields.items():
+        lines.append(f'  printf("{struct} %zu\\n", sizeof({struct}));')
+        for name, _ in binding._fields_:
+            lines.append(f'  printf("{struct}.{name} %zu\\n", offsetof({struct}, {name}));')
+    lines += ["  return 0;", "}"]
+    source = tmp_path / "layout.c"
+    source.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", str(ROOT / "include"),
+                    "-o", str(exe), str(source)], check=True, capture_output=True, text=True)
+    out = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                              text=True).stdout.split("\n") if line)
+    for struct, binding in fields.items():
+        assert int(out[struct]) == ctypes.sizeof(binding), struct
+        for name, _ in binding._fields_:
+            assert int(out[f"{struct}.{name}"]) == getattr(binding, name).offset, (struct, name)
