@@ -165,3 +165,25 @@ def test_rank_with_an_empty_slab():
         assert status == "ok" and converged, (rank, status, values)
         assert abs(values[0] - expected) <= 1e-10 * max(abs(expected), 1.0)
         assert applications == out[0][5]
+
+
+def test_partition_property():
+    """For any dimension and rank count: slabs are disjoint, cover every row in
+    order, and slab r starts at r * block in the gathered buffer."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=300, deadline=None)
+    @given(st.integers(1, 10**9), st.integers(1, 4096))
+    def check(dim, world):
+        part = RowPartition(dim, world)
+        assert (part.block - 1) * world < dim <= part.block * world  # block = ceil(dim / world)
+        end = 0
+        for r in range(world):
+            r0, rows = part.range(r)
+            assert rows >= 0 and r0 + rows <= dim
+            if rows:
+                assert r0 == end == r * part.block
+                end = r0 + rows
+        assert end == dim
+
+    check()
